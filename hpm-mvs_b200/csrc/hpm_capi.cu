@@ -1,0 +1,645 @@
+/*
+ * C ABI of the B200-native HPM-MVS PatchMatch path: context, device memory
+ * and pass orchestration.  Declarations and the reference interfaces they
+ * replace: include/hpm_b200.h.
+ *
+ * Memory: a context owns one set of device buffers sized for the largest
+ * problem it has seen (images, optional geometric depth maps, hypotheses,
+ * costs, view masks, prior planes and masks).  Nothing is freed between
+ * passes or problems, unlike the reference which allocates and frees every
+ * buffer per problem (HPM.cpp:591-700, 1283-1307).  All work is issued on the
+ * context's stream; the only host synchronisations are in the calls that
+ * return data to the host.
+ */
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "hpm_internal.h"
+
+using namespace hpm;
+
+struct hpm_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    char err[512] = {0};
+
+    int n = 0;
+    HpmCamera cams[kMaxViews];
+    float *d_img[kMaxViews] = {nullptr};
+    size_t img_cap[kMaxViews] = {0};
+    cudaArray_t arr[kMaxViews] = {nullptr};
+    int arr_w[kMaxViews] = {0}, arr_h[kMaxViews] = {0};
+    cudaTextureObject_t tex[kMaxViews] = {0};
+    float *d_depth[kMaxViews] = {nullptr};
+    size_t depth_cap[kMaxViews] = {0};
+    bool has_depth = false;
+    PairGeom *d_pair = nullptr;
+
+    float4 *d_planes = nullptr;
+    float *d_costs = nullptr;
+    uint32_t *d_views = nullptr;
+    float4 *d_prior = nullptr;
+    uint32_t *d_masks = nullptr;
+    size_t px_cap = 0;
+    bool has_prior = false;
+    bool has_state = false;
+
+    unsigned long long *d_counters = nullptr;
+    bool counting = false;
+
+    bool profiling = false;
+    std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> prof_events;
+    float prof_ms[4] = {0, 0, 0, 0};
+    int prof_cnt[4] = {0, 0, 0, 0};
+
+    uint32_t pass_counter = 0;
+
+    void *d_scratch = nullptr;
+    size_t scratch_cap = 0;
+};
+
+namespace {
+
+int fail(hpm_ctx *c, int code, const char *fmt, ...)
+{
+    if (c) {
+        va_list ap;
+        va_start(ap, fmt);
+        vsnprintf(c->err, sizeof(c->err), fmt, ap);
+        va_end(ap);
+    }
+    return code;
+}
+
+int cuda_fail(hpm_ctx *c, cudaError_t e, const char *what)
+{
+    return fail(c, e == cudaErrorMemoryAllocation ? HPM_ERR_NOMEM : HPM_ERR_CUDA, "%s: %s", what,
+                cudaGetErrorString(e));
+}
+
+#define CK(call, what)                                   \
+    do {                                                 \
+        cudaError_t e_ = (call);                         \
+        if (e_ != cudaSuccess) return cuda_fail(c, e_, what); \
+    } while (0)
+
+cudaError_t ensure(void **p, size_t *cap, size_t bytes)
+{
+    if (*cap >= bytes && *p) return cudaSuccess;
+    if (*p) cudaFree(*p);
+    *p = nullptr;
+    *cap = 0;
+    cudaError_t e = cudaMalloc(p, bytes);
+    if (e == cudaSuccess) *cap = bytes;
+    return e;
+}
+
+/* Float cudaArray + texture object of view i with the reference's sampling
+ * state (HPM.cpp:599-616): linear filter, unnormalised coordinates, element
+ * reads.  The reference asks for wrap addressing, which the hardware treats
+ * as clamp for unnormalised coordinates (pinned by tests/golden/tex_probe);
+ * clamp is requested explicitly here. */
+cudaError_t ensure_texture(hpm_ctx *c, int i, int w, int h)
+{
+    if (c->arr[i] && c->arr_w[i] == w && c->arr_h[i] == h) return cudaSuccess;
+    if (c->tex[i]) cudaDestroyTextureObject(c->tex[i]);
+    if (c->arr[i]) cudaFreeArray(c->arr[i]);
+    c->tex[i] = 0;
+    c->arr[i] = nullptr;
+    c->arr_w[i] = c->arr_h[i] = 0;
+    cudaChannelFormatDesc desc = cudaCreateChannelDesc(32, 0, 0, 0, cudaChannelFormatKindFloat);
+    cudaError_t e = cudaMallocArray(&c->arr[i], &desc, w, h);
+    if (e != cudaSuccess) return e;
+    cudaResourceDesc res;
+    memset(&res, 0, sizeof(res));
+    res.resType = cudaResourceTypeArray;
+    res.res.array.array = c->arr[i];
+    cudaTextureDesc td;
+    memset(&td, 0, sizeof(td));
+    td.addressMode[0] = cudaAddressModeClamp;
+    td.addressMode[1] = cudaAddressModeClamp;
+    td.filterMode = cudaFilterModeLinear;
+    td.readMode = cudaReadModeElementType;
+    td.normalizedCoords = 0;
+    e = cudaCreateTextureObject(&c->tex[i], &res, &td, nullptr);
+    if (e != cudaSuccess) return e;
+    c->arr_w[i] = w;
+    c->arr_h[i] = h;
+    return cudaSuccess;
+}
+
+int select_device(hpm_ctx *c)
+{
+    CK(cudaSetDevice(c->device), "cudaSetDevice");
+    return HPM_OK;
+}
+
+PMArgs make_args(hpm_ctx *c)
+{
+    PMArgs a;
+    memset(&a, 0, sizeof(a));
+    a.n = c->n;
+    a.W = c->cams[0].width;
+    a.H = c->cams[0].height;
+    a.rows_cov = rows_covered(a.H);
+    a.radius = 5;
+    a.radius_increment = 2;
+    a.sigma_spatial = 5.0f;
+    a.sigma_color = 3.0f;
+    a.top_k = 4;
+    for (int i = 0; i < c->n; ++i) {
+        a.cam[i] = c->cams[i];
+        a.view[i].img = c->d_img[i];
+        a.view[i].depth = c->has_depth ? c->d_depth[i] : nullptr;
+        a.view[i].tex = c->tex[i];
+        a.view[i].w = c->cams[i].width;
+        a.view[i].h = c->cams[i].height;
+    }
+    a.pair = c->d_pair;
+    a.planes = c->d_planes;
+    a.costs = c->d_costs;
+    a.views = c->d_views;
+    a.prior_planes = c->d_prior;
+    a.masks = c->d_masks;
+    a.counters = c->counting ? c->d_counters : nullptr;
+    return a;
+}
+
+size_t npx(const hpm_ctx *c) { return (size_t)c->cams[0].width * c->cams[0].height; }
+
+void prof_begin(hpm_ctx *c, int kind, cudaEvent_t *e0)
+{
+    *e0 = nullptr;
+    if (!c->profiling) return;
+    cudaEventCreate(e0);
+    cudaEventRecord(*e0, c->stream);
+    (void)kind;
+}
+
+void prof_end(hpm_ctx *c, int kind, cudaEvent_t e0)
+{
+    if (!c->profiling || !e0) return;
+    cudaEvent_t e1;
+    cudaEventCreate(&e1);
+    cudaEventRecord(e1, c->stream);
+    c->prof_events.push_back({kind, {e0, e1}});
+}
+
+}  // namespace
+
+extern "C" {
+
+void hpm_default_params(HpmParams *p)
+{
+    if (!p) return;
+    memset(p, 0, sizeof(*p));
+    p->max_iterations = 3;
+    p->patch_size = 11;
+    p->radius_increment = 2;
+    p->sigma_spatial = 5.0f;
+    p->sigma_color = 3.0f;
+    p->top_k = 4;
+    p->depth_min = 0.0f;
+    p->depth_max = 1.0f;
+}
+
+int hpm_create(hpm_ctx **out, int device)
+{
+    if (!out) return HPM_ERR_ARG;
+    *out = nullptr;
+    hpm_ctx *c = new (std::nothrow) hpm_ctx();
+    if (!c) return HPM_ERR_NOMEM;
+    c->device = device;
+    cudaError_t e = cudaSetDevice(device);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaMalloc(&c->d_pair, sizeof(PairGeom) * kMaxViews);
+    if (e == cudaSuccess) e = cudaMalloc(&c->d_counters, 2 * sizeof(unsigned long long));
+    if (e != cudaSuccess) {
+        delete c;
+        return e == cudaErrorMemoryAllocation ? HPM_ERR_NOMEM : HPM_ERR_CUDA;
+    }
+    *out = c;
+    return HPM_OK;
+}
+
+int hpm_destroy(hpm_ctx *c)
+{
+    if (!c) return HPM_ERR_ARG;
+    cudaSetDevice(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    for (int i = 0; i < kMaxViews; ++i) {
+        cudaFree(c->d_img[i]);
+        cudaFree(c->d_depth[i]);
+        if (c->tex[i]) cudaDestroyTextureObject(c->tex[i]);
+        if (c->arr[i]) cudaFreeArray(c->arr[i]);
+    }
+    cudaFree(c->d_pair);
+    cudaFree(c->d_planes);
+    cudaFree(c->d_costs);
+    cudaFree(c->d_views);
+    cudaFree(c->d_prior);
+    cudaFree(c->d_masks);
+    cudaFree(c->d_counters);
+    cudaFree(c->d_scratch);
+    for (auto &p : c->prof_events) {
+        cudaEventDestroy(p.second.first);
+        cudaEventDestroy(p.second.second);
+    }
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+    return HPM_OK;
+}
+
+const char *hpm_last_error(const hpm_ctx *c) { return c ? c->err : "null context"; }
+
+void *hpm_stream(hpm_ctx *c) { return c ? (void *)c->stream : nullptr; }
+
+int hpm_set_views(hpm_ctx *c, const float *const *images, const HpmCamera *cams, int num_images)
+{
+    if (!c) return HPM_ERR_ARG;
+    if (!images || !cams) return fail(c, HPM_ERR_ARG, "hpm_set_views: null images or cameras");
+    if (num_images < 2 || num_images > kMaxViews)
+        return fail(c, HPM_ERR_ARG, "hpm_set_views: num_images=%d outside [2, %d]", num_images, kMaxViews);
+    for (int i = 0; i < num_images; ++i) {
+        if (!images[i]) return fail(c, HPM_ERR_ARG, "hpm_set_views: image %d is null", i);
+        if (cams[i].width < 1 || cams[i].height < 1 || cams[i].width > 16384 || cams[i].height > 16384)
+            return fail(c, HPM_ERR_ARG, "hpm_set_views: image %d has size %dx%d", i, cams[i].width,
+                        cams[i].height);
+    }
+    int r = select_device(c);
+    if (r) return r;
+    for (int i = 0; i < num_images; ++i) {
+        const size_t bytes = sizeof(float) * cams[i].width * cams[i].height;
+        CK(ensure((void **)&c->d_img[i], &c->img_cap[i], bytes), "image alloc");
+        CK(cudaMemcpyAsync(c->d_img[i], images[i], bytes, cudaMemcpyHostToDevice, c->stream), "image upload");
+        CK(ensure_texture(c, i, cams[i].width, cams[i].height), "texture set-up");
+        CK(cudaMemcpy2DToArrayAsync(c->arr[i], 0, 0, c->d_img[i], sizeof(float) * cams[i].width,
+                                    sizeof(float) * cams[i].width, cams[i].height, cudaMemcpyDeviceToDevice,
+                                    c->stream),
+           "texture upload");
+        c->cams[i] = cams[i];
+    }
+    c->n = num_images;
+    c->has_depth = false;
+    c->has_prior = false;
+    const size_t n = npx(c);
+    if (c->px_cap < n) {
+        cudaFree(c->d_planes);
+        cudaFree(c->d_costs);
+        cudaFree(c->d_views);
+        cudaFree(c->d_prior);
+        cudaFree(c->d_masks);
+        c->d_planes = nullptr;
+        c->d_costs = nullptr;
+        c->d_views = nullptr;
+        c->d_prior = nullptr;
+        c->d_masks = nullptr;
+        c->px_cap = 0;
+        CK(cudaMalloc(&c->d_planes, sizeof(float4) * n), "state alloc");
+        CK(cudaMalloc(&c->d_costs, sizeof(float) * n), "state alloc");
+        CK(cudaMalloc(&c->d_views, sizeof(uint32_t) * n), "state alloc");
+        CK(cudaMalloc(&c->d_prior, sizeof(float4) * n), "state alloc");
+        CK(cudaMalloc(&c->d_masks, sizeof(uint32_t) * n), "state alloc");
+        c->px_cap = n;
+    }
+    CK(cudaMemsetAsync(c->d_planes, 0, sizeof(float4) * n, c->stream), "state clear");
+    CK(cudaMemsetAsync(c->d_costs, 0, sizeof(float) * n, c->stream), "state clear");
+    CK(cudaMemsetAsync(c->d_views, 0, sizeof(uint32_t) * n, c->stream), "state clear");
+    PMArgs a = make_args(c);
+    CK(launch_pair_geom(a, c->d_pair, c->stream), "pair geometry");
+    c->has_state = false;
+    /* synchronous semantics for the caller's host buffers */
+    CK(cudaStreamSynchronize(c->stream), "hpm_set_views");
+    return HPM_OK;
+}
+
+int hpm_set_geom_depths(hpm_ctx *c, const float *const *depths)
+{
+    if (!c) return HPM_ERR_ARG;
+    if (c->n < 2) return fail(c, HPM_ERR_STATE, "hpm_set_geom_depths before hpm_set_views");
+    if (!depths) return fail(c, HPM_ERR_ARG, "hpm_set_geom_depths: null");
+    int r = select_device(c);
+    if (r) return r;
+    for (int i = 0; i < c->n; ++i) {
+        if (!depths[i]) return fail(c, HPM_ERR_ARG, "hpm_set_geom_depths: depth %d is null", i);
+        const size_t bytes = sizeof(float) * c->cams[i].width * c->cams[i].height;
+        CK(ensure((void **)&c->d_depth[i], &c->depth_cap[i], bytes), "depth alloc");
+        CK(cudaMemcpyAsync(c->d_depth[i], depths[i], bytes, cudaMemcpyHostToDevice, c->stream), "depth upload");
+    }
+    c->has_depth = true;
+    CK(cudaStreamSynchronize(c->stream), "hpm_set_geom_depths");
+    return HPM_OK;
+}
+
+int hpm_set_hypotheses(hpm_ctx *c, const float *planes, const float *costs)
+{
+    if (!c) return HPM_ERR_ARG;
+    if (c->n < 2) return fail(c, HPM_ERR_STATE, "hpm_set_hypotheses before hpm_set_views");
+    if (!planes) return fail(c, HPM_ERR_ARG, "hpm_set_hypotheses: null planes");
+    int r = select_device(c);
+    if (r) return r;
+    const size_t n = npx(c);
+    CK(cudaMemcpyAsync(c->d_planes, planes, sizeof(float4) * n, cudaMemcpyHostToDevice, c->stream), "planes");
+    if (costs)
+        CK(cudaMemcpyAsync(c->d_costs, costs, sizeof(float) * n, cudaMemcpyHostToDevice, c->stream), "costs");
+    else
+        CK(cudaMemsetAsync(c->d_costs, 0, sizeof(float) * n, c->stream), "costs");
+    c->has_state = true;
+    CK(cudaStreamSynchronize(c->stream), "hpm_set_hypotheses");
+    return HPM_OK;
+}
+
+int hpm_set_prior(hpm_ctx *c, const float *prior_planes, const uint32_t *masks)
+{
+    if (!c) return HPM_ERR_ARG;
+    if (c->n < 2) return fail(c, HPM_ERR_STATE, "hpm_set_prior before hpm_set_views");
+    if (!prior_planes || !masks) return fail(c, HPM_ERR_ARG, "hpm_set_prior: null input");
+    int r = select_device(c);
+    if (r) return r;
+    const size_t n = npx(c);
+    CK(cudaMemcpyAsync(c->d_prior, prior_planes, sizeof(float4) * n, cudaMemcpyHostToDevice, c->stream), "prior");
+    CK(cudaMemcpyAsync(c->d_masks, masks, sizeof(uint32_t) * n, cudaMemcpyHostToDevice, c->stream), "masks");
+    c->has_prior = true;
+    CK(cudaStreamSynchronize(c->stream), "hpm_set_prior");
+    return HPM_OK;
+}
+
+int hpm_clear_prior(hpm_ctx *c)
+{
+    if (!c) return HPM_ERR_ARG;
+    c->has_prior = false;
+    return HPM_OK;
+}
+
+int hpm_run_patchmatch(hpm_ctx *c, const HpmParams *p)
+{
+    if (!c) return HPM_ERR_ARG;
+    if (!p) return fail(c, HPM_ERR_ARG, "hpm_run_patchmatch: null params");
+    if (c->n < 2) return fail(c, HPM_ERR_STATE, "hpm_run_patchmatch before hpm_set_views");
+    if (p->patch_size != 11 || p->radius_increment != 2)
+        return fail(c, HPM_ERR_ARG, "hpm_run_patchmatch: only the reference window (11, stride 2) is built");
+    if (p->geom_consistency && !c->has_depth)
+        return fail(c, HPM_ERR_STATE, "geometric consistency needs hpm_set_geom_depths");
+    if (p->planar_prior && !c->has_prior) return fail(c, HPM_ERR_STATE, "planar prior needs hpm_set_prior");
+    if (!(p->depth_max > p->depth_min)) return fail(c, HPM_ERR_ARG, "depth range is empty");
+    int r = select_device(c);
+    if (r) return r;
+    PMArgs a = make_args(c);
+    a.dmin = p->depth_min;
+    a.dmax = p->depth_max;
+    a.geom = p->geom_consistency ? 1 : 0;
+    a.prior = p->planar_prior ? 1 : 0;
+    a.sigma_spatial = p->sigma_spatial;
+    a.sigma_color = p->sigma_color;
+    a.top_k = p->top_k;
+    a.seed_lo = (uint32_t)p->seed;
+    a.seed_hi = (uint32_t)(p->seed >> 32);
+    a.salt = c->pass_counter++;
+    if (c->counting) CK(cudaMemsetAsync(c->d_counters, 0, 2 * sizeof(unsigned long long), c->stream), "counters");
+    const int iters = p->honour_max_iterations ? p->max_iterations : 3; /* HPM.cu:1933 */
+    cudaEvent_t e0;
+    prof_begin(c, 0, &e0);
+    CK(launch_init(a, c->stream), "init kernel");
+    prof_end(c, 0, e0);
+    for (int it = 0; it < iters; ++it) {
+        for (int color = 0; color < 2; ++color) {
+            prof_begin(c, 1, &e0);
+            CK(launch_propagate(a, it, color, c->stream), "propagate kernel");
+            prof_end(c, 1, e0);
+        }
+    }
+    prof_begin(c, 2, &e0);
+    CK(launch_depth_normal_filter(a, c->d_planes, c->d_costs, c->stream), "depth/normal + filter kernels");
+    prof_end(c, 2, e0);
+    c->has_state = true;
+    CK(cudaStreamSynchronize(c->stream), "hpm_run_patchmatch");
+    return HPM_OK;
+}
+
+int hpm_get_result(hpm_ctx *c, float *planes, float *costs)
+{
+    if (!c) return HPM_ERR_ARG;
+    if (c->n < 2) return fail(c, HPM_ERR_STATE, "hpm_get_result before hpm_set_views");
+    int r = select_device(c);
+    if (r) return r;
+    const size_t n = npx(c);
+    if (planes)
+        CK(cudaMemcpyAsync(planes, c->d_planes, sizeof(float4) * n, cudaMemcpyDeviceToHost, c->stream), "planes");
+    if (costs) CK(cudaMemcpyAsync(costs, c->d_costs, sizeof(float) * n, cudaMemcpyDeviceToHost, c->stream), "costs");
+    CK(cudaStreamSynchronize(c->stream), "hpm_get_result");
+    return HPM_OK;
+}
+
+int hpm_get_selected_views(hpm_ctx *c, uint32_t *views)
+{
+    if (!c || !views) return HPM_ERR_ARG;
+    if (c->n < 2) return fail(c, HPM_ERR_STATE, "hpm_get_selected_views before hpm_set_views");
+    int r = select_device(c);
+    if (r) return r;
+    CK(cudaMemcpyAsync(views, c->d_views, sizeof(uint32_t) * npx(c), cudaMemcpyDeviceToHost, c->stream), "views");
+    CK(cudaStreamSynchronize(c->stream), "hpm_get_selected_views");
+    return HPM_OK;
+}
+
+int hpm_device_state(hpm_ctx *c, float **planes, float **costs, uint32_t **views)
+{
+    if (!c) return HPM_ERR_ARG;
+    if (planes) *planes = (float *)c->d_planes;
+    if (costs) *costs = c->d_costs;
+    if (views) *views = c->d_views;
+    return HPM_OK;
+}
+
+static int scratch(hpm_ctx *c, size_t bytes, void **p)
+{
+    CK(ensure(&c->d_scratch, &c->scratch_cap, bytes), "scratch alloc");
+    *p = c->d_scratch;
+    return HPM_OK;
+}
+
+int hpm_cost_vectors(hpm_ctx *c, const float *planes, float *out)
+{
+    if (!c || !planes || !out) return HPM_ERR_ARG;
+    if (c->n < 2) return fail(c, HPM_ERR_STATE, "hpm_cost_vectors before hpm_set_views");
+    int r = select_device(c);
+    if (r) return r;
+    const size_t n = npx(c), S = c->n - 1;
+    void *buf;
+    r = scratch(c, n * (sizeof(float4) + S * sizeof(float)), &buf);
+    if (r) return r;
+    float4 *d_pl = (float4 *)buf;
+    float *d_out = (float *)(d_pl + n);
+    CK(cudaMemcpyAsync(d_pl, planes, sizeof(float4) * n, cudaMemcpyHostToDevice, c->stream), "planes");
+    PMArgs a = make_args(c);
+    CK(launch_cost_vectors(a, d_pl, d_out, c->stream), "cost vector kernel");
+    CK(cudaMemcpyAsync(out, d_out, sizeof(float) * n * S, cudaMemcpyDeviceToHost, c->stream), "out");
+    CK(cudaStreamSynchronize(c->stream), "hpm_cost_vectors");
+    return HPM_OK;
+}
+
+int hpm_initial_costs(hpm_ctx *c, const float *planes, float *out_cost, uint32_t *out_views)
+{
+    if (!c || !planes || !out_cost || !out_views) return HPM_ERR_ARG;
+    if (c->n < 2) return fail(c, HPM_ERR_STATE, "hpm_initial_costs before hpm_set_views");
+    int r = select_device(c);
+    if (r) return r;
+    const size_t n = npx(c);
+    void *buf;
+    r = scratch(c, n * (sizeof(float4) + sizeof(float) + sizeof(uint32_t)), &buf);
+    if (r) return r;
+    float4 *d_pl = (float4 *)buf;
+    float *d_c = (float *)(d_pl + n);
+    uint32_t *d_v = (uint32_t *)(d_c + n);
+    CK(cudaMemcpyAsync(d_pl, planes, sizeof(float4) * n, cudaMemcpyHostToDevice, c->stream), "planes");
+    PMArgs a = make_args(c);
+    CK(launch_initial_costs(a, d_pl, d_c, d_v, c->stream), "initial cost kernel");
+    CK(cudaMemcpyAsync(out_cost, d_c, sizeof(float) * n, cudaMemcpyDeviceToHost, c->stream), "cost");
+    CK(cudaMemcpyAsync(out_views, d_v, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost, c->stream), "views");
+    CK(cudaStreamSynchronize(c->stream), "hpm_initial_costs");
+    return HPM_OK;
+}
+
+int hpm_geom_costs(hpm_ctx *c, const float *planes, float *out)
+{
+    if (!c || !planes || !out) return HPM_ERR_ARG;
+    if (c->n < 2 || !c->has_depth) return fail(c, HPM_ERR_STATE, "hpm_geom_costs needs views and depth maps");
+    int r = select_device(c);
+    if (r) return r;
+    const size_t n = npx(c), S = c->n - 1;
+    void *buf;
+    r = scratch(c, n * (sizeof(float4) + S * sizeof(float)), &buf);
+    if (r) return r;
+    float4 *d_pl = (float4 *)buf;
+    float *d_out = (float *)(d_pl + n);
+    CK(cudaMemcpyAsync(d_pl, planes, sizeof(float4) * n, cudaMemcpyHostToDevice, c->stream), "planes");
+    PMArgs a = make_args(c);
+    CK(launch_geom_costs(a, d_pl, d_out, c->stream), "geom cost kernel");
+    CK(cudaMemcpyAsync(out, d_out, sizeof(float) * n * S, cudaMemcpyDeviceToHost, c->stream), "out");
+    CK(cudaStreamSynchronize(c->stream), "hpm_geom_costs");
+    return HPM_OK;
+}
+
+int hpm_depth_normal_filter(hpm_ctx *c, float *planes, const float *costs)
+{
+    if (!c || !planes || !costs) return HPM_ERR_ARG;
+    if (c->n < 2) return fail(c, HPM_ERR_STATE, "hpm_depth_normal_filter before hpm_set_views");
+    int r = select_device(c);
+    if (r) return r;
+    const size_t n = npx(c);
+    void *buf;
+    r = scratch(c, n * (sizeof(float4) + sizeof(float)), &buf);
+    if (r) return r;
+    float4 *d_pl = (float4 *)buf;
+    float *d_c = (float *)(d_pl + n);
+    CK(cudaMemcpyAsync(d_pl, planes, sizeof(float4) * n, cudaMemcpyHostToDevice, c->stream), "planes");
+    CK(cudaMemcpyAsync(d_c, costs, sizeof(float) * n, cudaMemcpyHostToDevice, c->stream), "costs");
+    PMArgs a = make_args(c);
+    CK(launch_depth_normal_filter(a, d_pl, d_c, c->stream), "depth/normal + filter kernels");
+    CK(cudaMemcpyAsync(planes, d_pl, sizeof(float4) * n, cudaMemcpyDeviceToHost, c->stream), "planes");
+    CK(cudaStreamSynchronize(c->stream), "hpm_depth_normal_filter");
+    return HPM_OK;
+}
+
+int hpm_jbu(hpm_ctx *c, const float *guide, int cols, int rows, const float *coarse_depth, const float *coarse_normal,
+            int s_cols, int s_rows, float *out_depth, float *out_normal)
+{
+    if (!c) return HPM_ERR_ARG;
+    if (!guide || !coarse_depth || !coarse_normal || !out_depth || !out_normal)
+        return fail(c, HPM_ERR_ARG, "hpm_jbu: null input");
+    if (cols < 1 || rows < 1 || s_cols < 1 || s_rows < 1 || s_cols > cols || s_rows > rows)
+        return fail(c, HPM_ERR_ARG, "hpm_jbu: bad sizes %dx%d <- %dx%d", cols, rows, s_cols, s_rows);
+    const int sr = rows / s_rows, sc = cols / s_cols;
+    const int image_scale = sr > sc ? sr : sc;
+    if (image_scale == 1) return HPM_OK; /* HPM.cpp:1219-1222 */
+    int r = select_device(c);
+    if (r) return r;
+    const size_t fine = (size_t)cols * rows, coarse = (size_t)s_cols * s_rows;
+    void *buf;
+    r = scratch(c, fine * sizeof(float) + coarse * sizeof(float4) + fine * (sizeof(float) + sizeof(float4)), &buf);
+    if (r) return r;
+    float4 *d_coarse = (float4 *)buf;
+    float4 *d_on = d_coarse + coarse;
+    float *d_guide = (float *)(d_on + fine);
+    float *d_od = d_guide + fine;
+    std::vector<float4> packed(coarse);
+    for (size_t i = 0; i < coarse; ++i)
+        packed[i] = make_float4(coarse_normal[3 * i], coarse_normal[3 * i + 1], coarse_normal[3 * i + 2],
+                                coarse_depth[i]);
+    CK(cudaMemcpyAsync(d_coarse, packed.data(), sizeof(float4) * coarse, cudaMemcpyHostToDevice, c->stream),
+       "coarse");
+    CK(cudaMemcpyAsync(d_guide, guide, sizeof(float) * fine, cudaMemcpyHostToDevice, c->stream), "guide");
+    cudaEvent_t e0;
+    prof_begin(c, 3, &e0);
+    CK(launch_jbu(d_guide, cols, rows, nullptr, d_coarse, s_cols, s_rows, image_scale, d_od, d_on, c->stream),
+       "jbu kernel");
+    prof_end(c, 3, e0);
+    std::vector<float4> on(fine);
+    CK(cudaMemcpyAsync(out_depth, d_od, sizeof(float) * fine, cudaMemcpyDeviceToHost, c->stream), "depth");
+    CK(cudaMemcpyAsync(on.data(), d_on, sizeof(float4) * fine, cudaMemcpyDeviceToHost, c->stream), "normal");
+    CK(cudaStreamSynchronize(c->stream), "hpm_jbu");
+    for (size_t i = 0; i < fine; ++i) {
+        out_normal[3 * i] = on[i].x;
+        out_normal[3 * i + 1] = on[i].y;
+        out_normal[3 * i + 2] = on[i].z;
+    }
+    return HPM_OK;
+}
+
+int hpm_profile_enable(hpm_ctx *c, int enable)
+{
+    if (!c) return HPM_ERR_ARG;
+    c->profiling = enable != 0;
+    for (int i = 0; i < 4; ++i) {
+        c->prof_ms[i] = 0;
+        c->prof_cnt[i] = 0;
+    }
+    for (auto &p : c->prof_events) {
+        cudaEventDestroy(p.second.first);
+        cudaEventDestroy(p.second.second);
+    }
+    c->prof_events.clear();
+    return HPM_OK;
+}
+
+int hpm_profile_read(hpm_ctx *c, float *ms4, int *counts4)
+{
+    if (!c) return HPM_ERR_ARG;
+    CK(cudaStreamSynchronize(c->stream), "hpm_profile_read");
+    for (auto &p : c->prof_events) {
+        float ms = 0;
+        cudaEventElapsedTime(&ms, p.second.first, p.second.second);
+        c->prof_ms[p.first] += ms;
+        c->prof_cnt[p.first] += 1;
+        cudaEventDestroy(p.second.first);
+        cudaEventDestroy(p.second.second);
+    }
+    c->prof_events.clear();
+    for (int i = 0; i < 4; ++i) {
+        if (ms4) ms4[i] = c->prof_ms[i];
+        if (counts4) counts4[i] = c->prof_cnt[i];
+    }
+    return HPM_OK;
+}
+
+int hpm_count_enable(hpm_ctx *c, int enable)
+{
+    if (!c) return HPM_ERR_ARG;
+    c->counting = enable != 0;
+    return HPM_OK;
+}
+
+int hpm_count_read(hpm_ctx *c, uint64_t *cv, uint64_t *geom)
+{
+    if (!c) return HPM_ERR_ARG;
+    unsigned long long h[2] = {0, 0};
+    CK(cudaMemcpyAsync(h, c->d_counters, sizeof(h), cudaMemcpyDeviceToHost, c->stream), "counters");
+    CK(cudaStreamSynchronize(c->stream), "hpm_count_read");
+    if (cv) *cv = h[0];
+    if (geom) *geom = h[1];
+    return HPM_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,75 @@
+/*
+ * Internal declarations shared by the CUDA kernels and the C-ABI layer of
+ * the B200-native HPM-MVS PatchMatch path.
+ */
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "hpm_b200.h"
+
+namespace hpm {
+
+constexpr int kMaxViews = HPM_MAX_IMAGES; /* reference + 32 sources */
+constexpr int kMaxSrc = kMaxViews - 1;
+constexpr int kTaps = 36; /* 6 x 6 taps of the 11x11 window, stride 2 */
+
+/* Per-view data of one problem, passed to kernels by value. */
+struct ViewDev {
+    const float *img;        /* h x w gray, linear (reference-window and JBU loads) */
+    const float *depth;      /* geometric-consistency depth map or nullptr */
+    cudaTextureObject_t tex; /* same image as a float cudaArray texture: linear filter, clamped edges */
+    int w, h;
+};
+
+/* Camera-pair quantities that do not depend on the hypothesis, computed on
+ * the device with the reference's own expressions (HPM.cu:229-255). */
+struct PairGeom {
+    float Rrel[9];
+    float trel[3];
+};
+
+/* Everything a PatchMatch kernel needs, passed by value (CUDA 12.1+ allows
+ * kernel parameter blocks larger than 4 KB). */
+struct PMArgs {
+    int n; /* images */
+    int W, H;
+    int rows_cov; /* rows reached by the reference's checkerboard grid */
+    float dmin, dmax;
+    int geom, prior;
+    uint32_t seed_lo, seed_hi, salt;
+    int radius, radius_increment;
+    float sigma_spatial, sigma_color;
+    int top_k;
+    HpmCamera cam[kMaxViews];
+    ViewDev view[kMaxViews];
+    const PairGeom *pair; /* [n], entry 0 unused */
+    float4 *planes;
+    float *costs;
+    uint32_t *views;
+    const float4 *prior_planes;
+    const uint32_t *masks;
+    float *cost_cache; /* [S][H][W] cost vector of the current hypothesis, or nullptr */
+    unsigned long long *counters; /* [2]: cost vectors, geom terms, or nullptr */
+};
+
+/* Launchers (hpm_pm.cu / hpm_jbu.cu). All asynchronous on `s`. */
+cudaError_t launch_pair_geom(const PMArgs &a, PairGeom *out, cudaStream_t s);
+cudaError_t launch_init(const PMArgs &a, cudaStream_t s);
+cudaError_t launch_propagate(const PMArgs &a, int iter, int color, cudaStream_t s);
+cudaError_t launch_depth_normal_filter(const PMArgs &a, float4 *planes, const float *costs, cudaStream_t s);
+cudaError_t launch_cost_vectors(const PMArgs &a, const float4 *planes, float *out, cudaStream_t s);
+cudaError_t launch_initial_costs(const PMArgs &a, const float4 *planes, float *cost, uint32_t *views,
+                                 cudaStream_t s);
+cudaError_t launch_geom_costs(const PMArgs &a, const float4 *planes, float *out, cudaStream_t s);
+cudaError_t launch_jbu(const float *guide, int cols, int rows, const float *coarse_depth,
+                       const float4 *coarse_normal, int s_cols, int s_rows, int image_scale, float *out_depth,
+                       float4 *out_normal, cudaStream_t s);
+
+int rows_covered(int H);
+
+}  // namespace hpm

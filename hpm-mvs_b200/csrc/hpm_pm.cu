@@ -1,0 +1,1075 @@
+/*
+ * PatchMatch kernels of the B200-native HPM-MVS path (sm_100a).
+ *
+ * Behaviour follows the reference's HPM-MVS/HPM.cu kernel for kernel; the
+ * per-function comments cite the lines.  What is different is how the work
+ * maps to the machine:
+ *
+ *  - Reference-window hoisting.  The reference recomputes the 36 bilateral
+ *    weights of a pixel's 11x11/stride-2 window (one exp, one sqrt, two
+ *    divides each) and all reference-side sums inside every NCC call
+ *    (HPM.cu:345-368), i.e. ~23 x S times per pixel per half-step.  Here they
+ *    are computed once per pixel per launch, with the reference's own
+ *    expressions (so the values are the same bits), and kept in shared memory
+ *    as a [tap][thread] array: each NCC tap then costs one shared load of the
+ *    weight and one of weight*ref instead of an exp, a sqrt and two texture
+ *    fetches.
+ *  - Source views are sampled by the texture unit (float cudaArray, linear
+ *    filter, clamped edges: the reference's own texture set-up), which is
+ *    the only way to get the hardware's filter arithmetic bit for bit
+ *    (its bilinear weights are 1.8 fixed point with round-half-up, and the
+ *    weighted sum is formed at reduced precision; a software gather
+ *    differs by up to ~0.5 gray levels per tap).
+ *  - Shared-memory cost matrix.  cost_array[8][32] (1.5 KB of local memory
+ *    per thread in the reference) becomes a [direction*S + view][thread]
+ *    shared array sized by the actual number of source views.
+ *  - Counter-based Philox random numbers: no 48-byte curand state per pixel
+ *    in HBM and no curand_init skip-ahead; draws come in the reference's
+ *    order.
+ *  - Half-step kernels are launched back to back on one stream with no
+ *    host synchronisation (the reference synchronises after every launch).
+ */
+#include <cfloat>
+
+#include "hpm_internal.h"
+
+namespace hpm {
+
+namespace {
+
+constexpr double kPiD = 3.14159265358979323846; /* M_PI, HPM-MVS/main.h:41 */
+constexpr int kBlockX = 32;
+constexpr int kBlockY = 2;
+constexpr int kBlock = kBlockX * kBlockY;
+
+/* ------------------------------------------------------------------ */
+/* Philox4x32-10 (Salmon et al., SC'11), counter = (pixel, step, n/4, salt) */
+/* ------------------------------------------------------------------ */
+struct Rng {
+    uint32_t k0, k1, pixel, step, salt, n;
+    uint32_t b0, b1, b2, b3;
+
+    __device__ void init(uint32_t klo, uint32_t khi, uint32_t px, uint32_t st, uint32_t sa)
+    {
+        k0 = klo;
+        k1 = khi;
+        pixel = px;
+        step = st;
+        salt = sa;
+        n = 0;
+    }
+
+    __device__ void block()
+    {
+        uint32_t c0 = pixel, c1 = step, c2 = n >> 2, c3 = salt;
+        uint32_t a0 = k0, a1 = k1;
+#pragma unroll
+        for (int r = 0; r < 10; ++r) {
+            const uint32_t lo0 = 0xD2511F53u * c0, hi0 = __umulhi(0xD2511F53u, c0);
+            const uint32_t lo1 = 0xCD9E8D57u * c2, hi1 = __umulhi(0xCD9E8D57u, c2);
+            const uint32_t n0 = hi1 ^ c1 ^ a0;
+            const uint32_t n2 = hi0 ^ c3 ^ a1;
+            c0 = n0;
+            c1 = lo1;
+            c2 = n2;
+            c3 = lo0;
+            a0 += 0x9E3779B9u;
+            a1 += 0xBB67AE85u;
+        }
+        b0 = c0;
+        b1 = c1;
+        b2 = c2;
+        b3 = c3;
+    }
+
+    /* uniform in (0,1]: ((x >> 8) + 1) * 2^-24 */
+    __device__ float uniform()
+    {
+        if ((n & 3u) == 0) block();
+        const uint32_t j = n & 3u;
+        const uint32_t x = j == 0 ? b0 : (j == 1 ? b1 : (j == 2 ? b2 : b3));
+        ++n;
+        return (float)((x >> 8) + 1u) * (1.0f / 16777216.0f);
+    }
+};
+
+/* ------------------------------------------------------------------ */
+/* Sampling                                                            */
+/* ------------------------------------------------------------------ */
+
+/* texel at integer position (tex2D at x+0.5, y+0.5), edges repeated */
+__device__ __forceinline__ float texel(const float *__restrict__ img, int w, int h, int x, int y)
+{
+    x = min(max(x, 0), w - 1);
+    y = min(max(y, 0), h - 1);
+    return __ldg(img + (size_t)y * w + x);
+}
+
+/* ------------------------------------------------------------------ */
+/* Geometry (HPM.cu:65-133, 227-316, 445-481)                           */
+/* ------------------------------------------------------------------ */
+
+__device__ __forceinline__ void normalize3(float4 &v) /* HPM.cu:77-84 */
+{
+    const float n2 = v.x * v.x + v.y * v.y + v.z * v.z;
+    const float inv = rsqrtf(n2);
+    v.x *= inv;
+    v.y *= inv;
+    v.z *= inv;
+}
+
+__device__ __forceinline__ float4 view_direction(const HpmCamera &c, int px, int py, float depth)
+{
+    float X0 = depth * (px - c.K[2]) / c.K[0];
+    float X1 = depth * (py - c.K[5]) / c.K[4];
+    float X2 = depth;
+    const float norm = sqrtf(X0 * X0 + X1 * X1 + X2 * X2);
+    return make_float4(X0 / norm, X1 / norm, X2 / norm, 0.0f);
+}
+
+__device__ __forceinline__ float distance_to_origin(const HpmCamera &c, int px, int py, float depth, float4 n)
+{
+    const float X0 = depth * (px - c.K[2]) / c.K[0];
+    const float X1 = depth * (py - c.K[5]) / c.K[4];
+    const float X2 = depth;
+    return -(n.x * X0 + n.y * X1 + n.z * X2);
+}
+
+__device__ __forceinline__ float depth_from_plane(const HpmCamera &c, float4 h, int px, int py)
+{
+    return -h.w * c.K[0] / ((px - c.K[2]) * h.x + (c.K[0] / c.K[4]) * (py - c.K[5]) * h.y + c.K[0] * h.z);
+}
+
+__device__ __forceinline__ float4 transform_normal(const HpmCamera &c, float4 h)
+{
+    float4 r;
+    r.x = c.R[0] * h.x + c.R[3] * h.y + c.R[6] * h.z;
+    r.y = c.R[1] * h.x + c.R[4] * h.y + c.R[7] * h.z;
+    r.z = c.R[2] * h.x + c.R[5] * h.y + c.R[8] * h.z;
+    r.w = h.w;
+    return r;
+}
+
+__device__ __forceinline__ float4 transform_normal_to_ref(const HpmCamera &c, float4 h)
+{
+    float4 r;
+    r.x = c.R[0] * h.x + c.R[1] * h.y + c.R[2] * h.z;
+    r.y = c.R[3] * h.x + c.R[4] * h.y + c.R[5] * h.z;
+    r.z = c.R[6] * h.x + c.R[7] * h.y + c.R[8] * h.z;
+    r.w = h.w;
+    return r;
+}
+
+__device__ __forceinline__ float dot3(float4 a, float4 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+
+__device__ float4 random_normal(const HpmCamera &c, int px, int py, Rng &rng, float depth) /* HPM.cu:135-161 */
+{
+    float q1 = 1.0f, q2 = 1.0f, s = 2.0f;
+    while (s >= 1.0f) {
+        q1 = 2.0f * rng.uniform() - 1.0f;
+        q2 = 2.0f * rng.uniform() - 1.0f;
+        s = q1 * q1 + q2 * q2;
+    }
+    const float sq = sqrtf(1.0f - s);
+    float4 n = make_float4(2.0f * q1 * sq, 2.0f * q2 * sq, 1.0f - 2.0f * s, 0.0f);
+    const float4 v = view_direction(c, px, py, depth);
+    if (n.x * v.x + n.y * v.y + n.z * v.z > 0.0f) {
+        n.x = -n.x;
+        n.y = -n.y;
+        n.z = -n.z;
+    }
+    normalize3(n);
+    return n;
+}
+
+__device__ float4 perturbed_normal(const HpmCamera &c, int px, int py, float4 normal, Rng &rng,
+                                   float pert) /* HPM.cu:163-198 */
+{
+    const float4 v = view_direction(c, px, py, 1.0f);
+    const float a1 = (rng.uniform() - 0.5f) * pert;
+    const float a2 = (rng.uniform() - 0.5f) * pert;
+    const float a3 = (rng.uniform() - 0.5f) * pert;
+    const float s1 = sinf(a1), s2 = sinf(a2), s3 = sinf(a3);
+    const float c1 = cosf(a1), c2 = cosf(a2), c3 = cosf(a3);
+    float R[9];
+    R[0] = c2 * c3;
+    R[1] = c3 * s1 * s2 - c1 * s3;
+    R[2] = s1 * s3 + c1 * c3 * s2;
+    R[3] = c2 * s3;
+    R[4] = c1 * c3 + s1 * s2 * s3;
+    R[5] = c1 * s2 * s3 - c3 * s1;
+    R[6] = -s2;
+    R[7] = c2 * s1;
+    R[8] = c1 * c2;
+    float4 p;
+    p.x = R[0] * normal.x + R[1] * normal.y + R[2] * normal.z;
+    p.y = R[3] * normal.x + R[4] * normal.y + R[5] * normal.z;
+    p.z = R[6] * normal.x + R[7] * normal.y + R[8] * normal.z;
+    p.w = normal.w;
+    if (dot3(p, v) >= 0.0f) p = normal;
+    normalize3(p);
+    return p;
+}
+
+/* ComputeHomography (HPM.cu:227-287) with the hypothesis-independent part
+ * (relative pose) precomputed per view pair. */
+__device__ __forceinline__ void homography(const HpmCamera &rc, const HpmCamera &sc, const PairGeom &g, float4 h,
+                                           float *H)
+{
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        H[3 * i + 0] = g.Rrel[3 * i + 0] - g.trel[i] * h.x / h.w;
+        H[3 * i + 1] = g.Rrel[3 * i + 1] - g.trel[i] * h.y / h.w;
+        H[3 * i + 2] = g.Rrel[3 * i + 2] - g.trel[i] * h.z / h.w;
+    }
+    float tmp[9];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        tmp[3 * i + 0] = H[3 * i + 0] / rc.K[0];
+        tmp[3 * i + 1] = H[3 * i + 1] / rc.K[4];
+        tmp[3 * i + 2] = -H[3 * i + 0] * rc.K[2] / rc.K[0] - H[3 * i + 1] * rc.K[5] / rc.K[4] + H[3 * i + 2];
+    }
+    H[0] = sc.K[0] * tmp[0] + sc.K[2] * tmp[6];
+    H[1] = sc.K[0] * tmp[1] + sc.K[2] * tmp[7];
+    H[2] = sc.K[0] * tmp[2] + sc.K[2] * tmp[8];
+    H[3] = sc.K[4] * tmp[3] + sc.K[5] * tmp[6];
+    H[4] = sc.K[4] * tmp[4] + sc.K[5] * tmp[7];
+    H[5] = sc.K[4] * tmp[5] + sc.K[5] * tmp[8];
+    H[6] = sc.K[8] * tmp[6];
+    H[7] = sc.K[8] * tmp[7];
+    H[8] = sc.K[8] * tmp[8];
+}
+
+/* ComputeCorrespondingPoint (HPM.cu:289-296).  Integer pixel coordinates
+ * are passed as floats: (float)(px + i) == (float)px + i exactly. */
+__device__ __forceinline__ float2 warp(const float *H, float px, float py)
+{
+    const float x = H[0] * px + H[1] * py + H[2];
+    const float y = H[3] * px + H[4] * py + H[5];
+    const float z = H[6] * px + H[7] * py + H[8];
+    return make_float2(x / z, y / z);
+}
+
+/* ------------------------------------------------------------------ */
+/* Hoisted reference window                                            */
+/* ------------------------------------------------------------------ */
+
+struct RefStats {
+    float inv;  /* 1 / sum of weights */
+    float mean; /* weighted mean of the reference window */
+    float var;  /* weighted variance of the reference window */
+};
+
+/* The reference-side half of ComputeBilateralNCC (HPM.cu:318-386) for pixel
+ * (px, py): per-tap weight and weight*ref into shared memory, sums in the
+ * reference's row-then-total order. */
+__device__ RefStats ref_window(const PMArgs &a, int px, int py, float *sW, float *sWR, int tid)
+{
+    const ViewDev &rv = a.view[0];
+    const float center = texel(rv.img, rv.w, rv.h, px, py);
+    float sum_ref = 0.0f, sum_ref_ref = 0.0f, wsum = 0.0f;
+    int t = 0;
+    for (int i = -5; i < 6; i += 2) {
+        float r_ref = 0.0f, r_rr = 0.0f, r_w = 0.0f;
+        for (int j = -5; j < 6; j += 2, ++t) {
+            const float rp = texel(rv.img, rv.w, rv.h, px + i, py + j);
+            const float x_dist = (float)i, y_dist = (float)j;
+            const float spatial_dist = sqrtf(x_dist * x_dist + y_dist * y_dist);
+            const float color_dist = fabsf(rp - center);
+            const float wgt = expf(-spatial_dist / (2.0f * a.sigma_spatial * a.sigma_spatial) -
+                                   color_dist / (2.0f * a.sigma_color * a.sigma_color));
+            sW[t * kBlock + tid] = wgt;
+            sWR[t * kBlock + tid] = wgt * rp;
+            r_ref += wgt * rp;
+            r_rr += wgt * rp * rp;
+            r_w += wgt;
+        }
+        sum_ref += r_ref;
+        sum_ref_ref += r_rr;
+        wsum += r_w;
+    }
+    RefStats s;
+    s.inv = 1.0f / wsum;
+    s.mean = sum_ref * s.inv;
+    const float mrr = sum_ref_ref * s.inv;
+    s.var = mrr - s.mean * s.mean;
+    return s;
+}
+
+/* The source-side half of ComputeBilateralNCC (HPM.cu:325-397). */
+__device__ float ncc(const PMArgs &a, int v, int px, int py, float4 h, const float *sW, const float *sWR, int tid,
+                     const RefStats &rs)
+{
+    const HpmCamera &sc = a.cam[v];
+    float H[9];
+    homography(a.cam[0], sc, a.pair[v], h, H);
+    const float fpx = (float)px, fpy = (float)py;
+    const float2 pt = warp(H, fpx, fpy);
+    if (pt.x >= sc.width || pt.x < 0.0f || pt.y >= sc.height || pt.y < 0.0f) return 2.0f;
+    if (rs.var < 1e-5f) return 2.0f; /* the reference reaches the same result after the taps */
+    const cudaTextureObject_t tex = a.view[v].tex;
+    float sum_src = 0.0f, sum_src_src = 0.0f, sum_ref_src = 0.0f;
+    int t = 0;
+#pragma unroll
+    for (int i = -5; i < 6; i += 2) {
+        float r_src = 0.0f, r_ss = 0.0f, r_rs = 0.0f;
+#pragma unroll
+        for (int j = -5; j < 6; j += 2, ++t) {
+            const float2 q = warp(H, fpx + (float)i, fpy + (float)j);
+            const float sp = tex2D<float>(tex, q.x + 0.5f, q.y + 0.5f);
+            const float wgt = sW[t * kBlock + tid];
+            const float wr = sWR[t * kBlock + tid];
+            r_src += wgt * sp;
+            r_ss += wgt * sp * sp;
+            r_rs += wr * sp;
+        }
+        sum_src += r_src;
+        sum_src_src += r_ss;
+        sum_ref_src += r_rs;
+    }
+    sum_src *= rs.inv;
+    sum_src_src *= rs.inv;
+    sum_ref_src *= rs.inv;
+    const float var_src = sum_src_src - sum_src * sum_src;
+    if (var_src < 1e-5f) return 2.0f;
+    const float covar = sum_ref_src - rs.mean * sum_src;
+    const float vv = sqrtf(rs.var * var_src);
+    return fmaxf(0.0f, fminf(2.0f, 1.0f - covar / vv));
+}
+
+/* ComputeMultiViewCostVector (HPM.cu:438-443) into a strided slot array. */
+__device__ __forceinline__ void cost_vector(const PMArgs &a, int px, int py, float4 h, const float *sW,
+                                            const float *sWR, int tid, const RefStats &rs, float *out,
+                                            int stride)
+{
+    for (int v = 1; v < a.n; ++v) out[(v - 1) * stride] = ncc(a, v, px, py, h, sW, sWR, tid, rs);
+    if (a.counters) atomicAdd(&a.counters[0], 1ull);
+}
+
+__device__ __forceinline__ void sort_small(float *d, int n) /* HPM.cu:3-12 */
+{
+    int j;
+    for (int i = 1; i < n; i++) {
+        const float tmp = d[i];
+        for (j = i; j >= 1 && tmp < d[j - 1]; j--) d[j] = d[j - 1];
+        d[j] = tmp;
+    }
+}
+
+/* ComputeMultiViewInitialCostandSelectedViews (HPM.cu:399-436) */
+__device__ float initial_cost(const PMArgs &a, int px, int py, float4 h, const float *sW, const float *sWR,
+                              int tid, const RefStats &rs, uint32_t *views)
+{
+    float cv[kMaxSrc], cp[kMaxSrc];
+    const int S = a.n - 1;
+    int valid = 0;
+    for (int v = 1; v < a.n; ++v) {
+        const float c = ncc(a, v, px, py, h, sW, sWR, tid, rs);
+        cv[v - 1] = c;
+        cp[v - 1] = c;
+        if (c < 2.0f) valid++;
+    }
+    if (a.counters) atomicAdd(&a.counters[0], 1ull);
+    sort_small(cv, S);
+    uint32_t sel = 0;
+    const int top_k = min(valid, a.top_k);
+    float result = 2.0f;
+    if (top_k > 0) {
+        float cost = 0.0f;
+        for (int i = 0; i < top_k; ++i) cost += cv[i];
+        const float thr = cv[top_k - 1];
+        for (int i = 0; i < S; ++i)
+            if (cp[i] <= thr) sel |= 1u << i;
+        result = cost / top_k;
+    }
+    *views = sel;
+    return result;
+}
+
+__device__ __forceinline__ void world_point(const HpmCamera &c, float x, float y, float depth, float *P)
+{
+    float X0 = depth * (x - c.K[2]) / c.K[0];
+    float X1 = depth * (y - c.K[5]) / c.K[4];
+    float X2 = depth;
+    const float T0 = c.R[0] * X0 + c.R[3] * X1 + c.R[6] * X2;
+    const float T1 = c.R[1] * X0 + c.R[4] * X1 + c.R[7] * X2;
+    const float T2 = c.R[2] * X0 + c.R[5] * X1 + c.R[8] * X2;
+    const float Cx = -(c.R[0] * c.t[0] + c.R[3] * c.t[1] + c.R[6] * c.t[2]);
+    const float Cy = -(c.R[1] * c.t[0] + c.R[4] * c.t[1] + c.R[7] * c.t[2]);
+    const float Cz = -(c.R[2] * c.t[0] + c.R[5] * c.t[1] + c.R[8] * c.t[2]);
+    P[0] = T0 + Cx;
+    P[1] = T1 + Cy;
+    P[2] = T2 + Cz;
+}
+
+__device__ __forceinline__ void project(const float *P, const HpmCamera &c, float *pt, float &depth)
+{
+    const float t0 = c.R[0] * P[0] + c.R[1] * P[1] + c.R[2] * P[2] + c.t[0];
+    const float t1 = c.R[3] * P[0] + c.R[4] * P[1] + c.R[5] * P[2] + c.t[1];
+    const float t2 = c.R[6] * P[0] + c.R[7] * P[1] + c.R[8] * P[2] + c.t[2];
+    depth = c.K[6] * t0 + c.K[7] * t1 + c.K[8] * t2;
+    pt[0] = (c.K[0] * t0 + c.K[1] * t1 + c.K[2] * t2) / depth;
+    pt[1] = (c.K[3] * t0 + c.K[4] * t1 + c.K[5] * t2) / depth;
+}
+
+/* ComputeGeomConsistencyCost (HPM.cu:483-508) */
+__device__ float geom_cost(const PMArgs &a, int v, float4 h, int px, int py)
+{
+    const HpmCamera &rc = a.cam[0], &sc = a.cam[v];
+    const float depth = depth_from_plane(rc, h, px, py);
+    float P[3], spt[2], sd;
+    world_point(rc, (float)px, (float)py, depth, P);
+    project(P, sc, spt, sd);
+    const ViewDev &sv = a.view[v];
+    const float src_depth = texel(sv.depth, sv.w, sv.h, __float2int_rz(spt[0]), __float2int_rz(spt[1]));
+    if (a.counters) atomicAdd(&a.counters[1], 1ull);
+    if (src_depth == 0.0f) return 5.0f;
+    float Q[3], bpt[2], rd;
+    world_point(sc, spt[0], spt[1], src_depth, Q);
+    project(Q, rc, bpt, rd);
+    const float dx = px - bpt[0], dy = py - bpt[1];
+    return fminf(5.0f, sqrtf(dx * dx + dy * dy));
+}
+
+/* ------------------------------------------------------------------ */
+/* Kernels                                                             */
+/* ------------------------------------------------------------------ */
+
+/* R_relative and t_relative of HPM.cu:229-255, with the same expressions. */
+__global__ void k_pair_geom(PMArgs a, PairGeom *out)
+{
+    const int v = threadIdx.x;
+    if (v < 1 || v >= a.n) return;
+    const HpmCamera &ref_camera = a.cam[0], &src_camera = a.cam[v];
+    float ref_C[3], src_C[3];
+    ref_C[0] = -(ref_camera.R[0] * ref_camera.t[0] + ref_camera.R[3] * ref_camera.t[1] + ref_camera.R[6] * ref_camera.t[2]);
+    ref_C[1] = -(ref_camera.R[1] * ref_camera.t[0] + ref_camera.R[4] * ref_camera.t[1] + ref_camera.R[7] * ref_camera.t[2]);
+    ref_C[2] = -(ref_camera.R[2] * ref_camera.t[0] + ref_camera.R[5] * ref_camera.t[1] + ref_camera.R[8] * ref_camera.t[2]);
+    src_C[0] = -(src_camera.R[0] * src_camera.t[0] + src_camera.R[3] * src_camera.t[1] + src_camera.R[6] * src_camera.t[2]);
+    src_C[1] = -(src_camera.R[1] * src_camera.t[0] + src_camera.R[4] * src_camera.t[1] + src_camera.R[7] * src_camera.t[2]);
+    src_C[2] = -(src_camera.R[2] * src_camera.t[0] + src_camera.R[5] * src_camera.t[1] + src_camera.R[8] * src_camera.t[2]);
+    PairGeom g;
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j)
+            g.Rrel[3 * i + j] = src_camera.R[3 * i + 0] * ref_camera.R[3 * j + 0] +
+                                src_camera.R[3 * i + 1] * ref_camera.R[3 * j + 1] +
+                                src_camera.R[3 * i + 2] * ref_camera.R[3 * j + 2];
+    float C_relative[3];
+    C_relative[0] = (ref_C[0] - src_C[0]);
+    C_relative[1] = (ref_C[1] - src_C[1]);
+    C_relative[2] = (ref_C[2] - src_C[2]);
+    for (int i = 0; i < 3; ++i)
+        g.trel[i] = src_camera.R[3 * i + 0] * C_relative[0] + src_camera.R[3 * i + 1] * C_relative[1] +
+                    src_camera.R[3 * i + 2] * C_relative[2];
+    out[v] = g;
+}
+
+/* RandomInitialization, HPM.cu:510-558.  One thread per pixel. */
+__global__ void __launch_bounds__(kBlock) k_init(PMArgs a)
+{
+    __shared__ float sW[kTaps * kBlock];
+    __shared__ float sWR[kTaps * kBlock];
+    const int tid = threadIdx.y * kBlockX + threadIdx.x;
+    const int px = blockIdx.x * kBlockX + threadIdx.x;
+    const int py = blockIdx.y * kBlockY + threadIdx.y;
+    if (px >= a.W || py >= a.H) return;
+    const int center = py * a.W + px;
+    const HpmCamera &cam = a.cam[0];
+    const RefStats rs = ref_window(a, px, py, sW, sWR, tid);
+    Rng rng;
+    rng.init(a.seed_lo, a.seed_hi, (uint32_t)center, 0u, a.salt);
+    float4 h;
+    if (a.geom) {
+        h = transform_normal_to_ref(cam, a.planes[center]);
+        const float depth = h.w;
+        h.w = distance_to_origin(cam, px, py, depth, h);
+    } else if (a.prior) {
+        if (a.masks[center] > 0 && a.costs[center] >= 0.1f) {
+            const float pert = 0.02f;
+            const float4 hp = a.prior_planes[center];
+            float dp = hp.w;
+            const float lo = (1 - 3 * pert) * dp;
+            const float hi = (1 + 3 * pert) * dp;
+            dp = rng.uniform() * (hi - lo) + lo;
+            h = perturbed_normal(cam, px, py, hp, rng, (float)(3 * pert * kPiD));
+            h.w = dp;
+        } else {
+            h = a.planes[center];
+            const float depth = h.w;
+            h.w = distance_to_origin(cam, px, py, depth, h);
+        }
+    } else {
+        const float depth = rng.uniform() * (a.dmax - a.dmin) + a.dmin;
+        h = random_normal(cam, px, py, rng, depth);
+        h.w = distance_to_origin(cam, px, py, depth, h);
+    }
+    uint32_t sel;
+    const float c = initial_cost(a, px, py, h, sW, sWR, tid, rs, &sel);
+    a.planes[center] = h;
+    a.costs[center] = c;
+    a.views[center] = sel;
+}
+
+/* Validity of the first site of direction k at extension round r (HPM.cu:1252-1445 and the
+ * Extended* functions 560-1034).  Directions: 0 left_up, 1 up_far, 2 right_up, 3 down_far,
+ * 4 right_down, 5 left_far, 6 left_down, 7 right_far (HPM.cu:1245). */
+__device__ __forceinline__ bool first_site_valid(int k, int r, int px, int py, int W, int H)
+{
+    const int s = 10 * r, d = 8 * r;
+    switch (k) {
+    case 1: return py > 4 + s;
+    case 3: return py < H - 5 - s;
+    case 5: return px > 4 + s;
+    case 7: return px < W - 5 - s;
+    case 0: return px > 4 + d && py > 5 + d;
+    case 2: return px < W - 6 - d && py > 4 + d;
+    case 4: return px < W - 5 - d && py < H - 6 - d;
+    default: return px > 5 + d && py < H - 5 - d;
+    }
+}
+
+/* NESP site choice of one direction at round r.  Strips: 5 sites 2 apart
+ * from +/-(5+10r), the right strip keeps the maximum (HPM.cu:1330, 744).
+ * Polylines: start (+/-5|6) shifted 8r outward, then 7 zig-zag steps of 2
+ * (HPM.cu:1346-1471). */
+__device__ int select_site(const PMArgs &a, int k, int r, int px, int py)
+{
+    const int W = a.W, H = a.H;
+    const float *costs = a.costs;
+    if (k & 1) {
+        const int dx = (k == 5) ? -1 : (k == 7 ? 1 : 0);
+        const int dy = (k == 1) ? -1 : (k == 3 ? 1 : 0);
+        const int off = 5 + 10 * r;
+        int best = (py + dy * off) * W + (px + dx * off);
+        float cmin = costs[best];
+        for (int i = 1; i < 5; ++i) {
+            bool ok;
+            switch (k) {
+            case 1: ok = py > 4 + 2 * i + 10 * r; break;
+            case 3: ok = py < H - 5 - 2 * i - 10 * r; break;
+            case 5: ok = px > 4 + 2 * i + 10 * r; break;
+            default: ok = px < W - 5 - 2 * i - 10 * r; break;
+            }
+            if (!ok) break;
+            const int q = (py + dy * (off + 2 * i)) * W + (px + dx * (off + 2 * i));
+            const float cq = costs[q];
+            if (k == 7 ? (cmin < cq) : (cq < cmin)) {
+                cmin = cq;
+                best = q;
+            }
+        }
+        return best;
+    }
+    int sx, sy, ex, ey, ox, oy; /* start, even step, odd step */
+    switch (k) {
+    case 0: sx = -5 - 8 * r; sy = -6 - 8 * r; ex = -2; ey = 0; ox = 0; oy = -2; break;
+    case 2: sx = 6 + 8 * r; sy = -5 - 8 * r; ex = 0; ey = -2; ox = 2; oy = 0; break;
+    case 4: sx = 5 + 8 * r; sy = 6 + 8 * r; ex = 2; ey = 0; ox = 0; oy = 2; break;
+    default: sx = -6 - 8 * r; sy = 5 + 8 * r; ex = 0; ey = 2; ox = -2; oy = 0; break;
+    }
+    int x = px + sx, y = py + sy;
+    int best = y * W + x;
+    float cmin = costs[best];
+    for (int i = 0; i < 7; ++i) {
+        if ((i & 1) == 0) {
+            x += ex;
+            y += ey;
+        } else {
+            x += ox;
+            y += oy;
+        }
+        if (x >= 0 && x < W && y < H && y >= 0) {
+            const int q = y * W + x;
+            const float cq = costs[q];
+            if (cq < cmin) {
+                cmin = cq;
+                best = q;
+            }
+        } else {
+            break;
+        }
+    }
+    return best;
+}
+
+__device__ __forceinline__ float restricted_prior(float depth_diff, float angle_cos, float two_dss, float two_ass)
+{
+    const float gamma = 0.5f;
+    const float angle_diff = acosf(angle_cos);
+    return gamma + expf(-depth_diff * depth_diff / two_dss) * expf(-angle_diff * angle_diff / two_ass);
+}
+
+/* One pixel of CheckerboardPropagation (HPM.cu:1222-1725) followed by
+ * PlaneHypothesisRefinement (HPM.cu:1143-1220). */
+__global__ void __launch_bounds__(kBlock) k_propagate(PMArgs a, int iter, int color)
+{
+    extern __shared__ float smem[];
+    float *sW = smem;
+    float *sWR = sW + kTaps * kBlock;
+    float *sCA = sWR + kTaps * kBlock; /* [8*S][kBlock] */
+    const int tid = threadIdx.y * kBlockX + threadIdx.x;
+    const int py = blockIdx.y * kBlockY + threadIdx.y;
+    const int px = blockIdx.x * (2 * kBlockX) + 2 * threadIdx.x + ((py + color) & 1);
+    if (px >= a.W || py >= a.rows_cov) return;
+    const int W = a.W, H = a.H, S = a.n - 1;
+    const int center = py * W + px;
+    const HpmCamera &cam = a.cam[0];
+    const RefStats rs = ref_window(a, px, py, sW, sWR, tid);
+    Rng rng;
+    rng.init(a.seed_lo, a.seed_hi, (uint32_t)center, (uint32_t)(1 + iter), a.salt);
+#define CA(k, v) sCA[((k) * S + (v)) * kBlock + tid]
+
+    for (int k = 0; k < 8; ++k)
+        for (int v = 0; v < S; ++v) CA(k, v) = 0.0f;
+    CA(0, 0) = 2.0f; /* float cost_array[8][32] = { 2.0f } (HPM.cu:1244) */
+
+    bool flag[8];
+    int pos[8];
+    pos[0] = center - 5 - 6 * W;
+    pos[1] = center - W * 5;
+    pos[2] = center + 6 - 5 * W;
+    pos[3] = center + W * 5;
+    pos[4] = center + 5 + 6 * W;
+    pos[5] = center - 5;
+    pos[6] = center - 6 + 5 * W;
+    pos[7] = center + 5;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        flag[k] = first_site_valid(k, 0, px, py, W, H);
+        if (flag[k]) {
+            pos[k] = select_site(a, k, 0, px, py);
+            cost_vector(a, px, py, a.planes[pos[k]], sW, sWR, tid, rs, &CA(k, 0), S * 0 + kBlock);
+        }
+    }
+
+    /* Extension: only the left-up polyline can extend, because
+     * bool symbol_eight_orientations[10] = { true } sets index 0 only
+     * (HPM.cu:1475).  JudgeExtend: HPM.cu:1036-1059. */
+    if (flag[0]) {
+        for (int r = 0; r < 3; ++r) {
+            const float good = (float)(0.8 * exp(-iter * iter * (3 - r) / 90.0));
+            int good_sum = 0, bad_sum = 0;
+            for (int v = 0; v < S; ++v) {
+                const float c = CA(0, v);
+                if (c < good) good_sum++;
+                if (c > 1.2f) bad_sum++;
+            }
+            if (good_sum >= 1 && bad_sum <= 2) break;
+            if (first_site_valid(0, r, px, py, W, H)) {
+                int best = select_site(a, 0, r, px, py);
+                bool fresh = true;
+                if (a.costs[best] > a.costs[pos[0]]) {
+                    best = pos[0];
+                    fresh = false;
+                }
+                pos[0] = best;
+                if (fresh) cost_vector(a, px, py, a.planes[best], sW, sWR, tid, rs, &CA(0, 0), kBlock);
+            }
+        }
+    }
+
+    /* Multi-hypothesis joint view selection, HPM.cu:1548-1613. */
+    float vw[kMaxSrc];
+    float sp[kMaxSrc];
+    const uint32_t nbm[4] = {flag[1] ? a.views[center - W * 5] : 0u, flag[3] ? a.views[center + W * 5] : 0u,
+                             flag[5] ? a.views[center - 5] : 0u, flag[7] ? a.views[center + 5] : 0u};
+    const float thr = (float)(0.8 * expf((float)(iter * iter) / (-90.0f)));
+    for (int v = 0; v < S; ++v) {
+        float prior = 0.0f;
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+            if (flag[2 * i + 1]) prior += ((nbm[i] >> v) & 1u) ? 0.9f : 0.1f;
+        float count = 0;
+        int count_false = 0;
+        float tmpw = 0;
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            const float c = CA(k, v);
+            if (c < thr) {
+                tmpw += expf(c * c / (-0.18f));
+                count++;
+            }
+            if (c > 1.2f) count_false++;
+        }
+        float p = 0.0f;
+        if (count > 2 && count_false < 3)
+            p = tmpw / count;
+        else if (count_false < 3)
+            p = expf(thr * thr / (-0.32f));
+        sp[v] = p * prior;
+        vw[v] = 0.0f;
+    }
+    {
+        float s = 0.0f;
+        for (int v = 0; v < S; ++v) s += sp[v];
+        const float inv = 1.0f / s;
+        float cum = 0.0f;
+        for (int v = 0; v < S; ++v) {
+            cum += sp[v] * inv;
+            sp[v] = cum;
+        }
+    }
+    for (int smp = 0; smp < 15; ++smp) {
+        const float rp = rng.uniform() - FLT_EPSILON;
+        for (int v = 0; v < S; ++v) {
+            if (sp[v] > rp) {
+                vw[v] += 1.0f;
+                break;
+            }
+        }
+    }
+    uint32_t tsv = 0;
+    float wn = 0.0f;
+    for (int v = 0; v < S; ++v)
+        if (vw[v] > 0) {
+            tsv |= 1u << v;
+            wn += vw[v];
+        }
+
+    float fc[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        float f = 0.0f;
+        const float4 hk = (a.geom && flag[k]) ? a.planes[pos[k]] : make_float4(0, 0, 0, 1);
+        for (int v = 0; v < S; ++v) {
+            if (vw[v] > 0) {
+                if (a.geom) {
+                    if (flag[k])
+                        f += vw[v] * (CA(k, v) + 0.1f * geom_cost(a, v + 1, hk, px, py));
+                    else
+                        f += vw[v] * (CA(k, v) + 0.1f * 5.0f);
+                } else {
+                    f += vw[v] * CA(k, v);
+                }
+            }
+        }
+        fc[k] = f / wn;
+    }
+    int min_idx = 0;
+    {
+        float m = fc[0];
+#pragma unroll
+        for (int k = 1; k < 8; ++k)
+            if (fc[k] <= m) {
+                m = fc[k];
+                min_idx = k;
+            }
+    }
+
+    float4 plane = a.planes[center];
+    /* re-score the current hypothesis (HPM.cu:1637-1650); the slot of
+     * direction 1 is free now that final costs are known */
+    float *cvn = &CA(1, 0);
+    cost_vector(a, px, py, plane, sW, sWR, tid, rs, cvn, kBlock);
+    float cost_now = 0.0f;
+    for (int v = 0; v < S; ++v) {
+        if (a.geom)
+            cost_now += vw[v] * (cvn[v * kBlock] + 0.1f * geom_cost(a, v + 1, plane, px, py));
+        else
+            cost_now += vw[v] * cvn[v * kBlock];
+    }
+    cost_now /= wn;
+    float cost = cost_now;
+    uint32_t sel = a.views[center];
+    float depth_now = depth_from_plane(cam, plane, px, py);
+
+    float restricted_cost = 0.0f;
+    if (a.prior) {
+        const float depth_sigma = (a.dmax - a.dmin) / 64.0f;
+        const float two_dss = 2 * depth_sigma * depth_sigma;
+        const float angle_sigma = (float)(kPiD * (5.0f / 180.0f));
+        const float two_ass = 2 * angle_sigma * angle_sigma;
+        const float4 pp = a.prior_planes[center];
+        const float depth_prior = depth_from_plane(cam, pp, px, py);
+        const float beta = 0.18f;
+        if (a.masks[center] > 0) {
+            float rfc[8];
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+                rfc[k] = 0.0f;
+                if (flag[k]) {
+                    const float4 hq = a.planes[pos[k]];
+                    const float dn = depth_from_plane(cam, hq, px, py);
+                    const float pr = restricted_prior(dn - depth_prior, dot3(pp, hq), two_dss, two_ass);
+                    rfc[k] = expf(-fc[k] * fc[k] / beta) * pr;
+                }
+            }
+            int max_idx = 0;
+            {
+                float m = rfc[0];
+#pragma unroll
+                for (int k = 1; k < 8; ++k)
+                    if (rfc[k] >= m) {
+                        m = rfc[k];
+                        max_idx = k;
+                    }
+            }
+            const float dn = depth_from_plane(cam, plane, px, py);
+            const float pr = restricted_prior(dn - depth_prior, dot3(pp, plane), two_dss, two_ass);
+            const float rcn = expf(-cost_now * cost_now / beta) * pr;
+            if (flag[max_idx]) {
+                const float4 hb = a.planes[pos[max_idx]];
+                const float db = depth_from_plane(cam, hb, px, py);
+                if (db >= a.dmin && db <= a.dmax && rfc[max_idx] > rcn) {
+                    depth_now = db;
+                    plane = hb;
+                    cost = fc[max_idx];
+                    restricted_cost = rfc[max_idx];
+                    sel = tsv;
+                }
+            }
+        } else if (flag[min_idx]) {
+            const float4 hb = a.planes[pos[min_idx]];
+            const float db = depth_from_plane(cam, hb, px, py);
+            if (db >= a.dmin && db <= a.dmax && fc[min_idx] < cost_now) {
+                depth_now = db;
+                plane = hb;
+                cost = fc[min_idx];
+            }
+        }
+    }
+    if (!a.prior && flag[min_idx]) {
+        const float4 hb = a.planes[pos[min_idx]];
+        const float db = depth_from_plane(cam, hb, px, py);
+        if (db >= a.dmin && db <= a.dmax && fc[min_idx] < cost_now) {
+            depth_now = db;
+            plane = hb;
+            cost = fc[min_idx];
+            sel = tsv;
+        }
+        if (cost != cost) {
+            depth_now = db;
+            plane = hb;
+            sel = tsv;
+        }
+    }
+
+    /* PlaneHypothesisRefinement, HPM.cu:1143-1220 */
+    {
+        const float pert = 0.02f;
+        const float depth_sigma = (a.dmax - a.dmin) / 64.0f;
+        const float two_dss = 2 * depth_sigma * depth_sigma;
+        const float angle_sigma = (float)(kPiD * (5.0f / 180.0f));
+        const float two_ass = 2 * angle_sigma * angle_sigma;
+        const float beta = 0.18f;
+        float depth_prior = 0.0f;
+        const bool use_prior = a.prior && a.masks[center] > 0;
+        float4 pp = make_float4(0, 0, 0, 0);
+        float depth_rand;
+        float4 n_rand;
+        if (use_prior) {
+            pp = a.prior_planes[center];
+            depth_prior = depth_from_plane(cam, pp, px, py);
+            depth_rand = rng.uniform() * 6 * depth_sigma + (depth_prior - 3 * depth_sigma);
+            n_rand = perturbed_normal(cam, px, py, pp, rng, angle_sigma);
+        } else {
+            depth_rand = rng.uniform() * (a.dmax - a.dmin) + a.dmin;
+            n_rand = random_normal(cam, px, py, rng, depth_now);
+        }
+        const float lo = (1 - pert) * depth_now, hi = (1 + pert) * depth_now;
+        const float depth_pert = rng.uniform() * (hi - lo) + lo;
+        const float4 n_pert = perturbed_normal(cam, px, py, plane, rng, (float)(pert * kPiD));
+        const float depths[5] = {depth_rand, depth_now, depth_rand, depth_now, depth_pert};
+        const float4 normals[5] = {plane, n_rand, n_rand, n_pert, plane};
+        float *cvr = &CA(2, 0);
+#pragma unroll 1
+        for (int i = 0; i < 5; ++i) {
+            float4 t = normals[i];
+            t.w = distance_to_origin(cam, px, py, depths[i], t);
+            cost_vector(a, px, py, t, sW, sWR, tid, rs, cvr, kBlock);
+            float tc = 0.0f;
+            for (int v = 0; v < S; ++v) {
+                if (vw[v] > 0) {
+                    if (a.geom)
+                        tc += vw[v] * (cvr[v * kBlock] + 0.1f * geom_cost(a, v + 1, t, px, py));
+                    else
+                        tc += vw[v] * cvr[v * kBlock];
+                }
+            }
+            tc /= wn;
+            const float depth_before = depth_from_plane(cam, t, px, py);
+            if (use_prior) {
+                const float dd = depths[i] - depth_prior;
+                const float pr = restricted_prior(dd, dot3(pp, t), two_dss, two_ass);
+                const float rtc = expf(-tc * tc / beta) * pr;
+                if (depth_before >= a.dmin && depth_before <= a.dmax && rtc > restricted_cost) {
+                    depth_now = depth_before;
+                    plane = t;
+                    cost = tc;
+                    restricted_cost = rtc;
+                }
+            } else {
+                if (depth_before >= a.dmin && depth_before <= a.dmax && tc < cost) {
+                    depth_now = depth_before;
+                    plane = t;
+                    cost = tc;
+                }
+            }
+        }
+    }
+#undef CA
+    a.planes[center] = plane;
+    a.costs[center] = cost;
+    a.views[center] = sel;
+}
+
+/* GetDepthandNormal, HPM.cu:1751-1764 */
+__global__ void k_depth_normal(PMArgs a, float4 *planes)
+{
+    const int px = blockIdx.x * blockDim.x + threadIdx.x;
+    const int py = blockIdx.y * blockDim.y + threadIdx.y;
+    if (px >= a.W || py >= a.H) return;
+    const int c = py * a.W + px;
+    float4 h = planes[c];
+    h.w = depth_from_plane(a.cam[0], h, px, py);
+    planes[c] = transform_normal(a.cam[0], h);
+}
+
+/* CheckerboardFilter, HPM.cu:1766-1904 */
+__global__ void k_filter(PMArgs a, float4 *pl, const float *costs, int color)
+{
+    const int py = blockIdx.y * blockDim.y + threadIdx.y;
+    const int px = blockIdx.x * (2 * blockDim.x) + 2 * threadIdx.x + ((py + color) & 1);
+    const int W = a.W, H = a.H;
+    if (px >= W || py >= a.rows_cov) return;
+    const int center = py * W + px;
+    if (costs[center] < 0.001f) return;
+    float f[21];
+    int n = 0;
+    f[n++] = pl[center].w;
+    const int left = center - 1, leftleft = center - 3, up = center - W, upup = center - 3 * W;
+    const int down = center + W, downdown = center + 3 * W, right = center + 1, rightright = center + 3;
+    if (py > 0) f[n++] = pl[up].w;
+    if (py > 2) f[n++] = pl[upup].w;
+    if (py > 4) f[n++] = pl[upup - W * 2].w;
+    if (py < H - 1) f[n++] = pl[down].w;
+    if (py < H - 3) f[n++] = pl[downdown].w;
+    if (py < H - 5) f[n++] = pl[downdown + W * 2].w;
+    if (px > 0) f[n++] = pl[left].w;
+    if (px > 2) f[n++] = pl[leftleft].w;
+    if (px > 4) f[n++] = pl[leftleft - 2].w;
+    if (px < W - 1) f[n++] = pl[right].w;
+    if (px < W - 3) f[n++] = pl[rightright].w;
+    if (px < W - 5) f[n++] = pl[rightright + 2].w;
+    if (py > 0 && px < W - 2) f[n++] = pl[up + 2].w;
+    if (py < H - 1 && px < W - 2) f[n++] = pl[down + 2].w;
+    if (py > 0 && px > 1) f[n++] = pl[up - 2].w;
+    if (py < H - 1 && px > 1) f[n++] = pl[down - 2].w;
+    if (px > 0 && py > 2) f[n++] = pl[left - W * 2].w;
+    if (px < W - 1 && py > 2) f[n++] = pl[right - W * 2].w;
+    if (px > 0 && py < H - 2) f[n++] = pl[left + W * 2].w;
+    if (px < W - 1 && py < H - 2) f[n++] = pl[right + W * 2].w;
+    sort_small(f, n);
+    const int m = n / 2;
+    pl[center].w = (n % 2 == 0) ? (f[m - 1] + f[m]) / 2 : f[m];
+}
+
+__global__ void __launch_bounds__(kBlock) k_cost_vectors(PMArgs a, const float4 *planes, float *out)
+{
+    __shared__ float sW[kTaps * kBlock];
+    __shared__ float sWR[kTaps * kBlock];
+    const int tid = threadIdx.y * kBlockX + threadIdx.x;
+    const int px = blockIdx.x * kBlockX + threadIdx.x;
+    const int py = blockIdx.y * kBlockY + threadIdx.y;
+    if (px >= a.W || py >= a.H) return;
+    const RefStats rs = ref_window(a, px, py, sW, sWR, tid);
+    const int c = py * a.W + px;
+    const int S = a.n - 1;
+    for (int v = 1; v < a.n; ++v) out[(size_t)c * S + v - 1] = ncc(a, v, px, py, planes[c], sW, sWR, tid, rs);
+}
+
+__global__ void __launch_bounds__(kBlock) k_initial_costs(PMArgs a, const float4 *planes, float *cost,
+                                                          uint32_t *views)
+{
+    __shared__ float sW[kTaps * kBlock];
+    __shared__ float sWR[kTaps * kBlock];
+    const int tid = threadIdx.y * kBlockX + threadIdx.x;
+    const int px = blockIdx.x * kBlockX + threadIdx.x;
+    const int py = blockIdx.y * kBlockY + threadIdx.y;
+    if (px >= a.W || py >= a.H) return;
+    const RefStats rs = ref_window(a, px, py, sW, sWR, tid);
+    const int c = py * a.W + px;
+    cost[c] = initial_cost(a, px, py, planes[c], sW, sWR, tid, rs, &views[c]);
+}
+
+__global__ void k_geom_costs(PMArgs a, const float4 *planes, float *out)
+{
+    const int px = blockIdx.x * blockDim.x + threadIdx.x;
+    const int py = blockIdx.y * blockDim.y + threadIdx.y;
+    if (px >= a.W || py >= a.H) return;
+    const int c = py * a.W + px;
+    const int S = a.n - 1;
+    for (int v = 1; v < a.n; ++v) out[(size_t)c * S + v - 1] = geom_cost(a, v, planes[c], px, py);
+}
+
+}  // namespace
+
+int rows_covered(int H)
+{
+    const int cov = 2 * (((H / 2) + 15) / 16) * 16;
+    return cov < H ? cov : H;
+}
+
+cudaError_t launch_pair_geom(const PMArgs &a, PairGeom *out, cudaStream_t s)
+{
+    k_pair_geom<<<1, 64, 0, s>>>(a, out);
+    return cudaGetLastError();
+}
+
+static dim3 pixel_grid(int W, int H) { return dim3((W + kBlockX - 1) / kBlockX, (H + kBlockY - 1) / kBlockY); }
+
+cudaError_t launch_init(const PMArgs &a, cudaStream_t s)
+{
+    k_init<<<pixel_grid(a.W, a.H), dim3(kBlockX, kBlockY), 0, s>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_propagate(const PMArgs &a, int iter, int color, cudaStream_t s)
+{
+    const int S = a.n - 1;
+    const size_t smem = (size_t)(2 * kTaps + 8 * S) * kBlock * sizeof(float);
+    static bool attr_set = false;
+    if (!attr_set) {
+        cudaFuncSetAttribute(k_propagate, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (2 * kTaps + 8 * kMaxSrc) * kBlock * (int)sizeof(float));
+        attr_set = true;
+    }
+    if (a.rows_cov <= 0) return cudaSuccess;
+    dim3 grid((a.W + 2 * kBlockX - 1) / (2 * kBlockX), (a.rows_cov + kBlockY - 1) / kBlockY);
+    k_propagate<<<grid, dim3(kBlockX, kBlockY), smem, s>>>(a, iter, color);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_depth_normal_filter(const PMArgs &a, float4 *planes, const float *costs, cudaStream_t s)
+{
+    dim3 b(16, 16), g((a.W + 15) / 16, (a.H + 15) / 16);
+    k_depth_normal<<<g, b, 0, s>>>(a, planes);
+    if (a.rows_cov > 0) {
+        dim3 fb(32, 8), fg((a.W + 63) / 64, (a.rows_cov + 7) / 8);
+        k_filter<<<fg, fb, 0, s>>>(a, planes, costs, 0);
+        k_filter<<<fg, fb, 0, s>>>(a, planes, costs, 1);
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_cost_vectors(const PMArgs &a, const float4 *planes, float *out, cudaStream_t s)
+{
+    k_cost_vectors<<<pixel_grid(a.W, a.H), dim3(kBlockX, kBlockY), 0, s>>>(a, planes, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_initial_costs(const PMArgs &a, const float4 *planes, float *cost, uint32_t *views,
+                                 cudaStream_t s)
+{
+    k_initial_costs<<<pixel_grid(a.W, a.H), dim3(kBlockX, kBlockY), 0, s>>>(a, planes, cost, views);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_geom_costs(const PMArgs &a, const float4 *planes, float *out, cudaStream_t s)
+{
+    dim3 b(16, 16), g((a.W + 15) / 16, (a.H + 15) / 16);
+    k_geom_costs<<<g, b, 0, s>>>(a, planes, out);
+    return cudaGetLastError();
+}
+
+}  // namespace hpm

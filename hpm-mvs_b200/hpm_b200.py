@@ -1,0 +1,278 @@
+"""Python binding of libhpm_b200.so (the C ABI in include/hpm_b200.h).
+
+This module is a thin ctypes layer for tests, the benchmark and Python
+callers; the product is the CUDA/C++ library.  It fails loudly when the
+library is missing: there is no CPU fallback.
+
+Array conventions follow the reference's host buffers:
+  images  float32 [H, W];  cams  structured array of CAMERA_DTYPE;
+  planes  float32 [H, W, 4];  costs  float32 [H, W].
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libhpm_b200.so")
+
+CAMERA_DTYPE = np.dtype(
+    [("K", "<f4", 9), ("R", "<f4", 9), ("t", "<f4", 3), ("height", "<i4"), ("width", "<i4"),
+     ("depth_min", "<f4"), ("depth_max", "<f4")]
+)
+MAX_IMAGES = 33
+
+HPM_OK = 0
+STATUS_NAMES = {0: "HPM_OK", -1: "HPM_ERR_ARG", -2: "HPM_ERR_CUDA", -3: "HPM_ERR_IO", -4: "HPM_ERR_STATE",
+                -5: "HPM_ERR_TIMEOUT", -6: "HPM_ERR_NOMEM"}
+
+# every symbol include/hpm_b200.h declares
+EXPORTED = [
+    "hpm_default_params", "hpm_create", "hpm_destroy", "hpm_last_error", "hpm_set_views", "hpm_set_geom_depths",
+    "hpm_set_hypotheses", "hpm_set_prior", "hpm_clear_prior", "hpm_run_patchmatch", "hpm_get_result",
+    "hpm_get_selected_views", "hpm_device_state", "hpm_stream", "hpm_jbu", "hpm_cost_vectors",
+    "hpm_initial_costs", "hpm_geom_costs", "hpm_depth_normal_filter", "hpm_profile_enable", "hpm_profile_read",
+    "hpm_count_enable", "hpm_count_read", "hpm_write_dmb", "hpm_read_dmb", "hpm_read_camera", "hpm_read_pair",
+]
+
+
+class HpmParams(ctypes.Structure):
+    _fields_ = [("max_iterations", ctypes.c_int), ("patch_size", ctypes.c_int), ("radius_increment", ctypes.c_int),
+                ("sigma_spatial", ctypes.c_float), ("sigma_color", ctypes.c_float), ("top_k", ctypes.c_int),
+                ("depth_min", ctypes.c_float), ("depth_max", ctypes.c_float), ("geom_consistency", ctypes.c_int),
+                ("multi_geometry", ctypes.c_int), ("planar_prior", ctypes.c_int),
+                ("honour_max_iterations", ctypes.c_int), ("seed", ctypes.c_uint64)]
+
+
+class HpmError(RuntimeError):
+    pass
+
+
+_lib = None
+
+
+def lib() -> ctypes.CDLL:
+    """Load the in-tree library; raises if it has not been built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise HpmError(f"{LIB_PATH} is missing: build it with `make -C hpm-mvs_b200`")
+        L = ctypes.CDLL(LIB_PATH)
+        L.hpm_last_error.restype = ctypes.c_char_p
+        L.hpm_last_error.argtypes = [ctypes.c_void_p]
+        L.hpm_stream.restype = ctypes.c_void_p
+        L.hpm_stream.argtypes = [ctypes.c_void_p]
+        L.hpm_create.argtypes = [ctypes.POINTER(ctypes.c_void_p), ctypes.c_int]
+        for name in ["hpm_destroy", "hpm_clear_prior"]:
+            getattr(L, name).argtypes = [ctypes.c_void_p]
+        _lib = L
+    return _lib
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(ctypes.c_void_p)
+
+
+def default_params(depth_min: float, depth_max: float, *, seed: int = 0, geom: bool = False,
+                   prior: bool = False, multi_geometry: bool = False) -> HpmParams:
+    p = HpmParams()
+    lib().hpm_default_params(ctypes.byref(p))
+    p.depth_min = depth_min
+    p.depth_max = depth_max
+    p.seed = seed
+    p.geom_consistency = int(geom)
+    p.planar_prior = int(prior)
+    p.multi_geometry = int(multi_geometry)
+    return p
+
+
+class Context:
+    """One hpm_ctx: device buffers of one problem plus its CUDA stream."""
+
+    def __init__(self, device: int = 0):
+        self._h = ctypes.c_void_p()
+        rc = lib().hpm_create(ctypes.byref(self._h), device)
+        if rc != HPM_OK:
+            raise HpmError(f"hpm_create failed: {STATUS_NAMES.get(rc, rc)}")
+        self.shape = None
+        self.n = 0
+
+    def close(self):
+        if self._h:
+            lib().hpm_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @property
+    def handle(self):
+        return self._h
+
+    def _check(self, rc: int, what: str) -> None:
+        if rc != HPM_OK:
+            msg = lib().hpm_last_error(self._h)
+            raise HpmError(f"{what}: {STATUS_NAMES.get(rc, rc)}: {msg.decode() if msg else ''}")
+
+    def set_views(self, images, cams) -> None:
+        imgs = [np.ascontiguousarray(i, dtype=np.float32) for i in images]
+        cams = np.ascontiguousarray(cams, dtype=CAMERA_DTYPE)
+        for i, im in enumerate(imgs):
+            if im.shape != (int(cams[i]["height"]), int(cams[i]["width"])):
+                raise ValueError(f"image {i} shape {im.shape} does not match its camera")
+        arr = (ctypes.c_void_p * len(imgs))(*[i.ctypes.data for i in imgs])
+        self._check(lib().hpm_set_views(self._h, arr, _p(cams), len(imgs)), "hpm_set_views")
+        self._imgs = imgs  # keep alive until the synchronous upload returned (it has)
+        self.shape = imgs[0].shape
+        self.n = len(imgs)
+
+    def set_geom_depths(self, depths) -> None:
+        ds = [np.ascontiguousarray(d, dtype=np.float32) for d in depths]
+        arr = (ctypes.c_void_p * len(ds))(*[d.ctypes.data for d in ds])
+        self._check(lib().hpm_set_geom_depths(self._h, arr), "hpm_set_geom_depths")
+
+    def set_hypotheses(self, planes, costs=None) -> None:
+        planes = np.ascontiguousarray(planes, dtype=np.float32)
+        costs = None if costs is None else np.ascontiguousarray(costs, dtype=np.float32)
+        self._check(lib().hpm_set_hypotheses(self._h, _p(planes), _p(costs)), "hpm_set_hypotheses")
+
+    def set_prior(self, prior_planes, masks) -> None:
+        pp = np.ascontiguousarray(prior_planes, dtype=np.float32)
+        mk = np.ascontiguousarray(masks, dtype=np.uint32)
+        self._check(lib().hpm_set_prior(self._h, _p(pp), _p(mk)), "hpm_set_prior")
+
+    def clear_prior(self) -> None:
+        self._check(lib().hpm_clear_prior(self._h), "hpm_clear_prior")
+
+    def run_patchmatch(self, params: HpmParams) -> None:
+        self._check(lib().hpm_run_patchmatch(self._h, ctypes.byref(params)), "hpm_run_patchmatch")
+
+    def get_result(self):
+        h, w = self.shape
+        planes = np.empty((h, w, 4), np.float32)
+        costs = np.empty((h, w), np.float32)
+        self._check(lib().hpm_get_result(self._h, _p(planes), _p(costs)), "hpm_get_result")
+        return planes, costs
+
+    def get_selected_views(self):
+        h, w = self.shape
+        v = np.empty((h, w), np.uint32)
+        self._check(lib().hpm_get_selected_views(self._h, _p(v)), "hpm_get_selected_views")
+        return v
+
+    def cost_vectors(self, planes):
+        h, w = self.shape
+        planes = np.ascontiguousarray(planes, dtype=np.float32)
+        out = np.empty((h, w, self.n - 1), np.float32)
+        self._check(lib().hpm_cost_vectors(self._h, _p(planes), _p(out)), "hpm_cost_vectors")
+        return out
+
+    def initial_costs(self, planes):
+        h, w = self.shape
+        planes = np.ascontiguousarray(planes, dtype=np.float32)
+        cost = np.empty((h, w), np.float32)
+        views = np.empty((h, w), np.uint32)
+        self._check(lib().hpm_initial_costs(self._h, _p(planes), _p(cost), _p(views)), "hpm_initial_costs")
+        return cost, views
+
+    def geom_costs(self, planes):
+        h, w = self.shape
+        planes = np.ascontiguousarray(planes, dtype=np.float32)
+        out = np.empty((h, w, self.n - 1), np.float32)
+        self._check(lib().hpm_geom_costs(self._h, _p(planes), _p(out)), "hpm_geom_costs")
+        return out
+
+    def depth_normal_filter(self, planes, costs):
+        planes = np.array(planes, dtype=np.float32, copy=True, order="C")
+        costs = np.ascontiguousarray(costs, dtype=np.float32)
+        self._check(lib().hpm_depth_normal_filter(self._h, _p(planes), _p(costs)), "hpm_depth_normal_filter")
+        return planes
+
+    def jbu(self, guide, coarse_depth, coarse_normal):
+        guide = np.ascontiguousarray(guide, dtype=np.float32)
+        cd = np.ascontiguousarray(coarse_depth, dtype=np.float32)
+        cn = np.ascontiguousarray(coarse_normal, dtype=np.float32)
+        rows, cols = guide.shape
+        s_rows, s_cols = cd.shape
+        od = np.zeros((rows, cols), np.float32)
+        on = np.zeros((rows, cols, 3), np.float32)
+        self._check(lib().hpm_jbu(self._h, _p(guide), cols, rows, _p(cd), _p(cn), s_cols, s_rows, _p(od), _p(on)),
+                    "hpm_jbu")
+        return od, on
+
+    def profile_enable(self, on: bool = True) -> None:
+        self._check(lib().hpm_profile_enable(self._h, int(on)), "hpm_profile_enable")
+
+    def profile_read(self):
+        ms = (ctypes.c_float * 4)()
+        cnt = (ctypes.c_int * 4)()
+        self._check(lib().hpm_profile_read(self._h, ms, cnt), "hpm_profile_read")
+        names = ["init", "propagate", "finalize", "jbu"]
+        return {n: (float(ms[i]), int(cnt[i])) for i, n in enumerate(names)}
+
+    def count_enable(self, on: bool = True) -> None:
+        self._check(lib().hpm_count_enable(self._h, int(on)), "hpm_count_enable")
+
+    def count_read(self):
+        a = ctypes.c_uint64()
+        b = ctypes.c_uint64()
+        self._check(lib().hpm_count_read(self._h, ctypes.byref(a), ctypes.byref(b)), "hpm_count_read")
+        return int(a.value), int(b.value)
+
+    def stream(self) -> int:
+        return int(lib().hpm_stream(self._h) or 0)
+
+
+def write_dmb(path: str, data: np.ndarray) -> None:
+    a = np.ascontiguousarray(data, dtype=np.float32)
+    h, w = a.shape[:2]
+    nb = 1 if a.ndim == 2 else a.shape[2]
+    rc = lib().hpm_write_dmb(path.encode(), _p(a), h, w, nb)
+    if rc != HPM_OK:
+        raise HpmError(f"hpm_write_dmb({path}): {STATUS_NAMES.get(rc, rc)}")
+
+
+def read_dmb(path: str) -> np.ndarray:
+    h, w, nb = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+    rc = lib().hpm_read_dmb(path.encode(), None, ctypes.c_size_t(0), ctypes.byref(h), ctypes.byref(w),
+                            ctypes.byref(nb))
+    if rc != HPM_OK:
+        raise HpmError(f"hpm_read_dmb({path}): {STATUS_NAMES.get(rc, rc)}")
+    out = np.empty((h.value, w.value, nb.value), np.float32)
+    rc = lib().hpm_read_dmb(path.encode(), _p(out), ctypes.c_size_t(out.size), None, None, None)
+    if rc != HPM_OK:
+        raise HpmError(f"hpm_read_dmb({path}): {STATUS_NAMES.get(rc, rc)}")
+    return out[..., 0] if nb.value == 1 else out
+
+
+def read_camera(path: str) -> np.ndarray:
+    cam = np.zeros(1, CAMERA_DTYPE)
+    rc = lib().hpm_read_camera(path.encode(), _p(cam))
+    if rc != HPM_OK:
+        raise HpmError(f"hpm_read_camera({path}): {STATUS_NAMES.get(rc, rc)}")
+    return cam[0]
+
+
+def read_pair(path: str):
+    n = ctypes.c_int()
+    rc = lib().hpm_read_pair(path.encode(), ctypes.byref(n), None, None, None, 0)
+    if rc != HPM_OK:
+        raise HpmError(f"hpm_read_pair({path}): {STATUS_NAMES.get(rc, rc)}")
+    refs = np.zeros(n.value, np.int32)
+    counts = np.zeros(n.value, np.int32)
+    srcs = np.zeros((n.value, MAX_IMAGES - 1), np.int32)
+    rc = lib().hpm_read_pair(path.encode(), ctypes.byref(n), _p(refs), _p(counts), _p(srcs), n.value)
+    if rc != HPM_OK:
+        raise HpmError(f"hpm_read_pair({path}): {STATUS_NAMES.get(rc, rc)}")
+    return [(int(refs[i]), [int(s) for s in srcs[i, :counts[i]]]) for i in range(n.value)]

@@ -1,0 +1,183 @@
+/*
+ * hpm_b200.h - C ABI of the B200-native HPM-MVS PatchMatch path.
+ *
+ * This is the drop-in boundary: plain pointers and sizes, no C++ or torch
+ * types, status codes instead of exit().  Each entry point names the
+ * reference interface it replaces (file:line in the HPM-MVS repository).
+ *
+ * Conventions (those of the reference's host buffers):
+ *   images        float32, row-major [height][width], gray 0..255
+ *                 (HPM.cpp:492-495 converts the uint8 image to float)
+ *   planes        float32 x4 per pixel, row-major: during PatchMatch
+ *                 (nx, ny, nz, dist) in the reference camera frame; after a
+ *                 pass (world-frame normal, depth)  (HPM.cu:1751-1764)
+ *   costs         float32 per pixel
+ *   view masks    uint32 per pixel, bit i = source view i selected
+ *   prior masks   uint32 per pixel, non-zero = a prior plane is present
+ *
+ * Every function returns HPM_OK (0) or a negative HpmStatus; the message of
+ * the last failure of a context is available from hpm_last_error().
+ * A context is used by one host thread at a time; all device work is issued
+ * on the context's own CUDA stream.
+ */
+#ifndef HPM_B200_H
+#define HPM_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    HPM_OK = 0,
+    HPM_ERR_ARG = -1,     /* invalid argument (null pointer, bad size, too many views) */
+    HPM_ERR_CUDA = -2,    /* a CUDA runtime call failed */
+    HPM_ERR_IO = -3,      /* a file could not be read or written */
+    HPM_ERR_STATE = -4,   /* call out of order (e.g. run before set_views) */
+    HPM_ERR_TIMEOUT = -5, /* a bounded device-side wait gave up */
+    HPM_ERR_NOMEM = -6    /* device allocation failed */
+} HpmStatus;
+
+/* Maximum number of images of one problem: the reference view plus 32
+ * sources (cost_vector[32], HPM.cu:402; 32-bit view masks, HPM.cu:55-63). */
+#define HPM_MAX_IMAGES 33
+
+/* Same layout as the reference's Camera (HPM-MVS/main.h:44-52). */
+typedef struct {
+    float K[9];
+    float R[9];
+    float t[3];
+    int height;
+    int width;
+    float depth_min;
+    float depth_max;
+} HpmCamera;
+
+/* Mirrors PatchMatchParams (HPM-MVS/HPM.h:29-46).  patch_size,
+ * radius_increment, sigma_spatial, sigma_color and top_k keep the
+ * reference's defaults (11, 2, 5, 3, 4); max_iterations is accepted but, as in
+ * the reference (HPM.cu:1933), every pass runs 3 iterations unless
+ * honour_max_iterations is set. */
+typedef struct {
+    int max_iterations;
+    int patch_size;
+    int radius_increment;
+    float sigma_spatial;
+    float sigma_color;
+    int top_k;
+    float depth_min; /* already widened: cam depth_min * 0.6 (HPM.cpp:553) */
+    float depth_max; /* already widened: cam depth_max * 1.2 (HPM.cpp:554) */
+    int geom_consistency;
+    int multi_geometry;
+    int planar_prior;
+    int honour_max_iterations; /* 0 = reference behaviour (always 3) */
+    uint64_t seed;             /* Philox key of this pass's random stream */
+} HpmParams;
+
+/* Fills p with the reference defaults (HPM.h:29-46). */
+void hpm_default_params(HpmParams *p);
+
+typedef struct hpm_ctx hpm_ctx;
+
+/* Creates a context on `device` (the reference hard-codes cudaSetDevice(0),
+ * main.cpp:38).  Replaces the HPM constructor (HPM.cpp:99). */
+int hpm_create(hpm_ctx **ctx, int device);
+/* Frees every device buffer; replaces HPM::~HPM / Release*Memory
+ * (HPM.cpp:101-133, 1283-1307). */
+int hpm_destroy(hpm_ctx *ctx);
+const char *hpm_last_error(const hpm_ctx *ctx);
+
+/* Uploads the images and cameras of one problem, reference view first.
+ * images[i] is cams[i].height x cams[i].width floats.  Replaces the texture
+ * set-up of HPM::CudaSpaceInitialization (HPM.cpp:591-633); the 3200-pixel
+ * cap of InuputInitialization (HPM.cpp:524-551) is the caller's job. */
+int hpm_set_views(hpm_ctx *ctx, const float *const *images, const HpmCamera *cams, int num_images);
+
+/* Depth maps of the reference and source views for the geometric-
+ * consistency term (HPM.cpp:561-588, 635-660); depths[i] has the size of
+ * cams[i] given to hpm_set_views. */
+int hpm_set_geom_depths(hpm_ctx *ctx, const float *const *depths);
+
+/* Seeds the hypothesis state (HPM.cpp:662-695: geometric passes load the
+ * previous depths/normals/costs).  planes may hold (world normal, depth) as
+ * written by a previous pass.  costs may be NULL (zeros). */
+int hpm_set_hypotheses(hpm_ctx *ctx, const float *planes, const float *costs);
+
+/* Planar prior of the next pass: per-pixel ref-frame plane (n, dist) and
+ * mask.  Replaces ReloadPlanarPriorInitialization (HPM.cpp:901-921) and
+ * CudaPlanarPriorInitializationSupplement (HPM.cpp:1099-1123). */
+int hpm_set_prior(hpm_ctx *ctx, const float *prior_planes, const uint32_t *masks);
+/* Drops the prior (HPM::ReleasePriorCudaMemory, HPM.cpp:1283-1286). */
+int hpm_clear_prior(hpm_ctx *ctx);
+
+/* One PatchMatch pass: initialisation, 3 red/black iterations, depth and
+ * normal conversion, checkerboard median filter.  Replaces
+ * HPM::RunPatchMatch (HPM.cu:1906-1957).  The hypothesis state stays on the
+ * device for the next pass, as in the reference. */
+int hpm_run_patchmatch(hpm_ctx *ctx, const HpmParams *params);
+
+/* Copies the pass result to the host: planes = (world normal, depth),
+ * costs.  Either pointer may be NULL.  Replaces the D2H copies of
+ * HPM.cu:1954-1955 and GetPlaneHypothesis / GetCost (HPM.cpp:739-747). */
+int hpm_get_result(hpm_ctx *ctx, float *planes, float *costs);
+/* Selected-view masks of the last pass (selected_views_cuda). */
+int hpm_get_selected_views(hpm_ctx *ctx, uint32_t *views);
+
+/* Device pointers of the state, for callers that keep data in HBM.
+ * Valid until the next hpm_set_views with a larger size or hpm_destroy. */
+int hpm_device_state(hpm_ctx *ctx, float **planes, float **costs, uint32_t **views);
+/* The context's CUDA stream (cudaStream_t as void*). */
+void *hpm_stream(hpm_ctx *ctx);
+
+/* Joint bilateral upsampling of a coarse prior (depth + world normal) to the
+ * guide's resolution.  Replaces HPM::JointBilateralUpsampling
+ * (HPM.cpp:1215-1281) and JBU::CudaRun / JBU_cu (HPM.cu:1984-2088).
+ * coarse_normal and out_normal are 3 floats per pixel.  Returns HPM_OK and
+ * leaves the outputs untouched when the integer scale is 1 (HPM.cpp:1219). */
+int hpm_jbu(hpm_ctx *ctx, const float *guide, int cols, int rows, const float *coarse_depth,
+            const float *coarse_normal, int s_cols, int s_rows, float *out_depth, float *out_normal);
+
+/* Deterministic building blocks exposed for parity checks. */
+
+/* ComputeMultiViewCostVector (HPM.cu:438-443) for one ref-frame plane per
+ * pixel of the current problem; out holds (num_images-1) floats per pixel. */
+int hpm_cost_vectors(hpm_ctx *ctx, const float *planes, float *out);
+/* ComputeMultiViewInitialCostandSelectedViews (HPM.cu:399-436) per pixel. */
+int hpm_initial_costs(hpm_ctx *ctx, const float *planes, float *out_cost, uint32_t *out_views);
+/* ComputeGeomConsistencyCost (HPM.cu:483-508) per pixel and source view,
+ * against the depth maps of hpm_set_geom_depths. */
+int hpm_geom_costs(hpm_ctx *ctx, const float *planes, float *out);
+/* GetDepthandNormal + Black/RedPixelFilter (HPM.cu:1751-1904) on given
+ * ref-frame planes and costs of the current problem (in place). */
+int hpm_depth_normal_filter(hpm_ctx *ctx, float *planes, const float *costs);
+
+/* Per-kernel CUDA-event timing of the passes run while enabled. */
+int hpm_profile_enable(hpm_ctx *ctx, int enable);
+/* kernel times in ms accumulated since enable: [init, propagate, finalize,
+ * jbu]; counts = launches of each.  Either pointer may be NULL. */
+int hpm_profile_read(hpm_ctx *ctx, float *ms4, int *counts4);
+/* Number of cost-vector evaluations made by the last pass (one evaluation =
+ * num_images-1 NCC windows); requires hpm_count_enable(ctx, 1) before it. */
+int hpm_count_enable(hpm_ctx *ctx, int enable);
+int hpm_count_read(hpm_ctx *ctx, uint64_t *cost_vectors, uint64_t *geom_terms);
+
+/* ---- files (drop-in formats) ---- */
+
+/* .dmb: int32 type=1, h, w, nb, then h*w*nb float32 (HPM.cpp:270-401). */
+int hpm_write_dmb(const char *path, const float *data, int h, int w, int nb);
+/* Reads header into *h,*w,*nb; when data is non-NULL also the payload
+ * (capacity cap floats). */
+int hpm_read_dmb(const char *path, float *data, size_t cap, int *h, int *w, int *nb);
+/* cams/%08d_cam.txt (ReadCamera, HPM.cpp:160-185).  width/height are left 0. */
+int hpm_read_camera(const char *path, HpmCamera *cam);
+/* pair.txt (GenerateSampleList, main.cpp:4-33): returns the problem count
+ * into *n; ref_ids[n], src_counts[n], src_ids[n][HPM_MAX_IMAGES-1] filled when
+ * non-NULL (sources with score <= 0 are dropped). */
+int hpm_read_pair(const char *path, int *n, int *ref_ids, int *src_counts, int *src_ids, int cap);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* HPM_B200_H */

@@ -1,0 +1,109 @@
+/*
+ * CPU oracle for the HPM-MVS PatchMatch hot path.
+ *
+ * TEST INFRASTRUCTURE ONLY.  Only tests/, __graft_entry__.smoke() and the
+ * CPU-baseline leg of bench.py may load this library, and only as the checker.
+ * The product (hpm-mvs_b200/) never links or calls it.
+ *
+ * It restates, in plain C99 with FP32 arithmetic where the reference uses
+ * FP32, the algorithm of the reference's HPM-MVS/HPM.cu (kernels) and the
+ * host prior stages of HPM-MVS/HPM.cpp and main.cpp.  Every function cites
+ * the reference lines it follows.  Two documented deviations:
+ *   - Random numbers: the reference seeds curand XORWOW with clock64()
+ *     (HPM.cu:521), so its runs are not reproducible.  The oracle and the
+ *     CUDA product draw from the same counter-based Philox4x32-10 stream,
+ *     in the reference's draw order, so that a stochastic half-step can be
+ *     compared pixel by pixel.
+ *   - Texture fetches: tex2D with cudaFilterModeLinear is emulated in
+ *     software (bilinear weights quantised to 8 fractional bits, clamped
+ *     edge addressing).  The quantisation rule is pinned against the
+ *     hardware by tests/golden (fixtures produced by oracle/_ref, the
+ *     reference's own HPM.cu compiled for sm_100a).
+ */
+#ifndef HPM_ORACLE_H
+#define HPM_ORACLE_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Same layout as the reference's Camera (HPM-MVS/main.h:44-52). */
+typedef struct {
+    float K[9];
+    float R[9];
+    float t[3];
+    int height;
+    int width;
+    float depth_min;
+    float depth_max;
+} OrCamera;
+
+typedef struct {
+    int geom_consistency; /* PatchMatchParams::geom_consistency */
+    int planar_prior;     /* PatchMatchParams::planar_prior */
+    float depth_min;      /* PatchMatchParams::depth_min (already x0.6) */
+    float depth_max;      /* PatchMatchParams::depth_max (already x1.2) */
+    uint64_t seed;        /* Philox key */
+    uint32_t salt;        /* per-pass stream id */
+    int half_steps;       /* propagation half-steps to run; the reference runs 6 */
+    int finalize;         /* run GetDepthandNormal + the two filters */
+} OrRunOpts;
+
+/* 0: bilinear weight = floor(frac * 256) / 256; 1: round-to-nearest. */
+void or_set_tex_rounding(int mode);
+int or_get_tex_rounding(void);
+
+float or_tex2d(const float *img, int w, int h, float u, float v);
+void or_homography(const OrCamera *ref, const OrCamera *src, const float *plane4, float *H9);
+
+int or_cost_vectors(int n_img, const float *const *imgs, const OrCamera *cams, const float *planes4, float *out);
+int or_initial_costs(int n_img, const float *const *imgs, const OrCamera *cams, const float *planes4,
+                     float *out_cost, uint32_t *out_views);
+int or_geom_costs(int n_img, const OrCamera *cams, const float *const *depths, const float *planes4, float *out);
+
+/* HPM::RunPatchMatch (HPM.cu:1906-1957).  planes_io/costs_io hold the
+ * hypothesis state carried between passes; views_out may be NULL. */
+int or_run_patchmatch(int n_img, const float *const *imgs, const OrCamera *cams, const OrRunOpts *opts,
+                      float *planes_io, float *costs_io, uint32_t *views_io, const float *prior_planes,
+                      const uint32_t *plane_masks, const float *const *depth_maps);
+
+int or_depth_normal_filter(const OrCamera *ref, float *planes_io, const float *costs);
+
+int or_jbu(const float *guide, int cols, int rows, const float *coarse_depth, const float *coarse_normal, int s_cols,
+           int s_rows, float *out_depth, float *out_normal);
+
+/* Raw Philox4x32-10 block: ctr4 is replaced by the output. */
+void or_philox4x32_10(uint32_t k0, uint32_t k1, uint32_t *ctr4);
+
+/* Philox4x32-10 uniform in (0,1] for draw `n` of (pixel, step, salt). */
+float or_philox_uniform(uint64_t seed, uint32_t pixel, uint32_t step, uint32_t salt, uint32_t n);
+
+/* ---- host prior stages (HPM.cpp / main.cpp) ---- */
+
+/* GetSupportPoints* (HPM.cpp:759-785, 1125-1179): xy pairs into out (capacity
+ * max_points); returns the count. */
+int or_support_points(const float *costs, int w, int h, int *out_xy, int max_points);
+
+/* GetPriorPlaneParams_factor (HPM.cpp:811-844). */
+void or_plane_from_triangle(const OrCamera *ref, const float *depth, int w, const int *tri6, float factor,
+                            float *out4);
+
+/* GetDepthFromPlaneParam_factor (HPM.cpp:846-849). */
+float or_depth_from_plane(const OrCamera *ref, const float *plane4, int x, int y, float factor);
+
+/* Triangle raster of main.cpp:96-116: writes idx+1 into mask for every kept
+ * triangle, later triangles overwriting earlier ones; returns the number of
+ * kept triangles and stores their vertex triples in kept6. */
+int or_raster_triangles(const int *tris6, int n_tris, int w, int h, float *mask, int *kept6);
+
+/* DepthsPredictSupplement (HPM.cpp:923-1097) with exact brute-force K=6
+ * nearest neighbours (the reference uses PCL KdTreeFLANN). */
+void or_knn_supplement(const OrCamera *ref, const int *pts_xy, int n_pts, const float *depth, int w, int h,
+                       float factor, float dmin, float dmax, float *plane_out4, float *mask);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

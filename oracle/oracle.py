@@ -1,0 +1,341 @@
+"""ctypes binding of the CPU oracle (liboracle.so) and of the reference shim
+(_ref/libhpm_ref.so, the reference's own HPM-MVS/HPM.cu compiled for sm_100a).
+
+TEST INFRASTRUCTURE ONLY: tests/, __graft_entry__.smoke() and bench.py's CPU
+baseline / reference arm use this module as the checker.  The product never
+imports it.
+
+Array conventions (match the reference's host buffers):
+  images        list of float32 [H, W] arrays (gray values, HPM.cpp:492-495)
+  cams          numpy structured array of CAMERA_DTYPE (HPM-MVS/main.h:44-52)
+  planes        float32 [H, W, 4] = (nx, ny, nz, w)
+  costs         float32 [H, W]
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_SO = os.path.join(HERE, "liboracle.so")
+REF_SO = os.path.join(HERE, "_ref", "libhpm_ref.so")
+
+CAMERA_DTYPE = np.dtype(
+    [("K", "<f4", 9), ("R", "<f4", 9), ("t", "<f4", 3), ("height", "<i4"), ("width", "<i4"),
+     ("depth_min", "<f4"), ("depth_max", "<f4")]
+)
+assert CAMERA_DTYPE.itemsize == 100
+
+
+class OrRunOpts(ctypes.Structure):
+    _fields_ = [("geom_consistency", ctypes.c_int), ("planar_prior", ctypes.c_int),
+                ("depth_min", ctypes.c_float), ("depth_max", ctypes.c_float),
+                ("seed", ctypes.c_uint64), ("salt", ctypes.c_uint32),
+                ("half_steps", ctypes.c_int), ("finalize", ctypes.c_int)]
+
+
+class RefRunOpts(ctypes.Structure):
+    _fields_ = [("geom_consistency", ctypes.c_int), ("planar_prior", ctypes.c_int),
+                ("multi_geometry", ctypes.c_int), ("depth_min", ctypes.c_float),
+                ("depth_max", ctypes.c_float), ("seed", ctypes.c_ulonglong)]
+
+
+def build_oracle() -> None:
+    subprocess.run(["make", "-s", "-C", HERE, "oracle"], check=True)
+
+
+_lib = None
+_ref = None
+
+
+def lib() -> ctypes.CDLL:
+    global _lib
+    if _lib is None:
+        if not os.path.exists(ORACLE_SO):
+            build_oracle()
+        _lib = ctypes.CDLL(ORACLE_SO)
+        _lib.or_tex2d.restype = ctypes.c_float
+        _lib.or_philox_uniform.restype = ctypes.c_float
+        _lib.or_philox_uniform.argtypes = [ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32,
+                                           ctypes.c_uint32]
+        _lib.or_depth_from_plane.restype = ctypes.c_float
+    return _lib
+
+
+def ref_available() -> bool:
+    return os.path.exists(REF_SO)
+
+
+def ref() -> ctypes.CDLL:
+    global _ref
+    if _ref is None:
+        _ref = ctypes.CDLL(REF_SO)
+    return _ref
+
+
+def _p(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+def _img_ptrs(images):
+    imgs = [np.ascontiguousarray(i, dtype=np.float32) for i in images]
+    arr = (ctypes.c_void_p * len(imgs))(*[i.ctypes.data for i in imgs])
+    return imgs, arr
+
+
+def _cams(cams):
+    c = np.ascontiguousarray(cams, dtype=CAMERA_DTYPE)
+    return c
+
+
+def set_tex_rounding(mode: int) -> None:
+    lib().or_set_tex_rounding(ctypes.c_int(mode))
+
+
+def tex2d(img: np.ndarray, u: float, v: float) -> float:
+    img = np.ascontiguousarray(img, dtype=np.float32)
+    h, w = img.shape
+    return lib().or_tex2d(_p(img), w, h, ctypes.c_float(u), ctypes.c_float(v))
+
+
+def homography(ref_cam, src_cam, plane) -> np.ndarray:
+    out = np.zeros(9, np.float32)
+    r = _cams(np.array([ref_cam], dtype=CAMERA_DTYPE))
+    s = _cams(np.array([src_cam], dtype=CAMERA_DTYPE))
+    pl = np.ascontiguousarray(plane, dtype=np.float32)
+    lib().or_homography(_p(r), _p(s), _p(pl), _p(out))
+    return out
+
+
+def cost_vectors(images, cams, planes) -> np.ndarray:
+    imgs, arr = _img_ptrs(images)
+    c = _cams(cams)
+    h, w = imgs[0].shape
+    planes = np.ascontiguousarray(planes, dtype=np.float32)
+    out = np.zeros((h, w, len(imgs) - 1), np.float32)
+    lib().or_cost_vectors(len(imgs), arr, _p(c), _p(planes), _p(out))
+    return out
+
+
+def initial_costs(images, cams, planes):
+    imgs, arr = _img_ptrs(images)
+    c = _cams(cams)
+    h, w = imgs[0].shape
+    planes = np.ascontiguousarray(planes, dtype=np.float32)
+    cost = np.zeros((h, w), np.float32)
+    views = np.zeros((h, w), np.uint32)
+    lib().or_initial_costs(len(imgs), arr, _p(c), _p(planes), _p(cost), _p(views))
+    return cost, views
+
+
+def geom_costs(cams, depth_maps, planes) -> np.ndarray:
+    dm, arr = _img_ptrs(depth_maps)
+    c = _cams(cams)
+    h, w = dm[0].shape
+    planes = np.ascontiguousarray(planes, dtype=np.float32)
+    out = np.zeros((h, w, len(dm) - 1), np.float32)
+    lib().or_geom_costs(len(dm), _p(c), arr, _p(planes), _p(out))
+    return out
+
+
+def run_patchmatch(images, cams, *, depth_min, depth_max, seed=0, salt=0, geom=False, prior=False,
+                   planes=None, costs=None, views=None, prior_planes=None, masks=None, depth_maps=None,
+                   half_steps=6, finalize=True):
+    """HPM::RunPatchMatch restated on the CPU; returns (planes, costs, views)."""
+    imgs, arr = _img_ptrs(images)
+    c = _cams(cams)
+    h, w = imgs[0].shape
+    planes = (np.zeros((h, w, 4), np.float32) if planes is None
+              else np.array(planes, dtype=np.float32, copy=True, order="C"))
+    costs = (np.zeros((h, w), np.float32) if costs is None
+             else np.array(costs, dtype=np.float32, copy=True, order="C"))
+    views = (np.zeros((h, w), np.uint32) if views is None
+             else np.array(views, dtype=np.uint32, copy=True, order="C"))
+    o = OrRunOpts(int(geom), int(prior), float(depth_min), float(depth_max), int(seed), int(salt),
+                  int(half_steps), int(finalize))
+    pp = None if prior_planes is None else np.ascontiguousarray(prior_planes, dtype=np.float32)
+    mk = None if masks is None else np.ascontiguousarray(masks, dtype=np.uint32)
+    dms, darr = (None, None) if depth_maps is None else _img_ptrs(depth_maps)
+    rc = lib().or_run_patchmatch(len(imgs), arr, _p(c), ctypes.byref(o), _p(planes), _p(costs), _p(views),
+                                 None if pp is None else _p(pp), None if mk is None else _p(mk), darr)
+    if rc != 0:
+        raise RuntimeError(f"or_run_patchmatch failed: {rc}")
+    return planes, costs, views
+
+
+def depth_normal_filter(ref_cam, planes, costs):
+    r = _cams(np.array([ref_cam], dtype=CAMERA_DTYPE))
+    planes = np.array(planes, dtype=np.float32, copy=True, order="C")
+    costs = np.ascontiguousarray(costs, dtype=np.float32)
+    lib().or_depth_normal_filter(_p(r), _p(planes), _p(costs))
+    return planes
+
+
+def jbu(guide, coarse_depth, coarse_normal):
+    guide = np.ascontiguousarray(guide, dtype=np.float32)
+    cd = np.ascontiguousarray(coarse_depth, dtype=np.float32)
+    cn = np.ascontiguousarray(coarse_normal, dtype=np.float32)
+    rows, cols = guide.shape
+    s_rows, s_cols = cd.shape
+    od = np.zeros((rows, cols), np.float32)
+    on = np.zeros((rows, cols, 3), np.float32)
+    rc = lib().or_jbu(_p(guide), cols, rows, _p(cd), _p(cn), s_cols, s_rows, _p(od), _p(on))
+    if rc == 1:
+        return None, None
+    return od, on
+
+
+def philox_uniform(seed, pixel, step, salt, n) -> float:
+    return lib().or_philox_uniform(seed, pixel, step, salt, n)
+
+
+def support_points(costs) -> np.ndarray:
+    costs = np.ascontiguousarray(costs, dtype=np.float32)
+    h, w = costs.shape
+    cap = ((w + 4) // 5) * ((h + 4) // 5)
+    out = np.zeros((cap, 2), np.int32)
+    n = lib().or_support_points(_p(costs), w, h, _p(out), cap)
+    return out[:n].copy()
+
+
+def plane_from_triangle(ref_cam, depth, tri, factor) -> np.ndarray:
+    r = _cams(np.array([ref_cam], dtype=CAMERA_DTYPE))
+    depth = np.ascontiguousarray(depth, dtype=np.float32)
+    t = np.ascontiguousarray(tri, dtype=np.int32).reshape(6)
+    out = np.zeros(4, np.float32)
+    lib().or_plane_from_triangle(_p(r), _p(depth), depth.shape[1], _p(t), ctypes.c_float(factor), _p(out))
+    return out
+
+
+def depth_from_plane(ref_cam, plane, x, y, factor) -> float:
+    r = _cams(np.array([ref_cam], dtype=CAMERA_DTYPE))
+    p = np.ascontiguousarray(plane, dtype=np.float32)
+    return lib().or_depth_from_plane(_p(r), _p(p), int(x), int(y), ctypes.c_float(factor))
+
+
+def raster_triangles(tris, w, h, mask=None):
+    t = np.ascontiguousarray(tris, dtype=np.int32).reshape(-1, 6)
+    mask = np.zeros((h, w), np.float32) if mask is None else np.array(mask, np.float32, copy=True, order="C")
+    kept = np.zeros_like(t)
+    n = lib().or_raster_triangles(_p(t), len(t), w, h, _p(mask), _p(kept))
+    return mask, kept[:n].copy()
+
+
+def knn_supplement(ref_cam, pts, depth, factor, dmin, dmax, mask):
+    r = _cams(np.array([ref_cam], dtype=CAMERA_DTYPE))
+    pts = np.ascontiguousarray(pts, dtype=np.int32).reshape(-1, 2)
+    depth = np.ascontiguousarray(depth, dtype=np.float32)
+    h, w = depth.shape
+    mask = np.array(mask, np.float32, copy=True, order="C")
+    planes = np.zeros((h, w, 4), np.float32)
+    lib().or_knn_supplement(_p(r), _p(pts), len(pts), _p(depth), w, h, ctypes.c_float(factor),
+                            ctypes.c_float(dmin), ctypes.c_float(dmax), _p(planes), _p(mask))
+    return planes, mask
+
+
+# ---------------------------------------------------------------- reference shim
+
+def ref_cost_vectors(images, cams, planes) -> np.ndarray:
+    imgs, arr = _img_ptrs(images)
+    c = _cams(cams)
+    h, w = imgs[0].shape
+    planes = np.ascontiguousarray(planes, dtype=np.float32)
+    out = np.zeros((h, w, len(imgs) - 1), np.float32)
+    rc = ref().hpm_ref_cost_vectors(len(imgs), arr, _p(c), _p(planes), _p(out))
+    if rc != 0:
+        raise RuntimeError(f"hpm_ref_cost_vectors: cuda error {rc}")
+    return out
+
+
+def ref_initial_costs(images, cams, planes):
+    imgs, arr = _img_ptrs(images)
+    c = _cams(cams)
+    h, w = imgs[0].shape
+    planes = np.ascontiguousarray(planes, dtype=np.float32)
+    cost = np.zeros((h, w), np.float32)
+    views = np.zeros((h, w), np.uint32)
+    rc = ref().hpm_ref_initial_costs(len(imgs), arr, _p(c), _p(planes), _p(cost), _p(views))
+    if rc != 0:
+        raise RuntimeError(f"hpm_ref_initial_costs: cuda error {rc}")
+    return cost, views
+
+
+def ref_geom_costs(cams, depth_maps, planes) -> np.ndarray:
+    dm, arr = _img_ptrs(depth_maps)
+    c = _cams(cams)
+    h, w = dm[0].shape
+    planes = np.ascontiguousarray(planes, dtype=np.float32)
+    out = np.zeros((h, w, len(dm) - 1), np.float32)
+    rc = ref().hpm_ref_geom_costs(len(dm), _p(c), arr, _p(planes), _p(out))
+    if rc != 0:
+        raise RuntimeError(f"hpm_ref_geom_costs: cuda error {rc}")
+    return out
+
+
+def ref_homography(ref_cam, src_cam, planes) -> np.ndarray:
+    r = _cams(np.array([ref_cam], dtype=CAMERA_DTYPE))
+    s = _cams(np.array([src_cam], dtype=CAMERA_DTYPE))
+    planes = np.ascontiguousarray(planes, dtype=np.float32).reshape(-1, 4)
+    out = np.zeros((len(planes), 9), np.float32)
+    rc = ref().hpm_ref_homography(_p(r), _p(s), _p(planes), len(planes), _p(out))
+    if rc != 0:
+        raise RuntimeError(f"hpm_ref_homography: cuda error {rc}")
+    return out
+
+
+def ref_tex_fetch(img, coords) -> np.ndarray:
+    img = np.ascontiguousarray(img, dtype=np.float32)
+    coords = np.ascontiguousarray(coords, dtype=np.float32).reshape(-1, 2)
+    out = np.zeros(len(coords), np.float32)
+    h, w = img.shape
+    rc = ref().hpm_ref_tex_fetch(_p(img), w, h, _p(coords), len(coords), _p(out))
+    if rc != 0:
+        raise RuntimeError(f"hpm_ref_tex_fetch: cuda error {rc}")
+    return out
+
+
+def ref_depth_normal_filter(ref_cam, planes, costs):
+    r = _cams(np.array([ref_cam], dtype=CAMERA_DTYPE))
+    planes = np.array(planes, dtype=np.float32, copy=True, order="C")
+    costs = np.ascontiguousarray(costs, dtype=np.float32)
+    rc = ref().hpm_ref_depth_normal_filter(_p(r), _p(planes), _p(costs))
+    if rc != 0:
+        raise RuntimeError(f"hpm_ref_depth_normal_filter: cuda error {rc}")
+    return planes
+
+
+def ref_jbu(guide, coarse_depth, coarse_normal):
+    guide = np.ascontiguousarray(guide, dtype=np.float32)
+    cd = np.ascontiguousarray(coarse_depth, dtype=np.float32)
+    cn = np.ascontiguousarray(coarse_normal, dtype=np.float32)
+    rows, cols = guide.shape
+    s_rows, s_cols = cd.shape
+    od = np.zeros((rows, cols), np.float32)
+    on = np.zeros((rows, cols, 3), np.float32)
+    rc = ref().hpm_ref_jbu(_p(guide), cols, rows, _p(cd), _p(cn), s_cols, s_rows, _p(od), _p(on))
+    if rc != 0:
+        raise RuntimeError(f"hpm_ref_jbu: cuda error {rc}")
+    return od, on
+
+
+def ref_run_patchmatch(images, cams, *, depth_min, depth_max, seed=0, geom=False, prior=False, multi_geometry=False,
+                       planes=None, costs=None, prior_planes=None, masks=None, depth_maps=None):
+    imgs, arr = _img_ptrs(images)
+    c = _cams(cams)
+    h, w = imgs[0].shape
+    planes = (np.zeros((h, w, 4), np.float32) if planes is None
+              else np.array(planes, dtype=np.float32, copy=True, order="C"))
+    costs = (np.zeros((h, w), np.float32) if costs is None
+             else np.array(costs, dtype=np.float32, copy=True, order="C"))
+    o = RefRunOpts(int(geom), int(prior), int(multi_geometry), float(depth_min), float(depth_max), int(seed))
+    pp = None if prior_planes is None else np.ascontiguousarray(prior_planes, dtype=np.float32)
+    mk = None if masks is None else np.ascontiguousarray(masks, dtype=np.uint32)
+    dms, darr = (None, None) if depth_maps is None else _img_ptrs(depth_maps)
+    rc = ref().hpm_ref_run_patchmatch(len(imgs), arr, _p(c), ctypes.byref(o), _p(planes), _p(costs),
+                                      None if pp is None else _p(pp), None if mk is None else _p(mk), darr)
+    if rc != 0:
+        raise RuntimeError(f"hpm_ref_run_patchmatch: cuda error {rc}")
+    return planes, costs

@@ -1,0 +1,162 @@
+"""Generate the golden fixtures of tests/golden/ from the reference's own code.
+
+Runs the reference's HPM-MVS/HPM.cu, compiled unchanged for sm_100a into
+oracle/_ref/libhpm_ref.so (recipe: oracle/Makefile), on a B200 and stores its
+outputs for small seeded inputs:
+
+  tex_probe.npz   tex2D<float> of the reference's texture set-up at chosen
+                  coordinates (bilinear weight quantisation, edge addressing)
+  ncc.npz         ComputeMultiViewCostVector / ComputeMultiViewInitialCost-
+                  andSelectedViews / ComputeHomography for fixed planes
+  geom.npz        ComputeGeomConsistencyCost for fixed planes and depth maps
+  jbu.npz         JBU_cu at x2 and x4
+  filter.npz      GetDepthandNormal + Black/RedPixelFilter
+  pm.npz          whole RunPatchMatch passes (plain; geometric) for the
+                  statistical comparison (the reference's RNG is curand
+                  XORWOW, so only statistics are comparable)
+
+Usage (on a GPU machine, from the repository root):
+    python tests/golden/make_golden.py [--out tests/golden]
+"""
+from __future__ import annotations
+
+import argparse
+import os
+import sys
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+sys.path[:0] = [os.path.join(ROOT, "hpm-mvs_b200"), os.path.join(ROOT, "oracle")]
+
+import oracle as orc  # noqa: E402
+import synthetic as syn  # noqa: E402
+
+W, H, NV = 96, 72, 5
+
+
+def small_scene(seed=0):
+    return syn.make_scene(seed, W, H, NV, n_planes=6, low_texture=0.25)
+
+
+def test_planes(sc, ref, rng):
+    gt = syn.gt_planes_ref_frame(sc, ref)
+    pert = gt.copy()
+    pert[..., 3] *= rng.uniform(0.97, 1.03, pert.shape[:2]).astype(np.float32)
+    # random planes facing the camera at random depths
+    n = rng.normal(size=gt.shape[:2] + (3,)).astype(np.float32)
+    n /= np.linalg.norm(n, axis=-1, keepdims=True)
+    n[..., 2] = -np.abs(n[..., 2]) - 0.2
+    n /= np.linalg.norm(n, axis=-1, keepdims=True)
+    cam = sc.cams[ref]
+    K = cam["K"].reshape(3, 3)
+    ys, xs = np.mgrid[0:H, 0:W].astype(np.float32)
+    d = rng.uniform(1.5, 9.0, gt.shape[:2]).astype(np.float32)
+    X = np.stack([d * (xs - K[0, 2]) / K[0, 0], d * (ys - K[1, 2]) / K[1, 1], d], -1)
+    rnd = np.concatenate([n, -(n * X).sum(-1, keepdims=True)], -1).astype(np.float32)
+    return np.stack([gt, pert, rnd])
+
+
+def tex_probe():
+    # texture A: value 256*x (y-independent); texture B: value 256*y
+    w, h = 6, 5
+    ta = np.tile(256.0 * np.arange(w, dtype=np.float32), (h, 1))
+    tb = np.tile(256.0 * np.arange(h, dtype=np.float32)[:, None], (1, w))
+    k = np.arange(4097, dtype=np.float32)
+    fine = np.stack([2.5 + k / 4096.0, np.full_like(k, 2.5)], -1)            # fractions along x
+    fine_y = np.stack([np.full_like(k, 2.5), 2.5 + k / 4096.0], -1)          # fractions along y
+    edge = np.arange(-4.0, w + 4.0, 0.125, dtype=np.float32)
+    edges = np.stack([edge, np.full_like(edge, 2.5)], -1)
+    edge_y = np.arange(-4.0, h + 4.0, 0.125, dtype=np.float32)
+    edges_y = np.stack([np.full_like(edge_y, 2.5), edge_y], -1)
+    big = np.array([[1e6, 2.5], [-1e6, 2.5], [2.5, 1e6], [2.5, -1e6], [3.0e9, 2.5]], np.float32)
+    rng = np.random.default_rng(7)
+    rnd = np.stack([rng.uniform(-1, w + 1, 2000), rng.uniform(-1, h + 1, 2000)], -1).astype(np.float32)
+    tr = rng.uniform(0, 255, (h, w)).astype(np.float32).round()
+    out = dict(ta=ta, tb=tb, tr=tr, fine=fine, fine_y=fine_y, edges=edges, edges_y=edges_y, big=big, rnd=rnd)
+    out["a_fine"] = orc.ref_tex_fetch(ta, fine)
+    out["b_fine_y"] = orc.ref_tex_fetch(tb, fine_y)
+    out["a_edges"] = orc.ref_tex_fetch(ta, edges)
+    out["b_edges_y"] = orc.ref_tex_fetch(tb, edges_y)
+    out["a_big"] = orc.ref_tex_fetch(ta, big)
+    out["b_big"] = orc.ref_tex_fetch(tb, big)
+    out["r_rnd"] = orc.ref_tex_fetch(tr, rnd)
+    # single-texel textures: the fetch returns that texel's effective weight
+    g = (np.arange(64, dtype=np.float32) - 32.0) / 32.0
+    gx, gy = np.meshgrid(g, g)
+    dgrid = np.stack([3.5 + gx.ravel(), 2.5 + gy.ravel()], -1).astype(np.float32)
+    out["dgrid"] = dgrid
+    for val in (1.0, 255.0, 0.7):
+        d = np.zeros((h, w), np.float32)
+        d[2, 3] = val
+        out[f"delta_{val}"] = orc.ref_tex_fetch(d, dgrid)
+    # random texture at coordinates on the exact 1/256 grid of both axes
+    A, B = np.meshgrid(np.arange(0, 256, 4, dtype=np.float32), np.arange(0, 256, 4, dtype=np.float32))
+    grid256 = np.stack([2.5 + A.ravel() / 256.0, 1.5 + B.ravel() / 256.0], -1).astype(np.float32)
+    out["grid256"] = grid256
+    out["r_grid256"] = orc.ref_tex_fetch(tr, grid256)
+    return out
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--out", default=os.path.join(ROOT, "tests", "golden"))
+    args = ap.parse_args()
+    os.makedirs(args.out, exist_ok=True)
+    if not orc.ref_available():
+        raise SystemExit("oracle/_ref/libhpm_ref.so is missing: build it with `make -C oracle ref`")
+    rng = np.random.default_rng(1234)
+
+    np.savez_compressed(os.path.join(args.out, "tex_probe.npz"), **tex_probe())
+
+    sc = small_scene(0)
+    ref = 2
+    imgs, cams = syn.view_set(sc, ref)
+    planes = test_planes(sc, ref, rng)
+    cv = np.stack([orc.ref_cost_vectors(imgs, cams, p) for p in planes])
+    ic = [orc.ref_initial_costs(imgs, cams, p) for p in planes]
+    homs = np.stack([orc.ref_homography(cams[0], cams[v], planes[2][::7, ::7].reshape(-1, 4)) for v in range(1, NV)])
+    np.savez_compressed(os.path.join(args.out, "ncc.npz"), images=np.stack([i.astype(np.uint8) for i in imgs]),
+                        cams=cams, planes=planes, cost_vectors=cv, init_cost=np.stack([c for c, _ in ic]),
+                        init_views=np.stack([v for _, v in ic]), hom_planes=planes[2][::7, ::7].reshape(-1, 4),
+                        homographies=homs)
+
+    depths = [sc.gt_depth[i] for i in [ref] + list(sc.pairs[ref][1])]
+    depths = [np.where(rng.random(d.shape) < 0.05, 0.0, d).astype(np.float32) for d in depths]
+    gc = np.stack([orc.ref_geom_costs(cams, depths, p) for p in planes])
+    np.savez_compressed(os.path.join(args.out, "geom.npz"), cams=cams, depths=np.stack(depths), planes=planes,
+                        geom_costs=gc)
+
+    guide = imgs[0]
+    jb = {}
+    for s in (2, 4):
+        cd = sc.gt_depth[ref][::s, ::s].copy()
+        cd[rng.random(cd.shape) < 0.1] = 0.0
+        cn = sc.gt_normal[ref][::s, ::s].copy()
+        od, on = orc.ref_jbu(guide, cd, cn)
+        jb[f"coarse_depth_{s}"] = cd
+        jb[f"coarse_normal_{s}"] = cn
+        jb[f"out_depth_{s}"] = od
+        jb[f"out_normal_{s}"] = on
+    np.savez_compressed(os.path.join(args.out, "jbu.npz"), guide=guide, **jb)
+
+    costs = rng.uniform(0, 1, (H, W)).astype(np.float32)
+    costs[rng.random((H, W)) < 0.1] = 0.0
+    filt = orc.ref_depth_normal_filter(cams[0], planes[1], costs)
+    np.savez_compressed(os.path.join(args.out, "filter.npz"), cams=cams, planes=planes[1], costs=costs,
+                        out=filt)
+
+    dmin, dmax = sc.depth_min * 0.6, sc.depth_max * 1.2
+    runs = {}
+    for seed in (1, 2):
+        pl, co = orc.ref_run_patchmatch(imgs, cams, depth_min=dmin, depth_max=dmax, seed=seed)
+        runs[f"plain_planes_{seed}"] = pl
+        runs[f"plain_costs_{seed}"] = co
+    np.savez_compressed(os.path.join(args.out, "pm.npz"), images=np.stack([i.astype(np.uint8) for i in imgs]),
+                        cams=cams, gt_depth=sc.gt_depth[ref], gt_normal=sc.gt_normal[ref], depth_min=dmin,
+                        depth_max=dmax, **runs)
+    print("golden fixtures written to", args.out)
+
+
+if __name__ == "__main__":
+    main()
