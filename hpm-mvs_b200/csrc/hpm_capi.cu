@@ -59,6 +59,15 @@ struct hpm_ctx {
 
     void *d_scratch = nullptr;
     size_t scratch_cap = 0;
+
+    float *d_cache = nullptr; /* cost vector of each pixel's current hypothesis, [S][H*W] */
+    size_t cache_cap = 0;
+    float *d_cand = nullptr; /* half-step hand-off: cost matrix rows [kCandRows*S][H*W] */
+    size_t cand_cap = 0;
+    int *d_pos = nullptr; /* chosen NESP sites [8][H*W] */
+    size_t pos_cap = 0;
+    uint32_t *d_flags = nullptr; /* valid-direction bits [H*W] */
+    size_t flags_cap = 0;
 };
 
 namespace {
@@ -165,6 +174,10 @@ PMArgs make_args(hpm_ctx *c)
     a.prior_planes = c->d_prior;
     a.masks = c->d_masks;
     a.counters = c->counting ? c->d_counters : nullptr;
+    a.cost_cache = c->d_cache;
+    a.cand_costs = c->d_cand;
+    a.cand_pos = c->d_pos;
+    a.cand_flags = c->d_flags;
     return a;
 }
 
@@ -244,6 +257,10 @@ int hpm_destroy(hpm_ctx *c)
     cudaFree(c->d_masks);
     cudaFree(c->d_counters);
     cudaFree(c->d_scratch);
+    cudaFree(c->d_cache);
+    cudaFree(c->d_cand);
+    cudaFree(c->d_pos);
+    cudaFree(c->d_flags);
     for (auto &p : c->prof_events) {
         cudaEventDestroy(p.second.first);
         cudaEventDestroy(p.second.second);
@@ -305,6 +322,10 @@ int hpm_set_views(hpm_ctx *c, const float *const *images, const HpmCamera *cams,
         CK(cudaMalloc(&c->d_masks, sizeof(uint32_t) * n), "state alloc");
         c->px_cap = n;
     }
+    CK(ensure((void **)&c->d_cache, &c->cache_cap, sizeof(float) * n * (num_images - 1)), "cache alloc");
+    CK(ensure((void **)&c->d_cand, &c->cand_cap, sizeof(float) * n * (num_images - 1) * kCandRows), "cand alloc");
+    CK(ensure((void **)&c->d_pos, &c->pos_cap, sizeof(int) * n * 8), "cand alloc");
+    CK(ensure((void **)&c->d_flags, &c->flags_cap, sizeof(uint32_t) * n), "cand alloc");
     CK(cudaMemsetAsync(c->d_planes, 0, sizeof(float4) * n, c->stream), "state clear");
     CK(cudaMemsetAsync(c->d_costs, 0, sizeof(float) * n, c->stream), "state clear");
     CK(cudaMemsetAsync(c->d_views, 0, sizeof(uint32_t) * n, c->stream), "state clear");

@@ -17,6 +17,7 @@ namespace hpm {
 constexpr int kMaxViews = HPM_MAX_IMAGES; /* reference + 32 sources */
 constexpr int kMaxSrc = kMaxViews - 1;
 constexpr int kTaps = 36; /* 6 x 6 taps of the 11x11 window, stride 2 */
+constexpr int kCandRows = 10; /* 8 NESP directions + 2 refinement scratch rows */
 
 /* Per-view data of one problem, passed to kernels by value. */
 struct ViewDev {
@@ -54,6 +55,13 @@ struct PMArgs {
     const float4 *prior_planes;
     const uint32_t *masks;
     float *cost_cache; /* [S][H][W] cost vector of the current hypothesis, or nullptr */
+    /* hand-off between the two kernels of a half-step (L2-resident):
+     * cand_costs [kCandRows*S][H*W] cost matrix rows (8 NESP directions and
+     * two refinement scratch rows), cand_pos [8][H*W] chosen sites,
+     * cand_flags [H*W] bit k = direction k valid */
+    float *cand_costs;
+    int *cand_pos;
+    uint32_t *cand_flags;
     unsigned long long *counters; /* [2]: cost vectors, geom terms, or nullptr */
 };
 

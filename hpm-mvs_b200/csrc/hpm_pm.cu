@@ -41,6 +41,15 @@ constexpr double kPiD = 3.14159265358979323846; /* M_PI, HPM-MVS/main.h:41 */
 constexpr int kBlockX = 32;
 constexpr int kBlockY = 2;
 constexpr int kBlock = kBlockX * kBlockY;
+#ifndef HPM_CV_INLINE
+#define HPM_CV_INLINE __noinline__
+#endif
+#ifndef HPM_P1_MIN_BLOCKS
+#define HPM_P1_MIN_BLOCKS 10
+#endif
+#ifndef HPM_P2_MIN_BLOCKS
+#define HPM_P2_MIN_BLOCKS 10
+#endif
 
 /* ------------------------------------------------------------------ */
 /* Philox4x32-10 (Salmon et al., SC'11), counter = (pixel, step, n/4, salt) */
@@ -261,9 +270,9 @@ struct RefStats {
 };
 
 /* The reference-side half of ComputeBilateralNCC (HPM.cu:318-386) for pixel
- * (px, py): per-tap weight and weight*ref into shared memory, sums in the
- * reference's row-then-total order. */
-__device__ RefStats ref_window(const PMArgs &a, int px, int py, float *sW, float *sWR, int tid)
+ * (px, py): per-tap (weight, weight*ref) into shared memory as one float2,
+ * sums in the reference's row-then-total order.  sWW is [tap][kBlock]. */
+__device__ RefStats ref_window(const PMArgs &a, int px, int py, float2 *sWW, int tid)
 {
     const ViewDev &rv = a.view[0];
     const float center = texel(rv.img, rv.w, rv.h, px, py);
@@ -278,8 +287,7 @@ __device__ RefStats ref_window(const PMArgs &a, int px, int py, float *sW, float
             const float color_dist = fabsf(rp - center);
             const float wgt = expf(-spatial_dist / (2.0f * a.sigma_spatial * a.sigma_spatial) -
                                    color_dist / (2.0f * a.sigma_color * a.sigma_color));
-            sW[t * kBlock + tid] = wgt;
-            sWR[t * kBlock + tid] = wgt * rp;
+            sWW[t * kBlock + tid] = make_float2(wgt, wgt * rp);
             r_ref += wgt * rp;
             r_rr += wgt * rp * rp;
             r_w += wgt;
@@ -297,8 +305,8 @@ __device__ RefStats ref_window(const PMArgs &a, int px, int py, float *sW, float
 }
 
 /* The source-side half of ComputeBilateralNCC (HPM.cu:325-397). */
-__device__ float ncc(const PMArgs &a, int v, int px, int py, float4 h, const float *sW, const float *sWR, int tid,
-                     const RefStats &rs)
+__device__ __forceinline__ float ncc(const PMArgs &a, int v, int px, int py, float4 h, const float2 *sWW, int tid,
+                                     const RefStats &rs)
 {
     const HpmCamera &sc = a.cam[v];
     float H[9];
@@ -317,11 +325,10 @@ __device__ float ncc(const PMArgs &a, int v, int px, int py, float4 h, const flo
         for (int j = -5; j < 6; j += 2, ++t) {
             const float2 q = warp(H, fpx + (float)i, fpy + (float)j);
             const float sp = tex2D<float>(tex, q.x + 0.5f, q.y + 0.5f);
-            const float wgt = sW[t * kBlock + tid];
-            const float wr = sWR[t * kBlock + tid];
-            r_src += wgt * sp;
-            r_ss += wgt * sp * sp;
-            r_rs += wr * sp;
+            const float2 ww = sWW[t * kBlock + tid];
+            r_src += ww.x * sp;
+            r_ss += ww.x * sp * sp;
+            r_rs += ww.y * sp;
         }
         sum_src += r_src;
         sum_src_src += r_ss;
@@ -337,12 +344,12 @@ __device__ float ncc(const PMArgs &a, int v, int px, int py, float4 h, const flo
     return fmaxf(0.0f, fminf(2.0f, 1.0f - covar / vv));
 }
 
-/* ComputeMultiViewCostVector (HPM.cu:438-443) into a strided slot array. */
-__device__ __forceinline__ void cost_vector(const PMArgs &a, int px, int py, float4 h, const float *sW,
-                                            const float *sWR, int tid, const RefStats &rs, float *out,
-                                            int stride)
+/* ComputeMultiViewCostVector (HPM.cu:438-443) into out[v * stride].  Kept
+ * out of line so that the 36-tap loop exists once in the binary. */
+__device__ HPM_CV_INLINE void cost_vector(const PMArgs &a, int px, int py, float4 h, const float2 *sWW, int tid,
+                                         RefStats rs, float *out, int stride)
 {
-    for (int v = 1; v < a.n; ++v) out[(v - 1) * stride] = ncc(a, v, px, py, h, sW, sWR, tid, rs);
+    for (int v = 1; v < a.n; ++v) out[(v - 1) * stride] = ncc(a, v, px, py, h, sWW, tid, rs);
     if (a.counters) atomicAdd(&a.counters[0], 1ull);
 }
 
@@ -356,30 +363,27 @@ __device__ __forceinline__ void sort_small(float *d, int n) /* HPM.cu:3-12 */
     }
 }
 
-/* ComputeMultiViewInitialCostandSelectedViews (HPM.cu:399-436) */
-__device__ float initial_cost(const PMArgs &a, int px, int py, float4 h, const float *sW, const float *sWR,
-                              int tid, const RefStats &rs, uint32_t *views)
+/* ComputeMultiViewInitialCostandSelectedViews (HPM.cu:399-436) from a cost
+ * vector cv[v * stride]. */
+__device__ float initial_cost_from(const PMArgs &a, const float *cv, int stride, uint32_t *views)
 {
-    float cv[kMaxSrc], cp[kMaxSrc];
+    float srt[kMaxSrc];
     const int S = a.n - 1;
     int valid = 0;
-    for (int v = 1; v < a.n; ++v) {
-        const float c = ncc(a, v, px, py, h, sW, sWR, tid, rs);
-        cv[v - 1] = c;
-        cp[v - 1] = c;
-        if (c < 2.0f) valid++;
+    for (int v = 0; v < S; ++v) {
+        srt[v] = cv[v * stride];
+        if (srt[v] < 2.0f) valid++;
     }
-    if (a.counters) atomicAdd(&a.counters[0], 1ull);
-    sort_small(cv, S);
+    sort_small(srt, S);
     uint32_t sel = 0;
     const int top_k = min(valid, a.top_k);
     float result = 2.0f;
     if (top_k > 0) {
         float cost = 0.0f;
-        for (int i = 0; i < top_k; ++i) cost += cv[i];
-        const float thr = cv[top_k - 1];
+        for (int i = 0; i < top_k; ++i) cost += srt[i];
+        const float thr = srt[top_k - 1];
         for (int i = 0; i < S; ++i)
-            if (cp[i] <= thr) sel |= 1u << i;
+            if (cv[i * stride] <= thr) sel |= 1u << i;
         result = cost / top_k;
     }
     *views = sel;
@@ -413,7 +417,7 @@ __device__ __forceinline__ void project(const float *P, const HpmCamera &c, floa
 }
 
 /* ComputeGeomConsistencyCost (HPM.cu:483-508) */
-__device__ float geom_cost(const PMArgs &a, int v, float4 h, int px, int py)
+__device__ __noinline__ float geom_cost(const PMArgs &a, int v, float4 h, int px, int py)
 {
     const HpmCamera &rc = a.cam[0], &sc = a.cam[v];
     const float depth = depth_from_plane(rc, h, px, py);
@@ -436,7 +440,7 @@ __device__ float geom_cost(const PMArgs &a, int v, float4 h, int px, int py)
 /* ------------------------------------------------------------------ */
 
 /* R_relative and t_relative of HPM.cu:229-255, with the same expressions. */
-__global__ void k_pair_geom(PMArgs a, PairGeom *out)
+__global__ void k_pair_geom(const __grid_constant__ PMArgs a, PairGeom *out)
 {
     const int v = threadIdx.x;
     if (v < 1 || v >= a.n) return;
@@ -464,18 +468,28 @@ __global__ void k_pair_geom(PMArgs a, PairGeom *out)
     out[v] = g;
 }
 
-/* RandomInitialization, HPM.cu:510-558.  One thread per pixel. */
-__global__ void __launch_bounds__(kBlock) k_init(PMArgs a)
+/* Cost-vector cache: for every pixel the cost vector of its current
+ * hypothesis, [view][pixel].  Written by the initialisation and by every
+ * update, read instead of re-scoring the current hypothesis
+ * (HPM.cu:1637-1638): NCC is a pure function of (pixel, plane, view), so the
+ * cached values are the ones the re-score would produce. */
+__device__ __forceinline__ float *cache_at(const PMArgs &a, int v, int center)
 {
-    __shared__ float sW[kTaps * kBlock];
-    __shared__ float sWR[kTaps * kBlock];
+    return a.cost_cache + (size_t)v * a.W * a.H + center;
+}
+
+/* RandomInitialization, HPM.cu:510-558.  One thread per pixel. */
+__global__ void __launch_bounds__(kBlock) k_init(const __grid_constant__ PMArgs a)
+{
+    __shared__ float2 sWW[kTaps * kBlock];
+    __shared__ float sCV[kMaxSrc * kBlock];
     const int tid = threadIdx.y * kBlockX + threadIdx.x;
     const int px = blockIdx.x * kBlockX + threadIdx.x;
     const int py = blockIdx.y * kBlockY + threadIdx.y;
     if (px >= a.W || py >= a.H) return;
     const int center = py * a.W + px;
     const HpmCamera &cam = a.cam[0];
-    const RefStats rs = ref_window(a, px, py, sW, sWR, tid);
+    const RefStats rs = ref_window(a, px, py, sWW, tid);
     Rng rng;
     rng.init(a.seed_lo, a.seed_hi, (uint32_t)center, 0u, a.salt);
     float4 h;
@@ -503,11 +517,15 @@ __global__ void __launch_bounds__(kBlock) k_init(PMArgs a)
         h = random_normal(cam, px, py, rng, depth);
         h.w = distance_to_origin(cam, px, py, depth, h);
     }
+    float *cv = sCV + tid;
+    cost_vector(a, px, py, h, sWW, tid, rs, cv, kBlock);
     uint32_t sel;
-    const float c = initial_cost(a, px, py, h, sW, sWR, tid, rs, &sel);
+    const float c = initial_cost_from(a, cv, kBlock, &sel);
     a.planes[center] = h;
     a.costs[center] = c;
     a.views[center] = sel;
+    if (a.cost_cache)
+        for (int v = 0; v < a.n - 1; ++v) *cache_at(a, v, center) = cv[v * kBlock];
 }
 
 /* Validity of the first site of direction k at extension round r (HPM.cu:1252-1445 and the
@@ -599,32 +617,46 @@ __device__ __forceinline__ float restricted_prior(float depth_diff, float angle_
     return gamma + expf(-depth_diff * depth_diff / two_dss) * expf(-angle_diff * angle_diff / two_ass);
 }
 
-/* One pixel of CheckerboardPropagation (HPM.cu:1222-1725) followed by
- * PlaneHypothesisRefinement (HPM.cu:1143-1220). */
-__global__ void __launch_bounds__(kBlock) k_propagate(PMArgs a, int iter, int color)
+__device__ __forceinline__ bool same_plane(float4 p, float4 q)
 {
-    extern __shared__ float smem[];
-    float *sW = smem;
-    float *sWR = sW + kTaps * kBlock;
-    float *sCA = sWR + kTaps * kBlock; /* [8*S][kBlock] */
+    return __float_as_uint(p.x) == __float_as_uint(q.x) && __float_as_uint(p.y) == __float_as_uint(q.y) &&
+           __float_as_uint(p.z) == __float_as_uint(q.z) && __float_as_uint(p.w) == __float_as_uint(q.w);
+}
+
+/* One red/black half-step runs as two kernels that hand the per-pixel cost
+ * matrix over through L2 instead of holding it in shared memory for the
+ * whole pixel update (8 x S floats per pixel is what limits occupancy):
+ *
+ *   k_prop_dirs    NESP site choice, direction cost vectors, extension
+ *                  (HPM.cu:1222-1543)
+ *   k_prop_refine  joint view selection, candidate choice and
+ *                  PlaneHypothesisRefinement (HPM.cu:1548-1725, 1143-1220)
+ *
+ * The other colour is read-only during both kernels, so splitting the pixel
+ * update changes nothing in what is computed. */
+
+#define CAG(k, v) a.cand_costs[(size_t)((k) * S + (v)) * npx + center]
+
+__global__ void __launch_bounds__(kBlock, HPM_P1_MIN_BLOCKS) k_prop_dirs(const __grid_constant__ PMArgs a, int iter,
+                                                                          int color)
+{
+    __shared__ float2 sWW[kTaps * kBlock];
     const int tid = threadIdx.y * kBlockX + threadIdx.x;
     const int py = blockIdx.y * kBlockY + threadIdx.y;
     const int px = blockIdx.x * (2 * kBlockX) + 2 * threadIdx.x + ((py + color) & 1);
     if (px >= a.W || py >= a.rows_cov) return;
     const int W = a.W, H = a.H, S = a.n - 1;
+    const size_t npx = (size_t)W * H;
     const int center = py * W + px;
-    const HpmCamera &cam = a.cam[0];
-    const RefStats rs = ref_window(a, px, py, sW, sWR, tid);
-    Rng rng;
-    rng.init(a.seed_lo, a.seed_hi, (uint32_t)center, (uint32_t)(1 + iter), a.salt);
-#define CA(k, v) sCA[((k) * S + (v)) * kBlock + tid]
+    const RefStats rs = ref_window(a, px, py, sWW, tid);
+    const float4 cur = a.planes[center];
 
     for (int k = 0; k < 8; ++k)
-        for (int v = 0; v < S; ++v) CA(k, v) = 0.0f;
-    CA(0, 0) = 2.0f; /* float cost_array[8][32] = { 2.0f } (HPM.cu:1244) */
+        for (int v = 0; v < S; ++v) CAG(k, v) = 0.0f;
+    CAG(0, 0) = 2.0f; /* float cost_array[8][32] = { 2.0f } (HPM.cu:1244) */
 
-    bool flag[8];
     int pos[8];
+    uint32_t flags = 0;
     pos[0] = center - 5 - 6 * W;
     pos[1] = center - W * 5;
     pos[2] = center + 6 - 5 * W;
@@ -633,58 +665,112 @@ __global__ void __launch_bounds__(kBlock) k_propagate(PMArgs a, int iter, int co
     pos[5] = center - 5;
     pos[6] = center - 6 + 5 * W;
     pos[7] = center + 5;
+    /* Identical planes give identical cost vectors: a candidate whose plane
+     * equals the current hypothesis (cost vector cached) or an earlier
+     * candidate reuses those values. */
 #pragma unroll
     for (int k = 0; k < 8; ++k) {
-        flag[k] = first_site_valid(k, 0, px, py, W, H);
-        if (flag[k]) {
-            pos[k] = select_site(a, k, 0, px, py);
-            cost_vector(a, px, py, a.planes[pos[k]], sW, sWR, tid, rs, &CA(k, 0), S * 0 + kBlock);
+        if (!first_site_valid(k, 0, px, py, W, H)) continue;
+        flags |= 1u << k;
+        pos[k] = select_site(a, k, 0, px, py);
+        const float4 c = a.planes[pos[k]];
+        if (same_plane(c, cur)) {
+            for (int v = 0; v < S; ++v) CAG(k, v) = *cache_at(a, v, center);
+            continue;
+        }
+        int src = -1;
+#pragma unroll
+        for (int j = 0; j < k; ++j)
+            if (src < 0 && ((flags >> j) & 1u) && same_plane(c, a.planes[pos[j]])) src = j;
+        if (src >= 0) {
+            for (int v = 0; v < S; ++v) CAG(k, v) = CAG(src, v);
+        } else {
+            cost_vector(a, px, py, c, sWW, tid, rs, &CAG(k, 0), (int)npx);
         }
     }
 
     /* Extension: only the left-up polyline can extend, because
      * bool symbol_eight_orientations[10] = { true } sets index 0 only
      * (HPM.cu:1475).  JudgeExtend: HPM.cu:1036-1059. */
-    if (flag[0]) {
+    if (flags & 1u) {
         for (int r = 0; r < 3; ++r) {
             const float good = (float)(0.8 * exp(-iter * iter * (3 - r) / 90.0));
             int good_sum = 0, bad_sum = 0;
             for (int v = 0; v < S; ++v) {
-                const float c = CA(0, v);
+                const float c = CAG(0, v);
                 if (c < good) good_sum++;
                 if (c > 1.2f) bad_sum++;
             }
             if (good_sum >= 1 && bad_sum <= 2) break;
-            if (first_site_valid(0, r, px, py, W, H)) {
-                int best = select_site(a, 0, r, px, py);
-                bool fresh = true;
-                if (a.costs[best] > a.costs[pos[0]]) {
-                    best = pos[0];
-                    fresh = false;
-                }
-                pos[0] = best;
-                if (fresh) cost_vector(a, px, py, a.planes[best], sW, sWR, tid, rs, &CA(0, 0), kBlock);
+            if (!first_site_valid(0, r, px, py, W, H)) continue; /* flag[0] is set: keep site and costs */
+            const int best = select_site(a, 0, r, px, py);
+            if (a.costs[best] > a.costs[pos[0]]) continue; /* the previous site is better: keep it */
+            const float4 prev = a.planes[pos[0]];
+            pos[0] = best;
+            const float4 p = a.planes[best];
+            if (same_plane(p, prev)) continue;
+            if (same_plane(p, cur)) {
+                for (int v = 0; v < S; ++v) CAG(0, v) = *cache_at(a, v, center);
+                continue;
+            }
+            int src = -1;
+#pragma unroll
+            for (int j = 1; j < 8; ++j)
+                if (src < 0 && ((flags >> j) & 1u) && same_plane(p, a.planes[pos[j]])) src = j;
+            if (src >= 0) {
+                for (int v = 0; v < S; ++v) CAG(0, v) = CAG(src, v);
+            } else {
+                cost_vector(a, px, py, p, sWW, tid, rs, &CAG(0, 0), (int)npx);
             }
         }
     }
+#pragma unroll
+    for (int k = 0; k < 8; ++k) a.cand_pos[(size_t)k * npx + center] = pos[k];
+    a.cand_flags[center] = flags;
+}
+
+template <int SMAX>
+__global__ void __launch_bounds__(kBlock, HPM_P2_MIN_BLOCKS) k_prop_refine(const __grid_constant__ PMArgs a, int iter,
+                                                                            int color)
+{
+    __shared__ float2 sWW[kTaps * kBlock];
+    const int tid = threadIdx.y * kBlockX + threadIdx.x;
+    const int py = blockIdx.y * kBlockY + threadIdx.y;
+    const int px = blockIdx.x * (2 * kBlockX) + 2 * threadIdx.x + ((py + color) & 1);
+    if (px >= a.W || py >= a.rows_cov) return;
+    const int W = a.W, S = a.n - 1;
+    const size_t npx = (size_t)W * a.H;
+    const int center = py * W + px;
+    const HpmCamera &cam = a.cam[0];
+    const uint32_t flags = a.cand_flags[center];
+    int pos[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) pos[k] = a.cand_pos[(size_t)k * npx + center];
+#define FLAG(k) (((flags >> (k)) & 1u) != 0)
+    Rng rng;
+    rng.init(a.seed_lo, a.seed_hi, (uint32_t)center, (uint32_t)(1 + iter), a.salt);
 
     /* Multi-hypothesis joint view selection, HPM.cu:1548-1613. */
-    float vw[kMaxSrc];
-    float sp[kMaxSrc];
-    const uint32_t nbm[4] = {flag[1] ? a.views[center - W * 5] : 0u, flag[3] ? a.views[center + W * 5] : 0u,
-                             flag[5] ? a.views[center - 5] : 0u, flag[7] ? a.views[center + 5] : 0u};
+    float vw[SMAX];
+    float sp[SMAX];
+    const uint32_t nbm[4] = {FLAG(1) ? a.views[center - W * 5] : 0u, FLAG(3) ? a.views[center + W * 5] : 0u,
+                             FLAG(5) ? a.views[center - 5] : 0u, FLAG(7) ? a.views[center + 5] : 0u};
     const float thr = (float)(0.8 * expf((float)(iter * iter) / (-90.0f)));
-    for (int v = 0; v < S; ++v) {
+#pragma unroll
+    for (int v = 0; v < SMAX; ++v) {
+        vw[v] = 0.0f;
+        sp[v] = 0.0f;
+        if (v >= S) continue;
         float prior = 0.0f;
 #pragma unroll
         for (int i = 0; i < 4; ++i)
-            if (flag[2 * i + 1]) prior += ((nbm[i] >> v) & 1u) ? 0.9f : 0.1f;
+            if (FLAG(2 * i + 1)) prior += ((nbm[i] >> v) & 1u) ? 0.9f : 0.1f;
         float count = 0;
         int count_false = 0;
         float tmpw = 0;
 #pragma unroll
         for (int k = 0; k < 8; ++k) {
-            const float c = CA(k, v);
+            const float c = CAG(k, v);
             if (c < thr) {
                 tmpw += expf(c * c / (-0.18f));
                 count++;
@@ -697,31 +783,37 @@ __global__ void __launch_bounds__(kBlock) k_propagate(PMArgs a, int iter, int co
         else if (count_false < 3)
             p = expf(thr * thr / (-0.32f));
         sp[v] = p * prior;
-        vw[v] = 0.0f;
     }
     {
         float s = 0.0f;
-        for (int v = 0; v < S; ++v) s += sp[v];
+#pragma unroll
+        for (int v = 0; v < SMAX; ++v)
+            if (v < S) s += sp[v];
         const float inv = 1.0f / s;
         float cum = 0.0f;
-        for (int v = 0; v < S; ++v) {
-            cum += sp[v] * inv;
-            sp[v] = cum;
-        }
+#pragma unroll
+        for (int v = 0; v < SMAX; ++v)
+            if (v < S) {
+                cum += sp[v] * inv;
+                sp[v] = cum;
+            }
     }
     for (int smp = 0; smp < 15; ++smp) {
         const float rp = rng.uniform() - FLT_EPSILON;
-        for (int v = 0; v < S; ++v) {
-            if (sp[v] > rp) {
+        bool done = false;
+#pragma unroll
+        for (int v = 0; v < SMAX; ++v) {
+            if (!done && v < S && sp[v] > rp) {
                 vw[v] += 1.0f;
-                break;
+                done = true;
             }
         }
     }
     uint32_t tsv = 0;
     float wn = 0.0f;
-    for (int v = 0; v < S; ++v)
-        if (vw[v] > 0) {
+#pragma unroll
+    for (int v = 0; v < SMAX; ++v)
+        if (v < S && vw[v] > 0) {
             tsv |= 1u << v;
             wn += vw[v];
         }
@@ -730,16 +822,18 @@ __global__ void __launch_bounds__(kBlock) k_propagate(PMArgs a, int iter, int co
 #pragma unroll
     for (int k = 0; k < 8; ++k) {
         float f = 0.0f;
-        const float4 hk = (a.geom && flag[k]) ? a.planes[pos[k]] : make_float4(0, 0, 0, 1);
-        for (int v = 0; v < S; ++v) {
-            if (vw[v] > 0) {
+        float4 hk = make_float4(0, 0, 0, 1);
+        if (a.geom && FLAG(k)) hk = a.planes[pos[k]];
+#pragma unroll
+        for (int v = 0; v < SMAX; ++v) {
+            if (v < S && vw[v] > 0) {
                 if (a.geom) {
-                    if (flag[k])
-                        f += vw[v] * (CA(k, v) + 0.1f * geom_cost(a, v + 1, hk, px, py));
+                    if (FLAG(k))
+                        f += vw[v] * (CAG(k, v) + 0.1f * geom_cost(a, v + 1, hk, px, py));
                     else
-                        f += vw[v] * (CA(k, v) + 0.1f * 5.0f);
+                        f += vw[v] * (CAG(k, v) + 0.1f * 5.0f);
                 } else {
-                    f += vw[v] * CA(k, v);
+                    f += vw[v] * CAG(k, v);
                 }
             }
         }
@@ -756,17 +850,19 @@ __global__ void __launch_bounds__(kBlock) k_propagate(PMArgs a, int iter, int co
             }
     }
 
-    float4 plane = a.planes[center];
-    /* re-score the current hypothesis (HPM.cu:1637-1650); the slot of
-     * direction 1 is free now that final costs are known */
-    float *cvn = &CA(1, 0);
-    cost_vector(a, px, py, plane, sW, sWR, tid, rs, cvn, kBlock);
+    /* re-score of the current hypothesis (HPM.cu:1637-1650), from the cache */
+    const float4 cur = a.planes[center];
+    float4 plane = cur;
+    int best_row = -1; /* -1: the cached current hypothesis */
     float cost_now = 0.0f;
-    for (int v = 0; v < S; ++v) {
-        if (a.geom)
-            cost_now += vw[v] * (cvn[v * kBlock] + 0.1f * geom_cost(a, v + 1, plane, px, py));
-        else
-            cost_now += vw[v] * cvn[v * kBlock];
+#pragma unroll
+    for (int v = 0; v < SMAX; ++v) {
+        if (v < S && vw[v] > 0) {
+            if (a.geom)
+                cost_now += vw[v] * (*cache_at(a, v, center) + 0.1f * geom_cost(a, v + 1, plane, px, py));
+            else
+                cost_now += vw[v] * *cache_at(a, v, center);
+        }
     }
     cost_now /= wn;
     float cost = cost_now;
@@ -787,7 +883,7 @@ __global__ void __launch_bounds__(kBlock) k_propagate(PMArgs a, int iter, int co
 #pragma unroll
             for (int k = 0; k < 8; ++k) {
                 rfc[k] = 0.0f;
-                if (flag[k]) {
+                if (FLAG(k)) {
                     const float4 hq = a.planes[pos[k]];
                     const float dn = depth_from_plane(cam, hq, px, py);
                     const float pr = restricted_prior(dn - depth_prior, dot3(pp, hq), two_dss, two_ass);
@@ -807,44 +903,49 @@ __global__ void __launch_bounds__(kBlock) k_propagate(PMArgs a, int iter, int co
             const float dn = depth_from_plane(cam, plane, px, py);
             const float pr = restricted_prior(dn - depth_prior, dot3(pp, plane), two_dss, two_ass);
             const float rcn = expf(-cost_now * cost_now / beta) * pr;
-            if (flag[max_idx]) {
+            if (FLAG(max_idx)) {
                 const float4 hb = a.planes[pos[max_idx]];
                 const float db = depth_from_plane(cam, hb, px, py);
                 if (db >= a.dmin && db <= a.dmax && rfc[max_idx] > rcn) {
                     depth_now = db;
                     plane = hb;
+                    best_row = max_idx;
                     cost = fc[max_idx];
                     restricted_cost = rfc[max_idx];
                     sel = tsv;
                 }
             }
-        } else if (flag[min_idx]) {
+        } else if (FLAG(min_idx)) {
             const float4 hb = a.planes[pos[min_idx]];
             const float db = depth_from_plane(cam, hb, px, py);
             if (db >= a.dmin && db <= a.dmax && fc[min_idx] < cost_now) {
                 depth_now = db;
                 plane = hb;
+                best_row = min_idx;
                 cost = fc[min_idx];
             }
         }
     }
-    if (!a.prior && flag[min_idx]) {
+    if (!a.prior && FLAG(min_idx)) {
         const float4 hb = a.planes[pos[min_idx]];
         const float db = depth_from_plane(cam, hb, px, py);
         if (db >= a.dmin && db <= a.dmax && fc[min_idx] < cost_now) {
             depth_now = db;
             plane = hb;
+            best_row = min_idx;
             cost = fc[min_idx];
             sel = tsv;
         }
         if (cost != cost) {
             depth_now = db;
             plane = hb;
+            best_row = min_idx;
             sel = tsv;
         }
     }
 
     /* PlaneHypothesisRefinement, HPM.cu:1143-1220 */
+    const RefStats rs = ref_window(a, px, py, sWW, tid);
     {
         const float pert = 0.02f;
         const float depth_sigma = (a.dmax - a.dmin) / 64.0f;
@@ -871,50 +972,54 @@ __global__ void __launch_bounds__(kBlock) k_propagate(PMArgs a, int iter, int co
         const float4 n_pert = perturbed_normal(cam, px, py, plane, rng, (float)(pert * kPiD));
         const float depths[5] = {depth_rand, depth_now, depth_rand, depth_now, depth_pert};
         const float4 normals[5] = {plane, n_rand, n_rand, n_pert, plane};
-        float *cvr = &CA(2, 0);
+        int scratch = 8;
 #pragma unroll 1
         for (int i = 0; i < 5; ++i) {
             float4 t = normals[i];
             t.w = distance_to_origin(cam, px, py, depths[i], t);
-            cost_vector(a, px, py, t, sW, sWR, tid, rs, cvr, kBlock);
+            cost_vector(a, px, py, t, sWW, tid, rs, &CAG(scratch, 0), (int)npx);
             float tc = 0.0f;
-            for (int v = 0; v < S; ++v) {
-                if (vw[v] > 0) {
+#pragma unroll
+            for (int v = 0; v < SMAX; ++v) {
+                if (v < S && vw[v] > 0) {
                     if (a.geom)
-                        tc += vw[v] * (cvr[v * kBlock] + 0.1f * geom_cost(a, v + 1, t, px, py));
+                        tc += vw[v] * (CAG(scratch, v) + 0.1f * geom_cost(a, v + 1, t, px, py));
                     else
-                        tc += vw[v] * cvr[v * kBlock];
+                        tc += vw[v] * CAG(scratch, v);
                 }
             }
             tc /= wn;
             const float depth_before = depth_from_plane(cam, t, px, py);
+            bool take;
             if (use_prior) {
                 const float dd = depths[i] - depth_prior;
                 const float pr = restricted_prior(dd, dot3(pp, t), two_dss, two_ass);
                 const float rtc = expf(-tc * tc / beta) * pr;
-                if (depth_before >= a.dmin && depth_before <= a.dmax && rtc > restricted_cost) {
-                    depth_now = depth_before;
-                    plane = t;
-                    cost = tc;
-                    restricted_cost = rtc;
-                }
+                take = depth_before >= a.dmin && depth_before <= a.dmax && rtc > restricted_cost;
+                if (take) restricted_cost = rtc;
             } else {
-                if (depth_before >= a.dmin && depth_before <= a.dmax && tc < cost) {
-                    depth_now = depth_before;
-                    plane = t;
-                    cost = tc;
-                }
+                take = depth_before >= a.dmin && depth_before <= a.dmax && tc < cost;
+            }
+            if (take) {
+                depth_now = depth_before;
+                plane = t;
+                cost = tc;
+                best_row = scratch;
+                scratch = (scratch == 8) ? 9 : 8;
             }
         }
     }
-#undef CA
     a.planes[center] = plane;
     a.costs[center] = cost;
     a.views[center] = sel;
+    if (best_row >= 0)
+        for (int v = 0; v < S; ++v) *cache_at(a, v, center) = CAG(best_row, v);
+#undef FLAG
 }
+#undef CAG
 
 /* GetDepthandNormal, HPM.cu:1751-1764 */
-__global__ void k_depth_normal(PMArgs a, float4 *planes)
+__global__ void k_depth_normal(const __grid_constant__ PMArgs a, float4 *planes)
 {
     const int px = blockIdx.x * blockDim.x + threadIdx.x;
     const int py = blockIdx.y * blockDim.y + threadIdx.y;
@@ -926,7 +1031,7 @@ __global__ void k_depth_normal(PMArgs a, float4 *planes)
 }
 
 /* CheckerboardFilter, HPM.cu:1766-1904 */
-__global__ void k_filter(PMArgs a, float4 *pl, const float *costs, int color)
+__global__ void k_filter(const __grid_constant__ PMArgs a, float4 *pl, const float *costs, int color)
 {
     const int py = blockIdx.y * blockDim.y + threadIdx.y;
     const int px = blockIdx.x * (2 * blockDim.x) + 2 * threadIdx.x + ((py + color) & 1);
@@ -964,35 +1069,36 @@ __global__ void k_filter(PMArgs a, float4 *pl, const float *costs, int color)
     pl[center].w = (n % 2 == 0) ? (f[m - 1] + f[m]) / 2 : f[m];
 }
 
-__global__ void __launch_bounds__(kBlock) k_cost_vectors(PMArgs a, const float4 *planes, float *out)
+__global__ void __launch_bounds__(kBlock) k_cost_vectors(const __grid_constant__ PMArgs a, const float4 *planes,
+                                                          float *out)
 {
-    __shared__ float sW[kTaps * kBlock];
-    __shared__ float sWR[kTaps * kBlock];
+    __shared__ float2 sWW[kTaps * kBlock];
     const int tid = threadIdx.y * kBlockX + threadIdx.x;
     const int px = blockIdx.x * kBlockX + threadIdx.x;
     const int py = blockIdx.y * kBlockY + threadIdx.y;
     if (px >= a.W || py >= a.H) return;
-    const RefStats rs = ref_window(a, px, py, sW, sWR, tid);
+    const RefStats rs = ref_window(a, px, py, sWW, tid);
     const int c = py * a.W + px;
     const int S = a.n - 1;
-    for (int v = 1; v < a.n; ++v) out[(size_t)c * S + v - 1] = ncc(a, v, px, py, planes[c], sW, sWR, tid, rs);
+    cost_vector(a, px, py, planes[c], sWW, tid, rs, out + (size_t)c * S, 1);
 }
 
-__global__ void __launch_bounds__(kBlock) k_initial_costs(PMArgs a, const float4 *planes, float *cost,
-                                                          uint32_t *views)
+__global__ void __launch_bounds__(kBlock) k_initial_costs(const __grid_constant__ PMArgs a, const float4 *planes,
+                                                          float *cost, uint32_t *views)
 {
-    __shared__ float sW[kTaps * kBlock];
-    __shared__ float sWR[kTaps * kBlock];
+    __shared__ float2 sWW[kTaps * kBlock];
+    __shared__ float sCV[kMaxSrc * kBlock];
     const int tid = threadIdx.y * kBlockX + threadIdx.x;
     const int px = blockIdx.x * kBlockX + threadIdx.x;
     const int py = blockIdx.y * kBlockY + threadIdx.y;
     if (px >= a.W || py >= a.H) return;
-    const RefStats rs = ref_window(a, px, py, sW, sWR, tid);
+    const RefStats rs = ref_window(a, px, py, sWW, tid);
     const int c = py * a.W + px;
-    cost[c] = initial_cost(a, px, py, planes[c], sW, sWR, tid, rs, &views[c]);
+    cost_vector(a, px, py, planes[c], sWW, tid, rs, sCV + tid, kBlock);
+    cost[c] = initial_cost_from(a, sCV + tid, kBlock, &views[c]);
 }
 
-__global__ void k_geom_costs(PMArgs a, const float4 *planes, float *out)
+__global__ void k_geom_costs(const __grid_constant__ PMArgs a, const float4 *planes, float *out)
 {
     const int px = blockIdx.x * blockDim.x + threadIdx.x;
     const int py = blockIdx.y * blockDim.y + threadIdx.y;
@@ -1000,6 +1106,15 @@ __global__ void k_geom_costs(PMArgs a, const float4 *planes, float *out)
     const int c = py * a.W + px;
     const int S = a.n - 1;
     for (int v = 1; v < a.n; ++v) out[(size_t)c * S + v - 1] = geom_cost(a, v, planes[c], px, py);
+}
+
+template <int SMAX>
+cudaError_t launch_prop_t(const PMArgs &a, int iter, int color, cudaStream_t s)
+{
+    dim3 grid((a.W + 2 * kBlockX - 1) / (2 * kBlockX), (a.rows_cov + kBlockY - 1) / kBlockY);
+    k_prop_dirs<<<grid, dim3(kBlockX, kBlockY), 0, s>>>(a, iter, color);
+    k_prop_refine<SMAX><<<grid, dim3(kBlockX, kBlockY), 0, s>>>(a, iter, color);
+    return cudaGetLastError();
 }
 
 }  // namespace
@@ -1026,18 +1141,13 @@ cudaError_t launch_init(const PMArgs &a, cudaStream_t s)
 
 cudaError_t launch_propagate(const PMArgs &a, int iter, int color, cudaStream_t s)
 {
-    const int S = a.n - 1;
-    const size_t smem = (size_t)(2 * kTaps + 8 * S) * kBlock * sizeof(float);
-    static bool attr_set = false;
-    if (!attr_set) {
-        cudaFuncSetAttribute(k_propagate, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (2 * kTaps + 8 * kMaxSrc) * kBlock * (int)sizeof(float));
-        attr_set = true;
-    }
     if (a.rows_cov <= 0) return cudaSuccess;
-    dim3 grid((a.W + 2 * kBlockX - 1) / (2 * kBlockX), (a.rows_cov + kBlockY - 1) / kBlockY);
-    k_propagate<<<grid, dim3(kBlockX, kBlockY), smem, s>>>(a, iter, color);
-    return cudaGetLastError();
+    const int S = a.n - 1;
+    if (S <= 4) return launch_prop_t<4>(a, iter, color, s);
+    if (S <= 8) return launch_prop_t<8>(a, iter, color, s);
+    if (S <= 12) return launch_prop_t<12>(a, iter, color, s);
+    if (S <= 16) return launch_prop_t<16>(a, iter, color, s);
+    return launch_prop_t<kMaxSrc>(a, iter, color, s);
 }
 
 cudaError_t launch_depth_normal_filter(const PMArgs &a, float4 *planes, const float *costs, cudaStream_t s)

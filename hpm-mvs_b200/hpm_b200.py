@@ -16,7 +16,7 @@ import os
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libhpm_b200.so")
+LIB_PATH = os.environ.get("HPM_B200_LIB", os.path.join(HERE, "libhpm_b200.so"))
 
 CAMERA_DTYPE = np.dtype(
     [("K", "<f4", 9), ("R", "<f4", 9), ("t", "<f4", 3), ("height", "<i4"), ("width", "<i4"),
