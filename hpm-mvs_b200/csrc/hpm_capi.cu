@@ -300,6 +300,7 @@ int hpm_set_views(hpm_ctx *c, const float *const *images, const HpmCamera *cams,
         c->cams[i] = cams[i];
     }
     c->n = num_images;
+    c->pass_counter = 0; /* random stream ids restart with every problem */
     c->has_depth = false;
     c->has_prior = false;
     const size_t n = npx(c);
@@ -395,7 +396,10 @@ int hpm_clear_prior(hpm_ctx *c)
     return HPM_OK;
 }
 
-int hpm_run_patchmatch(hpm_ctx *c, const HpmParams *p)
+/* One pass: initialisation, `half_steps` red/black half-steps (the
+ * reference runs 2 per iteration), then optionally depth/normal conversion
+ * and the two filter kernels.  Nothing waits on the host in between. */
+static int run_pass(hpm_ctx *c, const HpmParams *p, int half_steps, int finalize, bool sync)
 {
     if (!c) return HPM_ERR_ARG;
     if (!p) return fail(c, HPM_ERR_ARG, "hpm_run_patchmatch: null params");
@@ -406,6 +410,7 @@ int hpm_run_patchmatch(hpm_ctx *c, const HpmParams *p)
         return fail(c, HPM_ERR_STATE, "geometric consistency needs hpm_set_geom_depths");
     if (p->planar_prior && !c->has_prior) return fail(c, HPM_ERR_STATE, "planar prior needs hpm_set_prior");
     if (!(p->depth_max > p->depth_min)) return fail(c, HPM_ERR_ARG, "depth range is empty");
+    if (p->top_k < 1 || p->top_k > kMaxSrc) return fail(c, HPM_ERR_ARG, "top_k outside [1, %d]", kMaxSrc);
     int r = select_device(c);
     if (r) return r;
     PMArgs a = make_args(c);
@@ -420,24 +425,38 @@ int hpm_run_patchmatch(hpm_ctx *c, const HpmParams *p)
     a.seed_hi = (uint32_t)(p->seed >> 32);
     a.salt = c->pass_counter++;
     if (c->counting) CK(cudaMemsetAsync(c->d_counters, 0, 2 * sizeof(unsigned long long), c->stream), "counters");
-    const int iters = p->honour_max_iterations ? p->max_iterations : 3; /* HPM.cu:1933 */
     cudaEvent_t e0;
     prof_begin(c, 0, &e0);
     CK(launch_init(a, c->stream), "init kernel");
     prof_end(c, 0, e0);
-    for (int it = 0; it < iters; ++it) {
-        for (int color = 0; color < 2; ++color) {
-            prof_begin(c, 1, &e0);
-            CK(launch_propagate(a, it, color, c->stream), "propagate kernel");
-            prof_end(c, 1, e0);
-        }
+    for (int hs = 0; hs < half_steps; ++hs) {
+        prof_begin(c, 1, &e0);
+        CK(launch_propagate(a, hs / 2, hs % 2, c->stream), "propagate kernels");
+        prof_end(c, 1, e0);
     }
-    prof_begin(c, 2, &e0);
-    CK(launch_depth_normal_filter(a, c->d_planes, c->d_costs, c->stream), "depth/normal + filter kernels");
-    prof_end(c, 2, e0);
+    if (finalize) {
+        prof_begin(c, 2, &e0);
+        CK(launch_depth_normal_filter(a, c->d_planes, c->d_costs, c->stream), "depth/normal + filter kernels");
+        prof_end(c, 2, e0);
+    }
     c->has_state = true;
-    CK(cudaStreamSynchronize(c->stream), "hpm_run_patchmatch");
+    if (sync) CK(cudaStreamSynchronize(c->stream), "hpm_run_patchmatch");
     return HPM_OK;
+}
+
+int hpm_run_patchmatch(hpm_ctx *c, const HpmParams *p)
+{
+    if (!c || !p) return HPM_ERR_ARG;
+    const int iters = p->honour_max_iterations ? p->max_iterations : 3; /* HPM.cu:1933 */
+    if (iters < 0 || iters > 64) return fail(c, HPM_ERR_ARG, "max_iterations outside [0, 64]");
+    return run_pass(c, p, 2 * iters, 1, true);
+}
+
+int hpm_run_partial(hpm_ctx *c, const HpmParams *p, int half_steps, int finalize)
+{
+    if (!c || !p) return HPM_ERR_ARG;
+    if (half_steps < 0 || half_steps > 128) return fail(c, HPM_ERR_ARG, "half_steps outside [0, 128]");
+    return run_pass(c, p, half_steps, finalize, true);
 }
 
 int hpm_get_result(hpm_ctx *c, float *planes, float *costs)

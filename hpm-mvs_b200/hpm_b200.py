@@ -31,11 +31,22 @@ STATUS_NAMES = {0: "HPM_OK", -1: "HPM_ERR_ARG", -2: "HPM_ERR_CUDA", -3: "HPM_ERR
 # every symbol include/hpm_b200.h declares
 EXPORTED = [
     "hpm_default_params", "hpm_create", "hpm_destroy", "hpm_last_error", "hpm_set_views", "hpm_set_geom_depths",
-    "hpm_set_hypotheses", "hpm_set_prior", "hpm_clear_prior", "hpm_run_patchmatch", "hpm_get_result",
+    "hpm_set_hypotheses", "hpm_set_prior", "hpm_clear_prior", "hpm_run_patchmatch", "hpm_run_partial",
+    "hpm_get_result",
     "hpm_get_selected_views", "hpm_device_state", "hpm_stream", "hpm_jbu", "hpm_cost_vectors",
     "hpm_initial_costs", "hpm_geom_costs", "hpm_depth_normal_filter", "hpm_profile_enable", "hpm_profile_read",
     "hpm_count_enable", "hpm_count_read", "hpm_write_dmb", "hpm_read_dmb", "hpm_read_camera", "hpm_read_pair",
+    "hpm_fp32_peak",
 ]
+
+
+def fp32_peak(device: int = 0) -> float:
+    """Measured FP32 FMA throughput of the device in TFLOP/s."""
+    t = ctypes.c_float()
+    rc = lib().hpm_fp32_peak(device, ctypes.byref(t), None)
+    if rc != HPM_OK:
+        raise HpmError(f"hpm_fp32_peak: {STATUS_NAMES.get(rc, rc)}")
+    return float(t.value)
 
 
 class HpmParams(ctypes.Structure):
@@ -157,6 +168,10 @@ class Context:
 
     def run_patchmatch(self, params: HpmParams) -> None:
         self._check(lib().hpm_run_patchmatch(self._h, ctypes.byref(params)), "hpm_run_patchmatch")
+
+    def run_partial(self, params: HpmParams, half_steps: int, finalize: bool) -> None:
+        self._check(lib().hpm_run_partial(self._h, ctypes.byref(params), int(half_steps), int(finalize)),
+                    "hpm_run_partial")
 
     def get_result(self):
         h, w = self.shape

@@ -118,6 +118,12 @@ int hpm_clear_prior(hpm_ctx *ctx);
  * device for the next pass, as in the reference. */
 int hpm_run_patchmatch(hpm_ctx *ctx, const HpmParams *params);
 
+/* Parity entry point: the same pass cut after `half_steps` red/black
+ * half-steps (the reference runs 6), with or without the depth/normal
+ * conversion and filters.  Random streams match hpm_run_patchmatch: the k-th
+ * pass of a problem (counting from hpm_set_views) draws from stream k. */
+int hpm_run_partial(hpm_ctx *ctx, const HpmParams *params, int half_steps, int finalize);
+
 /* Copies the pass result to the host: planes = (world normal, depth),
  * costs.  Either pointer may be NULL.  Replaces the D2H copies of
  * HPM.cu:1954-1955 and GetPlaneHypothesis / GetCost (HPM.cpp:739-747). */
@@ -162,6 +168,12 @@ int hpm_profile_read(hpm_ctx *ctx, float *ms4, int *counts4);
  * num_images-1 NCC windows); requires hpm_count_enable(ctx, 1) before it. */
 int hpm_count_enable(hpm_ctx *ctx, int enable);
 int hpm_count_read(hpm_ctx *ctx, uint64_t *cost_vectors, uint64_t *geom_terms);
+
+/* Benchmark utility (no counterpart in the reference): measured FP32 FMA
+ * throughput of `device` in TFLOP/s, the roofline denominator of the
+ * PatchMatch kernels.  sm_clock_mhz_hint (may be NULL) receives the
+ * device's nominal SM clock. */
+int hpm_fp32_peak(int device, float *tflops, float *sm_clock_mhz_hint);
 
 /* ---- files (drop-in formats) ---- */
 
