@@ -36,7 +36,7 @@ EXPORTED = [
     "hpm_get_selected_views", "hpm_device_state", "hpm_stream", "hpm_jbu", "hpm_cost_vectors",
     "hpm_initial_costs", "hpm_geom_costs", "hpm_depth_normal_filter", "hpm_profile_enable", "hpm_profile_read",
     "hpm_count_enable", "hpm_count_read", "hpm_write_dmb", "hpm_read_dmb", "hpm_read_camera", "hpm_read_pair",
-    "hpm_fp32_peak",
+    "hpm_fp32_peak", "hpm_jbu_noalloc",
 ]
 
 

@@ -145,6 +145,30 @@ void *hpm_stream(hpm_ctx *ctx);
 int hpm_jbu(hpm_ctx *ctx, const float *guide, int cols, int rows, const float *coarse_depth,
             const float *coarse_normal, int s_cols, int s_rows, float *out_depth, float *out_normal);
 
+/* Joint bilateral upsampling that allocates nothing.  No counterpart in the
+ * reference.  For callers that may not call cudaMalloc while they run (a host
+ * that gives its whole device-memory budget to its own pool up front, or
+ * that must not add a device synchronisation or a memory-accounting change
+ * in its loop): no context is needed, every buffer is the caller's device
+ * memory (guide cols x rows floats; coarse_depth s_cols x s_rows floats;
+ * coarse_normal and out_normal 3 floats per pixel; out_depth cols x rows
+ * floats), and the work is queued on `stream` (cudaStream_t as void*, NULL
+ * for the default stream) of `device`.  Same computation as hpm_jbu.
+ *
+ * Its scratch is a fixed device array of HPM_JBU_NOALLOC_MAX_COARSE float4
+ * (16 MiB) that every GPU loading this library holds until the process
+ * exits; coarse grids with more pixels are rejected with HPM_ERR_ARG.  The
+ * first call on a device looks that array's address up (a CUDA symbol
+ * query), so make the first call on each device before any stream capture.
+ * All calls on a device share the array: calls that overlap on the GPU
+ * (different streams, or different host threads) race and must be ordered
+ * by the caller.  Returns HPM_OK without touching the outputs when the
+ * integer scale is 1, like hpm_jbu. */
+#define HPM_JBU_NOALLOC_MAX_COARSE (1 << 20)
+int hpm_jbu_noalloc(int device, const float *guide, int cols, int rows, const float *coarse_depth,
+                    const float *coarse_normal, int s_cols, int s_rows, float *out_depth, float *out_normal,
+                    void *stream);
+
 /* Deterministic building blocks exposed for parity checks. */
 
 /* ComputeMultiViewCostVector (HPM.cu:438-443) for one ref-frame plane per
