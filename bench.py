@@ -48,7 +48,13 @@ def parse_args():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    return ap.parse_args()
+    ap.add_argument("--size", default=None,
+                    help="WxH override of the workload's resolution (profiling captures use a smaller case)")
+    args = ap.parse_args()
+    if args.size:
+        w, h = (int(x) for x in args.size.lower().split("x"))
+        WORKLOAD.update(width=w, height=h, name=f"plain HPM PatchMatch pass, {w}x{h}, 10 sources")
+    return args
 
 
 class Dist:

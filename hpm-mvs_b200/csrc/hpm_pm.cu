@@ -15,14 +15,15 @@
  *    weight and one of weight*ref instead of an exp, a sqrt and two texture
  *    fetches.
  *  - Source views are sampled by the texture unit (float cudaArray, linear
- *    filter, clamped edges: the reference's own texture set-up), which is
- *    the only way to get the hardware's filter arithmetic bit for bit
- *    (its bilinear weights are 1.8 fixed point with round-half-up, and the
- *    weighted sum is formed at reduced precision; a software gather
- *    differs by up to ~0.5 gray levels per tap).
- *  - Shared-memory cost matrix.  cost_array[8][32] (1.5 KB of local memory
- *    per thread in the reference) becomes a [direction*S + view][thread]
- *    shared array sized by the actual number of source views.
+ *    filter, clamped edges: the reference's own texture set-up), so the
+ *    bilinear samples are the reference's bit for bit.  The filter rounds
+ *    coordinates to 1/256 (half up) and only the far corner's weight
+ *    A*B/256; a textbook bilinear gather differs by up to ~0.5 gray levels
+ *    per tap.
+ *  - The per-pixel cost matrix (cost_array[8][32], 1.5 KB of local memory per
+ *    thread in the reference) is handed from the site/direction kernel to the
+ *    selection/refinement kernel through L2, so that shared memory holds only
+ *    the 288-byte reference window per pixel.
  *  - Counter-based Philox random numbers: no 48-byte curand state per pixel
  *    in HBM and no curand_init skip-ahead; draws come in the reference's
  *    order.
