@@ -17,58 +17,9 @@
 #include <new>
 #include <vector>
 
-#include "hpm_internal.h"
+#include "hpm_capi_internal.h"
 
 using namespace hpm;
-
-struct hpm_ctx {
-    int device = 0;
-    cudaStream_t stream = nullptr;
-    char err[512] = {0};
-
-    int n = 0;
-    HpmCamera cams[kMaxViews];
-    float *d_img[kMaxViews] = {nullptr};
-    size_t img_cap[kMaxViews] = {0};
-    cudaArray_t arr[kMaxViews] = {nullptr};
-    int arr_w[kMaxViews] = {0}, arr_h[kMaxViews] = {0};
-    cudaTextureObject_t tex[kMaxViews] = {0};
-    float *d_depth[kMaxViews] = {nullptr};
-    size_t depth_cap[kMaxViews] = {0};
-    bool has_depth = false;
-    PairGeom *d_pair = nullptr;
-
-    float4 *d_planes = nullptr;
-    float *d_costs = nullptr;
-    uint32_t *d_views = nullptr;
-    float4 *d_prior = nullptr;
-    uint32_t *d_masks = nullptr;
-    size_t px_cap = 0;
-    bool has_prior = false;
-    bool has_state = false;
-
-    unsigned long long *d_counters = nullptr;
-    bool counting = false;
-
-    bool profiling = false;
-    std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> prof_events;
-    float prof_ms[4] = {0, 0, 0, 0};
-    int prof_cnt[4] = {0, 0, 0, 0};
-
-    uint32_t pass_counter = 0;
-
-    void *d_scratch = nullptr;
-    size_t scratch_cap = 0;
-
-    float *d_cache = nullptr; /* cost vector of each pixel's current hypothesis, [S][H*W] */
-    size_t cache_cap = 0;
-    float *d_cand = nullptr; /* half-step hand-off: cost matrix rows [kCandRows*S][H*W] */
-    size_t cand_cap = 0;
-    int *d_pos = nullptr; /* chosen NESP sites [8][H*W] */
-    size_t pos_cap = 0;
-    uint32_t *d_flags = nullptr; /* valid-direction bits [H*W] */
-    size_t flags_cap = 0;
-};
 
 namespace {
 
@@ -261,6 +212,7 @@ int hpm_destroy(hpm_ctx *c)
     cudaFree(c->d_cand);
     cudaFree(c->d_pos);
     cudaFree(c->d_flags);
+    ws_free(c);
     for (auto &p : c->prof_events) {
         cudaEventDestroy(p.second.first);
         cudaEventDestroy(p.second.second);
@@ -291,7 +243,7 @@ int hpm_set_views(hpm_ctx *c, const float *const *images, const HpmCamera *cams,
     for (int i = 0; i < num_images; ++i) {
         const size_t bytes = sizeof(float) * cams[i].width * cams[i].height;
         CK(ensure((void **)&c->d_img[i], &c->img_cap[i], bytes), "image alloc");
-        CK(cudaMemcpyAsync(c->d_img[i], images[i], bytes, cudaMemcpyHostToDevice, c->stream), "image upload");
+        CK(cudaMemcpyAsync(c->d_img[i], images[i], bytes, cudaMemcpyDefault, c->stream), "image upload");
         CK(ensure_texture(c, i, cams[i].width, cams[i].height), "texture set-up");
         CK(cudaMemcpy2DToArrayAsync(c->arr[i], 0, 0, c->d_img[i], sizeof(float) * cams[i].width,
                                     sizeof(float) * cams[i].width, cams[i].height, cudaMemcpyDeviceToDevice,
@@ -349,7 +301,7 @@ int hpm_set_geom_depths(hpm_ctx *c, const float *const *depths)
         if (!depths[i]) return fail(c, HPM_ERR_ARG, "hpm_set_geom_depths: depth %d is null", i);
         const size_t bytes = sizeof(float) * c->cams[i].width * c->cams[i].height;
         CK(ensure((void **)&c->d_depth[i], &c->depth_cap[i], bytes), "depth alloc");
-        CK(cudaMemcpyAsync(c->d_depth[i], depths[i], bytes, cudaMemcpyHostToDevice, c->stream), "depth upload");
+        CK(cudaMemcpyAsync(c->d_depth[i], depths[i], bytes, cudaMemcpyDefault, c->stream), "depth upload");
     }
     c->has_depth = true;
     CK(cudaStreamSynchronize(c->stream), "hpm_set_geom_depths");
@@ -364,9 +316,9 @@ int hpm_set_hypotheses(hpm_ctx *c, const float *planes, const float *costs)
     int r = select_device(c);
     if (r) return r;
     const size_t n = npx(c);
-    CK(cudaMemcpyAsync(c->d_planes, planes, sizeof(float4) * n, cudaMemcpyHostToDevice, c->stream), "planes");
+    CK(cudaMemcpyAsync(c->d_planes, planes, sizeof(float4) * n, cudaMemcpyDefault, c->stream), "planes");
     if (costs)
-        CK(cudaMemcpyAsync(c->d_costs, costs, sizeof(float) * n, cudaMemcpyHostToDevice, c->stream), "costs");
+        CK(cudaMemcpyAsync(c->d_costs, costs, sizeof(float) * n, cudaMemcpyDefault, c->stream), "costs");
     else
         CK(cudaMemsetAsync(c->d_costs, 0, sizeof(float) * n, c->stream), "costs");
     c->has_state = true;
@@ -382,8 +334,8 @@ int hpm_set_prior(hpm_ctx *c, const float *prior_planes, const uint32_t *masks)
     int r = select_device(c);
     if (r) return r;
     const size_t n = npx(c);
-    CK(cudaMemcpyAsync(c->d_prior, prior_planes, sizeof(float4) * n, cudaMemcpyHostToDevice, c->stream), "prior");
-    CK(cudaMemcpyAsync(c->d_masks, masks, sizeof(uint32_t) * n, cudaMemcpyHostToDevice, c->stream), "masks");
+    CK(cudaMemcpyAsync(c->d_prior, prior_planes, sizeof(float4) * n, cudaMemcpyDefault, c->stream), "prior");
+    CK(cudaMemcpyAsync(c->d_masks, masks, sizeof(uint32_t) * n, cudaMemcpyDefault, c->stream), "masks");
     c->has_prior = true;
     CK(cudaStreamSynchronize(c->stream), "hpm_set_prior");
     return HPM_OK;
@@ -424,7 +376,6 @@ static int run_pass(hpm_ctx *c, const HpmParams *p, int half_steps, int finalize
     a.seed_lo = (uint32_t)p->seed;
     a.seed_hi = (uint32_t)(p->seed >> 32);
     a.salt = c->pass_counter++;
-    if (c->counting) CK(cudaMemsetAsync(c->d_counters, 0, 2 * sizeof(unsigned long long), c->stream), "counters");
     cudaEvent_t e0;
     prof_begin(c, 0, &e0);
     CK(launch_init(a, c->stream), "init kernel");
@@ -667,6 +618,13 @@ int hpm_profile_read(hpm_ctx *c, float *ms4, int *counts4)
 int hpm_count_enable(hpm_ctx *c, int enable)
 {
     if (!c) return HPM_ERR_ARG;
+    /* the counters run from here over every later pass until disabled */
+    if (enable) {
+        int r = select_device(c);
+        if (r) return r;
+        CK(cudaMemsetAsync(c->d_counters, 0, 2 * sizeof(unsigned long long), c->stream), "counters");
+        CK(cudaStreamSynchronize(c->stream), "hpm_count_enable");
+    }
     c->counting = enable != 0;
     return HPM_OK;
 }
@@ -683,3 +641,114 @@ int hpm_count_read(hpm_ctx *c, uint64_t *cv, uint64_t *geom)
 }
 
 }  // extern "C"
+
+/* ---- helpers shared with the pass orchestration (hpm_flow.cu) ---- */
+
+int ctx_fail(hpm_ctx *c, int code, const char *fmt, ...)
+{
+    if (c) {
+        va_list ap;
+        va_start(ap, fmt);
+        vsnprintf(c->err, sizeof(c->err), fmt, ap);
+        va_end(ap);
+    }
+    return code;
+}
+
+int ctx_cuda_fail(hpm_ctx *c, cudaError_t e, const char *what) { return cuda_fail(c, e, what); }
+int ctx_select_device(hpm_ctx *c) { return select_device(c); }
+int ctx_run_pass(hpm_ctx *c, const HpmParams *p, int half_steps, int finalize)
+{
+    return run_pass(c, p, half_steps, finalize, true);
+}
+float *ctx_planes(hpm_ctx *c) { return reinterpret_cast<float *>(c->d_planes); }
+float *ctx_costs(hpm_ctx *c) { return c->d_costs; }
+float *ctx_prior(hpm_ctx *c) { return reinterpret_cast<float *>(c->d_prior); }
+uint32_t *ctx_masks(hpm_ctx *c) { return c->d_masks; }
+const float *ctx_image(hpm_ctx *c, int i) { return c->d_img[i]; }
+void ctx_mark_prior(hpm_ctx *c) { c->has_prior = true; }
+
+template <typename T>
+static cudaError_t grow(T **p, size_t *cap, size_t n)
+{
+    if (*p && *cap >= n) return cudaSuccess;
+    cudaFree(*p);
+    *p = nullptr;
+    *cap = 0;
+    cudaError_t e = cudaMalloc((void **)p, sizeof(T) * (n ? n : 1));
+    if (e == cudaSuccess) *cap = n;
+    return e;
+}
+
+cudaError_t ws_reserve(hpm_ctx *c, size_t npx, size_t nblocks)
+{
+    FlowWorkspace &w = c->flow;
+    if (w.lvl_cap < npx) {
+        size_t a = 0, b = 0, d = 0;
+        cudaError_t e = grow(&w.mask, &a, npx);
+        if (e == cudaSuccess) e = grow(&w.ids, &b, npx);
+        if (e == cudaSuccess) e = grow(&w.knn_planes, &d, npx);
+        if (e != cudaSuccess) return e;
+        w.lvl_cap = npx;
+    }
+    return grow(&w.blocks, &w.blocks_cap, nblocks);
+}
+
+cudaError_t ws_reserve_tris(hpm_ctx *c, size_t ntris)
+{
+    FlowWorkspace &w = c->flow;
+    if (w.tri_cap >= ntris && w.tris) return cudaSuccess;
+    size_t a = 0;
+    cudaError_t e = grow(&w.tris, &a, 6 * ntris);
+    if (e == cudaSuccess) e = grow(&w.tri_planes, &w.tri_cap, ntris);
+    return e;
+}
+
+cudaError_t ws_reserve_grid(hpm_ctx *c, size_t npts, size_t ncells)
+{
+    FlowWorkspace &w = c->flow;
+    if (w.pts_cap < npts || !w.pts) {
+        size_t a = 0;
+        cudaError_t e = grow(&w.pts, &a, npts);
+        if (e == cudaSuccess) e = grow(&w.cell_pts, &w.pts_cap, npts);
+        if (e != cudaSuccess) return e;
+    }
+    return grow(&w.cell_start, &w.cells_cap, ncells);
+}
+
+cudaError_t ws_reserve_full(hpm_ctx *c, size_t npx)
+{
+    FlowWorkspace &w = c->flow;
+    if (w.full_cap >= npx && w.full_depth) return cudaSuccess;
+    size_t a = 0, b = 0, d = 0, f = 0;
+    cudaError_t e = grow(&w.full_depth, &a, npx);
+    if (e == cudaSuccess) e = grow(&w.full_normal, &b, 3 * npx);
+    if (e == cudaSuccess) e = grow(&w.prior_depth, &d, npx);
+    if (e == cudaSuccess) e = grow(&w.up_depth, &f, npx);
+    if (e == cudaSuccess) e = grow(&w.up_normal, &w.full_cap, npx);
+    return e;
+}
+
+cudaError_t ws_reserve_coarse(hpm_ctx *c, size_t npx)
+{
+    FlowWorkspace &w = c->flow;
+    if (w.coarse_cap >= npx && w.c_depth) return cudaSuccess;
+    size_t a = 0, b = 0, d = 0, f = 0, g = 0;
+    cudaError_t e = grow(&w.c_depth, &a, npx);
+    if (e == cudaSuccess) e = grow(&w.c_cost, &b, npx);
+    if (e == cudaSuccess) e = grow(&w.c_normal, &d, 3 * npx);
+    if (e == cudaSuccess) e = grow(&w.c_prior_depth, &f, npx);
+    if (e == cudaSuccess) e = grow(&w.c_prior_normal, &g, 3 * npx);
+    if (e == cudaSuccess) e = grow(&w.c_packed, &w.coarse_cap, npx);
+    return e;
+}
+
+void ws_free(hpm_ctx *c)
+{
+    FlowWorkspace &w = c->flow;
+    void *ptrs[] = {w.full_depth, w.full_normal, w.prior_depth, w.up_depth, w.up_normal, w.mask, w.ids,
+                    w.knn_planes, w.blocks, w.c_depth, w.c_cost, w.c_normal, w.c_prior_depth, w.c_prior_normal,
+                    w.c_packed, w.tris, w.tri_planes, w.pts, w.cell_start, w.cell_pts};
+    for (void *p : ptrs) cudaFree(p);
+    w = FlowWorkspace();
+}

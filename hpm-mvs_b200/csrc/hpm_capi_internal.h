@@ -1,0 +1,113 @@
+/*
+ * The context behind the C ABI (hpm_ctx) and the helpers the pass
+ * orchestration (hpm_flow.cu) shares with hpm_capi.cu.
+ */
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <utility>
+#include <vector>
+
+#include "hpm_internal.h"
+
+namespace hpm {
+
+/* Device workspace of the planar-prior stages, grown on demand and reused
+ * by every problem of a context. */
+struct FlowWorkspace {
+    float *full_depth = nullptr, *full_normal = nullptr, *prior_depth = nullptr, *up_depth = nullptr;
+    float4 *up_normal = nullptr;
+    size_t full_cap = 0;
+    float *mask = nullptr;
+    int *ids = nullptr;
+    float4 *knn_planes = nullptr;
+    size_t lvl_cap = 0;
+    int2 *blocks = nullptr;
+    size_t blocks_cap = 0;
+    float *c_depth = nullptr, *c_cost = nullptr, *c_normal = nullptr, *c_prior_depth = nullptr,
+          *c_prior_normal = nullptr;
+    float4 *c_packed = nullptr;
+    size_t coarse_cap = 0;
+    int *tris = nullptr;
+    float4 *tri_planes = nullptr;
+    size_t tri_cap = 0;
+    int2 *pts = nullptr;
+    int *cell_start = nullptr, *cell_pts = nullptr;
+    size_t pts_cap = 0, cells_cap = 0;
+    bool has_prior_depth = false;
+    int last_points = 0, last_triangles = 0;
+};
+
+}  // namespace hpm
+
+struct hpm_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    char err[512] = {0};
+
+    int n = 0;
+    HpmCamera cams[hpm::kMaxViews];
+    float *d_img[hpm::kMaxViews] = {nullptr};
+    size_t img_cap[hpm::kMaxViews] = {0};
+    cudaArray_t arr[hpm::kMaxViews] = {nullptr};
+    int arr_w[hpm::kMaxViews] = {0}, arr_h[hpm::kMaxViews] = {0};
+    cudaTextureObject_t tex[hpm::kMaxViews] = {0};
+    float *d_depth[hpm::kMaxViews] = {nullptr};
+    size_t depth_cap[hpm::kMaxViews] = {0};
+    bool has_depth = false;
+    hpm::PairGeom *d_pair = nullptr;
+
+    float4 *d_planes = nullptr;
+    float *d_costs = nullptr;
+    uint32_t *d_views = nullptr;
+    float4 *d_prior = nullptr;
+    uint32_t *d_masks = nullptr;
+    size_t px_cap = 0;
+    bool has_prior = false;
+    bool has_state = false;
+
+    unsigned long long *d_counters = nullptr;
+    bool counting = false;
+
+    bool profiling = false;
+    std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> prof_events;
+    float prof_ms[4] = {0, 0, 0, 0};
+    int prof_cnt[4] = {0, 0, 0, 0};
+
+    uint32_t pass_counter = 0;
+
+    void *d_scratch = nullptr;
+    size_t scratch_cap = 0;
+
+    float *d_cache = nullptr; /* cost vector of each pixel's current hypothesis, [S][H*W] */
+    size_t cache_cap = 0;
+    float *d_cand = nullptr; /* half-step hand-off: cost matrix rows [kCandRows*S][H*W] */
+    size_t cand_cap = 0;
+    int *d_pos = nullptr; /* chosen NESP sites [8][H*W] */
+    size_t pos_cap = 0;
+    uint32_t *d_flags = nullptr; /* valid-direction bits [H*W] */
+    size_t flags_cap = 0;
+
+    hpm::FlowWorkspace flow;
+};
+
+int ctx_fail(hpm_ctx *c, int code, const char *fmt, ...);
+int ctx_cuda_fail(hpm_ctx *c, cudaError_t e, const char *what);
+int ctx_select_device(hpm_ctx *c);
+/* one pass: init, `half_steps` red/black half-steps, optional finalisation;
+ * synchronises the context's stream at the end */
+int ctx_run_pass(hpm_ctx *c, const HpmParams *p, int half_steps, int finalize);
+float *ctx_planes(hpm_ctx *c);
+float *ctx_costs(hpm_ctx *c);
+float *ctx_prior(hpm_ctx *c);
+uint32_t *ctx_masks(hpm_ctx *c);
+const float *ctx_image(hpm_ctx *c, int i);
+void ctx_mark_prior(hpm_ctx *c);
+cudaError_t ws_reserve(hpm_ctx *c, size_t npx, size_t nblocks);
+cudaError_t ws_reserve_tris(hpm_ctx *c, size_t ntris);
+cudaError_t ws_reserve_grid(hpm_ctx *c, size_t npts, size_t ncells);
+cudaError_t ws_reserve_full(hpm_ctx *c, size_t npx);
+cudaError_t ws_reserve_coarse(hpm_ctx *c, size_t npx);
+void ws_free(hpm_ctx *c);

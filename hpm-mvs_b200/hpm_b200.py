@@ -36,8 +36,30 @@ EXPORTED = [
     "hpm_get_selected_views", "hpm_device_state", "hpm_stream", "hpm_jbu", "hpm_cost_vectors",
     "hpm_initial_costs", "hpm_geom_costs", "hpm_depth_normal_filter", "hpm_profile_enable", "hpm_profile_read",
     "hpm_count_enable", "hpm_count_read", "hpm_write_dmb", "hpm_read_dmb", "hpm_read_camera", "hpm_read_pair",
-    "hpm_fp32_peak", "hpm_jbu_noalloc",
+    "hpm_fp32_peak", "hpm_jbu_noalloc", "hpm_process_problem", "hpm_last_prior_stats", "hpm_delaunay",
+    "hpm_prior_level", "hpm_run_scene",
 ]
+
+
+class HpmSceneOpts(ctypes.Structure):
+    _fields_ = [("planar_prior", ctypes.c_int), ("geom_iterations", ctypes.c_int), ("seed", ctypes.c_uint64),
+                ("pyramid_levels", ctypes.c_int)]
+
+
+class HpmProblemOpts(ctypes.Structure):
+    _fields_ = [("planar_prior", ctypes.c_int), ("geom_consistency", ctypes.c_int), ("multi_geometry", ctypes.c_int),
+                ("seed", ctypes.c_uint64), ("pyramid_levels", ctypes.c_int)]
+
+
+def delaunay(points: np.ndarray, w: int, h: int) -> np.ndarray:
+    """Triangles (n, 6) of the prior triangulation of integer points (n, 2)."""
+    pts = np.ascontiguousarray(points, dtype=np.int32).reshape(-1, 2)
+    n = lib().hpm_delaunay(_p(pts), len(pts), w, h, None, 0)
+    if n < 0:
+        raise HpmError(f"hpm_delaunay: {STATUS_NAMES.get(n, n)}")
+    out = np.zeros((max(n, 1), 6), np.int32)
+    n2 = lib().hpm_delaunay(_p(pts), len(pts), w, h, _p(out), len(out))
+    return out[:n2]
 
 
 def fp32_peak(device: int = 0) -> float:
@@ -172,6 +194,72 @@ class Context:
     def run_partial(self, params: HpmParams, half_steps: int, finalize: bool) -> None:
         self._check(lib().hpm_run_partial(self._h, ctypes.byref(params), int(half_steps), int(finalize)),
                     "hpm_run_partial")
+
+    def process_problem(self, *, planar_prior=True, geom=False, multi_geometry=False, seed=0, pyramid_levels=-1):
+        """ProcessProblem for the current views: returns (depth, normal, cost, prior_depth)."""
+        h, w = self.shape
+        depth = np.empty((h, w), np.float32)
+        normal = np.empty((h, w, 3), np.float32)
+        cost = np.empty((h, w), np.float32)
+        prior = np.empty((h, w), np.float32)
+        o = HpmProblemOpts(int(planar_prior), int(geom), int(multi_geometry), int(seed), int(pyramid_levels))
+        self._check(lib().hpm_process_problem(self._h, ctypes.byref(o), _p(depth), _p(normal), _p(cost), _p(prior)),
+                    "hpm_process_problem")
+        return depth, normal, cost, prior
+
+    def run_scene(self, images, cams, pairs, *, planar_prior=True, geom_iterations=2, seed=0, pyramid_levels=-1,
+                  images_are_device=False, outputs=True):
+        """The reference's main() over a scene.  images: per-view float32 [H, W]
+        arrays, or device pointers (ints) with images_are_device; pairs:
+        [(ref, [sources])].  Returns per-view (depth, normal, cost) lists when
+        outputs is true."""
+        n = len(cams)
+        cams = np.ascontiguousarray(cams, dtype=CAMERA_DTYPE)
+        if images_are_device:
+            ptrs = [int(p) for p in images]
+            keep = None
+        else:
+            keep = [np.ascontiguousarray(i, dtype=np.float32) for i in images]
+            ptrs = [k.ctypes.data for k in keep]
+        img_arr = (ctypes.c_void_p * n)(*ptrs)
+        refs = np.array([p[0] for p in pairs], np.int32)
+        counts = np.array([len(p[1]) for p in pairs], np.int32)
+        srcs = np.zeros((len(pairs), MAX_IMAGES - 1), np.int32)
+        for i, (_, s) in enumerate(pairs):
+            srcs[i, :len(s)] = s
+        o = HpmSceneOpts(int(planar_prior), int(geom_iterations), int(seed), int(pyramid_levels))
+        outs = None
+        if outputs:
+            outs = [(np.empty((int(c["height"]), int(c["width"])), np.float32),
+                     np.empty((int(c["height"]), int(c["width"]), 3), np.float32),
+                     np.empty((int(c["height"]), int(c["width"])), np.float32)) for c in cams]
+            arrs = [(ctypes.c_void_p * n)(*[o_[k].ctypes.data for o_ in outs]) for k in range(3)]
+        else:
+            arrs = [None, None, None]
+        self._check(lib().hpm_run_scene(self._h, n, img_arr, _p(cams), len(pairs), _p(refs), _p(counts), _p(srcs),
+                                        ctypes.byref(o), arrs[0], arrs[1], arrs[2]), "hpm_run_scene")
+        del keep
+        if outputs:
+            return [o_[0] for o_ in outs], [o_[1] for o_ in outs], [o_[2] for o_ in outs]
+        return None
+
+    def prior_level(self, level, depth, normal, cost):
+        """Prior of one pyramid level from given maps: (planes, masks, prior_depth)."""
+        h, w = self.shape
+        d = np.ascontiguousarray(depth, np.float32)
+        n = np.ascontiguousarray(normal, np.float32)
+        c = np.ascontiguousarray(cost, np.float32)
+        planes = np.empty((h, w, 4), np.float32)
+        masks = np.empty((h, w), np.uint32)
+        pd = np.empty((h, w), np.float32)
+        self._check(lib().hpm_prior_level(self._h, int(level), _p(d), _p(n), _p(c), _p(planes), _p(masks), _p(pd)),
+                    "hpm_prior_level")
+        return planes, masks, pd
+
+    def prior_stats(self):
+        a, b = ctypes.c_int(), ctypes.c_int()
+        self._check(lib().hpm_last_prior_stats(self._h, ctypes.byref(a), ctypes.byref(b)), "hpm_last_prior_stats")
+        return a.value, b.value
 
     def get_result(self):
         h, w = self.shape

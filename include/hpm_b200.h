@@ -124,6 +124,63 @@ int hpm_run_patchmatch(hpm_ctx *ctx, const HpmParams *params);
  * pass of a problem (counting from hpm_set_views) draws from stream k. */
 int hpm_run_partial(hpm_ctx *ctx, const HpmParams *params, int half_steps, int finalize);
 
+/* Options of one ProcessProblem call. */
+typedef struct {
+    int planar_prior;     /* pass set A: plain pass, then the planar-prior pyramid */
+    int geom_consistency; /* pass set B: one geometric-consistency pass */
+    int multi_geometry;   /* second geometric iteration (reads depths_geom) */
+    uint64_t seed;        /* Philox key of the passes of this problem */
+    int pyramid_levels;   /* coarse prior levels; -1 = ComputingMultiScaleSettings
+                             (HPM.cpp:851-860: halvings until max side <= 1000) */
+} HpmProblemOpts;
+
+/* One reference view through ProcessProblem (main.cpp:35-499) on the
+ * device: with planar_prior, the plain pass, then for each pyramid level
+ * (ComputingMultiScaleSettings, HPM.cpp:851-860) support points, Delaunay
+ * triangles, triangle planes and raster, the KNN supplement, (coarse levels)
+ * joint bilateral upsampling, and a PatchMatch pass with the prior; with
+ * geom_consistency, one geometric pass over the state and depth maps set by
+ * hpm_set_hypotheses / hpm_set_geom_depths.  The depth range is the
+ * reference camera's, widened x0.6 / x1.2 (HPM.cpp:553-554).  Outputs (any
+ * may be NULL): depth and cost maps, world normals (3 floats per pixel), and
+ * the full-scale prior depth map written to depths_prior.dmb by the
+ * reference (zeros when no prior ran). */
+int hpm_process_problem(hpm_ctx *ctx, const HpmProblemOpts *opts, float *depth, float *normal, float *cost,
+                        float *prior_depth);
+/* Options of a whole-scene run. */
+typedef struct {
+    int planar_prior;    /* pass set A with the planar-prior pyramid (the reference's default: 1) */
+    int geom_iterations; /* geometric iterations of pass set B (the reference's default: 2) */
+    uint64_t seed;
+    int pyramid_levels; /* -1 = the reference's rule */
+} HpmSceneOpts;
+
+/* The reference's main() (main.cpp:636-677) over a scene: ProcessProblem
+ * with the planar prior for every problem of pair.txt, then
+ * geom_iterations geometric passes over every problem, the first reading
+ * pass set A's depth maps, the later ones the geometric depth maps as they
+ * are being updated (the reference rewrites depths_geom.dmb view by view).
+ * All maps stay in HBM; the host only triangulates support points.
+ * images[v] / cams[v] describe view v (host or device pointers); problem p
+ * has reference ref_ids[p] and src_counts[p] sources
+ * src_ids[p * (HPM_MAX_IMAGES-1) + j].  Per-view outputs (arrays of
+ * n_views pointers, any may be NULL, host or device): final depth, world
+ * normal (3 floats/pixel), cost. */
+int hpm_run_scene(hpm_ctx *ctx, int n_views, const float *const *images, const HpmCamera *cams, int n_problems,
+                  const int *ref_ids, const int *src_counts, const int *src_ids, const HpmSceneOpts *opts,
+                  float *const *depths, float *const *normals, float *const *costs);
+
+/* Parity entry point: the prior of one pyramid level (0: 1/4 scale, 1: 1/2
+ * scale, 2: full scale) built from given full-resolution maps of the current
+ * reference view (depth, world normal 3 floats/pixel, cost) exactly as
+ * hpm_process_problem builds it after a pass.  Outputs (any may be NULL):
+ * ref-frame prior planes (4 floats/pixel) and masks of the next pass, and at
+ * full scale the prior depth map (zeros at coarse levels). */
+int hpm_prior_level(hpm_ctx *ctx, int level, const float *depth, const float *normal, const float *cost,
+                    float *prior_planes, uint32_t *masks, float *prior_depth);
+/* Support points and kept triangles of the last prior level built. */
+int hpm_last_prior_stats(hpm_ctx *ctx, int *points, int *triangles);
+
 /* Copies the pass result to the host: planes = (world normal, depth),
  * costs.  Either pointer may be NULL.  Replaces the D2H copies of
  * HPM.cu:1954-1955 and GetPlaneHypothesis / GetCost (HPM.cpp:739-747). */
@@ -171,6 +228,13 @@ int hpm_jbu_noalloc(int device, const float *guide, int cols, int rows, const fl
 
 /* Deterministic building blocks exposed for parity checks. */
 
+/* Delaunay triangulation of n integer points (xy pairs) used for the planar
+ * prior (replaces cv::Subdiv2D in DelaunayTriangulation, HPM.cpp:787-809,
+ * plus the inside-image filter of main.cpp:97).  Writes up to cap triangles
+ * (6 ints each) when tris is non-NULL; returns the triangle count or a
+ * negative status. */
+int hpm_delaunay(const int *xy, int n, int w, int h, int *tris, int cap);
+
 /* ComputeMultiViewCostVector (HPM.cu:438-443) for one ref-frame plane per
  * pixel of the current problem; out holds (num_images-1) floats per pixel. */
 int hpm_cost_vectors(hpm_ctx *ctx, const float *planes, float *out);
@@ -188,8 +252,10 @@ int hpm_profile_enable(hpm_ctx *ctx, int enable);
 /* kernel times in ms accumulated since enable: [init, propagate, finalize,
  * jbu]; counts = launches of each.  Either pointer may be NULL. */
 int hpm_profile_read(hpm_ctx *ctx, float *ms4, int *counts4);
-/* Number of cost-vector evaluations made by the last pass (one evaluation =
- * num_images-1 NCC windows); requires hpm_count_enable(ctx, 1) before it. */
+/* Work counters: cost-vector evaluations (one evaluation = num_images-1 NCC
+ * windows) and geometric-consistency terms, summed over every pass run since
+ * hpm_count_enable(ctx, 1), which zeroes them.  Diagnostic; no reference
+ * counterpart. */
 int hpm_count_enable(hpm_ctx *ctx, int enable);
 int hpm_count_read(hpm_ctx *ctx, uint64_t *cost_vectors, uint64_t *geom_terms);
 

@@ -1,0 +1,173 @@
+"""ProcessProblem on the GPU (hpm_process_problem) against the oracle's
+restatement of the reference flow (oracle/flow.py: oracle kernels + the
+reference's OpenCV calls), and the flow's effect at the reference's
+pyramid rule."""
+import numpy as np
+import pytest
+
+import flow as oflow
+import hpm_b200 as hb
+import synthetic as syn
+
+pytestmark = pytest.mark.gpu
+
+
+def _scene(seed, w, h, nv, **kw):
+    sc = syn.make_scene(seed, w, h, nv, **kw)
+    imgs, cams = syn.view_set(sc, nv // 2)
+    return sc, imgs, cams
+
+
+@pytest.mark.parametrize("levels", [0, 1])
+def test_flow_matches_oracle_flow(levels):
+    sc, imgs, cams = _scene(12, 160, 120, 5, n_planes=6, low_texture=0.4)
+    gt = sc.gt_depth[2]
+    with hb.Context() as ctx:
+        ctx.set_views(imgs, cams)
+        gd, gn, gc, gpd = ctx.process_problem(seed=3, pyramid_levels=levels)
+        n_pts, n_tri = ctx.prior_stats()
+    od, on, oc, opd = oflow.process_problem(imgs, cams, seed=3, pyramid_levels=levels)
+    assert n_pts > 50 and n_tri > 50
+    # the prior is built from a stochastic pass, so compare statistics: the
+    # full-scale prior depth map (depths_prior.dmb) covers as much, and the
+    # final %px agrees
+    cov_g, cov_o = (gpd > 0).mean(), (opd > 0).mean()
+    assert abs(cov_g - cov_o) <= 0.03, (cov_g, cov_o)
+    ag, ao = syn.depth_accuracy(gd, gt), syn.depth_accuracy(od, gt)
+    assert abs(ag - ao) <= 0.03, (ag, ao)
+
+
+def _prior_inputs(seed, w, h):
+    """Depth/normal/cost maps of a view as a pass would leave them: true
+    geometry with 1% depth noise, costs below 0.1 on 40% of the pixels."""
+    sc, imgs, cams = _scene(seed, w, h, 3, n_planes=6, n_spheres=2)
+    rng = np.random.default_rng(seed)
+    depth = (sc.gt_depth[1] * rng.uniform(0.99, 1.01, (h, w))).astype(np.float32)
+    normal = sc.gt_normal[1].astype(np.float32)
+    cost = np.where(rng.random((h, w)) < 0.4, rng.uniform(0, 0.1, (h, w)), rng.uniform(0.1, 2.0, (h, w)))
+    return imgs, cams, depth, normal, cost.astype(np.float32)
+
+
+@pytest.mark.parametrize("level", [2, 1, 0])
+def test_prior_level_matches_oracle(level):
+    """hpm_prior_level against the oracle's restatement of the same level on
+    identical inputs.  With the product's own triangulation handed to the
+    oracle the stages after the Delaunay must agree pixel for pixel (up to FP32
+    evaluation order); with OpenCV's Subdiv2D (same triangles, listed in
+    another order) they differ only on pixels of shared triangle edges."""
+    imgs, cams, depth, normal, cost = _prior_inputs(20 + level, 320, 240)
+    cam = cams[0]
+    dmin, dmax = cam["depth_min"] * np.float32(0.6), cam["depth_max"] * np.float32(1.2)
+    with hb.Context() as ctx:
+        ctx.set_views(imgs, cams)
+        gp, gm, gd = ctx.prior_level(level, depth, normal, cost)
+    # 1) the product's triangulation handed to the oracle: every later stage
+    #    agrees pixel for pixel
+    op, om, od = oflow.prior_level(cam, level, depth, normal, cost, imgs[0], dmin, dmax, triangles=hb.delaunay)
+    same = (gm != 0) == (om != 0)
+    assert same.mean() >= 0.995, same.mean()
+    both = (gm != 0) & (om != 0)
+    close = np.isclose(gp[both], op[both], rtol=1e-3, atol=1e-4).all(-1)
+    assert close.mean() >= 0.995, close.mean()
+    if level == 2:
+        np.testing.assert_allclose(gd[both][close], od[both][close], rtol=1e-4)
+    assert (gm != 0).mean() > 0.5
+    # 2) OpenCV's Subdiv2D (the reference's call) lists the same triangles in
+    #    another order, and the order decides which triangle owns a pixel on a
+    #    shared edge (the later one).  With 1% depth noise, neighbouring
+    #    triangle planes part by about 1%, so compare the depth each prior plane
+    #    implies at its pixel; the coarser the level, the larger the share of
+    #    edge pixels, and the JBU spreads each over its 11x11 window
+    op, om, od = oflow.prior_level(cam, level, depth, normal, cost, imgs[0], dmin, dmax)
+    K = cam["K"].reshape(3, 3)
+    ys, xs = np.mgrid[0:240, 0:320].astype(np.float64)
+
+    def implied(p):
+        den = (xs - K[0, 2]) * p[..., 0] + (K[0, 0] / K[1, 1]) * (ys - K[1, 2]) * p[..., 1] + K[0, 0] * p[..., 2]
+        return -p[..., 3] * K[0, 0] / np.where(den == 0, 1e-12, den)
+
+    both = (gm != 0) & (om != 0)
+    assert both.mean() >= 0.97 * max((gm != 0).mean(), (om != 0).mean())
+    rel = np.abs(implied(gp) - implied(op))[both] / np.abs(implied(op))[both]
+    assert (rel < 0.01).mean() >= {2: 0.97, 1: 0.93, 0: 0.88}[level], (rel < 0.01).mean()
+    assert np.median(rel) < 1e-3, np.median(rel)
+
+
+def test_prior_improves_low_texture_scene():
+    """At the reference's pyramid rule (one coarse level for 1040x780), the
+    prior passes raise %px over the plain pass on a 40%-low-texture scene."""
+    sc, imgs, cams = _scene(13, 1040, 780, 5, n_planes=10, n_spheres=3, low_texture=0.4)
+    gt = sc.gt_depth[2]
+    with hb.Context() as ctx:
+        ctx.set_views(imgs, cams)
+        d0, _, _, _ = ctx.process_problem(seed=1, planar_prior=False)
+        ctx.set_views(imgs, cams)
+        d1, n1, c1, pd = ctx.process_problem(seed=1, planar_prior=True)
+    a0, a1 = syn.depth_accuracy(d0, gt), syn.depth_accuracy(d1, gt)
+    assert (pd > 0).mean() > 0.5
+    assert a1 > a0 + 0.01, (a0, a1)
+    assert np.isfinite(n1).all()
+
+
+def test_geometric_pass_through_the_flow():
+    """Pass set B: depth maps of every view from pass set A, then one
+    geometric pass on the reference view (main.cpp:662-674)."""
+    sc = syn.make_scene(14, 240, 180, 5, n_planes=6)
+    depths, normals, costs = [], [], []
+    with hb.Context() as ctx:
+        for ref in range(5):
+            imgs, cams = syn.view_set(sc, ref)
+            ctx.set_views(imgs, cams)
+            d, n, c, _ = ctx.process_problem(seed=ref, planar_prior=True, pyramid_levels=0)
+            depths.append(d)
+            normals.append(n)
+            costs.append(c)
+        ref = 2
+        imgs, cams = syn.view_set(sc, ref)
+        ids = [ref] + list(sc.pairs[ref][1])
+        ctx.set_views(imgs, cams)
+        ctx.set_geom_depths([depths[i] for i in ids])
+        ctx.set_hypotheses(np.concatenate([normals[ref], depths[ref][..., None]], -1), costs[ref])
+        dg, ng, cg, _ = ctx.process_problem(seed=9, geom=True)
+    gt = sc.gt_depth[ref]
+    a_a, a_b = syn.depth_accuracy(depths[ref], gt), syn.depth_accuracy(dg, gt)
+    assert a_b >= a_a - 0.01, (a_a, a_b)
+
+
+def test_scene_driver_matches_per_view_loop():
+    """hpm_run_scene (main.cpp:636-677 in one call, maps resident on the
+    device) produces exactly what the per-view loop over hpm_process_problem
+    produces with the same seeds: pass set A for every view, then two
+    geometric iterations, the second reading the geometric maps in place."""
+    nv, seed = 5, 5
+    sc = syn.make_scene(15, 160, 120, nv, n_planes=6, low_texture=0.3)
+    imgs_all = [sc.images[v].astype(np.float32) for v in range(nv)]
+    cams_all = sc.cams
+    pairs = [(v, list(sc.pairs[v][1])) for v in range(nv)]
+    with hb.Context() as ctx:
+        sd, sn, scost = ctx.run_scene(imgs_all, cams_all, pairs, planar_prior=True, geom_iterations=2, seed=seed,
+                                      pyramid_levels=0)
+    depth_a, normal, cost = {}, {}, {}
+    with hb.Context() as ctx:
+        for p, (ref, srcs) in enumerate(pairs):
+            ids = [ref] + srcs
+            ctx.set_views([imgs_all[i] for i in ids], cams_all[ids])
+            d, n, c, _ = ctx.process_problem(seed=seed + p, planar_prior=True, pyramid_levels=0)
+            depth_a[ref], normal[ref], cost[ref] = d, n, c
+        depth_g = dict(depth_a)
+        for gi in range(2):
+            src = depth_a if gi == 0 else depth_g
+            for p, (ref, srcs) in enumerate(pairs):
+                ids = [ref] + srcs
+                ctx.set_views([imgs_all[i] for i in ids], cams_all[ids])
+                ctx.set_geom_depths([src[i] for i in ids])
+                ctx.set_hypotheses(np.concatenate([normal[ref], src[ref][..., None]], -1), cost[ref])
+                d, n, c, _ = ctx.process_problem(seed=seed + 1000003 * (gi + 1) + p, geom=True,
+                                                 multi_geometry=gi >= 1)
+                depth_g[ref], normal[ref], cost[ref] = d, n, c
+    for v in range(nv):
+        np.testing.assert_array_equal(sd[v], depth_g[v])
+        np.testing.assert_array_equal(sn[v], normal[v])
+        np.testing.assert_array_equal(scost[v], cost[v])
+    accs = [syn.depth_accuracy(sd[v], sc.gt_depth[v]) for v in range(nv)]
+    assert min(accs) > 0.5, accs
