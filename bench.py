@@ -1,24 +1,32 @@
 #!/usr/bin/env python
-"""Benchmark of the B200-native HPM-MVS PatchMatch path.
+"""Benchmark of the B200-native HPM-MVS depth estimation path.
 
-One JSON line on rank 0.  A *step* is the depth estimation of one reference
-view of the workload below through the product's C ABI.  Metric: depth
-Mpix/s (reference-view pixels at processed resolution per second).
+One JSON line on rank 0.  A *step* is the reference's main() over one scene
+(main.cpp:636-677): pass set A (ProcessProblem with the planar + KNN prior on
+every pyramid level) for every view, then the geometric-consistency
+iterations for every view.  Metric: depth Mpix/s = depth-map pixels of all
+views at processed resolution per second.
 
-  value   steps with the views already resident in HBM (hpm_run_patchmatch)
-  e2e     the same steps through the public API from pinned host memory:
-          hpm_set_views (H2D) + hpm_run_patchmatch + hpm_get_result (D2H)
+  value   steps with the images already resident in HBM (hpm_run_scene on
+          device pointers, the depth/normal/cost maps stay on the device)
+  e2e     the same steps through the public C ABI from pinned host memory:
+          images in, every view's depth, normal and cost maps out
   roofline  the dominant kernel pair (one red/black half-step: site/direction
           kernel + selection/refinement kernel) against the measured FP32 FMA
-          peak; algorithmic FLOPs = NCC taps x 34 + 80 per (hypothesis, view)
+          peak; algorithmic FLOPs = NCC taps x 34 + 80 per (hypothesis,
+          source view), + 120 per geometric-consistency term
   cpu_baseline  the CPU oracle (C restatement of the reference, OpenMP over
-          all host cores) on a bounded sample with the same per-pixel work
+          all host cores) on one view of the same scene recipe at 320x240
 
---impl reference times the reference's own HPM.cu (oracle/_ref: compiled
-unchanged for sm_100a) through its HPM::RunPatchMatch on the same workload.
+--impl reference times the reference's own HPM.cu kernels (oracle/_ref:
+compiled unchanged for sm_100a) through HPM::RunPatchMatch and
+JBU::CudaRun, with the host stages (support points, Delaunay via OpenCV,
+triangle raster, KNN prior, prior assembly) restated in C, on a bounded
+sample of the same scene: one view per step.
 
-Multi-GPU (torchrun): reference views shard over ranks with no data-path
-collective (weak scaling); the elapsed time is the max over ranks.
+Multi-GPU (torchrun): every rank processes its own scene (independent
+objects, no data-path collective; weak scaling); the elapsed time is the max
+over ranks.
 """
 from __future__ import annotations
 
@@ -37,23 +45,40 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path[:0] = [os.path.join(ROOT, "hpm-mvs_b200")]
 
 METRIC = "depth Mpix/s, plain vs batched prior-net form on 1 B200, at equal %px relerr<1%"
-WORKLOAD = dict(name="plain HPM PatchMatch pass, 1600x1200, 10 sources", width=1600, height=1200, n_views=11,
-                n_planes=20, n_spheres=5, low_texture=0.40)
+WORKLOAD = dict(width=1600, height=1200, n_views=11, n_planes=20, n_spheres=5, low_texture=0.40, pyramid_levels=2,
+                geom_iterations=2)
+
+# per-launch DRAM traffic of the half-step kernel pair, from the ncu capture
+# summarised in profiles/prop_kernels_1280x960_s10.md (1280x960, 10 sources),
+# scaled by pixels; the hand-off buffers grow with the pixel count
+TRAFFIC_BYTES_PER_PX_HALF_STEP = (596.144128 + 729.246720 + 944.850944 + 284.436992) * 1e6 / (1280 * 960)
+GEOM_TERM_FLOPS = 120  # two projections (world point + camera, 3x3 each) and the reprojection distance
+TAPS, NCC_FLOPS_PER_TAP, FLOPS_PER_HYP_VIEW = 36, 34, 80
+
+
+def workload_name():
+    w = WORKLOAD
+    return (f"full plain HPM scene: {w['n_views']} views of {w['width']}x{w['height']}, "
+            f"{w['n_views'] - 1} sources each, planar+KNN prior on a {w['pyramid_levels'] + 1}-level pyramid, "
+            f"{w['geom_iterations']} geometric iterations")
 
 
 def parse_args():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--size", default=None,
                     help="WxH override of the workload's resolution (profiling captures use a smaller case)")
+    ap.add_argument("--views", type=int, default=None, help="override of the scene's view count")
     args = ap.parse_args()
     if args.size:
         w, h = (int(x) for x in args.size.lower().split("x"))
-        WORKLOAD.update(width=w, height=h, name=f"plain HPM PatchMatch pass, {w}x{h}, 10 sources")
+        WORKLOAD.update(width=w, height=h)
+    if args.views:
+        WORKLOAD.update(n_views=args.views)
     return args
 
 
@@ -66,7 +91,7 @@ class Dist:
         if self.world > 1:
             import torch.distributed as dist
 
-            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
                                     device_id=__import__("torch").device("cuda", self.local))
             self.pg = True
 
@@ -131,64 +156,121 @@ class Clocks:
                 "reasons": reasons, "samples": len(rows)}
 
 
-def make_workload(seed):
+def make_scene(seed, width=None, height=None):
     import synthetic as syn
 
     w = WORKLOAD
-    sc = syn.make_scene(seed, w["width"], w["height"], w["n_views"], n_planes=w["n_planes"],
+    sc = syn.make_scene(seed, width or w["width"], height or w["height"], w["n_views"], n_planes=w["n_planes"],
                         n_spheres=w["n_spheres"], low_texture=w["low_texture"])
-    ref = w["n_views"] // 2
-    imgs, cams = syn.view_set(sc, ref)
-    return sc, ref, imgs, cams, sc.depth_min * 0.6, sc.depth_max * 1.2
+    images = [i.astype(np.float32) for i in sc.images]
+    pairs = [(v, list(sc.pairs[v][1])) for v in range(w["n_views"])]
+    return sc, images, pairs
+
+
+def passes_per_view():
+    w = WORKLOAD
+    return 1 + (w["pyramid_levels"] + 1) + w["geom_iterations"]
+
+
+def scene_accuracy(sc, depths, normals=None):
+    import synthetic as syn
+
+    per_view = {int(v): float(syn.depth_accuracy(d, sc.gt_depth[v])) for v, d in sorted(depths.items())}
+    out = {"px_relerr_lt_1pct": float(np.mean(list(per_view.values()))), "views": len(depths),
+           "per_view": per_view}
+    if normals is not None:
+        out["median_normal_err_deg"] = float(np.median(
+            [syn.normal_error_deg(normals[v], sc.gt_normal[v], sc.gt_depth[v]) for v in normals]))
+    return out
+
+
+def count_launches(fn):
+    """Kernels launched by fn(), from the CUDA activity trace (CUPTI)."""
+    import torch
+    from torch.profiler import ProfilerActivity, profile
+
+    with profile(activities=[ProfilerActivity.CUDA]) as prof:
+        fn()
+        torch.cuda.synchronize()
+    counts = {}
+    for e in prof.key_averages():
+        if e.device_type.name != "CUDA" or e.key.startswith(("Memcpy", "Memset")):
+            continue
+        counts[e.key] = counts.get(e.key, 0) + e.count
+    return counts
+
+
+def short_kernel_name(k):
+    k = k.replace("void ", "").replace("(anonymous namespace)::", "").split("(")[0]
+    return k.split("::")[-1] if "::" in k else k
 
 
 def cpu_baseline():
-    """Oracle on all host cores over a 320x240 crop of the workload's scene
-    geometry with the same number of source views (same per-pixel work)."""
+    """Oracle on all host cores: one view of a 320x240 scene of the same
+    recipe through the whole per-view flow (pass set A with the prior on
+    every level, then the geometric passes)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import oracle as orc
-    import synthetic as syn
+    import flow as oflow
 
     cores = os.cpu_count() or 1
     os.environ.setdefault("OMP_NUM_THREADS", str(cores))
-    w = WORKLOAD
-    sc = syn.make_scene(0, 320, 240, w["n_views"], n_planes=w["n_planes"], n_spheres=w["n_spheres"],
-                        low_texture=w["low_texture"])
-    imgs, cams = syn.view_set(sc, w["n_views"] // 2)
+    sc, images, pairs = make_scene(0, 320, 240)
+    ref = WORKLOAD["n_views"] // 2
+    ids = [ref] + pairs[ref][1]
+    imgs, cams = [images[i] for i in ids], sc.cams[ids]
     t0 = time.perf_counter()
-    orc.run_patchmatch(imgs, cams, depth_min=sc.depth_min * 0.6, depth_max=sc.depth_max * 1.2, seed=1)
+    d, n, c, _ = oflow.process_problem(imgs, cams, seed=1, pyramid_levels=WORKLOAD["pyramid_levels"])
+    # the sources' depth maps of a geometric pass: the scene's true depths
+    # stand in for the sources' own pass-A maps (same per-pixel work)
+    dm = [d] + [sc.gt_depth[i].astype(np.float32) for i in ids[1:]]
+    for gi in range(WORKLOAD["geom_iterations"]):
+        planes = np.concatenate([n, d[..., None]], -1)
+        d, n, c, _ = oflow.process_problem(imgs, cams, seed=2 + gi, geom=True, multi_geometry=gi > 0, planes=planes,
+                                           costs=c, depth_maps=dm)
+        dm[0] = d
     dt = time.perf_counter() - t0
     return {"value": 320 * 240 / dt / 1e6, "unit": "depth Mpix/s", "cores": int(os.environ["OMP_NUM_THREADS"]),
             "kind": "port", "seconds": dt,
-            "sample": "one full PatchMatch pass of a 320x240 view with 10 sources (same scene recipe, same "
-                      "per-pixel work as the 1600x1200 workload), CPU oracle (oracle/hpm_oracle.c), OpenMP"}
+            "sample": f"one view of a 320x240 scene of the same recipe ({len(ids) - 1} sources): plain pass, "
+                      f"{WORKLOAD['pyramid_levels'] + 1} prior levels, {WORKLOAD['geom_iterations']} geometric "
+                      "passes, CPU oracle (oracle/hpm_oracle.c, OpenMP; OpenCV resize and Delaunay)"}
 
 
 def run_ours(args, dist):
     import torch
 
     import hpm_b200 as hb
-    import synthetic as syn
 
     torch.cuda.set_device(dist.local)
-    sc, ref, imgs, cams, dmin, dmax = make_workload(seed=dist.rank)
-    W, H, S = WORKLOAD["width"], WORKLOAD["height"], WORKLOAD["n_views"] - 1
+    dev = f"cuda:{dist.local}"
+    w = WORKLOAD
+    sc, images, pairs = make_scene(seed=dist.rank)
+    nv, W, H, S = w["n_views"], w["width"], w["height"], w["n_views"] - 1
     npx = W * H
     peak = hb.fp32_peak(dist.local)
     ctx = hb.Context(dist.local)
-    stream = torch.cuda.ExternalStream(ctx.stream(), device=f"cuda:{dist.local}")
-    # pinned host copies of the step inputs and outputs for the end-to-end leg
-    pin_imgs = [torch.from_numpy(i).pin_memory() for i in imgs]
-    pin_planes = torch.empty((H, W, 4), dtype=torch.float32).pin_memory()
-    pin_costs = torch.empty((H, W), dtype=torch.float32).pin_memory()
-    ctx.set_views([p.numpy() for p in pin_imgs], cams)
+    stream = torch.cuda.ExternalStream(ctx.stream(), device=dev)
+    d_imgs = [torch.from_numpy(i).to(dev) for i in images]
+    d_ptrs = [t.data_ptr() for t in d_imgs]
+    torch.cuda.synchronize()
+    opts = dict(planar_prior=True, geom_iterations=w["geom_iterations"], pyramid_levels=w["pyramid_levels"])
+
+    def step(seed):
+        ctx.run_scene(d_ptrs, sc.cams, pairs, seed=seed, images_are_device=True, outputs=False, **opts)
+
     for i in range(args.warmup):
-        ctx.run_patchmatch(hb.default_params(dmin, dmax, seed=1000 + i))
-    # cost-vector evaluations of one pass (deterministic per seed), for the roofline
+        step(1000 + i)
+    # untimed re-runs of the first timed step: work counters (the counting
+    # atomics slow the kernels down) and the kernel launch list
     ctx.count_enable(True)
-    ctx.run_patchmatch(hb.default_params(dmin, dmax, seed=0))
+    step(0)
     n_cv, n_geom = ctx.count_read()
     ctx.count_enable(False)
+    try:
+        launches = count_launches(lambda: step(0))
+        launch_src = "CUDA activity trace (torch.profiler/CUPTI) of an untimed re-run of one step"
+    except Exception as e:  # noqa: BLE001 - the trace is evidence, not a requirement
+        launches, launch_src = {}, f"activity trace unavailable: {e!r}"[:200]
 
     dist.barrier()
     torch.cuda.synchronize()
@@ -197,7 +279,7 @@ def run_ours(args, dist):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
         for i in range(args.steps):
-            ctx.run_patchmatch(hb.default_params(dmin, dmax, seed=i))
+            step(i)
         e1.record(stream)
         e1.synchronize()
         prof = ctx.profile_read()
@@ -205,57 +287,72 @@ def run_ours(args, dist):
     dist.barrier()
     torch.cuda.synchronize()
     ms = dist.max(e0.elapsed_time(e1))
-    planes, costs = ctx.get_result()
-    acc = syn.depth_accuracy(planes[..., 3], sc.gt_depth[ref])
-    nerr = syn.normal_error_deg(planes[..., :3], sc.gt_normal[ref], sc.gt_depth[ref])
 
-    # end to end through the public API, pinned host buffers in and out
+    # end to end through the public API: pinned host images in, every
+    # view's depth, normal and cost maps out
+    pin_imgs = [torch.from_numpy(i).pin_memory() for i in images]
+    outs = ([torch.empty((H, W), dtype=torch.float32).pin_memory() for _ in range(nv)],
+            [torch.empty((H, W, 3), dtype=torch.float32).pin_memory() for _ in range(nv)],
+            [torch.empty((H, W), dtype=torch.float32).pin_memory() for _ in range(nv)])
+    out_np = tuple([t.numpy() for t in o] for o in outs)
+    host_imgs = [p.numpy() for p in pin_imgs]
     dist.barrier()
     torch.cuda.synchronize()
     f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     f0.record(stream)
     for i in range(args.steps):
-        ctx.set_views([p.numpy() for p in pin_imgs], cams)
-        ctx.run_patchmatch(hb.default_params(dmin, dmax, seed=i))
-        lp, lc = pin_planes.numpy(), pin_costs.numpy()
-        rc = hb.lib().hpm_get_result(ctx.handle, hb._p(lp), hb._p(lc))
-        if rc != hb.HPM_OK:
-            raise hb.HpmError("hpm_get_result failed")
+        ctx.run_scene(host_imgs, sc.cams, pairs, seed=i, outputs=out_np, **opts)
     f1.record(stream)
     f1.synchronize()
     dist.barrier()
     ms_e2e = dist.max(f0.elapsed_time(f1))
+    acc = scene_accuracy(sc, dict(enumerate(out_np[0])), dict(enumerate(out_np[1])))
     ctx.close()
 
-    launches_per_pass = 1 + 6 * 2 + 3
+    n_pass = nv * passes_per_view()
     prop_ms, prop_n = prof["propagate"]
-    half_ms = prop_ms / max(prop_n, 1)
-    cv_per_half = (n_cv - npx) / 6.0
-    flops_per_cv = S * (36 * 34 + 80)
-    achieved = cv_per_half * flops_per_cv / (half_ms * 1e-3) / 1e12
+    half_steps = prop_n // max(args.steps, 1)
+    cv_half = n_cv - n_pass * npx  # k_init evaluates one cost vector per pixel and pass
+    flops_step = cv_half * S * (TAPS * NCC_FLOPS_PER_TAP + FLOPS_PER_HYP_VIEW) + n_geom * GEOM_TERM_FLOPS
+    prop_ms_step = prop_ms / args.steps
+    achieved = flops_step / (prop_ms_step * 1e-3) / 1e12
+    n_launch = sum(launches.values())
     line = {
-        "metric": METRIC, "value": dist.world * args.steps * npx / (ms * 1e-3) / 1e6, "unit": "depth Mpix/s",
+        "metric": METRIC, "value": dist.world * args.steps * nv * npx / (ms * 1e-3) / 1e6, "unit": "depth Mpix/s",
         "n_gpus": dist.world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-        "data": "synthetic (seeded procedural scene, see hpm-mvs_b200/synthetic.py)",
-        "config": {"workload": WORKLOAD["name"], "width": W, "height": H, "sources": S,
-                   "scene": f"{WORKLOAD['n_planes']} planes + {WORKLOAD['n_spheres']} spheres, "
-                            f"{int(WORKLOAD['low_texture'] * 100)}% low-texture",
-                   "step": "one plain PatchMatch pass of one reference view: init, 3 red/black iterations, "
-                           "depth/normal, checkerboard filter (HPM::RunPatchMatch)",
-                   "l2": "inputs larger than L2 (11 views x 1600x1200 float images + texture arrays = 169 MB)",
-                   "parallelism": f"views sharded over {dist.world} GPU(s)"},
-        "accuracy": {"px_relerr_lt_1pct": acc, "median_normal_err_deg": nerr},
+        "data": "synthetic (seeded procedural scene, hpm-mvs_b200/synthetic.py; one scene per rank)",
+        "config": {"workload": workload_name(), "width": W, "height": H, "views": nv, "sources": S,
+                   "scene": f"{w['n_planes']} planes + {w['n_spheres']} spheres, "
+                            f"{int(w['low_texture'] * 100)}% low-texture",
+                   "step": "hpm_run_scene: pass set A (plain pass, then one prior pass per pyramid level: support "
+                           "points, Delaunay, raster, KNN prior, JBU) for every view, then the geometric "
+                           f"iterations for every view; {n_pass} PatchMatch passes",
+                   "pyramid_levels": w["pyramid_levels"] + 1, "knn_k": 6,
+                   "l2": f"inputs larger than L2 ({nv} views x {W}x{H} float images + texture arrays = "
+                         f"{2 * nv * npx * 4 / 1e6:.0f} MB, plus the per-view depth/normal/cost maps)",
+                   "parallelism": f"one scene per GPU, {dist.world} GPU(s)"},
+        "accuracy": acc,
         "clocks": clk.summary(),
-        "e2e": {"value": dist.world * args.steps * npx / (ms_e2e * 1e-3) / 1e6, "unit": "depth Mpix/s",
-                "h2d_bytes_per_step": int(sum(i.nbytes for i in imgs)), "d2h_bytes_per_step": int(npx * 20)},
-        "gpu_launches": launches_per_pass * args.steps,
+        "e2e": {"value": dist.world * args.steps * nv * npx / (ms_e2e * 1e-3) / 1e6, "unit": "depth Mpix/s",
+                "h2d_bytes_per_step": int(sum(i.nbytes for i in images)),
+                "d2h_bytes_per_step": int(nv * npx * 4 * 5)},
+        "gpu_launches": n_launch * args.steps,
+        "gpu_launches_per_step": {short_kernel_name(k): v for k, v in sorted(launches.items(), key=lambda x: -x[1])},
+        "gpu_launches_source": launch_src,
         "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                     "frac": achieved / peak, "traffic": None,
-                     "kernel": "k_prop_dirs + k_prop_refine (one half-step)",
-                     "peak_source": "measured FP32 FMA probe (hpm_fp32_peak); MEASURED_PEAKS.json has no FP32 figure",
-                     "half_step_ms": half_ms, "cost_vectors_per_half_step": cv_per_half,
-                     "flops_per_cost_vector": flops_per_cv},
+                     "frac": achieved / peak,
+                     "traffic": TRAFFIC_BYTES_PER_PX_HALF_STEP * npx,
+                     "traffic_note": "DRAM bytes per half-step (k_prop_dirs + k_prop_refine) from the ncu capture "
+                                     "at 1280x960, scaled by pixels",
+                     "kernel": "k_prop_dirs + k_prop_refine (one red/black half-step)",
+                     "peak_source": "measured FP32 FMA probe (hpm_fp32_peak) of measured; "
+                                    "MEASURED_PEAKS.json has no FP32 figure",
+                     "half_step_ms": prop_ms_step / max(half_steps, 1), "half_steps_per_step": half_steps,
+                     "propagate_ms_per_step": prop_ms_step,
+                     "propagate_share": prop_ms_step / (ms / args.steps),
+                     "cost_vectors_per_step": cv_half, "geom_terms_per_step": n_geom,
+                     "flops_per_cost_vector": S * (TAPS * NCC_FLOPS_PER_TAP + FLOPS_PER_HYP_VIEW)},
         "impl": "ours",
     }
     return line
@@ -264,60 +361,105 @@ def run_ours(args, dist):
 def run_reference(args, dist):
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as orc
-    import synthetic as syn
 
     if not orc.ref_available():
         return {"impl": "reference", "unavailable": "oracle/_ref/libhpm_ref.so (reference HPM.cu for sm_100a) "
                                                     "was not built: `make -C oracle ref` needs the reference tree"}
     import torch
 
-    torch.cuda.set_device(dist.local)
-    sc, ref, imgs, cams, dmin, dmax = make_workload(seed=dist.rank)
-    W, H = WORKLOAD["width"], WORKLOAD["height"]
-    npx = W * H
+    import flow as oflow
 
-    def call(seed):
+    torch.cuda.set_device(dist.local)
+    w = WORKLOAD
+    sc, images, pairs = make_scene(seed=0)
+    nv, W, H = w["n_views"], w["width"], w["height"]
+    npx = W * H
+    cores = os.cpu_count() or 1
+    os.environ.setdefault("OMP_NUM_THREADS", str(cores))
+
+    def quiet(fn):
         # the reference prints "iteration: i" from RunPatchMatch (HPM.cu:1943)
         sys.stdout.flush()
         saved = os.dup(1)
         devnull = os.open(os.devnull, os.O_WRONLY)
         os.dup2(devnull, 1)
         try:
-            return orc.ref_run_patchmatch(imgs, cams, depth_min=dmin, depth_max=dmax, seed=seed)
+            return fn()
         finally:
             os.dup2(saved, 1)
             os.close(saved)
             os.close(devnull)
 
+    def problem(v):
+        ids = [v] + pairs[v][1]
+        return ids, [images[i] for i in ids], sc.cams[ids]
+
+    def pass_a(v, seed):
+        ids, imgs, cams = problem(v)
+        return oflow.process_problem(imgs, cams, seed=seed, pyramid_levels=w["pyramid_levels"], backend="reference")
+
+    def geom(v, seed, gi, d_src, n, c):
+        ids, imgs, cams = problem(v)
+        planes = np.concatenate([n, d_src[v][..., None]], -1)
+        return oflow.process_problem(imgs, cams, seed=seed, geom=True, multi_geometry=gi > 0, planes=planes,
+                                     costs=c, depth_maps=[d_src[i] for i in ids], backend="reference")
+
+    # untimed: pass set A and the first geometric iteration of every view, the
+    # maps the sampled views' geometric passes read
+    depth_a, normal, cost, depth_g = {}, {}, {}, {}
+    for v in range(nv):
+        depth_a[v], normal[v], cost[v], _ = quiet(lambda: pass_a(v, 100 + v))
+    for v in range(nv):
+        depth_g[v], _, _, _ = quiet(lambda: geom(v, 200 + v, 0, depth_a, normal[v], cost[v]))
+
+    def step(i):
+        """The whole per-view flow of view i mod n: pass set A, then every
+        geometric iteration (the sources' maps from the untimed setup)."""
+        v = i % nv
+        d, n, c, _ = pass_a(v, 300 + i)
+        src = dict(depth_a)
+        src[v] = d
+        for gi in range(w["geom_iterations"]):
+            d, n, c, _ = geom(v, 1000 + i, gi, src, n, c)
+            src = dict(depth_g) if gi == 0 else src
+            src[v] = d
+        return v, d
+
+    # warm-up on the last views, timed steps from view 0 on (their accuracy
+    # compares with the per-view figures of the product's line)
     for i in range(args.warmup):
-        call(1000 + i)
+        quiet(lambda: step(nv - 1 - i % nv))
     torch.cuda.synchronize()
+    done = {}
     with Clocks(dist.local) as clk:
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
         for i in range(args.steps):
-            planes, costs = call(i)
+            v, d = quiet(lambda: step(i))
+            done[v] = d
         e1.record()
         e1.synchronize()
     ms = e0.elapsed_time(e1)
     value = args.steps * npx / (ms * 1e-3) / 1e6
-    acc = syn.depth_accuracy(planes[..., 3], sc.gt_depth[ref])
+    sample = (f"one view per step (timed step i: view i mod {nv}) of the {nv}-view scene: pass set A with the prior on "
+              f"{w['pyramid_levels'] + 1} levels, then {w['geom_iterations']} geometric passes; the reference's "
+              "HPM.cu kernels (oracle/_ref, compiled unchanged for sm_100a) on the B200 for the PatchMatch passes "
+              "and the JBU; host stages on the CPU: OpenCV resize and Delaunay, the oracle's C restatement of the "
+              f"support points, raster, KNN prior and prior assembly (OpenMP, {os.environ['OMP_NUM_THREADS']} "
+              "threads)")
     return {
         "metric": METRIC, "value": value, "unit": "depth Mpix/s", "n_gpus": 1, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded procedural scene)",
-        "config": {"workload": WORKLOAD["name"], "width": W, "height": H, "sources": WORKLOAD["n_views"] - 1,
-                   "step": "the reference's CudaSpaceInitialization-equivalent upload, HPM::RunPatchMatch "
-                           "(HPM.cu:1906-1957, with its per-launch device syncs) and result download"},
-        "accuracy": {"px_relerr_lt_1pct": acc},
+        "config": {"workload": workload_name(), "width": W, "height": H, "views": nv, "sources": nv - 1,
+                   "step": "the reference's per-view flow (main.cpp:35-499 for pass set A, main.cpp:662-674 for the "
+                           "geometric iterations) on one view"},
+        "accuracy": scene_accuracy(sc, done),
         "clocks": clk.summary(),
         "impl": "reference",
-        "cpu_baseline": {"value": value, "unit": "depth Mpix/s", "cores": 1, "kind": "reference",
-                         "sample": "the reference's own HPM.cu kernels, compiled unchanged for sm_100a and run on "
-                                   "the B200 (the reference has no CPU implementation of this path); one host "
-                                   "thread drives it"},
-        "e2e": {"value": value, "unit": "depth Mpix/s", "h2d_bytes_per_step": int(sum(i.nbytes for i in imgs)),
-                "d2h_bytes_per_step": int(npx * 20)},
+        "cpu_baseline": {"value": value, "unit": "depth Mpix/s", "cores": int(os.environ["OMP_NUM_THREADS"]),
+                         "kind": "reference", "sample": sample},
+        "e2e": {"value": value, "unit": "depth Mpix/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
 
 

@@ -211,8 +211,9 @@ class Context:
                   images_are_device=False, outputs=True):
         """The reference's main() over a scene.  images: per-view float32 [H, W]
         arrays, or device pointers (ints) with images_are_device; pairs:
-        [(ref, [sources])].  Returns per-view (depth, normal, cost) lists when
-        outputs is true."""
+        [(ref, [sources])].  outputs: True to return new per-view (depth,
+        normal, cost) lists, False for none (the maps stay on the device), or
+        a tuple of three caller-owned lists of float32 arrays to fill."""
         n = len(cams)
         cams = np.ascontiguousarray(cams, dtype=CAMERA_DTYPE)
         if images_are_device:
@@ -229,7 +230,16 @@ class Context:
             srcs[i, :len(s)] = s
         o = HpmSceneOpts(int(planar_prior), int(geom_iterations), int(seed), int(pyramid_levels))
         outs = None
-        if outputs:
+        if isinstance(outputs, (tuple, list)):
+            outs = list(zip(*outputs))
+            for v, c in enumerate(cams):
+                hw = (int(c["height"]), int(c["width"]))
+                for k, shape in enumerate([hw, hw + (3,), hw]):
+                    a = outs[v][k]
+                    if a.shape != shape or a.dtype != np.float32 or not a.flags.c_contiguous:
+                        raise ValueError(f"run_scene: output {k} of view {v} must be float32 {shape}, C order")
+            arrs = [(ctypes.c_void_p * n)(*[o_[k].ctypes.data for o_ in outs]) for k in range(3)]
+        elif outputs:
             outs = [(np.empty((int(c["height"]), int(c["width"])), np.float32),
                      np.empty((int(c["height"]), int(c["width"]), 3), np.float32),
                      np.empty((int(c["height"]), int(c["width"])), np.float32)) for c in cams]

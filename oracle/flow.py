@@ -39,11 +39,6 @@ def cv_triangles(pts: np.ndarray, w: int, h: int) -> np.ndarray:
     return t[keep]
 
 
-def _world(cam, n):
-    R = cam["R"].reshape(3, 3).astype(np.float32)
-    return (np.asarray(n, np.float32)[..., :3] @ R).astype(np.float32)  # R^T n for row vectors
-
-
 def level_masks(cam, depth, cost, factor, dmin, dmax, triangles=None):
     """Support points, triangles, raster, planes and KNN of one level: the
     reference's mask (float), triangle planes and KNN planes."""
@@ -56,95 +51,70 @@ def level_masks(cam, depth, cost, factor, dmin, dmax, triangles=None):
     return mask, tri_planes, knn_planes
 
 
-def prior_level(cam, level, depth, normal, cost, guide, dmin, dmax, triangles=None):
+def prior_level(cam, level, depth, normal, cost, guide, dmin, dmax, triangles=None, jbu=None):
     """Prior planes (ref frame), masks and (full scale) prior depth of one
-    pyramid level from full-resolution maps (main.cpp:78-478)."""
+    pyramid level from full-resolution maps (main.cpp:78-478).  jbu: the
+    joint bilateral upsampler (default: the oracle's)."""
     import cv2
 
     H, W = depth.shape
     dmin, dmax = np.float32(dmin), np.float32(dmax)
-    prior = np.zeros((H, W, 4), np.float32)
-    pmask = np.zeros((H, W), np.uint32)
-    prior_depth = np.zeros((H, W), np.float32)
     if level in (0, 1):
         f = 0.25 if level == 0 else 0.5
         ws, hs = int(round(W * f)), int(round(H * f))
         d_s = cv2.resize(depth, (ws, hs), interpolation=cv2.INTER_LINEAR)
         c_s = cv2.resize(cost, (ws, hs), interpolation=cv2.INTER_LINEAR)
         mask, tri_planes, knn_planes = level_masks(cam, d_s, c_s, f, dmin, dmax, triangles)
-        pd = np.zeros((hs, ws), np.float32)
-        pn = np.zeros((hs, ws, 3), np.float32)
-        for y in range(hs):  # main.cpp:124-162
-            for x in range(ws):
-                m = mask[y, x]
-                if m > 0:
-                    pl = tri_planes[int(m) - 1]
-                    d = orc.depth_from_plane(cam, pl, x, y, f)
-                    if d <= dmax * np.float32(1.2) and d >= dmin * np.float32(0.6):
-                        pd[y, x] = d
-                        pn[y, x] = _world(cam, pl)
-                elif m < -200:
-                    pl = knn_planes[y, x]
-                    d = orc.depth_from_plane(cam, pl, x, y, f)
-                    if dmin <= d <= dmax:
-                        pd[y, x] = d
-                        pn[y, x] = _world(cam, pl)
-        ud, un = orc.jbu(guide, pd, pn)
-        # main.cpp:179-203: world normal -> ref frame, depth -> plane distance
-        R = cam["R"].reshape(3, 3).astype(np.float32)
-        K = cam["K"].reshape(3, 3).astype(np.float32)
-        nref = (un @ R.T).astype(np.float32)
-        ys, xs = np.mgrid[0:H, 0:W].astype(np.float32)
-        X0 = ud * (xs - K[0, 2]) / K[0, 0]
-        X1 = ud * (ys - K[1, 2]) / K[1, 1]
-        dist = -(nref[..., 0] * X0 + nref[..., 1] * X1 + nref[..., 2] * ud)
-        ok = (ud <= dmax) & (ud >= dmin)
-        prior[ok] = np.concatenate([nref, dist[..., None]], -1)[ok]
-        pmask = ok.astype(np.uint32)
-    else:
-        mask, tri_planes, knn_planes = level_masks(cam, depth, cost, 1.0, dmin, dmax, triangles)
-        for y in range(H):  # main.cpp:426-454, HPM.cpp:1099-1123
-            for x in range(W):
-                m = mask[y, x]
-                if m > 0:
-                    pl = tri_planes[int(m) - 1]
-                    d = orc.depth_from_plane(cam, pl, x, y, 1.0)
-                    if dmin <= d <= dmax:
-                        prior_depth[y, x] = d
-                        prior[y, x] = pl
-                        pmask[y, x] = int(m)
-                elif m < -200:
-                    pl = knn_planes[y, x]
-                    d = orc.depth_from_plane(cam, pl, x, y, 1.0)
-                    if dmin <= d <= dmax:
-                        prior_depth[y, x] = d
-                        prior[y, x] = pl
-                        pmask[y, x] = 0xFFFFFF17  # (unsigned int)-233.0f
-    return prior, pmask, prior_depth
+        pd, pn = orc.prior_coarse(cam, mask, tri_planes, knn_planes, f, dmin, dmax)
+        ud, un = (jbu or orc.jbu)(guide, pd, pn)
+        prior, pmask = orc.prior_reload(cam, ud, un, dmin, dmax)
+        return prior, pmask, np.zeros((H, W), np.float32)
+    mask, tri_planes, knn_planes = level_masks(cam, depth, cost, 1.0, dmin, dmax, triangles)
+    return orc.prior_full(cam, mask, tri_planes, knn_planes, dmin, dmax)
+
+
+def _oracle_pass(images, cams, **kw):
+    return orc.run_patchmatch(images, cams, **kw)
+
+
+def _reference_pass(images, cams, *, salt=0, views=None, **kw):
+    """HPM::RunPatchMatch of the reference's own kernels (oracle/_ref); the
+    reference draws its random streams from clock64(), so salt and the
+    selected-view map do not apply."""
+    p, c = orc.ref_run_patchmatch(images, cams, **kw)
+    return p, c, None
 
 
 def process_problem(images, cams, *, seed=0, planar_prior=True, geom=False, multi_geometry=False, planes=None,
-                    costs=None, depth_maps=None, guide=None, pyramid_levels=-1):
-    """Returns (depth, world normal, cost, prior depth) of the reference view."""
+                    costs=None, depth_maps=None, guide=None, pyramid_levels=-1, backend="oracle"):
+    """Returns (depth, world normal, cost, prior depth) of the reference view.
+    backend "oracle": the oracle's CPU passes and JBU; "reference": the
+    reference's own CUDA kernels (oracle/_ref) for the passes and the JBU,
+    with the host stages above."""
+    ref = backend == "reference"
+    run = _reference_pass if ref else _oracle_pass
+    jbu = orc.ref_jbu if ref else orc.jbu
     cam = cams[0]
     H, W = images[0].shape
     dmin = np.float32(cam["depth_min"]) * np.float32(0.6)
     dmax = np.float32(cam["depth_max"]) * np.float32(1.2)
     salt = 0
     if geom:
-        p, c, v = orc.run_patchmatch(images, cams, depth_min=dmin, depth_max=dmax, seed=seed, salt=salt, geom=True,
-                                     planes=planes, costs=costs, depth_maps=depth_maps)
+        extra = {"multi_geometry": multi_geometry} if ref else {}
+        p, c, v = run(images, cams, depth_min=dmin, depth_max=dmax, seed=seed, salt=salt, geom=True,
+                      planes=planes, costs=costs, depth_maps=depth_maps, **extra)
         return p[..., 3].copy(), p[..., :3].copy(), c, np.zeros((H, W), np.float32)
-    p, c, v = orc.run_patchmatch(images, cams, depth_min=dmin, depth_max=dmax, seed=seed, salt=salt)
+    p, c, v = run(images, cams, depth_min=dmin, depth_max=dmax, seed=seed, salt=salt)
     prior_depth = np.zeros((H, W), np.float32)
     if planar_prior:
         guide = images[0] if guide is None else guide
         k = pyramid_levels if pyramid_levels >= 0 else scale_levels(W, H)
         for i in range(2 - k, 3):
-            prior, pmask, pd = prior_level(cam, i, p[..., 3].copy(), p[..., :3].copy(), c, guide, dmin, dmax)
+            prior, pmask, pd = prior_level(cam, i, p[..., 3].copy(), p[..., :3].copy(), c, guide, dmin, dmax,
+                                           jbu=jbu)
             if i not in (0, 1):
                 prior_depth = pd
             salt += 1
-            p, c, v = orc.run_patchmatch(images, cams, depth_min=dmin, depth_max=dmax, seed=seed, salt=salt, prior=True,
-                                         planes=p, costs=c, views=v, prior_planes=prior, masks=pmask)
+            p, c, v = run(images, cams, depth_min=dmin, depth_max=dmax, seed=seed + (salt if ref else 0), salt=salt,
+                          prior=True, planes=p, costs=c, views=v, prior_planes=prior, masks=pmask)
     return p[..., 3].copy(), p[..., :3].copy(), c, prior_depth

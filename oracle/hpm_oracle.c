@@ -1275,10 +1275,97 @@ static const int kTriples[20][3] = {{0, 1, 2}, {0, 1, 3}, {0, 1, 4}, {0, 2, 3}, 
                                     {1, 2, 4}, {1, 3, 4}, {2, 3, 4}, {0, 1, 5}, {0, 2, 5}, {0, 3, 5}, {0, 4, 5},
                                     {1, 2, 5}, {1, 3, 5}, {1, 4, 5}, {2, 3, 5}, {2, 4, 5}, {3, 4, 5}};
 
+/* Insert (d, k) into the sorted 6-list, ordered by distance, then index. */
+static void knn6_insert(long d, int k, long *bd, int *best, int *nb)
+{
+    if (*nb == 6 && (d > bd[5] || (d == bd[5] && k > best[5]))) return;
+    int pos = *nb < 6 ? (*nb)++ : 5;
+    while (pos > 0 && (bd[pos - 1] > d || (bd[pos - 1] == d && best[pos - 1] > k))) {
+        bd[pos] = bd[pos - 1];
+        best[pos] = best[pos - 1];
+        pos--;
+    }
+    bd[pos] = d;
+    best[pos] = k;
+}
+
+static void knn6_brute(const int *pts, int n_pts, int x, int y, int *best)
+{
+    long bd[6];
+    int nb = 0;
+    for (int k = 0; k < n_pts; ++k) {
+        const long dx = pts[2 * k] - x, dy = pts[2 * k + 1] - y;
+        knn6_insert(dx * dx + dy * dy, k, bd, best, &nb);
+    }
+}
+
+/* Uniform grid of kGridCell-pixel cells (CSR, indices ascending per cell). */
+enum { kGridCell = 8 };
+typedef struct {
+    int gw, gh;
+    int *start, *idx;
+} KnnGrid;
+
+static void knn_grid_build(KnnGrid *g, const int *pts, int n_pts, int w, int h)
+{
+    g->gw = (w + kGridCell - 1) / kGridCell;
+    g->gh = (h + kGridCell - 1) / kGridCell;
+    const int nc = g->gw * g->gh;
+    g->start = (int *)calloc((size_t)nc + 1, sizeof(int));
+    g->idx = (int *)malloc(sizeof(int) * (size_t)(n_pts > 0 ? n_pts : 1));
+    for (int k = 0; k < n_pts; ++k) g->start[1 + (pts[2 * k + 1] / kGridCell) * g->gw + pts[2 * k] / kGridCell]++;
+    for (int c = 0; c < nc; ++c) g->start[c + 1] += g->start[c];
+    int *fill = (int *)malloc(sizeof(int) * (size_t)nc);
+    memcpy(fill, g->start, sizeof(int) * (size_t)nc);
+    for (int k = 0; k < n_pts; ++k) g->idx[fill[(pts[2 * k + 1] / kGridCell) * g->gw + pts[2 * k] / kGridCell]++] = k;
+    free(fill);
+}
+
+/* Exact: rings of cells around the query's cell until the 6th distance is
+ * below the distance to anything outside the visited block. */
+static void knn6_grid(const KnnGrid *g, const int *pts, int x, int y, int *best)
+{
+    long bd[6];
+    int nb = 0;
+    const int cx = x / kGridCell, cy = y / kGridCell;
+    for (int r = 0;; ++r) {
+        for (int gy = cy - r; gy <= cy + r; ++gy) {
+            if (gy < 0 || gy >= g->gh) continue;
+            const int step = (gy == cy - r || gy == cy + r) ? 1 : 2 * r;
+            for (int gx = cx - r; gx <= cx + r; gx += step > 0 ? step : 1) {
+                if (gx < 0 || gx >= g->gw) continue;
+                const int c = gy * g->gw + gx;
+                for (int q = g->start[c]; q < g->start[c + 1]; ++q) {
+                    const int k = g->idx[q];
+                    const long dx = pts[2 * k] - x, dy = pts[2 * k + 1] - y;
+                    knn6_insert(dx * dx + dy * dy, k, bd, best, &nb);
+                }
+            }
+        }
+        if (cx - r <= 0 && cy - r <= 0 && cx + r >= g->gw - 1 && cy + r >= g->gh - 1) return;
+        if (nb == 6) {
+            /* nearest integer position outside cells [cx-r, cx+r] x [cy-r, cy+r] */
+            long b = x - ((long)(cx - r) * kGridCell - 1);
+            const long bx2 = (long)(cx + r + 1) * kGridCell - x;
+            const long by1 = y - ((long)(cy - r) * kGridCell - 1), by2 = (long)(cy + r + 1) * kGridCell - y;
+            if (bx2 < b) b = bx2;
+            if (by1 < b) b = by1;
+            if (by2 < b) b = by2;
+            if (bd[5] < b * b) return;
+        }
+    }
+}
+
+static int g_knn_grid = 1;
+
+void or_set_knn_grid(int on) { g_knn_grid = on; }
+
 void or_knn_supplement(const OrCamera *ref, const int *pts, int n_pts, const float *depth, int w, int h, float factor,
                        float dmin, float dmax, float *plane_out, float *mask)
 {
     if (n_pts < 6) return;
+    KnnGrid g = {0, 0, NULL, NULL};
+    if (g_knn_grid) knn_grid_build(&g, pts, n_pts, w, h);
 #ifdef _OPENMP
 #pragma omp parallel for schedule(dynamic, 4)
 #endif
@@ -1287,25 +1374,10 @@ void or_knn_supplement(const OrCamera *ref, const int *pts, int n_pts, const flo
             if (mask[(size_t)i * w + j] > 0) continue;
             /* exact 6 nearest support points; ties broken by insertion order */
             int best[6];
-            long bd[6];
-            int nb = 0;
-            for (int k = 0; k < n_pts; ++k) {
-                const long dx = pts[2 * k] - j, dy = pts[2 * k + 1] - i;
-                const long d = dx * dx + dy * dy;
-                if (nb < 6 || d < bd[nb - 1]) {
-                    int pos = nb < 6 ? nb : 5;
-                    while (pos > 0 && bd[pos - 1] > d) {
-                        if (pos < 6) {
-                            bd[pos] = bd[pos - 1];
-                            best[pos] = best[pos - 1];
-                        }
-                        pos--;
-                    }
-                    bd[pos] = d;
-                    best[pos] = k;
-                    if (nb < 6) nb++;
-                }
-            }
+            if (g_knn_grid)
+                knn6_grid(&g, pts, j, i, best);
+            else
+                knn6_brute(pts, n_pts, j, i, best);
             int sel = -1;
             for (int tI = 0; tI < 20; ++tI) {
                 if (not_on_line(pts + 2 * best[kTriples[tI][0]], pts + 2 * best[kTriples[tI][1]],
@@ -1326,6 +1398,112 @@ void or_knn_supplement(const OrCamera *ref, const int *pts, int n_pts, const flo
             if (d <= dmax && d >= dmin) {
                 mask[(size_t)i * w + j] = -233.0f;
                 memcpy(plane_out + 4 * ((size_t)i * w + j), n4, sizeof(n4));
+            }
+        }
+    }
+    free(g.start);
+    free(g.idx);
+}
+
+/* TransformNormal (HPM.cpp:872-880): ref-frame normal to world, R^T n. */
+static void to_world(const OrCamera *ref, const float *n, float *out)
+{
+    const float *R = ref->R;
+    out[0] = R[0] * n[0] + R[3] * n[1] + R[6] * n[2];
+    out[1] = R[1] * n[0] + R[4] * n[1] + R[7] * n[2];
+    out[2] = R[2] * n[0] + R[5] * n[1] + R[8] * n[2];
+}
+
+void or_prior_coarse(const OrCamera *ref, const float *mask, const float *tri_planes, int n_tri,
+                     const float *knn_planes, int w, int h, float factor, float dmin, float dmax, float *out_depth,
+                     float *out_normal3)
+{
+    for (size_t i = 0; i < (size_t)w * h; ++i) {
+        out_depth[i] = 0.0f;
+        out_normal3[3 * i] = out_normal3[3 * i + 1] = out_normal3[3 * i + 2] = 0.0f;
+    }
+    for (int y = 0; y < h; ++y) {
+        for (int x = 0; x < w; ++x) {
+            const size_t c = (size_t)y * w + x;
+            const float m = mask[c];
+            const float *pl = NULL;
+            float lo = dmin, hi = dmax;
+            if (m > 0) {
+                const int t = (int)m - 1;
+                if (t < 0 || t >= n_tri) continue;
+                pl = tri_planes + 4 * t;
+                lo = dmin * 0.6f; /* main.cpp:129 widens the range once more */
+                hi = dmax * 1.2f;
+            } else if (m < -200) {
+                pl = knn_planes + 4 * c;
+            } else {
+                continue;
+            }
+            const float d = or_depth_from_plane(ref, pl, x, y, factor);
+            if (d <= hi && d >= lo) {
+                out_depth[c] = d;
+                to_world(ref, pl, out_normal3 + 3 * c);
+            }
+        }
+    }
+}
+
+void or_prior_reload(const OrCamera *ref, const float *depth, const float *normal3, int w, int h, float dmin,
+                     float dmax, float *out4, unsigned int *out_mask)
+{
+    const float *R = ref->R, *K = ref->K;
+    for (int y = 0; y < h; ++y) {
+        for (int x = 0; x < w; ++x) {
+            const size_t c = (size_t)y * w + x;
+            const float d = depth[c];
+            out4[4 * c] = out4[4 * c + 1] = out4[4 * c + 2] = out4[4 * c + 3] = 0.0f;
+            out_mask[c] = 0;
+            if (!(d <= dmax && d >= dmin)) continue;
+            const float *n = normal3 + 3 * c;
+            /* TransformNormal2RefCam (HPM.cpp:882-890), GetDistance2Origin_factor (HPM.cpp:892-899) */
+            const float nx = R[0] * n[0] + R[1] * n[1] + R[2] * n[2];
+            const float ny = R[3] * n[0] + R[4] * n[1] + R[5] * n[2];
+            const float nz = R[6] * n[0] + R[7] * n[1] + R[8] * n[2];
+            const float X0 = d * ((float)x - K[2]) / K[0];
+            const float X1 = d * ((float)y - K[5]) / K[4];
+            out4[4 * c] = nx;
+            out4[4 * c + 1] = ny;
+            out4[4 * c + 2] = nz;
+            out4[4 * c + 3] = -(nx * X0 + ny * X1 + nz * d);
+            out_mask[c] = 1;
+        }
+    }
+}
+
+void or_prior_full(const OrCamera *ref, const float *mask, const float *tri_planes, int n_tri,
+                   const float *knn_planes, int w, int h, float dmin, float dmax, float *out4,
+                   unsigned int *out_mask, float *out_depth)
+{
+    for (int y = 0; y < h; ++y) {
+        for (int x = 0; x < w; ++x) {
+            const size_t c = (size_t)y * w + x;
+            const float m = mask[c];
+            out4[4 * c] = out4[4 * c + 1] = out4[4 * c + 2] = out4[4 * c + 3] = 0.0f;
+            out_mask[c] = 0;
+            out_depth[c] = 0.0f;
+            const float *pl = NULL;
+            unsigned int mv = 0;
+            if (m > 0) {
+                const int t = (int)m - 1;
+                if (t < 0 || t >= n_tri) continue;
+                pl = tri_planes + 4 * t;
+                mv = (unsigned int)(int)m;
+            } else if (m < -200) {
+                pl = knn_planes + 4 * c;
+                mv = 0xFFFFFF17u; /* (unsigned int)-233.0f, HPM.cpp:1112 */
+            } else {
+                continue;
+            }
+            const float d = or_depth_from_plane(ref, pl, x, y, 1.0f);
+            if (d <= dmax && d >= dmin) {
+                out_depth[c] = d;
+                memcpy(out4 + 4 * c, pl, 4 * sizeof(float));
+                out_mask[c] = mv;
             }
         }
     }

@@ -98,10 +98,34 @@ float or_depth_from_plane(const OrCamera *ref, const float *plane4, int x, int y
  * kept triangles and stores their vertex triples in kept6. */
 int or_raster_triangles(const int *tris6, int n_tris, int w, int h, float *mask, int *kept6);
 
-/* DepthsPredictSupplement (HPM.cpp:923-1097) with exact brute-force K=6
- * nearest neighbours (the reference uses PCL KdTreeFLANN). */
+/* DepthsPredictSupplement (HPM.cpp:923-1097) with exact K=6 nearest
+ * neighbours, ties to the lower support-point index (the reference uses PCL
+ * KdTreeFLANN, an exact kd-tree search).  The neighbours come from a uniform
+ * grid search (default) or a brute-force scan (or_set_knn_grid(0)); both are
+ * exact and give identical results. */
 void or_knn_supplement(const OrCamera *ref, const int *pts_xy, int n_pts, const float *depth, int w, int h,
                        float factor, float dmin, float dmax, float *plane_out4, float *mask);
+void or_set_knn_grid(int on);
+
+/* main.cpp:124-162 (coarse levels): prior depth and world normal at the
+ * level's resolution from the triangle raster (mask > 0: triangle mask-1,
+ * range widened to [0.6 dmin, 1.2 dmax]) and the KNN supplement (mask <
+ * -200, range [dmin, dmax]); zero elsewhere. */
+void or_prior_coarse(const OrCamera *ref, const float *mask, const float *tri_planes, int n_tri,
+                     const float *knn_planes, int w, int h, float factor, float dmin, float dmax, float *out_depth,
+                     float *out_normal3);
+
+/* main.cpp:179-203: upsampled depth and world normal to ref-frame prior
+ * planes (normal, distance to origin) and 0/1 masks. */
+void or_prior_reload(const OrCamera *ref, const float *depth, const float *normal3, int w, int h, float dmin,
+                     float dmax, float *out4, unsigned int *out_mask);
+
+/* main.cpp:426-454 with CudaPlanarPriorInitializationSupplement
+ * (HPM.cpp:1099-1123): full-scale prior planes, masks (triangle id or
+ * 0xFFFFFF17 for KNN planes) and the prior depth map (depths_prior.dmb). */
+void or_prior_full(const OrCamera *ref, const float *mask, const float *tri_planes, int n_tri,
+                   const float *knn_planes, int w, int h, float dmin, float dmax, float *out4,
+                   unsigned int *out_mask, float *out_depth);
 
 #ifdef __cplusplus
 }

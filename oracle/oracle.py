@@ -236,6 +236,55 @@ def knn_supplement(ref_cam, pts, depth, factor, dmin, dmax, mask):
     return planes, mask
 
 
+def set_knn_grid(on: bool) -> None:
+    """Neighbour search of knn_supplement: exact grid search (default) or the
+    brute-force scan; both give identical results."""
+    lib().or_set_knn_grid(ctypes.c_int(int(on)))
+
+
+def _f(x):
+    return ctypes.c_float(float(x))
+
+
+def prior_coarse(ref_cam, mask, tri_planes, knn_planes, factor, dmin, dmax):
+    """main.cpp:124-162: (prior depth, world normal) at the level's size."""
+    r = _cams(np.array([ref_cam], dtype=CAMERA_DTYPE))
+    mask = np.ascontiguousarray(mask, dtype=np.float32)
+    h, w = mask.shape
+    tp = np.ascontiguousarray(tri_planes, dtype=np.float32).reshape(-1, 4)
+    kp = np.ascontiguousarray(knn_planes, dtype=np.float32).reshape(h, w, 4)
+    d = np.zeros((h, w), np.float32)
+    n = np.zeros((h, w, 3), np.float32)
+    lib().or_prior_coarse(_p(r), _p(mask), _p(tp), len(tp), _p(kp), w, h, _f(factor), _f(dmin), _f(dmax), _p(d), _p(n))
+    return d, n
+
+
+def prior_reload(ref_cam, depth, normal, dmin, dmax):
+    """main.cpp:179-203: (ref-frame prior planes, 0/1 masks)."""
+    r = _cams(np.array([ref_cam], dtype=CAMERA_DTYPE))
+    depth = np.ascontiguousarray(depth, dtype=np.float32)
+    normal = np.ascontiguousarray(normal, dtype=np.float32)
+    h, w = depth.shape
+    out = np.zeros((h, w, 4), np.float32)
+    m = np.zeros((h, w), np.uint32)
+    lib().or_prior_reload(_p(r), _p(depth), _p(normal), w, h, _f(dmin), _f(dmax), _p(out), _p(m))
+    return out, m
+
+
+def prior_full(ref_cam, mask, tri_planes, knn_planes, dmin, dmax):
+    """main.cpp:426-454 + HPM.cpp:1099-1123: (prior planes, masks, prior depth)."""
+    r = _cams(np.array([ref_cam], dtype=CAMERA_DTYPE))
+    mask = np.ascontiguousarray(mask, dtype=np.float32)
+    h, w = mask.shape
+    tp = np.ascontiguousarray(tri_planes, dtype=np.float32).reshape(-1, 4)
+    kp = np.ascontiguousarray(knn_planes, dtype=np.float32).reshape(h, w, 4)
+    out = np.zeros((h, w, 4), np.float32)
+    m = np.zeros((h, w), np.uint32)
+    d = np.zeros((h, w), np.float32)
+    lib().or_prior_full(_p(r), _p(mask), _p(tp), len(tp), _p(kp), w, h, _f(dmin), _f(dmax), _p(out), _p(m), _p(d))
+    return out, m, d
+
+
 # ---------------------------------------------------------------- reference shim
 
 def ref_cost_vectors(images, cams, planes) -> np.ndarray:

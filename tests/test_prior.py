@@ -50,3 +50,28 @@ def test_oracle_flow_runs():
     d1, n1, c1, pd = oflow.process_problem(imgs, cams, seed=2, planar_prior=True, pyramid_levels=1)
     assert (pd > 0).mean() > 0.3
     assert syn.depth_accuracy(d1, gt) > 0.3
+
+
+@pytest.mark.parametrize("w,h,seed", [(64, 48, 0), (333, 211, 1), (800, 600, 2)])
+def test_knn_grid_search_equals_brute_force(w, h, seed):
+    """The oracle's grid neighbour search against its brute-force scan: the
+    same six neighbours (ties to the lower index), so the same KNN planes and
+    mask, on sparse and clustered support points."""
+    import oracle as orc
+
+    rng = np.random.default_rng(seed)
+    pts = [(cx + rng.integers(0, 5), cy + rng.integers(0, 5)) for cx in range(0, w - 4, 5)
+           for cy in range(0, h - 4, 5) if rng.random() < (0.05 if cx < w // 2 else 0.5)]
+    pts = np.array(pts, np.int32)
+    sc = syn.make_scene(seed, w, h, 2, n_planes=3)
+    cam, depth = sc.cams[0], sc.gt_depth[0].astype(np.float32)
+    mask0 = np.where(rng.random((h, w)) < 0.3, 1.0, 0.0).astype(np.float32)
+    try:
+        orc.set_knn_grid(False)
+        pb, mb = orc.knn_supplement(cam, pts, depth, 1.0, sc.depth_min, sc.depth_max, mask0)
+    finally:
+        orc.set_knn_grid(True)
+    pg, mg = orc.knn_supplement(cam, pts, depth, 1.0, sc.depth_min, sc.depth_max, mask0)
+    assert (mb < -200).mean() > 0.3
+    np.testing.assert_array_equal(mg, mb)
+    np.testing.assert_array_equal(pg, pb)
