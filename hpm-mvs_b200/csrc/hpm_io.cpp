@@ -8,14 +8,25 @@
  *             HPM.cpp:160-185)
  *   pair.txt  N, then per problem: ref_id, n_src, n_src x (id score); sources
  *             with score <= 0 are dropped (GenerateSampleList, main.cpp:4-33)
+ *   images    8-bit grayscale as cv::imread(path, IMREAD_GRAYSCALE) returns it
+ *             (HPM.cpp:492): binary PGM (P5, maxval 255) and PNG (8-bit gray,
+ *             gray+alpha, RGB, RGBA, palette; not interlaced).  Colour is
+ *             reduced the way libpng's rgb_to_gray does it for OpenCV's
+ *             coefficients 0.299/0.587: (9797 R + 19234 G + 3737 B) >> 15,
+ *             alpha is dropped.  JPEG is not decoded here.
  *
  * Unlike the reference (which prints and carries on, or dereferences NULL on
  * a failed fopen), every failure returns HPM_ERR_IO.
  */
+#include <cmath>
+#include <cstdint>
 #include <cstdio>
 #include <cstring>
 #include <fstream>
 #include <string>
+#include <vector>
+
+#include <zlib.h>
 
 #include "hpm_b200.h"
 
@@ -112,3 +123,198 @@ int hpm_read_pair(const char *path, int *n_out, int *ref_ids, int *src_counts, i
 }
 
 }  // extern "C"
+
+namespace {
+
+bool read_file(const char *path, std::vector<uint8_t> &out)
+{
+    FILE *f = fopen(path, "rb");
+    if (!f) return false;
+    out.clear();
+    uint8_t buf[1 << 16];
+    size_t n;
+    while ((n = fread(buf, 1, sizeof(buf), f)) > 0) out.insert(out.end(), buf, buf + n);
+    const bool ok = !ferror(f);
+    fclose(f);
+    return ok;
+}
+
+/* P5 header: magic, width, height, maxval, each separated by whitespace and
+ * '#' comments, then one whitespace byte before the raster. */
+int decode_pgm(const std::vector<uint8_t> &b, std::vector<uint8_t> &px, int *w, int *h)
+{
+    size_t i = 2;
+    long v[3];
+    for (int k = 0; k < 3; ++k) {
+        for (;;) {
+            if (i >= b.size()) return HPM_ERR_IO;
+            if (b[i] == '#') {
+                while (i < b.size() && b[i] != '\n') ++i;
+            } else if (b[i] == ' ' || b[i] == '\t' || b[i] == '\n' || b[i] == '\r') {
+                ++i;
+            } else {
+                break;
+            }
+        }
+        if (b[i] < '0' || b[i] > '9') return HPM_ERR_IO;
+        v[k] = 0;
+        while (i < b.size() && b[i] >= '0' && b[i] <= '9' && v[k] < (1L << 20)) v[k] = v[k] * 10 + (b[i++] - '0');
+    }
+    if (i >= b.size() || v[0] <= 0 || v[1] <= 0 || v[0] >= (1L << 16) || v[1] >= (1L << 16) || v[2] != 255)
+        return HPM_ERR_IO;
+    ++i; /* the single whitespace byte */
+    const size_t n = (size_t)v[0] * v[1];
+    if (b.size() - i < n) return HPM_ERR_IO;
+    px.assign(b.begin() + i, b.begin() + i + n);
+    *w = (int)v[0];
+    *h = (int)v[1];
+    return HPM_OK;
+}
+
+uint32_t be32(const uint8_t *p) { return (uint32_t)p[0] << 24 | (uint32_t)p[1] << 16 | (uint32_t)p[2] << 8 | p[3]; }
+
+int paeth(int a, int b, int c)
+{
+    const int p = a + b - c, pa = p > a ? p - a : a - p, pb = p > b ? p - b : b - p, pc = p > c ? p - c : c - p;
+    return (pa <= pb && pa <= pc) ? a : (pb <= pc ? b : c);
+}
+
+int decode_png(const std::vector<uint8_t> &b, std::vector<uint8_t> &px, int *w_out, int *h_out)
+{
+    static const uint8_t sig[8] = {137, 80, 78, 71, 13, 10, 26, 10};
+    if (b.size() < 33 || memcmp(b.data(), sig, 8) != 0) return HPM_ERR_IO;
+    size_t i = 8;
+    uint32_t w = 0, h = 0;
+    int depth = 0, ctype = -1, interlace = 0;
+    std::vector<uint8_t> idat, palette;
+    bool seen_end = false;
+    while (i + 12 <= b.size() && !seen_end) {
+        const uint32_t len = be32(&b[i]);
+        if (len > b.size() - i - 12) return HPM_ERR_IO;
+        const uint8_t *type = &b[i + 4], *data = &b[i + 8];
+        if (!memcmp(type, "IHDR", 4) && len >= 13) {
+            w = be32(data);
+            h = be32(data + 4);
+            depth = data[8];
+            ctype = data[9];
+            interlace = data[12];
+        } else if (!memcmp(type, "PLTE", 4)) {
+            palette.assign(data, data + len);
+        } else if (!memcmp(type, "IDAT", 4)) {
+            idat.insert(idat.end(), data, data + len);
+        } else if (!memcmp(type, "IEND", 4)) {
+            seen_end = true;
+        }
+        i += 12 + (size_t)len;
+    }
+    if (w == 0 || h == 0 || w >= (1u << 16) || h >= (1u << 16) || depth != 8 || interlace != 0) return HPM_ERR_IO;
+    int ch;
+    switch (ctype) {
+    case 0: ch = 1; break;
+    case 2: ch = 3; break;
+    case 3: ch = 1; break;
+    case 4: ch = 2; break;
+    case 6: ch = 4; break;
+    default: return HPM_ERR_IO;
+    }
+    if (ctype == 3 && (palette.size() < 3 || palette.size() % 3)) return HPM_ERR_IO;
+    const size_t stride = (size_t)w * ch;
+    std::vector<uint8_t> raw((stride + 1) * h);
+    uLongf raw_len = (uLongf)raw.size();
+    if (uncompress(raw.data(), &raw_len, idat.data(), (uLong)idat.size()) != Z_OK || raw_len != raw.size())
+        return HPM_ERR_IO;
+    /* undo the per-row filters (PNG spec, section 9) */
+    std::vector<uint8_t> img(stride * h);
+    for (uint32_t y = 0; y < h; ++y) {
+        const uint8_t f = raw[y * (stride + 1)];
+        const uint8_t *src = &raw[y * (stride + 1) + 1];
+        uint8_t *dst = &img[y * stride];
+        const uint8_t *up = y ? &img[(y - 1) * stride] : nullptr;
+        for (size_t x = 0; x < stride; ++x) {
+            const int a = x >= (size_t)ch ? dst[x - ch] : 0, u = up ? up[x] : 0,
+                      c = (up && x >= (size_t)ch) ? up[x - ch] : 0;
+            int pred;
+            switch (f) {
+            case 0: pred = 0; break;
+            case 1: pred = a; break;
+            case 2: pred = u; break;
+            case 3: pred = (a + u) >> 1; break;
+            case 4: pred = paeth(a, u, c); break;
+            default: return HPM_ERR_IO;
+            }
+            dst[x] = (uint8_t)(src[x] + pred);
+        }
+    }
+    px.resize((size_t)w * h);
+    for (size_t p = 0; p < (size_t)w * h; ++p) {
+        int r, g, bl;
+        if (ctype == 0 || ctype == 4) {
+            px[p] = img[p * ch];
+            continue;
+        }
+        if (ctype == 3) {
+            const size_t k = 3 * (size_t)img[p];
+            if (k + 2 >= palette.size()) return HPM_ERR_IO;
+            r = palette[k], g = palette[k + 1], bl = palette[k + 2];
+        } else {
+            r = img[p * ch], g = img[p * ch + 1], bl = img[p * ch + 2];
+        }
+        px[p] = (uint8_t)((9797 * r + 19234 * g + 3737 * bl) >> 15);
+    }
+    *w_out = (int)w;
+    *h_out = (int)h;
+    return HPM_OK;
+}
+
+}  // namespace
+
+extern "C" int hpm_resize_linear(const float *src, int sw, int sh, int ch, float *dst, int dw, int dh)
+{
+    if (!src || !dst || sw < 1 || sh < 1 || dw < 1 || dh < 1 || ch < 1) return HPM_ERR_ARG;
+    auto coef = [](int d, int sn, int dn, int &s0, int &s1, float &f) {
+        const double fd = (d + 0.5) * ((double)sn / dn) - 0.5;
+        int si = (int)std::floor(fd);
+        f = (float)(fd - si);
+        if (si < 0) f = 0.0f, si = 0;
+        if (si >= sn - 1) f = 0.0f, si = sn - 1;
+        s0 = si;
+        s1 = si + 1 < sn ? si + 1 : sn - 1;
+    };
+    std::vector<int> xs0(dw), xs1(dw);
+    std::vector<float> fxs(dw);
+    for (int x = 0; x < dw; ++x) coef(x, sw, dw, xs0[x], xs1[x], fxs[x]);
+    for (int y = 0; y < dh; ++y) {
+        int sy0, sy1;
+        float fy;
+        coef(y, sh, dh, sy0, sy1, fy);
+        const float *r0 = src + (size_t)sy0 * sw * ch, *r1 = src + (size_t)sy1 * sw * ch;
+        float *o = dst + (size_t)y * dw * ch;
+        for (int x = 0; x < dw; ++x) {
+            const float fx = fxs[x];
+            for (int c = 0; c < ch; ++c) {
+                const float a0 = r0[(size_t)xs0[x] * ch + c], b0 = r0[(size_t)xs1[x] * ch + c];
+                const float a1 = r1[(size_t)xs0[x] * ch + c], b1 = r1[(size_t)xs1[x] * ch + c];
+                const float h0 = std::fmaf(fx, b0 - a0, a0), h1 = std::fmaf(fx, b1 - a1, a1);
+                o[(size_t)x * ch + c] = std::fmaf(fy, h1 - h0, h0);
+            }
+        }
+    }
+    return HPM_OK;
+}
+
+extern "C" int hpm_read_gray8(const char *path, uint8_t *pixels, size_t cap, int *w, int *h)
+{
+    if (!path || !w || !h) return HPM_ERR_ARG;
+    std::vector<uint8_t> bytes, px;
+    if (!read_file(path, bytes) || bytes.size() < 2) return HPM_ERR_IO;
+    int r;
+    if (bytes[0] == 'P' && bytes[1] == '5')
+        r = decode_pgm(bytes, px, w, h);
+    else
+        r = decode_png(bytes, px, w, h);
+    if (r) return r;
+    if (!pixels) return HPM_OK;
+    if (cap < px.size()) return HPM_ERR_ARG;
+    memcpy(pixels, px.data(), px.size());
+    return HPM_OK;
+}

@@ -3,8 +3,7 @@
  * ProcessProblem, HPM-MVS/main.cpp:73-480, and HPM.cpp:759-1123).
  *
  *   k_resize          cv::resize INTER_LINEAR of depth / cost / normal maps
- *                     (main.cpp:84-86, 238-240); an exact 2:1 reduction is
- *                     OpenCV's area fast path (mean of 2x2)
+ *                     (main.cpp:84-86, 238-240)
  *   k_support_blocks  GetSupportPoints* (HPM.cpp:759-785, 1125-1179): argmin
  *                     cost per 5x5 block, kept when < 0.1
  *   k_tri_planes      GetPriorPlaneParams_factor (HPM.cpp:811-844)
@@ -31,40 +30,39 @@ namespace {
 
 /* ---------------- resize ---------------- */
 
+/* Source index pair and weight of output coordinate d (cv::resize
+ * INTER_LINEAR for float data, as OpenCV 4.x computes it: the fraction is
+ * taken in double precision and rounded once to float; edges clamp). */
+__device__ __forceinline__ void resize_coef(int d, int sn, int dn, int &s0, int &s1, float &f)
+{
+    const double fd = (d + 0.5) * ((double)sn / dn) - 0.5;
+    int s = (int)floor(fd);
+    f = (float)(fd - s);
+    if (s < 0) f = 0.0f, s = 0;
+    if (s >= sn - 1) f = 0.0f, s = sn - 1;
+    s0 = s;
+    s1 = min(s + 1, sn - 1);
+}
+
+/* Each pass blends a + f * (b - a) with one fused multiply-add, rows first,
+ * then columns; bit-exact with cv::resize (OpenCV 4.13) on float maps for
+ * every ratio tried, 2:1 and 4:1 included. */
 __global__ void k_resize(const float *__restrict__ src, int sw, int sh, int ch, float *__restrict__ dst, int dw,
-                         int dh, double scale_x, double scale_y, int area2)
+                         int dh)
 {
     const int dx = blockIdx.x * blockDim.x + threadIdx.x;
     const int dy = blockIdx.y * blockDim.y + threadIdx.y;
     if (dx >= dw || dy >= dh) return;
-    if (area2) { /* exact halving: mean of the 2x2 block */
-        const int sx = 2 * dx, sy = 2 * dy;
-        for (int c = 0; c < ch; ++c) {
-            const float a = src[((size_t)sy * sw + sx) * ch + c], b = src[((size_t)sy * sw + sx + 1) * ch + c];
-            const float e = src[((size_t)(sy + 1) * sw + sx) * ch + c];
-            const float f = src[((size_t)(sy + 1) * sw + sx + 1) * ch + c];
-            dst[((size_t)dy * dw + dx) * ch + c] = __fmul_rn(__fadd_rn(__fadd_rn(__fadd_rn(a, b), e), f), 0.25f);
-        }
-        return;
-    }
-    float fx = (float)((dx + 0.5) * scale_x - 0.5);
-    int sx = (int)floorf(fx);
-    fx = __fsub_rn(fx, (float)sx);
-    if (sx < 0) fx = 0.0f, sx = 0;
-    if (sx >= sw - 1) fx = 0.0f, sx = sw - 1;
-    float fy = (float)((dy + 0.5) * scale_y - 0.5);
-    int sy = (int)floorf(fy);
-    fy = __fsub_rn(fy, (float)sy);
-    if (sy < 0) fy = 0.0f, sy = 0;
-    if (sy >= sh - 1) fy = 0.0f, sy = sh - 1;
-    const int sx1 = min(sx + 1, sw - 1), sy1 = min(sy + 1, sh - 1);
-    const float ax0 = __fsub_rn(1.0f, fx), ay0 = __fsub_rn(1.0f, fy);
+    int sx0, sx1, sy0, sy1;
+    float fx, fy;
+    resize_coef(dx, sw, dw, sx0, sx1, fx);
+    resize_coef(dy, sh, dh, sy0, sy1, fy);
     for (int c = 0; c < ch; ++c) {
-        const float r0 = __fadd_rn(__fmul_rn(src[((size_t)sy * sw + sx) * ch + c], ax0),
-                                   __fmul_rn(src[((size_t)sy * sw + sx1) * ch + c], fx));
-        const float r1 = __fadd_rn(__fmul_rn(src[((size_t)sy1 * sw + sx) * ch + c], ax0),
-                                   __fmul_rn(src[((size_t)sy1 * sw + sx1) * ch + c], fx));
-        dst[((size_t)dy * dw + dx) * ch + c] = __fadd_rn(__fmul_rn(r0, ay0), __fmul_rn(r1, fy));
+        const float a0 = src[((size_t)sy0 * sw + sx0) * ch + c], b0 = src[((size_t)sy0 * sw + sx1) * ch + c];
+        const float a1 = src[((size_t)sy1 * sw + sx0) * ch + c], b1 = src[((size_t)sy1 * sw + sx1) * ch + c];
+        const float r0 = __fmaf_rn(fx, __fsub_rn(b0, a0), a0);
+        const float r1 = __fmaf_rn(fx, __fsub_rn(b1, a1), a1);
+        dst[((size_t)dy * dw + dx) * ch + c] = __fmaf_rn(fy, __fsub_rn(r1, r0), r0);
     }
 }
 
@@ -394,9 +392,7 @@ static dim3 grid2(int w, int h) { return dim3((w + 15) / 16, (h + 15) / 16); }
 
 cudaError_t prior_resize(const float *src, int sw, int sh, int ch, float *dst, int dw, int dh, cudaStream_t s)
 {
-    const double scale_x = (double)sw / dw, scale_y = (double)sh / dh; /* 1 / (dsize / ssize) */
-    const bool area2 = (sw == 2 * dw && sh == 2 * dh);
-    k_resize<<<grid2(dw, dh), dim3(16, 16), 0, s>>>(src, sw, sh, ch, dst, dw, dh, scale_x, scale_y, area2 ? 1 : 0);
+    k_resize<<<grid2(dw, dh), dim3(16, 16), 0, s>>>(src, sw, sh, ch, dst, dw, dh);
     return cudaGetLastError();
 }
 

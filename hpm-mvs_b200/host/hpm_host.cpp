@@ -1,0 +1,397 @@
+/*
+ * HPM class, GenerateSampleList and ProcessProblem over the C ABI; see
+ * hpm_host.h for what mirrors what.
+ */
+#include "hpm_host.h"
+
+#include <sys/stat.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <iomanip>
+#include <iostream>
+#include <sstream>
+
+namespace hpm_host {
+
+namespace {
+
+std::string id_path(const std::string &folder, int id, const char *suffix)
+{
+    std::ostringstream s;
+    s << folder << "/" << std::setw(8) << std::setfill('0') << id << suffix;
+    return s.str();
+}
+
+std::string result_folder(const std::string &dense_folder, int ref_id)
+{
+    std::ostringstream s;
+    s << dense_folder << "/HPM/2333_" << std::setw(8) << std::setfill('0') << ref_id;
+    return s.str();
+}
+
+float4 f4(float x, float y, float z, float w)
+{
+    float4 r;
+    r.x = x;
+    r.y = y;
+    r.z = z;
+    r.w = w;
+    return r;
+}
+
+bool exists(const std::string &p)
+{
+    struct stat st;
+    return stat(p.c_str(), &st) == 0;
+}
+
+void make_dir(const std::string &p)
+{
+    if (mkdir(p.c_str(), 0755) != 0 && !exists(p)) throw Error(HPM_ERR_IO, "cannot create " + p);
+}
+
+/* images/%08d.jpg in the reference; PNG and PGM are decoded here, JPEG by
+ * the Python front end (cv2) or after conversion. */
+std::vector<float> read_image(const std::string &dense_folder, int id, int *w, int *h)
+{
+    const std::string base = dense_folder + "/images";
+    for (const char *ext : {".png", ".pgm"}) {
+        const std::string p = id_path(base, id, ext);
+        if (!exists(p)) continue;
+        int rc = hpm_read_gray8(p.c_str(), nullptr, 0, w, h);
+        if (rc != HPM_OK) throw Error(rc, "cannot decode " + p);
+        std::vector<uint8_t> px((size_t)*w * *h);
+        rc = hpm_read_gray8(p.c_str(), px.data(), px.size(), w, h);
+        if (rc != HPM_OK) throw Error(rc, "cannot decode " + p);
+        return std::vector<float>(px.begin(), px.end()); /* convertTo(CV_32FC1), HPM.cpp:494 */
+    }
+    const std::string jpg = id_path(base, id, ".jpg");
+    if (exists(jpg))
+        throw Error(HPM_ERR_IO, jpg + ": JPEG is not decoded by the C++ host; run hpm-mvs_b200/hpm_mvs.py (OpenCV "
+                                      "decoding) or convert images/ to PNG");
+    throw Error(HPM_ERR_IO, "no image for view " + std::to_string(id) + " under " + base);
+}
+
+std::vector<float> read_dmb(const std::string &path, int *w, int *h, int want_nb)
+{
+    int nb = 0;
+    int rc = hpm_read_dmb(path.c_str(), nullptr, 0, h, w, &nb);
+    if (rc != HPM_OK || nb != want_nb) throw Error(rc ? rc : HPM_ERR_IO, "cannot read " + path);
+    std::vector<float> v((size_t)*w * *h * nb);
+    rc = hpm_read_dmb(path.c_str(), v.data(), v.size(), h, w, &nb);
+    if (rc != HPM_OK) throw Error(rc, "cannot read " + path);
+    return v;
+}
+
+void write_dmb(const std::string &path, const std::vector<float> &v, int w, int h, int nb)
+{
+    const int rc = hpm_write_dmb(path.c_str(), v.data(), h, w, nb);
+    if (rc != HPM_OK) throw Error(rc, "cannot write " + path);
+}
+
+}  // namespace
+
+void GenerateSampleList(const std::string &dense_folder, std::vector<Problem> &problems)
+{
+    const std::string path = dense_folder + "/pair.txt";
+    int n = 0;
+    int rc = hpm_read_pair(path.c_str(), &n, nullptr, nullptr, nullptr, 0);
+    if (rc != HPM_OK) throw Error(rc, "cannot read " + path);
+    std::vector<int> refs(n), counts(n), srcs((size_t)n * (HPM_MAX_IMAGES - 1));
+    rc = hpm_read_pair(path.c_str(), &n, refs.data(), counts.data(), srcs.data(), n);
+    if (rc != HPM_OK) throw Error(rc, "cannot read " + path);
+    problems.clear();
+    for (int i = 0; i < n; ++i) {
+        Problem p;
+        p.ref_image_id = refs[i];
+        p.src_image_ids.assign(srcs.begin() + (size_t)i * (HPM_MAX_IMAGES - 1),
+                               srcs.begin() + (size_t)i * (HPM_MAX_IMAGES - 1) + counts[i]);
+        problems.push_back(p);
+    }
+}
+
+HPM::HPM(int device)
+{
+    hpm_default_params(&params_);
+    check(hpm_create(&ctx_, device), "hpm_create");
+}
+
+HPM::~HPM()
+{
+    if (ctx_) hpm_destroy(ctx_);
+}
+
+void HPM::check(int rc, const char *what) const
+{
+    if (rc == HPM_OK) return;
+    std::string msg = what;
+    if (ctx_) msg += std::string(": ") + hpm_last_error(ctx_);
+    throw Error(rc, msg);
+}
+
+void HPM::InuputInitialization(const std::string &dense_folder, const Problem &problem)
+{
+    images_.clear();
+    cameras_.clear();
+    std::vector<int> ids{problem.ref_image_id};
+    ids.insert(ids.end(), problem.src_image_ids.begin(), problem.src_image_ids.end());
+    if ((int)ids.size() > HPM_MAX_IMAGES) throw Error(HPM_ERR_ARG, "more than 32 source images");
+    for (int id : ids) {
+        int w = 0, h = 0;
+        std::vector<float> img = read_image(dense_folder, id, &w, &h);
+        HpmCamera cam{};
+        const std::string cp = id_path(dense_folder + "/cams", id, "_cam.txt");
+        int rc = hpm_read_camera(cp.c_str(), &cam);
+        if (rc != HPM_OK) throw Error(rc, "cannot read " + cp);
+        /* the image cap of HPM.cpp:525-551 */
+        const int cap = 3200;
+        if (w > cap || h > cap) {
+            const float factor = std::min((float)cap / w, (float)cap / h);
+            const int nw = (int)std::round(w * factor), nh = (int)std::round(h * factor);
+            const float sx = nw / (float)w, sy = nh / (float)h;
+            std::vector<float> scaled((size_t)nw * nh);
+            check(hpm_resize_linear(img.data(), w, h, 1, scaled.data(), nw, nh), "image cap");
+            img.swap(scaled);
+            cam.K[0] *= sx;
+            cam.K[2] *= sx;
+            cam.K[4] *= sy;
+            cam.K[5] *= sy;
+            w = nw;
+            h = nh;
+        }
+        cam.width = w;
+        cam.height = h;
+        images_.push_back(std::move(img));
+        cameras_.push_back(cam);
+    }
+    params_.depth_min = cameras_[0].depth_min * 0.6f;
+    params_.depth_max = cameras_[0].depth_max * 1.2f;
+    depths_.clear();
+    seed_planes_.clear();
+    seed_costs_.clear();
+    if (params_.geom_consistency) {
+        const char *suffix = params_.multi_geometry ? "/depths_geom.dmb" : "/depths.dmb";
+        for (size_t i = 0; i < ids.size(); ++i) {
+            int w = 0, h = 0;
+            depths_.push_back(read_dmb(result_folder(dense_folder, ids[i]) + suffix, &w, &h, 1));
+            if (w != cameras_[i].width || h != cameras_[i].height)
+                throw Error(HPM_ERR_ARG, "depth map size differs from its image: view " + std::to_string(ids[i]));
+        }
+    }
+}
+
+void HPM::CudaSpaceInitialization(const std::string &dense_folder, const Problem &problem)
+{
+    std::vector<const float *> ptrs;
+    for (auto &img : images_) ptrs.push_back(img.data());
+    check(hpm_set_views(ctx_, ptrs.data(), cameras_.data(), (int)images_.size()), "hpm_set_views");
+    if (!params_.geom_consistency) return;
+    std::vector<const float *> dptrs;
+    for (auto &d : depths_) dptrs.push_back(d.data());
+    check(hpm_set_geom_depths(ctx_, dptrs.data()), "hpm_set_geom_depths");
+    /* the previous pass's hypotheses of the reference view (HPM.cpp:661-697) */
+    const std::string folder = result_folder(dense_folder, problem.ref_image_id);
+    int w = 0, h = 0;
+    const std::vector<float> normal = read_dmb(folder + "/normals.dmb", &w, &h, 3);
+    const std::vector<float> cost = read_dmb(folder + "/costs.dmb", &w, &h, 1);
+    const std::vector<float> &depth = depths_[0];
+    if (w != cameras_[0].width || h != cameras_[0].height) throw Error(HPM_ERR_ARG, "normals.dmb size");
+    seed_planes_.resize((size_t)4 * w * h);
+    for (size_t i = 0; i < (size_t)w * h; ++i) {
+        seed_planes_[4 * i] = normal[3 * i];
+        seed_planes_[4 * i + 1] = normal[3 * i + 1];
+        seed_planes_[4 * i + 2] = normal[3 * i + 2];
+        seed_planes_[4 * i + 3] = depth[i];
+    }
+    seed_costs_ = cost;
+    check(hpm_set_hypotheses(ctx_, seed_planes_.data(), seed_costs_.data()), "hpm_set_hypotheses");
+}
+
+void HPM::fetch_result()
+{
+    const size_t n = (size_t)GetReferenceImageWidth() * GetReferenceImageHeight();
+    planes_host_.resize(4 * n);
+    costs_host_.resize(n);
+    check(hpm_get_result(ctx_, planes_host_.data(), costs_host_.data()), "hpm_get_result");
+}
+
+void HPM::RunPatchMatch()
+{
+    check(hpm_run_patchmatch(ctx_, &params_), "hpm_run_patchmatch");
+    fetch_result();
+}
+
+void HPM::RunProblem(bool planar_prior, uint64_t seed, int pyramid_levels)
+{
+    const size_t n = (size_t)GetReferenceImageWidth() * GetReferenceImageHeight();
+    std::vector<float> depth(n), normal(3 * n), cost(n);
+    prior_depth_.assign(n, 0.0f);
+    HpmProblemOpts o{};
+    o.planar_prior = planar_prior && !params_.geom_consistency;
+    o.geom_consistency = params_.geom_consistency;
+    o.multi_geometry = params_.multi_geometry;
+    o.seed = seed;
+    o.pyramid_levels = pyramid_levels;
+    check(hpm_process_problem(ctx_, &o, depth.data(), normal.data(), cost.data(), prior_depth_.data()),
+          "hpm_process_problem");
+    planes_host_.resize(4 * n);
+    costs_host_ = cost;
+    for (size_t i = 0; i < n; ++i) {
+        planes_host_[4 * i] = normal[3 * i];
+        planes_host_[4 * i + 1] = normal[3 * i + 1];
+        planes_host_[4 * i + 2] = normal[3 * i + 2];
+        planes_host_[4 * i + 3] = depth[i];
+    }
+}
+
+void HPM::SetGeomConsistencyParams(bool multi_geometry)
+{
+    params_.geom_consistency = 1;
+    params_.max_iterations = 2; /* recorded, not used: every pass runs 3 iterations (HPM.cu:1933) */
+    if (multi_geometry) params_.multi_geometry = 1;
+}
+
+void HPM::SetPlanarPriorParams() { params_.planar_prior = 1; }
+
+int HPM::GetReferenceImageWidth() const { return cameras_.empty() ? 0 : cameras_[0].width; }
+int HPM::GetReferenceImageHeight() const { return cameras_.empty() ? 0 : cameras_[0].height; }
+
+const std::vector<float> &HPM::GetReferenceImage() const
+{
+    if (images_.empty()) throw Error(HPM_ERR_STATE, "GetReferenceImage before InuputInitialization");
+    return images_[0];
+}
+
+float4 HPM::GetPlaneHypothesis(int index) const
+{
+    if (index < 0 || (size_t)index * 4 >= planes_host_.size()) throw Error(HPM_ERR_ARG, "plane index");
+    return f4(planes_host_[4 * (size_t)index], planes_host_[4 * (size_t)index + 1],
+                       planes_host_[4 * (size_t)index + 2], planes_host_[4 * (size_t)index + 3]);
+}
+
+float HPM::GetCost(int index) const
+{
+    if (index < 0 || (size_t)index >= costs_host_.size()) throw Error(HPM_ERR_ARG, "cost index");
+    return costs_host_[index];
+}
+
+int HPM::ComputingMultiScaleSettings(int width, int height) const
+{
+    int max_size = std::max(width, height), k = 0;
+    while (max_size > 1000) {
+        max_size /= 2;
+        k++;
+    }
+    return k;
+}
+
+float4 HPM::TransformNormal(float4 p) const
+{
+    const float *R = cameras_.at(0).R;
+    return f4(R[0] * p.x + R[3] * p.y + R[6] * p.z, R[1] * p.x + R[4] * p.y + R[7] * p.z,
+                       R[2] * p.x + R[5] * p.y + R[8] * p.z, p.w);
+}
+
+float4 HPM::TransformNormal2RefCam(float4 p) const
+{
+    const float *R = cameras_.at(0).R;
+    return f4(R[0] * p.x + R[1] * p.y + R[2] * p.z, R[3] * p.x + R[4] * p.y + R[5] * p.z,
+                       R[6] * p.x + R[7] * p.y + R[8] * p.z, p.w);
+}
+
+float HPM::GetDistance2Origin_factor(int2 p, float depth, float4 normal, float /*factor: unused, as in the reference*/) const
+{
+    const float *K = cameras_.at(0).K;
+    const float X0 = depth * (p.x - K[2]) / K[0], X1 = depth * (p.y - K[5]) / K[4], X2 = depth;
+    return -(normal.x * X0 + normal.y * X1 + normal.z * X2);
+}
+
+float HPM::GetDepthFromPlaneParam_factor(float4 n, int x, int y, float factor) const
+{
+    const float *K = cameras_.at(0).K;
+    return -n.w * (K[0] * factor) /
+           ((x - K[2] * factor) * n.x + (K[0] / K[4]) * (y - K[5] * factor) * n.y + K[0] * factor * n.z);
+}
+
+std::vector<int> HPM::DelaunayTriangulation(int w, int h, const std::vector<int> &points) const
+{
+    const int n = (int)points.size() / 2;
+    const int cnt = hpm_delaunay(points.data(), n, w, h, nullptr, 0);
+    if (cnt < 0) throw Error(cnt, "hpm_delaunay");
+    std::vector<int> tris((size_t)6 * cnt);
+    const int got = hpm_delaunay(points.data(), n, w, h, tris.data(), cnt);
+    if (got < 0) throw Error(got, "hpm_delaunay");
+    tris.resize((size_t)6 * got);
+    return tris;
+}
+
+void HPM::JointBilateralUpsampling(const std::vector<float> &guide, const std::vector<float> &src_depth,
+                                   const std::vector<float> &src_normal, int s_cols, int s_rows,
+                                   std::vector<float> &up_depth, std::vector<float> &up_normal) const
+{
+    const int cols = GetReferenceImageWidth(), rows = GetReferenceImageHeight();
+    up_depth.assign((size_t)cols * rows, 0.0f);
+    up_normal.assign((size_t)3 * cols * rows, 0.0f);
+    check(hpm_jbu(ctx_, guide.data(), cols, rows, src_depth.data(), src_normal.data(), s_cols, s_rows,
+                  up_depth.data(), up_normal.data()),
+          "hpm_jbu");
+}
+
+void HPM::SetPlanarPrior(const std::vector<float> &prior_planes, const std::vector<uint32_t> &masks)
+{
+    check(hpm_set_prior(ctx_, prior_planes.data(), masks.data()), "hpm_set_prior");
+    params_.planar_prior = 1;
+}
+
+void HPM::ReleasePriorCudaMemory()
+{
+    hpm_clear_prior(ctx_);
+    params_.planar_prior = 0;
+}
+
+void HPM::ReleaseProblemCudaMemory() {}
+
+void HPM::ReleaseProblemHostMemory()
+{
+    std::vector<std::vector<float>>().swap(images_);
+    std::vector<std::vector<float>>().swap(depths_);
+    std::vector<float>().swap(seed_planes_);
+    std::vector<float>().swap(seed_costs_);
+}
+
+void ProcessProblem(const std::string &dense_folder, const Problem &problem, bool geom_consistency,
+                    bool planar_prior, bool multi_geometry, uint64_t seed, int pyramid_levels, int device)
+{
+    std::cout << "Processing image " << std::setw(8) << std::setfill('0') << problem.ref_image_id << "..."
+              << std::endl;
+    const std::string folder = result_folder(dense_folder, problem.ref_image_id);
+    make_dir(dense_folder + "/HPM");
+    make_dir(folder);
+    HPM hpm(device);
+    if (geom_consistency) hpm.SetGeomConsistencyParams(multi_geometry);
+    hpm.InuputInitialization(dense_folder, problem);
+    hpm.CudaSpaceInitialization(dense_folder, problem);
+    hpm.RunProblem(planar_prior, seed, pyramid_levels);
+
+    const int w = hpm.GetReferenceImageWidth(), h = hpm.GetReferenceImageHeight();
+    const size_t n = (size_t)w * h;
+    std::vector<float> depths(n), normals(3 * n), costs(n);
+    for (size_t i = 0; i < n; ++i) {
+        const float4 p = hpm.GetPlaneHypothesis((int)i);
+        depths[i] = p.w;
+        normals[3 * i] = p.x;
+        normals[3 * i + 1] = p.y;
+        normals[3 * i + 2] = p.z;
+        costs[i] = hpm.GetCost((int)i);
+    }
+    if (planar_prior && !geom_consistency) write_dmb(folder + "/depths_prior.dmb", hpm.GetPriorDepths(), w, h, 1);
+    write_dmb(folder + (geom_consistency ? "/depths_geom.dmb" : "/depths.dmb"), depths, w, h, 1);
+    write_dmb(folder + "/normals.dmb", normals, w, h, 3);
+    write_dmb(folder + "/costs.dmb", costs, w, h, 1);
+    std::cout << "Processing image " << std::setw(8) << std::setfill('0') << problem.ref_image_id << " done!"
+              << std::endl;
+}
+
+}  // namespace hpm_host

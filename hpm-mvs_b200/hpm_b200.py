@@ -37,7 +37,7 @@ EXPORTED = [
     "hpm_initial_costs", "hpm_geom_costs", "hpm_depth_normal_filter", "hpm_profile_enable", "hpm_profile_read",
     "hpm_count_enable", "hpm_count_read", "hpm_write_dmb", "hpm_read_dmb", "hpm_read_camera", "hpm_read_pair",
     "hpm_fp32_peak", "hpm_jbu_noalloc", "hpm_process_problem", "hpm_last_prior_stats", "hpm_delaunay",
-    "hpm_prior_level", "hpm_run_scene",
+    "hpm_prior_level", "hpm_run_scene", "hpm_read_gray8", "hpm_resize_linear",
 ]
 
 
@@ -375,6 +375,30 @@ def read_camera(path: str) -> np.ndarray:
     if rc != HPM_OK:
         raise HpmError(f"hpm_read_camera({path}): {STATUS_NAMES.get(rc, rc)}")
     return cam[0]
+
+
+def read_gray8(path: str) -> np.ndarray:
+    """images/ file as cv::imread(path, IMREAD_GRAYSCALE) gives it (PGM, PNG)."""
+    w, h = ctypes.c_int(), ctypes.c_int()
+    rc = lib().hpm_read_gray8(path.encode(), None, ctypes.c_size_t(0), ctypes.byref(w), ctypes.byref(h))
+    if rc != HPM_OK:
+        raise HpmError(f"hpm_read_gray8({path}) failed: {rc}")
+    out = np.empty((h.value, w.value), np.uint8)
+    rc = lib().hpm_read_gray8(path.encode(), _p(out), ctypes.c_size_t(out.nbytes), ctypes.byref(w), ctypes.byref(h))
+    if rc != HPM_OK:
+        raise HpmError(f"hpm_read_gray8({path}) failed: {rc}")
+    return out
+
+
+def resize_linear(src: np.ndarray, dw: int, dh: int) -> np.ndarray:
+    """cv::resize INTER_LINEAR of a float32 [H, W] or [H, W, C] map (host)."""
+    src = np.ascontiguousarray(src, dtype=np.float32)
+    ch = 1 if src.ndim == 2 else src.shape[2]
+    out = np.empty((dh, dw) if src.ndim == 2 else (dh, dw, ch), np.float32)
+    rc = lib().hpm_resize_linear(_p(src), src.shape[1], src.shape[0], ch, _p(out), dw, dh)
+    if rc != HPM_OK:
+        raise HpmError(f"hpm_resize_linear failed: {rc}")
+    return out
 
 
 def read_pair(path: str):

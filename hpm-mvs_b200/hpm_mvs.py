@@ -1,0 +1,110 @@
+#!/usr/bin/env python
+"""main() of HPM-MVS (main.cpp:636-677) from Python, for dense folders whose
+images/ are JPEG (decoded with OpenCV, as the reference does, HPM.cpp:492);
+the C++ host (hpm_mvs) reads PNG and PGM itself.
+
+    python hpm-mvs_b200/hpm_mvs.py dense_folder [--seed S] [--levels K]
+                                   [--geom-iterations G] [--no-prior] [--device D]
+
+Writes HPM/2333_%08d/{depths,depths_geom,normals,costs,depths_prior}.dmb like
+the reference's ProcessProblem.  Seeds as in the C++ host: problem p of pass
+set A uses S + p, of geometric iteration g S + 1000003 (g + 1) + p.
+"""
+from __future__ import annotations
+
+import argparse
+import os
+import sys
+
+import numpy as np
+
+sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
+import hpm_b200 as hb  # noqa: E402
+
+MAX_IMAGE_SIZE = 3200  # PatchMatchParams::max_image_size (HPM.h:35)
+
+
+def load_view(folder: str, vid: int):
+    """Gray float image and camera of one view, after the 3200-pixel cap
+    (InuputInitialization, HPM.cpp:482-551)."""
+    img = None
+    for ext in (".jpg", ".png", ".pgm"):
+        p = os.path.join(folder, "images", f"{vid:08d}{ext}")
+        if os.path.exists(p):
+            if ext == ".jpg":
+                import cv2
+
+                img = cv2.imread(p, cv2.IMREAD_GRAYSCALE)
+                if img is None:
+                    raise hb.HpmError(f"cannot decode {p}")
+            else:
+                img = hb.read_gray8(p)
+            break
+    if img is None:
+        raise hb.HpmError(f"no image for view {vid} under {folder}/images")
+    img = img.astype(np.float32)
+    cam = hb.read_camera(os.path.join(folder, "cams", f"{vid:08d}_cam.txt")).copy()
+    h, w = img.shape
+    if w > MAX_IMAGE_SIZE or h > MAX_IMAGE_SIZE:
+        factor = min(np.float32(MAX_IMAGE_SIZE) / np.float32(w), np.float32(MAX_IMAGE_SIZE) / np.float32(h))
+        nw, nh = int(round(w * float(factor))), int(round(h * float(factor)))
+        img = hb.resize_linear(img, nw, nh)
+        sx, sy = np.float32(nw) / np.float32(w), np.float32(nh) / np.float32(h)
+        K = cam["K"]
+        K[0] *= sx
+        K[2] *= sx
+        K[4] *= sy
+        K[5] *= sy
+        w, h = nw, nh
+    cam["width"], cam["height"] = w, h
+    return img, cam
+
+
+def process_problem(ctx, folder, ref, srcs, views, *, geom, planar_prior, multi_geometry, seed, levels):
+    """ProcessProblem (main.cpp:35-499) for one reference view."""
+    out = os.path.join(folder, "HPM", f"2333_{ref:08d}")
+    os.makedirs(out, exist_ok=True)
+    ids = [ref] + list(srcs)
+    ctx.set_views([views[i][0] for i in ids], np.array([views[i][1] for i in ids]))
+    if geom:
+        suffix = "depths_geom.dmb" if multi_geometry else "depths.dmb"
+        depths = [hb.read_dmb(os.path.join(folder, "HPM", f"2333_{i:08d}", suffix)) for i in ids]
+        normal = hb.read_dmb(os.path.join(out, "normals.dmb"))
+        cost = hb.read_dmb(os.path.join(out, "costs.dmb"))
+        ctx.set_geom_depths(depths)
+        ctx.set_hypotheses(np.concatenate([normal, depths[0][..., None]], -1), cost)
+    d, n, c, pd = ctx.process_problem(planar_prior=planar_prior and not geom, geom=geom,
+                                      multi_geometry=multi_geometry, seed=seed, pyramid_levels=levels)
+    if planar_prior and not geom:
+        hb.write_dmb(os.path.join(out, "depths_prior.dmb"), pd)
+    hb.write_dmb(os.path.join(out, "depths_geom.dmb" if geom else "depths.dmb"), d)
+    hb.write_dmb(os.path.join(out, "normals.dmb"), n)
+    hb.write_dmb(os.path.join(out, "costs.dmb"), c)
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
+    ap.add_argument("dense_folder")
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--levels", type=int, default=-1)
+    ap.add_argument("--geom-iterations", type=int, default=2)
+    ap.add_argument("--no-prior", action="store_true")
+    ap.add_argument("--device", type=int, default=0)
+    a = ap.parse_args(argv)
+    problems = hb.read_pair(os.path.join(a.dense_folder, "pair.txt"))
+    needed = sorted({p[0] for p in problems} | {s for p in problems for s in p[1]})
+    views = {v: load_view(a.dense_folder, v) for v in needed}
+    print(f"There are {len(problems)} problems needed to be processed!")
+    with hb.Context(a.device) as ctx:
+        for p, (ref, srcs) in enumerate(problems):
+            process_problem(ctx, a.dense_folder, ref, srcs, views, geom=False, planar_prior=not a.no_prior,
+                            multi_geometry=False, seed=a.seed + p, levels=a.levels)
+        for g in range(a.geom_iterations):
+            for p, (ref, srcs) in enumerate(problems):
+                process_problem(ctx, a.dense_folder, ref, srcs, views, geom=True, planar_prior=False,
+                                multi_geometry=g > 0, seed=a.seed + 1000003 * (g + 1) + p, levels=a.levels)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

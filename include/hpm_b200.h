@@ -274,6 +274,16 @@ int hpm_write_dmb(const char *path, const float *data, int h, int w, int nb);
 int hpm_read_dmb(const char *path, float *data, size_t cap, int *h, int *w, int *nb);
 /* cams/%08d_cam.txt (ReadCamera, HPM.cpp:160-185).  width/height are left 0. */
 int hpm_read_camera(const char *path, HpmCamera *cam);
+/* An 8-bit grayscale image as cv::imread(path, IMREAD_GRAYSCALE) returns it
+ * for the reference's images/ folder (HPM.cpp:492): binary PGM or 8-bit PNG
+ * (colour reduced as OpenCV's PNG reader does).  Sets *w, *h; copies the
+ * pixels when pixels is non-NULL (capacity cap bytes). */
+int hpm_read_gray8(const char *path, uint8_t *pixels, size_t cap, int *w, int *h);
+/* cv::resize(src, dst, Size(dw, dh), 0, 0, INTER_LINEAR) of a float map
+ * with ch interleaved channels, on the host: the image cap of
+ * InuputInitialization (HPM.cpp:525-551).  Same arithmetic as OpenCV 4.x
+ * (double-precision fractions, one fused a + f*(b-a) per direction). */
+int hpm_resize_linear(const float *src, int sw, int sh, int ch, float *dst, int dw, int dh);
 /* pair.txt (GenerateSampleList, main.cpp:4-33): returns the problem count
  * into *n; ref_ids[n], src_counts[n], src_ids[n][HPM_MAX_IMAGES-1] filled when
  * non-NULL (sources with score <= 0 are dropped). */

@@ -110,3 +110,17 @@ def test_default_params_are_the_reference_defaults():
     assert (p.max_iterations, p.patch_size, p.radius_increment, p.top_k) == (3, 11, 2, 4)
     assert (p.sigma_spatial, p.sigma_color) == (5.0, 3.0)
     assert p.geom_consistency == 0 and p.planar_prior == 0
+
+
+def test_host_binary_builds_and_runs_without_a_gpu_call():
+    """The C++ host mirror links against the C ABI and answers --help; a
+    missing dense folder is a clean error, not a crash."""
+    import os
+    import subprocess
+
+    exe = os.path.join(os.path.dirname(os.path.abspath(hb.__file__)), "hpm_mvs")
+    assert os.path.exists(exe), "make -C hpm-mvs_b200 builds hpm_mvs"
+    r = subprocess.run([exe, "--help"], capture_output=True, text=True, timeout=60)
+    assert r.returncode == 0 and "dense_folder" in r.stdout
+    r = subprocess.run([exe, "/nonexistent/folder"], capture_output=True, text=True, timeout=60)
+    assert r.returncode == 1 and "pair.txt" in r.stderr

@@ -171,3 +171,43 @@ def test_scene_driver_matches_per_view_loop():
         np.testing.assert_array_equal(scost[v], cost[v])
     accs = [syn.depth_accuracy(sd[v], sc.gt_depth[v]) for v in range(nv)]
     assert min(accs) > 0.5, accs
+
+
+def test_host_main_writes_the_scene_driver_maps(tmp_path):
+    """The C++ host (hpm_mvs: HPM class, ProcessProblem, main() over the C
+    ABI, reading images/ + cams/ + pair.txt and writing .dmb files) and the
+    Python front end give exactly the maps of hpm_run_scene on the same
+    decoded inputs and seeds."""
+    import os
+    import subprocess
+    import sys
+
+    here = os.path.dirname(os.path.abspath(hb.__file__))
+    sc = syn.make_scene(16, 160, 120, 4, n_planes=5, low_texture=0.3)
+    folder = str(tmp_path / "scene")
+    syn.write_dense_folder(sc, folder, ".png")
+    r = subprocess.run([os.path.join(here, "hpm_mvs"), folder, "--seed", "7", "--levels", "1"], capture_output=True,
+                       text=True, timeout=600)
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
+    pairs = hb.read_pair(os.path.join(folder, "pair.txt"))
+    imgs = [hb.read_gray8(os.path.join(folder, "images", f"{v:08d}.png")).astype(np.float32) for v in range(4)]
+    cams = np.array([hb.read_camera(os.path.join(folder, "cams", f"{v:08d}_cam.txt")) for v in range(4)])
+    for v in range(4):
+        cams[v]["width"], cams[v]["height"] = 160, 120
+    with hb.Context() as ctx:
+        sd, sn, scost = ctx.run_scene(imgs, cams, pairs, seed=7, pyramid_levels=1, geom_iterations=2)
+    for v in range(4):
+        out = os.path.join(folder, "HPM", f"2333_{v:08d}")
+        np.testing.assert_array_equal(hb.read_dmb(os.path.join(out, "depths_geom.dmb")), sd[v])
+        np.testing.assert_array_equal(hb.read_dmb(os.path.join(out, "normals.dmb")), sn[v])
+        np.testing.assert_array_equal(hb.read_dmb(os.path.join(out, "costs.dmb")), scost[v])
+        assert hb.read_dmb(os.path.join(out, "depths.dmb")).shape == (120, 160)
+        assert (hb.read_dmb(os.path.join(out, "depths_prior.dmb")) > 0).mean() > 0.3
+    # the Python front end over the same folder
+    py = str(tmp_path / "scene_py")
+    syn.write_dense_folder(sc, py, ".png")
+    r = subprocess.run([sys.executable, os.path.join(here, "hpm_mvs.py"), py, "--seed", "7", "--levels", "1"],
+                       capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
+    for v in range(4):
+        np.testing.assert_array_equal(hb.read_dmb(os.path.join(py, "HPM", f"2333_{v:08d}", "depths_geom.dmb")), sd[v])

@@ -1,0 +1,47 @@
+"""Host-side I/O of the drop-in: images/ decoding and the 3200-pixel image
+cap (InuputInitialization, HPM.cpp:482-554) against the OpenCV calls the
+reference makes (cv2 4.13 here)."""
+import os
+
+import numpy as np
+import pytest
+
+import hpm_b200 as hb
+
+cv2 = pytest.importorskip("cv2")
+
+
+@pytest.mark.parametrize("shape", [(37, 53), (64, 80, 3), (21, 33, 4), (100, 7, 3)])
+@pytest.mark.parametrize("ext", [".png", ".pgm"])
+def test_read_gray8_matches_imread(tmp_path, shape, ext):
+    if ext == ".pgm" and len(shape) == 3:
+        pytest.skip("PGM is single-channel")
+    rng = np.random.default_rng(sum(shape))
+    img = rng.integers(0, 256, shape, dtype=np.uint8)
+    for level in ([0, 6, 9] if ext == ".png" else [None]):
+        path = str(tmp_path / f"img{ext}")
+        cv2.imwrite(path, img, [] if level is None else [cv2.IMWRITE_PNG_COMPRESSION, level])
+        np.testing.assert_array_equal(hb.read_gray8(path), cv2.imread(path, cv2.IMREAD_GRAYSCALE))
+
+
+def test_read_gray8_rejects_bad_files(tmp_path):
+    bad = tmp_path / "x.png"
+    bad.write_bytes(b"\x89PNG\r\n\x1a\nnot a png")
+    with pytest.raises(hb.HpmError):
+        hb.read_gray8(str(bad))
+    with pytest.raises(hb.HpmError):
+        hb.read_gray8(str(tmp_path / "missing.png"))
+    jpg = str(tmp_path / "x.jpg")
+    cv2.imwrite(jpg, np.zeros((8, 8), np.uint8))
+    with pytest.raises(hb.HpmError):  # JPEG is decoded by the Python front end, not the C ABI
+        hb.read_gray8(jpg)
+
+
+@pytest.mark.parametrize("src,dst,ch", [((1600, 1200), (400, 300), 1), ((1600, 1200), (800, 600), 3),
+                                        ((6048, 4032), (3200, 2133), 1), ((605, 403), (1000, 666), 1),
+                                        ((7, 5), (3, 2), 3)])
+def test_resize_linear_matches_cv2(src, dst, ch):
+    rng = np.random.default_rng(src[0])
+    shape = (src[1], src[0]) if ch == 1 else (src[1], src[0], ch)
+    a = rng.uniform(-300, 300, shape).astype(np.float32)
+    np.testing.assert_array_equal(hb.resize_linear(a, *dst), cv2.resize(a, dst, interpolation=cv2.INTER_LINEAR))
