@@ -264,7 +264,7 @@ def run_ours(args, dist):
     # atomics slow the kernels down) and the kernel launch list
     ctx.count_enable(True)
     step(0)
-    n_cv, n_geom = ctx.count_read()
+    n_ncc, n_geom = ctx.count_read()
     ctx.count_enable(False)
     try:
         launches = count_launches(lambda: step(0))
@@ -312,8 +312,8 @@ def run_ours(args, dist):
     n_pass = nv * passes_per_view()
     prop_ms, prop_n = prof["propagate"]
     half_steps = prop_n // max(args.steps, 1)
-    cv_half = n_cv - n_pass * npx  # k_init evaluates one cost vector per pixel and pass
-    flops_step = cv_half * S * (TAPS * NCC_FLOPS_PER_TAP + FLOPS_PER_HYP_VIEW) + n_geom * GEOM_TERM_FLOPS
+    ncc_half = n_ncc - n_pass * npx * S  # k_init scores one hypothesis per pixel and pass
+    flops_step = ncc_half * (TAPS * NCC_FLOPS_PER_TAP + FLOPS_PER_HYP_VIEW) + n_geom * GEOM_TERM_FLOPS
     prop_ms_step = prop_ms / args.steps
     achieved = flops_step / (prop_ms_step * 1e-3) / 1e12
     n_launch = sum(launches.values())
@@ -351,8 +351,8 @@ def run_ours(args, dist):
                      "half_step_ms": prop_ms_step / max(half_steps, 1), "half_steps_per_step": half_steps,
                      "propagate_ms_per_step": prop_ms_step,
                      "propagate_share": prop_ms_step / (ms / args.steps),
-                     "cost_vectors_per_step": cv_half, "geom_terms_per_step": n_geom,
-                     "flops_per_cost_vector": S * (TAPS * NCC_FLOPS_PER_TAP + FLOPS_PER_HYP_VIEW)},
+                     "ncc_windows_per_step": ncc_half, "geom_terms_per_step": n_geom,
+                     "flops_per_ncc_window": TAPS * NCC_FLOPS_PER_TAP + FLOPS_PER_HYP_VIEW},
         "impl": "ours",
     }
     return line

@@ -17,7 +17,8 @@ namespace hpm {
 constexpr int kMaxViews = HPM_MAX_IMAGES; /* reference + 32 sources */
 constexpr int kMaxSrc = kMaxViews - 1;
 constexpr int kTaps = 36; /* 6 x 6 taps of the 11x11 window, stride 2 */
-constexpr int kCandRows = 10; /* 8 NESP directions + 2 refinement scratch rows */
+constexpr int kCandRows = 13;  /* 8 NESP directions + 5 refinement candidates */
+constexpr int kRefineRow = 8; /* first refinement row */
 
 /* Per-view data of one problem, passed to kernels by value. */
 struct ViewDev {
@@ -57,7 +58,7 @@ struct PMArgs {
     float *cost_cache; /* [S][H][W] cost vector of the current hypothesis, or nullptr */
     /* hand-off between the two kernels of a half-step (L2-resident):
      * cand_costs [kCandRows*S][H*W] cost matrix rows (8 NESP directions and
-     * two refinement scratch rows), cand_pos [8][H*W] chosen sites,
+     * the 5 refinement candidates), cand_pos [8][H*W] chosen sites,
      * cand_flags [H*W] bit k = direction k valid */
     float *cand_costs;
     int *cand_pos;

@@ -42,6 +42,25 @@ constexpr double kPiD = 3.14159265358979323846; /* M_PI, HPM-MVS/main.h:41 */
 constexpr int kBlockX = 32;
 constexpr int kBlockY = 2;
 constexpr int kBlock = kBlockX * kBlockY;
+
+/* Pixels of one half-step (one checkerboard colour) per warp: kWarpW per
+ * row over kWarpH rows, so that the 32 lanes sample a compact 2D patch of
+ * each source image (the texture cache is tiled in 2D).  A block is two
+ * such warps stacked vertically. */
+#ifndef HPM_WARP_W
+#define HPM_WARP_W 8
+#endif
+constexpr int kWarpW = HPM_WARP_W;
+constexpr int kWarpH = 32 / kWarpW;
+static_assert(kWarpW * kWarpH == 32 && kBlock == 64, "two warps per block");
+
+/* (px, py) of this thread in a half-step of `color` */
+__device__ __forceinline__ void half_step_pixel(int color, int &px, int &py)
+{
+    const int lane = threadIdx.x, wv = threadIdx.y;
+    py = blockIdx.y * (2 * kWarpH) + wv * kWarpH + lane / kWarpW;
+    px = blockIdx.x * (2 * kWarpW) + 2 * (lane % kWarpW) + ((py + color) & 1);
+}
 #ifndef HPM_CV_INLINE
 #define HPM_CV_INLINE __noinline__
 #endif
@@ -345,13 +364,24 @@ __device__ __forceinline__ float ncc(const PMArgs &a, int v, int px, int py, flo
     return fmaxf(0.0f, fminf(2.0f, 1.0f - covar / vv));
 }
 
+/* One NCC window for the loops that score several candidates view by view
+ * (inline by default; -DHPM_NCC_CALL=__noinline__ builds it out of line). */
+#ifndef HPM_NCC_CALL
+#define HPM_NCC_CALL __forceinline__
+#endif
+__device__ HPM_NCC_CALL float ncc_call(const PMArgs &a, int v, int px, int py, float4 h, const float2 *sWW, int tid,
+                                        RefStats rs)
+{
+    return ncc(a, v, px, py, h, sWW, tid, rs);
+}
+
 /* ComputeMultiViewCostVector (HPM.cu:438-443) into out[v * stride].  Kept
  * out of line so that the 36-tap loop exists once in the binary. */
 __device__ HPM_CV_INLINE void cost_vector(const PMArgs &a, int px, int py, float4 h, const float2 *sWW, int tid,
                                          RefStats rs, float *out, int stride)
 {
     for (int v = 1; v < a.n; ++v) out[(v - 1) * stride] = ncc(a, v, px, py, h, sWW, tid, rs);
-    if (a.counters) atomicAdd(&a.counters[0], 1ull);
+    if (a.counters) atomicAdd(&a.counters[0], (unsigned long long)(a.n - 1));
 }
 
 __device__ __forceinline__ void sort_small(float *d, int n) /* HPM.cu:3-12 */
@@ -643,18 +673,14 @@ __global__ void __launch_bounds__(kBlock, HPM_P1_MIN_BLOCKS) k_prop_dirs(const _
 {
     __shared__ float2 sWW[kTaps * kBlock];
     const int tid = threadIdx.y * kBlockX + threadIdx.x;
-    const int py = blockIdx.y * kBlockY + threadIdx.y;
-    const int px = blockIdx.x * (2 * kBlockX) + 2 * threadIdx.x + ((py + color) & 1);
+    int px, py;
+    half_step_pixel(color, px, py);
     if (px >= a.W || py >= a.rows_cov) return;
     const int W = a.W, H = a.H, S = a.n - 1;
     const size_t npx = (size_t)W * H;
     const int center = py * W + px;
     const RefStats rs = ref_window(a, px, py, sWW, tid);
     const float4 cur = a.planes[center];
-
-    for (int k = 0; k < 8; ++k)
-        for (int v = 0; v < S; ++v) CAG(k, v) = 0.0f;
-    CAG(0, 0) = 2.0f; /* float cost_array[8][32] = { 2.0f } (HPM.cu:1244) */
 
     int pos[8];
     uint32_t flags = 0;
@@ -666,27 +692,50 @@ __global__ void __launch_bounds__(kBlock, HPM_P1_MIN_BLOCKS) k_prop_dirs(const _
     pos[5] = center - 5;
     pos[6] = center - 6 + 5 * W;
     pos[7] = center + 5;
-    /* Identical planes give identical cost vectors: a candidate whose plane
-     * equals the current hypothesis (cost vector cached) or an earlier
-     * candidate reuses those values. */
+    /* 1) NESP sites of the 8 directions.  Identical planes give identical
+     * cost vectors: a candidate whose plane equals the current hypothesis
+     * (cost vector cached) or an earlier candidate reuses those values.
+     * src: 0..7 copy that row, 8 the cache, 9 evaluate. */
+    uint32_t src_code = 0; /* 4 bits per direction */
+    uint32_t eval_mask = 0;
 #pragma unroll
     for (int k = 0; k < 8; ++k) {
         if (!first_site_valid(k, 0, px, py, W, H)) continue;
         flags |= 1u << k;
         pos[k] = select_site(a, k, 0, px, py);
         const float4 c = a.planes[pos[k]];
-        if (same_plane(c, cur)) {
-            for (int v = 0; v < S; ++v) CAG(k, v) = *cache_at(a, v, center);
-            continue;
-        }
-        int src = -1;
+        int src = same_plane(c, cur) ? 8 : -1;
 #pragma unroll
         for (int j = 0; j < k; ++j)
             if (src < 0 && ((flags >> j) & 1u) && same_plane(c, a.planes[pos[j]])) src = j;
-        if (src >= 0) {
+        if (src < 0) {
+            src = 9;
+            eval_mask |= 1u << k;
+        }
+        src_code |= (uint32_t)src << (4 * k);
+    }
+    /* 2) the distinct candidates, view by view, so that the threads of a
+     * block sample one source image at a time (texture-cache locality) */
+    for (int v = 0; v < S; ++v) {
+        uint32_t m = eval_mask;
+        while (m) {
+            const int k = __ffs(m) - 1;
+            m &= m - 1;
+            CAG(k, v) = ncc_call(a, v + 1, px, py, a.planes[pos[k]], sWW, tid, rs);
+        }
+    }
+    if (a.counters && eval_mask) atomicAdd(&a.counters[0], (unsigned long long)(__popc(eval_mask) * S));
+    /* 3) copies in direction order, zeros for invalid directions
+     * (float cost_array[8][32] = { 2.0f } sets only [0][0], HPM.cu:1244) */
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        const int src = (src_code >> (4 * k)) & 15u;
+        if (!((flags >> k) & 1u)) {
+            for (int v = 0; v < S; ++v) CAG(k, v) = (k == 0 && v == 0) ? 2.0f : 0.0f;
+        } else if (src == 8) {
+            for (int v = 0; v < S; ++v) CAG(k, v) = *cache_at(a, v, center);
+        } else if (src < 8) {
             for (int v = 0; v < S; ++v) CAG(k, v) = CAG(src, v);
-        } else {
-            cost_vector(a, px, py, c, sWW, tid, rs, &CAG(k, 0), (int)npx);
         }
     }
 
@@ -736,8 +785,8 @@ __global__ void __launch_bounds__(kBlock, HPM_P2_MIN_BLOCKS) k_prop_refine(const
 {
     __shared__ float2 sWW[kTaps * kBlock];
     const int tid = threadIdx.y * kBlockX + threadIdx.x;
-    const int py = blockIdx.y * kBlockY + threadIdx.y;
-    const int px = blockIdx.x * (2 * kBlockX) + 2 * threadIdx.x + ((py + color) & 1);
+    int px, py;
+    half_step_pixel(color, px, py);
     if (px >= a.W || py >= a.rows_cov) return;
     const int W = a.W, S = a.n - 1;
     const size_t npx = (size_t)W * a.H;
@@ -812,11 +861,18 @@ __global__ void __launch_bounds__(kBlock, HPM_P2_MIN_BLOCKS) k_prop_refine(const
     }
     uint32_t tsv = 0;
     float wn = 0.0f;
+    /* the integer view weights, 4 bits per view (at most 15 draws), for
+     * loops over the selected views with a run-time index */
+    unsigned long long vw_lo = 0, vw_hi = 0;
 #pragma unroll
     for (int v = 0; v < SMAX; ++v)
         if (v < S && vw[v] > 0) {
             tsv |= 1u << v;
             wn += vw[v];
+            if (v < 16)
+                vw_lo |= (unsigned long long)vw[v] << (4 * v);
+            else
+                vw_hi |= (unsigned long long)vw[v] << (4 * (v - 16));
         }
 
     float fc[8];
@@ -973,40 +1029,53 @@ __global__ void __launch_bounds__(kBlock, HPM_P2_MIN_BLOCKS) k_prop_refine(const
         const float4 n_pert = perturbed_normal(cam, px, py, plane, rng, (float)(pert * kPiD));
         const float depths[5] = {depth_rand, depth_now, depth_rand, depth_now, depth_pert};
         const float4 normals[5] = {plane, n_rand, n_rand, n_pert, plane};
-        int scratch = 8;
-#pragma unroll 1
-        for (int i = 0; i < 5; ++i) {
-            float4 t = normals[i];
-            t.w = distance_to_origin(cam, px, py, depths[i], t);
-            cost_vector(a, px, py, t, sWW, tid, rs, &CAG(scratch, 0), (int)npx);
-            float tc = 0.0f;
+        /* The five candidates are built before any is scored (HPM.cu:1180-
+         * 1183), so they are scored view by view with the view index uniform
+         * across the warp (one source texture per texture instruction, one
+         * source image at a time per block); each NCC value goes to the
+         * candidate's hand-off row for the cache. */
+        float4 cand[5];
 #pragma unroll
-            for (int v = 0; v < SMAX; ++v) {
-                if (v < S && vw[v] > 0) {
+        for (int i = 0; i < 5; ++i) {
+            cand[i] = normals[i];
+            cand[i].w = distance_to_origin(cam, px, py, depths[i], cand[i]);
+        }
+        float tc[5] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+        for (int v = 0; v < S; ++v) {
+            const bool selected = (tsv >> v) & 1u;
+            const float w = (float)((v < 16 ? (vw_lo >> (4 * v)) : (vw_hi >> (4 * (v - 16)))) & 15ull);
+#pragma unroll 1
+            for (int i = 0; i < 5; ++i) {
+                const float c = ncc_call(a, v + 1, px, py, cand[i], sWW, tid, rs);
+                CAG(kRefineRow + i, v) = c;
+                if (selected) {
                     if (a.geom)
-                        tc += vw[v] * (CAG(scratch, v) + 0.1f * geom_cost(a, v + 1, t, px, py));
+                        tc[i] += w * (c + 0.1f * geom_cost(a, v + 1, cand[i], px, py));
                     else
-                        tc += vw[v] * CAG(scratch, v);
+                        tc[i] += w * c;
                 }
             }
-            tc /= wn;
-            const float depth_before = depth_from_plane(cam, t, px, py);
+        }
+        if (a.counters) atomicAdd(&a.counters[0], (unsigned long long)(5 * S));
+#pragma unroll
+        for (int i = 0; i < 5; ++i) {
+            const float tci = tc[i] / wn;
+            const float depth_before = depth_from_plane(cam, cand[i], px, py);
             bool take;
             if (use_prior) {
                 const float dd = depths[i] - depth_prior;
-                const float pr = restricted_prior(dd, dot3(pp, t), two_dss, two_ass);
-                const float rtc = expf(-tc * tc / beta) * pr;
+                const float pr = restricted_prior(dd, dot3(pp, cand[i]), two_dss, two_ass);
+                const float rtc = expf(-tci * tci / beta) * pr;
                 take = depth_before >= a.dmin && depth_before <= a.dmax && rtc > restricted_cost;
                 if (take) restricted_cost = rtc;
             } else {
-                take = depth_before >= a.dmin && depth_before <= a.dmax && tc < cost;
+                take = depth_before >= a.dmin && depth_before <= a.dmax && tci < cost;
             }
             if (take) {
                 depth_now = depth_before;
-                plane = t;
-                cost = tc;
-                best_row = scratch;
-                scratch = (scratch == 8) ? 9 : 8;
+                plane = cand[i];
+                cost = tci;
+                best_row = kRefineRow + i;
             }
         }
     }
@@ -1112,7 +1181,7 @@ __global__ void k_geom_costs(const __grid_constant__ PMArgs a, const float4 *pla
 template <int SMAX>
 cudaError_t launch_prop_t(const PMArgs &a, int iter, int color, cudaStream_t s)
 {
-    dim3 grid((a.W + 2 * kBlockX - 1) / (2 * kBlockX), (a.rows_cov + kBlockY - 1) / kBlockY);
+    dim3 grid((a.W + 2 * kWarpW - 1) / (2 * kWarpW), (a.rows_cov + 2 * kWarpH - 1) / (2 * kWarpH));
     k_prop_dirs<<<grid, dim3(kBlockX, kBlockY), 0, s>>>(a, iter, color);
     k_prop_refine<SMAX><<<grid, dim3(kBlockX, kBlockY), 0, s>>>(a, iter, color);
     return cudaGetLastError();

@@ -252,12 +252,12 @@ int hpm_profile_enable(hpm_ctx *ctx, int enable);
 /* kernel times in ms accumulated since enable: [init, propagate, finalize,
  * jbu]; counts = launches of each.  Either pointer may be NULL. */
 int hpm_profile_read(hpm_ctx *ctx, float *ms4, int *counts4);
-/* Work counters: cost-vector evaluations (one evaluation = num_images-1 NCC
- * windows) and geometric-consistency terms, summed over every pass run since
- * hpm_count_enable(ctx, 1), which zeroes them.  Diagnostic; no reference
- * counterpart. */
+/* Work counters: bilateral NCC window evaluations (one per hypothesis and
+ * source view) and geometric-consistency terms, summed over every pass run
+ * since hpm_count_enable(ctx, 1), which zeroes them.  Diagnostic; no
+ * reference counterpart. */
 int hpm_count_enable(hpm_ctx *ctx, int enable);
-int hpm_count_read(hpm_ctx *ctx, uint64_t *cost_vectors, uint64_t *geom_terms);
+int hpm_count_read(hpm_ctx *ctx, uint64_t *ncc_windows, uint64_t *geom_terms);
 
 /* Benchmark utility (no counterpart in the reference): measured FP32 FMA
  * throughput of `device` in TFLOP/s, the roofline denominator of the
