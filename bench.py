@@ -48,10 +48,10 @@ METRIC = "depth Mpix/s, plain vs batched prior-net form on 1 B200, at equal %px 
 WORKLOAD = dict(width=1600, height=1200, n_views=11, n_planes=20, n_spheres=5, low_texture=0.40, pyramid_levels=2,
                 geom_iterations=2)
 
-# per-launch DRAM traffic of the half-step kernel pair, from the ncu capture
-# summarised in profiles/prop_kernels_1280x960_s10.md (1280x960, 10 sources),
-# scaled by pixels; the hand-off buffers grow with the pixel count
-TRAFFIC_BYTES_PER_PX_HALF_STEP = (596.144128 + 729.246720 + 944.850944 + 284.436992) * 1e6 / (1280 * 960)
+# DRAM traffic of one half-step (k_prop_dirs + k_prop_refine), from the ncu
+# capture summarised in profiles/prop_kernels_1600x1200_s10.md (1600x1200,
+# 10 sources), per pixel: the hand-off buffers grow with the pixel count
+TRAFFIC_BYTES_PER_PX_HALF_STEP = (1597.430856 + 2447.062272) * 1e6 / (1600 * 1200)
 GEOM_TERM_FLOPS = 120  # two projections (world point + camera, 3x3 each) and the reprojection distance
 TAPS, NCC_FLOPS_PER_TAP, FLOPS_PER_HYP_VIEW = 36, 34, 80
 
@@ -73,6 +73,9 @@ def parse_args():
     ap.add_argument("--size", default=None,
                     help="WxH override of the workload's resolution (profiling captures use a smaller case)")
     ap.add_argument("--views", type=int, default=None, help="override of the scene's view count")
+    ap.add_argument("--pass-case", action="store_true",
+                    help="kernel-capture case: plain PatchMatch passes of one view of the scene (1 warm-up, then "
+                         "--steps passes); prints the half-step time instead of the bench line")
     args = ap.parse_args()
     if args.size:
         w, h = (int(x) for x in args.size.lower().split("x"))
@@ -358,6 +361,32 @@ def run_ours(args, dist):
     return line
 
 
+def run_pass_case(args):
+    """Plain passes of reference view n/2 of the bench scene, for ncu captures
+    of the half-step kernels."""
+    import hpm_b200 as hb
+    import synthetic as syn
+
+    sc, images, pairs = make_scene(0)
+    ref = WORKLOAD["n_views"] // 2
+    ids = [ref] + pairs[ref][1]
+    cam = sc.cams[ref]
+    dmin, dmax = cam["depth_min"] * np.float32(0.6), cam["depth_max"] * np.float32(1.2)
+    with hb.Context() as ctx:
+        ctx.set_views([images[i] for i in ids], sc.cams[ids])
+        ctx.run_patchmatch(hb.default_params(dmin, dmax, seed=99))
+        ctx.profile_enable(True)
+        for i in range(args.steps):
+            ctx.run_patchmatch(hb.default_params(dmin, dmax, seed=i))
+        prof = ctx.profile_read()
+        ctx.profile_enable(False)
+        planes, _ = ctx.get_result()
+    ms, n = prof["propagate"]
+    return {"case": f"plain passes of view {ref}, {WORKLOAD['width']}x{WORKLOAD['height']}, {len(ids) - 1} sources",
+            "half_step_ms": ms / max(n, 1), "init_ms": prof["init"][0] / max(prof["init"][1], 1),
+            "px_relerr_lt_1pct": float(syn.depth_accuracy(planes[..., 3], sc.gt_depth[ref]))}
+
+
 def run_reference(args, dist):
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as orc
@@ -467,6 +496,10 @@ def main():
     args = parse_args()
     dist = Dist(args.gpus)
     try:
+        if args.pass_case:
+            if dist.rank == 0:
+                print(json.dumps(run_pass_case(args)), flush=True)
+            return
         if args.impl == "reference":
             if dist.rank != 0:
                 return

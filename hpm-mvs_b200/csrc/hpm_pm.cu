@@ -1045,7 +1045,12 @@ __global__ void __launch_bounds__(kBlock, HPM_P2_MIN_BLOCKS) k_prop_refine(const
             const bool selected = (tsv >> v) & 1u;
             const float w = (float)((v < 16 ? (vw_lo >> (4 * v)) : (vw_hi >> (4 * (v - 16)))) & 15ull);
 #pragma unroll 1
-            for (int i = 0; i < 5; ++i) {
+            for (int k = 0; k < 5; ++k) {
+                /* candidates 0 and 2 share the random depth, hence the window
+                 * centre in every source view; 1, 3 and 4 sit at or near the
+                 * current depth: scoring 0, 2, 1, 3, 4 keeps windows with the
+                 * same centre back to back in the texture cache */
+                const int i = (0x43120 >> (4 * k)) & 15;
                 const float c = ncc_call(a, v + 1, px, py, cand[i], sWW, tid, rs);
                 CAG(kRefineRow + i, v) = c;
                 if (selected) {
