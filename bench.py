@@ -51,7 +51,7 @@ WORKLOAD = dict(width=1600, height=1200, n_views=11, n_planes=20, n_spheres=5, l
 # DRAM traffic of one half-step (k_prop_dirs + k_prop_refine), from the ncu
 # capture summarised in profiles/prop_kernels_1600x1200_s10.md (1600x1200,
 # 10 sources), per pixel: the hand-off buffers grow with the pixel count
-TRAFFIC_BYTES_PER_PX_HALF_STEP = (1597.430856 + 2447.062272) * 1e6 / (1600 * 1200)
+TRAFFIC_BYTES_PER_PX_HALF_STEP = (847.3 + 750.8 + 1805.0 + 623.2) * 1e6 / (1600 * 1200)
 GEOM_TERM_FLOPS = 120  # two projections (world point + camera, 3x3 each) and the reprojection distance
 TAPS, NCC_FLOPS_PER_TAP, FLOPS_PER_HYP_VIEW = 36, 34, 80
 
