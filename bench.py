@@ -86,16 +86,21 @@ def parse_args():
 
 
 class Dist:
-    def __init__(self, n):
+    """One process per GPU (RANK / LOCAL_RANK / WORLD_SIZE from torchrun).
+    Ranks exchange only timing: a barrier around the timed region and the
+    max of the elapsed times; the scenes themselves never cross ranks."""
+
+    def __init__(self, n, backend="nccl"):
         self.world = int(os.environ.get("WORLD_SIZE", "1"))
         self.rank = int(os.environ.get("RANK", "0"))
         self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.backend = backend
         self.pg = False
         if self.world > 1:
             import torch.distributed as dist
 
-            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
-                                    device_id=__import__("torch").device("cuda", self.local))
+            kw = {"device_id": __import__("torch").device("cuda", self.local)} if backend == "nccl" else {}
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300), **kw)
             self.pg = True
 
     def barrier(self):
@@ -110,7 +115,8 @@ class Dist:
         import torch
         import torch.distributed as dist
 
-        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{self.local}")
+        dev = f"cuda:{self.local}" if self.backend == "nccl" else "cpu"
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
@@ -157,6 +163,12 @@ class Clocks:
         reasons = [n for i, n in enumerate(names) if any(r[2 + i].strip() == "Active" for r in rows)]
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
                 "reasons": reasons, "samples": len(rows)}
+
+
+def job_mpix_per_s(world, steps, px_per_rank_step, max_ms):
+    """Whole-job depth Mpix/s: every rank processed `steps` scenes of
+    px_per_rank_step depth pixels; the job took the slowest rank's time."""
+    return world * steps * px_per_rank_step / (max_ms * 1e-3) / 1e6
 
 
 def make_scene(seed, width=None, height=None):
@@ -321,7 +333,7 @@ def run_ours(args, dist):
     achieved = flops_step / (prop_ms_step * 1e-3) / 1e12
     n_launch = sum(launches.values())
     line = {
-        "metric": METRIC, "value": dist.world * args.steps * nv * npx / (ms * 1e-3) / 1e6, "unit": "depth Mpix/s",
+        "metric": METRIC, "value": job_mpix_per_s(dist.world, args.steps, nv * npx, ms), "unit": "depth Mpix/s",
         "n_gpus": dist.world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded procedural scene, hpm-mvs_b200/synthetic.py; one scene per rank)",
@@ -337,7 +349,7 @@ def run_ours(args, dist):
                    "parallelism": f"one scene per GPU, {dist.world} GPU(s)"},
         "accuracy": acc,
         "clocks": clk.summary(),
-        "e2e": {"value": dist.world * args.steps * nv * npx / (ms_e2e * 1e-3) / 1e6, "unit": "depth Mpix/s",
+        "e2e": {"value": job_mpix_per_s(dist.world, args.steps, nv * npx, ms_e2e), "unit": "depth Mpix/s",
                 "h2d_bytes_per_step": int(sum(i.nbytes for i in images)),
                 "d2h_bytes_per_step": int(nv * npx * 4 * 5)},
         "gpu_launches": n_launch * args.steps,
