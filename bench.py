@@ -220,6 +220,35 @@ def short_kernel_name(k):
     return k.split("::")[-1] if "::" in k else k
 
 
+def time_fusion(sc, pairs, depths, normals, with_oracle):
+    """RunFusion (main.cpp:502-633) of the last timed step's maps: hpm_fuse
+    (consistency tests on the GPU, order-dependent masking on the host),
+    wall clock with host maps in and the point list out; beside it the
+    oracle's sequential restatement on one host core.  Not part of the
+    depth-map metric, as the reference's own timing leaves fusion out."""
+    import hpm_b200 as hb
+
+    colors = [np.repeat(g[..., None], 3, -1) for g in sc.images]
+    hb.fuse(sc.cams, depths, normals, colors, pairs)  # warm-up
+    t0 = time.perf_counter()
+    xyz, _, _ = hb.fuse(sc.cams, depths, normals, colors, pairs)
+    dt = time.perf_counter() - t0
+    npx = sum(d.size for d in depths)
+    out = {"ms_per_scene": dt * 1e3, "points": int(len(xyz)), "mpix_per_s": npx / dt / 1e6,
+           "what": "hpm_fuse of the scene's final depth/normal maps (11 views), host buffers in and out"}
+    if with_oracle:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle as orc
+
+        t0 = time.perf_counter()
+        oxyz, _, _ = orc.fuse(sc.cams, depths, normals, colors, pairs)
+        odt = time.perf_counter() - t0
+        out["cpu_oracle"] = {"ms_per_scene": odt * 1e3, "points": int(len(oxyz)), "mpix_per_s": npx / odt / 1e6,
+                             "cores": 1, "kind": "port",
+                             "sample": "the same maps through or_fuse (the reference's sequential loop in C)"}
+    return out
+
+
 def cpu_baseline():
     """Oracle on all host cores: one view of a 320x240 scene of the same
     recipe through the whole per-view flow (pass set A with the prior on
@@ -323,6 +352,7 @@ def run_ours(args, dist):
     ms_e2e = dist.max(f0.elapsed_time(f1))
     acc = scene_accuracy(sc, dict(enumerate(out_np[0])), dict(enumerate(out_np[1])))
     ctx.close()
+    fusion = time_fusion(sc, pairs, out_np[0], out_np[1], dist.rank == 0 and dist.world == 1)
 
     n_pass = nv * passes_per_view()
     prop_ms, prop_n = prof["propagate"]
@@ -368,6 +398,7 @@ def run_ours(args, dist):
                      "propagate_share": prop_ms_step / (ms / args.steps),
                      "ncc_windows_per_step": ncc_half, "geom_terms_per_step": n_geom,
                      "flops_per_ncc_window": TAPS * NCC_FLOPS_PER_TAP + FLOPS_PER_HYP_VIEW},
+        "fusion": fusion,
         "impl": "ours",
     }
     return line

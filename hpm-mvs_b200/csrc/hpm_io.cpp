@@ -179,7 +179,8 @@ int paeth(int a, int b, int c)
     return (pa <= pb && pa <= pc) ? a : (pb <= pc ? b : c);
 }
 
-int decode_png(const std::vector<uint8_t> &b, std::vector<uint8_t> &px, int *w_out, int *h_out)
+/* out_ch 1: gray as IMREAD_GRAYSCALE; 3: B, G, R as IMREAD_COLOR */
+int decode_png(const std::vector<uint8_t> &b, std::vector<uint8_t> &px, int *w_out, int *h_out, int out_ch)
 {
     static const uint8_t sig[8] = {137, 80, 78, 71, 13, 10, 26, 10};
     if (b.size() < 33 || memcmp(b.data(), sig, 8) != 0) return HPM_ERR_IO;
@@ -245,21 +246,27 @@ int decode_png(const std::vector<uint8_t> &b, std::vector<uint8_t> &px, int *w_o
             dst[x] = (uint8_t)(src[x] + pred);
         }
     }
-    px.resize((size_t)w * h);
+    px.resize((size_t)w * h * out_ch);
     for (size_t p = 0; p < (size_t)w * h; ++p) {
         int r, g, bl;
         if (ctype == 0 || ctype == 4) {
-            px[p] = img[p * ch];
-            continue;
-        }
-        if (ctype == 3) {
+            r = g = bl = img[p * ch];
+        } else if (ctype == 3) {
             const size_t k = 3 * (size_t)img[p];
             if (k + 2 >= palette.size()) return HPM_ERR_IO;
             r = palette[k], g = palette[k + 1], bl = palette[k + 2];
         } else {
             r = img[p * ch], g = img[p * ch + 1], bl = img[p * ch + 2];
         }
-        px[p] = (uint8_t)((9797 * r + 19234 * g + 3737 * bl) >> 15);
+        if (out_ch == 3) {
+            px[3 * p] = (uint8_t)bl;
+            px[3 * p + 1] = (uint8_t)g;
+            px[3 * p + 2] = (uint8_t)r;
+        } else if (ctype == 0 || ctype == 4) {
+            px[p] = (uint8_t)r;
+        } else {
+            px[p] = (uint8_t)((9797 * r + 19234 * g + 3737 * bl) >> 15);
+        }
     }
     *w_out = (int)w;
     *h_out = (int)h;
@@ -302,19 +309,35 @@ extern "C" int hpm_resize_linear(const float *src, int sw, int sh, int ch, float
     return HPM_OK;
 }
 
-extern "C" int hpm_read_gray8(const char *path, uint8_t *pixels, size_t cap, int *w, int *h)
+static int read_image8(const char *path, uint8_t *pixels, size_t cap, int *w, int *h, int out_ch)
 {
     if (!path || !w || !h) return HPM_ERR_ARG;
     std::vector<uint8_t> bytes, px;
     if (!read_file(path, bytes) || bytes.size() < 2) return HPM_ERR_IO;
     int r;
-    if (bytes[0] == 'P' && bytes[1] == '5')
+    if (bytes[0] == 'P' && bytes[1] == '5') {
         r = decode_pgm(bytes, px, w, h);
-    else
-        r = decode_png(bytes, px, w, h);
+        if (!r && out_ch == 3) {
+            std::vector<uint8_t> c(px.size() * 3);
+            for (size_t p = 0; p < px.size(); ++p) c[3 * p] = c[3 * p + 1] = c[3 * p + 2] = px[p];
+            px.swap(c);
+        }
+    } else {
+        r = decode_png(bytes, px, w, h, out_ch);
+    }
     if (r) return r;
     if (!pixels) return HPM_OK;
     if (cap < px.size()) return HPM_ERR_ARG;
     memcpy(pixels, px.data(), px.size());
     return HPM_OK;
+}
+
+extern "C" int hpm_read_gray8(const char *path, uint8_t *pixels, size_t cap, int *w, int *h)
+{
+    return read_image8(path, pixels, cap, w, h, 1);
+}
+
+extern "C" int hpm_read_bgr8(const char *path, uint8_t *pixels, size_t cap, int *w, int *h)
+{
+    return read_image8(path, pixels, cap, w, h, 3);
 }

@@ -361,6 +361,75 @@ void HPM::ReleaseProblemHostMemory()
     std::vector<float>().swap(seed_costs_);
 }
 
+long long RunFusion(const std::string &dense_folder, const std::vector<Problem> &problems, bool geom_consistency,
+                    int device)
+{
+    const int n = (int)problems.size();
+    std::vector<HpmCamera> cams(n);
+    std::vector<std::vector<float>> depths(n), normals(n);
+    std::vector<std::vector<uint8_t>> colors(n);
+    std::vector<int> refs(n), counts(n), srcs((size_t)n * (HPM_MAX_IMAGES - 1), 0);
+    for (int i = 0; i < n; ++i) {
+        /* the reference indexes views by problem order (main.cpp:517-546) */
+        const int id = problems[i].ref_image_id;
+        const std::string folder = result_folder(dense_folder, id);
+        int w = 0, h = 0;
+        depths[i] = read_dmb(folder + (geom_consistency ? "/depths_geom.dmb" : "/depths.dmb"), &w, &h, 1);
+        normals[i] = read_dmb(folder + "/normals.dmb", &w, &h, 3);
+        HpmCamera cam{};
+        const std::string cp = id_path(dense_folder + "/cams", id, "_cam.txt");
+        int rc = hpm_read_camera(cp.c_str(), &cam);
+        if (rc != HPM_OK) throw Error(rc, "cannot read " + cp);
+        int iw = 0, ih = 0;
+        std::string ip;
+        for (const char *ext : {".png", ".pgm"})
+            if (ip.empty() && exists(id_path(dense_folder + "/images", id, ext))) ip = id_path(dense_folder + "/images", id, ext);
+        if (ip.empty()) throw Error(HPM_ERR_IO, "no PNG/PGM colour image for view " + std::to_string(id));
+        rc = hpm_read_bgr8(ip.c_str(), nullptr, 0, &iw, &ih);
+        std::vector<uint8_t> bgr((size_t)3 * iw * ih);
+        if (rc == HPM_OK) rc = hpm_read_bgr8(ip.c_str(), bgr.data(), bgr.size(), &iw, &ih);
+        if (rc != HPM_OK) throw Error(rc, "cannot decode " + ip);
+        if (iw != w || ih != h) { /* RescaleImageAndCamera, HPM.cpp:187-208 */
+            std::vector<float> f(bgr.begin(), bgr.end()), g((size_t)3 * w * h);
+            int r2 = hpm_resize_linear(f.data(), iw, ih, 3, g.data(), w, h);
+            if (r2 != HPM_OK) throw Error(r2, "colour resize");
+            bgr.resize(g.size());
+            for (size_t k = 0; k < g.size(); ++k) bgr[k] = (uint8_t)std::min(255.0f, std::max(0.0f, std::round(g[k])));
+            const float sx = w / (float)iw, sy = h / (float)ih;
+            cam.K[0] *= sx;
+            cam.K[2] *= sx;
+            cam.K[4] *= sy;
+            cam.K[5] *= sy;
+        }
+        cam.width = w;
+        cam.height = h;
+        cams[i] = cam;
+        colors[i] = std::move(bgr);
+        refs[i] = i;
+        counts[i] = (int)problems[i].src_image_ids.size();
+        for (int j = 0; j < counts[i]; ++j) srcs[(size_t)i * (HPM_MAX_IMAGES - 1) + j] = problems[i].src_image_ids[j];
+    }
+    std::vector<const float *> dp(n), np_(n);
+    std::vector<const uint8_t *> cp(n);
+    size_t cap = 0;
+    for (int i = 0; i < n; ++i) {
+        dp[i] = depths[i].data();
+        np_[i] = normals[i].data();
+        cp[i] = colors[i].data();
+        cap += depths[i].size();
+    }
+    std::vector<float> xyz(3 * cap), nrm(3 * cap);
+    std::vector<uint8_t> col(3 * cap);
+    long long count = 0;
+    int rc = hpm_fuse(device, n, cams.data(), dp.data(), np_.data(), cp.data(), n, refs.data(), counts.data(),
+                      srcs.data(), xyz.data(), nrm.data(), col.data(), (long long)cap, &count);
+    if (rc != HPM_OK) throw Error(rc, "hpm_fuse");
+    const std::string ply = dense_folder + "/HPM/HPM_model.ply";
+    rc = hpm_write_ply(ply.c_str(), count, xyz.data(), nrm.data(), col.data());
+    if (rc != HPM_OK) throw Error(rc, "cannot write " + ply);
+    return count;
+}
+
 void ProcessProblem(const std::string &dense_folder, const Problem &problem, bool geom_consistency,
                     bool planar_prior, bool multi_geometry, uint64_t seed, int pyramid_levels, int device)
 {

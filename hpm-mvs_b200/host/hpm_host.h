@@ -115,6 +115,15 @@ private:
     std::vector<float> seed_planes_, seed_costs_;
 };
 
+/* RunFusion (main.cpp:502-633): fuses the depth maps of every problem
+ * (depths_geom.dmb with geom_consistency, else depths.dmb) and normals.dmb
+ * into dense_folder/HPM/HPM_model.ply; returns the number of points.
+ * Colours come from images/ (PNG or PGM); an image whose size differs from
+ * its depth map is resized bilinearly (RescaleImageAndCamera,
+ * HPM.cpp:187-208), not bit-exactly as OpenCV's 8-bit path. */
+long long RunFusion(const std::string &dense_folder, const std::vector<Problem> &problems, bool geom_consistency,
+                    int device = 0);
+
 /* ProcessProblem (main.cpp:35-499): one reference view, outputs written
  * under dense_folder/HPM/2333_%08d/. */
 void ProcessProblem(const std::string &dense_folder, const Problem &problem, bool geom_consistency,

@@ -1,11 +1,11 @@
 /*
  * main() of HPM-MVS (main.cpp:636-677) on the B200 path: pass set A
- * (ProcessProblem with the planar prior) for every problem of pair.txt, then
- * two geometric-consistency iterations over every problem.  Fusion
- * (RunFusion, main.cpp:502-633) is not part of this path and is not run.
+ * (ProcessProblem with the planar prior) for every problem of pair.txt, two
+ * geometric-consistency iterations over every problem, then the fusion
+ * into HPM/HPM_model.ply (RunFusion, main.cpp:502-633).
  *
  *   hpm_mvs dense_folder [--seed S] [--levels K] [--device D] [--no-prior]
- *                        [--geom-iterations G]
+ *                        [--geom-iterations G] [--no-fusion]
  *
  * Problem p of pass set A uses seed S + p; problem p of geometric iteration
  * g uses S + 1000003 (g + 1) + p, the seeds hpm_run_scene uses, so both
@@ -23,14 +23,14 @@ int main(int argc, char **argv)
 {
     if (argc < 2 || !strcmp(argv[1], "-h") || !strcmp(argv[1], "--help")) {
         std::cout << "USAGE: hpm_mvs dense_folder [--seed S] [--levels K] [--device D] [--no-prior] "
-                     "[--geom-iterations G]"
+                     "[--geom-iterations G] [--no-fusion]"
                   << std::endl;
         return argc < 2 ? -1 : 0;
     }
     const std::string dense_folder = argv[1];
     uint64_t seed = 0;
     int levels = -1, device = 0, geom_iterations = 2;
-    bool planar_prior = true;
+    bool planar_prior = true, fusion = true;
     for (int i = 2; i < argc; ++i) {
         const std::string a = argv[i];
         auto next = [&](const char *name) -> const char * {
@@ -50,6 +50,8 @@ int main(int argc, char **argv)
             geom_iterations = std::atoi(next("--geom-iterations"));
         else if (a == "--no-prior")
             planar_prior = false;
+        else if (a == "--no-fusion")
+            fusion = false;
         else {
             std::cerr << "unknown option " << a << std::endl;
             return 2;
@@ -65,6 +67,10 @@ int main(int argc, char **argv)
             for (size_t p = 0; p < problems.size(); ++p)
                 hpm_host::ProcessProblem(dense_folder, problems[p], true, false, g > 0,
                                          seed + 1000003ull * (g + 1) + p, levels, device);
+        if (fusion) {
+            const long long n = hpm_host::RunFusion(dense_folder, problems, geom_iterations > 0, device);
+            std::cout << "Fused " << n << " points into " << dense_folder << "/HPM/HPM_model.ply" << std::endl;
+        }
     } catch (const hpm_host::Error &e) {
         std::cerr << "hpm_mvs: " << e.what() << " (status " << e.code << ")" << std::endl;
         return 1;

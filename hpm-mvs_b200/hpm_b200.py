@@ -38,6 +38,7 @@ EXPORTED = [
     "hpm_count_enable", "hpm_count_read", "hpm_write_dmb", "hpm_read_dmb", "hpm_read_camera", "hpm_read_pair",
     "hpm_fp32_peak", "hpm_jbu_noalloc", "hpm_process_problem", "hpm_last_prior_stats", "hpm_delaunay",
     "hpm_prior_level", "hpm_run_scene", "hpm_read_gray8", "hpm_resize_linear",
+    "hpm_fuse", "hpm_write_ply", "hpm_read_bgr8",
 ]
 
 
@@ -388,6 +389,55 @@ def read_gray8(path: str) -> np.ndarray:
     if rc != HPM_OK:
         raise HpmError(f"hpm_read_gray8({path}) failed: {rc}")
     return out
+
+
+def read_bgr8(path: str) -> np.ndarray:
+    """images/ file as cv::imread(path, IMREAD_COLOR) gives it: uint8 [H, W, 3], B G R."""
+    w, h = ctypes.c_int(), ctypes.c_int()
+    rc = lib().hpm_read_bgr8(path.encode(), None, ctypes.c_size_t(0), ctypes.byref(w), ctypes.byref(h))
+    if rc != HPM_OK:
+        raise HpmError(f"hpm_read_bgr8({path}) failed: {rc}")
+    out = np.empty((h.value, w.value, 3), np.uint8)
+    rc = lib().hpm_read_bgr8(path.encode(), _p(out), ctypes.c_size_t(out.nbytes), ctypes.byref(w), ctypes.byref(h))
+    if rc != HPM_OK:
+        raise HpmError(f"hpm_read_bgr8({path}) failed: {rc}")
+    return out
+
+
+def fuse(cams, depths, normals, colors, problems, device: int = 0):
+    """RunFusion (main.cpp:502-633): (xyz [n,3], normal [n,3], bgr [n,3] uint8)
+    in the reference's order.  problems: [(ref, [sources])]."""
+    n = len(cams)
+    cams = np.ascontiguousarray(cams, dtype=CAMERA_DTYPE)
+    ds = [np.ascontiguousarray(d, dtype=np.float32) for d in depths]
+    ns_ = [np.ascontiguousarray(x, dtype=np.float32) for x in normals]
+    cs = [np.ascontiguousarray(c, dtype=np.uint8) for c in colors]
+    arr = lambda xs: (ctypes.c_void_p * n)(*[x.ctypes.data for x in xs])  # noqa: E731
+    refs = np.array([p[0] for p in problems], np.int32)
+    counts = np.array([len(p[1]) for p in problems], np.int32)
+    srcs = np.zeros((max(len(problems), 1), MAX_IMAGES - 1), np.int32)
+    for i, (_, s) in enumerate(problems):
+        srcs[i, :len(s)] = s
+    cap = sum(d.size for d in ds)
+    xyz = np.empty((cap, 3), np.float32)
+    nrm = np.empty((cap, 3), np.float32)
+    bgr = np.empty((cap, 3), np.uint8)
+    cnt = ctypes.c_longlong()
+    rc = lib().hpm_fuse(device, n, _p(cams), arr(ds), arr(ns_), arr(cs), len(problems), _p(refs), _p(counts),
+                        _p(srcs), _p(xyz), _p(nrm), _p(bgr), ctypes.c_longlong(cap), ctypes.byref(cnt))
+    if rc != HPM_OK:
+        raise HpmError(f"hpm_fuse: {STATUS_NAMES.get(rc, rc)}")
+    k = cnt.value
+    return xyz[:k].copy(), nrm[:k].copy(), bgr[:k].copy()
+
+
+def write_ply(path: str, xyz, normal, bgr) -> None:
+    xyz = np.ascontiguousarray(xyz, dtype=np.float32)
+    normal = np.ascontiguousarray(normal, dtype=np.float32)
+    bgr = np.ascontiguousarray(bgr, dtype=np.uint8)
+    rc = lib().hpm_write_ply(path.encode(), ctypes.c_longlong(len(xyz)), _p(xyz), _p(normal), _p(bgr))
+    if rc != HPM_OK:
+        raise HpmError(f"hpm_write_ply({path}): {STATUS_NAMES.get(rc, rc)}")
 
 
 def resize_linear(src: np.ndarray, dw: int, dh: int) -> np.ndarray:

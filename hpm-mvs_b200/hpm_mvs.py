@@ -5,9 +5,11 @@ the C++ host (hpm_mvs) reads PNG and PGM itself.
 
     python hpm-mvs_b200/hpm_mvs.py dense_folder [--seed S] [--levels K]
                                    [--geom-iterations G] [--no-prior] [--device D]
+                                   [--no-fusion]
 
 Writes HPM/2333_%08d/{depths,depths_geom,normals,costs,depths_prior}.dmb like
-the reference's ProcessProblem.  Seeds as in the C++ host: problem p of pass
+the reference's ProcessProblem, then fuses them into HPM/HPM_model.ply
+(RunFusion).  Seeds as in the C++ host: problem p of pass
 set A uses S + p, of geometric iteration g S + 1000003 (g + 1) + p.
 """
 from __future__ import annotations
@@ -82,6 +84,46 @@ def process_problem(ctx, folder, ref, srcs, views, *, geom, planar_prior, multi_
     hb.write_dmb(os.path.join(out, "costs.dmb"), c)
 
 
+def run_fusion(folder, problems, geom_consistency, device=0):
+    """RunFusion (main.cpp:502-633) with OpenCV's colour decoding and
+    RescaleImageAndCamera (HPM.cpp:187-208); returns the point count."""
+    import cv2
+
+    cams, depths, normals, colors = [], [], [], []
+    for ref, _ in problems:
+        out = os.path.join(folder, "HPM", f"2333_{ref:08d}")
+        d = hb.read_dmb(os.path.join(out, "depths_geom.dmb" if geom_consistency else "depths.dmb"))
+        n = hb.read_dmb(os.path.join(out, "normals.dmb"))
+        cam = hb.read_camera(os.path.join(folder, "cams", f"{ref:08d}_cam.txt")).copy()
+        img = None
+        for ext in (".jpg", ".png", ".pgm"):
+            p = os.path.join(folder, "images", f"{ref:08d}{ext}")
+            if os.path.exists(p):
+                img = cv2.imread(p, cv2.IMREAD_COLOR)
+                break
+        if img is None:
+            raise hb.HpmError(f"no colour image for view {ref}")
+        h, w = d.shape
+        if img.shape[:2] != (h, w):
+            sx, sy = np.float32(w) / np.float32(img.shape[1]), np.float32(h) / np.float32(img.shape[0])
+            img = cv2.resize(img, (w, h), interpolation=cv2.INTER_LINEAR)
+            K = cam["K"]
+            K[0] *= sx
+            K[2] *= sx
+            K[4] *= sy
+            K[5] *= sy
+        cam["width"], cam["height"] = w, h
+        cams.append(cam)
+        depths.append(d)
+        normals.append(n)
+        colors.append(img)
+    # the reference indexes views by problem order (main.cpp:517-546)
+    probs = [(i, list(srcs)) for i, (_, srcs) in enumerate(problems)]
+    xyz, nrm, bgr = hb.fuse(np.array(cams), depths, normals, colors, probs, device)
+    hb.write_ply(os.path.join(folder, "HPM", "HPM_model.ply"), xyz, nrm, bgr)
+    return len(xyz)
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
     ap.add_argument("dense_folder")
@@ -90,6 +132,7 @@ def main(argv=None):
     ap.add_argument("--geom-iterations", type=int, default=2)
     ap.add_argument("--no-prior", action="store_true")
     ap.add_argument("--device", type=int, default=0)
+    ap.add_argument("--no-fusion", action="store_true")
     a = ap.parse_args(argv)
     problems = hb.read_pair(os.path.join(a.dense_folder, "pair.txt"))
     needed = sorted({p[0] for p in problems} | {s for p in problems for s in p[1]})
@@ -103,6 +146,9 @@ def main(argv=None):
             for p, (ref, srcs) in enumerate(problems):
                 process_problem(ctx, a.dense_folder, ref, srcs, views, geom=True, planar_prior=False,
                                 multi_geometry=g > 0, seed=a.seed + 1000003 * (g + 1) + p, levels=a.levels)
+    if not a.no_fusion:
+        n = run_fusion(a.dense_folder, problems, a.geom_iterations > 0, a.device)
+        print(f"Fused {n} points into {a.dense_folder}/HPM/HPM_model.ply")
     return 0
 
 

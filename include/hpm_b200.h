@@ -226,6 +226,27 @@ int hpm_jbu_noalloc(int device, const float *guide, int cols, int rows, const fl
                     const float *coarse_normal, int s_cols, int s_rows, float *out_depth, float *out_normal,
                     void *stream);
 
+/* Fusion of a scene's maps into a coloured point cloud: RunFusion
+ * (main.cpp:502-633).  View v has depth (h*w floats), world normal (3
+ * floats per pixel), colour (3 bytes per pixel, B, G, R as cv::imread gives
+ * it, at the depth map's size: the caller resizes it like
+ * RescaleImageAndCamera, HPM.cpp:187-208) and camera cams[v] (of the depth
+ * map's size).  Problems as in hpm_run_scene; a problem's views are indexed
+ * by view id, as the reference indexes them when problem i has reference
+ * view i.  Points come in the reference's order (problem by problem, pixel
+ * by pixel); up to cap are written (xyz, normal, colour), *n_points gets the
+ * full count.  Inputs may be host or device memory.  The consistency tests
+ * run on the GPU, the order-dependent masking on the host. */
+int hpm_fuse(int device, int n_views, const HpmCamera *cams, const float *const *depths,
+             const float *const *normals, const uint8_t *const *colors, int n_problems, const int *ref_ids,
+             const int *src_counts, const int *src_ids, float *out_xyz, float *out_normal, uint8_t *out_bgr,
+             long long cap, long long *n_points);
+/* StoreColorPlyFileBinaryPointCloud (HPM.cpp:403-456): binary little-endian
+ * PLY, x y z nx ny nz as float, red green blue as uchar, non-finite
+ * coordinates written as the origin.  Points are written in order (the
+ * reference's OpenMP loop writes them in an order that varies by run). */
+int hpm_write_ply(const char *path, long long n, const float *xyz, const float *normal, const uint8_t *bgr);
+
 /* Deterministic building blocks exposed for parity checks. */
 
 /* Delaunay triangulation of n integer points (xy pairs) used for the planar
@@ -279,6 +300,10 @@ int hpm_read_camera(const char *path, HpmCamera *cam);
  * (colour reduced as OpenCV's PNG reader does).  Sets *w, *h; copies the
  * pixels when pixels is non-NULL (capacity cap bytes). */
 int hpm_read_gray8(const char *path, uint8_t *pixels, size_t cap, int *w, int *h);
+/* A colour image as cv::imread(path, IMREAD_COLOR) returns it for the
+ * fusion (main.cpp:520): 3 bytes per pixel in B, G, R order; PGM and gray
+ * PNG are replicated to the three channels, alpha is dropped. */
+int hpm_read_bgr8(const char *path, uint8_t *pixels, size_t cap, int *w, int *h);
 /* cv::resize(src, dst, Size(dw, dh), 0, 0, INTER_LINEAR) of a float map
  * with ch interleaved channels, on the host: the image cap of
  * InuputInitialization (HPM.cpp:525-551).  Same arithmetic as OpenCV 4.x

@@ -1508,3 +1508,126 @@ void or_prior_full(const OrCamera *ref, const float *mask, const float *tri_plan
         }
     }
 }
+
+/* ------------------------------------------------------------------ */
+/* Fusion (RunFusion, main.cpp:502-633)                                */
+/* ------------------------------------------------------------------ */
+
+/* Get3DPointonWorld (HPM.cpp:210-234) */
+static void fu_world(const OrCamera *c, int x, int y, float depth, float *X)
+{
+    const float px = depth * ((float)x - c->K[2]) / c->K[0];
+    const float py = depth * ((float)y - c->K[5]) / c->K[4];
+    const float pz = depth;
+    const float *R = c->R, *t = c->t;
+    const float tx = R[0] * px + R[3] * py + R[6] * pz;
+    const float ty = R[1] * px + R[4] * py + R[7] * pz;
+    const float tz = R[2] * px + R[5] * py + R[8] * pz;
+    const float cx = -(R[0] * t[0] + R[3] * t[1] + R[6] * t[2]);
+    const float cy = -(R[1] * t[0] + R[4] * t[1] + R[7] * t[2]);
+    const float cz = -(R[2] * t[0] + R[5] * t[1] + R[8] * t[2]);
+    X[0] = tx + cx;
+    X[1] = ty + cy;
+    X[2] = tz + cz;
+}
+
+/* ProjectonCamera (HPM.cpp:247-257) */
+static void fu_project(const float *X, const OrCamera *c, float *pt, float *depth)
+{
+    const float *R = c->R, *K = c->K, *t = c->t;
+    const float x = R[0] * X[0] + R[1] * X[1] + R[2] * X[2] + t[0];
+    const float y = R[3] * X[0] + R[4] * X[1] + R[5] * X[2] + t[1];
+    const float z = R[6] * X[0] + R[7] * X[1] + R[8] * X[2] + t[2];
+    *depth = K[6] * x + K[7] * y + K[8] * z;
+    pt[0] = (K[0] * x + K[1] * y + K[2] * z) / *depth;
+    pt[1] = (K[3] * x + K[4] * y + K[5] * z) / *depth;
+}
+
+/* (int)f of the reference's x86 host build: truncation, INT_MIN (the
+ * "integer indefinite" of cvttss2si) for NaN and out-of-range values */
+static int trunc_int(float f)
+{
+    if (f != f || f >= 2147483648.0f || f < -2147483648.0f) return (-2147483647 - 1);
+    return (int)f;
+}
+
+/* GetAngle (HPM.cpp:259-268) */
+static float fu_angle(const float *a, const float *b)
+{
+    const float d = a[0] * b[0] + a[1] * b[1] + a[2] * b[2];
+    const float ang = acosf(d);
+    return ang != ang ? 0.0f : ang;
+}
+
+long or_fuse(int n_views, const OrCamera *cams, const float *const *depths, const float *const *normals,
+             const unsigned char *const *colors, int n_problems, const int *ref_ids, const int *src_counts,
+             const int *src_ids, float *out_xyz, float *out_normal, float *out_color, long cap)
+{
+    unsigned char **masks = (unsigned char **)calloc((size_t)n_views, sizeof(*masks));
+    for (int v = 0; v < n_views; ++v) masks[v] = (unsigned char *)calloc((size_t)cams[v].width * cams[v].height, 1);
+    long n_out = 0;
+    for (int pi = 0; pi < n_problems; ++pi) {
+        const int i = ref_ids[pi];
+        const OrCamera *ci = &cams[i];
+        const int cols = ci->width, rows = ci->height, ns = src_counts[pi];
+        int used_x[32], used_y[32];
+        for (int j = 0; j < ns; ++j) used_x[j] = used_y[j] = -1; /* kept across pixels (main.cpp:557) */
+        for (int r = 0; r < rows; ++r) {
+            for (int c = 0; c < cols; ++c) {
+                const size_t ctr = (size_t)r * cols + c;
+                if (masks[i][ctr] == 1) continue;
+                const float ref_depth = depths[i][ctr];
+                const float *ref_n = normals[i] + 3 * ctr;
+                if (ref_depth <= 0.0) continue;
+                float X[3];
+                fu_world(ci, c, r, ref_depth, X);
+                int num = 0;
+                float dyn = 0;
+                for (int j = 0; j < ns; ++j) {
+                    const int s = src_ids[pi * 32 + j];
+                    const OrCamera *cs = &cams[s];
+                    float pt[2], proj_depth;
+                    fu_project(X, cs, pt, &proj_depth);
+                    const int sr = trunc_int(pt[1] + 0.5f), sc = trunc_int(pt[0] + 0.5f);
+                    if (sc >= 0 && sc < cs->width && sr >= 0 && sr < cs->height) {
+                        const size_t sctr = (size_t)sr * cs->width + sc;
+                        if (masks[s][sctr] == 1) continue;
+                        const float src_depth = depths[s][sctr];
+                        const float *src_n = normals[s] + 3 * sctr;
+                        if (src_depth <= 0.0) continue;
+                        float Y[3], tp[2];
+                        fu_world(cs, sc, sr, src_depth, Y);
+                        fu_project(Y, ci, tp, &proj_depth);
+                        const float dx = (float)c - tp[0], dy = (float)r - tp[1];
+                        const float reproj = (float)sqrt((double)dx * dx + (double)dy * dy);
+                        const float rel = fabsf(proj_depth - ref_depth) / ref_depth;
+                        const float ang = fu_angle(ref_n, src_n);
+                        if (reproj < 2.0f && rel < 0.01f && ang < 0.174533f) {
+                            used_x[j] = sc;
+                            used_y[j] = sr;
+                            const float idx = reproj + 200 * rel + ang * 10;
+                            dyn += expf(-idx);
+                            num++;
+                        }
+                    }
+                }
+                if (num >= 1 && (dyn > 0.3 * num)) {
+                    if (n_out < cap) {
+                        memcpy(out_xyz + 3 * n_out, X, sizeof(X));
+                        memcpy(out_normal + 3 * n_out, ref_n, 3 * sizeof(float));
+                        for (int k = 0; k < 3; ++k) out_color[3 * n_out + k] = (float)colors[i][3 * ctr + k];
+                    }
+                    n_out++;
+                    for (int j = 0; j < ns; ++j) {
+                        if (used_x[j] == -1) continue;
+                        const int s = src_ids[pi * 32 + j];
+                        masks[s][(size_t)used_y[j] * cams[s].width + used_x[j]] = 1;
+                    }
+                }
+            }
+        }
+    }
+    for (int v = 0; v < n_views; ++v) free(masks[v]);
+    free(masks);
+    return n_out;
+}

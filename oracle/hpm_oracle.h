@@ -127,6 +127,20 @@ void or_prior_full(const OrCamera *ref, const float *mask, const float *tri_plan
                    const float *knn_planes, int w, int h, float dmin, float dmax, float *out4,
                    unsigned int *out_mask, float *out_depth);
 
+/* ---- fusion (RunFusion, main.cpp:502-633) ---- */
+
+/* Fused point cloud of a scene, sequentially as the reference: views in
+ * problem order, pixels row by row, the masks of already fused source
+ * pixels and the used_list that persists across the pixels of a view.
+ * View v's maps (depth h*w, world normal 3 floats/pixel, BGR colour 3 bytes
+ * per pixel) and camera match in size; problem p has reference ref_ids[p]
+ * and src_counts[p] sources src_ids[p*32 + j] (view ids index the maps).
+ * Writes up to cap points (xyz, normal, colour as floats in B, G, R order)
+ * and returns the count (more than cap means the output was cut). */
+long or_fuse(int n_views, const OrCamera *cams, const float *const *depths, const float *const *normals,
+             const unsigned char *const *colors, int n_problems, const int *ref_ids, const int *src_counts,
+             const int *src_ids, float *out_xyz, float *out_normal, float *out_color, long cap);
+
 #ifdef __cplusplus
 }
 #endif

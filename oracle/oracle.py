@@ -285,6 +285,30 @@ def prior_full(ref_cam, mask, tri_planes, knn_planes, dmin, dmax):
     return out, m, d
 
 
+def fuse(cams, depths, normals, colors, problems):
+    """or_fuse: the reference's sequential RunFusion (xyz, normal, colour as
+    floats B G R), in the reference's order."""
+    n = len(cams)
+    c = _cams(cams)
+    ds = [np.ascontiguousarray(d, dtype=np.float32) for d in depths]
+    ns_ = [np.ascontiguousarray(x, dtype=np.float32) for x in normals]
+    cs = [np.ascontiguousarray(x, dtype=np.uint8) for x in colors]
+    arr = lambda xs: (ctypes.c_void_p * n)(*[x.ctypes.data for x in xs])  # noqa: E731
+    refs = np.array([p[0] for p in problems], np.int32)
+    counts = np.array([len(p[1]) for p in problems], np.int32)
+    srcs = np.zeros((max(len(problems), 1), 32), np.int32)
+    for i, (_, s) in enumerate(problems):
+        srcs[i, :len(s)] = s
+    cap = sum(d.size for d in ds)
+    xyz = np.empty((cap, 3), np.float32)
+    nrm = np.empty((cap, 3), np.float32)
+    col = np.empty((cap, 3), np.float32)
+    lib().or_fuse.restype = ctypes.c_long
+    k = lib().or_fuse(n, _p(c), arr(ds), arr(ns_), arr(cs), len(problems), _p(refs), _p(counts), _p(srcs), _p(xyz),
+                      _p(nrm), _p(col), ctypes.c_long(cap))
+    return xyz[:k].copy(), nrm[:k].copy(), col[:k].copy()
+
+
 # ---------------------------------------------------------------- reference shim
 
 def ref_cost_vectors(images, cams, planes) -> np.ndarray:

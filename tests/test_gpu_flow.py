@@ -211,3 +211,6 @@ def test_host_main_writes_the_scene_driver_maps(tmp_path):
     assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
     for v in range(4):
         np.testing.assert_array_equal(hb.read_dmb(os.path.join(py, "HPM", f"2333_{v:08d}", "depths_geom.dmb")), sd[v])
+    # both fused the same maps into the same point cloud (HPM/HPM_model.ply)
+    plys = [open(os.path.join(f, "HPM", "HPM_model.ply"), "rb").read() for f in (folder, py)]
+    assert plys[0] == plys[1] and plys[0].startswith(b"ply\n") and len(plys[0]) > 10000
