@@ -73,6 +73,9 @@ def parse_args():
     ap.add_argument("--size", default=None,
                     help="WxH override of the workload's resolution (profiling captures use a smaller case)")
     ap.add_argument("--views", type=int, default=None, help="override of the scene's view count")
+    ap.add_argument("--shard", choices=["scenes", "views"], default="scenes",
+                    help="N>1: one scene per rank (weak scaling, no collective) or one scene's views split over the "
+                         "ranks with an all-gather of depth maps before each geometric iteration (strong scaling)")
     ap.add_argument("--pass-case", action="store_true",
                     help="kernel-capture case: plain PatchMatch passes of one view of the scene (1 warm-up, then "
                          "--steps passes); prints the half-step time instead of the bench line")
@@ -404,6 +407,61 @@ def run_ours(args, dist):
     return line
 
 
+def run_view_shards(args, dist):
+    """One scene, its problems split over the ranks (scene_dist.py): timed
+    from the host images to every rank's final maps on the host."""
+    import torch
+    import torch.distributed as tdist
+
+    import hpm_b200 as hb
+    import scene_dist
+
+    torch.cuda.set_device(dist.local)
+    dev = f"cuda:{dist.local}"
+    w = WORKLOAD
+    sc, images, pairs = make_scene(seed=0)
+    nv, W, H = w["n_views"], w["width"], w["height"]
+    shapes = {v: (H, W) for v in range(nv)}
+    pg = tdist if dist.pg else None
+    ctx = hb.Context(dist.local)
+
+    def step(seed):
+        solver = scene_dist.GpuSolver(ctx, images, sc.cams, pairs, seed=seed, pyramid_levels=w["pyramid_levels"],
+                                      device=dev)
+        mine, _ = scene_dist.run_scene_sharded(solver, pairs, shapes, geom_iterations=w["geom_iterations"], dist=pg)
+        return {v: m[0].cpu().numpy() for v, m in mine.items()}
+
+    for i in range(args.warmup):
+        step(1000 + i)
+    dist.barrier()
+    torch.cuda.synchronize()
+    with Clocks(dist.local) as clk:
+        t0 = time.perf_counter()
+        for i in range(args.steps):
+            out = step(i)
+        torch.cuda.synchronize()
+        elapsed = (time.perf_counter() - t0) * 1e3
+    dist.barrier()
+    ms = dist.max(elapsed)
+    ctx.close()
+    value = args.steps * nv * W * H / (ms * 1e-3) / 1e6
+    return {
+        "metric": METRIC, "value": value, "unit": "depth Mpix/s", "n_gpus": dist.world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "strong",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded procedural scene, shared by all ranks)",
+        "config": {"workload": workload_name(), "width": W, "height": H, "views": nv,
+                   "parallelism": f"views of one scene split over {dist.world} GPU(s); all-gather of depth maps "
+                                  "(NCCL) before each geometric iteration",
+                   "l2": "inputs larger than L2 (see the default mode)"},
+        "accuracy": scene_accuracy(sc, out),
+        "clocks": clk.summary(),
+        "e2e": {"value": value, "unit": "depth Mpix/s", "h2d_bytes_per_step": int(sum(i.nbytes for i in images)),
+                "d2h_bytes_per_step": int(len(out) * W * H * 4),
+                "note": "host images in, each rank's final depth maps out; timed on the host around whole steps"},
+        "impl": "ours",
+    }
+
+
 def run_pass_case(args):
     """Plain passes of reference view n/2 of the bench scene, for ncu captures
     of the half-step kernels."""
@@ -547,6 +605,8 @@ def main():
             if dist.rank != 0:
                 return
             line = run_reference(args, dist)
+        elif args.shard == "views":
+            line = run_view_shards(args, dist)
         else:
             line = run_ours(args, dist)
             if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:

@@ -214,3 +214,40 @@ def test_host_main_writes_the_scene_driver_maps(tmp_path):
     # both fused the same maps into the same point cloud (HPM/HPM_model.ply)
     plys = [open(os.path.join(f, "HPM", "HPM_model.ply"), "rb").read() for f in (folder, py)]
     assert plys[0] == plys[1] and plys[0].startswith(b"ply\n") and len(plys[0]) > 10000
+
+
+def test_view_sharded_driver_on_the_gpu():
+    """scene_dist.run_scene_sharded with the C-ABI solver (maps on the
+    device, one rank) gives exactly the maps of the same schedule written
+    with the Python API: pass set A, then geometric iterations that read the
+    previous iteration's maps of every view."""
+    import scene_dist
+
+    nv = 4
+    sc = syn.make_scene(18, 128, 96, nv, n_planes=4, low_texture=0.3)
+    imgs = [i.astype(np.float32) for i in sc.images]
+    pairs = [(v, list(sc.pairs[v][1])) for v in range(nv)]
+    shapes = {v: (96, 128) for v in range(nv)}
+    with hb.Context() as ctx:
+        solver = scene_dist.GpuSolver(ctx, imgs, sc.cams, pairs, seed=3, pyramid_levels=0)
+        mine, all_depth = scene_dist.run_scene_sharded(solver, pairs, shapes, geom_iterations=2)
+        got = {v: mine[v][0].cpu().numpy() for v in mine}
+    with hb.Context() as ctx:
+        cur, nrm, cst = {}, {}, {}
+        for p, (ref, srcs) in enumerate(pairs):
+            ids = [ref] + srcs
+            ctx.set_views([imgs[i] for i in ids], sc.cams[ids])
+            cur[ref], nrm[ref], cst[ref], _ = ctx.process_problem(seed=3 + p, planar_prior=True, pyramid_levels=0)
+        for it in range(2):
+            new = {}
+            for p, (ref, srcs) in enumerate(pairs):
+                ids = [ref] + srcs
+                ctx.set_views([imgs[i] for i in ids], sc.cams[ids])
+                ctx.set_geom_depths([cur[i] for i in ids])
+                ctx.set_hypotheses(np.concatenate([nrm[ref], cur[ref][..., None]], -1), cst[ref])
+                new[ref], nrm[ref], cst[ref], _ = ctx.process_problem(seed=3 + 1000003 * (it + 1) + p, geom=True,
+                                                                      multi_geometry=it > 0)
+            cur = new
+    for v in range(nv):
+        np.testing.assert_array_equal(got[v], cur[v])
+        np.testing.assert_array_equal(all_depth[v].cpu().numpy(), cur[v])
