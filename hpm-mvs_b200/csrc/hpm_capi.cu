@@ -192,6 +192,8 @@ int hpm_create(hpm_ctx **out, int device)
 int hpm_destroy(hpm_ctx *c)
 {
     if (!c) return HPM_ERR_ARG;
+    if (c->peer) hpm_destroy(c->peer);
+    c->peer = nullptr;
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
     for (int i = 0; i < kMaxViews; ++i) {
@@ -207,6 +209,7 @@ int hpm_destroy(hpm_ctx *c)
     cudaFree(c->d_prior);
     cudaFree(c->d_masks);
     cudaFree(c->d_counters);
+    cudaFree(c->d_scene);
     cudaFree(c->d_scratch);
     cudaFree(c->d_cache);
     cudaFree(c->d_cand);
@@ -615,6 +618,14 @@ int hpm_profile_read(hpm_ctx *c, float *ms4, int *counts4)
     return HPM_OK;
 }
 
+int hpm_set_scene_workers(hpm_ctx *c, int workers)
+{
+    if (!c) return HPM_ERR_ARG;
+    if (workers < 1 || workers > 2) return fail(c, HPM_ERR_ARG, "hpm_set_scene_workers: %d is not 1 or 2", workers);
+    c->scene_workers = workers;
+    return HPM_OK;
+}
+
 int hpm_count_enable(hpm_ctx *c, int enable)
 {
     if (!c) return HPM_ERR_ARG;
@@ -752,3 +763,6 @@ void ws_free(hpm_ctx *c)
     for (void *p : ptrs) cudaFree(p);
     w = FlowWorkspace();
 }
+
+cudaError_t ctx_scene_arena(hpm_ctx *c, size_t bytes) { return ensure((void **)&c->d_scene, &c->scene_cap, bytes); }
+float *ctx_scene_base(hpm_ctx *c) { return c->d_scene; }

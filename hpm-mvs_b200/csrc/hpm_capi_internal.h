@@ -7,6 +7,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <mutex>
 #include <utility>
 #include <vector>
 
@@ -91,6 +92,18 @@ struct hpm_ctx {
     size_t flags_cap = 0;
 
     hpm::FlowWorkspace flow;
+    float *d_scene = nullptr; /* hpm_run_scene's per-view maps, grown on demand */
+    size_t scene_cap = 0;
+
+    /* hpm_run_scene hands pass set A's problems to this context and a peer
+     * (same device, own stream) from two host threads.  The threads pass a
+     * GPU token: a thread holds it while its kernels run and releases it
+     * only while its host triangulates support points, so the other
+     * problem's kernels fill that gap and the two problems' kernels never
+     * share the GPU (their images would compete for L2 and texture caches). */
+    int scene_workers = 2;
+    hpm_ctx *peer = nullptr;
+    std::mutex *gpu_token = nullptr;
 };
 
 int ctx_fail(hpm_ctx *c, int code, const char *fmt, ...);
@@ -100,6 +113,8 @@ int ctx_select_device(hpm_ctx *c);
  * synchronises the context's stream at the end */
 int ctx_run_pass(hpm_ctx *c, const HpmParams *p, int half_steps, int finalize);
 float *ctx_planes(hpm_ctx *c);
+cudaError_t ctx_scene_arena(hpm_ctx *c, size_t bytes);
+float *ctx_scene_base(hpm_ctx *c);
 float *ctx_costs(hpm_ctx *c);
 float *ctx_prior(hpm_ctx *c);
 uint32_t *ctx_masks(hpm_ctx *c);

@@ -8,8 +8,11 @@
  * reference copies every map to the host between passes and runs the prior
  * stages there (support points, Subdiv2D, PCL kd-tree KNN, per-pixel loops).
  */
+#include <atomic>
 #include <cmath>
 #include <cstring>
+#include <mutex>
+#include <thread>
 #include <vector>
 
 #include "hpm_capi_internal.h"
@@ -86,7 +89,11 @@ static int build_level_prior(hpm_ctx *c, const HpmCamera &cam, const float *d_co
         }
     const int np = (int)xy.size() / 2;
     std::vector<int> tris;
+    /* the stream is idle here: another scene worker may use the GPU while
+     * this host thread triangulates */
+    if (c->gpu_token) c->gpu_token->unlock();
     delaunay(xy, w, h, tris);
+    if (c->gpu_token) c->gpu_token->lock();
     const int nt = (int)tris.size() / 6;
     CK(ws_reserve_tris(c, nt), "triangle buffers");
     if (nt > 0) CK(cudaMemcpyAsync(ws.tris, tris.data(), sizeof(int) * tris.size(), cudaMemcpyHostToDevice, s), "tris");
@@ -279,13 +286,9 @@ __global__ void k_pack_planes(const float *__restrict__ normal3, const float *__
     planes[i] = make_float4(normal3[3 * i], normal3[3 * i + 1], normal3[3 * i + 2], depth[i]);
 }
 
+/* per-view maps of a scene, carved from one arena kept in the context */
 struct SceneMaps {
     std::vector<float *> img, depth_a, depth_g, normal, cost;
-    ~SceneMaps()
-    {
-        for (auto *v : {&img, &depth_a, &depth_g, &normal, &cost})
-            for (float *p : *v) cudaFree(p);
-    }
 };
 
 }  // namespace
@@ -310,26 +313,24 @@ extern "C" int hpm_run_scene(hpm_ctx *c, int n_views, const float *const *images
     if (r) return r;
     cudaStream_t s = c->stream;
     SceneMaps m;
+    size_t total = 0; /* floats: image, pass-A depth, geometric depth, normal (3), cost */
+    for (int v = 0; v < n_views; ++v) total += 7 * (((size_t)cams[v].width * cams[v].height + 63) & ~(size_t)63);
+    CK(ctx_scene_arena(c, total * sizeof(float)), "scene buffers");
+    float *cur = ctx_scene_base(c);
     for (int v = 0; v < n_views; ++v) {
-        const size_t np = (size_t)cams[v].width * cams[v].height;
-        float *a = nullptr, *b = nullptr, *d = nullptr, *nn = nullptr, *cc = nullptr;
-        cudaMalloc(&a, sizeof(float) * np);
-        cudaMalloc(&b, sizeof(float) * np);
-        cudaMalloc(&d, sizeof(float) * np);
-        cudaMalloc(&nn, sizeof(float) * 3 * np);
-        cudaError_t e = cudaMalloc(&cc, sizeof(float) * np);
-        m.img.push_back(a);
-        m.depth_a.push_back(b);
-        m.depth_g.push_back(d);
-        m.normal.push_back(nn);
-        m.cost.push_back(cc);
-        CK(e, "scene buffers");
-        CK(cudaMemcpyAsync(a, images[v], sizeof(float) * np, cudaMemcpyDefault, s), "scene images");
+        const size_t np = (size_t)cams[v].width * cams[v].height, st = (np + 63) & ~(size_t)63;
+        m.img.push_back(cur);
+        m.depth_a.push_back(cur + st);
+        m.depth_g.push_back(cur + 2 * st);
+        m.normal.push_back(cur + 3 * st);
+        m.cost.push_back(cur + 6 * st);
+        cur += 7 * st;
+        CK(cudaMemcpyAsync(m.img[v], images[v], sizeof(float) * np, cudaMemcpyDefault, s), "scene images");
     }
-    const float *pimg[kMaxViews];
-    float *pdep[kMaxViews];
-    HpmCamera pcam[kMaxViews];
-    auto load_problem = [&](int p) -> int {
+    /* the views of problem p on context cc */
+    auto load_problem = [&](hpm_ctx *cc, int p) -> int {
+        const float *pimg[kMaxViews];
+        HpmCamera pcam[kMaxViews];
         const int ref = ref_ids[p], ns = src_counts[p];
         pimg[0] = m.img[ref];
         pcam[0] = cams[ref];
@@ -338,17 +339,55 @@ extern "C" int hpm_run_scene(hpm_ctx *c, int n_views, const float *const *images
             pimg[j + 1] = m.img[sv];
             pcam[j + 1] = cams[sv];
         }
-        return hpm_set_views(c, pimg, pcam, ns + 1);
+        return hpm_set_views(cc, pimg, pcam, ns + 1);
     };
-    /* pass set A: ProcessProblem(geom = false, planar_prior) for every view */
-    for (int p = 0; p < n_problems; ++p) {
-        r = load_problem(p);
-        if (r) return r;
-        HpmProblemOpts po = {o->planar_prior, 0, 0, o->seed + (uint64_t)p, o->pyramid_levels};
-        const int ref = ref_ids[p];
-        r = hpm_process_problem(c, &po, m.depth_a[ref], m.normal[ref], m.cost[ref], nullptr);
-        if (r) return r;
+    CK(cudaStreamSynchronize(s), "scene images");
+    /* pass set A: ProcessProblem(geom = false, planar_prior) for every view.
+     * The problems are independent; with two workers they are handed out to
+     * this context and its peer from two host threads that pass the GPU
+     * token (see hpm_ctx::gpu_token). */
+    {
+        const int workers = (c->scene_workers > 1 && n_problems > 1) ? 2 : 1;
+        if (workers == 2 && !c->peer) {
+            r = hpm_create(&c->peer, c->device);
+            if (r) return ctx_fail(c, r, "hpm_run_scene: second context");
+        }
+        std::mutex token;
+        hpm_ctx *ctxs[2] = {c, workers == 2 ? c->peer : nullptr};
+        if (workers == 2) c->gpu_token = c->peer->gpu_token = &token;
+        std::atomic<int> next{0};
+        int rcs[2] = {HPM_OK, HPM_OK};
+        auto work = [&](int wi) {
+            hpm_ctx *cc = ctxs[wi];
+            for (;;) {
+                const int p = next.fetch_add(1);
+                if (p >= n_problems) return;
+                std::unique_lock<std::mutex> hold(token);
+                int rr = load_problem(cc, p);
+                if (!rr) {
+                    HpmProblemOpts po = {o->planar_prior, 0, 0, o->seed + (uint64_t)p, o->pyramid_levels};
+                    const int ref = ref_ids[p];
+                    rr = hpm_process_problem(cc, &po, m.depth_a[ref], m.normal[ref], m.cost[ref], nullptr);
+                }
+                if (rr) {
+                    rcs[wi] = rr;
+                    next.store(n_problems); /* stop the other worker too */
+                    return;
+                }
+            }
+        };
+        if (workers == 2) {
+            std::thread helper(work, 1);
+            work(0);
+            helper.join();
+            c->gpu_token = c->peer->gpu_token = nullptr;
+        } else {
+            work(0);
+        }
+        if (rcs[0]) return rcs[0];
+        if (rcs[1]) return ctx_fail(c, rcs[1], "hpm_run_scene (second context): %s", hpm_last_error(c->peer));
     }
+    float *pdep[kMaxViews];
     /* pass set B: geometric iterations (main.cpp:662-674) */
     for (int gi = 0; gi < o->geom_iterations; ++gi) {
         std::vector<float *> &src_depths = gi == 0 ? m.depth_a : m.depth_g;
@@ -358,7 +397,7 @@ extern "C" int hpm_run_scene(hpm_ctx *c, int n_views, const float *const *images
                                    cudaMemcpyDeviceToDevice, s),
                    "scene copy");
         for (int p = 0; p < n_problems; ++p) {
-            r = load_problem(p);
+            r = load_problem(c, p);
             if (r) return r;
             const int ref = ref_ids[p], ns = src_counts[p];
             pdep[0] = src_depths[ref];

@@ -147,12 +147,32 @@ __global__ void k_tri_planes(HpmCamera cam, const float *__restrict__ depth, int
     planes[t] = plane_from_vertices(cam, depth, w, v, factor);
 }
 
-/* Raster of main.cpp:96-116 for kept triangle t (id t+1).  The loop runs in
+/* Raster of main.cpp:96-116 for kept triangle t (id t+1).  The loops run in
  * float with the reference's mixed float/double expression; the largest id
- * wins a pixel, as sequential overwriting in triangle order does. */
-__global__ void k_tri_raster(const int *__restrict__ tris, int n, int w, int *__restrict__ ids)
+ * wins a pixel, as sequential overwriting in triangle order does.
+ *
+ * One warp per triangle.  Both loop variables start at 0 and advance by the
+ * same float step, so they walk the same sequence of partial sums: lane 0
+ * writes it to shared memory once, and the lanes split the outer loop.  A
+ * triangle whose sequence does not fit (an edge longer than kSeq pixels)
+ * runs the reference's two loops on lane 0. */
+constexpr int kSeq = 2048;
+
+__device__ __forceinline__ void raster_px(const int *v, float p, float q, int w, int *ids, int id)
 {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const double rest = __dsub_rn(__dsub_rn(1.0, (double)p), (double)q);
+    const double xs = __dadd_rn((double)__fadd_rn(__fmul_rn(p, (float)v[0]), __fmul_rn(q, (float)v[2])),
+                                __dmul_rn(rest, (double)v[4]));
+    const double ys = __dadd_rn((double)__fadd_rn(__fmul_rn(p, (float)v[1]), __fmul_rn(q, (float)v[3])),
+                                __dmul_rn(rest, (double)v[5]));
+    atomicMax(&ids[(size_t)(int)ys * w + (int)xs], id);
+}
+
+__global__ void __launch_bounds__(128) k_tri_raster(const int *__restrict__ tris, int n, int w, int *__restrict__ ids)
+{
+    __shared__ float seq_s[4][kSeq];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int t = blockIdx.x * 4 + warp;
     if (t >= n) return;
     const int *v = tris + 6 * t;
     const float L01 = (float)sqrt((double)(v[0] - v[2]) * (v[0] - v[2]) + (double)(v[1] - v[3]) * (v[1] - v[3]));
@@ -160,16 +180,29 @@ __global__ void k_tri_raster(const int *__restrict__ tris, int n, int w, int *__
     const float L12 = (float)sqrt((double)(v[2] - v[4]) * (v[2] - v[4]) + (double)(v[3] - v[5]) * (v[3] - v[5]));
     const float mx = fmaxf(L01, fmaxf(L02, L12));
     const float step = (float)(1.0 / (double)mx);
-    for (float p = 0; (double)p < 1.0; p = __fadd_rn(p, step)) {
-        for (float q = 0; (double)q < 1.0 - (double)p; q = __fadd_rn(q, step)) {
-            const double rest = __dsub_rn(__dsub_rn(1.0, (double)p), (double)q);
-            const double xs = __dadd_rn((double)__fadd_rn(__fmul_rn(p, (float)v[0]), __fmul_rn(q, (float)v[2])),
-                                        __dmul_rn(rest, (double)v[4]));
-            const double ys = __dadd_rn((double)__fadd_rn(__fmul_rn(p, (float)v[1]), __fmul_rn(q, (float)v[3])),
-                                        __dmul_rn(rest, (double)v[5]));
-            const int x = (int)xs, y = (int)ys;
-            atomicMax(&ids[(size_t)y * w + x], t + 1);
+    float *seq = seq_s[warp];
+    int len = 0, fits = 1;
+    if (lane == 0) {
+        float p = 0;
+        while ((double)p < 1.0 && len < kSeq) {
+            seq[len++] = p;
+            p = __fadd_rn(p, step);
         }
+        fits = (double)p >= 1.0;
+    }
+    len = __shfl_sync(0xffffffffu, len, 0);
+    fits = __shfl_sync(0xffffffffu, fits, 0);
+    __syncwarp();
+    if (!fits) {
+        if (lane == 0)
+            for (float p = 0; (double)p < 1.0; p = __fadd_rn(p, step))
+                for (float q = 0; (double)q < 1.0 - (double)p; q = __fadd_rn(q, step)) raster_px(v, p, q, w, ids, t + 1);
+        return;
+    }
+    for (int k = lane; k < len; k += 32) {
+        const float p = seq[k];
+        const double lim = 1.0 - (double)p;
+        for (int m = 0; m < len && (double)seq[m] < lim; ++m) raster_px(v, p, seq[m], w, ids, t + 1);
     }
 }
 
@@ -410,7 +443,7 @@ cudaError_t prior_triangles(const HpmCamera &cam, const float *depth, int w, int
     cudaError_t e = cudaMemsetAsync(ids, 0, sizeof(int) * (size_t)w * h, s);
     if (e != cudaSuccess || n == 0) return e;
     k_tri_planes<<<(n + 127) / 128, 128, 0, s>>>(cam, depth, w, tris, n, factor, planes);
-    k_tri_raster<<<(n + 127) / 128, 128, 0, s>>>(tris, n, w, ids);
+    k_tri_raster<<<(n + 3) / 4, 128, 0, s>>>(tris, n, w, ids);
     return cudaGetLastError();
 }
 

@@ -38,7 +38,7 @@ EXPORTED = [
     "hpm_count_enable", "hpm_count_read", "hpm_write_dmb", "hpm_read_dmb", "hpm_read_camera", "hpm_read_pair",
     "hpm_fp32_peak", "hpm_jbu_noalloc", "hpm_process_problem", "hpm_last_prior_stats", "hpm_delaunay",
     "hpm_prior_level", "hpm_run_scene", "hpm_read_gray8", "hpm_resize_linear",
-    "hpm_fuse", "hpm_write_ply", "hpm_read_bgr8",
+    "hpm_fuse", "hpm_write_ply", "hpm_read_bgr8", "hpm_set_scene_workers",
 ]
 
 
@@ -337,6 +337,9 @@ class Context:
 
     def count_enable(self, on: bool = True) -> None:
         self._check(lib().hpm_count_enable(self._h, int(on)), "hpm_count_enable")
+
+    def set_scene_workers(self, workers: int) -> None:
+        self._check(lib().hpm_set_scene_workers(self._h, int(workers)), "hpm_set_scene_workers")
 
     def count_read(self):
         a = ctypes.c_uint64()

@@ -169,6 +169,17 @@ typedef struct {
 int hpm_run_scene(hpm_ctx *ctx, int n_views, const float *const *images, const HpmCamera *cams, int n_problems,
                   const int *ref_ids, const int *src_counts, const int *src_ids, const HpmSceneOpts *opts,
                   float *const *depths, float *const *normals, float *const *costs);
+/* Host threads of hpm_run_scene's pass set A (1 or 2, default 2; no
+ * counterpart in the reference).  With 2, pass set A's problems go to this
+ * context and a second one on the same device (created on first use, freed
+ * with this one; it holds its own working buffers, about as much device
+ * memory again) from two host threads.  Only one thread's kernels run at a
+ * time; the other thread may meanwhile triangulate support points on the
+ * host, so the GPU does not wait for the Delaunay.  The maps do not depend on
+ * the setting: each problem draws from its own seed.  The geometric
+ * iterations always run on this context, problem after problem.  Counters
+ * and CUDA-event profiles cover this context's work only. */
+int hpm_set_scene_workers(hpm_ctx *ctx, int workers);
 
 /* Parity entry point: the prior of one pyramid level (0: 1/4 scale, 1: 1/2
  * scale, 2: full scale) built from given full-resolution maps of the current

@@ -251,3 +251,23 @@ def test_view_sharded_driver_on_the_gpu():
     for v in range(nv):
         np.testing.assert_array_equal(got[v], cur[v])
         np.testing.assert_array_equal(all_depth[v].cpu().numpy(), cur[v])
+
+
+def test_scene_workers_give_the_same_maps():
+    """Pass set A on one or on two contexts (hpm_set_scene_workers): the
+    problems are independent and each draws from its own seed, so the maps
+    are identical."""
+    nv = 4
+    sc = syn.make_scene(17, 128, 96, nv, n_planes=4, low_texture=0.3)
+    imgs = [sc.images[v].astype(np.float32) for v in range(nv)]
+    pairs = [(v, list(sc.pairs[v][1])) for v in range(nv)]
+    outs = []
+    for workers in (1, 2):
+        with hb.Context() as ctx:
+            ctx.set_scene_workers(workers)
+            outs.append(ctx.run_scene(imgs, sc.cams, pairs, seed=3, pyramid_levels=1, geom_iterations=2))
+            outs.append(ctx.run_scene(imgs, sc.cams, pairs, seed=3, pyramid_levels=1, geom_iterations=2))
+    for k in range(3):
+        for v in range(nv):
+            for o in outs[1:]:
+                np.testing.assert_array_equal(outs[0][k][v], o[k][v])
