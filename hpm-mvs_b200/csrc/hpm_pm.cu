@@ -134,6 +134,15 @@ __device__ __forceinline__ float texel(const float *__restrict__ img, int w, int
     return __ldg(img + (size_t)y * w + x);
 }
 
+/* The hoisted reference window has one entry per tap and pixel in shared
+ * memory: (weight, weight x reference pixel) as float2 (WinPair), or the
+ * weight alone (WinWeight), the reference pixel then being re-read through
+ * L1 at each use.  The weight-only form halves the shared memory; it suits
+ * k_init (2.75 against 4.7 ms at 1600x1200), while in the half-step kernels
+ * the extra L1 loads compete with the texture path (10.2 against 5.4 ms). */
+typedef float2 WinPair;
+typedef float WinWeight;
+
 /* ------------------------------------------------------------------ */
 /* Geometry (HPM.cu:65-133, 227-316, 445-481)                           */
 /* ------------------------------------------------------------------ */
@@ -292,7 +301,8 @@ struct RefStats {
 /* The reference-side half of ComputeBilateralNCC (HPM.cu:318-386) for pixel
  * (px, py): per-tap (weight, weight*ref) into shared memory as one float2,
  * sums in the reference's row-then-total order.  sWW is [tap][kBlock]. */
-__device__ RefStats ref_window(const PMArgs &a, int px, int py, float2 *sWW, int tid)
+template <typename Win>
+__device__ RefStats ref_window(const PMArgs &a, int px, int py, Win *sWW, int tid)
 {
     const ViewDev &rv = a.view[0];
     const float center = texel(rv.img, rv.w, rv.h, px, py);
@@ -307,7 +317,10 @@ __device__ RefStats ref_window(const PMArgs &a, int px, int py, float2 *sWW, int
             const float color_dist = fabsf(rp - center);
             const float wgt = expf(-spatial_dist / (2.0f * a.sigma_spatial * a.sigma_spatial) -
                                    color_dist / (2.0f * a.sigma_color * a.sigma_color));
-            sWW[t * kBlock + tid] = make_float2(wgt, wgt * rp);
+            if constexpr (sizeof(Win) == sizeof(float))
+                sWW[t * kBlock + tid] = wgt;
+            else
+                sWW[t * kBlock + tid] = make_float2(wgt, wgt * rp);
             r_ref += wgt * rp;
             r_rr += wgt * rp * rp;
             r_w += wgt;
@@ -325,7 +338,8 @@ __device__ RefStats ref_window(const PMArgs &a, int px, int py, float2 *sWW, int
 }
 
 /* The source-side half of ComputeBilateralNCC (HPM.cu:325-397). */
-__device__ __forceinline__ float ncc(const PMArgs &a, int v, int px, int py, float4 h, const float2 *sWW, int tid,
+template <typename Win>
+__device__ __forceinline__ float ncc(const PMArgs &a, int v, int px, int py, float4 h, const Win *sWW, int tid,
                                      const RefStats &rs)
 {
     const HpmCamera &sc = a.cam[v];
@@ -345,7 +359,13 @@ __device__ __forceinline__ float ncc(const PMArgs &a, int v, int px, int py, flo
         for (int j = -5; j < 6; j += 2, ++t) {
             const float2 q = warp(H, fpx + (float)i, fpy + (float)j);
             const float sp = tex2D<float>(tex, q.x + 0.5f, q.y + 0.5f);
-            const float2 ww = sWW[t * kBlock + tid];
+            float2 ww;
+            if constexpr (sizeof(Win) == sizeof(float)) {
+                const float wt = sWW[t * kBlock + tid];
+                ww = make_float2(wt, wt * texel(a.view[0].img, a.view[0].w, a.view[0].h, px + i, py + j));
+            } else {
+                ww = sWW[t * kBlock + tid];
+            }
             r_src += ww.x * sp;
             r_ss += ww.x * sp * sp;
             r_rs += ww.y * sp;
@@ -369,7 +389,8 @@ __device__ __forceinline__ float ncc(const PMArgs &a, int v, int px, int py, flo
 #ifndef HPM_NCC_CALL
 #define HPM_NCC_CALL __forceinline__
 #endif
-__device__ HPM_NCC_CALL float ncc_call(const PMArgs &a, int v, int px, int py, float4 h, const float2 *sWW, int tid,
+template <typename Win>
+__device__ HPM_NCC_CALL float ncc_call(const PMArgs &a, int v, int px, int py, float4 h, const Win *sWW, int tid,
                                         RefStats rs)
 {
     return ncc(a, v, px, py, h, sWW, tid, rs);
@@ -377,7 +398,8 @@ __device__ HPM_NCC_CALL float ncc_call(const PMArgs &a, int v, int px, int py, f
 
 /* ComputeMultiViewCostVector (HPM.cu:438-443) into out[v * stride].  Kept
  * out of line so that the 36-tap loop exists once in the binary. */
-__device__ HPM_CV_INLINE void cost_vector(const PMArgs &a, int px, int py, float4 h, const float2 *sWW, int tid,
+template <typename Win>
+__device__ HPM_CV_INLINE void cost_vector(const PMArgs &a, int px, int py, float4 h, const Win *sWW, int tid,
                                          RefStats rs, float *out, int stride)
 {
     for (int v = 1; v < a.n; ++v) out[(v - 1) * stride] = ncc(a, v, px, py, h, sWW, tid, rs);
@@ -512,7 +534,7 @@ __device__ __forceinline__ float *cache_at(const PMArgs &a, int v, int center)
 /* RandomInitialization, HPM.cu:510-558.  One thread per pixel. */
 __global__ void __launch_bounds__(kBlock) k_init(const __grid_constant__ PMArgs a)
 {
-    __shared__ float2 sWW[kTaps * kBlock];
+    __shared__ WinWeight sWW[kTaps * kBlock];
     __shared__ float sCV[kMaxSrc * kBlock];
     const int tid = threadIdx.y * kBlockX + threadIdx.x;
     const int px = blockIdx.x * kBlockX + threadIdx.x;
@@ -671,7 +693,7 @@ __device__ __forceinline__ bool same_plane(float4 p, float4 q)
 __global__ void __launch_bounds__(kBlock, HPM_P1_MIN_BLOCKS) k_prop_dirs(const __grid_constant__ PMArgs a, int iter,
                                                                           int color)
 {
-    __shared__ float2 sWW[kTaps * kBlock];
+    __shared__ WinPair sWW[kTaps * kBlock];
     const int tid = threadIdx.y * kBlockX + threadIdx.x;
     int px, py;
     half_step_pixel(color, px, py);
@@ -783,7 +805,7 @@ template <int SMAX>
 __global__ void __launch_bounds__(kBlock, HPM_P2_MIN_BLOCKS) k_prop_refine(const __grid_constant__ PMArgs a, int iter,
                                                                             int color)
 {
-    __shared__ float2 sWW[kTaps * kBlock];
+    __shared__ WinPair sWW[kTaps * kBlock];
     const int tid = threadIdx.y * kBlockX + threadIdx.x;
     int px, py;
     half_step_pixel(color, px, py);
@@ -1147,7 +1169,7 @@ __global__ void k_filter(const __grid_constant__ PMArgs a, float4 *pl, const flo
 __global__ void __launch_bounds__(kBlock) k_cost_vectors(const __grid_constant__ PMArgs a, const float4 *planes,
                                                           float *out)
 {
-    __shared__ float2 sWW[kTaps * kBlock];
+    __shared__ WinPair sWW[kTaps * kBlock];
     const int tid = threadIdx.y * kBlockX + threadIdx.x;
     const int px = blockIdx.x * kBlockX + threadIdx.x;
     const int py = blockIdx.y * kBlockY + threadIdx.y;
@@ -1161,7 +1183,7 @@ __global__ void __launch_bounds__(kBlock) k_cost_vectors(const __grid_constant__
 __global__ void __launch_bounds__(kBlock) k_initial_costs(const __grid_constant__ PMArgs a, const float4 *planes,
                                                           float *cost, uint32_t *views)
 {
-    __shared__ float2 sWW[kTaps * kBlock];
+    __shared__ WinPair sWW[kTaps * kBlock];
     __shared__ float sCV[kMaxSrc * kBlock];
     const int tid = threadIdx.y * kBlockX + threadIdx.x;
     const int px = blockIdx.x * kBlockX + threadIdx.x;
