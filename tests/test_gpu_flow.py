@@ -7,6 +7,7 @@ import pytest
 
 import flow as oflow
 import hpm_b200 as hb
+import oracle as orc
 import synthetic as syn
 
 pytestmark = pytest.mark.gpu
@@ -271,3 +272,30 @@ def test_scene_workers_give_the_same_maps():
         for v in range(nv):
             for o in outs[1:]:
                 np.testing.assert_array_equal(outs[0][k][v], o[k][v])
+
+
+@pytest.mark.skipif(not orc.ref_available(), reason="reference shim oracle/_ref not built")
+def test_prior_flow_accuracy_matches_reference_kernels():
+    """Pass set A (plain pass + planar prior on two pyramid levels) through
+    the product and through the reference's own kernels (oracle/_ref, with
+    the host stages restated): %px with relative depth error < 1% at most
+    0.5 pp below the reference's and median normal error at most 1 degree
+    above (equal or better), averaged over four views and two seeds of a
+    400x300 scene."""
+    sc = syn.make_scene(21, 400, 300, 6, n_planes=8, n_spheres=2, low_texture=0.4)
+    ra, rn, ga, gn = [], [], [], []
+    with hb.Context() as ctx:
+        for ref in (1, 2, 3, 4):
+            imgs, cams = syn.view_set(sc, ref)
+            gt, gtn = sc.gt_depth[ref], sc.gt_normal[ref]
+            for s in range(2):
+                d, n, _, _ = oflow.process_problem(imgs, cams, seed=50 + 10 * ref + s, pyramid_levels=1,
+                                                   backend="reference")
+                ra.append(syn.depth_accuracy(d, gt))
+                rn.append(syn.normal_error_deg(n, gtn, gt))
+                ctx.set_views(imgs, cams)
+                d, n, _, _ = ctx.process_problem(seed=10 * ref + s, pyramid_levels=1)
+                ga.append(syn.depth_accuracy(d, gt))
+                gn.append(syn.normal_error_deg(n, gtn, gt))
+    assert np.mean(ga) >= np.mean(ra) - 0.005, (np.mean(ra), np.mean(ga))
+    assert np.mean(gn) <= np.mean(rn) + 1.0, (np.mean(rn), np.mean(gn))
