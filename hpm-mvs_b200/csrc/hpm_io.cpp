@@ -9,11 +9,12 @@
  *   pair.txt  N, then per problem: ref_id, n_src, n_src x (id score); sources
  *             with score <= 0 are dropped (GenerateSampleList, main.cpp:4-33)
  *   images    8-bit grayscale as cv::imread(path, IMREAD_GRAYSCALE) returns it
- *             (HPM.cpp:492): binary PGM (P5, maxval 255) and PNG (8-bit gray,
- *             gray+alpha, RGB, RGBA, palette; not interlaced).  Colour is
- *             reduced the way libpng's rgb_to_gray does it for OpenCV's
- *             coefficients 0.299/0.587: (9797 R + 19234 G + 3737 B) >> 15,
- *             alpha is dropped.  JPEG is not decoded here.
+ *             (HPM.cpp:492), and B, G, R as IMREAD_COLOR (main.cpp:523):
+ *             JPEG (hpm_jpeg.cpp), binary PGM (P5, maxval 255) and PNG (8-bit
+ *             gray, gray+alpha, RGB, RGBA, palette; not interlaced).  PNG
+ *             colour is reduced the way libpng's rgb_to_gray does it for
+ *             OpenCV's coefficients 0.299/0.587: (9797 R + 19234 G + 3737 B)
+ *             >> 15, alpha is dropped.
  *
  * Unlike the reference (which prints and carries on, or dereferences NULL on
  * a failed fopen), every failure returns HPM_ERR_IO.
@@ -29,6 +30,7 @@
 #include <zlib.h>
 
 #include "hpm_b200.h"
+#include "hpm_jpeg.h"
 
 extern "C" {
 
@@ -315,7 +317,10 @@ static int read_image8(const char *path, uint8_t *pixels, size_t cap, int *w, in
     std::vector<uint8_t> bytes, px;
     if (!read_file(path, bytes) || bytes.size() < 2) return HPM_ERR_IO;
     int r;
-    if (bytes[0] == 'P' && bytes[1] == '5') {
+    if (bytes[0] == 0xFF && bytes[1] == 0xD8) {
+        if (!pixels) return hpm_jpeg_size(bytes.data(), bytes.size(), w, h); /* size query: markers only */
+        r = hpm_decode_jpeg(bytes.data(), bytes.size(), px, w, h, out_ch);
+    } else if (bytes[0] == 'P' && bytes[1] == '5') {
         r = decode_pgm(bytes, px, w, h);
         if (!r && out_ch == 3) {
             std::vector<uint8_t> c(px.size() * 3);

@@ -9,9 +9,15 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
+#include <exception>
 #include <iomanip>
 #include <iostream>
+#include <map>
+#include <memory>
+#include <mutex>
 #include <sstream>
+#include <thread>
 
 namespace hpm_host {
 
@@ -52,26 +58,100 @@ void make_dir(const std::string &p)
     if (mkdir(p.c_str(), 0755) != 0 && !exists(p)) throw Error(HPM_ERR_IO, "cannot create " + p);
 }
 
-/* images/%08d.jpg in the reference; PNG and PGM are decoded here, JPEG by
- * the Python front end (cv2) or after conversion. */
-std::vector<float> read_image(const std::string &dense_folder, int id, int *w, int *h)
+/* images/%08d.jpg in the reference (HPM.cpp:490); .png and .pgm are also
+ * accepted, in that order after .jpg. */
+std::string image_path(const std::string &dense_folder, int id)
 {
     const std::string base = dense_folder + "/images";
-    for (const char *ext : {".png", ".pgm"}) {
+    for (const char *ext : {".jpg", ".png", ".pgm"}) {
         const std::string p = id_path(base, id, ext);
-        if (!exists(p)) continue;
-        int rc = hpm_read_gray8(p.c_str(), nullptr, 0, w, h);
-        if (rc != HPM_OK) throw Error(rc, "cannot decode " + p);
-        std::vector<uint8_t> px((size_t)*w * *h);
-        rc = hpm_read_gray8(p.c_str(), px.data(), px.size(), w, h);
-        if (rc != HPM_OK) throw Error(rc, "cannot decode " + p);
-        return std::vector<float>(px.begin(), px.end()); /* convertTo(CV_32FC1), HPM.cpp:494 */
+        if (exists(p)) return p;
     }
-    const std::string jpg = id_path(base, id, ".jpg");
-    if (exists(jpg))
-        throw Error(HPM_ERR_IO, jpg + ": JPEG is not decoded by the C++ host; run hpm-mvs_b200/hpm_mvs.py (OpenCV "
-                                      "decoding) or convert images/ to PNG");
     throw Error(HPM_ERR_IO, "no image for view " + std::to_string(id) + " under " + base);
+}
+
+/* Decoded images, kept for the whole process: the reference decodes every
+ * view again for each problem and pass (11 views x 3 passes per problem of
+ * a plain scene); here each file is decoded once while its size and
+ * modification time stay the same.  HPM_IMAGE_CACHE_MB bounds the bytes
+ * kept (default 8192, 0 disables); the oldest entries leave first. */
+class ImageCache {
+public:
+    using Pixels = std::shared_ptr<const std::vector<uint8_t>>;
+
+    /* keep false: decode without storing (a file read once) */
+    Pixels get(const std::string &path, int channels, int *w, int *h, bool keep = true)
+    {
+        struct stat st;
+        if (stat(path.c_str(), &st) != 0) throw Error(HPM_ERR_IO, "cannot read " + path);
+        const std::string key = path + (channels == 3 ? "#bgr" : "#gray");
+        {
+            std::lock_guard<std::mutex> g(mu_);
+            auto it = map_.find(key);
+            if (it != map_.end() && it->second.size == (long long)st.st_size &&
+                it->second.mtime_ns == mtime_ns(st)) {
+                *w = it->second.w;
+                *h = it->second.h;
+                return it->second.px;
+            }
+        }
+        auto read = channels == 3 ? hpm_read_bgr8 : hpm_read_gray8;
+        int rc = read(path.c_str(), nullptr, 0, w, h);
+        if (rc != HPM_OK) throw Error(rc, "cannot decode " + path);
+        auto px = std::make_shared<std::vector<uint8_t>>((size_t)*w * *h * channels);
+        rc = read(path.c_str(), px->data(), px->size(), w, h);
+        if (rc != HPM_OK) throw Error(rc, "cannot decode " + path);
+        std::lock_guard<std::mutex> g(mu_);
+        const size_t cap = cap_bytes();
+        if (keep && px->size() <= cap) {
+            auto old = map_.find(key);
+            if (old != map_.end()) {
+                bytes_ -= old->second.px->size();
+                map_.erase(old);
+            }
+            while (bytes_ + px->size() > cap && !map_.empty()) {
+                auto oldest = std::min_element(map_.begin(), map_.end(), [](const auto &a, const auto &b) {
+                    return a.second.order < b.second.order;
+                });
+                bytes_ -= oldest->second.px->size();
+                map_.erase(oldest);
+            }
+            map_[key] = Entry{px, *w, *h, (long long)st.st_size, mtime_ns(st), next_++};
+            bytes_ += px->size();
+        }
+        return px;
+    }
+
+private:
+    struct Entry {
+        Pixels px;
+        int w, h;
+        long long size, mtime_ns;
+        unsigned long long order;
+    };
+    static long long mtime_ns(const struct stat &st) { return (long long)st.st_mtim.tv_sec * 1000000000LL + st.st_mtim.tv_nsec; }
+    static size_t cap_bytes()
+    {
+        const char *e = getenv("HPM_IMAGE_CACHE_MB");
+        const long long mb = e ? atoll(e) : 8192;
+        return mb > 0 ? (size_t)mb << 20 : 0;
+    }
+    std::mutex mu_;
+    std::map<std::string, Entry> map_;
+    size_t bytes_ = 0;
+    unsigned long long next_ = 0;
+};
+
+ImageCache &image_cache()
+{
+    static ImageCache c;
+    return c;
+}
+
+std::vector<float> read_image(const std::string &dense_folder, int id, int *w, int *h)
+{
+    const auto px = image_cache().get(image_path(dense_folder, id), 1, w, h);
+    return std::vector<float>(px->begin(), px->end()); /* convertTo(CV_32FC1), HPM.cpp:494 */
 }
 
 std::vector<float> read_dmb(const std::string &path, int *w, int *h, int want_nb)
@@ -138,34 +218,51 @@ void HPM::InuputInitialization(const std::string &dense_folder, const Problem &p
     std::vector<int> ids{problem.ref_image_id};
     ids.insert(ids.end(), problem.src_image_ids.begin(), problem.src_image_ids.end());
     if ((int)ids.size() > HPM_MAX_IMAGES) throw Error(HPM_ERR_ARG, "more than 32 source images");
-    for (int id : ids) {
-        int w = 0, h = 0;
-        std::vector<float> img = read_image(dense_folder, id, &w, &h);
-        HpmCamera cam{};
-        const std::string cp = id_path(dense_folder + "/cams", id, "_cam.txt");
-        int rc = hpm_read_camera(cp.c_str(), &cam);
-        if (rc != HPM_OK) throw Error(rc, "cannot read " + cp);
-        /* the image cap of HPM.cpp:525-551 */
-        const int cap = 3200;
-        if (w > cap || h > cap) {
-            const float factor = std::min((float)cap / w, (float)cap / h);
-            const int nw = (int)std::round(w * factor), nh = (int)std::round(h * factor);
-            const float sx = nw / (float)w, sy = nh / (float)h;
-            std::vector<float> scaled((size_t)nw * nh);
-            check(hpm_resize_linear(img.data(), w, h, 1, scaled.data(), nw, nh), "image cap");
-            img.swap(scaled);
-            cam.K[0] *= sx;
-            cam.K[2] *= sx;
-            cam.K[4] *= sy;
-            cam.K[5] *= sy;
-            w = nw;
-            h = nh;
+    const size_t n = ids.size();
+    images_.resize(n);
+    cameras_.resize(n);
+    /* the views of a problem are read and decoded on threads of their own */
+    std::vector<std::exception_ptr> errors(n);
+    auto load = [&](size_t i) {
+        try {
+            const int id = ids[i];
+            int w = 0, h = 0;
+            std::vector<float> img = read_image(dense_folder, id, &w, &h);
+            HpmCamera cam{};
+            const std::string cp = id_path(dense_folder + "/cams", id, "_cam.txt");
+            int rc = hpm_read_camera(cp.c_str(), &cam);
+            if (rc != HPM_OK) throw Error(rc, "cannot read " + cp);
+            /* the image cap of HPM.cpp:525-551 */
+            const int cap = 3200;
+            if (w > cap || h > cap) {
+                const float factor = std::min((float)cap / w, (float)cap / h);
+                const int nw = (int)std::round(w * factor), nh = (int)std::round(h * factor);
+                const float sx = nw / (float)w, sy = nh / (float)h;
+                std::vector<float> scaled((size_t)nw * nh);
+                rc = hpm_resize_linear(img.data(), w, h, 1, scaled.data(), nw, nh);
+                if (rc != HPM_OK) throw Error(rc, "image cap");
+                img.swap(scaled);
+                cam.K[0] *= sx;
+                cam.K[2] *= sx;
+                cam.K[4] *= sy;
+                cam.K[5] *= sy;
+                w = nw;
+                h = nh;
+            }
+            cam.width = w;
+            cam.height = h;
+            images_[i] = std::move(img);
+            cameras_[i] = cam;
+        } catch (...) {
+            errors[i] = std::current_exception();
         }
-        cam.width = w;
-        cam.height = h;
-        images_.push_back(std::move(img));
-        cameras_.push_back(cam);
-    }
+    };
+    std::vector<std::thread> workers;
+    for (size_t i = 1; i < n; ++i) workers.emplace_back(load, i);
+    load(0);
+    for (auto &t : workers) t.join();
+    for (auto &e : errors)
+        if (e) std::rethrow_exception(e);
     params_.depth_min = cameras_[0].depth_min * 0.6f;
     params_.depth_max = cameras_[0].depth_max * 1.2f;
     depths_.clear();
@@ -381,15 +478,13 @@ long long RunFusion(const std::string &dense_folder, const std::vector<Problem> 
         int rc = hpm_read_camera(cp.c_str(), &cam);
         if (rc != HPM_OK) throw Error(rc, "cannot read " + cp);
         int iw = 0, ih = 0;
-        std::string ip;
-        for (const char *ext : {".png", ".pgm"})
-            if (ip.empty() && exists(id_path(dense_folder + "/images", id, ext))) ip = id_path(dense_folder + "/images", id, ext);
-        if (ip.empty()) throw Error(HPM_ERR_IO, "no PNG/PGM colour image for view " + std::to_string(id));
-        rc = hpm_read_bgr8(ip.c_str(), nullptr, 0, &iw, &ih);
-        std::vector<uint8_t> bgr((size_t)3 * iw * ih);
-        if (rc == HPM_OK) rc = hpm_read_bgr8(ip.c_str(), bgr.data(), bgr.size(), &iw, &ih);
-        if (rc != HPM_OK) throw Error(rc, "cannot decode " + ip);
-        if (iw != w || ih != h) { /* RescaleImageAndCamera, HPM.cpp:187-208 */
+        const std::string ip = image_path(dense_folder, id);
+        std::vector<uint8_t> bgr(*image_cache().get(ip, 3, &iw, &ih, false));
+        if (iw != w || ih != h) {
+            /* RescaleImageAndCamera, HPM.cpp:187-208.  The reference resizes
+             * the 8-bit image with OpenCV's fixed-point bilinear; this is the
+             * float bilinear rounded, which differs from it by 1 in about an
+             * eighth of the colour bytes (images above the 3200-pixel cap). */
             std::vector<float> f(bgr.begin(), bgr.end()), g((size_t)3 * w * h);
             int r2 = hpm_resize_linear(f.data(), iw, ih, 3, g.data(), w, h);
             if (r2 != HPM_OK) throw Error(r2, "colour resize");

@@ -382,7 +382,7 @@ def read_camera(path: str) -> np.ndarray:
 
 
 def read_gray8(path: str) -> np.ndarray:
-    """images/ file as cv::imread(path, IMREAD_GRAYSCALE) gives it (PGM, PNG)."""
+    """images/ file as cv::imread(path, IMREAD_GRAYSCALE) gives it (JPEG, PNG, PGM)."""
     w, h = ctypes.c_int(), ctypes.c_int()
     rc = lib().hpm_read_gray8(path.encode(), None, ctypes.c_size_t(0), ctypes.byref(w), ctypes.byref(h))
     if rc != HPM_OK:

@@ -1,7 +1,7 @@
 #!/usr/bin/env python
-"""main() of HPM-MVS (main.cpp:636-677) from Python, for dense folders whose
-images/ are JPEG (decoded with OpenCV, as the reference does, HPM.cpp:492);
-the C++ host (hpm_mvs) reads PNG and PGM itself.
+"""main() of HPM-MVS (main.cpp:636-677) from Python, over the same C ABI as
+the C++ host (hpm_mvs): images/%08d.jpg (or .png, .pgm) decoded by the
+library to the bytes cv::imread gives (HPM.cpp:492, main.cpp:523).
 
     python hpm-mvs_b200/hpm_mvs.py dense_folder [--seed S] [--levels K]
                                    [--geom-iterations G] [--no-prior] [--device D]
@@ -33,14 +33,7 @@ def load_view(folder: str, vid: int):
     for ext in (".jpg", ".png", ".pgm"):
         p = os.path.join(folder, "images", f"{vid:08d}{ext}")
         if os.path.exists(p):
-            if ext == ".jpg":
-                import cv2
-
-                img = cv2.imread(p, cv2.IMREAD_GRAYSCALE)
-                if img is None:
-                    raise hb.HpmError(f"cannot decode {p}")
-            else:
-                img = hb.read_gray8(p)
+            img = hb.read_gray8(p)
             break
     if img is None:
         raise hb.HpmError(f"no image for view {vid} under {folder}/images")
@@ -85,10 +78,9 @@ def process_problem(ctx, folder, ref, srcs, views, *, geom, planar_prior, multi_
 
 
 def run_fusion(folder, problems, geom_consistency, device=0):
-    """RunFusion (main.cpp:502-633) with OpenCV's colour decoding and
-    RescaleImageAndCamera (HPM.cpp:187-208); returns the point count."""
-    import cv2
-
+    """RunFusion (main.cpp:502-633) with RescaleImageAndCamera
+    (HPM.cpp:187-208), whose 8-bit resize is OpenCV's own (cv2.resize, only
+    for images larger than their depth maps); returns the point count."""
     cams, depths, normals, colors = [], [], [], []
     for ref, _ in problems:
         out = os.path.join(folder, "HPM", f"2333_{ref:08d}")
@@ -99,12 +91,14 @@ def run_fusion(folder, problems, geom_consistency, device=0):
         for ext in (".jpg", ".png", ".pgm"):
             p = os.path.join(folder, "images", f"{ref:08d}{ext}")
             if os.path.exists(p):
-                img = cv2.imread(p, cv2.IMREAD_COLOR)
+                img = hb.read_bgr8(p)
                 break
         if img is None:
             raise hb.HpmError(f"no colour image for view {ref}")
         h, w = d.shape
         if img.shape[:2] != (h, w):
+            import cv2
+
             sx, sy = np.float32(w) / np.float32(img.shape[1]), np.float32(h) / np.float32(img.shape[0])
             img = cv2.resize(img, (w, h), interpolation=cv2.INTER_LINEAR)
             K = cam["K"]

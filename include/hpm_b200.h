@@ -307,13 +307,15 @@ int hpm_read_dmb(const char *path, float *data, size_t cap, int *h, int *w, int 
 /* cams/%08d_cam.txt (ReadCamera, HPM.cpp:160-185).  width/height are left 0. */
 int hpm_read_camera(const char *path, HpmCamera *cam);
 /* An 8-bit grayscale image as cv::imread(path, IMREAD_GRAYSCALE) returns it
- * for the reference's images/ folder (HPM.cpp:492): binary PGM or 8-bit PNG
- * (colour reduced as OpenCV's PNG reader does).  Sets *w, *h; copies the
- * pixels when pixels is non-NULL (capacity cap bytes). */
+ * for the reference's images/%08d.jpg (HPM.cpp:490-492): JPEG (baseline,
+ * extended sequential or progressive Huffman; EXIF orientation applied),
+ * binary PGM or 8-bit PNG (colour reduced as OpenCV's PNG reader does),
+ * recognised by content.  Sets *w, *h; copies the pixels when pixels is
+ * non-NULL (capacity cap bytes). */
 int hpm_read_gray8(const char *path, uint8_t *pixels, size_t cap, int *w, int *h);
 /* A colour image as cv::imread(path, IMREAD_COLOR) returns it for the
- * fusion (main.cpp:520): 3 bytes per pixel in B, G, R order; PGM and gray
- * PNG are replicated to the three channels, alpha is dropped. */
+ * fusion (main.cpp:520-523): 3 bytes per pixel in B, G, R order; gray JPEG,
+ * PGM and gray PNG are replicated to the three channels, alpha is dropped. */
 int hpm_read_bgr8(const char *path, uint8_t *pixels, size_t cap, int *w, int *h);
 /* cv::resize(src, dst, Size(dw, dh), 0, 0, INTER_LINEAR) of a float map
  * with ch interleaved channels, on the host: the image cap of

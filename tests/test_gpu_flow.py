@@ -174,24 +174,28 @@ def test_scene_driver_matches_per_view_loop():
     assert min(accs) > 0.5, accs
 
 
-def test_host_main_writes_the_scene_driver_maps(tmp_path):
+@pytest.mark.parametrize("ext", [".jpg", ".png"])
+def test_host_main_writes_the_scene_driver_maps(tmp_path, ext):
     """The C++ host (hpm_mvs: HPM class, ProcessProblem, main() over the C
     ABI, reading images/ + cams/ + pair.txt and writing .dmb files) and the
     Python front end give exactly the maps of hpm_run_scene on the same
-    decoded inputs and seeds."""
+    seeds and on the images as cv::imread decodes them (JPEG, the
+    reference's images/%08d.jpg, or PNG)."""
     import os
     import subprocess
     import sys
 
+    cv2 = pytest.importorskip("cv2")
     here = os.path.dirname(os.path.abspath(hb.__file__))
     sc = syn.make_scene(16, 160, 120, 4, n_planes=5, low_texture=0.3)
     folder = str(tmp_path / "scene")
-    syn.write_dense_folder(sc, folder, ".png")
+    syn.write_dense_folder(sc, folder, ext)
     r = subprocess.run([os.path.join(here, "hpm_mvs"), folder, "--seed", "7", "--levels", "1"], capture_output=True,
                        text=True, timeout=600)
     assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
     pairs = hb.read_pair(os.path.join(folder, "pair.txt"))
-    imgs = [hb.read_gray8(os.path.join(folder, "images", f"{v:08d}.png")).astype(np.float32) for v in range(4)]
+    imgs = [cv2.imread(os.path.join(folder, "images", f"{v:08d}{ext}"), cv2.IMREAD_GRAYSCALE).astype(np.float32)
+            for v in range(4)]
     cams = np.array([hb.read_camera(os.path.join(folder, "cams", f"{v:08d}_cam.txt")) for v in range(4)])
     for v in range(4):
         cams[v]["width"], cams[v]["height"] = 160, 120
@@ -206,7 +210,7 @@ def test_host_main_writes_the_scene_driver_maps(tmp_path):
         assert (hb.read_dmb(os.path.join(out, "depths_prior.dmb")) > 0).mean() > 0.3
     # the Python front end over the same folder
     py = str(tmp_path / "scene_py")
-    syn.write_dense_folder(sc, py, ".png")
+    syn.write_dense_folder(sc, py, ext)
     r = subprocess.run([sys.executable, os.path.join(here, "hpm_mvs.py"), py, "--seed", "7", "--levels", "1"],
                        capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
