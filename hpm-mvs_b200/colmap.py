@@ -17,7 +17,7 @@ writes them (colmap2mvsnet_acm.py:304-451):
                      points (integer scores); a pair whose 75th-percentile
                      triangulation angle is under 1 degree scores 0
   images/%08d.jpg    the images, renumbered in image-id order (--png: PNG
-                     instead, which the C++ host reads)
+                     instead)
 The view scores need no host pool: one pass over the 3D points' tracks
 accumulates every pair at once.
 """
@@ -247,7 +247,7 @@ def main(argv=None):
     ap.add_argument("--max_d", type=int, default=192)
     ap.add_argument("--interval_scale", type=float, default=1)
     ap.add_argument("--model_ext", default=".txt", choices=[".txt", ".bin"])
-    ap.add_argument("--png", action="store_true", help="write images/ as PNG (read by the C++ host)")
+    ap.add_argument("--png", action="store_true", help="write images/ as PNG instead of JPEG")
     a = ap.parse_args(argv)
     convert(a.dense_folder, a.save_folder, a.max_d, a.interval_scale, a.model_ext, a.png)
     return 0
