@@ -595,12 +595,19 @@ int hpm_profile_enable(hpm_ctx *c, int enable)
         cudaEventDestroy(p.second.second);
     }
     c->prof_events.clear();
+    if (c->peer) hpm_profile_enable(c->peer, enable);
     return HPM_OK;
 }
 
 int hpm_profile_read(hpm_ctx *c, float *ms4, int *counts4)
 {
     if (!c) return HPM_ERR_ARG;
+    float peer_ms[4] = {0, 0, 0, 0};
+    int peer_cnt[4] = {0, 0, 0, 0};
+    if (c->peer) {
+        const int r = hpm_profile_read(c->peer, peer_ms, peer_cnt);
+        if (r) return fail(c, r, "hpm_profile_read (second context): %s", hpm_last_error(c->peer));
+    }
     CK(cudaStreamSynchronize(c->stream), "hpm_profile_read");
     for (auto &p : c->prof_events) {
         float ms = 0;
@@ -612,8 +619,8 @@ int hpm_profile_read(hpm_ctx *c, float *ms4, int *counts4)
     }
     c->prof_events.clear();
     for (int i = 0; i < 4; ++i) {
-        if (ms4) ms4[i] = c->prof_ms[i];
-        if (counts4) counts4[i] = c->prof_cnt[i];
+        if (ms4) ms4[i] = c->prof_ms[i] + peer_ms[i];
+        if (counts4) counts4[i] = c->prof_cnt[i] + peer_cnt[i];
     }
     return HPM_OK;
 }
@@ -637,17 +644,26 @@ int hpm_count_enable(hpm_ctx *c, int enable)
         CK(cudaStreamSynchronize(c->stream), "hpm_count_enable");
     }
     c->counting = enable != 0;
+    if (c->peer) {
+        const int r = hpm_count_enable(c->peer, enable);
+        if (r) return fail(c, r, "hpm_count_enable (second context): %s", hpm_last_error(c->peer));
+    }
     return HPM_OK;
 }
 
 int hpm_count_read(hpm_ctx *c, uint64_t *cv, uint64_t *geom)
 {
     if (!c) return HPM_ERR_ARG;
+    uint64_t peer_cv = 0, peer_geom = 0;
+    if (c->peer) {
+        const int r = hpm_count_read(c->peer, &peer_cv, &peer_geom);
+        if (r) return fail(c, r, "hpm_count_read (second context): %s", hpm_last_error(c->peer));
+    }
     unsigned long long h[2] = {0, 0};
     CK(cudaMemcpyAsync(h, c->d_counters, sizeof(h), cudaMemcpyDeviceToHost, c->stream), "counters");
     CK(cudaStreamSynchronize(c->stream), "hpm_count_read");
-    if (cv) *cv = h[0];
-    if (geom) *geom = h[1];
+    if (cv) *cv = h[0] + peer_cv;
+    if (geom) *geom = h[1] + peer_geom;
     return HPM_OK;
 }
 

@@ -351,6 +351,12 @@ extern "C" int hpm_run_scene(hpm_ctx *c, int n_views, const float *const *images
         if (workers == 2 && !c->peer) {
             r = hpm_create(&c->peer, c->device);
             if (r) return ctx_fail(c, r, "hpm_run_scene: second context");
+            /* the peer's work is profiled and counted with this context's */
+            if (c->profiling) hpm_profile_enable(c->peer, 1);
+            if (c->counting) {
+                r = hpm_count_enable(c->peer, 1);
+                if (r) return ctx_fail(c, r, "hpm_run_scene: second context counters");
+            }
         }
         std::mutex token;
         hpm_ctx *ctxs[2] = {c, workers == 2 ? c->peer : nullptr};

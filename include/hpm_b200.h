@@ -178,7 +178,8 @@ int hpm_run_scene(hpm_ctx *ctx, int n_views, const float *const *images, const H
  * host, so the GPU does not wait for the Delaunay.  The maps do not depend on
  * the setting: each problem draws from its own seed.  The geometric
  * iterations always run on this context, problem after problem.  Counters
- * and CUDA-event profiles cover this context's work only. */
+ * and CUDA-event profiles (hpm_count_*, hpm_profile_*) cover the work of
+ * both contexts. */
 int hpm_set_scene_workers(hpm_ctx *ctx, int workers);
 
 /* Parity entry point: the prior of one pyramid level (0: 1/4 scale, 1: 1/2

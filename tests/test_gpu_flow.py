@@ -278,6 +278,31 @@ def test_scene_workers_give_the_same_maps():
                 np.testing.assert_array_equal(outs[0][k][v], o[k][v])
 
 
+def test_scene_counters_and_profiles_cover_both_workers():
+    """NCC-window counters and CUDA-event profiles of hpm_run_scene include
+    the second context's share of pass set A: the counts do not depend on
+    how the problems are split."""
+    nv = 4
+    sc = syn.make_scene(19, 128, 96, nv, n_planes=4, low_texture=0.3)
+    imgs = [sc.images[v].astype(np.float32) for v in range(nv)]
+    pairs = [(v, list(sc.pairs[v][1])) for v in range(nv)]
+    got = []
+    for workers in (1, 2):
+        with hb.Context() as ctx:
+            ctx.set_scene_workers(workers)
+            ctx.run_scene(imgs, sc.cams, pairs, seed=5, pyramid_levels=1, geom_iterations=2)  # creates the peer
+            ctx.count_enable(True)
+            ctx.profile_enable(True)
+            ctx.run_scene(imgs, sc.cams, pairs, seed=5, pyramid_levels=1, geom_iterations=2)
+            counts = ctx.count_read()
+            prof = ctx.profile_read()
+            ctx.count_enable(False)
+            ctx.profile_enable(False)
+            got.append((counts, {k: v[1] for k, v in prof.items()}))
+    assert got[0][0][0] > 0 and got[0][1]["propagate"] > 0
+    assert got[0] == got[1], got
+
+
 @pytest.mark.skipif(not orc.ref_available(), reason="reference shim oracle/_ref not built")
 def test_prior_flow_accuracy_matches_reference_kernels():
     """Pass set A (plain pass + planar prior on two pyramid levels) through
