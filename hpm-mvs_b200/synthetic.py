@@ -111,8 +111,14 @@ def _basis(n):
 def make_scene(seed: int, width: int, height: int, n_views: int, *, n_planes: int = 6, n_spheres: int = 0,
                low_texture: float = 0.25, depth_range=(2.0, 8.0), fx: float | None = None,
                arc_radius: float = 5.0, arc_step_deg: float = 8.0, noise_sigma: float = 2.0,
-               n_sources: int | None = None, texel_m: float | None = None, tex_size: int = 1024) -> Scene:
+               n_sources: int | None = None, texel_m: float | None = None, tex_size: int = 1024,
+               sizes=None) -> Scene:
+    """sizes: per-view (width, height) for scenes of uneven resolution; each
+    view's focal length scales with its width (fx given for `width`), so all
+    views see the same field of view."""
     rng = np.random.default_rng(seed)
+    sizes = [(width, height)] * n_views if sizes is None else [(int(w), int(h)) for w, h in sizes]
+    assert len(sizes) == n_views
     if fx is None:
         fx = 512.0 * width / 640.0
     dmin, dmax = depth_range
@@ -152,25 +158,25 @@ def make_scene(seed: int, width: int, height: int, n_views: int, *, n_planes: in
         o["tex"] += np.where(o["flat"], rng.normal(0, 2.0, o["tex"].shape), 0).astype(np.float32)
 
     # ---- cameras -------------------------------------------------------
-    K = np.array([[fx, 0, width / 2.0], [0, fx, height / 2.0], [0, 0, 1.0]])
+    Ks = [np.array([[fx * w / width, 0, w / 2.0], [0, fx * w / width, h / 2.0], [0, 0, 1.0]]) for w, h in sizes]
     cams = np.zeros(n_views, CAMERA_DTYPE)
     angles = [(i - (n_views - 1) / 2.0) * math.radians(arc_step_deg) for i in range(n_views)]
     for i, a in enumerate(angles):
         pos = center + arc_radius * np.array([math.sin(a), 0.0, -math.cos(a)])
         R, t = look_at(pos, center)
-        cams[i]["K"] = K.reshape(-1)
+        cams[i]["K"] = Ks[i].reshape(-1)
         cams[i]["R"] = R.reshape(-1)
         cams[i]["t"] = t
-        cams[i]["height"] = height
-        cams[i]["width"] = width
+        cams[i]["width"], cams[i]["height"] = sizes[i]
         cams[i]["depth_min"] = dmin
         cams[i]["depth_max"] = dmax
 
     # ---- render --------------------------------------------------------
-    ys, xs = np.mgrid[0:height, 0:width].astype(np.float64)
     images, gt_depth, gt_normal = [], [], []
-    Kinv = np.linalg.inv(K)
     for i in range(n_views):
+        width, height = sizes[i]
+        ys, xs = np.mgrid[0:height, 0:width].astype(np.float64)
+        Kinv = np.linalg.inv(Ks[i])
         R = cams[i]["R"].reshape(3, 3).astype(np.float64)
         t = cams[i]["t"].astype(np.float64)
         C = -R.T @ t

@@ -135,13 +135,19 @@ def test_geometric_pass_through_the_flow():
     assert a_b >= a_a - 0.01, (a_a, a_b)
 
 
-def test_scene_driver_matches_per_view_loop():
+UNEVEN = [(160, 120), (192, 144), (128, 96), (176, 132), (144, 108)]
+
+
+@pytest.mark.parametrize("sizes", [None, UNEVEN], ids=["even", "uneven"])
+def test_scene_driver_matches_per_view_loop(sizes):
     """hpm_run_scene (main.cpp:636-677 in one call, maps resident on the
     device) produces exactly what the per-view loop over hpm_process_problem
     produces with the same seeds: pass set A for every view, then two
-    geometric iterations, the second reading the geometric maps in place."""
+    geometric iterations, the second reading the geometric maps in place.
+    Also for a scene whose views have five different resolutions (each
+    view's maps at its own size, sources sampled at theirs)."""
     nv, seed = 5, 5
-    sc = syn.make_scene(15, 160, 120, nv, n_planes=6, low_texture=0.3)
+    sc = syn.make_scene(15, 160, 120, nv, n_planes=6, low_texture=0.3, sizes=sizes)
     imgs_all = [sc.images[v].astype(np.float32) for v in range(nv)]
     cams_all = sc.cams
     pairs = [(v, list(sc.pairs[v][1])) for v in range(nv)]
@@ -167,6 +173,7 @@ def test_scene_driver_matches_per_view_loop():
                                                  multi_geometry=gi >= 1)
                 depth_g[ref], normal[ref], cost[ref] = d, n, c
     for v in range(nv):
+        assert sd[v].shape == sc.gt_depth[v].shape
         np.testing.assert_array_equal(sd[v], depth_g[v])
         np.testing.assert_array_equal(sn[v], normal[v])
         np.testing.assert_array_equal(scost[v], cost[v])

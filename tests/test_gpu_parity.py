@@ -96,9 +96,11 @@ def _scene(seed, w, h, nv, **kw):
     return sc, imgs, cams, sc.depth_min * 0.6, sc.depth_max * 1.2
 
 
-@pytest.mark.parametrize("half_steps", [0, 1, 2])
-def test_half_steps_agree_with_oracle(half_steps):
-    sc, imgs, cams, dmin, dmax = _scene(3, 128, 96, 5)
+@pytest.mark.parametrize("half_steps,sizes", [(0, None), (1, None), (2, None),
+                                              (2, [(128, 96), (160, 120), (96, 72), (144, 108), (112, 84)])])
+def test_half_steps_agree_with_oracle(half_steps, sizes):
+    """Also with sources of other resolutions than the reference view."""
+    sc, imgs, cams, dmin, dmax = _scene(3, 128, 96, 5, sizes=sizes)
     op, oc, ov = orc.run_patchmatch(imgs, cams, depth_min=dmin, depth_max=dmax, seed=7, salt=0,
                                     half_steps=half_steps, finalize=False)
     with hb.Context() as ctx:

@@ -206,3 +206,26 @@ def test_rounding_switch(mode):
         assert orc.lib().or_get_tex_rounding() == mode
     finally:
         orc.set_tex_rounding(1)
+
+
+def test_uneven_view_sizes_are_consistent():
+    """Scenes whose views have different resolutions (synthetic sizes=):
+    each view renders at its own size with its own intrinsics, and the
+    oracle, sampling each source at its own size, scores the reference
+    view's ground-truth planes as well as in the same scene at one size,
+    and much better than perturbed planes."""
+    sizes = [(96, 72), (128, 96), (64, 48), (112, 84)]
+    med = {}
+    for tag, sz in (("even", None), ("uneven", sizes)):
+        sc = syn.make_scene(4, 96, 72, 4, n_planes=3, sizes=sz)
+        if sz is not None:
+            assert [i.shape for i in sc.images] == [(h, w) for w, h in sizes]
+            assert [(int(c["width"]), int(c["height"])) for c in sc.cams] == sizes
+        imgs, cams = syn.view_set(sc, 0)
+        gt = syn.gt_planes_ref_frame(sc, 0)
+        rand = gt.copy()
+        rand[..., 3] *= np.random.default_rng(0).uniform(0.7, 1.3, rand.shape[:2]).astype(np.float32)
+        med[tag] = (np.median(orc.cost_vectors(imgs, cams, gt).min(-1)),
+                    np.median(orc.cost_vectors(imgs, cams, rand).min(-1)))
+    good, bad = med["uneven"]
+    assert good <= med["even"][0] + 0.05 and good < 0.7 * bad, med
