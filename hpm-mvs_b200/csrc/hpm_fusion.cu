@@ -26,8 +26,11 @@
 #include <cfloat>
 #include <climits>
 #include <cmath>
+#include <condition_variable>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
+#include <thread>
 #include <vector>
 
 #include "hpm_internal.h"
@@ -208,15 +211,25 @@ extern "C" int hpm_fuse(int device, int n_views, const HpmCamera *cams, const fl
     }
     int max_ns = 1;
     for (int p = 0; p < n_problems; ++p) max_ns = src_counts[p] > max_ns ? src_counts[p] : max_ns;
-    DevBuf<int> d_src;
-    DevBuf<float> d_w, d_pt;
-    FCK(d_src.alloc(max_px * max_ns));
-    FCK(d_w.alloc(max_px * max_ns));
-    FCK(d_pt.alloc(3 * max_px));
-    std::vector<int> h_src(max_px * max_ns);
-    std::vector<float> h_w(max_px * max_ns), h_pt(3 * max_px);
-    long long n_out = 0;
-    for (int pi = 0; pi < n_problems; ++pi) {
+    /* Two slots of pair data.  A producer thread runs the kernel of problem
+     * p + 1 and copies its pairs to the host (pageable memory, so each copy
+     * holds its thread until done) while this thread runs problem p's
+     * ordered pass. */
+    struct Slot {
+        DevBuf<int> d_src;
+        DevBuf<float> d_w, d_pt;
+        std::vector<int> h_src;
+        std::vector<float> h_w, h_pt;
+    } slots[2];
+    for (Slot &sl : slots) {
+        FCK(sl.d_src.alloc(max_px * max_ns));
+        FCK(sl.d_w.alloc(max_px * max_ns));
+        FCK(sl.d_pt.alloc(3 * max_px));
+        sl.h_src.resize(max_px * max_ns);
+        sl.h_w.resize(max_px * max_ns);
+        sl.h_pt.resize(3 * max_px);
+    }
+    auto produce = [&](int pi, Slot &sl) -> int {
         const int i = ref_ids[pi], ns = src_counts[pi];
         const size_t npx = (size_t)cams[i].width * cams[i].height;
         FuseArgs a;
@@ -231,22 +244,92 @@ extern "C" int hpm_fuse(int device, int n_views, const HpmCamera *cams, const fl
             a.src_depth[j] = d_depth[s].p;
             a.src_normal[j] = d_normal[s].p;
         }
-        a.pair_src = d_src.p;
-        a.pair_w = d_w.p;
-        a.point = d_pt.p;
+        a.pair_src = sl.d_src.p;
+        a.pair_w = sl.d_w.p;
+        a.point = sl.d_pt.p;
         if (ns > 0) {
             const long long total = (long long)npx * ns;
             k_fuse_pairs<<<(unsigned)((total + 255) / 256), 256, 0, st>>>(a, (int)npx);
             FCK(cudaGetLastError());
-            FCK(cudaMemcpyAsync(h_src.data(), d_src.p, sizeof(int) * total, cudaMemcpyDeviceToHost, st));
-            FCK(cudaMemcpyAsync(h_w.data(), d_w.p, sizeof(float) * total, cudaMemcpyDeviceToHost, st));
-            FCK(cudaMemcpyAsync(h_pt.data(), d_pt.p, sizeof(float) * 3 * npx, cudaMemcpyDeviceToHost, st));
+            FCK(cudaMemcpyAsync(sl.h_src.data(), sl.d_src.p, sizeof(int) * total, cudaMemcpyDeviceToHost, st));
+            FCK(cudaMemcpyAsync(sl.h_w.data(), sl.d_w.p, sizeof(float) * total, cudaMemcpyDeviceToHost, st));
+            FCK(cudaMemcpyAsync(sl.h_pt.data(), sl.d_pt.p, sizeof(float) * 3 * npx, cudaMemcpyDeviceToHost, st));
         }
         FCK(cudaStreamSynchronize(st));
+        return HPM_OK;
+    };
+    std::mutex mu;
+    std::condition_variable cv;
+    int ready[2] = {-1, -1}; /* problem whose pairs a slot holds, -1 while free */
+    bool stop = false;
+    int produce_rc = HPM_OK;
+    std::thread producer([&] {
+        const int rc0 = cudaSetDevice(device) == cudaSuccess ? HPM_OK : HPM_ERR_CUDA;
+        for (int pi = 0; pi < n_problems; ++pi) {
+            const int k = pi & 1;
+            {
+                std::unique_lock<std::mutex> l(mu);
+                cv.wait(l, [&] { return ready[k] == -1 || stop; });
+                if (stop) return;
+            }
+            const int rc = rc0 ? rc0 : produce(pi, slots[k]);
+            {
+                std::lock_guard<std::mutex> l(mu);
+                if (rc) produce_rc = rc;
+                else ready[k] = pi;
+            }
+            cv.notify_all();
+            if (rc) return;
+        }
+    });
+    struct Joiner {
+        std::thread &t;
+        std::mutex &mu;
+        std::condition_variable &cv;
+        bool &stop;
+        ~Joiner()
+        {
+            {
+                std::lock_guard<std::mutex> l(mu);
+                stop = true;
+            }
+            cv.notify_all();
+            t.join();
+        }
+    } joiner{producer, mu, cv, stop};
+    long long n_out = 0;
+    for (int pi = 0; pi < n_problems; ++pi) {
+        const int i = ref_ids[pi], ns = src_counts[pi];
+        const size_t npx = (size_t)cams[i].width * cams[i].height;
+        const int k = pi & 1;
+        {
+            std::unique_lock<std::mutex> l(mu);
+            cv.wait(l, [&] { return ready[k] == pi || produce_rc != HPM_OK; });
+            if (ready[k] != pi) return produce_rc;
+        }
+        struct Release {
+            int &slot;
+            std::mutex &mu;
+            std::condition_variable &cv;
+            ~Release()
+            {
+                {
+                    std::lock_guard<std::mutex> l(mu);
+                    slot = -1;
+                }
+                cv.notify_all();
+            }
+        } release{ready[k], mu, cv};
+        const std::vector<int> &h_src = slots[k].h_src;
+        const std::vector<float> &h_w = slots[k].h_w, &h_pt = slots[k].h_pt;
         if (ns == 0) continue; /* no source: no pixel can be consistent */
         /* main.cpp:553-620 in order: masks and the per-view used_list */
         int used[kMaxSrc];
-        for (int j = 0; j < ns; ++j) used[j] = -1;
+        uint8_t *msrc[kMaxSrc];
+        for (int j = 0; j < ns; ++j) {
+            used[j] = -1;
+            msrc[j] = masks[src_ids[pi * kMaxSrc + j]].data();
+        }
         std::vector<uint8_t> &mi = masks[i];
         for (size_t p = 0; p < npx; ++p) {
             if (mi[p] == 1) continue;
@@ -256,7 +339,7 @@ extern "C" int hpm_fuse(int device, int n_views, const HpmCamera *cams, const fl
             float dyn = 0.0f;
             for (int j = 0; j < ns; ++j) {
                 if (ps[j] < 0) continue;
-                if (masks[src_ids[pi * kMaxSrc + j]][ps[j]] == 1) continue;
+                if (msrc[j][ps[j]] == 1) continue;
                 used[j] = ps[j];
                 dyn += pw[j];
                 num++;
@@ -269,7 +352,7 @@ extern "C" int hpm_fuse(int device, int n_views, const HpmCamera *cams, const fl
                 }
                 n_out++;
                 for (int j = 0; j < ns; ++j)
-                    if (used[j] != -1) masks[src_ids[pi * kMaxSrc + j]][used[j]] = 1;
+                    if (used[j] != -1) msrc[j][used[j]] = 1;
             }
         }
     }
