@@ -312,3 +312,37 @@ def normal_error_deg(normal: np.ndarray, gt: np.ndarray, gt_depth: np.ndarray) -
     ok = na > 0
     cos = (a[ok] * b[ok]).sum(-1) / na[ok]
     return float(np.degrees(np.median(np.arccos(np.clip(cos, -1, 1))))) if ok.any() else 180.0
+
+
+def main(argv=None) -> None:
+    """Write a seeded scene as a dense folder (images/, cams/, pair.txt) for
+    hpm_mvs or the reference's executable, with the ground-truth depth maps
+    as gt/%08d.dmb."""
+    import argparse
+    import os
+
+    ap = argparse.ArgumentParser(description="seeded synthetic scene as an HPM-MVS dense folder")
+    ap.add_argument("folder")
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--views", type=int, default=11)
+    ap.add_argument("--size", default="1600x1200", help="WxH")
+    ap.add_argument("--sources", type=int, default=10)
+    ap.add_argument("--planes", type=int, default=20)
+    ap.add_argument("--spheres", type=int, default=5)
+    ap.add_argument("--low-texture", type=float, default=0.4)
+    ap.add_argument("--ext", default=".jpg", choices=[".jpg", ".png", ".pgm"])
+    a = ap.parse_args(argv)
+    w, h = (int(x) for x in a.size.lower().split("x"))
+    sc = make_scene(a.seed, w, h, a.views, n_planes=a.planes, n_spheres=a.spheres, low_texture=a.low_texture,
+                    n_sources=a.sources)
+    write_dense_folder(sc, a.folder, a.ext)
+    os.makedirs(os.path.join(a.folder, "gt"), exist_ok=True)
+    for i, d in enumerate(sc.gt_depth):
+        with open(os.path.join(a.folder, "gt", f"{i:08d}.dmb"), "wb") as f:  # .dmb: type 1, h, w, 1 channel
+            f.write(np.array([1, d.shape[0], d.shape[1], 1], np.int32).tobytes())
+            f.write(np.ascontiguousarray(d, np.float32).tobytes())
+    print(f"wrote {a.views} views of {w}x{h} to {a.folder}")
+
+
+if __name__ == "__main__":
+    main()

@@ -41,3 +41,19 @@ def test_resize_linear_matches_cv2(src, dst, ch):
     shape = (src[1], src[0]) if ch == 1 else (src[1], src[0], ch)
     a = rng.uniform(-300, 300, shape).astype(np.float32)
     np.testing.assert_array_equal(hb.resize_linear(a, *dst), cv2.resize(a, dst, interpolation=cv2.INTER_LINEAR))
+
+
+def test_synthetic_scene_command_writes_a_dense_folder(tmp_path):
+    """python hpm-mvs_b200/synthetic.py FOLDER writes images/%08d.jpg,
+    cams/%08d_cam.txt and pair.txt in the reference's layout, plus the
+    ground-truth depth maps as gt/%08d.dmb, all readable through the C ABI."""
+    import synthetic as syn
+
+    folder = str(tmp_path / "scene")
+    syn.main([folder, "--views", "3", "--size", "64x48", "--sources", "2", "--planes", "2", "--spheres", "0"])
+    assert hb.read_pair(os.path.join(folder, "pair.txt")) == [(0, [1, 2]), (1, [0, 2]), (2, [1, 0])]
+    for v in range(3):
+        assert hb.read_gray8(os.path.join(folder, "images", f"{v:08d}.jpg")).shape == (48, 64)
+        assert hb.read_camera(os.path.join(folder, "cams", f"{v:08d}_cam.txt"))["depth_max"] > 0
+        gt = hb.read_dmb(os.path.join(folder, "gt", f"{v:08d}.dmb"))
+        assert gt.shape == (48, 64) and (gt > 0).mean() > 0.9
