@@ -298,6 +298,16 @@ extern "C" int hpm_run_scene(hpm_ctx *c, int n_views, const float *const *images
                              const HpmSceneOpts *o, float *const *out_depths, float *const *out_normals,
                              float *const *out_costs)
 {
+    return hpm_run_scene_ex(c, n_views, images, cams, n_problems, ref_ids, src_counts, src_ids, o, out_depths,
+                            out_normals, out_costs, nullptr, nullptr);
+}
+
+extern "C" int hpm_run_scene_ex(hpm_ctx *c, int n_views, const float *const *images, const HpmCamera *cams,
+                                int n_problems, const int *ref_ids, const int *src_counts, const int *src_ids,
+                                const HpmSceneOpts *o, float *const *out_depths, float *const *out_normals,
+                                float *const *out_costs, float *const *out_pass_depths,
+                                float *const *out_prior_depths)
+{
     if (!c || !images || !cams || !ref_ids || !src_counts || !src_ids || !o) return HPM_ERR_ARG;
     if (n_views < 2 || n_problems < 1) return ctx_fail(c, HPM_ERR_ARG, "hpm_run_scene: %d views, %d problems", n_views,
                                                        n_problems);
@@ -373,7 +383,8 @@ extern "C" int hpm_run_scene(hpm_ctx *c, int n_views, const float *const *images
                 if (!rr) {
                     HpmProblemOpts po = {o->planar_prior, 0, 0, o->seed + (uint64_t)p, o->pyramid_levels};
                     const int ref = ref_ids[p];
-                    rr = hpm_process_problem(cc, &po, m.depth_a[ref], m.normal[ref], m.cost[ref], nullptr);
+                    float *prior_out = out_prior_depths ? out_prior_depths[ref] : nullptr;
+                    rr = hpm_process_problem(cc, &po, m.depth_a[ref], m.normal[ref], m.cost[ref], prior_out);
                 }
                 if (rr) {
                     rcs[wi] = rr;
@@ -429,6 +440,8 @@ extern "C" int hpm_run_scene(hpm_ctx *c, int n_views, const float *const *images
             CK(cudaMemcpyAsync(out_normals[v], m.normal[v], sizeof(float) * 3 * np, cudaMemcpyDefault, s), "out");
         if (out_costs && out_costs[v])
             CK(cudaMemcpyAsync(out_costs[v], m.cost[v], sizeof(float) * np, cudaMemcpyDefault, s), "out");
+        if (out_pass_depths && out_pass_depths[v])
+            CK(cudaMemcpyAsync(out_pass_depths[v], m.depth_a[v], sizeof(float) * np, cudaMemcpyDefault, s), "out");
     }
     CK(cudaStreamSynchronize(s), "hpm_run_scene");
     return HPM_OK;

@@ -7,6 +7,7 @@
 #include <sys/stat.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -154,6 +155,60 @@ std::vector<float> read_image(const std::string &dense_folder, int id, int *w, i
     return std::vector<float>(px->begin(), px->end()); /* convertTo(CV_32FC1), HPM.cpp:494 */
 }
 
+/* One view as InuputInitialization reads it (HPM.cpp:482-551): the gray
+ * image as floats, its camera, both scaled down to the 3200-pixel cap. */
+void load_view(const std::string &dense_folder, int id, std::vector<float> &img, HpmCamera &cam)
+{
+    int w = 0, h = 0;
+    img = read_image(dense_folder, id, &w, &h);
+    cam = HpmCamera{};
+    const std::string cp = id_path(dense_folder + "/cams", id, "_cam.txt");
+    int rc = hpm_read_camera(cp.c_str(), &cam);
+    if (rc != HPM_OK) throw Error(rc, "cannot read " + cp);
+    const int cap = 3200; /* HPM.cpp:525-551 */
+    if (w > cap || h > cap) {
+        const float factor = std::min((float)cap / w, (float)cap / h);
+        const int nw = (int)std::round(w * factor), nh = (int)std::round(h * factor);
+        const float sx = nw / (float)w, sy = nh / (float)h;
+        std::vector<float> scaled((size_t)nw * nh);
+        rc = hpm_resize_linear(img.data(), w, h, 1, scaled.data(), nw, nh);
+        if (rc != HPM_OK) throw Error(rc, "image cap");
+        img.swap(scaled);
+        cam.K[0] *= sx;
+        cam.K[2] *= sx;
+        cam.K[4] *= sy;
+        cam.K[5] *= sy;
+        w = nw;
+        h = nh;
+    }
+    cam.width = w;
+    cam.height = h;
+}
+
+/* f(i) for i in [0, n) on up to `threads` host threads; the first exception
+ * is rethrown */
+template <typename F>
+void parallel_for(size_t n, unsigned threads, F f)
+{
+    std::atomic<size_t> next{0};
+    std::vector<std::exception_ptr> errors(n);
+    auto run = [&] {
+        for (size_t i; (i = next.fetch_add(1)) < n;) {
+            try {
+                f(i);
+            } catch (...) {
+                errors[i] = std::current_exception();
+            }
+        }
+    };
+    std::vector<std::thread> pool;
+    for (unsigned t = 1; t < std::min<size_t>(threads, n); ++t) pool.emplace_back(run);
+    run();
+    for (auto &t : pool) t.join();
+    for (auto &e : errors)
+        if (e) std::rethrow_exception(e);
+}
+
 std::vector<float> read_dmb(const std::string &path, int *w, int *h, int want_nb)
 {
     int nb = 0;
@@ -222,47 +277,7 @@ void HPM::InuputInitialization(const std::string &dense_folder, const Problem &p
     images_.resize(n);
     cameras_.resize(n);
     /* the views of a problem are read and decoded on threads of their own */
-    std::vector<std::exception_ptr> errors(n);
-    auto load = [&](size_t i) {
-        try {
-            const int id = ids[i];
-            int w = 0, h = 0;
-            std::vector<float> img = read_image(dense_folder, id, &w, &h);
-            HpmCamera cam{};
-            const std::string cp = id_path(dense_folder + "/cams", id, "_cam.txt");
-            int rc = hpm_read_camera(cp.c_str(), &cam);
-            if (rc != HPM_OK) throw Error(rc, "cannot read " + cp);
-            /* the image cap of HPM.cpp:525-551 */
-            const int cap = 3200;
-            if (w > cap || h > cap) {
-                const float factor = std::min((float)cap / w, (float)cap / h);
-                const int nw = (int)std::round(w * factor), nh = (int)std::round(h * factor);
-                const float sx = nw / (float)w, sy = nh / (float)h;
-                std::vector<float> scaled((size_t)nw * nh);
-                rc = hpm_resize_linear(img.data(), w, h, 1, scaled.data(), nw, nh);
-                if (rc != HPM_OK) throw Error(rc, "image cap");
-                img.swap(scaled);
-                cam.K[0] *= sx;
-                cam.K[2] *= sx;
-                cam.K[4] *= sy;
-                cam.K[5] *= sy;
-                w = nw;
-                h = nh;
-            }
-            cam.width = w;
-            cam.height = h;
-            images_[i] = std::move(img);
-            cameras_[i] = cam;
-        } catch (...) {
-            errors[i] = std::current_exception();
-        }
-    };
-    std::vector<std::thread> workers;
-    for (size_t i = 1; i < n; ++i) workers.emplace_back(load, i);
-    load(0);
-    for (auto &t : workers) t.join();
-    for (auto &e : errors)
-        if (e) std::rethrow_exception(e);
+    parallel_for(n, (unsigned)n, [&](size_t i) { load_view(dense_folder, ids[i], images_[i], cameras_[i]); });
     params_.depth_min = cameras_[0].depth_min * 0.6f;
     params_.depth_max = cameras_[0].depth_max * 1.2f;
     depths_.clear();
@@ -556,6 +571,79 @@ void ProcessProblem(const std::string &dense_folder, const Problem &problem, boo
     write_dmb(folder + "/costs.dmb", costs, w, h, 1);
     std::cout << "Processing image " << std::setw(8) << std::setfill('0') << problem.ref_image_id << " done!"
               << std::endl;
+}
+
+void RunScene(const std::string &dense_folder, const std::vector<Problem> &problems, bool planar_prior,
+              int geom_iterations, uint64_t seed, int pyramid_levels, int device)
+{
+    /* every view a problem names, numbered in order of appearance */
+    std::map<int, int> index;
+    std::vector<int> ids;
+    auto add = [&](int id) {
+        if (index.emplace(id, (int)ids.size()).second) ids.push_back(id);
+    };
+    for (const Problem &p : problems) {
+        if ((int)p.src_image_ids.size() + 1 > HPM_MAX_IMAGES) throw Error(HPM_ERR_ARG, "more than 32 source images");
+        add(p.ref_image_id);
+        for (int sid : p.src_image_ids) add(sid);
+    }
+    const size_t n = ids.size(), np = problems.size();
+    const unsigned threads = std::max(1u, std::thread::hardware_concurrency());
+    std::vector<std::vector<float>> images(n);
+    std::vector<HpmCamera> cams(n);
+    parallel_for(n, threads, [&](size_t i) { load_view(dense_folder, ids[i], images[i], cams[i]); });
+    std::vector<int> refs(np), counts(np), srcs(np * (HPM_MAX_IMAGES - 1), 0);
+    for (size_t p = 0; p < np; ++p) {
+        refs[p] = index[problems[p].ref_image_id];
+        counts[p] = (int)problems[p].src_image_ids.size();
+        for (int j = 0; j < counts[p]; ++j) srcs[p * (HPM_MAX_IMAGES - 1) + j] = index[problems[p].src_image_ids[j]];
+    }
+    /* outputs for the views that are references: final depth, normal and
+     * cost, pass set A's depth and the prior depth */
+    std::vector<std::vector<float>> depth(n), normal(n), cost(n), pass(n), prior(n);
+    std::vector<const float *> img_ptr(n);
+    std::vector<float *> pd(n, nullptr), pn(n, nullptr), pc(n, nullptr), pp(n, nullptr), pr(n, nullptr);
+    for (size_t i = 0; i < n; ++i) img_ptr[i] = images[i].data();
+    for (size_t p = 0; p < np; ++p) {
+        const int v = refs[p];
+        const size_t npx = (size_t)cams[v].width * cams[v].height;
+        depth[v].resize(npx);
+        normal[v].resize(3 * npx);
+        cost[v].resize(npx);
+        pass[v].resize(npx);
+        if (planar_prior) prior[v].resize(npx);
+        pd[v] = depth[v].data();
+        pn[v] = normal[v].data();
+        pc[v] = cost[v].data();
+        pp[v] = pass[v].data();
+        if (planar_prior) pr[v] = prior[v].data();
+    }
+    hpm_ctx *ctx = nullptr;
+    int rc = hpm_create(&ctx, device);
+    if (rc != HPM_OK) throw Error(rc, "hpm_create");
+    struct Destroy {
+        hpm_ctx *c;
+        ~Destroy() { hpm_destroy(c); }
+    } destroy{ctx};
+    const HpmSceneOpts o = {planar_prior ? 1 : 0, geom_iterations, seed, pyramid_levels};
+    rc = hpm_run_scene_ex(ctx, (int)n, img_ptr.data(), cams.data(), (int)np, refs.data(), counts.data(), srcs.data(),
+                          &o, pd.data(), pn.data(), pc.data(), pp.data(), pr.data());
+    if (rc != HPM_OK) throw Error(rc, std::string("hpm_run_scene_ex: ") + hpm_last_error(ctx));
+    /* the files ProcessProblem leaves behind for each reference view:
+     * pass set A's depth, prior depth, normal and cost, then the geometric
+     * passes' depth, normal and cost over them (main.cpp:481-497) */
+    make_dir(dense_folder + "/HPM");
+    parallel_for(np, threads, [&](size_t p) {
+        const int v = refs[p], w = cams[v].width, h = cams[v].height;
+        const std::string folder = result_folder(dense_folder, problems[p].ref_image_id);
+        make_dir(folder);
+        if (planar_prior) write_dmb(folder + "/depths_prior.dmb", prior[v], w, h, 1);
+        write_dmb(folder + "/depths.dmb", pass[v], w, h, 1);
+        if (geom_iterations > 0) write_dmb(folder + "/depths_geom.dmb", depth[v], w, h, 1);
+        write_dmb(folder + "/normals.dmb", normal[v], w, h, 3);
+        write_dmb(folder + "/costs.dmb", cost[v], w, h, 1);
+    });
+    std::cout << "Processed " << np << " problems (" << n << " views) in one scene run" << std::endl;
 }
 
 }  // namespace hpm_host

@@ -118,8 +118,8 @@ private:
 /* RunFusion (main.cpp:502-633): fuses the depth maps of every problem
  * (depths_geom.dmb with geom_consistency, else depths.dmb) and normals.dmb
  * into dense_folder/HPM/HPM_model.ply; returns the number of points.
- * Colours come from images/ (PNG or PGM); an image whose size differs from
- * its depth map is resized bilinearly (RescaleImageAndCamera,
+ * Colours come from images/ (JPEG, PNG or PGM); an image whose size differs
+ * from its depth map is resized bilinearly (RescaleImageAndCamera,
  * HPM.cpp:187-208), not bit-exactly as OpenCV's 8-bit path. */
 long long RunFusion(const std::string &dense_folder, const std::vector<Problem> &problems, bool geom_consistency,
                     int device = 0);
@@ -129,5 +129,15 @@ long long RunFusion(const std::string &dense_folder, const std::vector<Problem> 
 void ProcessProblem(const std::string &dense_folder, const Problem &problem, bool geom_consistency,
                     bool planar_prior, bool multi_geometry = false, uint64_t seed = 0, int pyramid_levels = -1,
                     int device = 0);
+
+/* main()'s depth estimation (main.cpp:646-674) in one hpm_run_scene_ex
+ * call: pass set A, then geom_iterations geometric iterations, over every
+ * problem, with the maps kept in device memory between passes; then, for
+ * every problem, the files the per-problem loop leaves (depths.dmb,
+ * depths_prior.dmb, depths_geom.dmb, normals.dmb, costs.dmb).  Seeds as in
+ * that loop (S + p, S + 1000003 (g + 1) + p), hence the same files.  Host
+ * memory: about 20 bytes per pixel of each reference view, plus the images. */
+void RunScene(const std::string &dense_folder, const std::vector<Problem> &problems, bool planar_prior,
+              int geom_iterations, uint64_t seed, int pyramid_levels, int device);
 
 }  // namespace hpm_host

@@ -37,7 +37,7 @@ EXPORTED = [
     "hpm_initial_costs", "hpm_geom_costs", "hpm_depth_normal_filter", "hpm_profile_enable", "hpm_profile_read",
     "hpm_count_enable", "hpm_count_read", "hpm_write_dmb", "hpm_read_dmb", "hpm_read_camera", "hpm_read_pair",
     "hpm_fp32_peak", "hpm_jbu_noalloc", "hpm_process_problem", "hpm_last_prior_stats", "hpm_delaunay",
-    "hpm_prior_level", "hpm_run_scene", "hpm_read_gray8", "hpm_resize_linear",
+    "hpm_prior_level", "hpm_run_scene", "hpm_run_scene_ex", "hpm_read_gray8", "hpm_resize_linear",
     "hpm_fuse", "hpm_write_ply", "hpm_read_bgr8", "hpm_set_scene_workers",
 ]
 
@@ -209,12 +209,14 @@ class Context:
         return depth, normal, cost, prior
 
     def run_scene(self, images, cams, pairs, *, planar_prior=True, geom_iterations=2, seed=0, pyramid_levels=-1,
-                  images_are_device=False, outputs=True):
+                  images_are_device=False, outputs=True, extra_maps=False):
         """The reference's main() over a scene.  images: per-view float32 [H, W]
         arrays, or device pointers (ints) with images_are_device; pairs:
         [(ref, [sources])].  outputs: True to return new per-view (depth,
         normal, cost) lists, False for none (the maps stay on the device), or
-        a tuple of three caller-owned lists of float32 arrays to fill."""
+        a tuple of three caller-owned lists of float32 arrays to fill.
+        extra_maps (with outputs=True): also return each view's pass-set-A
+        depth and prior depth (hpm_run_scene_ex), five lists in all."""
         n = len(cams)
         cams = np.ascontiguousarray(cams, dtype=CAMERA_DTYPE)
         if images_are_device:
@@ -247,11 +249,21 @@ class Context:
             arrs = [(ctypes.c_void_p * n)(*[o_[k].ctypes.data for o_ in outs]) for k in range(3)]
         else:
             arrs = [None, None, None]
-        self._check(lib().hpm_run_scene(self._h, n, img_arr, _p(cams), len(pairs), _p(refs), _p(counts), _p(srcs),
-                                        ctypes.byref(o), arrs[0], arrs[1], arrs[2]), "hpm_run_scene")
+        if extra_maps:
+            if outputs is not True:
+                raise ValueError("run_scene: extra_maps needs outputs=True")
+            extra = [[np.empty((int(c["height"]), int(c["width"])), np.float32) for c in cams] for _ in range(2)]
+            ex = [(ctypes.c_void_p * n)(*[a.ctypes.data for a in e]) for e in extra]
+            self._check(lib().hpm_run_scene_ex(self._h, n, img_arr, _p(cams), len(pairs), _p(refs), _p(counts),
+                                               _p(srcs), ctypes.byref(o), arrs[0], arrs[1], arrs[2], ex[0], ex[1]),
+                        "hpm_run_scene_ex")
+        else:
+            self._check(lib().hpm_run_scene(self._h, n, img_arr, _p(cams), len(pairs), _p(refs), _p(counts),
+                                            _p(srcs), ctypes.byref(o), arrs[0], arrs[1], arrs[2]), "hpm_run_scene")
         del keep
         if outputs:
-            return [o_[0] for o_ in outs], [o_[1] for o_ in outs], [o_[2] for o_ in outs]
+            res = [o_[0] for o_ in outs], [o_[1] for o_ in outs], [o_[2] for o_ in outs]
+            return res + tuple(extra) if extra_maps else res
         return None
 
     def prior_level(self, level, depth, normal, cost):

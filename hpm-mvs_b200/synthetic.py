@@ -314,6 +314,14 @@ def normal_error_deg(normal: np.ndarray, gt: np.ndarray, gt_depth: np.ndarray) -
     return float(np.degrees(np.median(np.arccos(np.clip(cos, -1, 1))))) if ok.any() else 180.0
 
 
+def _read_dmb(path):
+    """A .dmb map (int32 type, h, w, channels; then float32) as [h, w] or [h, w, c]."""
+    raw = np.fromfile(path, np.uint8)
+    _, h, w, nb = np.frombuffer(raw[:16].tobytes(), np.int32)
+    a = np.frombuffer(raw[16:].tobytes(), np.float32).reshape(h, w, nb)
+    return a[..., 0] if nb == 1 else a
+
+
 def main(argv=None) -> None:
     """Write a seeded scene as a dense folder (images/, cams/, pair.txt) for
     hpm_mvs or the reference's executable, with the ground-truth depth maps
@@ -331,7 +339,18 @@ def main(argv=None) -> None:
     ap.add_argument("--spheres", type=int, default=5)
     ap.add_argument("--low-texture", type=float, default=0.4)
     ap.add_argument("--ext", default=".jpg", choices=[".jpg", ".png", ".pgm"])
+    ap.add_argument("--score", action="store_true",
+                    help="instead of writing, score FOLDER/HPM/2333_%%08d/depths_geom.dmb against FOLDER/gt")
     a = ap.parse_args(argv)
+    if a.score:
+        accs = []
+        for name in sorted(os.listdir(os.path.join(a.folder, "gt"))):
+            v = int(name.split(".")[0])
+            res = os.path.join(a.folder, "HPM", f"2333_{v:08d}", "depths_geom.dmb")
+            if os.path.exists(res):
+                accs.append(depth_accuracy(_read_dmb(res), _read_dmb(os.path.join(a.folder, "gt", name))))
+        print(f"views {len(accs)} px_relerr_lt_1pct {np.mean(accs) if accs else float('nan'):.4f}")
+        return
     w, h = (int(x) for x in a.size.lower().split("x"))
     sc = make_scene(a.seed, w, h, a.views, n_planes=a.planes, n_spheres=a.spheres, low_texture=a.low_texture,
                     n_sources=a.sources)

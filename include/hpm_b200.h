@@ -169,6 +169,15 @@ typedef struct {
 int hpm_run_scene(hpm_ctx *ctx, int n_views, const float *const *images, const HpmCamera *cams, int n_problems,
                   const int *ref_ids, const int *src_counts, const int *src_ids, const HpmSceneOpts *opts,
                   float *const *depths, float *const *normals, float *const *costs);
+/* hpm_run_scene plus the two other maps the reference's ProcessProblem
+ * writes per view in pass set A (main.cpp:481-497): pass_depths[v], the
+ * depth map after pass set A (depths.dmb), and prior_depths[v], the
+ * full-scale planar-prior depth (depths_prior.dmb; zeros without a prior).
+ * Either array, and any entry, may be NULL. */
+int hpm_run_scene_ex(hpm_ctx *ctx, int n_views, const float *const *images, const HpmCamera *cams,
+                     int n_problems, const int *ref_ids, const int *src_counts, const int *src_ids,
+                     const HpmSceneOpts *opts, float *const *depths, float *const *normals, float *const *costs,
+                     float *const *pass_depths, float *const *prior_depths);
 /* Host threads of hpm_run_scene's pass set A (1 or 2, default 2; no
  * counterpart in the reference).  With 2, pass set A's problems go to this
  * context and a second one on the same device (created on first use, freed

@@ -184,10 +184,11 @@ def test_scene_driver_matches_per_view_loop(sizes):
 @pytest.mark.parametrize("ext", [".jpg", ".png"])
 def test_host_main_writes_the_scene_driver_maps(tmp_path, ext):
     """The C++ host (hpm_mvs: HPM class, ProcessProblem, main() over the C
-    ABI, reading images/ + cams/ + pair.txt and writing .dmb files) and the
-    Python front end give exactly the maps of hpm_run_scene on the same
-    seeds and on the images as cv::imread decodes them (JPEG, the
-    reference's images/%08d.jpg, or PNG)."""
+    ABI, reading images/ + cams/ + pair.txt and writing .dmb files), in its
+    scene form and problem by problem, and the Python front end give
+    exactly the maps of hpm_run_scene_ex on the same seeds and on the images
+    as cv::imread decodes them (JPEG, the reference's images/%08d.jpg, or
+    PNG)."""
     import os
     import subprocess
     import sys
@@ -195,11 +196,12 @@ def test_host_main_writes_the_scene_driver_maps(tmp_path, ext):
     cv2 = pytest.importorskip("cv2")
     here = os.path.dirname(os.path.abspath(hb.__file__))
     sc = syn.make_scene(16, 160, 120, 4, n_planes=5, low_texture=0.3)
-    folder = str(tmp_path / "scene")
-    syn.write_dense_folder(sc, folder, ext)
-    r = subprocess.run([os.path.join(here, "hpm_mvs"), folder, "--seed", "7", "--levels", "1"], capture_output=True,
-                       text=True, timeout=600)
-    assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
+    folder, per_problem = str(tmp_path / "scene"), str(tmp_path / "scene_pp")
+    for f, extra in ((folder, []), (per_problem, ["--per-problem"])):
+        syn.write_dense_folder(sc, f, ext)
+        r = subprocess.run([os.path.join(here, "hpm_mvs"), f, "--seed", "7", "--levels", "1"] + extra,
+                           capture_output=True, text=True, timeout=600)
+        assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
     pairs = hb.read_pair(os.path.join(folder, "pair.txt"))
     imgs = [cv2.imread(os.path.join(folder, "images", f"{v:08d}{ext}"), cv2.IMREAD_GRAYSCALE).astype(np.float32)
             for v in range(4)]
@@ -207,14 +209,17 @@ def test_host_main_writes_the_scene_driver_maps(tmp_path, ext):
     for v in range(4):
         cams[v]["width"], cams[v]["height"] = 160, 120
     with hb.Context() as ctx:
-        sd, sn, scost = ctx.run_scene(imgs, cams, pairs, seed=7, pyramid_levels=1, geom_iterations=2)
+        sd, sn, scost, spass, sprior = ctx.run_scene(imgs, cams, pairs, seed=7, pyramid_levels=1, geom_iterations=2,
+                                                     extra_maps=True)
+    names = ["depths_geom.dmb", "normals.dmb", "costs.dmb", "depths.dmb", "depths_prior.dmb"]
     for v in range(4):
         out = os.path.join(folder, "HPM", f"2333_{v:08d}")
-        np.testing.assert_array_equal(hb.read_dmb(os.path.join(out, "depths_geom.dmb")), sd[v])
-        np.testing.assert_array_equal(hb.read_dmb(os.path.join(out, "normals.dmb")), sn[v])
-        np.testing.assert_array_equal(hb.read_dmb(os.path.join(out, "costs.dmb")), scost[v])
-        assert hb.read_dmb(os.path.join(out, "depths.dmb")).shape == (120, 160)
-        assert (hb.read_dmb(os.path.join(out, "depths_prior.dmb")) > 0).mean() > 0.3
+        for name, want in zip(names, (sd[v], sn[v], scost[v], spass[v], sprior[v])):
+            np.testing.assert_array_equal(hb.read_dmb(os.path.join(out, name)), want)
+            # the reference's problem-by-problem order (--per-problem) writes the same files
+            pp = os.path.join(per_problem, "HPM", f"2333_{v:08d}", name)
+            assert open(pp, "rb").read() == open(os.path.join(out, name), "rb").read(), (v, name)
+        assert (sprior[v] > 0).mean() > 0.3
     # the Python front end over the same folder
     py = str(tmp_path / "scene_py")
     syn.write_dense_folder(sc, py, ext)
@@ -223,9 +228,9 @@ def test_host_main_writes_the_scene_driver_maps(tmp_path, ext):
     assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
     for v in range(4):
         np.testing.assert_array_equal(hb.read_dmb(os.path.join(py, "HPM", f"2333_{v:08d}", "depths_geom.dmb")), sd[v])
-    # both fused the same maps into the same point cloud (HPM/HPM_model.ply)
-    plys = [open(os.path.join(f, "HPM", "HPM_model.ply"), "rb").read() for f in (folder, py)]
-    assert plys[0] == plys[1] and plys[0].startswith(b"ply\n") and len(plys[0]) > 10000
+    # all three fused the same maps into the same point cloud (HPM/HPM_model.ply)
+    plys = [open(os.path.join(f, "HPM", "HPM_model.ply"), "rb").read() for f in (folder, per_problem, py)]
+    assert plys[0] == plys[1] == plys[2] and plys[0].startswith(b"ply\n") and len(plys[0]) > 10000
 
 
 def test_view_sharded_driver_on_the_gpu():
