@@ -402,7 +402,7 @@ template <typename Win>
 __device__ HPM_CV_INLINE void cost_vector(const PMArgs &a, int px, int py, float4 h, const Win *sWW, int tid,
                                          RefStats rs, float *out, int stride)
 {
-    for (int v = 1; v < a.n; ++v) out[(v - 1) * stride] = ncc(a, v, px, py, h, sWW, tid, rs);
+    for (int v = 1; v < a.n; ++v) out[(size_t)(v - 1) * stride] = ncc(a, v, px, py, h, sWW, tid, rs);
     if (a.counters) atomicAdd(&a.counters[0], (unsigned long long)(a.n - 1));
 }
 
@@ -424,7 +424,7 @@ __device__ float initial_cost_from(const PMArgs &a, const float *cv, int stride,
     const int S = a.n - 1;
     int valid = 0;
     for (int v = 0; v < S; ++v) {
-        srt[v] = cv[v * stride];
+        srt[v] = cv[(size_t)v * stride];
         if (srt[v] < 2.0f) valid++;
     }
     sort_small(srt, S);
@@ -436,7 +436,7 @@ __device__ float initial_cost_from(const PMArgs &a, const float *cv, int stride,
         for (int i = 0; i < top_k; ++i) cost += srt[i];
         const float thr = srt[top_k - 1];
         for (int i = 0; i < S; ++i)
-            if (cv[i * stride] <= thr) sel |= 1u << i;
+            if (cv[(size_t)i * stride] <= thr) sel |= 1u << i;
         result = cost / top_k;
     }
     *views = sel;
