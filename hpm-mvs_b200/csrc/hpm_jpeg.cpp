@@ -80,6 +80,7 @@ struct Huffman {
         for (int l = 1; l <= 16; ++l) {
             valoff[l] = k - code;
             for (int i = 0; i < counts[l - 1]; ++i, ++k, ++code) {
+                if (code >= (1 << l)) return false; /* more codes than the length allows */
                 if (l <= kLook) {
                     const int lo = code << (kLook - l), n = 1 << (kLook - l);
                     for (int j = 0; j < n; ++j) {
@@ -88,7 +89,6 @@ struct Huffman {
                     }
                 }
             }
-            if (code > (1 << l)) return false; /* more codes than the length allows */
             maxcode[l] = counts[l - 1] ? code - 1 : -1;
             code <<= 1;
         }

@@ -181,3 +181,51 @@ def test_rejected_files(tmp_path):
         f.write(bytes(buf[:sof + 6]))  # ends inside the frame header
     with pytest.raises(hb.HpmError):
         hb.read_gray8(path)
+
+
+def test_huffman_table_with_too_many_codes_is_rejected(tmp_path):
+    """A DHT whose counts ask for more codes of a length than that length
+    has (3 one-bit codes) is an error, not a write past the decode table."""
+    buf = bytearray(encode(picture(2, 24, 16), 90, "444"))
+    i = buf.index(b"\xff\xc4") + 5  # the 16 code counts of the first table
+    counts = buf[i:i + 16]
+    last = max(k for k in range(16) if counts[k] >= 2)
+    buf[i] += 3
+    buf[i + last] -= 3 if counts[last] >= 3 else 2
+    if counts[last] < 3:
+        buf[i] -= 1
+    path = str(tmp_path / "x.jpg")
+    with open(path, "wb") as f:
+        f.write(bytes(buf))
+    with pytest.raises(hb.HpmError):
+        hb.read_gray8(path)
+
+
+def test_damaged_files_decode_or_fail_cleanly(tmp_path):
+    """Bytes changed, inserted or removed anywhere in valid files, or the file
+    cut short: every read either returns an image or raises HpmError."""
+    rng = np.random.default_rng(0)
+    bases = [encode(picture(s, 40, 28), 85, smp, prog, rst) for s, smp, prog, rst in
+             [(1, "420", 0, 0), (2, "444", 1, 0), (3, "422", 0, 2), (4, "420", 1, 3)]]
+    path = str(tmp_path / "x.jpg")
+    for it in range(300):
+        b = bytearray(bases[it % len(bases)])
+        for _ in range(int(rng.integers(1, 6))):
+            i = int(rng.integers(2, len(b)))
+            op = int(rng.integers(0, 3))
+            if op == 0:
+                b[i] = int(rng.integers(0, 256))
+            elif op == 1:
+                b.insert(i, int(rng.integers(0, 256)))
+            elif len(b) > 10:
+                del b[i]
+        if rng.random() < 0.2:
+            b = b[:int(rng.integers(2, len(b)))]
+        with open(path, "wb") as f:
+            f.write(bytes(b))
+        for read in (hb.read_gray8, hb.read_bgr8):
+            try:
+                img = read(path)
+                assert img.dtype == np.uint8 and img.size > 0
+            except hb.HpmError:
+                pass
