@@ -5,7 +5,7 @@ library to the bytes cv::imread gives (HPM.cpp:492, main.cpp:523).
 
     python hpm-mvs_b200/hpm_mvs.py dense_folder [--seed S] [--levels K]
                                    [--geom-iterations G] [--no-prior] [--device D]
-                                   [--no-fusion]
+                                   [--no-fusion] [--per-problem]
 
 Writes HPM/2333_%08d/{depths,depths_geom,normals,costs,depths_prior}.dmb like
 the reference's ProcessProblem, then fuses them into HPM/HPM_model.ply
@@ -77,6 +77,27 @@ def process_problem(ctx, folder, ref, srcs, views, *, geom, planar_prior, multi_
     hb.write_dmb(os.path.join(out, "costs.dmb"), c)
 
 
+def run_scene(ctx, folder, problems, needed, views, *, planar_prior, geom_iterations, seed, levels):
+    """All passes in one hpm_run_scene_ex call (maps in device memory between
+    passes), then the files ProcessProblem leaves for every problem."""
+    index = {v: i for i, v in enumerate(needed)}
+    pairs = [(index[ref], [index[s] for s in srcs]) for ref, srcs in problems]
+    d, n, c, pa, pr = ctx.run_scene([views[v][0] for v in needed], np.array([views[v][1] for v in needed]), pairs,
+                                    planar_prior=planar_prior, geom_iterations=geom_iterations, seed=seed,
+                                    pyramid_levels=levels, extra_maps=True)
+    for ref, _ in problems:
+        i = index[ref]
+        out = os.path.join(folder, "HPM", f"2333_{ref:08d}")
+        os.makedirs(out, exist_ok=True)
+        if planar_prior:
+            hb.write_dmb(os.path.join(out, "depths_prior.dmb"), pr[i])
+        hb.write_dmb(os.path.join(out, "depths.dmb"), pa[i])
+        if geom_iterations > 0:
+            hb.write_dmb(os.path.join(out, "depths_geom.dmb"), d[i])
+        hb.write_dmb(os.path.join(out, "normals.dmb"), n[i])
+        hb.write_dmb(os.path.join(out, "costs.dmb"), c[i])
+
+
 def run_fusion(folder, problems, geom_consistency, device=0):
     """RunFusion (main.cpp:502-633) with RescaleImageAndCamera
     (HPM.cpp:187-208), whose 8-bit resize is OpenCV's own (cv2.resize, only
@@ -127,19 +148,25 @@ def main(argv=None):
     ap.add_argument("--no-prior", action="store_true")
     ap.add_argument("--device", type=int, default=0)
     ap.add_argument("--no-fusion", action="store_true")
+    ap.add_argument("--per-problem", action="store_true",
+                    help="ProcessProblem problem by problem through .dmb files, as the reference runs")
     a = ap.parse_args(argv)
     problems = hb.read_pair(os.path.join(a.dense_folder, "pair.txt"))
     needed = sorted({p[0] for p in problems} | {s for p in problems for s in p[1]})
     views = {v: load_view(a.dense_folder, v) for v in needed}
     print(f"There are {len(problems)} problems needed to be processed!")
     with hb.Context(a.device) as ctx:
-        for p, (ref, srcs) in enumerate(problems):
-            process_problem(ctx, a.dense_folder, ref, srcs, views, geom=False, planar_prior=not a.no_prior,
-                            multi_geometry=False, seed=a.seed + p, levels=a.levels)
-        for g in range(a.geom_iterations):
+        if a.per_problem:
             for p, (ref, srcs) in enumerate(problems):
-                process_problem(ctx, a.dense_folder, ref, srcs, views, geom=True, planar_prior=False,
-                                multi_geometry=g > 0, seed=a.seed + 1000003 * (g + 1) + p, levels=a.levels)
+                process_problem(ctx, a.dense_folder, ref, srcs, views, geom=False, planar_prior=not a.no_prior,
+                                multi_geometry=False, seed=a.seed + p, levels=a.levels)
+            for g in range(a.geom_iterations):
+                for p, (ref, srcs) in enumerate(problems):
+                    process_problem(ctx, a.dense_folder, ref, srcs, views, geom=True, planar_prior=False,
+                                    multi_geometry=g > 0, seed=a.seed + 1000003 * (g + 1) + p, levels=a.levels)
+        else:
+            run_scene(ctx, a.dense_folder, problems, needed, views, planar_prior=not a.no_prior,
+                      geom_iterations=a.geom_iterations, seed=a.seed, levels=a.levels)
     if not a.no_fusion:
         n = run_fusion(a.dense_folder, problems, a.geom_iterations > 0, a.device)
         print(f"Fused {n} points into {a.dense_folder}/HPM/HPM_model.ply")

@@ -220,17 +220,22 @@ def test_host_main_writes_the_scene_driver_maps(tmp_path, ext):
             pp = os.path.join(per_problem, "HPM", f"2333_{v:08d}", name)
             assert open(pp, "rb").read() == open(os.path.join(out, name), "rb").read(), (v, name)
         assert (sprior[v] > 0).mean() > 0.3
-    # the Python front end over the same folder
-    py = str(tmp_path / "scene_py")
-    syn.write_dense_folder(sc, py, ext)
-    r = subprocess.run([sys.executable, os.path.join(here, "hpm_mvs.py"), py, "--seed", "7", "--levels", "1"],
-                       capture_output=True, text=True, timeout=600)
-    assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
-    for v in range(4):
-        np.testing.assert_array_equal(hb.read_dmb(os.path.join(py, "HPM", f"2333_{v:08d}", "depths_geom.dmb")), sd[v])
-    # all three fused the same maps into the same point cloud (HPM/HPM_model.ply)
-    plys = [open(os.path.join(f, "HPM", "HPM_model.ply"), "rb").read() for f in (folder, per_problem, py)]
-    assert plys[0] == plys[1] == plys[2] and plys[0].startswith(b"ply\n") and len(plys[0]) > 10000
+    # the Python front end over the same folder, in both forms, writes the same files
+    pys = []
+    for tag, extra in (("py", []), ("py_pp", ["--per-problem"])):
+        py = str(tmp_path / f"scene_{tag}")
+        syn.write_dense_folder(sc, py, ext)
+        r = subprocess.run([sys.executable, os.path.join(here, "hpm_mvs.py"), py, "--seed", "7", "--levels", "1"]
+                           + extra, capture_output=True, text=True, timeout=600)
+        assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
+        for v in range(4):
+            for name in names:
+                a = open(os.path.join(py, "HPM", f"2333_{v:08d}", name), "rb").read()
+                assert a == open(os.path.join(folder, "HPM", f"2333_{v:08d}", name), "rb").read(), (tag, v, name)
+        pys.append(py)
+    # all fused the same maps into the same point cloud (HPM/HPM_model.ply)
+    plys = [open(os.path.join(f, "HPM", "HPM_model.ply"), "rb").read() for f in [folder, per_problem] + pys]
+    assert all(p == plys[0] for p in plys) and plys[0].startswith(b"ply\n") and len(plys[0]) > 10000
 
 
 def test_view_sharded_driver_on_the_gpu():
