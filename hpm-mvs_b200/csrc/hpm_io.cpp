@@ -19,6 +19,7 @@
  * Unlike the reference (which prints and carries on, or dereferences NULL on
  * a failed fopen), every failure returns HPM_ERR_IO.
  */
+#include <algorithm>
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
@@ -306,6 +307,53 @@ extern "C" int hpm_resize_linear(const float *src, int sw, int sh, int ch, float
                 const float h0 = std::fmaf(fx, b0 - a0, a0), h1 = std::fmaf(fx, b1 - a1, a1);
                 o[(size_t)x * ch + c] = std::fmaf(fy, h1 - h0, h0);
             }
+        }
+    }
+    return HPM_OK;
+}
+
+/* cv::resize(INTER_LINEAR) of an 8-bit image as OpenCV 4.13 computes it:
+ * 11-bit fixed-point weights round((1 - f) 2048) and round(f 2048) from the
+ * float source coordinate (d + 0.5) s - 0.5; horizontally the fraction is
+ * zeroed where the left or right tap leaves the image, vertically both rows
+ * are clamped into it and the fraction is kept; the vertical blend is
+ * ((H0 >> 4) b0 >> 16) + ((H1 >> 4) b1 >> 16), rounded by (x + 2) >> 2.
+ * Checked byte for byte against cv2.resize for down- and upscales. */
+extern "C" int hpm_resize_linear_u8(const uint8_t *src, int sw, int sh, int ch, uint8_t *dst, int dw, int dh)
+{
+    if (!src || !dst || sw < 1 || sh < 1 || dw < 1 || dh < 1 || ch < 1) return HPM_ERR_ARG;
+    const double scale_x = (double)sw / dw, scale_y = (double)sh / dh;
+    std::vector<int> x0(dw), x1(dw), a0(dw), a1(dw);
+    for (int x = 0; x < dw; ++x) {
+        float f = (float)((x + 0.5) * scale_x - 0.5);
+        int sx = (int)std::floor(f);
+        f -= (float)sx;
+        if (sx < 0) f = 0.0f, sx = 0;
+        if (sx >= sw - 1) f = 0.0f, sx = sw - 1;
+        x0[x] = sx;
+        x1[x] = std::min(sx + 1, sw - 1);
+        a0[x] = (int)std::lrintf((1.0f - f) * 2048.0f);
+        a1[x] = (int)std::lrintf(f * 2048.0f);
+    }
+    std::vector<int> h0((size_t)dw * ch), h1((size_t)dw * ch);
+    auto horizontal = [&](int row, std::vector<int> &out) {
+        const uint8_t *r = src + (size_t)row * sw * ch;
+        for (int x = 0; x < dw; ++x)
+            for (int c = 0; c < ch; ++c)
+                out[(size_t)x * ch + c] = r[(size_t)x0[x] * ch + c] * a0[x] + r[(size_t)x1[x] * ch + c] * a1[x];
+    };
+    for (int y = 0; y < dh; ++y) {
+        float f = (float)((y + 0.5) * scale_y - 0.5);
+        const int sy = (int)std::floor(f);
+        f -= (float)sy;
+        const int r0 = std::min(std::max(sy, 0), sh - 1), r1 = std::min(std::max(sy + 1, 0), sh - 1);
+        const int b0 = (int)std::lrintf((1.0f - f) * 2048.0f), b1 = (int)std::lrintf(f * 2048.0f);
+        horizontal(r0, h0);
+        horizontal(r1, h1);
+        uint8_t *o = dst + (size_t)y * dw * ch;
+        for (size_t k = 0; k < (size_t)dw * ch; ++k) {
+            const int v = ((((h0[k] >> 4) * b0) >> 16) + (((h1[k] >> 4) * b1) >> 16) + 2) >> 2;
+            o[k] = (uint8_t)(v < 0 ? 0 : v > 255 ? 255 : v);
         }
     }
     return HPM_OK;

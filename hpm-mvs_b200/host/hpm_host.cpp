@@ -496,15 +496,11 @@ long long RunFusion(const std::string &dense_folder, const std::vector<Problem> 
         const std::string ip = image_path(dense_folder, id);
         std::vector<uint8_t> bgr(*image_cache().get(ip, 3, &iw, &ih, false));
         if (iw != w || ih != h) {
-            /* RescaleImageAndCamera, HPM.cpp:187-208.  The reference resizes
-             * the 8-bit image with OpenCV's fixed-point bilinear; this is the
-             * float bilinear rounded, which differs from it by 1 in about an
-             * eighth of the colour bytes (images above the 3200-pixel cap). */
-            std::vector<float> f(bgr.begin(), bgr.end()), g((size_t)3 * w * h);
-            int r2 = hpm_resize_linear(f.data(), iw, ih, 3, g.data(), w, h);
+            /* RescaleImageAndCamera, HPM.cpp:187-208: OpenCV's 8-bit bilinear */
+            std::vector<uint8_t> g((size_t)3 * w * h);
+            int r2 = hpm_resize_linear_u8(bgr.data(), iw, ih, 3, g.data(), w, h);
             if (r2 != HPM_OK) throw Error(r2, "colour resize");
-            bgr.resize(g.size());
-            for (size_t k = 0; k < g.size(); ++k) bgr[k] = (uint8_t)std::min(255.0f, std::max(0.0f, std::round(g[k])));
+            bgr.swap(g);
             const float sx = w / (float)iw, sy = h / (float)ih;
             cam.K[0] *= sx;
             cam.K[2] *= sx;

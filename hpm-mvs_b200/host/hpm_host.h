@@ -119,8 +119,8 @@ private:
  * (depths_geom.dmb with geom_consistency, else depths.dmb) and normals.dmb
  * into dense_folder/HPM/HPM_model.ply; returns the number of points.
  * Colours come from images/ (JPEG, PNG or PGM); an image whose size differs
- * from its depth map is resized bilinearly (RescaleImageAndCamera,
- * HPM.cpp:187-208), not bit-exactly as OpenCV's 8-bit path. */
+ * from its depth map is resized as RescaleImageAndCamera does it
+ * (HPM.cpp:187-208, OpenCV's 8-bit bilinear, byte for byte). */
 long long RunFusion(const std::string &dense_folder, const std::vector<Problem> &problems, bool geom_consistency,
                     int device = 0);
 

@@ -38,7 +38,7 @@ EXPORTED = [
     "hpm_count_enable", "hpm_count_read", "hpm_write_dmb", "hpm_read_dmb", "hpm_read_camera", "hpm_read_pair",
     "hpm_fp32_peak", "hpm_jbu_noalloc", "hpm_process_problem", "hpm_last_prior_stats", "hpm_delaunay",
     "hpm_prior_level", "hpm_run_scene", "hpm_run_scene_ex", "hpm_read_gray8", "hpm_resize_linear",
-    "hpm_fuse", "hpm_write_ply", "hpm_read_bgr8", "hpm_set_scene_workers",
+    "hpm_fuse", "hpm_write_ply", "hpm_read_bgr8", "hpm_set_scene_workers", "hpm_resize_linear_u8",
 ]
 
 
@@ -453,6 +453,17 @@ def write_ply(path: str, xyz, normal, bgr) -> None:
     rc = lib().hpm_write_ply(path.encode(), ctypes.c_longlong(len(xyz)), _p(xyz), _p(normal), _p(bgr))
     if rc != HPM_OK:
         raise HpmError(f"hpm_write_ply({path}): {STATUS_NAMES.get(rc, rc)}")
+
+
+def resize_linear_u8(src: np.ndarray, dw: int, dh: int) -> np.ndarray:
+    """cv::resize INTER_LINEAR of a uint8 [H, W] or [H, W, C] image, byte for byte (host)."""
+    src = np.ascontiguousarray(src, dtype=np.uint8)
+    ch = 1 if src.ndim == 2 else src.shape[2]
+    out = np.empty((dh, dw) if src.ndim == 2 else (dh, dw, ch), np.uint8)
+    rc = lib().hpm_resize_linear_u8(_p(src), src.shape[1], src.shape[0], ch, _p(out), dw, dh)
+    if rc != HPM_OK:
+        raise HpmError(f"hpm_resize_linear_u8: {rc}")
+    return out
 
 
 def resize_linear(src: np.ndarray, dw: int, dh: int) -> np.ndarray:

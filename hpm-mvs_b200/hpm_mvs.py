@@ -100,8 +100,8 @@ def run_scene(ctx, folder, problems, needed, views, *, planar_prior, geom_iterat
 
 def run_fusion(folder, problems, geom_consistency, device=0):
     """RunFusion (main.cpp:502-633) with RescaleImageAndCamera
-    (HPM.cpp:187-208), whose 8-bit resize is OpenCV's own (cv2.resize, only
-    for images larger than their depth maps); returns the point count."""
+    (HPM.cpp:187-208: OpenCV's 8-bit bilinear, reproduced by
+    hpm_resize_linear_u8); returns the point count."""
     cams, depths, normals, colors = [], [], [], []
     for ref, _ in problems:
         out = os.path.join(folder, "HPM", f"2333_{ref:08d}")
@@ -118,10 +118,8 @@ def run_fusion(folder, problems, geom_consistency, device=0):
             raise hb.HpmError(f"no colour image for view {ref}")
         h, w = d.shape
         if img.shape[:2] != (h, w):
-            import cv2
-
             sx, sy = np.float32(w) / np.float32(img.shape[1]), np.float32(h) / np.float32(img.shape[0])
-            img = cv2.resize(img, (w, h), interpolation=cv2.INTER_LINEAR)
+            img = hb.resize_linear_u8(img, w, h)
             K = cam["K"]
             K[0] *= sx
             K[2] *= sx

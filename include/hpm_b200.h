@@ -332,6 +332,11 @@ int hpm_read_bgr8(const char *path, uint8_t *pixels, size_t cap, int *w, int *h)
  * InuputInitialization (HPM.cpp:525-551).  Same arithmetic as OpenCV 4.x
  * (double-precision fractions, one fused a + f*(b-a) per direction). */
 int hpm_resize_linear(const float *src, int sw, int sh, int ch, float *dst, int dw, int dh);
+/* cv::resize(src, dst, Size(dw, dh), 0, 0, INTER_LINEAR) of an 8-bit image
+ * of ch interleaved channels, byte for byte as OpenCV computes it, as in
+ * RescaleImageAndCamera (HPM.cpp:187-208), which resizes the fusion's colour
+ * images (cv::Mat_<cv::Vec3b>) to their depth maps. */
+int hpm_resize_linear_u8(const uint8_t *src, int sw, int sh, int ch, uint8_t *dst, int dw, int dh);
 /* pair.txt (GenerateSampleList, main.cpp:4-33): returns the problem count
  * into *n; ref_ids[n], src_counts[n], src_ids[n][HPM_MAX_IMAGES-1] filled when
  * non-NULL (sources with score <= 0 are dropped). */

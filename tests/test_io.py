@@ -57,3 +57,17 @@ def test_synthetic_scene_command_writes_a_dense_folder(tmp_path):
         assert hb.read_camera(os.path.join(folder, "cams", f"{v:08d}_cam.txt"))["depth_max"] > 0
         gt = hb.read_dmb(os.path.join(folder, "gt", f"{v:08d}.dmb"))
         assert gt.shape == (48, 64) and (gt > 0).mean() > 0.9
+
+
+@pytest.mark.parametrize("src,dst,ch", [((4000, 3000), (3200, 2400), 3), ((3301, 2001), (3200, 1940), 3),
+                                        ((641, 479), (500, 377), 3), ((640, 480), (320, 240), 3),
+                                        ((97, 61), (200, 130), 3), ((33, 17), (34, 18), 1), ((1600, 1200), (1599, 1199), 1)])
+def test_resize_linear_u8_matches_cv2(src, dst, ch):
+    """RescaleImageAndCamera (HPM.cpp:187-208) resizes the fusion's 8-bit
+    colour images with cv::resize INTER_LINEAR: the fixed-point result is
+    reproduced byte for byte, downscales (the 3200-pixel cap), 2:1 and
+    upscales alike."""
+    rng = np.random.default_rng(src[0] + dst[0] + ch)
+    shape = (src[1], src[0], ch) if ch > 1 else (src[1], src[0])
+    img = rng.integers(0, 256, shape, dtype=np.uint8)
+    np.testing.assert_array_equal(hb.resize_linear_u8(img, *dst), cv2.resize(img, dst, interpolation=cv2.INTER_LINEAR))
