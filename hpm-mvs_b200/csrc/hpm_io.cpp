@@ -322,7 +322,9 @@ extern "C" int hpm_resize_linear(const float *src, int sw, int sh, int ch, float
 extern "C" int hpm_resize_linear_u8(const uint8_t *src, int sw, int sh, int ch, uint8_t *dst, int dw, int dh)
 {
     if (!src || !dst || sw < 1 || sh < 1 || dw < 1 || dh < 1 || ch < 1) return HPM_ERR_ARG;
-    const double scale_x = (double)sw / dw, scale_y = (double)sh / dh;
+    /* the scale as OpenCV forms it, 1 / (dst / src): sw / dw can differ from
+     * it by one ulp, which can move a floor or an 11-bit weight */
+    const double scale_x = 1.0 / ((double)dw / sw), scale_y = 1.0 / ((double)dh / sh);
     std::vector<int> x0(dw), x1(dw), a0(dw), a1(dw);
     for (int x = 0; x < dw; ++x) {
         float f = (float)((x + 0.5) * scale_x - 0.5);

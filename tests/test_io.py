@@ -71,3 +71,19 @@ def test_resize_linear_u8_matches_cv2(src, dst, ch):
     shape = (src[1], src[0], ch) if ch > 1 else (src[1], src[0])
     img = rng.integers(0, 256, shape, dtype=np.uint8)
     np.testing.assert_array_equal(hb.resize_linear_u8(img, *dst), cv2.resize(img, dst, interpolation=cv2.INTER_LINEAR))
+
+
+def test_resize_linear_u8_random_sizes_match_cv2():
+    """A seeded sweep of source and destination sizes (down, up, mixed, one
+    axis unchanged), so that the byte equality does not rest on the handful
+    of sizes above."""
+    rng = np.random.default_rng(2024)
+    for _ in range(300):
+        sw, sh = (int(x) for x in rng.integers(1, 260, 2))
+        dw, dh = (int(x) for x in rng.integers(1, 260, 2))
+        ch = int(rng.choice([1, 3]))
+        shape = (sh, sw, ch) if ch > 1 else (sh, sw)
+        img = rng.integers(0, 256, shape, dtype=np.uint8)
+        np.testing.assert_array_equal(hb.resize_linear_u8(img, dw, dh),
+                                      cv2.resize(img, (dw, dh), interpolation=cv2.INTER_LINEAR),
+                                      err_msg=f"{sw}x{sh} -> {dw}x{dh}, {ch} channels")
