@@ -48,9 +48,9 @@ METRIC = "depth Mpix/s, plain vs batched prior-net form on 1 B200, at equal %px 
 WORKLOAD = dict(width=1600, height=1200, n_views=11, n_planes=20, n_spheres=5, low_texture=0.40, pyramid_levels=2,
                 geom_iterations=2)
 
-# DRAM traffic of one half-step (k_prop_dirs + k_prop_refine), from the ncu
-# capture summarised in profiles/prop_kernels_1600x1200_s10.md (1600x1200,
-# 10 sources), per pixel: the hand-off buffers grow with the pixel count
+# DRAM traffic of one half-step (k_prop_dirs + k_prop_refine), from an ncu
+# capture of `bench.py --pass-case` (1600x1200, 10 sources), per pixel: the
+# hand-off buffers grow with the pixel count
 TRAFFIC_BYTES_PER_PX_HALF_STEP = (847.3 + 750.8 + 1805.0 + 623.2) * 1e6 / (1600 * 1200)
 GEOM_TERM_FLOPS = 120  # two projections (world point + camera, 3x3 each) and the reprojection distance
 TAPS, NCC_FLOPS_PER_TAP, FLOPS_PER_HYP_VIEW = 36, 34, 80
@@ -392,7 +392,8 @@ def run_ours(args, dist):
                      "frac": achieved / peak,
                      "traffic": TRAFFIC_BYTES_PER_PX_HALF_STEP * npx,
                      "traffic_note": "DRAM bytes per half-step (k_prop_dirs + k_prop_refine) from the ncu capture "
-                                     "at 1280x960, scaled by pixels",
+                                     "of bench.py --pass-case at 1600x1200 (10 sources), per pixel of the "
+                                     "workload",
                      "kernel": "k_prop_dirs + k_prop_refine (one red/black half-step)",
                      "peak_source": "measured FP32 FMA probe (hpm_fp32_peak) of measured; "
                                     "MEASURED_PEAKS.json has no FP32 figure",

@@ -474,6 +474,32 @@ int hpm_cost_vectors(hpm_ctx *c, const float *planes, float *out)
     return HPM_OK;
 }
 
+int hpm_tap_samples(hpm_ctx *c, const float *planes, const int *pixels, int n, float *out, int *inside)
+{
+    if (!c || !planes || (!pixels && n > 0) || n < 0 || !out || !inside) return HPM_ERR_ARG;
+    if (c->n < 2) return fail(c, HPM_ERR_STATE, "hpm_tap_samples before hpm_set_views");
+    const size_t np = npx(c), S = c->n - 1;
+    for (int k = 0; k < n; ++k)
+        if (pixels[k] < 0 || (size_t)pixels[k] >= np) return fail(c, HPM_ERR_ARG, "pixel index %d outside the view", pixels[k]);
+    int r = select_device(c);
+    if (r) return r;
+    void *buf;
+    r = scratch(c, np * sizeof(float4) + (size_t)n * (sizeof(int) + S * (kTaps * sizeof(float) + sizeof(int))), &buf);
+    if (r) return r;
+    float4 *d_pl = (float4 *)buf;
+    float *d_out = (float *)(d_pl + np);
+    int *d_in = (int *)(d_out + (size_t)n * S * kTaps);
+    int *d_px = d_in + (size_t)n * S;
+    CK(cudaMemcpyAsync(d_pl, planes, sizeof(float4) * np, cudaMemcpyHostToDevice, c->stream), "planes");
+    if (n > 0) CK(cudaMemcpyAsync(d_px, pixels, sizeof(int) * n, cudaMemcpyHostToDevice, c->stream), "pixels");
+    PMArgs a = make_args(c);
+    CK(launch_tap_samples(a, d_pl, d_px, n, d_out, d_in, c->stream), "tap sample kernel");
+    CK(cudaMemcpyAsync(out, d_out, sizeof(float) * n * S * kTaps, cudaMemcpyDeviceToHost, c->stream), "samples");
+    CK(cudaMemcpyAsync(inside, d_in, sizeof(int) * n * S, cudaMemcpyDeviceToHost, c->stream), "inside");
+    CK(cudaStreamSynchronize(c->stream), "hpm_tap_samples");
+    return HPM_OK;
+}
+
 int hpm_initial_costs(hpm_ctx *c, const float *planes, float *out_cost, uint32_t *out_views)
 {
     if (!c || !planes || !out_cost || !out_views) return HPM_ERR_ARG;

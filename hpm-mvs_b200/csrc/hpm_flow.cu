@@ -101,12 +101,10 @@ static int build_level_prior(hpm_ctx *c, const HpmCamera &cam, const float *d_co
     CK(prior_ids_to_mask(ws.ids, (int)npx, ws.mask, s), "mask");
     /* KNN supplement over a uniform cell grid (counting sort on the host) */
     if (np >= 6) {
-        const int cell = 8, gw = (w + cell - 1) / cell, gh = (h + cell - 1) / cell;
-        std::vector<int> start(gw * gh + 1, 0), order(np);
-        for (int k = 0; k < np; ++k) start[(xy[2 * k + 1] / cell) * gw + xy[2 * k] / cell + 1]++;
-        for (int i = 0; i < gw * gh; ++i) start[i + 1] += start[i];
-        std::vector<int> fill(start.begin(), start.end() - 1);
-        for (int k = 0; k < np; ++k) order[fill[(xy[2 * k + 1] / cell) * gw + xy[2 * k] / cell]++] = k;
+        const int cell = 8;
+        int gw, gh;
+        std::vector<int> start, order;
+        knn_grid(xy.data(), np, w, h, cell, gw, gh, start, order);
         CK(ws_reserve_grid(c, np, gw * gh + 1), "knn grid");
         CK(cudaMemcpyAsync(ws.pts, xy.data(), sizeof(int) * 2 * np, cudaMemcpyHostToDevice, s), "points");
         CK(cudaMemcpyAsync(ws.cell_start, start.data(), sizeof(int) * start.size(), cudaMemcpyHostToDevice, s), "grid");

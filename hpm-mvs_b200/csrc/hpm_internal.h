@@ -75,6 +75,8 @@ cudaError_t launch_cost_vectors(const PMArgs &a, const float4 *planes, float *ou
 cudaError_t launch_initial_costs(const PMArgs &a, const float4 *planes, float *cost, uint32_t *views,
                                  cudaStream_t s);
 cudaError_t launch_geom_costs(const PMArgs &a, const float4 *planes, float *out, cudaStream_t s);
+cudaError_t launch_tap_samples(const PMArgs &a, const float4 *planes, const int *pixels, int n, float *out,
+                               int *inside, cudaStream_t s);
 cudaError_t launch_jbu(const float *guide, int cols, int rows, const float *coarse_depth,
                        const float4 *coarse_normal, int s_cols, int s_rows, int image_scale, float *out_depth,
                        float4 *out_normal, cudaStream_t s);

@@ -337,6 +337,16 @@ __device__ RefStats ref_window(const PMArgs &a, int px, int py, Win *sWW, int ti
     return s;
 }
 
+/* Source sample of tap (i, j) of pixel (fpx, fpy): the warped tap position
+ * (ComputeCorrespondingPoint, HPM.cu:289-296) through the texture unit at
+ * +0.5 (HPM.cu:358-359).  One definition for the NCC and the tap-sample
+ * export, so that both evaluate the same expression. */
+__device__ __forceinline__ float tap_sample(cudaTextureObject_t tex, const float *H, float fpx, float fpy, int i, int j)
+{
+    const float2 q = warp(H, fpx + (float)i, fpy + (float)j);
+    return tex2D<float>(tex, q.x + 0.5f, q.y + 0.5f);
+}
+
 /* The source-side half of ComputeBilateralNCC (HPM.cu:325-397). */
 template <typename Win>
 __device__ __forceinline__ float ncc(const PMArgs &a, int v, int px, int py, float4 h, const Win *sWW, int tid,
@@ -357,8 +367,7 @@ __device__ __forceinline__ float ncc(const PMArgs &a, int v, int px, int py, flo
         float r_src = 0.0f, r_ss = 0.0f, r_rs = 0.0f;
 #pragma unroll
         for (int j = -5; j < 6; j += 2, ++t) {
-            const float2 q = warp(H, fpx + (float)i, fpy + (float)j);
-            const float sp = tex2D<float>(tex, q.x + 0.5f, q.y + 0.5f);
+            const float sp = tap_sample(tex, H, fpx, fpy, i, j);
             float2 ww;
             if constexpr (sizeof(Win) == sizeof(float)) {
                 const float wt = sWW[t * kBlock + tid];
@@ -1205,6 +1214,29 @@ __global__ void k_geom_costs(const __grid_constant__ PMArgs a, const float4 *pla
     for (int v = 1; v < a.n; ++v) out[(size_t)c * S + v - 1] = geom_cost(a, v, planes[c], px, py);
 }
 
+/* The 36 source samples of the NCC window of listed pixels, per source view
+ * (the values ncc() weighs), and whether the warped centre is inside. */
+__global__ void k_tap_samples(const __grid_constant__ PMArgs a, const float4 *planes, const int *pixels, int n,
+                              float *out, int *inside)
+{
+    const int S = a.n - 1;
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n * S) return;
+    const int pi = k / S, v = k % S + 1;
+    const int px = pixels[pi] % a.W, py = pixels[pi] / a.W;
+    const HpmCamera &sc = a.cam[v];
+    float H[9];
+    homography(a.cam[0], sc, a.pair[v], planes[pixels[pi]], H);
+    const float fpx = (float)px, fpy = (float)py;
+    const float2 pt = warp(H, fpx, fpy);
+    inside[k] = !(pt.x >= sc.width || pt.x < 0.0f || pt.y >= sc.height || pt.y < 0.0f);
+    int t = 0;
+#pragma unroll
+    for (int i = -5; i < 6; i += 2)
+#pragma unroll
+        for (int j = -5; j < 6; j += 2, ++t) out[(size_t)k * kTaps + t] = tap_sample(a.view[v].tex, H, fpx, fpy, i, j);
+}
+
 template <int SMAX>
 cudaError_t launch_prop_t(const PMArgs &a, int iter, int color, cudaStream_t s)
 {
@@ -1269,6 +1301,14 @@ cudaError_t launch_initial_costs(const PMArgs &a, const float4 *planes, float *c
                                  cudaStream_t s)
 {
     k_initial_costs<<<pixel_grid(a.W, a.H), dim3(kBlockX, kBlockY), 0, s>>>(a, planes, cost, views);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_tap_samples(const PMArgs &a, const float4 *planes, const int *pixels, int n, float *out,
+                               int *inside, cudaStream_t s)
+{
+    const int total = n * (a.n - 1);
+    if (total > 0) k_tap_samples<<<(total + 127) / 128, 128, 0, s>>>(a, planes, pixels, n, out, inside);
     return cudaGetLastError();
 }
 

@@ -228,23 +228,15 @@ __constant__ unsigned char kTriples[20][3] = {{0, 1, 2}, {0, 1, 3}, {0, 1, 4}, {
                                               {0, 3, 5}, {0, 4, 5}, {1, 2, 5}, {1, 3, 5}, {1, 4, 5}, {2, 3, 5},
                                               {2, 4, 5}, {3, 4, 5}};
 
-/* One thread per pixel whose mask is <= 0.  The 6 nearest support points
- * (squared distance, ties to the lower point index) come from rings of
- * cells of a uniform grid: a ring is searched only while it can still hold a
- * point closer than the current 6th.  Then the first non-collinear triple,
- * the plane fit and the depth-range test of HPM.cpp:982-1093. */
-__global__ void k_knn_prior(HpmCamera cam, const int2 *__restrict__ pts, const int *__restrict__ cell_start,
-                            const int *__restrict__ cell_pts, int cell, int gw, int gh, const float *__restrict__ depth,
-                            int w, int h, float factor, float dmin, float dmax, float *__restrict__ mask,
-                            float4 *__restrict__ planes)
+/* The 6 support points nearest to (x, y) (squared distance, ties to the
+ * lower point index): rings of cells of a uniform grid around the query's
+ * cell, a ring searched only while it can still hold a point closer than the
+ * current 6th.  Returns how many were found (fewer than 6 only when there
+ * are fewer points); bi gets their indices nearest first. */
+__device__ int knn6(int x, int y, const int2 *__restrict__ pts, const int *__restrict__ cell_start,
+                    const int *__restrict__ cell_pts, int cell, int gw, int gh, int *bi)
 {
-    const int x = blockIdx.x * blockDim.x + threadIdx.x;
-    const int y = blockIdx.y * blockDim.y + threadIdx.y;
-    if (x >= w || y >= h) return;
-    const size_t c = (size_t)y * w + x;
-    if (mask[c] > 0) return;
     long long bd[6];
-    int bi[6];
     int nb = 0;
     const int cx = min(x / cell, gw - 1), cy = min(y / cell, gh - 1);
     const int max_ring = max(gw, gh);
@@ -280,6 +272,24 @@ __global__ void k_knn_prior(HpmCamera cam, const int2 *__restrict__ pts, const i
             }
         }
     }
+    return nb;
+}
+
+/* One thread per pixel whose mask is <= 0: its 6 nearest support points
+ * (knn6), then the first non-collinear triple, the plane fit and the
+ * depth-range test of HPM.cpp:982-1093. */
+__global__ void k_knn_prior(HpmCamera cam, const int2 *__restrict__ pts, const int *__restrict__ cell_start,
+                            const int *__restrict__ cell_pts, int cell, int gw, int gh, const float *__restrict__ depth,
+                            int w, int h, float factor, float dmin, float dmax, float *__restrict__ mask,
+                            float4 *__restrict__ planes)
+{
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (x >= w || y >= h) return;
+    const size_t c = (size_t)y * w + x;
+    if (mask[c] > 0) return;
+    int bi[6];
+    const int nb = knn6(x, y, pts, cell_start, cell_pts, cell, gw, gh, bi);
     if (nb < 6) return;
     int sel = -1;
     for (int t = 0; t < 20 && sel < 0; ++t)
@@ -296,6 +306,25 @@ __global__ void k_knn_prior(HpmCamera cam, const int2 *__restrict__ pts, const i
         mask[c] = -233.0f;
         planes[c] = n4;
     }
+}
+
+/* The index sets alone: nn6[6 c + k] = k-th nearest support point of pixel c
+ * (mask <= 0, or every pixel without a mask), -1 elsewhere or past the
+ * number of points. */
+__global__ void k_knn6_ids(const int2 *__restrict__ pts, const int *__restrict__ cell_start,
+                           const int *__restrict__ cell_pts, int cell, int gw, int gh, int w, int h,
+                           const float *__restrict__ mask, int *__restrict__ nn6)
+{
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (x >= w || y >= h) return;
+    const size_t c = (size_t)y * w + x;
+    int bi[6] = {-1, -1, -1, -1, -1, -1};
+    if (!mask || mask[c] <= 0) {
+        const int nb = knn6(x, y, pts, cell_start, cell_pts, cell, gw, gh, bi);
+        for (int k = nb; k < 6; ++k) bi[k] = -1;
+    }
+    for (int k = 0; k < 6; ++k) nn6[6 * c + k] = bi[k];
 }
 
 /* ---------------- prior assembly ---------------- */
@@ -444,6 +473,19 @@ cudaError_t prior_triangles(const HpmCamera &cam, const float *depth, int w, int
     if (e != cudaSuccess || n == 0) return e;
     k_tri_planes<<<(n + 127) / 128, 128, 0, s>>>(cam, depth, w, tris, n, factor, planes);
     k_tri_raster<<<(n + 3) / 4, 128, 0, s>>>(tris, n, w, ids);
+    return cudaGetLastError();
+}
+
+cudaError_t prior_raster(const int *tris, int n, int w, int *ids, cudaStream_t s)
+{
+    if (n > 0) k_tri_raster<<<(n + 3) / 4, 128, 0, s>>>(tris, n, w, ids);
+    return cudaGetLastError();
+}
+
+cudaError_t prior_knn_ids(const int2 *pts, const int *cell_start, const int *cell_pts, int cell, int gw, int gh, int w,
+                          int h, const float *mask, int *nn6, cudaStream_t s)
+{
+    k_knn6_ids<<<grid2(w, h), dim3(16, 16), 0, s>>>(pts, cell_start, cell_pts, cell, gw, gh, w, h, mask, nn6);
     return cudaGetLastError();
 }
 

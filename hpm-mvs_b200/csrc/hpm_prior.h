@@ -17,6 +17,13 @@ cudaError_t prior_resize(const float *src, int sw, int sh, int ch, float *dst, i
 cudaError_t prior_support_blocks(const float *costs, int w, int h, int2 *out, int *nblocks, cudaStream_t s);
 cudaError_t prior_triangles(const HpmCamera &cam, const float *depth, int w, int h, const int *tris, int n,
                             float factor, float4 *planes, int *ids, cudaStream_t s);
+cudaError_t prior_raster(const int *tris, int n, int w, int *ids, cudaStream_t s);
+cudaError_t prior_knn_ids(const int2 *pts, const int *cell_start, const int *cell_pts, int cell, int gw, int gh, int w,
+                          int h, const float *mask, int *nn6, cudaStream_t s);
+/* Uniform grid of `cell`-pixel cells over w x h for the kNN search (CSR:
+ * start[gw*gh+1], order[n] point indices ascending within a cell). */
+void knn_grid(const int *xy, int n, int w, int h, int cell, int &gw, int &gh, std::vector<int> &start,
+              std::vector<int> &order);
 cudaError_t prior_ids_to_mask(const int *ids, int n, float *mask, cudaStream_t s);
 cudaError_t prior_knn(const HpmCamera &cam, const int2 *pts, const int *cell_start, const int *cell_pts, int cell,
                       int gw, int gh, const float *depth, int w, int h, float factor, float dmin, float dmax, float *mask,

@@ -39,6 +39,8 @@ EXPORTED = [
     "hpm_fp32_peak", "hpm_jbu_noalloc", "hpm_process_problem", "hpm_last_prior_stats", "hpm_delaunay",
     "hpm_prior_level", "hpm_run_scene", "hpm_run_scene_ex", "hpm_read_gray8", "hpm_resize_linear",
     "hpm_fuse", "hpm_write_ply", "hpm_read_bgr8", "hpm_set_scene_workers", "hpm_resize_linear_u8",
+    "hpm_raster_triangles", "hpm_knn6", "hpm_tap_samples", "hpm_net_pack_weights", "hpm_net_conv3x3",
+    "hpm_net_conv_wgrad",
 ]
 
 
@@ -61,6 +63,29 @@ def delaunay(points: np.ndarray, w: int, h: int) -> np.ndarray:
     out = np.zeros((max(n, 1), 6), np.int32)
     n2 = lib().hpm_delaunay(_p(pts), len(pts), w, h, _p(out), len(out))
     return out[:n2]
+
+
+def raster_triangles(tris: np.ndarray, w: int, h: int, device: int = 0) -> np.ndarray:
+    """Triangle-id raster (h, w) int32 of the prior: index + 1 of the last
+    triangle reaching each pixel, 0 where none does."""
+    t = np.ascontiguousarray(tris, dtype=np.int32).reshape(-1, 6)
+    ids = np.zeros((h, w), np.int32)
+    rc = lib().hpm_raster_triangles(device, _p(t), len(t), w, h, _p(ids))
+    if rc != HPM_OK:
+        raise HpmError(f"hpm_raster_triangles: {STATUS_NAMES.get(rc, rc)}")
+    return ids
+
+
+def knn6(points: np.ndarray, w: int, h: int, mask=None, device: int = 0) -> np.ndarray:
+    """(h, w, 6) int32 indices of the 6 nearest support points per pixel
+    (mask <= 0, or all pixels), nearest first, -1 where not searched."""
+    pts = np.ascontiguousarray(points, dtype=np.int32).reshape(-1, 2)
+    out = np.zeros((h, w, 6), np.int32)
+    m = None if mask is None else np.ascontiguousarray(mask, dtype=np.float32)
+    rc = lib().hpm_knn6(device, _p(pts), len(pts), w, h, None if m is None else _p(m), _p(out))
+    if rc != HPM_OK:
+        raise HpmError(f"hpm_knn6: {STATUS_NAMES.get(rc, rc)}")
+    return out
 
 
 def fp32_peak(device: int = 0) -> float:
@@ -303,6 +328,17 @@ class Context:
         out = np.empty((h, w, self.n - 1), np.float32)
         self._check(lib().hpm_cost_vectors(self._h, _p(planes), _p(out)), "hpm_cost_vectors")
         return out
+
+    def tap_samples(self, planes, pixels):
+        """(samples [n][S][36], inside [n][S] bool) of the NCC windows of the
+        listed pixels (flat indices)."""
+        pl = np.ascontiguousarray(planes, dtype=np.float32)
+        px = np.ascontiguousarray(pixels, dtype=np.int32)
+        S = self.n - 1
+        out = np.zeros((len(px), S, 36), np.float32)
+        inside = np.zeros((len(px), S), np.int32)
+        self._check(lib().hpm_tap_samples(self._h, _p(pl), _p(px), len(px), _p(out), _p(inside)), "hpm_tap_samples")
+        return out, inside.astype(bool)
 
     def initial_costs(self, planes):
         h, w = self.shape

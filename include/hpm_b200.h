@@ -234,18 +234,50 @@ int hpm_jbu(hpm_ctx *ctx, const float *guide, int cols, int rows, const float *c
  * for the default stream) of `device`.  Same computation as hpm_jbu.
  *
  * Its scratch is a fixed device array of HPM_JBU_NOALLOC_MAX_COARSE float4
- * (16 MiB) that every GPU loading this library holds until the process
- * exits; coarse grids with more pixels are rejected with HPM_ERR_ARG.  The
- * first call on a device looks that array's address up (a CUDA symbol
- * query), so make the first call on each device before any stream capture.
- * All calls on a device share the array: calls that overlap on the GPU
- * (different streams, or different host threads) race and must be ordered
- * by the caller.  Returns HPM_OK without touching the outputs when the
+ * (16 MiB) that every GPU using this library holds until the process exits;
+ * coarse grids with more pixels are rejected with HPM_ERR_ARG.  The array
+ * takes its device memory when CUDA loads the library's device code on the
+ * device: under CUDA's default lazy module loading that is the first call of
+ * this function there.  So make the first call on each device before the
+ * caller reserves its memory budget and before any stream capture; later
+ * calls allocate nothing.  All calls on a device share the array: calls that
+ * overlap on the GPU (different streams, or different host threads) race and
+ * must be ordered by the caller.  The caller's current device is restored
+ * before returning.  Returns HPM_OK without touching the outputs when the
  * integer scale is 1, like hpm_jbu. */
 #define HPM_JBU_NOALLOC_MAX_COARSE (1 << 20)
 int hpm_jbu_noalloc(int device, const float *guide, int cols, int rows, const float *coarse_depth,
                     const float *coarse_normal, int s_cols, int s_rows, float *out_depth, float *out_normal,
                     void *stream);
+
+/* ---- Proposal network of the prior-net form (no counterpart in the
+ * reference).  Device pointers, work queued on `stream` (cudaStream_t as
+ * void*, NULL for the default stream) of the current device. ---- */
+
+/* Packs 3x3 weights [cout][cin][3][3] FP32 (PyTorch's OIHW) into the BF16
+ * shared-memory image the convolution reads: 9 * cin * cout BF16 values.
+ * mode 0: the layer's forward convolution; mode 1: its data-gradient
+ * convolution (kernel flipped, cin and cout exchanged).  Channel counts 16 or
+ * 32. */
+int hpm_net_pack_weights(const float *weights, int cout, int cin, int mode, void *packed, void *stream);
+
+/* 3x3 convolution, stride 1, zero padding 1, of an h x w NHWC BF16 image with
+ * cin channels into cout channels, on the tensor cores (tcgen05, FP32
+ * accumulation in TMEM).  epilogue 0: ReLU(acc + bias) as BF16; 1: acc + bias
+ * as FP32; 2: acc where aux (NHWC BF16, cout channels) is > 0, else 0, as BF16
+ * (the data gradient through the ReLU that produced aux).  use_tma selects
+ * TMA staging of the input halo (else thread loads).  err (device int, may be
+ * NULL) is set non-zero if a bounded wait ran out. */
+int hpm_net_conv3x3(const void *x, int h, int w, int cin, const void *packed, const float *bias, int cout,
+                    int epilogue, const void *aux, void *y, int use_tma, int *err, void *stream);
+
+/* Gradients of a 3x3 convolution layer: dw[cout][cin][3][3] += the weight
+ * gradient of input x (NHWC BF16, cin channels) and output gradient dy (NHWC
+ * BF16, cout channels), on the tensor cores (pixels as the reduction
+ * dimension, FP32 accumulation in TMEM); db[cout] += the bias gradient when
+ * db is non-NULL.  Both accumulate into the caller's FP32 buffers. */
+int hpm_net_conv_wgrad(const void *x, const void *dy, int h, int w, int cin, int cout, float *dw, float *db,
+                       int *err, void *stream);
 
 /* Fusion of a scene's maps into a coloured point cloud: RunFusion
  * (main.cpp:502-633).  View v has depth (h*w floats), world normal (3
@@ -277,9 +309,31 @@ int hpm_write_ply(const char *path, long long n, const float *xyz, const float *
  * negative status. */
 int hpm_delaunay(const int *xy, int n, int w, int h, int *tris, int cap);
 
+/* Triangle raster of the planar prior (main.cpp:96-116): n triangles (6 ints
+ * each, every vertex inside the w x h image) walked with the reference's
+ * barycentric steps; ids[y * w + x] = index + 1 of the last triangle that
+ * reaches the pixel, 0 where none does.  Host buffers; runs the raster kernel
+ * of hpm_process_problem on `device`. */
+int hpm_raster_triangles(int device, const int *tris, int n, int w, int h, int *ids);
+
+/* The 6 nearest of n support points (xy pairs inside the image) for every
+ * pixel whose mask is <= 0 (every pixel when mask is NULL), as the PCL
+ * kd-tree search of DepthsPredictSupplement (HPM.cpp:939-962) finds them:
+ * nn6[6 * (y * w + x) + k] = index of the k-th nearest by squared distance,
+ * ties to the lower index (PCL leaves tie order unspecified), -1 elsewhere.
+ * Host buffers; runs the kNN search of hpm_process_problem on `device`. */
+int hpm_knn6(int device, const int *xy, int n, int w, int h, const float *mask, int *nn6);
+
 /* ComputeMultiViewCostVector (HPM.cu:438-443) for one ref-frame plane per
  * pixel of the current problem; out holds (num_images-1) floats per pixel. */
 int hpm_cost_vectors(hpm_ctx *ctx, const float *planes, float *out);
+/* The 36 source-image samples the NCC window of ComputeBilateralNCC
+ * (HPM.cu:337-359) weighs, for n listed pixels (index y * w + x) and every
+ * source view: out [n][S][36] floats, inside [n][S] = 0 where the warped
+ * centre leaves the source image (the NCC is then 2).  Planes as for
+ * hpm_cost_vectors.  Lets a parity check tell a tap that the texture unit
+ * rounded to another 1/256 step apart from every other difference. */
+int hpm_tap_samples(hpm_ctx *ctx, const float *planes, const int *pixels, int n, float *out, int *inside);
 /* ComputeMultiViewInitialCostandSelectedViews (HPM.cu:399-436) per pixel. */
 int hpm_initial_costs(hpm_ctx *ctx, const float *planes, float *out_cost, uint32_t *out_views);
 /* ComputeGeomConsistencyCost (HPM.cu:483-508) per pixel and source view,

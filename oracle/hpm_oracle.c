@@ -1356,6 +1356,22 @@ static void knn6_grid(const KnnGrid *g, const int *pts, int x, int y, int *best)
     }
 }
 
+/* The 6 nearest of n_pts points for every pixel whose mask is <= 0 (every
+ * pixel without a mask), by brute force; -1 elsewhere and past n_pts. */
+void or_knn6(const int *pts, int n_pts, int w, int h, const float *mask, int *nn6)
+{
+#ifdef _OPENMP
+#pragma omp parallel for schedule(dynamic, 4)
+#endif
+    for (int y = 0; y < h; ++y)
+        for (int x = 0; x < w; ++x) {
+            int *o = nn6 + 6 * ((size_t)y * w + x);
+            for (int k = 0; k < 6; ++k) o[k] = -1;
+            if (mask && mask[(size_t)y * w + x] > 0) continue;
+            knn6_brute(pts, n_pts, x, y, o);
+        }
+}
+
 static int g_knn_grid = 1;
 
 void or_set_knn_grid(int on) { g_knn_grid = on; }
@@ -1630,4 +1646,297 @@ long or_fuse(int n_views, const OrCamera *cams, const float *const *depths, cons
     for (int v = 0; v < n_views; ++v) free(masks[v]);
     free(masks);
     return n_out;
+}
+
+/* ------------------------------------------------------------------ */
+/* NCC error bound: what an FP32 evaluation of ComputeBilateralNCC may  */
+/* differ by, tap coordinates being rounded differently                 */
+/* ------------------------------------------------------------------ */
+
+/* Value with a first-order bound on the rounding error that an FP32
+ * evaluation of the same expression accumulates: each add or multiply may
+ * round by one unit in the last place (2^-23 relative covers it), each
+ * divide by two (fast-math division), and errors of the operands propagate.
+ * The value itself is computed in double precision. */
+typedef struct {
+    double v, e;
+} EV;
+
+#define EV_EPS (1.0 / 8388608.0) /* 2^-23 */
+static EV ev(double v) { EV r = {v, 0.0}; return r; }
+static EV ev_add(EV a, EV b) { EV r = {a.v + b.v, 0}; r.e = a.e + b.e + EV_EPS * fabs(r.v); return r; }
+static EV ev_sub(EV a, EV b) { EV r = {a.v - b.v, 0}; r.e = a.e + b.e + EV_EPS * fabs(r.v); return r; }
+static EV ev_mul(EV a, EV b)
+{
+    EV r = {a.v * b.v, 0};
+    r.e = fabs(a.v) * b.e + fabs(b.v) * a.e + a.e * b.e + EV_EPS * fabs(r.v);
+    return r;
+}
+static EV ev_div(EV a, EV b)
+{
+    EV r = {a.v / b.v, 0};
+    const double den = fabs(b.v) - b.e;
+    r.e = den > 0 ? (a.e + fabs(r.v) * b.e) / den + 2.0 * EV_EPS * fabs(r.v) : INFINITY;
+    return r;
+}
+static EV ev_neg(EV a) { EV r = {-a.v, a.e}; return r; }
+
+/* ComputeHomography (HPM.cu:227-287), the same steps, with error bounds. */
+static void homography_e(const OrCamera *ref, const OrCamera *src, F4 hf, EV *H)
+{
+    EV rR[9], sR[9], rt[3], st[3], rK[9], sK[9];
+    for (int i = 0; i < 9; ++i) rR[i] = ev(ref->R[i]), sR[i] = ev(src->R[i]), rK[i] = ev(ref->K[i]), sK[i] = ev(src->K[i]);
+    for (int i = 0; i < 3; ++i) rt[i] = ev(ref->t[i]), st[i] = ev(src->t[i]);
+    const EV h[4] = {ev(hf.x), ev(hf.y), ev(hf.z), ev(hf.w)};
+    EV rC[3], sC[3], Rr[9], Cr[3], tr[3], tmp[9];
+    for (int i = 0; i < 3; ++i) {
+        rC[i] = ev_neg(ev_add(ev_add(ev_mul(rR[i], rt[0]), ev_mul(rR[3 + i], rt[1])), ev_mul(rR[6 + i], rt[2])));
+        sC[i] = ev_neg(ev_add(ev_add(ev_mul(sR[i], st[0]), ev_mul(sR[3 + i], st[1])), ev_mul(sR[6 + i], st[2])));
+    }
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j)
+            Rr[3 * i + j] = ev_add(ev_add(ev_mul(sR[3 * i], rR[j]), ev_mul(sR[3 * i + 1], rR[3 + j])),
+                                   ev_mul(sR[3 * i + 2], rR[6 + j]));
+    for (int i = 0; i < 3; ++i) Cr[i] = ev_sub(rC[i], sC[i]);
+    for (int i = 0; i < 3; ++i)
+        tr[i] = ev_add(ev_add(ev_mul(sR[3 * i], Cr[0]), ev_mul(sR[3 * i + 1], Cr[1])), ev_mul(sR[3 * i + 2], Cr[2]));
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) H[3 * i + j] = ev_sub(Rr[3 * i + j], ev_div(ev_mul(tr[i], h[j]), h[3]));
+    for (int i = 0; i < 3; ++i) {
+        tmp[3 * i + 0] = ev_div(H[3 * i + 0], rK[0]);
+        tmp[3 * i + 1] = ev_div(H[3 * i + 1], rK[4]);
+        tmp[3 * i + 2] = ev_add(ev_sub(ev_div(ev_mul(ev_neg(H[3 * i + 0]), rK[2]), rK[0]),
+                                       ev_div(ev_mul(H[3 * i + 1], rK[5]), rK[4])),
+                                H[3 * i + 2]);
+    }
+    H[0] = ev_add(ev_mul(sK[0], tmp[0]), ev_mul(sK[2], tmp[6]));
+    H[1] = ev_add(ev_mul(sK[0], tmp[1]), ev_mul(sK[2], tmp[7]));
+    H[2] = ev_add(ev_mul(sK[0], tmp[2]), ev_mul(sK[2], tmp[8]));
+    H[3] = ev_add(ev_mul(sK[4], tmp[3]), ev_mul(sK[5], tmp[6]));
+    H[4] = ev_add(ev_mul(sK[4], tmp[4]), ev_mul(sK[5], tmp[7]));
+    H[5] = ev_add(ev_mul(sK[4], tmp[5]), ev_mul(sK[5], tmp[8]));
+    H[6] = ev_mul(sK[8], tmp[6]);
+    H[7] = ev_mul(sK[8], tmp[7]);
+    H[8] = ev_mul(sK[8], tmp[8]);
+}
+
+/* ComputeCorrespondingPoint (HPM.cu:289-296) with error bounds. */
+static void warp_e(const EV *H, int px, int py, EV *u, EV *v)
+{
+    const EV x = ev(px), y = ev(py);
+    const EV a = ev_add(ev_add(ev_mul(H[0], x), ev_mul(H[1], y)), H[2]);
+    const EV b = ev_add(ev_add(ev_mul(H[3], x), ev_mul(H[4], y)), H[5]);
+    const EV z = ev_add(ev_add(ev_mul(H[6], x), ev_mul(H[7], y)), H[8]);
+    *u = ev_div(a, z);
+    *v = ev_div(b, z);
+}
+
+static double ulpf(float u)
+{
+    const float a = fabsf(u);
+    return (double)(nextafterf(a, INFINITY) - a);
+}
+
+/* Texture sample with the fixed-point coordinate of each axis moved by
+ * dq steps of 1/256 (the neighbouring rounding of the same coordinate). */
+static float tex2d_q(const float *img, int w, int h, float u, float v, int dqa, int dqb)
+{
+    int ia[2], A[2];
+    const float uv[2] = {u, v};
+    const int n[2] = {w, h}, dq[2] = {dqa, dqb};
+    int i0[2], i1[2];
+    for (int ax = 0; ax < 2; ++ax) {
+        double xb = (double)uv[ax] - 0.5;
+        if (xb != xb) xb = 0.0;
+        if (xb < -2.0) xb = -2.0;
+        if (xb > (double)n[ax] + 1.0) xb = (double)n[ax] + 1.0;
+        const double q = floor(xb * 256.0 + 0.5) + dq[ax];
+        const double i = floor(q / 256.0);
+        A[ax] = (int)(q - i * 256.0);
+        ia[ax] = (int)i;
+        i0[ax] = clampi(ia[ax], 0, n[ax] - 1);
+        i1[ax] = clampi(ia[ax] + 1, 0, n[ax] - 1);
+    }
+    const int w11 = (A[0] * A[1] + 128) >> 8;
+    const int w10 = A[0] - w11, w01 = A[1] - w11, w00 = 256 - A[0] - A[1] + w11;
+    const double t00 = img[(size_t)i0[1] * w + i0[0]], t10 = img[(size_t)i0[1] * w + i1[0]];
+    const double t01 = img[(size_t)i1[1] * w + i0[0]], t11 = img[(size_t)i1[1] * w + i1[0]];
+    return (float)((w00 * t00 + w10 * t10 + w01 * t01 + w11 * t11) / 256.0);
+}
+
+/* Distance (in 1/256 steps) of a coordinate's scaled value from the rounding
+ * boundary of the texture unit's 8-bit fraction, and the direction to the
+ * other rounding: A = floor(256 (u - 0.5) + 1/2). */
+static double step_margin(double u, int *dq)
+{
+    const double s = (u - 0.5) * 256.0 + 0.5;
+    const double f = s - floor(s); /* boundary at f = 0 (and 1) */
+    *dq = f < 0.5 ? -1 : 1;
+    return f < 0.5 ? f : 1.0 - f;
+}
+
+/* One NCC with its bound.  Returns the oracle's cost; *bound is the largest
+ * change that moving any subset of the taps whose coordinates lie within
+ * the coordinate tolerance of a 1/256 rounding step across that step can
+ * cause, to first order (sum of |d cost / d sample| x |sample change|), or 2
+ * when the centre lies within the tolerance of the image border or a
+ * variance cut lies within reach (either decision may then flip).
+ * Coordinate tolerance of a tap: k_err times the propagated rounding-error
+ * bound of its FP32 coordinate (homography_e, warp_e). */
+static float ncc_with_bound(const Ctx *c, int v, int px, int py, F4 h, float k_err, float *bound, float *acc,
+                            int *kind)
+{
+    *acc = 0.0f;
+    *kind = 0; /* bit 0: a tap near a weight step; bit 1: a decision may flip */
+    const OrCamera *ref = &c->cams[0], *src = &c->cams[v];
+    const float *rimg = c->imgs[0], *simg = c->imgs[v];
+    *bound = 0.0f;
+    float H[9];
+    EV He[9];
+    homography(ref, src, h, H);
+    homography_e(ref, src, h, He);
+    float cx, cy;
+    warp(H, px, py, &cx, &cy);
+    {
+        EV ue, ve;
+        warp_e(He, px, py, &ue, &ve);
+        const double cxd = ue.v, cyd = ve.v, tx = k_err * ue.e, ty = k_err * ve.e;
+        if (fabs(cxd) <= tx || fabs(cxd - src->width) <= tx || fabs(cyd) <= ty || fabs(cyd - src->height) <= ty) {
+            *bound = 2.0f;
+            *kind = 2;
+            return bilateral_ncc(c, v, px, py, h);
+        }
+    }
+    const float cost = bilateral_ncc(c, v, px, py, h);
+    if (cx >= (float)src->width || cx < 0.0f || cy >= (float)src->height || cy < 0.0f) return cost;
+    double w[36], r[36], s[36], ds[36];
+    const float rc = texel(rimg, ref->width, ref->height, px, py);
+    int t = 0;
+    for (int i = -5; i < 6; i += 2)
+        for (int j = -5; j < 6; j += 2, ++t) {
+            const int qx = px + i, qy = py + j;
+            const float rp = texel(rimg, ref->width, ref->height, qx, qy);
+            float sx, sy;
+            warp(H, qx, qy, &sx, &sy);
+            EV ue, ve;
+            warp_e(He, qx, qy, &ue, &ve);
+            const double sxd = ue.v, syd = ve.v;
+            const float u = sx + 0.5f, vv = sy + 0.5f;
+            const float sp = or_tex2d(simg, src->width, src->height, u, vv);
+            /* the + 0.5 rounds once more */
+            const double tx = k_err * (ue.e + EV_EPS * fabs(sxd + 0.5)), ty = k_err * (ve.e + EV_EPS * fabs(syd + 0.5));
+            int dqa = 0, dqb = 0;
+            const int near_a = step_margin(sxd + 0.5, &dqa) <= 256.0 * tx;
+            const int near_b = step_margin(syd + 0.5, &dqb) <= 256.0 * ty;
+            double d = 0.0;
+            if (near_a) d = fmax(d, fabs((double)tex2d_q(simg, src->width, src->height, u, vv, dqa, 0) - sp));
+            if (near_b) d = fmax(d, fabs((double)tex2d_q(simg, src->width, src->height, u, vv, 0, dqb) - sp));
+            if (near_a && near_b)
+                d = fmax(d, fabs((double)tex2d_q(simg, src->width, src->height, u, vv, dqa, dqb) - sp));
+            /* the oracle's own rounding may sit on either side: include the
+             * current rounding's neighbours in both directions */
+            if (near_a) d = fmax(d, fabs((double)tex2d_q(simg, src->width, src->height, u, vv, -dqa, 0) - sp));
+            if (near_b) d = fmax(d, fabs((double)tex2d_q(simg, src->width, src->height, u, vv, 0, -dqb) - sp));
+            const double sdist = sqrt((double)(i * i + j * j));
+            w[t] = exp(-sdist / 50.0 - fabs((double)rp - rc) / 18.0);
+            r[t] = rp;
+            s[t] = sp;
+            ds[t] = d;
+            if (d > 0.0) *kind |= 1;
+        }
+    double W = 0, mr = 0, mrr = 0, ms = 0, mss = 0, mrs = 0;
+    for (t = 0; t < 36; ++t) {
+        W += w[t];
+        mr += w[t] * r[t];
+        mrr += w[t] * r[t] * r[t];
+        ms += w[t] * s[t];
+        mss += w[t] * s[t] * s[t];
+        mrs += w[t] * r[t] * s[t];
+    }
+    mr /= W, mrr /= W, ms /= W, mss /= W, mrs /= W;
+    const double var_r = mrr - mr * mr, var_s = mss - ms * ms;
+    if (fabs(var_r - 1e-5) <= 1e-8 || fabs(var_s - 1e-5) <= 1e-8 + 1e-3 * 1e-5) {
+        *bound = 2.0f;
+        *kind |= 2;
+        return cost;
+    }
+    if (var_r < 1e-5 || var_s < 1e-5) {
+        /* a sample change can still lift var_s over the cut */
+        double dv = 0;
+        for (t = 0; t < 36; ++t) dv += w[t] / W * (2 * fabs(s[t] - ms) + ds[t]) * ds[t];
+        if (var_r >= 1e-5 && var_s + dv >= 1e-5) *bound = 2.0f, *kind |= 2;
+        return cost;
+    }
+    const double covar = mrs - mr * ms, vv = sqrt(var_r * var_s);
+    /* FP32 accumulation: each weighted sum is 36 terms of at most three
+     * rounded factors, added as 6 rows of 6 and scaled by 1/W, so it lies
+     * within g = 16 units of 2^-24 of its exact value (all terms positive);
+     * the variances and the covariance then cancel, most of all in flat
+     * windows.  Any two FP32 evaluations lie within twice this of each other. */
+    const double u = 1.0 / 16777216.0, g = 16.0 * u;
+    const double e_var_r = g * mrr + 2.0 * mr * g * mr + u * (mrr + mr * mr);
+    const double e_var_s = g * mss + 2.0 * ms * g * ms + u * (mss + ms * ms);
+    const double e_cov = g * mrs + mr * g * ms + ms * g * mr + u * (mrs + mr * ms);
+    const double e_c = e_cov / vv + fabs(covar) / vv * (0.5 * (e_var_r / var_r + e_var_s / var_s) + u) + u;
+    *acc = (float)(2.0 * e_c);
+    double b = 0, dvar_tot = 0;
+    for (t = 0; t < 36; ++t) {
+        if (ds[t] == 0.0) continue;
+        const double dvar = w[t] / W * 2.0 * (s[t] - ms);
+        const double dcov = w[t] / W * (r[t] - mr);
+        const double dvv = var_r * dvar / (2.0 * vv);
+        b += fabs((dcov * vv - covar * dvv) / (vv * vv)) * ds[t];
+        dvar_tot += (fabs(dvar) + w[t] / W * ds[t]) * ds[t];
+    }
+    if (var_s - dvar_tot < 1e-5) b = 2.0, *kind |= 2; /* the variance cut itself is within reach */
+    *bound = (float)b;
+    return cost;
+}
+
+int or_ncc_bounds_px(int n_img, const float *const *imgs, const OrCamera *cams, const float *planes4, float k_err,
+                     const int *pixels, int n_pixels, float *out_cost, float *out_bound, float *out_acc, int *out_kind)
+{
+    Ctx c;
+    memset(&c, 0, sizeof(c));
+    c.n = n_img;
+    c.imgs = imgs;
+    c.cams = cams;
+    c.W = cams[0].width;
+    c.H = cams[0].height;
+    const F4 *pl = (const F4 *)planes4;
+#ifdef _OPENMP
+#pragma omp parallel for schedule(dynamic, 16)
+#endif
+    for (int k = 0; k < n_pixels; ++k) {
+        const int x = pixels[k] % c.W, y = pixels[k] / c.W;
+        for (int v = 1; v < n_img; ++v) {
+            const size_t o = (size_t)k * (n_img - 1) + v - 1;
+            out_cost[o] = ncc_with_bound(&c, v, x, y, pl[pixels[k]], k_err, &out_bound[o], &out_acc[o], &out_kind[o]);
+        }
+    }
+    return 0;
+}
+
+int or_ncc_bounds(int n_img, const float *const *imgs, const OrCamera *cams, const float *planes4, float k_err,
+                  float *out_cost, float *out_bound, float *out_acc, int *out_kind)
+{
+    Ctx c;
+    memset(&c, 0, sizeof(c));
+    c.n = n_img;
+    c.imgs = imgs;
+    c.cams = cams;
+    c.W = cams[0].width;
+    c.H = cams[0].height;
+    const F4 *pl = (const F4 *)planes4;
+#ifdef _OPENMP
+#pragma omp parallel for schedule(dynamic, 4)
+#endif
+    for (int y = 0; y < c.H; ++y)
+        for (int x = 0; x < c.W; ++x)
+            for (int v = 1; v < n_img; ++v) {
+                const size_t o = ((size_t)y * c.W + x) * (n_img - 1) + v - 1;
+                out_cost[o] = ncc_with_bound(&c, v, x, y, pl[y * c.W + x], k_err, &out_bound[o], &out_acc[o],
+                                             &out_kind[o]);
+            }
+    return 0;
 }

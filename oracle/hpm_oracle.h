@@ -59,6 +59,19 @@ float or_tex2d(const float *img, int w, int h, float u, float v);
 void or_homography(const OrCamera *ref, const OrCamera *src, const float *plane4, float *H9);
 
 int or_cost_vectors(int n_img, const float *const *imgs, const OrCamera *cams, const float *planes4, float *out);
+/* The cost vectors of or_cost_vectors and, per value, what an FP32
+ * evaluation may differ by.  out_bound: the first-order effect of moving the
+ * taps whose coordinates lie within k_err x their propagated rounding-error
+ * bound of a 1/256 texture-weight step across it, or 2 where the centre's
+ * in-image test or a variance cut may flip.  out_acc: twice the first-order
+ * bound of the FP32 accumulation error of the window sums (large in flat
+ * windows, where the variances cancel).  out_kind: bit 0 a tap lies near a
+ * weight step, bit 1 a decision may flip. */
+int or_ncc_bounds(int n_img, const float *const *imgs, const OrCamera *cams, const float *planes4, float k_err,
+                  float *out_cost, float *out_bound, float *out_acc, int *out_kind);
+/* The same at n_pixels listed pixels (index y * W + x): outputs [n_pixels][S]. */
+int or_ncc_bounds_px(int n_img, const float *const *imgs, const OrCamera *cams, const float *planes4, float k_err,
+                     const int *pixels, int n_pixels, float *out_cost, float *out_bound, float *out_acc, int *out_kind);
 int or_initial_costs(int n_img, const float *const *imgs, const OrCamera *cams, const float *planes4,
                      float *out_cost, uint32_t *out_views);
 int or_geom_costs(int n_img, const OrCamera *cams, const float *const *depths, const float *planes4, float *out);
@@ -97,6 +110,9 @@ float or_depth_from_plane(const OrCamera *ref, const float *plane4, int x, int y
  * triangle, later triangles overwriting earlier ones; returns the number of
  * kept triangles and stores their vertex triples in kept6. */
 int or_raster_triangles(const int *tris6, int n_tris, int w, int h, float *mask, int *kept6);
+/* 6 nearest points per pixel (mask <= 0, or every pixel), brute force,
+ * ties to the lower index: nn6[6 * (y * w + x) + k], -1 elsewhere. */
+void or_knn6(const int *pts, int n_pts, int w, int h, const float *mask, int *nn6);
 
 /* DepthsPredictSupplement (HPM.cpp:923-1097) with exact K=6 nearest
  * neighbours, ties to the lower support-point index (the reference uses PCL

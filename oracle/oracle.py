@@ -120,6 +120,35 @@ def cost_vectors(images, cams, planes) -> np.ndarray:
     return out
 
 
+def ncc_bounds(images, cams, planes, k_err=1.0, pixels=None):
+    """Cost vectors with per-value bounds (or_ncc_bounds): (cost, bound,
+    acc, kind).  bound: what rounding the tap coordinates differently (up to
+    k_err x their propagated first-order error bound) can change, 2 where a
+    decision may flip; acc: twice the FP32 accumulation-error bound of the
+    window sums; kind: bit 0 a tap near a texture-weight step, bit 1 a
+    decision may flip.  pixels: flat indices y*W+x to evaluate only those
+    (outputs [len(pixels)][S])."""
+    imgs, arr = _img_ptrs(images)
+    c = _cams(cams)
+    h, w = imgs[0].shape
+    planes = np.ascontiguousarray(planes, dtype=np.float32)
+    if pixels is not None:
+        px = np.ascontiguousarray(pixels, dtype=np.int32)
+        shp = (len(px), len(imgs) - 1)
+        cost, bound, acc = (np.zeros(shp, np.float32) for _ in range(3))
+        kind = np.zeros(shp, np.int32)
+        lib().or_ncc_bounds_px(len(imgs), arr, _p(c), _p(planes), ctypes.c_float(k_err), _p(px), len(px), _p(cost),
+                               _p(bound), _p(acc), _p(kind))
+        return cost, bound, acc, kind
+    cost = np.zeros((h, w, len(imgs) - 1), np.float32)
+    bound = np.zeros_like(cost)
+    acc = np.zeros_like(cost)
+    kind = np.zeros(cost.shape, np.int32)
+    lib().or_ncc_bounds(len(imgs), arr, _p(c), _p(planes), ctypes.c_float(k_err), _p(cost), _p(bound), _p(acc),
+                        _p(kind))
+    return cost, bound, acc, kind
+
+
 def initial_costs(images, cams, planes):
     imgs, arr = _img_ptrs(images)
     c = _cams(cams)
@@ -222,6 +251,15 @@ def raster_triangles(tris, w, h, mask=None):
     kept = np.zeros_like(t)
     n = lib().or_raster_triangles(_p(t), len(t), w, h, _p(mask), _p(kept))
     return mask, kept[:n].copy()
+
+
+def knn6(pts, w, h, mask=None):
+    """(h, w, 6) indices of the 6 nearest points per pixel (brute force)."""
+    pts = np.ascontiguousarray(pts, dtype=np.int32).reshape(-1, 2)
+    out = np.zeros((h, w, 6), np.int32)
+    m = None if mask is None else np.ascontiguousarray(mask, dtype=np.float32)
+    lib().or_knn6(_p(pts), len(pts), w, h, None if m is None else _p(m), _p(out))
+    return out
 
 
 def knn_supplement(ref_cam, pts, depth, factor, dmin, dmax, mask):
@@ -348,6 +386,22 @@ def ref_geom_costs(cams, depth_maps, planes) -> np.ndarray:
     return out
 
 
+def ref_tap_samples(images, cams, planes, pixels):
+    """The reference's 36 source-texture samples per (listed pixel, source
+    view) of ComputeBilateralNCC, and whether the warped centre is inside."""
+    imgs, arr = _img_ptrs(images)
+    c = _cams(cams)
+    planes = np.ascontiguousarray(planes, dtype=np.float32)
+    px = np.ascontiguousarray(pixels, dtype=np.int32)
+    S = len(imgs) - 1
+    out = np.zeros((len(px), S, 36), np.float32)
+    inside = np.zeros((len(px), S), np.int32)
+    rc = ref().hpm_ref_tap_samples(len(imgs), arr, _p(c), _p(planes), _p(px), len(px), _p(out), _p(inside))
+    if rc != 0:
+        raise RuntimeError(f"hpm_ref_tap_samples: cuda error {rc}")
+    return out, inside.astype(bool)
+
+
 def ref_homography(ref_cam, src_cam, planes) -> np.ndarray:
     r = _cams(np.array([ref_cam], dtype=CAMERA_DTYPE))
     s = _cams(np.array([src_cam], dtype=CAMERA_DTYPE))
@@ -395,7 +449,10 @@ def ref_jbu(guide, coarse_depth, coarse_normal):
 
 
 def ref_run_patchmatch(images, cams, *, depth_min, depth_max, seed=0, geom=False, prior=False, multi_geometry=False,
-                       planes=None, costs=None, prior_planes=None, masks=None, depth_maps=None):
+                       planes=None, costs=None, prior_planes=None, masks=None, depth_maps=None, timed=False):
+    """HPM::RunPatchMatch of the reference (shim).  timed=True launches the
+    same kernels with CUDA events around each and also returns their times
+    (ms): init, the six half-steps, GetDepthandNormal, the two filters."""
     imgs, arr = _img_ptrs(images)
     c = _cams(cams)
     h, w = imgs[0].shape
@@ -407,8 +464,16 @@ def ref_run_patchmatch(images, cams, *, depth_min, depth_max, seed=0, geom=False
     pp = None if prior_planes is None else np.ascontiguousarray(prior_planes, dtype=np.float32)
     mk = None if masks is None else np.ascontiguousarray(masks, dtype=np.uint32)
     dms, darr = (None, None) if depth_maps is None else _img_ptrs(depth_maps)
-    rc = ref().hpm_ref_run_patchmatch(len(imgs), arr, _p(c), ctypes.byref(o), _p(planes), _p(costs),
-                                      None if pp is None else _p(pp), None if mk is None else _p(mk), darr)
+    args = (len(imgs), arr, _p(c), ctypes.byref(o), _p(planes), _p(costs), None if pp is None else _p(pp),
+            None if mk is None else _p(mk), darr)
+    if timed:
+        ms = np.zeros(10, np.float32)
+        rc = ref().hpm_ref_run_patchmatch_timed(*args, _p(ms))
+    else:
+        rc = ref().hpm_ref_run_patchmatch(*args)
     if rc != 0:
         raise RuntimeError(f"hpm_ref_run_patchmatch: cuda error {rc}")
+    if timed:
+        return planes, costs, {"init": float(ms[0]), "half_steps": [float(x) for x in ms[1:7]],
+                               "depth_normal": float(ms[7]), "filter": [float(ms[8]), float(ms[9])]}
     return planes, costs

@@ -168,6 +168,31 @@ __global__ void k_tex_fetch(cudaTextureObject_t t, const float2 *coords, int n, 
     out[i] = tex2D<float>(t, coords[i].x, coords[i].y);
 }
 
+/* The 36 source-texture samples of ComputeBilateralNCC (HPM.cu:337-359) for
+ * listed pixels and every source view, with the reference's own
+ * ComputeHomography and ComputeCorrespondingPoint; inside[k] = 0 where the
+ * warped centre leaves the source image (the NCC is then 2). */
+__global__ void k_tap_samples(cudaTextureObjects *tex, Camera *cams, const float4 *planes, const int *pixels, int n,
+                              int num_images, float *out, int *inside)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    const int S = num_images - 1;
+    if (k >= n * S) return;
+    const int pi = k / S, v = k % S + 1;
+    const int w = cams[0].width;
+    const int2 p = make_int2(pixels[pi] % w, pixels[pi] / w);
+    float H[9];
+    ComputeHomography(cams[0], cams[v], planes[pixels[pi]], H);
+    const float2 pt = ComputeCorrespondingPoint(H, p);
+    inside[k] = !(pt.x >= cams[v].width || pt.x < 0.0f || pt.y >= cams[v].height || pt.y < 0.0f);
+    int t = 0;
+    for (int i = -5; i < 6; i += 2)
+        for (int j = -5; j < 6; j += 2, ++t) {
+            const float2 src_pt = ComputeCorrespondingPoint(H, make_int2(p.x + i, p.y + j));
+            out[(size_t)k * 36 + t] = tex2D<float>(tex[0].images[v], src_pt.x + 0.5f, src_pt.y + 0.5f);
+        }
+}
+
 int status(cudaError_t e)
 {
     if (e == cudaSuccess && hpm_ref_first_error != cudaSuccess) e = hpm_ref_first_error;
@@ -193,12 +218,77 @@ typedef struct {
 int hpm_ref_sizeof_camera(void) { return (int)sizeof(Camera); }
 int hpm_ref_sizeof_params(void) { return (int)sizeof(PatchMatchParams); }
 
-/* One HPM::RunPatchMatch (HPM.cu:1906-1957) on a fresh problem.  planes_io /
- * costs_io seed the hypothesis state (the reference keeps that state on the
- * device between passes of one HPM object); on return they hold the result. */
-int hpm_ref_run_patchmatch(int num_images, const float *const *images, const Camera *cams, const HpmRefRunOpts *o,
-                           float *planes_io, float *costs_io, const float *prior_planes,
-                           const unsigned int *plane_masks, const float *const *depth_maps)
+}  // extern "C"
+
+namespace {
+
+/* HPM::RunPatchMatch (HPM.cu:1906-1957) with a CUDA event pair around each of
+ * its launches: the same grids, kernels and arguments, in the same order,
+ * with the reference's synchronisation after each.  ms_out gets 10 kernel
+ * times: RandomInitialization, the 6 Black/RedPixelUpdate half-steps,
+ * GetDepthandNormal, BlackPixelFilter, RedPixelFilter. */
+cudaError_t run_patchmatch_timed(HPM &hpm, float *ms_out)
+{
+    const int width = hpm.cameras[0].width, height = hpm.cameras[0].height;
+    const dim3 gi((width + 15) / 16, (height + 15) / 16), bi(16, 16);
+    const dim3 gc((width + 31) / 32, ((height / 2) + 15) / 16), bc(32, 16);
+    cudaEvent_t ev[20];
+    for (auto &e : ev) cudaEventCreate(&e);
+    int k = 0;
+    cudaEventRecord(ev[2 * k]);
+    RandomInitialization<<<gi, bi>>>(hpm.texture_objects_cuda, hpm.cameras_cuda, hpm.plane_hypotheses_cuda,
+                                     hpm.costs_cuda, hpm.rand_states_cuda, hpm.selected_views_cuda,
+                                     hpm.prior_planes_cuda, hpm.plane_masks_cuda, hpm.params);
+    cudaEventRecord(ev[2 * k + 1]);
+    cudaDeviceSynchronize();
+    ++k;
+    for (int i = 0; i < 3; ++i) {
+        for (int color = 0; color < 2; ++color) {
+            cudaEventRecord(ev[2 * k]);
+            if (color == 0)
+                BlackPixelUpdate<<<gc, bc>>>(hpm.texture_objects_cuda, hpm.texture_depths_cuda, hpm.cameras_cuda,
+                                             hpm.plane_hypotheses_cuda, hpm.costs_cuda, hpm.rand_states_cuda,
+                                             hpm.selected_views_cuda, hpm.prior_planes_cuda, hpm.plane_masks_cuda,
+                                             hpm.params, i);
+            else
+                RedPixelUpdate<<<gc, bc>>>(hpm.texture_objects_cuda, hpm.texture_depths_cuda, hpm.cameras_cuda,
+                                           hpm.plane_hypotheses_cuda, hpm.costs_cuda, hpm.rand_states_cuda,
+                                           hpm.selected_views_cuda, hpm.prior_planes_cuda, hpm.plane_masks_cuda,
+                                           hpm.params, i);
+            cudaEventRecord(ev[2 * k + 1]);
+            cudaDeviceSynchronize();
+            ++k;
+        }
+    }
+    cudaEventRecord(ev[2 * k]);
+    GetDepthandNormal<<<gi, bi>>>(hpm.cameras_cuda, hpm.plane_hypotheses_cuda, hpm.params);
+    cudaEventRecord(ev[2 * k + 1]);
+    cudaDeviceSynchronize();
+    ++k;
+    cudaEventRecord(ev[2 * k]);
+    BlackPixelFilter<<<gc, bc>>>(hpm.cameras_cuda, hpm.plane_hypotheses_cuda, hpm.costs_cuda);
+    cudaEventRecord(ev[2 * k + 1]);
+    cudaDeviceSynchronize();
+    ++k;
+    cudaEventRecord(ev[2 * k]);
+    RedPixelFilter<<<gc, bc>>>(hpm.cameras_cuda, hpm.plane_hypotheses_cuda, hpm.costs_cuda);
+    cudaEventRecord(ev[2 * k + 1]);
+    cudaError_t e = cudaDeviceSynchronize();
+    ++k;
+    for (int j = 0; j < k; ++j) cudaEventElapsedTime(&ms_out[j], ev[2 * j], ev[2 * j + 1]);
+    for (auto &x : ev) cudaEventDestroy(x);
+    if (e == cudaSuccess) e = cudaGetLastError();
+    if (e == cudaSuccess)
+        e = cudaMemcpy(hpm.plane_hypotheses_host, hpm.plane_hypotheses_cuda, sizeof(float4) * width * height,
+                       cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess)
+        e = cudaMemcpy(hpm.costs_host, hpm.costs_cuda, sizeof(float) * width * height, cudaMemcpyDeviceToHost);
+    return e;
+}
+
+int run_patchmatch_impl(int num_images, const float *const *images, const Camera *cams, const HpmRefRunOpts *o,
+                        float *planes_io, float *costs_io, const float *prior_planes, const unsigned int *plane_masks,
+                        const float *const *depth_maps, float *ms_out)
 {
     Problem pr;
     cudaError_t e = pr.init(num_images, images, cams, o->geom_consistency ? depth_maps : nullptr);
@@ -237,7 +327,9 @@ int hpm_ref_run_patchmatch(int num_images, const float *const *images, const Cam
         e = cudaMemcpy(hpm.prior_planes_cuda, prior_planes, sizeof(float4) * npx, cudaMemcpyHostToDevice);
     if (e == cudaSuccess && plane_masks)
         e = cudaMemcpy(hpm.plane_masks_cuda, plane_masks, sizeof(unsigned int) * npx, cudaMemcpyHostToDevice);
-    if (e == cudaSuccess) {
+    if (e == cudaSuccess && ms_out) {
+        e = run_patchmatch_timed(hpm, ms_out);
+    } else if (e == cudaSuccess) {
         hpm.RunPatchMatch();
         e = cudaDeviceSynchronize();
     }
@@ -253,6 +345,62 @@ int hpm_ref_run_patchmatch(int num_images, const float *const *images, const Cam
     cudaFree(hpm.plane_masks_cuda);
     delete[] hpm.plane_hypotheses_host;
     delete[] hpm.costs_host;
+    return status(e);
+}
+
+}  // namespace
+
+extern "C" {
+
+/* One HPM::RunPatchMatch (HPM.cu:1906-1957) on a fresh problem.  planes_io /
+ * costs_io seed the hypothesis state (the reference keeps that state on the
+ * device between passes of one HPM object); on return they hold the result. */
+int hpm_ref_run_patchmatch(int num_images, const float *const *images, const Camera *cams, const HpmRefRunOpts *o,
+                           float *planes_io, float *costs_io, const float *prior_planes,
+                           const unsigned int *plane_masks, const float *const *depth_maps)
+{
+    return run_patchmatch_impl(num_images, images, cams, o, planes_io, costs_io, prior_planes, plane_masks,
+                               depth_maps, nullptr);
+}
+
+/* The same pass with each kernel timed by CUDA events (ms_out: 10 floats,
+ * see run_patchmatch_timed). */
+int hpm_ref_run_patchmatch_timed(int num_images, const float *const *images, const Camera *cams,
+                                 const HpmRefRunOpts *o, float *planes_io, float *costs_io, const float *prior_planes,
+                                 const unsigned int *plane_masks, const float *const *depth_maps, float *ms_out)
+{
+    return run_patchmatch_impl(num_images, images, cams, o, planes_io, costs_io, prior_planes, plane_masks,
+                               depth_maps, ms_out);
+}
+
+/* Tap samples of listed pixels (k_tap_samples): out [n][S][36], inside [n][S]. */
+int hpm_ref_tap_samples(int num_images, const float *const *images, const Camera *cams, const float *planes,
+                        const int *pixels, int n, float *out, int *inside)
+{
+    Problem pr;
+    cudaError_t e = pr.init(num_images, images, cams, nullptr);
+    if (e != cudaSuccess) return status(e);
+    const size_t npx = (size_t)cams[0].width * cams[0].height;
+    const int S = num_images - 1;
+    float4 *d_planes = nullptr;
+    int *d_pix = nullptr, *d_in = nullptr;
+    float *d_out = nullptr;
+    e = cudaMalloc(&d_planes, sizeof(float4) * npx);
+    if (e == cudaSuccess) e = cudaMalloc(&d_pix, sizeof(int) * n);
+    if (e == cudaSuccess) e = cudaMalloc(&d_in, sizeof(int) * (size_t)n * S);
+    if (e == cudaSuccess) e = cudaMalloc(&d_out, sizeof(float) * (size_t)n * S * 36);
+    if (e == cudaSuccess) e = cudaMemcpy(d_planes, planes, sizeof(float4) * npx, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(d_pix, pixels, sizeof(int) * n, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) {
+        k_tap_samples<<<(n * S + 127) / 128, 128>>>(pr.tex_d, pr.cams_d, d_planes, d_pix, n, num_images, d_out, d_in);
+        e = cudaDeviceSynchronize();
+    }
+    if (e == cudaSuccess) e = cudaMemcpy(out, d_out, sizeof(float) * (size_t)n * S * 36, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(inside, d_in, sizeof(int) * (size_t)n * S, cudaMemcpyDeviceToHost);
+    cudaFree(d_planes);
+    cudaFree(d_pix);
+    cudaFree(d_in);
+    cudaFree(d_out);
     return status(e);
 }
 

@@ -14,13 +14,23 @@ outputs for small seeded inputs:
   pm.npz          whole RunPatchMatch passes (plain; geometric) for the
                   statistical comparison (the reference's RNG is curand
                   XORWOW, so only statistics are comparable)
+  cfg1_640x480.npz, cfg2_800x600_s10.npz
+                  the same deterministic pieces at the bench's own sizes:
+                  config 1 (5 views of 640x480, 4 sources) and an 11-view
+                  scene of config 2's recipe at 800x600 (10 sources, the
+                  middle level of the bench's pyramid).  The scenes are
+                  rebuilt from their seeds by the tests (a SHA-256 of the
+                  images guards the generator); outputs are kept at 4096
+                  sampled pixels, plus the reference's whole-pass accuracy
+                  and kernel times over four seeds.
 
 Usage (on a GPU machine, from the repository root):
-    python tests/golden/make_golden.py [--out tests/golden]
+    python tests/golden/make_golden.py [--out tests/golden] [--only small|bench]
 """
 from __future__ import annotations
 
 import argparse
+import hashlib
 import os
 import sys
 
@@ -41,6 +51,7 @@ def small_scene(seed=0):
 
 def test_planes(sc, ref, rng):
     gt = syn.gt_planes_ref_frame(sc, ref)
+    H, W = gt.shape[:2]
     pert = gt.copy()
     pert[..., 3] *= rng.uniform(0.97, 1.03, pert.shape[:2]).astype(np.float32)
     # random planes facing the camera at random depths
@@ -98,13 +109,97 @@ def tex_probe():
     return out
 
 
+# the bench-size cases: scene recipe, reference view, seed of the inputs
+BENCH_CASES = {
+    "cfg1_640x480": dict(scene=dict(seed=11, width=640, height=480, n_views=5, n_planes=6, low_texture=0.25), ref=2,
+                         seed=501),
+    "cfg2_800x600_s10": dict(scene=dict(seed=12, width=800, height=600, n_views=11, n_planes=20, n_spheres=5,
+                                        low_texture=0.40), ref=5, seed=502),
+}
+N_SAMPLES = 4096
+STAT_SEEDS = (100, 101, 102, 103)
+
+
+def images_sha256(imgs):
+    h = hashlib.sha256()
+    for i in imgs:
+        h.update(np.ascontiguousarray(i, dtype=np.uint8).tobytes())
+    return h.hexdigest()
+
+
+def bench_case_inputs(name):
+    """Every input of a bench-size case, rebuilt deterministically from the
+    case's seeds: the scene, the problem's images and cameras, three plane
+    fields (true, perturbed, random), the geometric depth maps, the JBU
+    coarse inputs, the filter's costs and the sampled pixels."""
+    case = BENCH_CASES[name]
+    kw = dict(case["scene"])
+    sc = syn.make_scene(kw.pop("seed"), kw.pop("width"), kw.pop("height"), kw.pop("n_views"), **kw)
+    ref = case["ref"]
+    imgs, cams = syn.view_set(sc, ref)
+    rng = np.random.default_rng(case["seed"])
+    planes = test_planes(sc, ref, rng)
+    ids = [ref] + list(sc.pairs[ref][1])
+    depths = [np.where(rng.random(sc.gt_depth[i].shape) < 0.05, 0.0, sc.gt_depth[i]).astype(np.float32) for i in ids]
+    jbu = {}
+    for s in (2, 4):
+        cd = sc.gt_depth[ref][::s, ::s].copy()
+        cd[rng.random(cd.shape) < 0.1] = 0.0
+        jbu[s] = (cd, np.ascontiguousarray(sc.gt_normal[ref][::s, ::s]))
+    h, w = imgs[0].shape
+    costs = rng.uniform(0, 1, (h, w)).astype(np.float32)
+    costs[rng.random((h, w)) < 0.1] = 0.0
+    pixels = np.sort(rng.choice(h * w, N_SAMPLES, replace=False)).astype(np.int32)
+    return dict(sc=sc, ref=ref, imgs=imgs, cams=cams, planes=planes, depths=depths, jbu=jbu, costs=costs,
+                pixels=pixels)
+
+
+def bench_cases(out_dir):
+    for name in BENCH_CASES:
+        c = bench_case_inputs(name)
+        imgs, cams, planes, px = c["imgs"], c["cams"], c["planes"], c["pixels"]
+        sc, ref = c["sc"], c["ref"]
+        h, w = imgs[0].shape
+        S = len(imgs) - 1
+        flat = lambda a: a.reshape(h * w, *a.shape[2:])[px]  # noqa: E731
+        out = dict(images_sha256=images_sha256(imgs), planes_sha256=hashlib.sha256(planes.tobytes()).hexdigest(),
+                   pixels=px, planes=np.stack([flat(p) for p in planes]))
+        out["cost_vectors"] = np.stack([flat(orc.ref_cost_vectors(imgs, cams, p)) for p in planes])
+        ic = [orc.ref_initial_costs(imgs, cams, p) for p in planes]
+        out["init_cost"] = np.stack([flat(a) for a, _ in ic])
+        out["init_views"] = np.stack([flat(v) for _, v in ic])
+        out["geom_costs"] = np.stack([flat(orc.ref_geom_costs(cams, c["depths"], p)) for p in planes])
+        for s, (cd, cn) in c["jbu"].items():
+            od, on = orc.ref_jbu(imgs[0], cd, cn)
+            out[f"jbu_depth_{s}"] = flat(od)
+            out[f"jbu_normal_{s}"] = flat(on)
+        out["filter"] = flat(orc.ref_depth_normal_filter(cams[0], planes[1], c["costs"]))
+        dmin, dmax = sc.depth_min * 0.6, sc.depth_max * 1.2
+        acc, nerr, times = [], [], []
+        for seed in STAT_SEEDS:
+            pl, _, t = orc.ref_run_patchmatch(imgs, cams, depth_min=dmin, depth_max=dmax, seed=seed, timed=True)
+            acc.append(syn.depth_accuracy(pl[..., 3], sc.gt_depth[ref]))
+            nerr.append(syn.normal_error_deg(pl[..., :3], sc.gt_normal[ref], sc.gt_depth[ref]))
+            times.append([t["init"]] + t["half_steps"] + [t["depth_normal"]] + t["filter"])
+        out.update(pass_accuracy=np.array(acc), pass_normal_err_deg=np.array(nerr),
+                   pass_kernel_ms=np.array(times, np.float32), sources=S)
+        np.savez_compressed(os.path.join(out_dir, f"{name}.npz"), **out)
+        print(name, "reference pass accuracy", np.round(acc, 4), "normal err", np.round(nerr, 2),
+              "half-step ms", np.round(np.mean(np.array(times)[:, 1:7]), 3))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", default=os.path.join(ROOT, "tests", "golden"))
+    ap.add_argument("--only", choices=["small", "bench"], default=None)
     args = ap.parse_args()
     os.makedirs(args.out, exist_ok=True)
     if not orc.ref_available():
         raise SystemExit("oracle/_ref/libhpm_ref.so is missing: build it with `make -C oracle ref`")
+    if args.only != "small":
+        bench_cases(args.out)
+    if args.only == "bench":
+        return
     rng = np.random.default_rng(1234)
 
     np.savez_compressed(os.path.join(args.out, "tex_probe.npz"), **tex_probe())

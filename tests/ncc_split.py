@@ -1,0 +1,63 @@
+"""Splitting a difference between two GPU evaluations of ComputeBilateralNCC
+(HPM.cu:325-397) into its two causes.
+
+Both evaluations report the 36 source samples of each window (the product's
+hpm_tap_samples, the reference shim's hpm_ref_tap_samples).  Where the
+texture unit rounded a tap coordinate of one of them to another 1/256 step,
+the samples differ; the exact effect of that is the float64 NCC of one
+side's samples minus the float64 NCC of the other's.  What remains,
+
+    residual = (cost_a - cost_b) - (ncc64(samples_a) - ncc64(samples_b)),
+
+is the FP32 evaluation of the same samples, which the tests hold to 1e-4
+relative with no exceptions.
+"""
+import numpy as np
+
+OFFS = np.array([(i, j) for i in range(-5, 6, 2) for j in range(-5, 6, 2)])  # tap order (i outer, j inner)
+
+
+def ref_window(ref_img, pixels):
+    """Reference-window pixels (n, 36) and bilateral weights (n, 36) in
+    float64, with the reference's clamped integer texel reads."""
+    h, w = ref_img.shape
+    px, py = pixels % w, pixels // w
+    xs = np.clip(px[:, None] + OFFS[None, :, 0], 0, w - 1)
+    ys = np.clip(py[:, None] + OFFS[None, :, 1], 0, h - 1)
+    r = ref_img[ys, xs].astype(np.float64)
+    rc = ref_img[py, px].astype(np.float64)[:, None]
+    sd = np.sqrt((OFFS ** 2).sum(-1)).astype(np.float64)[None, :]
+    wgt = np.exp(-sd / (2 * 5.0 ** 2) - np.abs(r - rc) / (2 * 3.0 ** 2))
+    return r, wgt
+
+
+def ncc64(r, wgt, s):
+    """NCC cost in float64 of samples s (n, S, 36) against windows (n, 36)."""
+    W = wgt.sum(-1)[:, None]
+    wn = (wgt / W)[:, None, :]
+    rr = r[:, None, :]
+    mr, mrr = (wn * rr).sum(-1), (wn * rr * rr).sum(-1)
+    ms, mss, mrs = (wn * s).sum(-1), (wn * s * s).sum(-1), (wn * rr * s).sum(-1)
+    var_r, var_s = mrr - mr * mr, mss - ms * ms
+    cov = mrs - mr * ms
+    with np.errstate(invalid="ignore", divide="ignore"):
+        c = 1.0 - cov / np.sqrt(var_r * var_s)
+    c = np.clip(c, 0.0, 2.0)
+    return np.where((var_r < 1e-5) | (var_s < 1e-5), 2.0, c)
+
+
+def split(cost_a, cost_b, samples_a, samples_b, inside_a, inside_b, ref_img, pixels):
+    """(crossed, effect, residual) per (pixel, view): crossed where any tap
+    sample differs; effect = exact change those samples cause; residual =
+    the rest of cost_a - cost_b.  Where one side has the centre outside and
+    the other inside, crossed is True and effect takes the whole difference."""
+    r, wgt = ref_window(ref_img, pixels)
+    sa, sb = samples_a.astype(np.float64), samples_b.astype(np.float64)
+    d = cost_a.astype(np.float64) - cost_b.astype(np.float64)
+    both_in = inside_a & inside_b
+    crossed = (samples_a != samples_b).any(-1) & both_in
+    effect = np.where(crossed, ncc64(r, wgt, sa) - ncc64(r, wgt, sb), 0.0)
+    flip = inside_a != inside_b
+    effect = np.where(flip, d, effect)
+    crossed = crossed | flip
+    return crossed, effect, d - effect
