@@ -554,20 +554,35 @@ def run_reference(args, dist):
             d, n, c, _ = geom(v, 1000 + i, gi, src, n, c)
             src = dict(depth_g) if gi == 0 else src
             src[v] = d
-        return v, d
+        return v, d, n
+
+    # the reference's kernels one by one (untimed region): a plain
+    # RunPatchMatch of view 0 at the workload's size with CUDA events around
+    # each of its launches (the shim's timed copy of HPM.cu:1906-1957)
+    ids0, imgs0, cams0 = problem(0)
+    cam0 = cams0[0]
+    quiet(lambda: orc.ref_run_patchmatch(imgs0, cams0, depth_min=cam0["depth_min"] * 0.6,
+                                         depth_max=cam0["depth_max"] * 1.2, seed=5, timed=True))
+    _, _, kt = quiet(lambda: orc.ref_run_patchmatch(imgs0, cams0, depth_min=cam0["depth_min"] * 0.6,
+                                                   depth_max=cam0["depth_max"] * 1.2, seed=6, timed=True))
+    kernel_ms = {"init": kt["init"], "half_step_mean": float(np.mean(kt["half_steps"])),
+                 "half_steps": kt["half_steps"], "depth_normal": kt["depth_normal"], "filters": kt["filter"],
+                 "what": f"one plain RunPatchMatch of view 0 ({W}x{H}, {len(ids0) - 1} sources), the reference's "
+                         "kernels timed one by one with CUDA events"}
 
     # warm-up on the last views, timed steps from view 0 on (their accuracy
     # compares with the per-view figures of the product's line)
     for i in range(args.warmup):
         quiet(lambda: step(nv - 1 - i % nv))
     torch.cuda.synchronize()
-    done = {}
+    done, done_n = {}, {}
     with Clocks(dist.local) as clk:
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
         for i in range(args.steps):
-            v, d = quiet(lambda: step(i))
+            v, d, n = quiet(lambda: step(i))
             done[v] = d
+            done_n[v] = n
         e1.record()
         e1.synchronize()
     ms = e0.elapsed_time(e1)
@@ -585,7 +600,8 @@ def run_reference(args, dist):
         "config": {"workload": workload_name(), "width": W, "height": H, "views": nv, "sources": nv - 1,
                    "step": "the reference's per-view flow (main.cpp:35-499 for pass set A, main.cpp:662-674 for the "
                            "geometric iterations) on one view"},
-        "accuracy": scene_accuracy(sc, done),
+        "accuracy": scene_accuracy(sc, done, done_n),
+        "reference_kernel_ms": kernel_ms,
         "clocks": clk.summary(),
         "impl": "reference",
         "cpu_baseline": {"value": value, "unit": "depth Mpix/s", "cores": int(os.environ["OMP_NUM_THREADS"]),

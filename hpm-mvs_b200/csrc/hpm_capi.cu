@@ -17,6 +17,8 @@
 #include <new>
 #include <vector>
 
+#include <cuda_bf16.h>
+
 #include "hpm_capi_internal.h"
 
 using namespace hpm;
@@ -129,6 +131,7 @@ PMArgs make_args(hpm_ctx *c)
     a.cand_costs = c->d_cand;
     a.cand_pos = c->d_pos;
     a.cand_flags = c->d_flags;
+    a.proposals = c->proposals;
     return a;
 }
 
@@ -216,6 +219,7 @@ int hpm_destroy(hpm_ctx *c)
     cudaFree(c->d_pos);
     cudaFree(c->d_flags);
     ws_free(c);
+    net_free(c);
     for (auto &p : c->prof_events) {
         cudaEventDestroy(p.second.first);
         cudaEventDestroy(p.second.second);
@@ -720,6 +724,7 @@ float *ctx_prior(hpm_ctx *c) { return reinterpret_cast<float *>(c->d_prior); }
 uint32_t *ctx_masks(hpm_ctx *c) { return c->d_masks; }
 const float *ctx_image(hpm_ctx *c, int i) { return c->d_img[i]; }
 void ctx_mark_prior(hpm_ctx *c) { c->has_prior = true; }
+void ctx_mark_state(hpm_ctx *c) { c->has_state = true; }
 
 template <typename T>
 static cudaError_t grow(T **p, size_t *cap, size_t n)
@@ -804,6 +809,52 @@ void ws_free(hpm_ctx *c)
                     w.c_packed, w.tris, w.tri_planes, w.pts, w.cell_start, w.cell_pts};
     for (void *p : ptrs) cudaFree(p);
     w = FlowWorkspace();
+}
+
+cudaError_t net_reserve(hpm_ctx *c, size_t coarse_px, size_t coarse_img_floats)
+{
+    NetWorkspace &w = c->net;
+    cudaError_t e = cudaSuccess;
+    if (!w.err) {
+        e = cudaMalloc((void **)&w.err, sizeof(int));
+        if (e == cudaSuccess) e = cudaMemset(w.err, 0, sizeof(int));
+        if (e != cudaSuccess) return e;
+    }
+    if (w.cimg_cap < coarse_img_floats || !w.cimg) e = grow(&w.cimg, &w.cimg_cap, coarse_img_floats);
+    if (e != cudaSuccess || (w.cap >= coarse_px && w.x0)) return e;
+    size_t a = 0, b = 0, d = 0, f = 0, g = 0;
+    __nv_bfloat16 *x0 = static_cast<__nv_bfloat16 *>(w.x0), *a0 = static_cast<__nv_bfloat16 *>(w.a[0]),
+                  *a1 = static_cast<__nv_bfloat16 *>(w.a[1]), *a2 = static_cast<__nv_bfloat16 *>(w.a[2]);
+    e = grow(&x0, &a, 16 * coarse_px);
+    if (e == cudaSuccess) e = grow(&a0, &b, 32 * coarse_px);
+    if (e == cudaSuccess) e = grow(&a1, &d, 32 * coarse_px);
+    if (e == cudaSuccess) e = grow(&a2, &f, 32 * coarse_px);
+    if (e == cudaSuccess) e = grow(&w.out, &g, 16 * coarse_px);
+    w.x0 = x0;
+    w.a[0] = a0;
+    w.a[1] = a1;
+    w.a[2] = a2;
+    if (e == cudaSuccess) e = grow(&w.prop, &w.cap, coarse_px);
+    return e;
+}
+
+cudaError_t net_reserve_full(hpm_ctx *c, size_t npx)
+{
+    NetWorkspace &w = c->net;
+    if (w.full_cap >= npx && w.up_depth) return cudaSuccess;
+    size_t a = 0, b = 0;
+    cudaError_t e = grow(&w.up_depth, &a, npx);
+    if (e == cudaSuccess) e = grow(&w.up_normal, &b, npx);
+    if (e == cudaSuccess) e = grow(&w.cand, &w.full_cap, npx);
+    return e;
+}
+
+void net_free(hpm_ctx *c)
+{
+    NetWorkspace &w = c->net;
+    void *ptrs[] = {w.x0, w.a[0], w.a[1], w.a[2], w.out, w.prop, w.cimg, w.up_depth, w.up_normal, w.cand, w.err};
+    for (void *p : ptrs) cudaFree(p);
+    w = NetWorkspace();
 }
 
 cudaError_t ctx_scene_arena(hpm_ctx *c, size_t bytes) { return ensure((void **)&c->d_scene, &c->scene_cap, bytes); }

@@ -41,6 +41,22 @@ struct FlowWorkspace {
     int last_points = 0, last_triangles = 0;
 };
 
+/* Device buffers of the prior-net form's coarse stage and network, grown on
+ * demand and reused by every problem of a context. */
+struct NetWorkspace {
+    void *x0 = nullptr;            /* network input, [coarse px][16] BF16 */
+    void *a[3] = {nullptr, nullptr, nullptr}; /* hidden activations, [coarse px][32] BF16 */
+    float *out = nullptr;          /* last layer, [coarse px][16] FP32 */
+    float4 *prop = nullptr;        /* head: world normal, depth per coarse pixel */
+    size_t cap = 0;
+    float *cimg = nullptr;         /* the problem's 1/4-scale images */
+    size_t cimg_cap = 0;
+    float *up_depth = nullptr;     /* upsampled proposal, full scale */
+    float4 *up_normal = nullptr, *cand = nullptr;
+    size_t full_cap = 0;
+    int *err = nullptr;            /* status of the tensor-core kernels */
+};
+
 }  // namespace hpm
 
 struct hpm_ctx {
@@ -91,6 +107,10 @@ struct hpm_ctx {
     uint32_t *d_flags = nullptr; /* valid-direction bits [H*W] */
     size_t flags_cap = 0;
 
+    /* prior-net form: the network's proposed plane per pixel (ref-frame
+     * normal, distance) for the next pass, or nullptr (plain form) */
+    const float4 *proposals = nullptr;
+    hpm::NetWorkspace net;
     hpm::FlowWorkspace flow;
     float *d_scene = nullptr; /* hpm_run_scene's per-view maps, grown on demand */
     size_t scene_cap = 0;
@@ -126,3 +146,19 @@ cudaError_t ws_reserve_grid(hpm_ctx *c, size_t npts, size_t ncells);
 cudaError_t ws_reserve_full(hpm_ctx *c, size_t npx);
 cudaError_t ws_reserve_coarse(hpm_ctx *c, size_t npx);
 void ws_free(hpm_ctx *c);
+/* hypotheses written on the device count as the pass state */
+void ctx_mark_state(hpm_ctx *c);
+cudaError_t net_reserve(hpm_ctx *c, size_t coarse_px, size_t coarse_img_floats);
+cudaError_t net_reserve_full(hpm_ctx *c, size_t npx);
+void net_free(hpm_ctx *c);
+
+namespace hpm {
+/* hpm_flow.cu helpers shared with the prior-net form */
+cudaError_t flow_split_state(const float4 *planes, int n, float *depth, float *normal3, cudaStream_t s);
+cudaError_t flow_pack4(const float *depth, const float *normal3, int n, float4 *out, cudaStream_t s);
+int flow_level_prior(hpm_ctx *c, const HpmCamera &cam, const float *d_cost, const float *d_depth, int w, int h,
+                     float factor, float dmin, float dmax);
+/* hpm_priornet.cu */
+int net_problem(hpm_ctx *c, int n, const float *const *images, const HpmCamera *cams, const HpmNetWeights *net,
+                uint64_t seed, float *depth_out, float *normal_out, float *cost_out);
+}  // namespace hpm

@@ -63,6 +63,18 @@ int grid1(int n) { return (n + 255) / 256; }
         if (e_ != cudaSuccess) return ctx_cuda_fail(c, e_, what); \
     } while (0)
 
+cudaError_t hpm::flow_split_state(const float4 *planes, int n, float *depth, float *normal3, cudaStream_t s)
+{
+    k_split_state<<<grid1(n), 256, 0, s>>>(planes, n, depth, normal3);
+    return cudaGetLastError();
+}
+
+cudaError_t hpm::flow_pack4(const float *depth, const float *normal3, int n, float4 *out, cudaStream_t s)
+{
+    k_pack4<<<grid1(n), 256, 0, s>>>(depth, normal3, n, out);
+    return cudaGetLastError();
+}
+
 /* Support points of a cost map in the reference's block order, the
  * triangulation, raster and plane fits, and the KNN supplement: leaves
  * ws.mask (reference mask values: triangle id, -233 for KNN, 0), ws.ids,
@@ -123,6 +135,12 @@ static int build_level_prior(hpm_ctx *c, const HpmCamera &cam, const float *d_co
  * scale; main.cpp:78-478) from the full-resolution maps in ws.full_depth,
  * ws.full_normal and d_cost: leaves the ref-frame prior planes and masks of
  * the next pass in the context (and, at full scale, the prior depth map). */
+int hpm::flow_level_prior(hpm_ctx *c, const HpmCamera &cam, const float *d_cost, const float *d_depth, int w, int h,
+                          float factor, float dmin, float dmax)
+{
+    return build_level_prior(c, cam, d_cost, d_depth, w, h, factor, dmin, dmax);
+}
+
 static int level_prior_from_maps(hpm_ctx *c, int i, const float *d_cost, float dmin, float dmax)
 {
     const HpmCamera cam = c->cams[0];
@@ -300,11 +318,39 @@ extern "C" int hpm_run_scene(hpm_ctx *c, int n_views, const float *const *images
                             out_normals, out_costs, nullptr, nullptr);
 }
 
+static int run_scene_impl(hpm_ctx *c, int n_views, const float *const *images, const HpmCamera *cams,
+                          int n_problems, const int *ref_ids, const int *src_counts, const int *src_ids,
+                          const HpmSceneOpts *o, const HpmNetWeights *net, float *const *out_depths,
+                          float *const *out_normals, float *const *out_costs, float *const *out_pass_depths,
+                          float *const *out_prior_depths);
+
 extern "C" int hpm_run_scene_ex(hpm_ctx *c, int n_views, const float *const *images, const HpmCamera *cams,
                                 int n_problems, const int *ref_ids, const int *src_counts, const int *src_ids,
                                 const HpmSceneOpts *o, float *const *out_depths, float *const *out_normals,
                                 float *const *out_costs, float *const *out_pass_depths,
                                 float *const *out_prior_depths)
+{
+    return run_scene_impl(c, n_views, images, cams, n_problems, ref_ids, src_counts, src_ids, o, nullptr, out_depths,
+                          out_normals, out_costs, out_pass_depths, out_prior_depths);
+}
+
+extern "C" int hpm_run_scene_net(hpm_ctx *c, int n_views, const float *const *images, const HpmCamera *cams,
+                                 int n_problems, const int *ref_ids, const int *src_counts, const int *src_ids,
+                                 const HpmSceneOpts *o, const HpmNetWeights *net, float *const *out_depths,
+                                 float *const *out_normals, float *const *out_costs)
+{
+    if (!net) return HPM_ERR_ARG;
+    for (int l = 0; l < 4; ++l)
+        if (!net->packed[l] || !net->bias[l]) return HPM_ERR_ARG;
+    return run_scene_impl(c, n_views, images, cams, n_problems, ref_ids, src_counts, src_ids, o, net, out_depths,
+                          out_normals, out_costs, nullptr, nullptr);
+}
+
+static int run_scene_impl(hpm_ctx *c, int n_views, const float *const *images, const HpmCamera *cams,
+                          int n_problems, const int *ref_ids, const int *src_counts, const int *src_ids,
+                          const HpmSceneOpts *o, const HpmNetWeights *net, float *const *out_depths,
+                          float *const *out_normals, float *const *out_costs, float *const *out_pass_depths,
+                          float *const *out_prior_depths)
 {
     if (!c || !images || !cams || !ref_ids || !src_counts || !src_ids || !o) return HPM_ERR_ARG;
     if (n_views < 2 || n_problems < 1) return ctx_fail(c, HPM_ERR_ARG, "hpm_run_scene: %d views, %d problems", n_views,
@@ -335,10 +381,8 @@ extern "C" int hpm_run_scene_ex(hpm_ctx *c, int n_views, const float *const *ima
         cur += 7 * st;
         CK(cudaMemcpyAsync(m.img[v], images[v], sizeof(float) * np, cudaMemcpyDefault, s), "scene images");
     }
-    /* the views of problem p on context cc */
-    auto load_problem = [&](hpm_ctx *cc, int p) -> int {
-        const float *pimg[kMaxViews];
-        HpmCamera pcam[kMaxViews];
+    /* the views of problem p */
+    auto gather = [&](int p, const float **pimg, HpmCamera *pcam) -> int {
         const int ref = ref_ids[p], ns = src_counts[p];
         pimg[0] = m.img[ref];
         pcam[0] = cams[ref];
@@ -347,7 +391,13 @@ extern "C" int hpm_run_scene_ex(hpm_ctx *c, int n_views, const float *const *ima
             pimg[j + 1] = m.img[sv];
             pcam[j + 1] = cams[sv];
         }
-        return hpm_set_views(cc, pimg, pcam, ns + 1);
+        return ns + 1;
+    };
+    auto load_problem = [&](hpm_ctx *cc, int p) -> int {
+        const float *pimg[kMaxViews];
+        HpmCamera pcam[kMaxViews];
+        const int n = gather(p, pimg, pcam);
+        return hpm_set_views(cc, pimg, pcam, n);
     };
     CK(cudaStreamSynchronize(s), "scene images");
     /* pass set A: ProcessProblem(geom = false, planar_prior) for every view.
@@ -355,7 +405,8 @@ extern "C" int hpm_run_scene_ex(hpm_ctx *c, int n_views, const float *const *ima
      * this context and its peer from two host threads that pass the GPU
      * token (see hpm_ctx::gpu_token). */
     {
-        const int workers = (c->scene_workers > 1 && n_problems > 1) ? 2 : 1;
+        /* the prior-net form triangulates only at the coarse scale: one worker */
+        const int workers = (c->scene_workers > 1 && n_problems > 1 && !net) ? 2 : 1;
         if (workers == 2 && !c->peer) {
             r = hpm_create(&c->peer, c->device);
             if (r) return ctx_fail(c, r, "hpm_run_scene: second context");
@@ -377,8 +428,23 @@ extern "C" int hpm_run_scene_ex(hpm_ctx *c, int n_views, const float *const *ima
                 const int p = next.fetch_add(1);
                 if (p >= n_problems) return;
                 std::unique_lock<std::mutex> hold(token);
-                int rr = load_problem(cc, p);
-                if (!rr) {
+                int rr;
+                if (net) {
+                    const float *pimg[kMaxViews];
+                    HpmCamera pcam[kMaxViews];
+                    const int n = gather(p, pimg, pcam), ref = ref_ids[p];
+                    rr = net_problem(cc, n, pimg, pcam, net, o->seed + (uint64_t)p, m.depth_a[ref], m.normal[ref],
+                                     m.cost[ref]);
+                    if (rr == HPM_OK && out_prior_depths && out_prior_depths[ref])
+                        rr = cudaMemsetAsync(out_prior_depths[ref], 0,
+                                             sizeof(float) * cams[ref].width * cams[ref].height, cc->stream) ==
+                                     cudaSuccess
+                                 ? HPM_OK
+                                 : HPM_ERR_CUDA;
+                } else {
+                    rr = load_problem(cc, p);
+                }
+                if (!rr && !net) {
                     HpmProblemOpts po = {o->planar_prior, 0, 0, o->seed + (uint64_t)p, o->pyramid_levels};
                     const int ref = ref_ids[p];
                     float *prior_out = out_prior_depths ? out_prior_depths[ref] : nullptr;

@@ -17,7 +17,7 @@ namespace hpm {
 constexpr int kMaxViews = HPM_MAX_IMAGES; /* reference + 32 sources */
 constexpr int kMaxSrc = kMaxViews - 1;
 constexpr int kTaps = 36; /* 6 x 6 taps of the 11x11 window, stride 2 */
-constexpr int kCandRows = 13;  /* 8 NESP directions + 5 refinement candidates */
+constexpr int kCandRows = 14;  /* 8 NESP directions + 5 refinement candidates + 1 network proposal */
 constexpr int kRefineRow = 8; /* first refinement row */
 
 /* Per-view data of one problem, passed to kernels by value. */
@@ -64,6 +64,9 @@ struct PMArgs {
     int *cand_pos;
     uint32_t *cand_flags;
     unsigned long long *counters; /* [2]: cost vectors, geom terms, or nullptr */
+    /* prior-net form: per pixel a proposed plane (ref-frame normal, distance),
+     * scored as one more refinement candidate; nullptr in the plain form */
+    const float4 *proposals;
 };
 
 /* Launchers (hpm_pm.cu / hpm_jbu.cu). All asynchronous on `s`. */

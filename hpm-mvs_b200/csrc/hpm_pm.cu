@@ -31,6 +31,7 @@
  *    host synchronisation (the reference synchronises after every launch).
  */
 #include <cfloat>
+#include <cstdlib>
 
 #include "hpm_internal.h"
 
@@ -391,6 +392,100 @@ __device__ __forceinline__ float ncc(const PMArgs &a, int v, int px, int py, flo
     const float covar = sum_ref_src - rs.mean * sum_src;
     const float vv = sqrtf(rs.var * var_src);
     return fmaxf(0.0f, fminf(2.0f, 1.0f - covar / vv));
+}
+
+/* The NCC of every active lane's own (pixel, plane) for source view v,
+ * computed cooperatively: groups of 6 lanes take one window at a time, each
+ * lane one tap column i of the 6 (ComputeBilateralNCC's outer loop,
+ * HPM.cu:347-377) with its 6 inner taps, so that a texture instruction of the
+ * warp samples 5 windows, 6 neighbouring taps each, instead of 32 windows
+ * that may lie far apart (a random-depth candidate's windows scatter along
+ * the epipolar lines).  The owner lane's homography and reference statistics
+ * reach its group by shuffles; the group adds its 6 column sums in the
+ * column order of the serial loop, so every cost equals ncc()'s bit for bit.
+ * sLane / sCost: 32 ints / floats of this warp's shared scratch. */
+template <typename Win>
+__device__ __forceinline__ float ncc_coop(const PMArgs &a, int v, int px, int py, float4 h, const Win *sWW, int tid,
+                                          const RefStats &rs, int *sLane, float *sCost)
+{
+    const unsigned mask = __activemask();
+    const int lane = threadIdx.x & 31;
+    const int rank = __popc(mask & ((1u << lane) - 1u));
+    const int A = __popc(mask), G = A / 6;
+    if (G == 0) return ncc(a, v, px, py, h, sWW, tid, rs);
+    const HpmCamera &sc = a.cam[v];
+    float H[9];
+    homography(a.cam[0], sc, a.pair[v], h, H);
+    const float2 pt = warp(H, (float)px, (float)py);
+    const bool live = !(pt.x >= sc.width || pt.x < 0.0f || pt.y >= sc.height || pt.y < 0.0f) && !(rs.var < 1e-5f);
+    sLane[rank] = lane;
+    __syncwarp(mask);
+    const cudaTextureObject_t tex = a.view[v].tex;
+    const int g = rank / 6, col = rank - 6 * g;
+    const int rounds = (A + G - 1) / G;
+    for (int r = 0; r < rounds; ++r) {
+        const int j = r * G + g;
+        const bool has_job = g < G && j < A;
+        const int owner = sLane[has_job ? j : 0];
+        const float ox = __shfl_sync(mask, (float)px, owner), oy = __shfl_sync(mask, (float)py, owner);
+        const int otid = __shfl_sync(mask, tid, owner);
+        const int olive = __shfl_sync(mask, live ? 1 : 0, owner);
+        float Ho[9];
+#pragma unroll
+        for (int k = 0; k < 9; ++k) Ho[k] = __shfl_sync(mask, H[k], owner);
+        float r_src = 0.0f, r_ss = 0.0f, r_rs = 0.0f;
+        if (has_job && olive) {
+            const int i = -5 + 2 * col;
+#pragma unroll
+            for (int jj = 0; jj < 6; ++jj) {
+                const float sp = tap_sample(tex, Ho, ox, oy, i, -5 + 2 * jj);
+                float2 ww;
+                if constexpr (sizeof(Win) == sizeof(float)) {
+                    const float wt = sWW[(col * 6 + jj) * kBlock + otid];
+                    ww = make_float2(wt, wt * texel(a.view[0].img, a.view[0].w, a.view[0].h, (int)ox + i,
+                                                    (int)oy - 5 + 2 * jj));
+                } else {
+                    ww = sWW[(col * 6 + jj) * kBlock + otid];
+                }
+                r_src += ww.x * sp;
+                r_ss += ww.x * sp * sp;
+                r_rs += ww.y * sp;
+            }
+        }
+        /* the column sums in column order, as the serial loop adds them */
+        float sum_src = 0.0f, sum_ss = 0.0f, sum_rs = 0.0f;
+#pragma unroll
+        for (int c = 0; c < 6; ++c) {
+            const int src_lane = sLane[has_job ? 6 * g + c : 0];
+            const float a0 = __shfl_sync(mask, r_src, src_lane);
+            const float a1 = __shfl_sync(mask, r_ss, src_lane);
+            const float a2 = __shfl_sync(mask, r_rs, src_lane);
+            sum_src += a0;
+            sum_ss += a1;
+            sum_rs += a2;
+        }
+        const float oinv = __shfl_sync(mask, rs.inv, owner), omean = __shfl_sync(mask, rs.mean, owner);
+        const float ovar = __shfl_sync(mask, rs.var, owner);
+        if (has_job && col == 0) {
+            float cost = 2.0f;
+            if (olive) {
+                sum_src *= oinv;
+                sum_ss *= oinv;
+                sum_rs *= oinv;
+                const float var_src = sum_ss - sum_src * sum_src;
+                if (!(var_src < 1e-5f)) {
+                    const float covar = sum_rs - omean * sum_src;
+                    const float vv = sqrtf(ovar * var_src);
+                    cost = fmaxf(0.0f, fminf(2.0f, 1.0f - covar / vv));
+                }
+            }
+            sCost[owner] = cost;
+        }
+    }
+    __syncwarp(mask);
+    const float c = sCost[lane];
+    __syncwarp(mask);
+    return c;
 }
 
 /* One NCC window for the loops that score several candidates view by view
@@ -810,11 +905,17 @@ __global__ void __launch_bounds__(kBlock, HPM_P1_MIN_BLOCKS) k_prop_dirs(const _
     a.cand_flags[center] = flags;
 }
 
-template <int SMAX>
+/* PROP: the prior-net form, whose network proposal a.proposals[center] is a
+ * sixth refinement candidate, scored by the same NCC (and prior terms) as the
+ * other five and accepted by the same rule.  It takes no random draws, so
+ * the random stream of the other candidates is unchanged. */
+template <int SMAX, bool PROP, bool COOP>
 __global__ void __launch_bounds__(kBlock, HPM_P2_MIN_BLOCKS) k_prop_refine(const __grid_constant__ PMArgs a, int iter,
                                                                             int color)
 {
     __shared__ WinPair sWW[kTaps * kBlock];
+    __shared__ int sLane[kBlockY][32];
+    __shared__ float sCost[kBlockY][32];
     const int tid = threadIdx.y * kBlockX + threadIdx.x;
     int px, py;
     half_step_pixel(color, px, py);
@@ -1065,23 +1166,50 @@ __global__ void __launch_bounds__(kBlock, HPM_P2_MIN_BLOCKS) k_prop_refine(const
          * across the warp (one source texture per texture instruction, one
          * source image at a time per block); each NCC value goes to the
          * candidate's hand-off row for the cache. */
-        float4 cand[5];
+        constexpr int NC = PROP ? 6 : 5;
+        float4 cand[NC];
+        float cand_depth[NC];
 #pragma unroll
         for (int i = 0; i < 5; ++i) {
             cand[i] = normals[i];
             cand[i].w = distance_to_origin(cam, px, py, depths[i], cand[i]);
+            cand_depth[i] = depths[i];
         }
-        float tc[5] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+        if constexpr (PROP) {
+            cand[5] = a.proposals[center];
+            cand_depth[5] = depth_from_plane(cam, cand[5], px, py);
+        }
+        float tc[NC];
+#pragma unroll
+        for (int i = 0; i < NC; ++i) tc[i] = 0.0f;
         for (int v = 0; v < S; ++v) {
             const bool selected = (tsv >> v) & 1u;
             const float w = (float)((v < 16 ? (vw_lo >> (4 * v)) : (vw_hi >> (4 * (v - 16)))) & 15ull);
+            if constexpr (COOP) {
+                /* candidates 0 and 2 (the random depth): their windows
+                 * scatter along the epipolar lines, so the warp scores them
+                 * together, window by window (ncc_coop) */
+#pragma unroll
+                for (int q = 0; q < 2; ++q) {
+                    const int i = 2 * q;
+                    const float c = ncc_coop(a, v + 1, px, py, cand[i], sWW, tid, rs, sLane[threadIdx.y],
+                                             sCost[threadIdx.y]);
+                    CAG(kRefineRow + i, v) = c;
+                    if (selected) {
+                        if (a.geom)
+                            tc[i] += w * (c + 0.1f * geom_cost(a, v + 1, cand[i], px, py));
+                        else
+                            tc[i] += w * c;
+                    }
+                }
+            }
 #pragma unroll 1
-            for (int k = 0; k < 5; ++k) {
+            for (int k = COOP ? 2 : 0; k < NC; ++k) {
                 /* candidates 0 and 2 share the random depth, hence the window
                  * centre in every source view; 1, 3 and 4 sit at or near the
                  * current depth: scoring 0, 2, 1, 3, 4 keeps windows with the
                  * same centre back to back in the texture cache */
-                const int i = (0x43120 >> (4 * k)) & 15;
+                const int i = (0x543120 >> (4 * k)) & 15;
                 const float c = ncc_call(a, v + 1, px, py, cand[i], sWW, tid, rs);
                 CAG(kRefineRow + i, v) = c;
                 if (selected) {
@@ -1092,14 +1220,14 @@ __global__ void __launch_bounds__(kBlock, HPM_P2_MIN_BLOCKS) k_prop_refine(const
                 }
             }
         }
-        if (a.counters) atomicAdd(&a.counters[0], (unsigned long long)(5 * S));
+        if (a.counters) atomicAdd(&a.counters[0], (unsigned long long)(NC * S));
 #pragma unroll
-        for (int i = 0; i < 5; ++i) {
+        for (int i = 0; i < NC; ++i) {
             const float tci = tc[i] / wn;
             const float depth_before = depth_from_plane(cam, cand[i], px, py);
             bool take;
             if (use_prior) {
-                const float dd = depths[i] - depth_prior;
+                const float dd = cand_depth[i] - depth_prior;
                 const float pr = restricted_prior(dd, dot3(pp, cand[i]), two_dss, two_ass);
                 const float rtc = expf(-tci * tci / beta) * pr;
                 take = depth_before >= a.dmin && depth_before <= a.dmax && rtc > restricted_cost;
@@ -1237,12 +1365,35 @@ __global__ void k_tap_samples(const __grid_constant__ PMArgs a, const float4 *pl
         for (int j = -5; j < 6; j += 2, ++t) out[(size_t)k * kTaps + t] = tap_sample(a.view[v].tex, H, fpx, fpy, i, j);
 }
 
+/* Cooperative scoring of the random-depth refinement candidates (ncc_coop);
+ * HPM_REFINE_COOP=0 in the environment selects the one-window-per-lane loop
+ * (same results) for comparison. */
+bool refine_coop()
+{
+    static const bool on = [] {
+        const char *e = getenv("HPM_REFINE_COOP");
+        return !(e && e[0] == '0');
+    }();
+    return on;
+}
+
 template <int SMAX>
 cudaError_t launch_prop_t(const PMArgs &a, int iter, int color, cudaStream_t s)
 {
     dim3 grid((a.W + 2 * kWarpW - 1) / (2 * kWarpW), (a.rows_cov + 2 * kWarpH - 1) / (2 * kWarpH));
     k_prop_dirs<<<grid, dim3(kBlockX, kBlockY), 0, s>>>(a, iter, color);
-    k_prop_refine<SMAX><<<grid, dim3(kBlockX, kBlockY), 0, s>>>(a, iter, color);
+    const dim3 b(kBlockX, kBlockY);
+    if (refine_coop()) {
+        if (a.proposals)
+            k_prop_refine<SMAX, true, true><<<grid, b, 0, s>>>(a, iter, color);
+        else
+            k_prop_refine<SMAX, false, true><<<grid, b, 0, s>>>(a, iter, color);
+    } else {
+        if (a.proposals)
+            k_prop_refine<SMAX, true, false><<<grid, b, 0, s>>>(a, iter, color);
+        else
+            k_prop_refine<SMAX, false, false><<<grid, b, 0, s>>>(a, iter, color);
+    }
     return cudaGetLastError();
 }
 

@@ -40,13 +40,18 @@ EXPORTED = [
     "hpm_prior_level", "hpm_run_scene", "hpm_run_scene_ex", "hpm_read_gray8", "hpm_resize_linear",
     "hpm_fuse", "hpm_write_ply", "hpm_read_bgr8", "hpm_set_scene_workers", "hpm_resize_linear_u8",
     "hpm_raster_triangles", "hpm_knn6", "hpm_tap_samples", "hpm_net_pack_weights", "hpm_net_conv3x3",
-    "hpm_net_conv_wgrad",
+    "hpm_net_conv_wgrad", "hpm_run_scene_net", "hpm_net_coarse_inputs", "hpm_net_targets", "hpm_net_loss",
+    "hpm_net_adam",
 ]
 
 
 class HpmSceneOpts(ctypes.Structure):
     _fields_ = [("planar_prior", ctypes.c_int), ("geom_iterations", ctypes.c_int), ("seed", ctypes.c_uint64),
                 ("pyramid_levels", ctypes.c_int)]
+
+
+class HpmNetWeights(ctypes.Structure):
+    _fields_ = [("packed", ctypes.c_void_p * 4), ("bias", ctypes.c_void_p * 4)]
 
 
 class HpmProblemOpts(ctypes.Structure):
@@ -234,14 +239,16 @@ class Context:
         return depth, normal, cost, prior
 
     def run_scene(self, images, cams, pairs, *, planar_prior=True, geom_iterations=2, seed=0, pyramid_levels=-1,
-                  images_are_device=False, outputs=True, extra_maps=False):
+                  images_are_device=False, outputs=True, extra_maps=False, net=None):
         """The reference's main() over a scene.  images: per-view float32 [H, W]
         arrays, or device pointers (ints) with images_are_device; pairs:
         [(ref, [sources])].  outputs: True to return new per-view (depth,
         normal, cost) lists, False for none (the maps stay on the device), or
         a tuple of three caller-owned lists of float32 arrays to fill.
         extra_maps (with outputs=True): also return each view's pass-set-A
-        depth and prior depth (hpm_run_scene_ex), five lists in all."""
+        depth and prior depth (hpm_run_scene_ex), five lists in all.
+        net: an HpmNetWeights (priornet.Net.weights()) to run the prior-net
+        form (hpm_run_scene_net) instead of the plain form."""
         n = len(cams)
         cams = np.ascontiguousarray(cams, dtype=CAMERA_DTYPE)
         if images_are_device:
@@ -274,7 +281,13 @@ class Context:
             arrs = [(ctypes.c_void_p * n)(*[o_[k].ctypes.data for o_ in outs]) for k in range(3)]
         else:
             arrs = [None, None, None]
-        if extra_maps:
+        if net is not None:
+            if extra_maps:
+                raise ValueError("run_scene: extra_maps is not available in the prior-net form")
+            self._check(lib().hpm_run_scene_net(self._h, n, img_arr, _p(cams), len(pairs), _p(refs), _p(counts),
+                                                _p(srcs), ctypes.byref(o), ctypes.byref(net), arrs[0], arrs[1],
+                                                arrs[2]), "hpm_run_scene_net")
+        elif extra_maps:
             if outputs is not True:
                 raise ValueError("run_scene: extra_maps needs outputs=True")
             extra = [[np.empty((int(c["height"]), int(c["width"])), np.float32) for c in cams] for _ in range(2)]

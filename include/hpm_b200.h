@@ -271,6 +271,55 @@ int hpm_net_pack_weights(const float *weights, int cout, int cin, int mode, void
 int hpm_net_conv3x3(const void *x, int h, int w, int cin, const void *packed, const float *bias, int cout,
                     int epilogue, const void *aux, void *y, int use_tma, int *err, void *stream);
 
+/* Trained weights of the proposal network, device pointers: per layer the
+ * packed BF16 weights (hpm_net_pack_weights, mode 0) and the FP32 bias.
+ * Layers: 16->32, 32->32, 32->32 (ReLU), 32->16 (linear head). */
+typedef struct {
+    const void *packed[4];
+    const float *bias[4];
+} HpmNetWeights;
+
+/* hpm_run_scene_ex in the prior-net form.  Pass set A of each problem is: a
+ * plain pass on 1/4-scale views, the coarse planar prior, the network's plane
+ * per coarse pixel (from the coarse image, the pass's depth, normal and
+ * confidence, and the prior's depth), then ONE full-scale prior pass whose
+ * initial hypothesis is the network's proposal (upsampled by JBU) and whose
+ * refinement scores the proposal as a sixth candidate with the unchanged NCC
+ * cost; the planar prior is the coarse one, upsampled as the plain form's
+ * coarsest level.  The geometric iterations are the plain form's.
+ * opts->pyramid_levels is not used. */
+int hpm_run_scene_net(hpm_ctx *ctx, int n_views, const float *const *images, const HpmCamera *cams, int n_problems,
+                      const int *ref_ids, const int *src_counts, const int *src_ids, const HpmSceneOpts *opts,
+                      const HpmNetWeights *net, float *const *out_depths, float *const *out_normals,
+                      float *const *out_costs);
+
+/* The network's input for one problem (views as for hpm_set_views, full
+ * scale): the coarse stage of the prior-net form (1/4-scale plain pass with
+ * seed, coarse planar prior), written to x0 ([*ch][*cw][16] BF16, host or
+ * device, at most cap_px pixels).  Leaves the coarse problem in the context. */
+int hpm_net_coarse_inputs(hpm_ctx *ctx, int num_images, const float *const *images, const HpmCamera *cams,
+                          uint64_t seed, void *x0, size_t cap_px, int *cw, int *ch);
+
+/* Training targets of a view for the network, at the coarse size cw x ch:
+ * the view's final depth and world normal (device), kept where the
+ * multi-view test of RunFusion (main.cpp:575-612, without its
+ * order-dependent masking) passes against the sources' maps (device
+ * pointers); out: depth, reference-frame normal (3 floats) and mask per
+ * coarse pixel (device). */
+int hpm_net_targets(int device, const HpmCamera *ref_cam, const float *depth, const float *normal, int n_sources,
+                    const HpmCamera *src_cams, const float *const *src_depths, const float *const *src_normals, int cw,
+                    int ch, float *t_depth, float *t_normal, uint8_t *t_mask, void *stream);
+
+/* Training loss of the head on n pixels (device buffers): masked relative
+ * depth error plus lambda (1 - cos) of the normal; dy gets the output
+ * gradient (BF16, 16 channels) times inv_count, *loss the loss sum. */
+int hpm_net_loss(const float *out16, const float *t_depth, const float *t_normal, const uint8_t *t_mask, int n,
+                 float dmin, float dmax, float lambda, float inv_count, void *dy, float *loss, void *stream);
+
+/* One Adam step on n FP32 parameters (device); clears the gradients. */
+int hpm_net_adam(float *params, float *grads, float *m, float *v, int n, float lr, float beta1, float beta2, float eps,
+                 int step, void *stream);
+
 /* Gradients of a 3x3 convolution layer: dw[cout][cin][3][3] += the weight
  * gradient of input x (NHWC BF16, cin channels) and output gradient dy (NHWC
  * BF16, cout channels), on the tensor cores (pixels as the reduction

@@ -275,6 +275,31 @@ def test_view_sharded_driver_on_the_gpu():
         np.testing.assert_array_equal(all_depth[v].cpu().numpy(), cur[v])
 
 
+def test_view_sharded_iterations_keep_the_accuracy():
+    """Sharding a scene's views over ranks makes the geometric iterations read
+    the previous iteration's maps of every view (Jacobi order); one rank
+    (hpm_run_scene) reads maps already updated in place, as the reference does
+    (Gauss-Seidel order).  The two orders reach the same accuracy within 1.5
+    percentage points of pixels with relative depth error < 1 %, averaged over
+    the views of a 6-view scene and two seeds."""
+    import scene_dist
+
+    nv, w, h = 6, 320, 240
+    sc = syn.make_scene(31, w, h, nv, n_planes=8, n_spheres=2, low_texture=0.4)
+    imgs = [i.astype(np.float32) for i in sc.images]
+    pairs = [(v, list(sc.pairs[v][1])) for v in range(nv)]
+    shapes = {v: (h, w) for v in range(nv)}
+    acc_gs, acc_j = [], []
+    for seed in (3, 4):
+        with hb.Context() as ctx:
+            d, _, _ = ctx.run_scene(imgs, sc.cams, pairs, seed=seed, pyramid_levels=1)
+            acc_gs.append(np.mean([syn.depth_accuracy(d[v], sc.gt_depth[v]) for v in range(nv)]))
+            solver = scene_dist.GpuSolver(ctx, imgs, sc.cams, pairs, seed=seed, pyramid_levels=1)
+            mine, _ = scene_dist.run_scene_sharded(solver, pairs, shapes, geom_iterations=2)
+            acc_j.append(np.mean([syn.depth_accuracy(mine[v][0].cpu().numpy(), sc.gt_depth[v]) for v in range(nv)]))
+    assert abs(np.mean(acc_gs) - np.mean(acc_j)) <= 0.015, (acc_gs, acc_j)
+
+
 def test_scene_workers_give_the_same_maps():
     """Pass set A on one or on two contexts (hpm_set_scene_workers): the
     problems are independent and each draws from its own seed, so the maps

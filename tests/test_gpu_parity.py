@@ -122,6 +122,30 @@ def test_half_steps_agree_with_oracle(half_steps, sizes):
     assert (gv[same] == ov[same]).mean() >= 0.99
 
 
+@pytest.mark.parametrize("sources", [4, 5, 10, 16, 32])
+def test_half_steps_agree_with_oracle_for_every_refinement_width(sources):
+    """Every instantiation of the refinement kernel (k_prop_refine<4>, <8>,
+    <12>, <16>, <32> for 4, 5, 10, 16 and 32 sources) against the oracle,
+    pixel by pixel, after two iterations (four half-steps)."""
+    step = {4: 8.0, 5: 6.0, 10: 3.0, 16: 2.0, 32: 1.0}[sources]
+    sc = syn.make_scene(20 + sources, 112, 84, sources + 1, n_planes=6, n_spheres=1, arc_step_deg=step)
+    ref = (sources + 1) // 2
+    imgs, cams = syn.view_set(sc, ref)
+    dmin, dmax = sc.depth_min * 0.6, sc.depth_max * 1.2
+    op, oc, ov = orc.run_patchmatch(imgs, cams, depth_min=dmin, depth_max=dmax, seed=17, salt=0, half_steps=4,
+                                    finalize=False)
+    with hb.Context() as ctx:
+        ctx.set_views(imgs, cams)
+        ctx.run_partial(hb.default_params(dmin, dmax, seed=17), 4, False)
+        gp, gc = ctx.get_result()
+        gv = ctx.get_selected_views()
+    same = np.isclose(gp, op, rtol=1e-4, atol=1e-6).all(-1)
+    assert same.mean() >= 0.93, same.mean()
+    close = np.isclose(gc[same], oc[same], rtol=1e-3, atol=1e-3, equal_nan=True)
+    assert close.mean() >= 0.99, close.mean()
+    assert (gv[same] == ov[same]).mean() >= 0.98
+
+
 def test_full_pass_agrees_with_oracle_statistics():
     sc, imgs, cams, dmin, dmax = _scene(4, 160, 120, 5)
     gt, gn = sc.gt_depth[2], sc.gt_normal[2]
@@ -272,3 +296,37 @@ def test_max_sources():
     with hb.Context() as ctx, pytest.raises(hb.HpmError, match="ARG"):
         sc34 = syn.make_scene(9, 16, 12, 34, n_planes=1, arc_step_deg=1.0)
         ctx.set_views([i.astype(np.float32) for i in sc34.images], sc34.cams)
+
+
+_COOP_SCRIPT = r"""
+import sys, numpy as np
+sys.path[:0] = sys.argv[1:3]
+import hpm_b200 as hb, synthetic as syn
+sc = syn.make_scene(13, 200, 150, 11, n_planes=8, n_spheres=2, arc_step_deg=3.0)
+imgs, cams = syn.view_set(sc, 5)
+dmin, dmax = sc.depth_min * 0.6, sc.depth_max * 1.2
+with hb.Context() as ctx:
+    ctx.set_views(imgs, cams)
+    ctx.run_partial(hb.default_params(dmin, dmax, seed=9), 4, False)
+    p, c = ctx.get_result()
+np.savez(sys.argv[3], planes=p, costs=c)
+"""
+
+
+def test_cooperative_refinement_is_bit_identical(tmp_path):
+    """The random-depth refinement candidates scored warp-cooperatively
+    (default) and one window per lane (HPM_REFINE_COOP=0) give the same
+    bits after four half-steps at 10 sources (k_prop_refine<12>)."""
+    import subprocess
+    import sys
+
+    from conftest import ORACLE, PKG
+
+    outs = {}
+    for m in ("0", "1"):
+        path = tmp_path / f"coop{m}.npz"
+        env = dict(os.environ, HPM_REFINE_COOP=m)
+        subprocess.run([sys.executable, "-c", _COOP_SCRIPT, PKG, ORACLE, str(path)], check=True, env=env)
+        outs[m] = np.load(path)
+    np.testing.assert_array_equal(outs["1"]["planes"], outs["0"]["planes"])
+    np.testing.assert_array_equal(outs["1"]["costs"], outs["0"]["costs"])
