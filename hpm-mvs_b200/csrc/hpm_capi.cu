@@ -197,6 +197,8 @@ int hpm_destroy(hpm_ctx *c)
     if (!c) return HPM_ERR_ARG;
     if (c->peer) hpm_destroy(c->peer);
     c->peer = nullptr;
+    if (c->coarse) hpm_destroy(c->coarse);
+    c->coarse = nullptr;
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
     for (int i = 0; i < kMaxViews; ++i) {

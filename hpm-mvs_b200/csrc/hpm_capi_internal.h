@@ -111,6 +111,9 @@ struct hpm_ctx {
      * normal, distance) for the next pass, or nullptr (plain form) */
     const float4 *proposals = nullptr;
     hpm::NetWorkspace net;
+    /* prior-net form: the context that holds a problem's 1/4-scale views,
+     * so that this one keeps its full-scale views and texture arrays */
+    hpm_ctx *coarse = nullptr;
     hpm::FlowWorkspace flow;
     float *d_scene = nullptr; /* hpm_run_scene's per-view maps, grown on demand */
     size_t scene_cap = 0;

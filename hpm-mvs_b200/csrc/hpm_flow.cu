@@ -405,8 +405,7 @@ static int run_scene_impl(hpm_ctx *c, int n_views, const float *const *images, c
      * this context and its peer from two host threads that pass the GPU
      * token (see hpm_ctx::gpu_token). */
     {
-        /* the prior-net form triangulates only at the coarse scale: one worker */
-        const int workers = (c->scene_workers > 1 && n_problems > 1 && !net) ? 2 : 1;
+        const int workers = (c->scene_workers > 1 && n_problems > 1) ? 2 : 1;
         if (workers == 2 && !c->peer) {
             r = hpm_create(&c->peer, c->device);
             if (r) return ctx_fail(c, r, "hpm_run_scene: second context");

@@ -31,7 +31,6 @@
  *    host synchronisation (the reference synchronises after every launch).
  */
 #include <cfloat>
-#include <cstdlib>
 
 #include "hpm_internal.h"
 
@@ -394,100 +393,6 @@ __device__ __forceinline__ float ncc(const PMArgs &a, int v, int px, int py, flo
     return fmaxf(0.0f, fminf(2.0f, 1.0f - covar / vv));
 }
 
-/* The NCC of every active lane's own (pixel, plane) for source view v,
- * computed cooperatively: groups of 6 lanes take one window at a time, each
- * lane one tap column i of the 6 (ComputeBilateralNCC's outer loop,
- * HPM.cu:347-377) with its 6 inner taps, so that a texture instruction of the
- * warp samples 5 windows, 6 neighbouring taps each, instead of 32 windows
- * that may lie far apart (a random-depth candidate's windows scatter along
- * the epipolar lines).  The owner lane's homography and reference statistics
- * reach its group by shuffles; the group adds its 6 column sums in the
- * column order of the serial loop, so every cost equals ncc()'s bit for bit.
- * sLane / sCost: 32 ints / floats of this warp's shared scratch. */
-template <typename Win>
-__device__ __forceinline__ float ncc_coop(const PMArgs &a, int v, int px, int py, float4 h, const Win *sWW, int tid,
-                                          const RefStats &rs, int *sLane, float *sCost)
-{
-    const unsigned mask = __activemask();
-    const int lane = threadIdx.x & 31;
-    const int rank = __popc(mask & ((1u << lane) - 1u));
-    const int A = __popc(mask), G = A / 6;
-    if (G == 0) return ncc(a, v, px, py, h, sWW, tid, rs);
-    const HpmCamera &sc = a.cam[v];
-    float H[9];
-    homography(a.cam[0], sc, a.pair[v], h, H);
-    const float2 pt = warp(H, (float)px, (float)py);
-    const bool live = !(pt.x >= sc.width || pt.x < 0.0f || pt.y >= sc.height || pt.y < 0.0f) && !(rs.var < 1e-5f);
-    sLane[rank] = lane;
-    __syncwarp(mask);
-    const cudaTextureObject_t tex = a.view[v].tex;
-    const int g = rank / 6, col = rank - 6 * g;
-    const int rounds = (A + G - 1) / G;
-    for (int r = 0; r < rounds; ++r) {
-        const int j = r * G + g;
-        const bool has_job = g < G && j < A;
-        const int owner = sLane[has_job ? j : 0];
-        const float ox = __shfl_sync(mask, (float)px, owner), oy = __shfl_sync(mask, (float)py, owner);
-        const int otid = __shfl_sync(mask, tid, owner);
-        const int olive = __shfl_sync(mask, live ? 1 : 0, owner);
-        float Ho[9];
-#pragma unroll
-        for (int k = 0; k < 9; ++k) Ho[k] = __shfl_sync(mask, H[k], owner);
-        float r_src = 0.0f, r_ss = 0.0f, r_rs = 0.0f;
-        if (has_job && olive) {
-            const int i = -5 + 2 * col;
-#pragma unroll
-            for (int jj = 0; jj < 6; ++jj) {
-                const float sp = tap_sample(tex, Ho, ox, oy, i, -5 + 2 * jj);
-                float2 ww;
-                if constexpr (sizeof(Win) == sizeof(float)) {
-                    const float wt = sWW[(col * 6 + jj) * kBlock + otid];
-                    ww = make_float2(wt, wt * texel(a.view[0].img, a.view[0].w, a.view[0].h, (int)ox + i,
-                                                    (int)oy - 5 + 2 * jj));
-                } else {
-                    ww = sWW[(col * 6 + jj) * kBlock + otid];
-                }
-                r_src += ww.x * sp;
-                r_ss += ww.x * sp * sp;
-                r_rs += ww.y * sp;
-            }
-        }
-        /* the column sums in column order, as the serial loop adds them */
-        float sum_src = 0.0f, sum_ss = 0.0f, sum_rs = 0.0f;
-#pragma unroll
-        for (int c = 0; c < 6; ++c) {
-            const int src_lane = sLane[has_job ? 6 * g + c : 0];
-            const float a0 = __shfl_sync(mask, r_src, src_lane);
-            const float a1 = __shfl_sync(mask, r_ss, src_lane);
-            const float a2 = __shfl_sync(mask, r_rs, src_lane);
-            sum_src += a0;
-            sum_ss += a1;
-            sum_rs += a2;
-        }
-        const float oinv = __shfl_sync(mask, rs.inv, owner), omean = __shfl_sync(mask, rs.mean, owner);
-        const float ovar = __shfl_sync(mask, rs.var, owner);
-        if (has_job && col == 0) {
-            float cost = 2.0f;
-            if (olive) {
-                sum_src *= oinv;
-                sum_ss *= oinv;
-                sum_rs *= oinv;
-                const float var_src = sum_ss - sum_src * sum_src;
-                if (!(var_src < 1e-5f)) {
-                    const float covar = sum_rs - omean * sum_src;
-                    const float vv = sqrtf(ovar * var_src);
-                    cost = fmaxf(0.0f, fminf(2.0f, 1.0f - covar / vv));
-                }
-            }
-            sCost[owner] = cost;
-        }
-    }
-    __syncwarp(mask);
-    const float c = sCost[lane];
-    __syncwarp(mask);
-    return c;
-}
-
 /* One NCC window for the loops that score several candidates view by view
  * (inline by default; -DHPM_NCC_CALL=__noinline__ builds it out of line). */
 #ifndef HPM_NCC_CALL
@@ -794,6 +699,27 @@ __device__ __forceinline__ bool same_plane(float4 p, float4 q)
 
 #define CAG(k, v) a.cand_costs[(size_t)((k) * S + (v)) * npx + center]
 
+/* Where the cost row of direction k lives, 4 bits per direction in the
+ * pixel's hand-off code (cand_flags): the row itself, the cost-vector cache
+ * (the candidate equals the current hypothesis), the row of an earlier
+ * direction with the same plane, or nowhere (an invalid direction, whose row
+ * holds 2 at [0][0] and 0 elsewhere because float cost_array[8][32] =
+ * { 2.0f } sets only [0][0], HPM.cu:1244).  Copies and invalid rows are
+ * resolved on reading instead of being written out. */
+constexpr uint32_t kRowCache = 8, kRowOwn = 9, kRowNone = 10;
+constexpr uint32_t kCodeAllNone = 0xAAAAAAAAu;
+
+__device__ __forceinline__ bool dir_valid(uint32_t code, int k) { return ((code >> (4 * k)) & 15u) != kRowNone; }
+
+__device__ __forceinline__ float dir_cost(const PMArgs &a, uint32_t code, int k, int v, int S, size_t npx, int center)
+{
+    const uint32_t src = (code >> (4 * k)) & 15u;
+    if (src == kRowOwn) return CAG(k, v);
+    if (src == kRowCache) return *cache_at(a, v, center);
+    if (src < 8) return CAG(src, v);
+    return (k == 0 && v == 0) ? 2.0f : 0.0f;
+}
+
 __global__ void __launch_bounds__(kBlock, HPM_P1_MIN_BLOCKS) k_prop_dirs(const __grid_constant__ PMArgs a, int iter,
                                                                           int color)
 {
@@ -820,9 +746,9 @@ __global__ void __launch_bounds__(kBlock, HPM_P1_MIN_BLOCKS) k_prop_dirs(const _
     pos[7] = center + 5;
     /* 1) NESP sites of the 8 directions.  Identical planes give identical
      * cost vectors: a candidate whose plane equals the current hypothesis
-     * (cost vector cached) or an earlier candidate reuses those values.
-     * src: 0..7 copy that row, 8 the cache, 9 evaluate. */
-    uint32_t src_code = 0; /* 4 bits per direction */
+     * (cost vector cached) or an earlier candidate reuses those values
+     * (dir_cost resolves the row on reading). */
+    uint32_t code = kCodeAllNone; /* 4 bits per direction */
     uint32_t eval_mask = 0;
 #pragma unroll
     for (int k = 0; k < 8; ++k) {
@@ -830,15 +756,15 @@ __global__ void __launch_bounds__(kBlock, HPM_P1_MIN_BLOCKS) k_prop_dirs(const _
         flags |= 1u << k;
         pos[k] = select_site(a, k, 0, px, py);
         const float4 c = a.planes[pos[k]];
-        int src = same_plane(c, cur) ? 8 : -1;
+        uint32_t src = same_plane(c, cur) ? kRowCache : kRowNone;
 #pragma unroll
         for (int j = 0; j < k; ++j)
-            if (src < 0 && ((flags >> j) & 1u) && same_plane(c, a.planes[pos[j]])) src = j;
-        if (src < 0) {
-            src = 9;
+            if (src == kRowNone && ((flags >> j) & 1u) && same_plane(c, a.planes[pos[j]])) src = (uint32_t)j;
+        if (src == kRowNone) {
+            src = kRowOwn;
             eval_mask |= 1u << k;
         }
-        src_code |= (uint32_t)src << (4 * k);
+        code = (code & ~(15u << (4 * k))) | (src << (4 * k));
     }
     /* 2) the distinct candidates, view by view, so that the threads of a
      * block sample one source image at a time (texture-cache locality) */
@@ -851,29 +777,17 @@ __global__ void __launch_bounds__(kBlock, HPM_P1_MIN_BLOCKS) k_prop_dirs(const _
         }
     }
     if (a.counters && eval_mask) atomicAdd(&a.counters[0], (unsigned long long)(__popc(eval_mask) * S));
-    /* 3) copies in direction order, zeros for invalid directions
-     * (float cost_array[8][32] = { 2.0f } sets only [0][0], HPM.cu:1244) */
-#pragma unroll
-    for (int k = 0; k < 8; ++k) {
-        const int src = (src_code >> (4 * k)) & 15u;
-        if (!((flags >> k) & 1u)) {
-            for (int v = 0; v < S; ++v) CAG(k, v) = (k == 0 && v == 0) ? 2.0f : 0.0f;
-        } else if (src == 8) {
-            for (int v = 0; v < S; ++v) CAG(k, v) = *cache_at(a, v, center);
-        } else if (src < 8) {
-            for (int v = 0; v < S; ++v) CAG(k, v) = CAG(src, v);
-        }
-    }
 
     /* Extension: only the left-up polyline can extend, because
      * bool symbol_eight_orientations[10] = { true } sets index 0 only
      * (HPM.cu:1475).  JudgeExtend: HPM.cu:1036-1059. */
     if (flags & 1u) {
+        bool detached = false; /* rows that copy direction 0's first row hold their own copy */
         for (int r = 0; r < 3; ++r) {
             const float good = (float)(0.8 * exp(-iter * iter * (3 - r) / 90.0));
             int good_sum = 0, bad_sum = 0;
             for (int v = 0; v < S; ++v) {
-                const float c = CAG(0, v);
+                const float c = dir_cost(a, code, 0, v, S, npx, center);
                 if (c < good) good_sum++;
                 if (c > 1.2f) bad_sum++;
             }
@@ -885,8 +799,19 @@ __global__ void __launch_bounds__(kBlock, HPM_P1_MIN_BLOCKS) k_prop_dirs(const _
             pos[0] = best;
             const float4 p = a.planes[best];
             if (same_plane(p, prev)) continue;
+            /* direction 0's row changes: the rows that refer to it keep the
+             * values it had when they were chosen */
+            if (!detached) {
+                detached = true;
+#pragma unroll
+                for (int k = 1; k < 8; ++k)
+                    if (((code >> (4 * k)) & 15u) == 0u) {
+                        for (int v = 0; v < S; ++v) CAG(k, v) = dir_cost(a, code, 0, v, S, npx, center);
+                        code = (code & ~(15u << (4 * k))) | (kRowOwn << (4 * k));
+                    }
+            }
             if (same_plane(p, cur)) {
-                for (int v = 0; v < S; ++v) CAG(0, v) = *cache_at(a, v, center);
+                code = (code & ~15u) | kRowCache;
                 continue;
             }
             int src = -1;
@@ -894,28 +819,28 @@ __global__ void __launch_bounds__(kBlock, HPM_P1_MIN_BLOCKS) k_prop_dirs(const _
             for (int j = 1; j < 8; ++j)
                 if (src < 0 && ((flags >> j) & 1u) && same_plane(p, a.planes[pos[j]])) src = j;
             if (src >= 0) {
-                for (int v = 0; v < S; ++v) CAG(0, v) = CAG(src, v);
+                const uint32_t sj = (code >> (4 * src)) & 15u;
+                code = (code & ~15u) | (sj == kRowOwn ? (uint32_t)src : sj);
             } else {
                 cost_vector(a, px, py, p, sWW, tid, rs, &CAG(0, 0), (int)npx);
+                code = (code & ~15u) | kRowOwn;
             }
         }
     }
 #pragma unroll
     for (int k = 0; k < 8; ++k) a.cand_pos[(size_t)k * npx + center] = pos[k];
-    a.cand_flags[center] = flags;
+    a.cand_flags[center] = code;
 }
 
 /* PROP: the prior-net form, whose network proposal a.proposals[center] is a
  * sixth refinement candidate, scored by the same NCC (and prior terms) as the
  * other five and accepted by the same rule.  It takes no random draws, so
  * the random stream of the other candidates is unchanged. */
-template <int SMAX, bool PROP, bool COOP>
+template <int SMAX, bool PROP>
 __global__ void __launch_bounds__(kBlock, HPM_P2_MIN_BLOCKS) k_prop_refine(const __grid_constant__ PMArgs a, int iter,
                                                                             int color)
 {
     __shared__ WinPair sWW[kTaps * kBlock];
-    __shared__ int sLane[kBlockY][32];
-    __shared__ float sCost[kBlockY][32];
     const int tid = threadIdx.y * kBlockX + threadIdx.x;
     int px, py;
     half_step_pixel(color, px, py);
@@ -924,7 +849,11 @@ __global__ void __launch_bounds__(kBlock, HPM_P2_MIN_BLOCKS) k_prop_refine(const
     const size_t npx = (size_t)W * a.H;
     const int center = py * W + px;
     const HpmCamera &cam = a.cam[0];
-    const uint32_t flags = a.cand_flags[center];
+    const uint32_t code = a.cand_flags[center];
+    uint32_t flags = 0;
+#pragma unroll
+    for (int k = 0; k < 8; ++k)
+        if (dir_valid(code, k)) flags |= 1u << k;
     int pos[8];
 #pragma unroll
     for (int k = 0; k < 8; ++k) pos[k] = a.cand_pos[(size_t)k * npx + center];
@@ -952,7 +881,7 @@ __global__ void __launch_bounds__(kBlock, HPM_P2_MIN_BLOCKS) k_prop_refine(const
         float tmpw = 0;
 #pragma unroll
         for (int k = 0; k < 8; ++k) {
-            const float c = CAG(k, v);
+            const float c = dir_cost(a, code, k, v, S, npx, center);
             if (c < thr) {
                 tmpw += expf(c * c / (-0.18f));
                 count++;
@@ -1018,11 +947,11 @@ __global__ void __launch_bounds__(kBlock, HPM_P2_MIN_BLOCKS) k_prop_refine(const
             if (v < S && vw[v] > 0) {
                 if (a.geom) {
                     if (FLAG(k))
-                        f += vw[v] * (CAG(k, v) + 0.1f * geom_cost(a, v + 1, hk, px, py));
+                        f += vw[v] * (dir_cost(a, code, k, v, S, npx, center) + 0.1f * geom_cost(a, v + 1, hk, px, py));
                     else
-                        f += vw[v] * (CAG(k, v) + 0.1f * 5.0f);
+                        f += vw[v] * (dir_cost(a, code, k, v, S, npx, center) + 0.1f * 5.0f);
                 } else {
-                    f += vw[v] * CAG(k, v);
+                    f += vw[v] * dir_cost(a, code, k, v, S, npx, center);
                 }
             }
         }
@@ -1185,26 +1114,8 @@ __global__ void __launch_bounds__(kBlock, HPM_P2_MIN_BLOCKS) k_prop_refine(const
         for (int v = 0; v < S; ++v) {
             const bool selected = (tsv >> v) & 1u;
             const float w = (float)((v < 16 ? (vw_lo >> (4 * v)) : (vw_hi >> (4 * (v - 16)))) & 15ull);
-            if constexpr (COOP) {
-                /* candidates 0 and 2 (the random depth): their windows
-                 * scatter along the epipolar lines, so the warp scores them
-                 * together, window by window (ncc_coop) */
-#pragma unroll
-                for (int q = 0; q < 2; ++q) {
-                    const int i = 2 * q;
-                    const float c = ncc_coop(a, v + 1, px, py, cand[i], sWW, tid, rs, sLane[threadIdx.y],
-                                             sCost[threadIdx.y]);
-                    CAG(kRefineRow + i, v) = c;
-                    if (selected) {
-                        if (a.geom)
-                            tc[i] += w * (c + 0.1f * geom_cost(a, v + 1, cand[i], px, py));
-                        else
-                            tc[i] += w * c;
-                    }
-                }
-            }
 #pragma unroll 1
-            for (int k = COOP ? 2 : 0; k < NC; ++k) {
+            for (int k = 0; k < NC; ++k) {
                 /* candidates 0 and 2 share the random depth, hence the window
                  * centre in every source view; 1, 3 and 4 sit at or near the
                  * current depth: scoring 0, 2, 1, 3, 4 keeps windows with the
@@ -1246,8 +1157,11 @@ __global__ void __launch_bounds__(kBlock, HPM_P2_MIN_BLOCKS) k_prop_refine(const
     a.planes[center] = plane;
     a.costs[center] = cost;
     a.views[center] = sel;
-    if (best_row >= 0)
+    if (best_row >= kRefineRow) {
         for (int v = 0; v < S; ++v) *cache_at(a, v, center) = CAG(best_row, v);
+    } else if (best_row >= 0 && ((code >> (4 * best_row)) & 15u) != kRowCache) {
+        for (int v = 0; v < S; ++v) *cache_at(a, v, center) = dir_cost(a, code, best_row, v, S, npx, center);
+    }
 #undef FLAG
 }
 #undef CAG
@@ -1365,35 +1279,15 @@ __global__ void k_tap_samples(const __grid_constant__ PMArgs a, const float4 *pl
         for (int j = -5; j < 6; j += 2, ++t) out[(size_t)k * kTaps + t] = tap_sample(a.view[v].tex, H, fpx, fpy, i, j);
 }
 
-/* Cooperative scoring of the random-depth refinement candidates (ncc_coop);
- * HPM_REFINE_COOP=0 in the environment selects the one-window-per-lane loop
- * (same results) for comparison. */
-bool refine_coop()
-{
-    static const bool on = [] {
-        const char *e = getenv("HPM_REFINE_COOP");
-        return !(e && e[0] == '0');
-    }();
-    return on;
-}
-
 template <int SMAX>
 cudaError_t launch_prop_t(const PMArgs &a, int iter, int color, cudaStream_t s)
 {
     dim3 grid((a.W + 2 * kWarpW - 1) / (2 * kWarpW), (a.rows_cov + 2 * kWarpH - 1) / (2 * kWarpH));
     k_prop_dirs<<<grid, dim3(kBlockX, kBlockY), 0, s>>>(a, iter, color);
-    const dim3 b(kBlockX, kBlockY);
-    if (refine_coop()) {
-        if (a.proposals)
-            k_prop_refine<SMAX, true, true><<<grid, b, 0, s>>>(a, iter, color);
-        else
-            k_prop_refine<SMAX, false, true><<<grid, b, 0, s>>>(a, iter, color);
-    } else {
-        if (a.proposals)
-            k_prop_refine<SMAX, true, false><<<grid, b, 0, s>>>(a, iter, color);
-        else
-            k_prop_refine<SMAX, false, false><<<grid, b, 0, s>>>(a, iter, color);
-    }
+    if (a.proposals)
+        k_prop_refine<SMAX, true><<<grid, dim3(kBlockX, kBlockY), 0, s>>>(a, iter, color);
+    else
+        k_prop_refine<SMAX, false><<<grid, dim3(kBlockX, kBlockY), 0, s>>>(a, iter, color);
     return cudaGetLastError();
 }
 

@@ -279,10 +279,11 @@ using namespace hpm;
 namespace hpm {
 
 /* Coarse stage of one problem (the views of images/cams, full scale, host or
- * device): 1/4-scale views, the plain pass on them, its planar prior, and
- * the network's input in ws_net.x0.  Leaves the coarse problem loaded in the
- * context, the coarse prior in ws.c_prior_depth / c_prior_normal, and the
- * coarse size in *cw x *ch. */
+ * device): 1/4-scale views, the plain pass on them (in the context's coarse
+ * sub-context, so that this context's full-scale views stay loaded), its
+ * planar prior, and the network's input in ws_net.x0.  Leaves the coarse
+ * prior in ws.c_prior_depth / c_prior_normal and the coarse size in
+ * *cw x *ch. */
 int net_coarse_stage(hpm_ctx *c, int n, const float *const *images, const HpmCamera *cams, uint64_t seed, int *cw,
                      int *ch)
 {
@@ -327,26 +328,35 @@ int net_coarse_stage(hpm_ctx *c, int n, const float *const *images, const HpmCam
         cimgs[j] = cur;
         cur += ((size_t)vw * vh + 63) & ~(size_t)63;
     }
-    int r = hpm_set_views(c, cimgs, ccams, n);
-    if (r) return r;
+    /* the coarse problem lives in a context of its own (created once) */
+    if (!c->coarse) {
+        int rc = hpm_create(&c->coarse, c->device);
+        if (rc) return ctx_fail(c, rc, "prior-net form: coarse context");
+        c->coarse->scene_workers = 1;
+    }
+    hpm_ctx *cc = c->coarse;
+    CK(cudaStreamSynchronize(s), "coarse images");
+    int r = hpm_set_views(cc, cimgs, ccams, n);
+    if (r) return ctx_fail(c, r, "prior-net form: %s", hpm_last_error(cc));
     HpmParams p;
     hpm_default_params(&p);
     p.depth_min = cams[0].depth_min * 0.6f;
     p.depth_max = cams[0].depth_max * 1.2f;
     p.seed = seed;
-    r = ctx_run_pass(c, &p, 6, 1);
-    if (r) return r;
+    r = ctx_run_pass(cc, &p, 6, 1); /* ends with a synchronisation of its stream */
+    if (r) return ctx_fail(c, r, "prior-net form: %s", hpm_last_error(cc));
     const size_t cn = (size_t)w * h;
     CK(ws_reserve_coarse(c, cn), "coarse buffers");
-    CK(flow_split_state(reinterpret_cast<const float4 *>(ctx_planes(c)), (int)cn, ws.c_depth, ws.c_normal, s), "split");
-    r = flow_level_prior(c, ccams[0], ctx_costs(c), ws.c_depth, w, h, 1.0f, p.depth_min, p.depth_max);
+    const float4 *cplanes = reinterpret_cast<const float4 *>(ctx_planes(cc));
+    const float *ccost = ctx_costs(cc);
+    CK(flow_split_state(cplanes, (int)cn, ws.c_depth, ws.c_normal, s), "split");
+    r = flow_level_prior(c, ccams[0], ccost, ws.c_depth, w, h, 1.0f, p.depth_min, p.depth_max);
     if (r) return r;
     CK(prior_coarse(ccams[0], w, h, 1.0f, p.depth_min, p.depth_max, ws.mask, ws.ids, ws.tri_planes, ws.knn_planes,
                     ws.c_prior_depth, ws.c_prior_normal, s),
        "coarse prior");
-    k_net_input<<<grid1(cn), 256, 0, s>>>(ccams[0], cimgs[0], reinterpret_cast<const float4 *>(ctx_planes(c)),
-                                          ctx_costs(c), ws.c_prior_depth, (int)cn, p.depth_min, p.depth_max,
-                                          static_cast<__nv_bfloat16 *>(nw.x0));
+    k_net_input<<<grid1(cn), 256, 0, s>>>(ccams[0], cimgs[0], cplanes, ccost, ws.c_prior_depth, (int)cn, p.depth_min,
+                                          p.depth_max, static_cast<__nv_bfloat16 *>(nw.x0));
     CK(cudaGetLastError(), "net input");
     *cw = w;
     *ch = h;
@@ -381,7 +391,7 @@ int net_problem(hpm_ctx *c, int n, const float *const *images, const HpmCamera *
     int cw, ch;
     int r = net_coarse_stage(c, n, images, cams, seed, &cw, &ch);
     if (r) return r;
-    const HpmCamera ccam = c->cams[0];
+    const HpmCamera ccam = c->coarse->cams[0];
     const float dmin = cams[0].depth_min * 0.6f, dmax = cams[0].depth_max * 1.2f;
     r = net_forward(c, net, ccam, cw, ch, dmin, dmax);
     if (r) return r;

@@ -1878,7 +1878,22 @@ static float ncc_with_bound(const Ctx *c, int v, int px, int py, F4 h, float k_e
     const double e_var_s = g * mss + 2.0 * ms * g * ms + u * (mss + ms * ms);
     const double e_cov = g * mrs + mr * g * ms + ms * g * mr + u * (mrs + mr * ms);
     const double e_c = e_cov / vv + fabs(covar) / vv * (0.5 * (e_var_r / var_r + e_var_s / var_s) + u) + u;
-    *acc = (float)(2.0 * e_c);
+    /* The bilateral weights: an FP32 evaluation's exp of an argument formed
+     * with approximate division differs from the exact weight by a few
+     * parts in 1e6 (CUDA documents __expf to 2 + floor(1.173 |x|) ulp, and
+     * |x| < 15 here; the argument adds ~2 ulp of |x|).  First-order effect
+     * of a relative error eps_w on every weight, signs taken worst case:
+     * d cost / d w_t from the weighted means (d m / d w_t = (v_t - m) / W). */
+    const double eps_w = 1e-5;
+    double e_w = 0.0;
+    for (t = 0; t < 36; ++t) {
+        const double dmr = (r[t] - mr) / W, dms = (s[t] - ms) / W;
+        const double dmrr = (r[t] * r[t] - mrr) / W, dmss = (s[t] * s[t] - mss) / W, dmrs = (r[t] * s[t] - mrs) / W;
+        const double dvr = dmrr - 2.0 * mr * dmr, dvs = dmss - 2.0 * ms * dms, dcov = dmrs - mr * dms - ms * dmr;
+        const double dc = -(dcov / vv - covar / (2.0 * vv) * (dvr / var_r + dvs / var_s));
+        e_w += fabs(dc) * eps_w * w[t];
+    }
+    *acc = (float)(2.0 * (e_c + e_w));
     double b = 0, dvar_tot = 0;
     for (t = 0; t < 36; ++t) {
         if (ds[t] == 0.0) continue;

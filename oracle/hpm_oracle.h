@@ -64,8 +64,9 @@ int or_cost_vectors(int n_img, const float *const *imgs, const OrCamera *cams, c
  * taps whose coordinates lie within k_err x their propagated rounding-error
  * bound of a 1/256 texture-weight step across it, or 2 where the centre's
  * in-image test or a variance cut may flip.  out_acc: twice the first-order
- * bound of the FP32 accumulation error of the window sums (large in flat
- * windows, where the variances cancel).  out_kind: bit 0 a tap lies near a
+ * bound of the FP32 arithmetic on given samples: the accumulation error of
+ * the window sums and a relative error of 1e-5 on every bilateral weight
+ * (large in flat windows, where the variances cancel).  out_kind: bit 0 a tap lies near a
  * weight step, bit 1 a decision may flip. */
 int or_ncc_bounds(int n_img, const float *const *imgs, const OrCamera *cams, const float *planes4, float k_err,
                   float *out_cost, float *out_bound, float *out_acc, int *out_kind);

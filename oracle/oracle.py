@@ -124,8 +124,9 @@ def ncc_bounds(images, cams, planes, k_err=1.0, pixels=None):
     """Cost vectors with per-value bounds (or_ncc_bounds): (cost, bound,
     acc, kind).  bound: what rounding the tap coordinates differently (up to
     k_err x their propagated first-order error bound) can change, 2 where a
-    decision may flip; acc: twice the FP32 accumulation-error bound of the
-    window sums; kind: bit 0 a tap near a texture-weight step, bit 1 a
+    decision may flip; acc: twice the first-order bound of the FP32
+    arithmetic on given samples (window sums, and 1e-5 relative on every
+    bilateral weight); kind: bit 0 a tap near a texture-weight step, bit 1 a
     decision may flip.  pixels: flat indices y*W+x to evaluate only those
     (outputs [len(pixels)][S])."""
     imgs, arr = _img_ptrs(images)

@@ -61,3 +61,21 @@ def split(cost_a, cost_b, samples_a, samples_b, inside_a, inside_b, ref_img, pix
     effect = np.where(flip, d, effect)
     crossed = crossed | flip
     return crossed, effect, d - effect
+
+
+MARGIN = 1.25  # first-order bounds: 25 % for the second-order terms they leave out
+
+
+def check_within_bound(got, ref, bound, what):
+    """|got - ref| <= 1e-4 max(1, |ref|) + MARGIN * bound for every value,
+    and <= 1e-4 max(1, |ref|) alone where the bound is below 1e-4 (well
+    conditioned).  Returns the fraction of values within 1e-4."""
+    got, ref = np.asarray(got, np.float64), np.asarray(ref, np.float64)
+    d = np.abs(got - ref)
+    tol = 1e-4 * np.maximum(1.0, np.abs(ref))
+    over = d > tol + MARGIN * bound
+    assert not over.any(), (f"{what}: {int(over.sum())} values beyond the bound, worst excess "
+                            f"{float((d - tol - MARGIN * bound).max()):.3g}")
+    calm = bound < 1e-4
+    assert (d[calm] <= tol[calm]).all(), f"{what}: {int((d[calm] > tol[calm]).sum())} well-conditioned values off"
+    return float((d <= tol).mean())

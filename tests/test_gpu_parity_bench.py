@@ -6,14 +6,17 @@ The reference's outputs come from its own HPM.cu kernels on a B200
 (tests/golden/make_golden.py, --only bench), kept at 4096 sampled pixels;
 the scenes and inputs are rebuilt from their seeds here.
 
-NCC tolerance, from the oracle's error analysis (or_ncc_bounds):
-  * every value:   |d| <= 1e-4 max(1, |ref|) + bound + acc, where bound is
-    the first-order effect of moving across their 1/256 texture-weight step
-    the taps whose coordinates lie within TWICE the propagated FP32
-    rounding-error bound of that step, and acc twice the FP32
-    accumulation-error bound of the window sums;
-  * values with no tap near a step, no decision within reach and
-    acc < 1e-4 (well conditioned): |d| <= 1e-4 max(1, |ref|), no exceptions.
+NCC tolerance.  The product's and the reference's texture samples must be
+identical (hpm_tap_samples against the reference shim's): no tap may round
+differently.  The costs then differ only by FP32 arithmetic on the same
+samples (the bilateral weights' exp and the window sums, whose variances
+cancel in flat windows), bounded by the oracle's error analysis
+(or_ncc_bounds, acc).  Against the oracle, whose tap coordinates round on
+their own, the bound adds the first-order effect of the taps whose
+coordinates lie within TWICE their propagated rounding-error bound of a
+1/256 weight step.  ncc_split.check_within_bound applies it (with a 25 %
+margin for second-order terms) and holds well-conditioned values (bound
+below 1e-4) to 1e-4 with no exceptions.
 """
 import hashlib
 import os
@@ -25,6 +28,7 @@ import pytest
 from conftest import GOLDEN, golden
 
 import hpm_b200 as hb
+import ncc_split
 import oracle as orc
 import synthetic as syn
 
@@ -55,28 +59,24 @@ def _sample(a, px):
     return a.reshape(h * w, *a.shape[2:])[px]
 
 
-def _check_ncc(got, ref, bound, acc, kind, what):
-    got, ref = got.astype(np.float64), ref.astype(np.float64)
-    d = np.abs(got - ref)
-    tol = 1e-4 * np.maximum(1.0, np.abs(ref))
-    over = d > tol + bound + acc
-    assert not over.any(), f"{what}: {over.sum()} values beyond the bound, worst excess {(d - tol - bound - acc).max():.3g}"
-    clean = (kind == 0) & (acc < 1e-4)
-    assert clean.mean() > 0.02, clean.mean()
-    assert (d[clean] <= tol[clean]).all(), f"{what}: clean values beyond 1e-4: {(d[clean] > tol[clean]).sum()}"
-    assert d.mean() <= 2e-4, d.mean()
-    return clean.mean()
-
-
 def test_cost_vectors_vs_reference_and_oracle(case):
+    """Same texture samples as the reference's kernels, costs within the
+    FP32 arithmetic bound; against the oracle within the bound that also
+    covers taps crossing a weight step."""
     name, g, c, ctx = case
     px = c["pixels"]
     for k, p in enumerate(c["planes"]):
         got = _sample(ctx.cost_vectors(p), px)
-        ocost, bound, acc, kind = orc.ncc_bounds(c["imgs"], c["cams"], p, K_ERR, pixels=px)
-        _check_ncc(got, g["cost_vectors"][k], bound, acc, kind, f"{name} field {k} vs reference")
-        _check_ncc(got, ocost, bound, acc, kind, f"{name} field {k} vs oracle")
-        _check_ncc(ocost, g["cost_vectors"][k], bound, acc, kind, f"{name} field {k} oracle vs reference")
+        ocost, bound, acc, _ = orc.ncc_bounds(c["imgs"], c["cams"], p, K_ERR, pixels=px)
+        if orc.ref_available():
+            sg, ig = ctx.tap_samples(p, px)
+            sr, ir = orc.ref_tap_samples(c["imgs"], c["cams"], p, px)
+            np.testing.assert_array_equal(ig, ir)
+            np.testing.assert_array_equal(sg[ig], sr[ir])
+        ref = g["cost_vectors"][k]
+        ncc_split.check_within_bound(got, ref, acc, f"{name} field {k} vs reference")
+        ncc_split.check_within_bound(got, ocost, bound + acc, f"{name} field {k} vs oracle")
+        ncc_split.check_within_bound(ocost, ref, bound + acc, f"{name} field {k} oracle vs reference")
 
 
 def test_initial_costs_vs_reference(case):
@@ -89,7 +89,7 @@ def test_initial_costs_vs_reference(case):
         _, bound, acc, _ = orc.ncc_bounds(c["imgs"], c["cams"], p, K_ERR, pixels=px)
         ref = g["init_cost"][k].astype(np.float64)
         d = np.abs(_sample(cost, px) - ref)
-        tol = 1e-4 * np.maximum(1.0, np.abs(ref)) + (bound + acc).max(-1)
+        tol = 1e-4 * np.maximum(1.0, np.abs(ref)) + ncc_split.MARGIN * (bound + acc).max(-1)
         assert (d <= tol).all(), (d - tol).max()
         assert (_sample(views, px) == g["init_views"][k]).mean() >= 0.99
 
