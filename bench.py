@@ -46,7 +46,14 @@ sys.path[:0] = [os.path.join(ROOT, "hpm-mvs_b200")]
 
 METRIC = "depth Mpix/s, plain vs batched prior-net form on 1 B200, at equal %px relerr<1%"
 WORKLOAD = dict(width=1600, height=1200, n_views=11, n_planes=20, n_spheres=5, low_texture=0.40, pyramid_levels=2,
-                geom_iterations=2)
+                geom_iterations=2, depth_range=(2.0, 8.0), name="full plain HPM scene")
+# stress test: 6048x4032 views, which the reference caps to 3200x2133
+# (HPM.cpp:525-551, max_image_size 3200): the scene is rendered at the capped
+# size directly; its pyramid follows the reference's rule at that size
+# (ComputingMultiScaleSettings, HPM.cpp:851-860: 2 levels below full scale)
+STRESS = dict(width=3200, height=2133, n_views=20, n_planes=20, n_spheres=5, low_texture=0.50, pyramid_levels=2,
+              geom_iterations=2, depth_range=(1.0, 30.0),
+              name="stress scene (6048x4032 capped to 3200x2133 as the reference does)")
 
 # DRAM traffic of one half-step (k_prop_dirs + k_prop_refine), from an ncu
 # capture of `bench.py --pass-case` (1600x1200, 10 sources), per pixel: the
@@ -58,7 +65,7 @@ TAPS, NCC_FLOPS_PER_TAP, FLOPS_PER_HYP_VIEW = 36, 34, 80
 
 def workload_name():
     w = WORKLOAD
-    return (f"full plain HPM scene: {w['n_views']} views of {w['width']}x{w['height']}, "
+    return (f"{w['name']}: {w['n_views']} views of {w['width']}x{w['height']}, "
             f"{w['n_views'] - 1} sources each, planar+KNN prior on a {w['pyramid_levels'] + 1}-level pyramid, "
             f"{w['geom_iterations']} geometric iterations")
 
@@ -70,6 +77,9 @@ def parse_args():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--config", choices=["plain-hpm", "stress"], default="plain-hpm",
+                    help="plain-hpm: 11 views of 1600x1200 (the metric's configuration); stress: 20 views of "
+                         "6048x4032 capped to 3200x2133, 50%% low texture, depth 1-30 m (one step takes minutes)")
     ap.add_argument("--size", default=None,
                     help="WxH override of the workload's resolution (profiling captures use a smaller case)")
     ap.add_argument("--views", type=int, default=None, help="override of the scene's view count")
@@ -80,6 +90,8 @@ def parse_args():
                     help="kernel-capture case: plain PatchMatch passes of one view of the scene (1 warm-up, then "
                          "--steps passes); prints the half-step time instead of the bench line")
     args = ap.parse_args()
+    if args.config == "stress":
+        WORKLOAD.update(STRESS)
     if args.size:
         w, h = (int(x) for x in args.size.lower().split("x"))
         WORKLOAD.update(width=w, height=h)
@@ -179,7 +191,7 @@ def make_scene(seed, width=None, height=None):
 
     w = WORKLOAD
     sc = syn.make_scene(seed, width or w["width"], height or w["height"], w["n_views"], n_planes=w["n_planes"],
-                        n_spheres=w["n_spheres"], low_texture=w["low_texture"])
+                        n_spheres=w["n_spheres"], low_texture=w["low_texture"], depth_range=w["depth_range"])
     images = [i.astype(np.float32) for i in sc.images]
     pairs = [(v, list(sc.pairs[v][1])) for v in range(w["n_views"])]
     return sc, images, pairs
@@ -354,6 +366,7 @@ def run_ours(args, dist):
     dist.barrier()
     ms_e2e = dist.max(f0.elapsed_time(f1))
     acc = scene_accuracy(sc, dict(enumerate(out_np[0])), dict(enumerate(out_np[1])))
+    net_form = prior_net_form(args, dist, ctx, sc, d_ptrs, pairs, stream, ms / args.steps, acc, out_np)
     ctx.close()
     fusion = time_fusion(sc, pairs, out_np[0], out_np[1], dist.rank == 0 and dist.world == 1)
 
@@ -403,9 +416,57 @@ def run_ours(args, dist):
                      "ncc_windows_per_step": ncc_half, "geom_terms_per_step": n_geom,
                      "flops_per_ncc_window": TAPS * NCC_FLOPS_PER_TAP + FLOPS_PER_HYP_VIEW},
         "fusion": fusion,
+        "prior_net_form": net_form,
         "impl": "ours",
     }
     return line
+
+
+def prior_net_form(args, dist, ctx, sc, d_ptrs, pairs, stream, plain_ms, plain_acc, out_np):
+    """The prior-net form on the same scene and timing rules (device-resident
+    images, CUDA events on the context's stream): per problem a 1/4-scale
+    plain pass, the coarse planar prior, the BF16 network's proposal, one
+    full-scale prior pass that starts from and scores the proposal, then the
+    geometric iterations.  Accuracy from an untimed run with the maps out."""
+    import torch
+
+    import priornet
+
+    if not os.path.exists(priornet.WEIGHTS_FILE):
+        return {"unavailable": "no trained weights (hpm-mvs_b200/priornet_weights.npz)"}
+    net = priornet.Net.load(device=dist.local)
+    meta = dict(np.load(priornet.WEIGHTS_FILE))
+    geom = int(meta["geom_iterations"]) if "geom_iterations" in meta else WORKLOAD["geom_iterations"]
+    extra = int(meta["extra_passes"]) if "extra_passes" in meta else 0
+    wts = net.weights()
+    w = WORKLOAD
+    npx = w["n_views"] * w["width"] * w["height"]
+
+    def step(seed, outputs=False):
+        return ctx.run_scene(d_ptrs, sc.cams, pairs, seed=seed, images_are_device=True, outputs=outputs,
+                             geom_iterations=geom, pyramid_levels=extra, net=wts)
+
+    for i in range(args.warmup):
+        step(2000 + i)
+    dist.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for i in range(args.steps):
+        step(i)
+    e1.record(stream)
+    e1.synchronize()
+    dist.barrier()
+    ms = dist.max(e0.elapsed_time(e1)) / args.steps
+    step(0, outputs=out_np)
+    acc = scene_accuracy(sc, dict(enumerate(out_np[0])), dict(enumerate(out_np[1])))
+    value = job_mpix_per_s(dist.world, 1, npx, ms)
+    return {"value": value, "unit": "depth Mpix/s", "ms_per_step": ms, "geom_iterations": geom,
+            "extra_full_scale_prior_passes": extra,
+            "speedup_vs_plain": plain_ms / ms, "accuracy": acc,
+            "px_relerr_lt_1pct_minus_plain": acc["px_relerr_lt_1pct"] - plain_acc["px_relerr_lt_1pct"],
+            "network": "4 layers of 3x3 conv, 32 channels, BF16 on tcgen05 (FP32 accumulation in TMEM), "
+                       "at 1/4 scale; weights hpm-mvs_b200/priornet_weights.npz"}
 
 
 def run_view_shards(args, dist):

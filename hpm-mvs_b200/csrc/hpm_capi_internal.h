@@ -161,7 +161,10 @@ cudaError_t flow_split_state(const float4 *planes, int n, float *depth, float *n
 cudaError_t flow_pack4(const float *depth, const float *normal3, int n, float4 *out, cudaStream_t s);
 int flow_level_prior(hpm_ctx *c, const HpmCamera &cam, const float *d_cost, const float *d_depth, int w, int h,
                      float factor, float dmin, float dmax);
+/* the prior of pyramid level `level` (2: full scale) from flow.full_depth /
+ * full_normal and d_cost, into the context's prior planes and masks */
+int flow_prior_from_maps(hpm_ctx *c, int level, const float *d_cost, float dmin, float dmax);
 /* hpm_priornet.cu */
 int net_problem(hpm_ctx *c, int n, const float *const *images, const HpmCamera *cams, const HpmNetWeights *net,
-                uint64_t seed, float *depth_out, float *normal_out, float *cost_out);
+                uint64_t seed, int extra_passes, float *depth_out, float *normal_out, float *cost_out);
 }  // namespace hpm

@@ -182,6 +182,11 @@ static int level_prior_from_maps(hpm_ctx *c, int i, const float *d_cost, float d
     return HPM_OK;
 }
 
+int hpm::flow_prior_from_maps(hpm_ctx *c, int level, const float *d_cost, float dmin, float dmax)
+{
+    return level_prior_from_maps(c, level, d_cost, dmin, dmax);
+}
+
 extern "C" int hpm_prior_level(hpm_ctx *c, int level, const float *depth, const float *normal, const float *cost,
                                float *prior_planes, uint32_t *masks, float *prior_depth)
 {
@@ -432,7 +437,8 @@ static int run_scene_impl(hpm_ctx *c, int n_views, const float *const *images, c
                     const float *pimg[kMaxViews];
                     HpmCamera pcam[kMaxViews];
                     const int n = gather(p, pimg, pcam), ref = ref_ids[p];
-                    rr = net_problem(cc, n, pimg, pcam, net, o->seed + (uint64_t)p, m.depth_a[ref], m.normal[ref],
+                    rr = net_problem(cc, n, pimg, pcam, net, o->seed + (uint64_t)p,
+                                     o->pyramid_levels > 0 ? o->pyramid_levels : 0, m.depth_a[ref], m.normal[ref],
                                      m.cost[ref]);
                     if (rr == HPM_OK && out_prior_depths && out_prior_depths[ref])
                         rr = cudaMemsetAsync(out_prior_depths[ref], 0,

@@ -384,9 +384,10 @@ int net_forward(hpm_ctx *c, const HpmNetWeights *net, const HpmCamera &ccam, int
  * stage and the network, then one full-scale PatchMatch pass with the
  * coarse planar prior (upsampled by JBU, as the plain form's coarsest level)
  * and the network's proposal as the initial hypothesis and as a sixth
- * refinement candidate.  Outputs like hpm_process_problem. */
+ * refinement candidate, then extra_passes more full-scale prior passes.
+ * Outputs like hpm_process_problem. */
 int net_problem(hpm_ctx *c, int n, const float *const *images, const HpmCamera *cams, const HpmNetWeights *net,
-                uint64_t seed, float *depth_out, float *normal_out, float *cost_out)
+                uint64_t seed, int extra_passes, float *depth_out, float *normal_out, float *cost_out)
 {
     int cw, ch;
     int r = net_coarse_stage(c, n, images, cams, seed, &cw, &ch);
@@ -428,10 +429,23 @@ int net_problem(hpm_ctx *c, int n, const float *const *images, const HpmCamera *
     p.planar_prior = 1;
     c->proposals = nw.cand;
     r = ctx_run_pass(c, &p, 6, 1);
-    c->proposals = nullptr;
-    if (r) return r;
     CK(flow_split_state(reinterpret_cast<const float4 *>(ctx_planes(c)), (int)npx, ws.full_depth, ws.full_normal, s),
        "split");
+    /* optional further full-scale prior passes: the planar prior rebuilt
+     * from the last pass (the plain form's finest level), the proposal
+     * still a candidate */
+    for (int e = 0; e < extra_passes && r == HPM_OK; ++e) {
+        r = flow_prior_from_maps(c, 2, ctx_costs(c), dmin, dmax);
+        if (r) break;
+        p.seed += 0x632BE59BD9B4E019ull;
+        r = ctx_run_pass(c, &p, 6, 1);
+        if (r) break;
+        CK(flow_split_state(reinterpret_cast<const float4 *>(ctx_planes(c)), (int)npx, ws.full_depth, ws.full_normal,
+                            s),
+           "split");
+    }
+    c->proposals = nullptr;
+    if (r) return r;
     if (depth_out) CK(cudaMemcpyAsync(depth_out, ws.full_depth, sizeof(float) * npx, cudaMemcpyDefault, s), "out");
     if (normal_out)
         CK(cudaMemcpyAsync(normal_out, ws.full_normal, sizeof(float) * 3 * npx, cudaMemcpyDefault, s), "out");

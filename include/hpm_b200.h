@@ -286,8 +286,10 @@ typedef struct {
  * initial hypothesis is the network's proposal (upsampled by JBU) and whose
  * refinement scores the proposal as a sixth candidate with the unchanged NCC
  * cost; the planar prior is the coarse one, upsampled as the plain form's
- * coarsest level.  The geometric iterations are the plain form's.
- * opts->pyramid_levels is not used. */
+ * coarsest level.  opts->pyramid_levels > 0 adds that many full-scale
+ * prior passes, each with the planar prior rebuilt from the previous pass
+ * (the plain form's finest level) and the proposal still a candidate.  The
+ * geometric iterations are the plain form's. */
 int hpm_run_scene_net(hpm_ctx *ctx, int n_views, const float *const *images, const HpmCamera *cams, int n_problems,
                       const int *ref_ids, const int *src_counts, const int *src_ids, const HpmSceneOpts *opts,
                       const HpmNetWeights *net, float *const *out_depths, float *const *out_normals,
