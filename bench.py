@@ -54,6 +54,12 @@ WORKLOAD = dict(width=1600, height=1200, n_views=11, n_planes=20, n_spheres=5, l
 STRESS = dict(width=3200, height=2133, n_views=20, n_planes=20, n_spheres=5, low_texture=0.50, pyramid_levels=2,
               geom_iterations=2, depth_range=(1.0, 30.0),
               name="stress scene (6048x4032 capped to 3200x2133 as the reference does)")
+# batched form: all 24 reference views of one scene at three sizes, each with
+# 10 sources, the pyramid by the reference's rule per view size
+BATCHED = dict(width=1920, height=1080, n_views=24, n_planes=20, n_spheres=5, low_texture=0.40, pyramid_levels=-1,
+               geom_iterations=2, depth_range=(2.0, 8.0), arc_step_deg=3.0, n_sources=10,
+               sizes=[(1920, 1080)] * 8 + [(1600, 1200)] * 8 + [(960, 540)] * 8,
+               name="batched scene (8 views of 1920x1080, 8 of 1600x1200, 8 of 960x540)")
 
 # DRAM traffic of one half-step (k_prop_dirs + k_prop_refine), from an ncu
 # capture of `bench.py --pass-case` (1600x1200, 10 sources), per pixel: the
@@ -77,9 +83,11 @@ def parse_args():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--config", choices=["plain-hpm", "stress"], default="plain-hpm",
+    ap.add_argument("--config", choices=["plain-hpm", "stress", "batched"], default="plain-hpm",
                     help="plain-hpm: 11 views of 1600x1200 (the metric's configuration); stress: 20 views of "
-                         "6048x4032 capped to 3200x2133, 50%% low texture, depth 1-30 m (one step takes minutes)")
+                         "6048x4032 capped to 3200x2133, 50%% low texture, depth 1-30 m (one step takes minutes); "
+                         "batched: 24 views at three sizes through hpm_run_scene_batched against the per-problem "
+                         "driver")
     ap.add_argument("--size", default=None,
                     help="WxH override of the workload's resolution (profiling captures use a smaller case)")
     ap.add_argument("--views", type=int, default=None, help="override of the scene's view count")
@@ -92,6 +100,8 @@ def parse_args():
     args = ap.parse_args()
     if args.config == "stress":
         WORKLOAD.update(STRESS)
+    elif args.config == "batched":
+        WORKLOAD.update(BATCHED)
     if args.size:
         w, h = (int(x) for x in args.size.lower().split("x"))
         WORKLOAD.update(width=w, height=h)
@@ -190,8 +200,9 @@ def make_scene(seed, width=None, height=None):
     import synthetic as syn
 
     w = WORKLOAD
+    extra = {k: w[k] for k in ("sizes", "arc_step_deg", "n_sources") if k in w and not (width or height)}
     sc = syn.make_scene(seed, width or w["width"], height or w["height"], w["n_views"], n_planes=w["n_planes"],
-                        n_spheres=w["n_spheres"], low_texture=w["low_texture"], depth_range=w["depth_range"])
+                        n_spheres=w["n_spheres"], low_texture=w["low_texture"], depth_range=w["depth_range"], **extra)
     images = [i.astype(np.float32) for i in sc.images]
     pairs = [(v, list(sc.pairs[v][1])) for v in range(w["n_views"])]
     return sc, images, pairs
@@ -469,6 +480,59 @@ def prior_net_form(args, dist, ctx, sc, d_ptrs, pairs, stream, plain_ms, plain_a
                        "at 1/4 scale; weights hpm-mvs_b200/priornet_weights.npz"}
 
 
+def run_batched(args, dist):
+    """The batched form against the per-problem driver on the same scene of
+    uneven view sizes: both device-resident, CUDA events on the context's
+    stream, whole-scene steps."""
+    import torch
+
+    import hpm_b200 as hb
+
+    torch.cuda.set_device(dist.local)
+    dev = f"cuda:{dist.local}"
+    w = WORKLOAD
+    sc, images, pairs = make_scene(seed=dist.rank)
+    npx = sum(i.size for i in images)
+    ctx = hb.Context(dist.local)
+    stream = torch.cuda.ExternalStream(ctx.stream(), device=dev)
+    d_imgs = [torch.from_numpy(i).to(dev) for i in images]
+    d_ptrs = [t.data_ptr() for t in d_imgs]
+    torch.cuda.synchronize()
+    opts = dict(geom_iterations=w["geom_iterations"], pyramid_levels=w["pyramid_levels"], images_are_device=True)
+    res = {}
+    for form, batched in (("batched", True), ("per_problem", False)):
+        for i in range(args.warmup):
+            ctx.run_scene(d_ptrs, sc.cams, pairs, seed=500 + i, outputs=False, batched=batched, **opts)
+        dist.barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with Clocks(dist.local) as clk:
+            e0.record(stream)
+            for i in range(args.steps):
+                ctx.run_scene(d_ptrs, sc.cams, pairs, seed=i, outputs=False, batched=batched, **opts)
+            e1.record(stream)
+            e1.synchronize()
+        dist.barrier()
+        ms = dist.max(e0.elapsed_time(e1)) / args.steps
+        d, n, _ = ctx.run_scene(d_ptrs, sc.cams, pairs, seed=0, batched=batched, **opts)
+        res[form] = {"ms_per_step": ms, "value": job_mpix_per_s(dist.world, 1, npx, ms),
+                     "accuracy": scene_accuracy(sc, dict(enumerate(d)), dict(enumerate(n))), "clocks": clk.summary()}
+    ctx.close()
+    b = res["batched"]
+    return {
+        "metric": METRIC, "value": b["value"], "unit": "depth Mpix/s", "n_gpus": dist.world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": b["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded procedural scene of uneven view sizes)",
+        "config": {"workload": workload_name(), "views": w["n_views"], "sizes": "8x1920x1080, 8x1600x1200, 8x960x540",
+                   "sources": 10, "pyramid": "reference rule per view size", "geom_iterations": w["geom_iterations"],
+                   "form": "hpm_run_scene_batched: one persistent launch per kernel and half-step over all 24 "
+                           "problems, passes replayed from a CUDA graph, tiles tuned per view size"},
+        "accuracy": b["accuracy"], "clocks": b["clocks"],
+        "per_problem_form": res["per_problem"], "speedup_vs_per_problem": res["per_problem"]["ms_per_step"] /
+        b["ms_per_step"], "impl": "ours",
+    }
+
+
 def run_view_shards(args, dist):
     """One scene, its problems split over the ranks (scene_dist.py): timed
     from the host images to every rank's final maps on the host."""
@@ -685,6 +749,8 @@ def main():
             line = run_reference(args, dist)
         elif args.shard == "views":
             line = run_view_shards(args, dist)
+        elif args.config == "batched":
+            line = run_batched(args, dist)
         else:
             line = run_ours(args, dist)
             if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:

@@ -1,0 +1,375 @@
+/*
+ * The batched form of a scene (hpm_run_scene_batched): every problem of the
+ * scene advances together, one persistent launch per kernel and half-step
+ * covering the tiles of all problems, whatever their sizes.
+ *
+ * The reference runs the problems one after another (main.cpp:658-674),
+ * each with its own launches (HPM.cu:1906-1957).  Here each problem keeps
+ * its own context (views and texture arrays, hypothesis state, hand-off
+ * buffers); their kernel arguments sit side by side in device memory and a
+ * work list maps every CTA iteration to a (problem, tile) pair
+ * (hpm_pm.cu: k_init_batch, k_prop_dirs_batch, k_prop_refine_batch).
+ *
+ *  - One pass (initialisation, 6 half-steps, depth/normal and the filter)
+ *    is captured once per scene as a CUDA graph and replayed for every pass
+ *    that covers all problems; before each replay only the argument array is
+ *    refreshed (seeds, pass flags).
+ *  - The half-step tile (pixels of one colour per warp row: 4, 8 or 16) is
+ *    picked per view size by timing one half-step of each on the scene's
+ *    first problem of that size (kept in the context for later scenes).
+ *  - Pass set A advances in lock step: the plain pass of every problem, then
+ *    each pyramid level's prior (built per problem on the host and device,
+ *    as in hpm_process_problem) and the batched prior pass.  Problems whose
+ *    pyramid is shorter join at its first level (levels aligned at the full
+ *    scale).
+ *  - The geometric iterations read the previous iteration's maps of every
+ *    view (as the view-sharded driver does); the reference's in-place order
+ *    would serialise the problems.
+ *
+ * Per-pixel results do not depend on the tile shape or on which CTA
+ * computes them, so pass set A equals hpm_process_problem's on a fresh
+ * context per problem bit for bit.
+ */
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "hpm_capi_internal.h"
+#include "hpm_prior.h"
+
+using namespace hpm;
+
+#define CK(call, what)                                            \
+    do {                                                          \
+        cudaError_t e_ = (call);                                  \
+        if (e_ != cudaSuccess) return ctx_cuda_fail(c, e_, what); \
+    } while (0)
+
+namespace {
+
+int scale_levels_of(int w, int h) /* ComputingMultiScaleSettings, HPM.cpp:851-860 */
+{
+    int m = w > h ? w : h, k = 0;
+    while (m > 1000) {
+        m /= 2;
+        k++;
+    }
+    return k;
+}
+
+__global__ void k_pack_maps(const float *__restrict__ normal3, const float *__restrict__ depth, int n,
+                            float4 *__restrict__ planes)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    planes[i] = make_float4(normal3[3 * i], normal3[3 * i + 1], normal3[3 * i + 2], depth[i]);
+}
+
+/* A batch of problem contexts with its device work lists and, once
+ * captured, the graph of one pass. */
+struct Plan {
+    std::vector<hpm_ctx *> ctxs;
+    std::vector<PMArgs> args; /* host copy, refreshed per pass */
+    void *dev = nullptr;      /* args + work lists */
+    BatchList init{}, half{};
+    int smax = 0;
+    cudaGraphExec_t exec = nullptr;
+
+    ~Plan()
+    {
+        if (exec) cudaGraphExecDestroy(exec);
+        cudaFree(dev);
+    }
+};
+
+int make_plan(hpm_ctx *c, const std::vector<hpm_ctx *> &ctxs, const std::vector<int> &ww, Plan &pl)
+{
+    const int n = (int)ctxs.size();
+    pl.ctxs = ctxs;
+    pl.args.assign(n, PMArgs());
+    std::vector<int> ifirst(n + 1, 0), igx(n), hfirst(n + 1, 0), hgx(n);
+    pl.smax = 0;
+    for (int i = 0; i < n; ++i) {
+        const HpmCamera &cam = ctxs[i]->cams[0];
+        igx[i] = (cam.width + 31) / 32;
+        ifirst[i + 1] = ifirst[i] + igx[i] * ((cam.height + 1) / 2);
+        hfirst[i + 1] = hfirst[i] + half_step_tiles(cam.width, rows_covered(cam.height), ww[i], &hgx[i]);
+        pl.smax = std::max(pl.smax, ctxs[i]->n - 1);
+    }
+    const size_t argb = sizeof(PMArgs) * n, ints = sizeof(int) * (size_t)(5 * n + 2);
+    CK(cudaMalloc(&pl.dev, argb + ints), "batch lists");
+    std::vector<int> host;
+    host.insert(host.end(), ifirst.begin(), ifirst.end());
+    host.insert(host.end(), igx.begin(), igx.end());
+    host.insert(host.end(), hfirst.begin(), hfirst.end());
+    host.insert(host.end(), hgx.begin(), hgx.end());
+    host.insert(host.end(), ww.begin(), ww.end());
+    int *d = reinterpret_cast<int *>(static_cast<char *>(pl.dev) + argb);
+    CK(cudaMemcpy(d, host.data(), sizeof(int) * host.size(), cudaMemcpyHostToDevice), "batch lists");
+    const PMArgs *dargs = static_cast<const PMArgs *>(pl.dev);
+    pl.init = BatchList{dargs, d, d + n + 1, nullptr, n, ifirst[n]};
+    pl.half = BatchList{dargs, d + 2 * n + 1, d + 3 * n + 2, d + 4 * n + 2, n, hfirst[n]};
+    return HPM_OK;
+}
+
+/* the launches of one pass on stream s: initialisation, 6 half-steps,
+ * depth/normal and the filter of every problem */
+cudaError_t launch_pass(const Plan &pl, cudaStream_t s)
+{
+    cudaError_t e = launch_batch_init(pl.init, 0, s);
+    for (int hs = 0; hs < 6 && e == cudaSuccess; ++hs) e = launch_batch_propagate(pl.half, pl.smax, hs / 2, hs % 2, 0, s);
+    for (size_t i = 0; i < pl.ctxs.size() && e == cudaSuccess; ++i)
+        e = launch_depth_normal_filter(pl.args[i], reinterpret_cast<float4 *>(ctx_planes(pl.ctxs[i])),
+                                       ctx_costs(pl.ctxs[i]), s);
+    return e;
+}
+
+/* One batched pass with per-problem parameters. */
+int batch_pass(hpm_ctx *c, Plan &pl, const std::vector<HpmParams> &params)
+{
+    cudaStream_t s = c->stream;
+    for (size_t i = 0; i < pl.ctxs.size(); ++i) {
+        const int r = ctx_pass_args(pl.ctxs[i], &params[i], &pl.args[i]);
+        if (r) return ctx_fail(c, r, "batched pass, problem %zu: %s", i, hpm_last_error(pl.ctxs[i]));
+    }
+    CK(cudaMemcpyAsync(pl.dev, pl.args.data(), sizeof(PMArgs) * pl.args.size(), cudaMemcpyHostToDevice, s), "args");
+    if (!pl.exec) {
+        /* capture the pass once; its kernels read their arguments from pl.dev,
+         * the per-problem finalisation's arguments do not change between passes */
+        cudaGraph_t g = nullptr;
+        CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "graph capture");
+        const cudaError_t le = launch_pass(pl, s);
+        const cudaError_t ce = cudaStreamEndCapture(s, &g);
+        CK(le, "batched pass launches");
+        CK(ce, "graph capture");
+        const cudaError_t ie = cudaGraphInstantiate(&pl.exec, g, 0);
+        cudaGraphDestroy(g);
+        CK(ie, "graph instantiate");
+    }
+    CK(cudaGraphLaunch(pl.exec, s), "graph launch");
+    CK(cudaStreamSynchronize(s), "batched pass");
+    return HPM_OK;
+}
+
+/* The half-step tile width for each problem: per view size the fastest of
+ * 4, 8 and 16 pixels per warp row, timed on one half-step of the scene's first
+ * problem of that size (its state is re-initialised by the real passes). */
+int tune_tiles(hpm_ctx *c, const std::vector<hpm_ctx *> &ctxs, const std::vector<HpmParams> &params,
+               std::vector<int> &ww)
+{
+    ww.assign(ctxs.size(), 8);
+    for (size_t i = 0; i < ctxs.size(); ++i) {
+        const HpmCamera &cam = ctxs[i]->cams[0];
+        const long long key = ((long long)cam.width << 32) | (unsigned)cam.height;
+        int found = 0;
+        for (auto &kv : c->tile_ww)
+            if (kv.first == key) found = kv.second;
+        if (!found) {
+            float best = 1e30f;
+            for (int cand : {4, 8, 16}) {
+                Plan one;
+                int r = make_plan(c, {ctxs[i]}, {cand}, one);
+                if (r) return r;
+                r = ctx_pass_args(ctxs[i], &params[i], &one.args[0]);
+                if (r) return ctx_fail(c, r, "tile tuning: %s", hpm_last_error(ctxs[i]));
+                CK(cudaMemcpy(one.dev, one.args.data(), sizeof(PMArgs), cudaMemcpyHostToDevice), "args");
+                CK(launch_batch_init(one.init, 0, c->stream), "tuning init");
+                cudaEvent_t e0, e1;
+                cudaEventCreate(&e0);
+                cudaEventCreate(&e1);
+                cudaEventRecord(e0, c->stream);
+                CK(launch_batch_propagate(one.half, one.smax, 0, 0, 0, c->stream), "tuning half-step");
+                cudaEventRecord(e1, c->stream);
+                CK(cudaEventSynchronize(e1), "tuning");
+                float ms = 0.0f;
+                cudaEventElapsedTime(&ms, e0, e1);
+                cudaEventDestroy(e0);
+                cudaEventDestroy(e1);
+                if (ms < best) {
+                    best = ms;
+                    found = cand;
+                }
+            }
+            c->tile_ww.push_back({key, found});
+            ctx_reset_salt(ctxs[i]);
+        }
+        ww[i] = found;
+    }
+    return HPM_OK;
+}
+
+}  // namespace
+
+extern "C" int hpm_run_scene_batched(hpm_ctx *c, int n_views, const float *const *images, const HpmCamera *cams,
+                                     int n_problems, const int *ref_ids, const int *src_counts, const int *src_ids,
+                                     const HpmSceneOpts *o, float *const *out_depths, float *const *out_normals,
+                                     float *const *out_costs)
+{
+    if (!c || !images || !cams || !ref_ids || !src_counts || !src_ids || !o) return HPM_ERR_ARG;
+    if (n_views < 2 || n_problems < 1)
+        return ctx_fail(c, HPM_ERR_ARG, "hpm_run_scene_batched: %d views, %d problems", n_views, n_problems);
+    for (int p = 0; p < n_problems; ++p) {
+        if (ref_ids[p] < 0 || ref_ids[p] >= n_views || src_counts[p] < 1 || src_counts[p] > kMaxSrc)
+            return ctx_fail(c, HPM_ERR_ARG, "hpm_run_scene_batched: problem %d is malformed", p);
+        for (int j = 0; j < src_counts[p]; ++j) {
+            const int sv = src_ids[p * kMaxSrc + j];
+            if (sv < 0 || sv >= n_views)
+                return ctx_fail(c, HPM_ERR_ARG, "hpm_run_scene_batched: problem %d source %d", p, sv);
+        }
+    }
+    int r = ctx_select_device(c);
+    if (r) return r;
+    cudaStream_t s = c->stream;
+    /* per view: image, pass-A depth, two geometric depth buffers, normal (3), cost */
+    std::vector<float *> img(n_views), dep_a(n_views), dep_g0(n_views), dep_g1(n_views), nrm(n_views), cst(n_views);
+    size_t total = 0;
+    for (int v = 0; v < n_views; ++v) total += 8 * (((size_t)cams[v].width * cams[v].height + 63) & ~(size_t)63);
+    CK(ctx_scene_arena(c, total * sizeof(float)), "scene buffers");
+    float *cur = ctx_scene_base(c);
+    CK(cudaMemsetAsync(cur, 0, total * sizeof(float), s), "scene buffers");
+    for (int v = 0; v < n_views; ++v) {
+        const size_t np = (size_t)cams[v].width * cams[v].height, st = (np + 63) & ~(size_t)63;
+        img[v] = cur;
+        dep_a[v] = cur + st;
+        dep_g0[v] = cur + 2 * st;
+        dep_g1[v] = cur + 3 * st;
+        nrm[v] = cur + 4 * st;
+        cst[v] = cur + 7 * st;
+        cur += 8 * st;
+        CK(cudaMemcpyAsync(img[v], images[v], sizeof(float) * np, cudaMemcpyDefault, s), "scene images");
+    }
+    CK(cudaStreamSynchronize(s), "scene images");
+    /* one context per problem, kept for later scenes */
+    while ((int)c->batch.size() < n_problems) {
+        hpm_ctx *b = nullptr;
+        r = hpm_create(&b, c->device);
+        if (r) return ctx_fail(c, r, "hpm_run_scene_batched: problem context");
+        hpm_set_scene_workers(b, 1);
+        c->batch.push_back(b);
+    }
+    std::vector<hpm_ctx *> pc(c->batch.begin(), c->batch.begin() + n_problems);
+    std::vector<HpmParams> params(n_problems);
+    std::vector<int> levels(n_problems);
+    for (int p = 0; p < n_problems; ++p) {
+        const float *pimg[kMaxViews];
+        HpmCamera pcam[kMaxViews];
+        const int ref = ref_ids[p], ns = src_counts[p];
+        pimg[0] = img[ref];
+        pcam[0] = cams[ref];
+        for (int j = 0; j < ns; ++j) {
+            const int sv = src_ids[p * kMaxSrc + j];
+            pimg[j + 1] = img[sv];
+            pcam[j + 1] = cams[sv];
+        }
+        r = hpm_set_views(pc[p], pimg, pcam, ns + 1);
+        if (r) return ctx_fail(c, r, "hpm_run_scene_batched, problem %d: %s", p, hpm_last_error(pc[p]));
+        hpm_clear_prior(pc[p]);
+        ctx_reset_salt(pc[p]);
+        hpm_default_params(&params[p]);
+        params[p].depth_min = cams[ref].depth_min * 0.6f; /* InuputInitialization, HPM.cpp:553-554 */
+        params[p].depth_max = cams[ref].depth_max * 1.2f;
+        params[p].seed = o->seed + (uint64_t)p;
+        levels[p] = o->pyramid_levels >= 0 ? o->pyramid_levels : scale_levels_of(cams[ref].width, cams[ref].height);
+    }
+    std::vector<int> ww;
+    r = tune_tiles(c, pc, params, ww);
+    if (r) return r;
+
+    /* one plan (and graph) for the passes that cover every problem */
+    Plan all;
+    r = make_plan(c, pc, ww, all);
+    if (r) return r;
+    /* pass set A: the plain pass of every problem */
+    r = batch_pass(c, all, params);
+    if (r) return r;
+    /* the prior passes, levels aligned at the full scale */
+    if (o->planar_prior) {
+        const int kmax = *std::max_element(levels.begin(), levels.end());
+        for (int round = 0; round <= kmax; ++round) {
+            const int level = 2 - kmax + round; /* 0: 1/4 scale, 1: 1/2, 2: full */
+            std::vector<hpm_ctx *> sub;
+            std::vector<HpmParams> sp;
+            std::vector<int> sw;
+            for (int p = 0; p < n_problems; ++p) {
+                if (level < 2 - levels[p]) continue;
+                hpm_ctx *b = pc[p];
+                const size_t np = (size_t)b->cams[0].width * b->cams[0].height;
+                CK(ws_reserve_full(b, np), "flow workspace");
+                CK(flow_split_state(reinterpret_cast<const float4 *>(ctx_planes(b)), (int)np, b->flow.full_depth,
+                                    b->flow.full_normal, b->stream),
+                   "split");
+                r = flow_prior_from_maps(b, level, ctx_costs(b), params[p].depth_min, params[p].depth_max);
+                if (r) return ctx_fail(c, r, "hpm_run_scene_batched, problem %d: %s", p, hpm_last_error(b));
+                CK(cudaStreamSynchronize(b->stream), "prior");
+                HpmParams q = params[p];
+                q.planar_prior = 1;
+                sub.push_back(b);
+                sp.push_back(q);
+                sw.push_back(ww[p]);
+            }
+            if (sub.size() == pc.size()) {
+                r = batch_pass(c, all, sp);
+            } else {
+                Plan pl;
+                r = make_plan(c, sub, sw, pl);
+                if (!r) r = batch_pass(c, pl, sp);
+            }
+            if (r) return r;
+        }
+    }
+    for (int p = 0; p < n_problems; ++p) {
+        const int ref = ref_ids[p];
+        const size_t np = (size_t)cams[ref].width * cams[ref].height;
+        CK(flow_split_state(reinterpret_cast<const float4 *>(ctx_planes(pc[p])), (int)np, dep_a[ref], nrm[ref], s),
+           "split");
+        CK(cudaMemcpyAsync(cst[ref], ctx_costs(pc[p]), sizeof(float) * np, cudaMemcpyDeviceToDevice, s), "costs");
+    }
+    CK(cudaStreamSynchronize(s), "pass set A");
+
+    /* geometric iterations: each reads the previous iteration's maps of every view */
+    std::vector<float *> *src = &dep_a, *dst = &dep_g0;
+    for (int gi = 0; gi < o->geom_iterations; ++gi) {
+        std::vector<HpmParams> gp(n_problems);
+        for (int p = 0; p < n_problems; ++p) {
+            const int ref = ref_ids[p], ns = src_counts[p];
+            const float *pd[kMaxViews];
+            pd[0] = (*src)[ref];
+            for (int j = 0; j < ns; ++j) pd[j + 1] = (*src)[src_ids[p * kMaxSrc + j]];
+            r = hpm_set_geom_depths(pc[p], pd);
+            if (r) return ctx_fail(c, r, "hpm_run_scene_batched, problem %d: %s", p, hpm_last_error(pc[p]));
+            const int np = cams[ref].width * cams[ref].height;
+            k_pack_maps<<<(np + 255) / 256, 256, 0, s>>>(nrm[ref], (*src)[ref], np,
+                                                          reinterpret_cast<float4 *>(ctx_planes(pc[p])));
+            CK(cudaMemcpyAsync(ctx_costs(pc[p]), cst[ref], sizeof(float) * np, cudaMemcpyDeviceToDevice, s), "costs");
+            gp[p] = params[p];
+            gp[p].geom_consistency = 1;
+            gp[p].multi_geometry = gi >= 1;
+            gp[p].seed = o->seed + 1000003ull * (gi + 1) + (uint64_t)p;
+        }
+        CK(cudaStreamSynchronize(s), "geometric set-up");
+        r = batch_pass(c, all, gp);
+        if (r) return r;
+        for (int p = 0; p < n_problems; ++p) {
+            const int ref = ref_ids[p];
+            const size_t np = (size_t)cams[ref].width * cams[ref].height;
+            CK(flow_split_state(reinterpret_cast<const float4 *>(ctx_planes(pc[p])), (int)np, (*dst)[ref], nrm[ref],
+                                s),
+               "split");
+            CK(cudaMemcpyAsync(cst[ref], ctx_costs(pc[p]), sizeof(float) * np, cudaMemcpyDeviceToDevice, s), "costs");
+        }
+        CK(cudaStreamSynchronize(s), "geometric iteration");
+        src = dst;
+        dst = (dst == &dep_g0) ? &dep_g1 : &dep_g0;
+    }
+    for (int v = 0; v < n_views; ++v) {
+        const size_t np = (size_t)cams[v].width * cams[v].height;
+        if (out_depths && out_depths[v])
+            CK(cudaMemcpyAsync(out_depths[v], (*src)[v], sizeof(float) * np, cudaMemcpyDefault, s), "out");
+        if (out_normals && out_normals[v])
+            CK(cudaMemcpyAsync(out_normals[v], nrm[v], sizeof(float) * 3 * np, cudaMemcpyDefault, s), "out");
+        if (out_costs && out_costs[v])
+            CK(cudaMemcpyAsync(out_costs[v], cst[v], sizeof(float) * np, cudaMemcpyDefault, s), "out");
+    }
+    CK(cudaStreamSynchronize(s), "hpm_run_scene_batched");
+    return HPM_OK;
+}

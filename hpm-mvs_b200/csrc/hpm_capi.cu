@@ -199,6 +199,8 @@ int hpm_destroy(hpm_ctx *c)
     c->peer = nullptr;
     if (c->coarse) hpm_destroy(c->coarse);
     c->coarse = nullptr;
+    for (hpm_ctx *b : c->batch) hpm_destroy(b);
+    c->batch.clear();
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
     for (int i = 0; i < kMaxViews; ++i) {
@@ -356,6 +358,38 @@ int hpm_clear_prior(hpm_ctx *c)
     c->has_prior = false;
     return HPM_OK;
 }
+
+/* The kernel arguments of one pass of context c with parameters p (checks
+ * as hpm_run_patchmatch; takes the pass's random-stream salt). */
+extern "C++" int ctx_pass_args(hpm_ctx *c, const HpmParams *p, PMArgs *out)
+{
+    if (!c) return HPM_ERR_ARG;
+    if (!p) return fail(c, HPM_ERR_ARG, "hpm_run_patchmatch: null params");
+    if (c->n < 2) return fail(c, HPM_ERR_STATE, "hpm_run_patchmatch before hpm_set_views");
+    if (p->patch_size != 11 || p->radius_increment != 2)
+        return fail(c, HPM_ERR_ARG, "hpm_run_patchmatch: only the reference window (11, stride 2) is built");
+    if (p->geom_consistency && !c->has_depth)
+        return fail(c, HPM_ERR_STATE, "geometric consistency needs hpm_set_geom_depths");
+    if (p->planar_prior && !c->has_prior) return fail(c, HPM_ERR_STATE, "planar prior needs hpm_set_prior");
+    if (!(p->depth_max > p->depth_min)) return fail(c, HPM_ERR_ARG, "depth range is empty");
+    if (p->top_k < 1 || p->top_k > kMaxSrc) return fail(c, HPM_ERR_ARG, "top_k outside [1, %d]", kMaxSrc);
+    PMArgs a = make_args(c);
+    a.dmin = p->depth_min;
+    a.dmax = p->depth_max;
+    a.geom = p->geom_consistency ? 1 : 0;
+    a.prior = p->planar_prior ? 1 : 0;
+    a.sigma_spatial = p->sigma_spatial;
+    a.sigma_color = p->sigma_color;
+    a.top_k = p->top_k;
+    a.seed_lo = (uint32_t)p->seed;
+    a.seed_hi = (uint32_t)(p->seed >> 32);
+    a.salt = c->pass_counter++;
+    c->has_state = true;
+    *out = a;
+    return HPM_OK;
+}
+
+extern "C++" void ctx_reset_salt(hpm_ctx *c) { c->pass_counter = 0; }
 
 /* One pass: initialisation, `half_steps` red/black half-steps (the
  * reference runs 2 per iteration), then optionally depth/normal conversion

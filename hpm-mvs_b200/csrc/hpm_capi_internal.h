@@ -114,6 +114,10 @@ struct hpm_ctx {
     /* prior-net form: the context that holds a problem's 1/4-scale views,
      * so that this one keeps its full-scale views and texture arrays */
     hpm_ctx *coarse = nullptr;
+    /* batched form: one context per problem of the last batched scene, and
+     * the autotuned half-step tile width per view size (width << 32 | rows) */
+    std::vector<hpm_ctx *> batch;
+    std::vector<std::pair<long long, int>> tile_ww;
     hpm::FlowWorkspace flow;
     float *d_scene = nullptr; /* hpm_run_scene's per-view maps, grown on demand */
     size_t scene_cap = 0;
@@ -149,6 +153,11 @@ cudaError_t ws_reserve_grid(hpm_ctx *c, size_t npts, size_t ncells);
 cudaError_t ws_reserve_full(hpm_ctx *c, size_t npx);
 cudaError_t ws_reserve_coarse(hpm_ctx *c, size_t npx);
 void ws_free(hpm_ctx *c);
+/* the arguments of one pass (validated as hpm_run_patchmatch; takes the
+ * pass's random-stream salt) for a batched launch */
+int ctx_pass_args(hpm_ctx *c, const HpmParams *p, hpm::PMArgs *out);
+/* restart the context's pass numbering (the salt of its random streams) */
+void ctx_reset_salt(hpm_ctx *c);
 /* hypotheses written on the device count as the pass state */
 void ctx_mark_state(hpm_ctx *c);
 cudaError_t net_reserve(hpm_ctx *c, size_t coarse_px, size_t coarse_img_floats);

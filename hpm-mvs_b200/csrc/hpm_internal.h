@@ -86,4 +86,25 @@ cudaError_t launch_jbu(const float *guide, int cols, int rows, const float *coar
 
 int rows_covered(int H);
 
+/* A batch of problems for one persistent launch: problem p's PMArgs sit in
+ * args[p] (device memory) and its work items are [first[p], first[p + 1]):
+ * item i of problem p is tile (i % gx[p], i / gx[p]); half-step tiles have
+ * warps of ww[p] pixels of one colour per row over 32 / ww[p] rows, the
+ * initialisation's tiles are 32 x 2 pixels. */
+struct BatchList {
+    const PMArgs *args;
+    const int *first; /* [n + 1] */
+    const int *gx;    /* [n] */
+    const int *ww;    /* [n], half-step lists only */
+    int n;
+    int total;
+};
+
+/* Persistent launches over a batch (hpm_pm.cu); ctas = 0 picks the number
+ * of CTAs that fit on the device at once. */
+cudaError_t launch_batch_init(const BatchList &b, int ctas, cudaStream_t s);
+cudaError_t launch_batch_propagate(const BatchList &b, int smax, int iter, int color, int ctas, cudaStream_t s);
+/* grid width of problem a's half-step tiles of width ww, and their count */
+int half_step_tiles(int W, int rows_cov, int ww, int *gx);
+
 }  // namespace hpm

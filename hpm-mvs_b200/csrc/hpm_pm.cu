@@ -54,12 +54,20 @@ constexpr int kWarpW = HPM_WARP_W;
 constexpr int kWarpH = 32 / kWarpW;
 static_assert(kWarpW * kWarpH == 32 && kBlock == 64, "two warps per block");
 
-/* (px, py) of this thread in a half-step of `color` */
+/* (px, py) of this thread in a half-step of `color`, for the block's tile
+ * (bx, by) of tiles whose warps cover ww pixels of one colour per row over
+ * 32 / ww rows (the plain launches use ww = kWarpW and the block index; the
+ * batched launches take both from their work list) */
+__device__ __forceinline__ void half_step_pixel_at(int bx, int by, int ww, int color, int &px, int &py)
+{
+    const int lane = threadIdx.x, wv = threadIdx.y, wh = 32 / ww;
+    py = by * (2 * wh) + wv * wh + lane / ww;
+    px = bx * (2 * ww) + 2 * (lane % ww) + ((py + color) & 1);
+}
+
 __device__ __forceinline__ void half_step_pixel(int color, int &px, int &py)
 {
-    const int lane = threadIdx.x, wv = threadIdx.y;
-    py = blockIdx.y * (2 * kWarpH) + wv * kWarpH + lane / kWarpW;
-    px = blockIdx.x * (2 * kWarpW) + 2 * (lane % kWarpW) + ((py + color) & 1);
+    half_step_pixel_at(blockIdx.x, blockIdx.y, kWarpW, color, px, py);
 }
 #ifndef HPM_CV_INLINE
 #define HPM_CV_INLINE __noinline__
@@ -541,13 +549,8 @@ __device__ __forceinline__ float *cache_at(const PMArgs &a, int v, int center)
 }
 
 /* RandomInitialization, HPM.cu:510-558.  One thread per pixel. */
-__global__ void __launch_bounds__(kBlock) k_init(const __grid_constant__ PMArgs a)
+__device__ __forceinline__ void init_body(const PMArgs &a, int px, int py, WinWeight *sWW, float *sCV, int tid)
 {
-    __shared__ WinWeight sWW[kTaps * kBlock];
-    __shared__ float sCV[kMaxSrc * kBlock];
-    const int tid = threadIdx.y * kBlockX + threadIdx.x;
-    const int px = blockIdx.x * kBlockX + threadIdx.x;
-    const int py = blockIdx.y * kBlockY + threadIdx.y;
     if (px >= a.W || py >= a.H) return;
     const int center = py * a.W + px;
     const HpmCamera &cam = a.cam[0];
@@ -588,6 +591,14 @@ __global__ void __launch_bounds__(kBlock) k_init(const __grid_constant__ PMArgs 
     a.views[center] = sel;
     if (a.cost_cache)
         for (int v = 0; v < a.n - 1; ++v) *cache_at(a, v, center) = cv[v * kBlock];
+}
+
+__global__ void __launch_bounds__(kBlock) k_init(const __grid_constant__ PMArgs a)
+{
+    __shared__ WinWeight sWW[kTaps * kBlock];
+    __shared__ float sCV[kMaxSrc * kBlock];
+    const int tid = threadIdx.y * kBlockX + threadIdx.x;
+    init_body(a, blockIdx.x * kBlockX + threadIdx.x, blockIdx.y * kBlockY + threadIdx.y, sWW, sCV, tid);
 }
 
 /* Validity of the first site of direction k at extension round r (HPM.cu:1252-1445 and the
@@ -720,13 +731,8 @@ __device__ __forceinline__ float dir_cost(const PMArgs &a, uint32_t code, int k,
     return (k == 0 && v == 0) ? 2.0f : 0.0f;
 }
 
-__global__ void __launch_bounds__(kBlock, HPM_P1_MIN_BLOCKS) k_prop_dirs(const __grid_constant__ PMArgs a, int iter,
-                                                                          int color)
+__device__ __forceinline__ void prop_dirs_body(const PMArgs &a, int iter, int px, int py, WinPair *sWW, int tid)
 {
-    __shared__ WinPair sWW[kTaps * kBlock];
-    const int tid = threadIdx.y * kBlockX + threadIdx.x;
-    int px, py;
-    half_step_pixel(color, px, py);
     if (px >= a.W || py >= a.rows_cov) return;
     const int W = a.W, H = a.H, S = a.n - 1;
     const size_t npx = (size_t)W * H;
@@ -832,18 +838,23 @@ __global__ void __launch_bounds__(kBlock, HPM_P1_MIN_BLOCKS) k_prop_dirs(const _
     a.cand_flags[center] = code;
 }
 
-/* PROP: the prior-net form, whose network proposal a.proposals[center] is a
- * sixth refinement candidate, scored by the same NCC (and prior terms) as the
- * other five and accepted by the same rule.  It takes no random draws, so
- * the random stream of the other candidates is unchanged. */
-template <int SMAX, bool PROP>
-__global__ void __launch_bounds__(kBlock, HPM_P2_MIN_BLOCKS) k_prop_refine(const __grid_constant__ PMArgs a, int iter,
-                                                                            int color)
+__global__ void __launch_bounds__(kBlock, HPM_P1_MIN_BLOCKS) k_prop_dirs(const __grid_constant__ PMArgs a, int iter,
+                                                                          int color)
 {
     __shared__ WinPair sWW[kTaps * kBlock];
     const int tid = threadIdx.y * kBlockX + threadIdx.x;
     int px, py;
     half_step_pixel(color, px, py);
+    prop_dirs_body(a, iter, px, py, sWW, tid);
+}
+
+/* PROP: the prior-net form, whose network proposal a.proposals[center] is a
+ * sixth refinement candidate, scored by the same NCC (and prior terms) as the
+ * other five and accepted by the same rule.  It takes no random draws, so
+ * the random stream of the other candidates is unchanged. */
+template <int SMAX, bool PROP>
+__device__ __forceinline__ void prop_refine_body(const PMArgs &a, int iter, int px, int py, WinPair *sWW, int tid)
+{
     if (px >= a.W || py >= a.rows_cov) return;
     const int W = a.W, S = a.n - 1;
     const size_t npx = (size_t)W * a.H;
@@ -1164,6 +1175,17 @@ __global__ void __launch_bounds__(kBlock, HPM_P2_MIN_BLOCKS) k_prop_refine(const
     }
 #undef FLAG
 }
+
+template <int SMAX, bool PROP>
+__global__ void __launch_bounds__(kBlock, HPM_P2_MIN_BLOCKS) k_prop_refine(const __grid_constant__ PMArgs a, int iter,
+                                                                            int color)
+{
+    __shared__ WinPair sWW[kTaps * kBlock];
+    const int tid = threadIdx.y * kBlockX + threadIdx.x;
+    int px, py;
+    half_step_pixel(color, px, py);
+    prop_refine_body<SMAX, PROP>(a, iter, px, py, sWW, tid);
+}
 #undef CAG
 
 /* GetDepthandNormal, HPM.cu:1751-1764 */
@@ -1279,6 +1301,85 @@ __global__ void k_tap_samples(const __grid_constant__ PMArgs a, const float4 *pl
         for (int j = -5; j < 6; j += 2, ++t) out[(size_t)k * kTaps + t] = tap_sample(a.view[v].tex, H, fpx, fpy, i, j);
 }
 
+/* ------------------------------------------------------------------ */
+/* Batched persistent launches: every problem of a batch in one launch  */
+/* ------------------------------------------------------------------ */
+
+/* the problem that owns work item id: the largest p with first[p] <= id */
+__device__ __forceinline__ int batch_problem(const int *first, int n, int id)
+{
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (first[mid] <= id)
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    return lo;
+}
+
+__global__ void __launch_bounds__(kBlock) k_init_batch(const __grid_constant__ BatchList b)
+{
+    __shared__ WinWeight sWW[kTaps * kBlock];
+    __shared__ float sCV[kMaxSrc * kBlock];
+    const int tid = threadIdx.y * kBlockX + threadIdx.x;
+    for (int id = blockIdx.x; id < b.total; id += gridDim.x) {
+        const int p = batch_problem(b.first, b.n, id), local = id - b.first[p];
+        const int bx = local % b.gx[p], by = local / b.gx[p];
+        init_body(b.args[p], bx * kBlockX + threadIdx.x, by * kBlockY + threadIdx.y, sWW, sCV, tid);
+    }
+}
+
+__global__ void __launch_bounds__(kBlock, HPM_P1_MIN_BLOCKS) k_prop_dirs_batch(const __grid_constant__ BatchList b,
+                                                                                int iter, int color)
+{
+    __shared__ WinPair sWW[kTaps * kBlock];
+    const int tid = threadIdx.y * kBlockX + threadIdx.x;
+    for (int id = blockIdx.x; id < b.total; id += gridDim.x) {
+        const int p = batch_problem(b.first, b.n, id), local = id - b.first[p];
+        int px, py;
+        half_step_pixel_at(local % b.gx[p], local / b.gx[p], b.ww[p], color, px, py);
+        prop_dirs_body(b.args[p], iter, px, py, sWW, tid);
+    }
+}
+
+template <int SMAX>
+__global__ void __launch_bounds__(kBlock, HPM_P2_MIN_BLOCKS) k_prop_refine_batch(const __grid_constant__ BatchList b,
+                                                                                  int iter, int color)
+{
+    __shared__ WinPair sWW[kTaps * kBlock];
+    const int tid = threadIdx.y * kBlockX + threadIdx.x;
+    for (int id = blockIdx.x; id < b.total; id += gridDim.x) {
+        const int p = batch_problem(b.first, b.n, id), local = id - b.first[p];
+        int px, py;
+        half_step_pixel_at(local % b.gx[p], local / b.gx[p], b.ww[p], color, px, py);
+        prop_refine_body<SMAX, false>(b.args[p], iter, px, py, sWW, tid);
+    }
+}
+
+template <typename K>
+int resident_ctas(K kern)
+{
+    int dev = 0, sms = 0, per_sm = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) !=
+                                                  cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kBlock, 0) != cudaSuccess)
+        return 148 * 8;
+    return sms * (per_sm > 0 ? per_sm : 1);
+}
+
+template <int SMAX>
+cudaError_t launch_batch_prop_t(const BatchList &b, int iter, int color, int ctas, cudaStream_t s)
+{
+    const dim3 blk(kBlockX, kBlockY);
+    const int c1 = ctas > 0 ? ctas : resident_ctas(k_prop_dirs_batch);
+    k_prop_dirs_batch<<<b.total < c1 ? b.total : c1, blk, 0, s>>>(b, iter, color);
+    const int c2 = ctas > 0 ? ctas : resident_ctas(k_prop_refine_batch<SMAX>);
+    k_prop_refine_batch<SMAX><<<b.total < c2 ? b.total : c2, blk, 0, s>>>(b, iter, color);
+    return cudaGetLastError();
+}
+
 template <int SMAX>
 cudaError_t launch_prop_t(const PMArgs &a, int iter, int color, cudaStream_t s)
 {
@@ -1322,6 +1423,31 @@ cudaError_t launch_propagate(const PMArgs &a, int iter, int color, cudaStream_t 
     if (S <= 12) return launch_prop_t<12>(a, iter, color, s);
     if (S <= 16) return launch_prop_t<16>(a, iter, color, s);
     return launch_prop_t<kMaxSrc>(a, iter, color, s);
+}
+
+int half_step_tiles(int W, int rows_cov, int ww, int *gx)
+{
+    const int wh = 32 / ww;
+    *gx = (W + 2 * ww - 1) / (2 * ww);
+    return *gx * ((rows_cov + 2 * wh - 1) / (2 * wh));
+}
+
+cudaError_t launch_batch_init(const BatchList &b, int ctas, cudaStream_t s)
+{
+    if (b.total <= 0) return cudaSuccess;
+    const int c = ctas > 0 ? ctas : resident_ctas(k_init_batch);
+    k_init_batch<<<b.total < c ? b.total : c, dim3(kBlockX, kBlockY), 0, s>>>(b);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_batch_propagate(const BatchList &b, int smax, int iter, int color, int ctas, cudaStream_t s)
+{
+    if (b.total <= 0) return cudaSuccess;
+    if (smax <= 4) return launch_batch_prop_t<4>(b, iter, color, ctas, s);
+    if (smax <= 8) return launch_batch_prop_t<8>(b, iter, color, ctas, s);
+    if (smax <= 12) return launch_batch_prop_t<12>(b, iter, color, ctas, s);
+    if (smax <= 16) return launch_batch_prop_t<16>(b, iter, color, ctas, s);
+    return launch_batch_prop_t<kMaxSrc>(b, iter, color, ctas, s);
 }
 
 cudaError_t launch_depth_normal_filter(const PMArgs &a, float4 *planes, const float *costs, cudaStream_t s)

@@ -41,7 +41,7 @@ EXPORTED = [
     "hpm_fuse", "hpm_write_ply", "hpm_read_bgr8", "hpm_set_scene_workers", "hpm_resize_linear_u8",
     "hpm_raster_triangles", "hpm_knn6", "hpm_tap_samples", "hpm_net_pack_weights", "hpm_net_conv3x3",
     "hpm_net_conv_wgrad", "hpm_run_scene_net", "hpm_net_coarse_inputs", "hpm_net_targets", "hpm_net_loss",
-    "hpm_net_adam",
+    "hpm_net_adam", "hpm_run_scene_batched",
 ]
 
 
@@ -239,7 +239,7 @@ class Context:
         return depth, normal, cost, prior
 
     def run_scene(self, images, cams, pairs, *, planar_prior=True, geom_iterations=2, seed=0, pyramid_levels=-1,
-                  images_are_device=False, outputs=True, extra_maps=False, net=None):
+                  images_are_device=False, outputs=True, extra_maps=False, net=None, batched=False):
         """The reference's main() over a scene.  images: per-view float32 [H, W]
         arrays, or device pointers (ints) with images_are_device; pairs:
         [(ref, [sources])].  outputs: True to return new per-view (depth,
@@ -248,7 +248,8 @@ class Context:
         extra_maps (with outputs=True): also return each view's pass-set-A
         depth and prior depth (hpm_run_scene_ex), five lists in all.
         net: an HpmNetWeights (priornet.Net.weights()) to run the prior-net
-        form (hpm_run_scene_net) instead of the plain form."""
+        form (hpm_run_scene_net) instead of the plain form.  batched: the
+        batched form (hpm_run_scene_batched)."""
         n = len(cams)
         cams = np.ascontiguousarray(cams, dtype=CAMERA_DTYPE)
         if images_are_device:
@@ -281,7 +282,13 @@ class Context:
             arrs = [(ctypes.c_void_p * n)(*[o_[k].ctypes.data for o_ in outs]) for k in range(3)]
         else:
             arrs = [None, None, None]
-        if net is not None:
+        if batched:
+            if extra_maps or net is not None:
+                raise ValueError("run_scene: the batched form has no extra maps and no network")
+            self._check(lib().hpm_run_scene_batched(self._h, n, img_arr, _p(cams), len(pairs), _p(refs), _p(counts),
+                                                    _p(srcs), ctypes.byref(o), arrs[0], arrs[1], arrs[2]),
+                        "hpm_run_scene_batched")
+        elif net is not None:
             if extra_maps:
                 raise ValueError("run_scene: extra_maps is not available in the prior-net form")
             self._check(lib().hpm_run_scene_net(self._h, n, img_arr, _p(cams), len(pairs), _p(refs), _p(counts),

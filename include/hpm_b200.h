@@ -295,6 +295,19 @@ int hpm_run_scene_net(hpm_ctx *ctx, int n_views, const float *const *images, con
                       const HpmNetWeights *net, float *const *out_depths, float *const *out_normals,
                       float *const *out_costs);
 
+/* hpm_run_scene in the batched form: every problem of the scene advances
+ * together, one persistent launch per kernel and half-step covering the
+ * tiles of all problems (of any sizes); a pass is captured once as a CUDA
+ * graph and replayed; the half-step tile shape is tuned per view size.  Pass
+ * set A equals hpm_process_problem's on a fresh context per problem; the
+ * geometric iterations read the previous iteration's maps of every view
+ * (the reference's in-place order, main.cpp:662-674, would serialise the
+ * problems).  Keeps one context per problem inside ctx for later scenes. */
+int hpm_run_scene_batched(hpm_ctx *ctx, int n_views, const float *const *images, const HpmCamera *cams,
+                          int n_problems, const int *ref_ids, const int *src_counts, const int *src_ids,
+                          const HpmSceneOpts *opts, float *const *out_depths, float *const *out_normals,
+                          float *const *out_costs);
+
 /* The network's input for one problem (views as for hpm_set_views, full
  * scale): the coarse stage of the prior-net form (1/4-scale plain pass with
  * seed, coarse planar prior), written to x0 ([*ch][*cw][16] BF16, host or
