@@ -31,6 +31,7 @@
  *    host synchronisation (the reference synchronises after every launch).
  */
 #include <cfloat>
+#include <cstdlib>
 
 #include "hpm_internal.h"
 
@@ -399,6 +400,79 @@ __device__ __forceinline__ float ncc(const PMArgs &a, int v, int px, int py, flo
     const float covar = sum_ref_src - rs.mean * sum_src;
     const float vv = sqrtf(rs.var * var_src);
     return fmaxf(0.0f, fminf(2.0f, 1.0f - covar / vv));
+}
+
+/* ncc() of two planes with the same depth at the pixel (the window centres
+ * coincide in every source view) in one tap loop: each tap fetches both
+ * samples, so that two texture requests are in flight and the second finds
+ * most of its texels in L1.  Each NCC keeps ncc()'s own accumulation order,
+ * so both results equal ncc()'s bit for bit. */
+template <typename Win>
+__device__ __forceinline__ float2 ncc_pair(const PMArgs &a, int v, int px, int py, float4 h0, float4 h1,
+                                           const Win *sWW, int tid, const RefStats &rs)
+{
+    const HpmCamera &sc = a.cam[v];
+    float H0[9], H1[9];
+    homography(a.cam[0], sc, a.pair[v], h0, H0);
+    homography(a.cam[0], sc, a.pair[v], h1, H1);
+    const float fpx = (float)px, fpy = (float)py;
+    const float2 p0 = warp(H0, fpx, fpy), p1 = warp(H1, fpx, fpy);
+    const bool in0 = !(p0.x >= sc.width || p0.x < 0.0f || p0.y >= sc.height || p0.y < 0.0f);
+    const bool in1 = !(p1.x >= sc.width || p1.x < 0.0f || p1.y >= sc.height || p1.y < 0.0f);
+    if ((!in0 && !in1) || rs.var < 1e-5f) return make_float2(2.0f, 2.0f);
+    const cudaTextureObject_t tex = a.view[v].tex;
+    float s0 = 0.0f, ss0 = 0.0f, rs0 = 0.0f, s1 = 0.0f, ss1 = 0.0f, rs1 = 0.0f;
+    int t = 0;
+#pragma unroll
+    for (int i = -5; i < 6; i += 2) {
+        float a0 = 0.0f, b0 = 0.0f, c0 = 0.0f, a1 = 0.0f, b1 = 0.0f, c1 = 0.0f;
+#pragma unroll
+        for (int j = -5; j < 6; j += 2, ++t) {
+            const float sp0 = in0 ? tap_sample(tex, H0, fpx, fpy, i, j) : 0.0f;
+            const float sp1 = in1 ? tap_sample(tex, H1, fpx, fpy, i, j) : 0.0f;
+            float2 ww;
+            if constexpr (sizeof(Win) == sizeof(float)) {
+                const float wt = sWW[t * kBlock + tid];
+                ww = make_float2(wt, wt * texel(a.view[0].img, a.view[0].w, a.view[0].h, px + i, py + j));
+            } else {
+                ww = sWW[t * kBlock + tid];
+            }
+            a0 += ww.x * sp0;
+            b0 += ww.x * sp0 * sp0;
+            c0 += ww.y * sp0;
+            a1 += ww.x * sp1;
+            b1 += ww.x * sp1 * sp1;
+            c1 += ww.y * sp1;
+        }
+        s0 += a0;
+        ss0 += b0;
+        rs0 += c0;
+        s1 += a1;
+        ss1 += b1;
+        rs1 += c1;
+    }
+    float2 out = make_float2(2.0f, 2.0f);
+    if (in0) {
+        s0 *= rs.inv;
+        ss0 *= rs.inv;
+        rs0 *= rs.inv;
+        const float var0 = ss0 - s0 * s0;
+        if (!(var0 < 1e-5f)) {
+            const float cov = rs0 - rs.mean * s0;
+            out.x = fmaxf(0.0f, fminf(2.0f, 1.0f - cov / sqrtf(rs.var * var0)));
+        }
+    }
+    if (in1) {
+        s1 *= rs.inv;
+        ss1 *= rs.inv;
+        rs1 *= rs.inv;
+        const float var1 = ss1 - s1 * s1;
+        if (!(var1 < 1e-5f)) {
+            const float cov = rs1 - rs.mean * s1;
+            out.y = fmaxf(0.0f, fminf(2.0f, 1.0f - cov / sqrtf(rs.var * var1)));
+        }
+    }
+    return out;
 }
 
 /* One NCC window for the loops that score several candidates view by view
@@ -852,7 +926,7 @@ __global__ void __launch_bounds__(kBlock, HPM_P1_MIN_BLOCKS) k_prop_dirs(const _
  * sixth refinement candidate, scored by the same NCC (and prior terms) as the
  * other five and accepted by the same rule.  It takes no random draws, so
  * the random stream of the other candidates is unchanged. */
-template <int SMAX, bool PROP>
+template <int SMAX, bool PROP, bool PAIR = false>
 __device__ __forceinline__ void prop_refine_body(const PMArgs &a, int iter, int px, int py, WinPair *sWW, int tid)
 {
     if (px >= a.W || py >= a.rows_cov) return;
@@ -1125,8 +1199,24 @@ __device__ __forceinline__ void prop_refine_body(const PMArgs &a, int iter, int 
         for (int v = 0; v < S; ++v) {
             const bool selected = (tsv >> v) & 1u;
             const float w = (float)((v < 16 ? (vw_lo >> (4 * v)) : (vw_hi >> (4 * (v - 16)))) & 15ull);
+            if constexpr (PAIR) {
+                /* candidates 0 and 2 share the random depth: one tap loop */
+                const float2 c02 = ncc_pair(a, v + 1, px, py, cand[0], cand[2], sWW, tid, rs);
+#pragma unroll
+                for (int q = 0; q < 2; ++q) {
+                    const int i = 2 * q;
+                    const float c = q ? c02.y : c02.x;
+                    CAG(kRefineRow + i, v) = c;
+                    if (selected) {
+                        if (a.geom)
+                            tc[i] += w * (c + 0.1f * geom_cost(a, v + 1, cand[i], px, py));
+                        else
+                            tc[i] += w * c;
+                    }
+                }
+            }
 #pragma unroll 1
-            for (int k = 0; k < NC; ++k) {
+            for (int k = PAIR ? 2 : 0; k < NC; ++k) {
                 /* candidates 0 and 2 share the random depth, hence the window
                  * centre in every source view; 1, 3 and 4 sit at or near the
                  * current depth: scoring 0, 2, 1, 3, 4 keeps windows with the
@@ -1176,7 +1266,7 @@ __device__ __forceinline__ void prop_refine_body(const PMArgs &a, int iter, int 
 #undef FLAG
 }
 
-template <int SMAX, bool PROP>
+template <int SMAX, bool PROP, bool PAIR>
 __global__ void __launch_bounds__(kBlock, HPM_P2_MIN_BLOCKS) k_prop_refine(const __grid_constant__ PMArgs a, int iter,
                                                                             int color)
 {
@@ -1184,7 +1274,7 @@ __global__ void __launch_bounds__(kBlock, HPM_P2_MIN_BLOCKS) k_prop_refine(const
     const int tid = threadIdx.y * kBlockX + threadIdx.x;
     int px, py;
     half_step_pixel(color, px, py);
-    prop_refine_body<SMAX, PROP>(a, iter, px, py, sWW, tid);
+    prop_refine_body<SMAX, PROP, PAIR>(a, iter, px, py, sWW, tid);
 }
 #undef CAG
 
@@ -1380,15 +1470,29 @@ cudaError_t launch_batch_prop_t(const BatchList &b, int iter, int color, int cta
     return cudaGetLastError();
 }
 
+/* HPM_REFINE_PAIR=1 in the environment scores the two random-depth
+ * refinement candidates in one tap loop (ncc_pair; same results) */
+bool refine_pair()
+{
+    static const bool on = [] {
+        const char *e = getenv("HPM_REFINE_PAIR");
+        return e && e[0] == '1';
+    }();
+    return on;
+}
+
 template <int SMAX>
 cudaError_t launch_prop_t(const PMArgs &a, int iter, int color, cudaStream_t s)
 {
     dim3 grid((a.W + 2 * kWarpW - 1) / (2 * kWarpW), (a.rows_cov + 2 * kWarpH - 1) / (2 * kWarpH));
     k_prop_dirs<<<grid, dim3(kBlockX, kBlockY), 0, s>>>(a, iter, color);
+    const dim3 b(kBlockX, kBlockY);
     if (a.proposals)
-        k_prop_refine<SMAX, true><<<grid, dim3(kBlockX, kBlockY), 0, s>>>(a, iter, color);
+        k_prop_refine<SMAX, true, false><<<grid, b, 0, s>>>(a, iter, color);
+    else if (refine_pair())
+        k_prop_refine<SMAX, false, true><<<grid, b, 0, s>>>(a, iter, color);
     else
-        k_prop_refine<SMAX, false><<<grid, dim3(kBlockX, kBlockY), 0, s>>>(a, iter, color);
+        k_prop_refine<SMAX, false, false><<<grid, b, 0, s>>>(a, iter, color);
     return cudaGetLastError();
 }
 

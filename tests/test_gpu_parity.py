@@ -317,3 +317,37 @@ def test_max_sources():
         sc34 = syn.make_scene(9, 16, 12, 34, n_planes=1, arc_step_deg=1.0)
         ctx.set_views([i.astype(np.float32) for i in sc34.images], sc34.cams)
 
+
+
+_PAIR_SCRIPT = r"""
+import sys, numpy as np
+sys.path[:0] = sys.argv[1:3]
+import hpm_b200 as hb, synthetic as syn
+sc = syn.make_scene(13, 200, 150, 11, n_planes=8, n_spheres=2, arc_step_deg=3.0)
+imgs, cams = syn.view_set(sc, 5)
+dmin, dmax = sc.depth_min * 0.6, sc.depth_max * 1.2
+with hb.Context() as ctx:
+    ctx.set_views(imgs, cams)
+    ctx.run_partial(hb.default_params(dmin, dmax, seed=9), 4, False)
+    p, c = ctx.get_result()
+np.savez(sys.argv[3], planes=p, costs=c)
+"""
+
+
+def test_paired_refinement_scoring_is_bit_identical(tmp_path):
+    """The two random-depth refinement candidates scored in one tap loop
+    (HPM_REFINE_PAIR=1) and one at a time give the same bits after four
+    half-steps at 10 sources (k_prop_refine<12>)."""
+    import subprocess
+    import sys
+
+    from conftest import ORACLE, PKG
+
+    outs = {}
+    for m in ("0", "1"):
+        path = tmp_path / f"pair{m}.npz"
+        env = dict(os.environ, HPM_REFINE_PAIR=m)
+        subprocess.run([sys.executable, "-c", _PAIR_SCRIPT, PKG, ORACLE, str(path)], check=True, env=env)
+        outs[m] = np.load(path)
+    np.testing.assert_array_equal(outs["1"]["planes"], outs["0"]["planes"])
+    np.testing.assert_array_equal(outs["1"]["costs"], outs["0"]["costs"])
