@@ -449,13 +449,14 @@ def prior_net_form(args, dist, ctx, sc, d_ptrs, pairs, stream, plain_ms, plain_a
     meta = dict(np.load(priornet.WEIGHTS_FILE))
     geom = int(meta["geom_iterations"]) if "geom_iterations" in meta else WORKLOAD["geom_iterations"]
     extra = int(meta["extra_passes"]) if "extra_passes" in meta else 0
+    prior = int(meta["prior"]) if "prior" in meta else 1
     wts = net.weights()
     w = WORKLOAD
     npx = w["n_views"] * w["width"] * w["height"]
 
     def step(seed, outputs=False):
         return ctx.run_scene(d_ptrs, sc.cams, pairs, seed=seed, images_are_device=True, outputs=outputs,
-                             geom_iterations=geom, pyramid_levels=extra, net=wts)
+                             geom_iterations=geom, pyramid_levels=extra, planar_prior=prior, net=wts)
 
     for i in range(args.warmup):
         step(2000 + i)
@@ -473,7 +474,7 @@ def prior_net_form(args, dist, ctx, sc, d_ptrs, pairs, stream, plain_ms, plain_a
     acc = scene_accuracy(sc, dict(enumerate(out_np[0])), dict(enumerate(out_np[1])))
     value = job_mpix_per_s(dist.world, 1, npx, ms)
     return {"value": value, "unit": "depth Mpix/s", "ms_per_step": ms, "geom_iterations": geom,
-            "extra_full_scale_prior_passes": extra,
+            "extra_full_scale_prior_passes": extra, "proposal_as_planar_prior": prior == 2,
             "speedup_vs_plain": plain_ms / ms, "accuracy": acc,
             "px_relerr_lt_1pct_minus_plain": acc["px_relerr_lt_1pct"] - plain_acc["px_relerr_lt_1pct"],
             "network": "4 layers of 3x3 conv, 32 channels, BF16 on tcgen05 (FP32 accumulation in TMEM), "

@@ -175,5 +175,6 @@ int flow_level_prior(hpm_ctx *c, const HpmCamera &cam, const float *d_cost, cons
 int flow_prior_from_maps(hpm_ctx *c, int level, const float *d_cost, float dmin, float dmax);
 /* hpm_priornet.cu */
 int net_problem(hpm_ctx *c, int n, const float *const *images, const HpmCamera *cams, const HpmNetWeights *net,
-                uint64_t seed, int extra_passes, float *depth_out, float *normal_out, float *cost_out);
+                uint64_t seed, int extra_passes, int prior_mode, float *depth_out, float *normal_out,
+                float *cost_out);
 }  // namespace hpm

@@ -438,8 +438,8 @@ static int run_scene_impl(hpm_ctx *c, int n_views, const float *const *images, c
                     HpmCamera pcam[kMaxViews];
                     const int n = gather(p, pimg, pcam), ref = ref_ids[p];
                     rr = net_problem(cc, n, pimg, pcam, net, o->seed + (uint64_t)p,
-                                     o->pyramid_levels > 0 ? o->pyramid_levels : 0, m.depth_a[ref], m.normal[ref],
-                                     m.cost[ref]);
+                                     o->pyramid_levels > 0 ? o->pyramid_levels : 0, o->planar_prior, m.depth_a[ref],
+                                     m.normal[ref], m.cost[ref]);
                     if (rr == HPM_OK && out_prior_depths && out_prior_depths[ref])
                         rr = cudaMemsetAsync(out_prior_depths[ref], 0,
                                              sizeof(float) * cams[ref].width * cams[ref].height, cc->stream) ==

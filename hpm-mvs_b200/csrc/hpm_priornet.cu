@@ -385,9 +385,10 @@ int net_forward(hpm_ctx *c, const HpmNetWeights *net, const HpmCamera &ccam, int
  * coarse planar prior (upsampled by JBU, as the plain form's coarsest level)
  * and the network's proposal as the initial hypothesis and as a sixth
  * refinement candidate, then extra_passes more full-scale prior passes.
- * Outputs like hpm_process_problem. */
+ * prior_mode 2 makes the upsampled proposal the first pass's planar prior
+ * instead of the coarse triangulation.  Outputs like hpm_process_problem. */
 int net_problem(hpm_ctx *c, int n, const float *const *images, const HpmCamera *cams, const HpmNetWeights *net,
-                uint64_t seed, int extra_passes, float *depth_out, float *normal_out, float *cost_out)
+                uint64_t seed, int extra_passes, int prior_mode, float *depth_out, float *normal_out, float *cost_out)
 {
     int cw, ch;
     int r = net_coarse_stage(c, n, images, cams, seed, &cw, &ch);
@@ -407,15 +408,23 @@ int net_problem(hpm_ctx *c, int n, const float *const *images, const HpmCamera *
     CK(ws_reserve_full(c, npx), "flow workspace");
     CK(net_reserve_full(c, npx), "prior-net buffers");
     const int sr = H / ch, sc = W / cw, scale = sr > sc ? sr : sc;
-    /* the coarse planar prior, as the plain form's coarsest level */
-    CK(flow_pack4(ws.c_prior_depth, ws.c_prior_normal, (int)cn, ws.c_packed, s), "pack");
-    CK(launch_jbu(ctx_image(c, 0), W, H, nullptr, ws.c_packed, cw, ch, scale, ws.up_depth, ws.up_normal, s), "jbu");
-    CK(prior_reload(cam, W, H, dmin, dmax, ws.up_depth, ws.up_normal, reinterpret_cast<float4 *>(ctx_prior(c)),
-                    ctx_masks(c), s),
-       "prior reload");
-    ctx_mark_prior(c);
-    /* the proposal: initial hypothesis and candidate */
+    /* the proposal, upsampled: initial hypothesis and candidate */
     CK(launch_jbu(ctx_image(c, 0), W, H, nullptr, nw.prop, cw, ch, scale, nw.up_depth, nw.up_normal, s), "jbu");
+    if (prior_mode == 2) {
+        /* the proposal is also the planar prior */
+        CK(prior_reload(cam, W, H, dmin, dmax, nw.up_depth, nw.up_normal, reinterpret_cast<float4 *>(ctx_prior(c)),
+                        ctx_masks(c), s),
+           "prior reload");
+    } else {
+        /* the coarse planar prior, as the plain form's coarsest level */
+        CK(flow_pack4(ws.c_prior_depth, ws.c_prior_normal, (int)cn, ws.c_packed, s), "pack");
+        CK(launch_jbu(ctx_image(c, 0), W, H, nullptr, ws.c_packed, cw, ch, scale, ws.up_depth, ws.up_normal, s),
+           "jbu");
+        CK(prior_reload(cam, W, H, dmin, dmax, ws.up_depth, ws.up_normal, reinterpret_cast<float4 *>(ctx_prior(c)),
+                        ctx_masks(c), s),
+           "prior reload");
+    }
+    ctx_mark_prior(c);
     dim3 b(16, 16), g((W + 15) / 16, (H + 15) / 16);
     k_proposal_planes<<<g, b, 0, s>>>(cam, nw.up_depth, nw.up_normal, W, H, reinterpret_cast<float4 *>(ctx_planes(c)),
                                      ctx_costs(c), nw.cand);

@@ -307,8 +307,9 @@ def main():
     ap.add_argument("--steps", type=int, default=1500)
     ap.add_argument("--batch", type=int, default=8)
     ap.add_argument("--lr", type=float, default=1e-3)
-    ap.add_argument("--schedules", default="0:2,1:2,0:1,1:1",
-                    help="prior-net schedules to evaluate, extra full-scale prior passes:geometric iterations")
+    ap.add_argument("--schedules", default="0:2:1,0:2:2,1:2:1,0:1:1,0:1:2,1:1:1",
+                    help="prior-net schedules to evaluate, extra full-scale prior passes:geometric iterations:"
+                         "planar prior of the first full-scale pass (1 the coarse triangulation, 2 the proposal)")
     ap.add_argument("--workers", type=int, default=0)
     ap.add_argument("--size", default=None, help="WxH of the scenes (default 1600x1200)")
     ap.add_argument("--out", default=".")
@@ -317,7 +318,7 @@ def main():
     if args.size:
         recipe["width"], recipe["height"] = (int(x) for x in args.size.lower().split("x"))
     workers = args.workers or max(1, (os.cpu_count() or 2) * 2 // 3)
-    schedules = [tuple(int(x) for x in t.split(":")) for t in args.schedules.split(",")]
+    schedules = [tuple(int(x) for x in (t + ":1").split(":")[:3]) for t in args.schedules.split(",")]
     train_seeds = list(range(1000, 1000 + args.scenes))
     eval_seeds = list(range(9000, 9000 + args.eval_scenes))
     log = lambda m: print(m, file=sys.stderr, flush=True)  # noqa: E731
@@ -353,8 +354,9 @@ def main():
             row = {"seed": sc["seed"]}
             ev = []
             for form, kw in [("plain", dict(geom_iterations=2))] + [
-                    (f"net_e{e}_g{g}", dict(pyramid_levels=e, geom_iterations=g, net=net.weights()))
-                    for e, g in schedules]:
+                    (f"net_e{e}_g{g}_p{m}", dict(pyramid_levels=e, geom_iterations=g, planar_prior=m,
+                                                 net=net.weights()))
+                    for e, g, m in schedules]:
                 ctx.run_scene(sc["images"], sc["cams"], sc["pairs"], seed=sc["seed"], **kw)  # warm-up
                 torch.cuda.synchronize()
                 t0 = time.time()
@@ -370,22 +372,23 @@ def main():
             rows.append(row)
             log(json.dumps(row))
         summary["eval"] = rows
-        forms = ["plain"] + [f"net_e{e}_g{g}" for e, g in schedules]
+        forms = ["plain"] + [f"net_e{e}_g{g}_p{m}" for e, g, m in schedules]
         for form in forms:
             summary[f"eval_{form}"] = {k: float(np.mean([r[form][k] for r in rows]))
                                        for k in ("mpix_per_s", "px_relerr_lt_1pct", "median_normal_err_deg")}
         # the schedule the scene driver uses: the fastest whose accuracy is
         # within 0.5 pp of the plain form's, else the most accurate
         plain_acc = summary["eval_plain"]["px_relerr_lt_1pct"]
-        ok = [(summary[f"eval_net_e{e}_g{g}"]["mpix_per_s"], e, g) for e, g in schedules
-              if summary[f"eval_net_e{e}_g{g}"]["px_relerr_lt_1pct"] >= plain_acc - 0.005]
+        ev = lambda e, g, m: summary[f"eval_net_e{e}_g{g}_p{m}"]  # noqa: E731
+        ok = [(ev(e, g, m)["mpix_per_s"], e, g, m) for e, g, m in schedules
+              if ev(e, g, m)["px_relerr_lt_1pct"] >= plain_acc - 0.005]
         if ok:
-            _, e, g = max(ok)
+            _, e, g, m = max(ok)
         else:
-            _, e, g = max((summary[f"eval_net_e{e}_g{g}"]["px_relerr_lt_1pct"], e, g) for e, g in schedules)
-        summary["chosen_schedule"] = {"extra_passes": e, "geom_iterations": g}
+            _, e, g, m = max((ev(e, g, m)["px_relerr_lt_1pct"], e, g, m) for e, g, m in schedules)
+        summary["chosen_schedule"] = {"extra_passes": e, "geom_iterations": g, "prior": m}
         net.save(os.path.join(args.out, "priornet_weights.npz"), loss=np.array(curve, np.float32),
-                 extra_passes=e, geom_iterations=g, train_scenes=args.scenes, steps=args.steps)
+                 extra_passes=e, geom_iterations=g, prior=m, train_scenes=args.scenes, steps=args.steps)
     with open(os.path.join(args.out, "priornet_summary.json"), "w") as f:
         json.dump(summary, f, indent=1)
     print(json.dumps({k: v for k, v in summary.items() if k != "eval"}))

@@ -288,7 +288,9 @@ typedef struct {
  * cost; the planar prior is the coarse one, upsampled as the plain form's
  * coarsest level.  opts->pyramid_levels > 0 adds that many full-scale
  * prior passes, each with the planar prior rebuilt from the previous pass
- * (the plain form's finest level) and the proposal still a candidate.  The
+ * (the plain form's finest level) and the proposal still a candidate.
+ * opts->planar_prior == 2 makes the upsampled proposal itself the first
+ * full-scale pass's planar prior instead of the coarse triangulation's.  The
  * geometric iterations are the plain form's. */
 int hpm_run_scene_net(hpm_ctx *ctx, int n_views, const float *const *images, const HpmCamera *cams, int n_problems,
                       const int *ref_ids, const int *src_counts, const int *src_ids, const HpmSceneOpts *opts,
