@@ -35,6 +35,7 @@
 #include <vector>
 
 #include "hpm_capi_internal.h"
+#include "hpm_nvtx.h"
 #include "hpm_prior.h"
 
 using namespace hpm;
@@ -219,6 +220,7 @@ extern "C" int hpm_run_scene_batched(hpm_ctx *c, int n_views, const float *const
     }
     int r = ctx_select_device(c);
     if (r) return r;
+    const Range range("batched scene %d views", n_views);
     cudaStream_t s = c->stream;
     /* per view: image, pass-A depth, two geometric depth buffers, normal (3), cost */
     std::vector<float *> img(n_views), dep_a(n_views), dep_g0(n_views), dep_g1(n_views), nrm(n_views), cst(n_views);
@@ -329,6 +331,7 @@ extern "C" int hpm_run_scene_batched(hpm_ctx *c, int n_views, const float *const
     /* geometric iterations: each reads the previous iteration's maps of every view */
     std::vector<float *> *src = &dep_a, *dst = &dep_g0;
     for (int gi = 0; gi < o->geom_iterations; ++gi) {
+        const Range iteration("batched geometric iteration %d", gi);
         std::vector<HpmParams> gp(n_problems);
         for (int p = 0; p < n_problems; ++p) {
             const int ref = ref_ids[p], ns = src_counts[p];

@@ -20,6 +20,7 @@
 #include <cuda_bf16.h>
 
 #include "hpm_capi_internal.h"
+#include "hpm_nvtx.h"
 
 using namespace hpm;
 
@@ -408,6 +409,7 @@ static int run_pass(hpm_ctx *c, const HpmParams *p, int half_steps, int finalize
     if (p->top_k < 1 || p->top_k > kMaxSrc) return fail(c, HPM_ERR_ARG, "top_k outside [1, %d]", kMaxSrc);
     int r = select_device(c);
     if (r) return r;
+    const Range range("pass geom=%d prior=%d", p->geom_consistency ? 1 : 0, p->planar_prior ? 1 : 0);
     PMArgs a = make_args(c);
     a.dmin = p->depth_min;
     a.dmax = p->depth_max;

@@ -16,6 +16,7 @@
 #include <vector>
 
 #include "hpm_capi_internal.h"
+#include "hpm_nvtx.h"
 #include "hpm_prior.h"
 
 using namespace hpm;
@@ -231,6 +232,7 @@ extern "C" int hpm_process_problem(hpm_ctx *c, const HpmProblemOpts *o, float *d
     if (r) return r;
     const HpmCamera cam = c->cams[0];
     const int W = cam.width, H = cam.height;
+    const Range range("problem %dx%d geom=%d", W, H, o->geom_consistency);
     const size_t npx = (size_t)W * H;
     cudaStream_t s = c->stream;
     HpmParams p;
@@ -252,6 +254,7 @@ extern "C" int hpm_process_problem(hpm_ctx *c, const HpmProblemOpts *o, float *d
             CK(ws_reserve_full(c, npx), "flow workspace");
             const int k = o->pyramid_levels >= 0 ? o->pyramid_levels : scale_levels(W, H);
             for (int i = 2 - k; i <= 2; ++i) {
+                const Range level("prior level %d", i);
                 CK(cudaGetLastError(), "flow");
                 k_split_state<<<grid1((int)npx), 256, 0, s>>>(reinterpret_cast<const float4 *>(ctx_planes(c)), (int)npx,
                                                               ws.full_depth, ws.full_normal);
@@ -370,6 +373,7 @@ static int run_scene_impl(hpm_ctx *c, int n_views, const float *const *images, c
     }
     int r = ctx_select_device(c);
     if (r) return r;
+    const Range range(net ? "scene %d views (prior-net form)" : "scene %d views", n_views);
     cudaStream_t s = c->stream;
     SceneMaps m;
     size_t total = 0; /* floats: image, pass-A depth, geometric depth, normal (3), cost */
@@ -476,6 +480,7 @@ static int run_scene_impl(hpm_ctx *c, int n_views, const float *const *images, c
     float *pdep[kMaxViews];
     /* pass set B: geometric iterations (main.cpp:662-674) */
     for (int gi = 0; gi < o->geom_iterations; ++gi) {
+        const Range iteration("geometric iteration %d", gi);
         std::vector<float *> &src_depths = gi == 0 ? m.depth_a : m.depth_g;
         if (gi == 0)
             for (int v = 0; v < n_views; ++v)

@@ -34,6 +34,7 @@
 #include <vector>
 
 #include "hpm_internal.h"
+#include "hpm_nvtx.h"
 
 namespace {
 
@@ -179,6 +180,7 @@ extern "C" int hpm_fuse(int device, int n_views, const HpmCamera *cams, const fl
             if (src_ids[p * kMaxSrc + j] < 0 || src_ids[p * kMaxSrc + j] >= n_views) return HPM_ERR_ARG;
     }
     if (cudaSetDevice(device) != cudaSuccess) return HPM_ERR_CUDA;
+    const hpm::Range range("fusion %d problems", n_problems);
     cudaStream_t st;
     if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) return HPM_ERR_CUDA;
     struct StreamGuard {

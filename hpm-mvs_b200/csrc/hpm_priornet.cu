@@ -19,6 +19,7 @@
 
 #include "hpm_capi_internal.h"
 #include "hpm_net.h"
+#include "hpm_nvtx.h"
 #include "hpm_prior.h"
 
 namespace hpm {
@@ -390,12 +391,16 @@ int net_forward(hpm_ctx *c, const HpmNetWeights *net, const HpmCamera &ccam, int
 int net_problem(hpm_ctx *c, int n, const float *const *images, const HpmCamera *cams, const HpmNetWeights *net,
                 uint64_t seed, int extra_passes, int prior_mode, float *depth_out, float *normal_out, float *cost_out)
 {
+    const Range range("prior-net problem %dx%d", cams[0].width, cams[0].height);
     int cw, ch;
     int r = net_coarse_stage(c, n, images, cams, seed, &cw, &ch);
     if (r) return r;
     const HpmCamera ccam = c->coarse->cams[0];
     const float dmin = cams[0].depth_min * 0.6f, dmax = cams[0].depth_max * 1.2f;
-    r = net_forward(c, net, ccam, cw, ch, dmin, dmax);
+    {
+        const Range network("network %dx%d", cw, ch);
+        r = net_forward(c, net, ccam, cw, ch, dmin, dmax);
+    }
     if (r) return r;
     r = hpm_set_views(c, images, cams, n);
     if (r) return r;
