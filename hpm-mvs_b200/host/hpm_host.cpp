@@ -12,6 +12,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <exception>
+#include <fstream>
 #include <iomanip>
 #include <iostream>
 #include <map>
@@ -640,6 +641,41 @@ void RunScene(const std::string &dense_folder, const std::vector<Problem> &probl
         write_dmb(folder + "/costs.dmb", cost[v], w, h, 1);
     });
     std::cout << "Processed " << np << " problems (" << n << " views) in one scene run" << std::endl;
+}
+
+Progress::Progress(const std::string &dense_folder, const std::string &settings, bool resume)
+    : path_(dense_folder + "/HPM/progress.txt")
+{
+    make_dir(dense_folder + "/HPM");
+    const std::string head = "settings " + settings;
+    if (resume) {
+        std::ifstream in(path_);
+        std::string line;
+        if (in && std::getline(in, line)) {
+            if (line != head) throw Error(HPM_ERR_ARG, "cannot resume: " + path_ + " was written with " + line);
+            while (std::getline(in, line))
+                if (!line.empty()) steps_.push_back(line);
+            return;
+        }
+    }
+    std::ofstream out(path_, std::ios::trunc);
+    out << head << "\n";
+    out.flush();
+    if (!out) throw Error(HPM_ERR_IO, "cannot write " + path_);
+}
+
+bool Progress::done(const std::string &step) const
+{
+    return std::find(steps_.begin(), steps_.end(), step) != steps_.end();
+}
+
+void Progress::mark(const std::string &step)
+{
+    std::ofstream out(path_, std::ios::app);
+    out << step << "\n";
+    out.flush();
+    if (!out) throw Error(HPM_ERR_IO, "cannot write " + path_);
+    steps_.push_back(step);
 }
 
 }  // namespace hpm_host

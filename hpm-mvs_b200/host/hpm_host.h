@@ -140,4 +140,27 @@ void ProcessProblem(const std::string &dense_folder, const Problem &problem, boo
 void RunScene(const std::string &dense_folder, const std::vector<Problem> &problems, bool planar_prior,
               int geom_iterations, uint64_t seed, int pyramid_levels, int device);
 
+/* What main() has finished in a dense folder, so that a run can stop and be
+ * resumed (the reference has no such log; its passes only exchange .dmb
+ * files).  dense_folder/HPM/progress.txt holds a line naming the run's
+ * settings, then one line per finished step, appended and flushed after
+ * that step's files are written:
+ *   "A <ref_id>"        pass set A of a problem (ProcessProblem)
+ *   "G<g> <ref_id>"     geometric iteration g of a problem
+ *   "scene"             the whole depth estimation of the scene form
+ *   "fusion"            HPM/HPM_model.ply
+ * A fresh run (resume false) starts an empty log; resuming a log written
+ * with other settings throws.  A step cut off while its files were being
+ * written is not in the log and runs again from the files as they are. */
+class Progress {
+public:
+    Progress(const std::string &dense_folder, const std::string &settings, bool resume);
+    bool done(const std::string &step) const;
+    void mark(const std::string &step);
+
+private:
+    std::string path_;
+    std::vector<std::string> steps_;
+};
+
 }  // namespace hpm_host

@@ -6,6 +6,7 @@
  *
  *   hpm_mvs dense_folder [--seed S] [--levels K] [--device D] [--no-prior]
  *                        [--geom-iterations G] [--no-fusion] [--per-problem]
+ *                        [--resume] [--stop-after N]
  *
  * By default the passes run as one scene (RunScene: maps in device memory
  * between passes, pass set A on two host threads, files written at the
@@ -14,10 +15,18 @@
  * Problem p of pass set A uses seed S + p; problem p of geometric iteration
  * g uses S + 1000003 (g + 1) + p, in both forms, so both write the same
  * files.
+ *
+ * Every finished step is logged in HPM/progress.txt (hpm_host::Progress).
+ * --stop-after N ends the run, with status 0, once N steps of this run have
+ * finished (a problem of pass set A or of a geometric iteration, the scene
+ * of the scene form, the fusion); --resume skips the steps the log holds, so
+ * a scene can be computed in several runs.  Both forms resume to the files
+ * one uninterrupted run writes.
  */
 #include <cstdlib>
 #include <cstring>
 #include <iostream>
+#include <sstream>
 #include <string>
 #include <vector>
 
@@ -27,14 +36,15 @@ int main(int argc, char **argv)
 {
     if (argc < 2 || !strcmp(argv[1], "-h") || !strcmp(argv[1], "--help")) {
         std::cout << "USAGE: hpm_mvs dense_folder [--seed S] [--levels K] [--device D] [--no-prior] "
-                     "[--geom-iterations G] [--no-fusion] [--per-problem]"
+                     "[--geom-iterations G] [--no-fusion] [--per-problem] [--resume] [--stop-after N]"
                   << std::endl;
         return argc < 2 ? -1 : 0;
     }
     const std::string dense_folder = argv[1];
     uint64_t seed = 0;
     int levels = -1, device = 0, geom_iterations = 2;
-    bool planar_prior = true, fusion = true, per_problem = false;
+    bool planar_prior = true, fusion = true, per_problem = false, resume = false;
+    long long stop_after = -1;
     for (int i = 2; i < argc; ++i) {
         const std::string a = argv[i];
         auto next = [&](const char *name) -> const char * {
@@ -58,6 +68,10 @@ int main(int argc, char **argv)
             fusion = false;
         else if (a == "--per-problem")
             per_problem = true;
+        else if (a == "--resume")
+            resume = true;
+        else if (a == "--stop-after")
+            stop_after = std::atoll(next("--stop-after"));
         else {
             std::cerr << "unknown option " << a << std::endl;
             return 2;
@@ -67,21 +81,50 @@ int main(int argc, char **argv)
         std::vector<hpm_host::Problem> problems;
         hpm_host::GenerateSampleList(dense_folder, problems);
         std::cout << "There are " << problems.size() << " problems needed to be processed!" << std::endl;
+        std::ostringstream settings;
+        settings << "seed=" << seed << " levels=" << levels << " prior=" << planar_prior
+                 << " geom_iterations=" << geom_iterations << " form=" << (per_problem ? "per-problem" : "scene");
+        hpm_host::Progress progress(dense_folder, settings.str(), resume);
+        long long steps = 0;
+        /* runs one step unless the log holds it; false once --stop-after is reached */
+        auto step = [&](const std::string &name, auto work) {
+            if (progress.done(name)) return true;
+            if (stop_after >= 0 && steps >= stop_after) return false;
+            work();
+            progress.mark(name);
+            ++steps;
+            return true;
+        };
+        auto stopped = [&]() {
+            std::cout << "Stopped after " << steps << " steps; --resume continues" << std::endl;
+            return 0;
+        };
         if (!per_problem) {
-            hpm_host::RunScene(dense_folder, problems, planar_prior, geom_iterations, seed, levels, device);
+            if (!step("scene", [&] {
+                    hpm_host::RunScene(dense_folder, problems, planar_prior, geom_iterations, seed, levels, device);
+                }))
+                return stopped();
         } else {
             for (size_t p = 0; p < problems.size(); ++p)
-                hpm_host::ProcessProblem(dense_folder, problems[p], false, planar_prior, false, seed + p, levels,
-                                         device);
+                if (!step("A " + std::to_string(problems[p].ref_image_id), [&] {
+                        hpm_host::ProcessProblem(dense_folder, problems[p], false, planar_prior, false, seed + p,
+                                                 levels, device);
+                    }))
+                    return stopped();
             for (int g = 0; g < geom_iterations; ++g)
                 for (size_t p = 0; p < problems.size(); ++p)
-                    hpm_host::ProcessProblem(dense_folder, problems[p], true, false, g > 0,
-                                             seed + 1000003ull * (g + 1) + p, levels, device);
+                    if (!step("G" + std::to_string(g) + " " + std::to_string(problems[p].ref_image_id), [&] {
+                            hpm_host::ProcessProblem(dense_folder, problems[p], true, false, g > 0,
+                                                     seed + 1000003ull * (g + 1) + p, levels, device);
+                        }))
+                        return stopped();
         }
-        if (fusion) {
-            const long long n = hpm_host::RunFusion(dense_folder, problems, geom_iterations > 0, device);
-            std::cout << "Fused " << n << " points into " << dense_folder << "/HPM/HPM_model.ply" << std::endl;
-        }
+        if (fusion &&
+            !step("fusion", [&] {
+                const long long n = hpm_host::RunFusion(dense_folder, problems, geom_iterations > 0, device);
+                std::cout << "Fused " << n << " points into " << dense_folder << "/HPM/HPM_model.ply" << std::endl;
+            }))
+            return stopped();
     } catch (const hpm_host::Error &e) {
         std::cerr << "hpm_mvs: " << e.what() << " (status " << e.code << ")" << std::endl;
         return 1;

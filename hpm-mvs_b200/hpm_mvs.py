@@ -5,12 +5,16 @@ library to the bytes cv::imread gives (HPM.cpp:492, main.cpp:523).
 
     python hpm-mvs_b200/hpm_mvs.py dense_folder [--seed S] [--levels K]
                                    [--geom-iterations G] [--no-prior] [--device D]
-                                   [--no-fusion] [--per-problem]
+                                   [--no-fusion] [--per-problem] [--resume] [--stop-after N]
 
 Writes HPM/2333_%08d/{depths,depths_geom,normals,costs,depths_prior}.dmb like
 the reference's ProcessProblem, then fuses them into HPM/HPM_model.ply
 (RunFusion).  Seeds as in the C++ host: problem p of pass
 set A uses S + p, of geometric iteration g S + 1000003 (g + 1) + p.
+
+Finished steps are logged in HPM/progress.txt, in the C++ host's format
+(Progress): --stop-after N ends the run once N steps have finished, --resume
+skips the logged steps.
 """
 from __future__ import annotations
 
@@ -137,6 +141,42 @@ def run_fusion(folder, problems, geom_consistency, device=0):
     return len(xyz)
 
 
+class Progress:
+    """The step log of a dense folder, HPM/progress.txt: a settings line,
+    then one line per finished step ("A <ref>", "G<g> <ref>", "scene",
+    "fusion"), appended after the step's files are written.  Resuming a log
+    written with other settings raises."""
+
+    def __init__(self, folder: str, settings: str, resume: bool):
+        os.makedirs(os.path.join(folder, "HPM"), exist_ok=True)
+        self.path = os.path.join(folder, "HPM", "progress.txt")
+        head = "settings " + settings
+        self.steps: list[str] = []
+        if resume and os.path.exists(self.path):
+            with open(self.path) as f:
+                lines = f.read().splitlines()
+            if lines:
+                if lines[0] != head:
+                    raise hb.HpmError(f"cannot resume: {self.path} was written with {lines[0]}")
+                self.steps = [ln for ln in lines[1:] if ln]
+                return
+        with open(self.path, "w") as f:
+            f.write(head + "\n")
+
+    def done(self, step: str) -> bool:
+        return step in self.steps
+
+    def mark(self, step: str) -> None:
+        with open(self.path, "a") as f:
+            f.write(step + "\n")
+            f.flush()
+        self.steps.append(step)
+
+
+class Stopped(Exception):
+    pass
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
     ap.add_argument("dense_folder")
@@ -148,28 +188,70 @@ def main(argv=None):
     ap.add_argument("--no-fusion", action="store_true")
     ap.add_argument("--per-problem", action="store_true",
                     help="ProcessProblem problem by problem through .dmb files, as the reference runs")
+    ap.add_argument("--resume", action="store_true", help="skip the steps HPM/progress.txt lists")
+    ap.add_argument("--stop-after", type=int, default=-1, help="stop once this many steps have finished")
     a = ap.parse_args(argv)
     problems = hb.read_pair(os.path.join(a.dense_folder, "pair.txt"))
-    needed = sorted({p[0] for p in problems} | {s for p in problems for s in p[1]})
-    views = {v: load_view(a.dense_folder, v) for v in needed}
     print(f"There are {len(problems)} problems needed to be processed!")
-    with hb.Context(a.device) as ctx:
+    settings = (f"seed={a.seed} levels={a.levels} prior={int(not a.no_prior)} geom_iterations={a.geom_iterations} "
+                f"form={'per-problem' if a.per_problem else 'scene'}")
+    progress = Progress(a.dense_folder, settings, a.resume)
+    count = [0]
+
+    def step(name, work):
+        if progress.done(name):
+            return
+        if 0 <= a.stop_after <= count[0]:
+            raise Stopped
+        work()
+        progress.mark(name)
+        count[0] += 1
+
+    state = {}
+
+    def ctx():
+        """the views and the context, made on the first step that needs them"""
+        if "ctx" not in state:
+            needed = sorted({p[0] for p in problems} | {s for p in problems for s in p[1]})
+            state["needed"] = needed
+            state["views"] = {v: load_view(a.dense_folder, v) for v in needed}
+            state["ctx"] = hb.Context(a.device)
+        return state["ctx"]
+
+    try:
         if a.per_problem:
             for p, (ref, srcs) in enumerate(problems):
-                process_problem(ctx, a.dense_folder, ref, srcs, views, geom=False, planar_prior=not a.no_prior,
-                                multi_geometry=False, seed=a.seed + p, levels=a.levels)
+                step(f"A {ref}", lambda: process_problem(ctx(), a.dense_folder, ref, srcs, state["views"], geom=False,
+                                                         planar_prior=not a.no_prior, multi_geometry=False,
+                                                         seed=a.seed + p, levels=a.levels))
             for g in range(a.geom_iterations):
                 for p, (ref, srcs) in enumerate(problems):
-                    process_problem(ctx, a.dense_folder, ref, srcs, views, geom=True, planar_prior=False,
-                                    multi_geometry=g > 0, seed=a.seed + 1000003 * (g + 1) + p, levels=a.levels)
+                    step(f"G{g} {ref}",
+                         lambda: process_problem(ctx(), a.dense_folder, ref, srcs, state["views"], geom=True,
+                                                 planar_prior=False, multi_geometry=g > 0,
+                                                 seed=a.seed + 1000003 * (g + 1) + p, levels=a.levels))
         else:
-            run_scene(ctx, a.dense_folder, problems, needed, views, planar_prior=not a.no_prior,
-                      geom_iterations=a.geom_iterations, seed=a.seed, levels=a.levels)
-    if not a.no_fusion:
-        n = run_fusion(a.dense_folder, problems, a.geom_iterations > 0, a.device)
-        print(f"Fused {n} points into {a.dense_folder}/HPM/HPM_model.ply")
+            step("scene", lambda: run_scene(ctx(), a.dense_folder, problems, state["needed"], state["views"],
+                                            planar_prior=not a.no_prior, geom_iterations=a.geom_iterations,
+                                            seed=a.seed, levels=a.levels))
+        if "ctx" in state:
+            state.pop("ctx").close()
+        if not a.no_fusion:
+            def fusion():
+                n = run_fusion(a.dense_folder, problems, a.geom_iterations > 0, a.device)
+                print(f"Fused {n} points into {a.dense_folder}/HPM/HPM_model.ply")
+            step("fusion", fusion)
+    except Stopped:
+        print(f"Stopped after {count[0]} steps; --resume continues")
+    finally:
+        if "ctx" in state:
+            state.pop("ctx").close()
     return 0
 
 
 if __name__ == "__main__":
-    sys.exit(main())
+    try:
+        sys.exit(main())
+    except hb.HpmError as e:
+        print(f"hpm_mvs: {e}", file=sys.stderr)
+        sys.exit(1)

@@ -238,6 +238,51 @@ def test_host_main_writes_the_scene_driver_maps(tmp_path, ext):
     assert all(p == plys[0] for p in plys) and plys[0].startswith(b"ply\n") and len(plys[0]) > 10000
 
 
+@pytest.mark.parametrize("front_end", ["cpp", "py"])
+def test_stopped_and_resumed_runs_write_the_files_of_one_run(tmp_path, front_end):
+    """hpm_mvs --stop-after N then --resume, in chunks, problem by problem
+    (the geometric iterations update the files in place, so each step must
+    start from exactly the files the one uninterrupted run had) and in the
+    scene form: every .dmb file and the PLY equal one uninterrupted run's."""
+    import os
+    import subprocess
+    import sys
+
+    here = os.path.dirname(os.path.abspath(hb.__file__))
+    exe = [os.path.join(here, "hpm_mvs")] if front_end == "cpp" else [sys.executable, os.path.join(here, "hpm_mvs.py")]
+    sc = syn.make_scene(19, 128, 96, 4, n_planes=4, low_texture=0.3)
+
+    def run(folder, *extra):
+        r = subprocess.run(exe + [folder, "--seed", "5", "--levels", "1"] + list(extra), capture_output=True,
+                           text=True, timeout=600)
+        assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
+        return r.stdout
+
+    for form in ([], ["--per-problem"]):
+        whole, chunked = str(tmp_path / f"whole{len(form)}"), str(tmp_path / f"chunked{len(form)}")
+        syn.write_dense_folder(sc, whole)
+        syn.write_dense_folder(sc, chunked)
+        run(whole, *form)
+        # per problem: 4 + 2 x 4 problem steps and the fusion, in chunks of 3; scene form: scene, fusion
+        chunks = 0
+        while True:
+            out = run(chunked, *form, "--resume", "--stop-after", "3" if form else "1")
+            chunks += 1
+            if "Stopped after" not in out:
+                break
+        assert chunks == (5 if form else 2), chunks
+        names = ["depths_geom.dmb", "normals.dmb", "costs.dmb", "depths.dmb", "depths_prior.dmb"]
+        for v in range(4):
+            for name in names:
+                a = open(os.path.join(whole, "HPM", f"2333_{v:08d}", name), "rb").read()
+                assert a == open(os.path.join(chunked, "HPM", f"2333_{v:08d}", name), "rb").read(), (form, v, name)
+        ply = [open(os.path.join(f, "HPM", "HPM_model.ply"), "rb").read() for f in (whole, chunked)]
+        assert ply[0] == ply[1] and len(ply[0]) > 1000
+        # a finished log: --resume does nothing
+        assert "Stopped" not in run(chunked, *form, "--resume") and \
+            open(os.path.join(chunked, "HPM", "HPM_model.ply"), "rb").read() == ply[0]
+
+
 def test_view_sharded_driver_on_the_gpu():
     """scene_dist.run_scene_sharded with the C-ABI solver (maps on the
     device, one rank) gives exactly the maps of the same schedule written

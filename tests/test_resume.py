@@ -1,0 +1,56 @@
+"""The step log behind --resume / --stop-after of the two front ends
+(hpm_mvs and hpm_mvs.py), without a GPU: a run stopped before its first step
+writes the log's settings line; resuming with the same settings keeps the
+logged steps, with other settings fails, and a fresh run starts an empty
+log.  Both front ends write the same log."""
+import os
+import subprocess
+import sys
+
+import pytest
+
+from conftest import PKG
+
+import hpm_mvs
+import synthetic as syn
+
+
+def _folder(tmp_path, name):
+    sc = syn.make_scene(3, 64, 48, 3, n_planes=3)
+    f = str(tmp_path / name)
+    syn.write_dense_folder(sc, f)
+    return f
+
+
+def test_python_progress_log(tmp_path):
+    f = str(tmp_path / "d")
+    os.makedirs(f)
+    p = hpm_mvs.Progress(f, "seed=1", resume=False)
+    p.mark("A 0")
+    p.mark("A 1")
+    q = hpm_mvs.Progress(f, "seed=1", resume=True)
+    assert q.done("A 0") and q.done("A 1") and not q.done("G0 0")
+    with pytest.raises(Exception, match="cannot resume"):
+        hpm_mvs.Progress(f, "seed=2", resume=True)
+    r = hpm_mvs.Progress(f, "seed=2", resume=False)
+    assert not r.done("A 0")
+    assert open(os.path.join(f, "HPM", "progress.txt")).read() == "settings seed=2\n"
+
+
+@pytest.mark.parametrize("front_end", ["cpp", "py"])
+def test_front_end_stops_before_any_work_and_refuses_other_settings(tmp_path, front_end):
+    exe = [os.path.join(PKG, "hpm_mvs")] if front_end == "cpp" else [sys.executable, os.path.join(PKG, "hpm_mvs.py")]
+    if front_end == "cpp" and not os.path.exists(exe[0]):
+        pytest.skip("make -C hpm-mvs_b200 builds hpm_mvs")
+    f = _folder(tmp_path, front_end)
+    r = subprocess.run(exe + [f, "--seed", "4", "--per-problem", "--stop-after", "0"], capture_output=True, text=True,
+                       timeout=120)
+    assert r.returncode == 0 and "Stopped after 0 steps" in r.stdout, r.stdout + r.stderr
+    log = open(os.path.join(f, "HPM", "progress.txt")).read()
+    assert log == "settings seed=4 levels=-1 prior=1 geom_iterations=2 form=per-problem\n"
+    r = subprocess.run(exe + [f, "--seed", "5", "--per-problem", "--resume", "--stop-after", "0"], capture_output=True,
+                       text=True, timeout=120)
+    assert r.returncode != 0 and "cannot resume" in (r.stdout + r.stderr)
+    r = subprocess.run(exe + [f, "--seed", "4", "--per-problem", "--resume", "--stop-after", "0"], capture_output=True,
+                       text=True, timeout=120)
+    assert r.returncode == 0 and open(os.path.join(f, "HPM", "progress.txt")).read() == log
