@@ -67,18 +67,20 @@ __global__ void k_pack_maps(const float *__restrict__ normal3, const float *__re
 }
 
 /* A batch of problem contexts with its device work lists and, once
- * captured, the graph of one pass. */
+ * captured, the graph of one pass: one graph for the plain kernels and one
+ * for the prior-net form's (the proposal candidate). */
 struct Plan {
     std::vector<hpm_ctx *> ctxs;
     std::vector<PMArgs> args; /* host copy, refreshed per pass */
     void *dev = nullptr;      /* args + work lists */
     BatchList init{}, half{};
     int smax = 0;
-    cudaGraphExec_t exec = nullptr;
+    cudaGraphExec_t exec[2] = {nullptr, nullptr};
 
     ~Plan()
     {
-        if (exec) cudaGraphExecDestroy(exec);
+        for (cudaGraphExec_t e : exec)
+            if (e) cudaGraphExecDestroy(e);
         cudaFree(dev);
     }
 };
@@ -115,39 +117,46 @@ int make_plan(hpm_ctx *c, const std::vector<hpm_ctx *> &ctxs, const std::vector<
 
 /* the launches of one pass on stream s: initialisation, 6 half-steps,
  * depth/normal and the filter of every problem */
-cudaError_t launch_pass(const Plan &pl, cudaStream_t s)
+cudaError_t launch_pass(const Plan &pl, bool proposals, cudaStream_t s)
 {
     cudaError_t e = launch_batch_init(pl.init, 0, s);
-    for (int hs = 0; hs < 6 && e == cudaSuccess; ++hs) e = launch_batch_propagate(pl.half, pl.smax, hs / 2, hs % 2, 0, s);
+    for (int hs = 0; hs < 6 && e == cudaSuccess; ++hs)
+        e = launch_batch_propagate(pl.half, pl.smax, hs / 2, hs % 2, 0, proposals, s);
     for (size_t i = 0; i < pl.ctxs.size() && e == cudaSuccess; ++i)
         e = launch_depth_normal_filter(pl.args[i], reinterpret_cast<float4 *>(ctx_planes(pl.ctxs[i])),
                                        ctx_costs(pl.ctxs[i]), s);
     return e;
 }
 
-/* One batched pass with per-problem parameters. */
+/* One batched pass with per-problem parameters; with the proposal
+ * candidate when every problem has one (the prior-net form). */
 int batch_pass(hpm_ctx *c, Plan &pl, const std::vector<HpmParams> &params)
 {
     cudaStream_t s = c->stream;
+    int with = 0;
     for (size_t i = 0; i < pl.ctxs.size(); ++i) {
         const int r = ctx_pass_args(pl.ctxs[i], &params[i], &pl.args[i]);
         if (r) return ctx_fail(c, r, "batched pass, problem %zu: %s", i, hpm_last_error(pl.ctxs[i]));
+        with += pl.args[i].proposals != nullptr;
     }
+    if (with != 0 && with != (int)pl.ctxs.size())
+        return ctx_fail(c, HPM_ERR_STATE, "batched pass: %d of %zu problems have proposals", with, pl.ctxs.size());
+    const int g_id = with ? 1 : 0;
     CK(cudaMemcpyAsync(pl.dev, pl.args.data(), sizeof(PMArgs) * pl.args.size(), cudaMemcpyHostToDevice, s), "args");
-    if (!pl.exec) {
+    if (!pl.exec[g_id]) {
         /* capture the pass once; its kernels read their arguments from pl.dev,
          * the per-problem finalisation's arguments do not change between passes */
         cudaGraph_t g = nullptr;
         CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "graph capture");
-        const cudaError_t le = launch_pass(pl, s);
+        const cudaError_t le = launch_pass(pl, g_id == 1, s);
         const cudaError_t ce = cudaStreamEndCapture(s, &g);
         CK(le, "batched pass launches");
         CK(ce, "graph capture");
-        const cudaError_t ie = cudaGraphInstantiate(&pl.exec, g, 0);
+        const cudaError_t ie = cudaGraphInstantiate(&pl.exec[g_id], g, 0);
         cudaGraphDestroy(g);
         CK(ie, "graph instantiate");
     }
-    CK(cudaGraphLaunch(pl.exec, s), "graph launch");
+    CK(cudaGraphLaunch(pl.exec[g_id], s), "graph launch");
     CK(cudaStreamSynchronize(s), "batched pass");
     return HPM_OK;
 }
@@ -179,7 +188,7 @@ int tune_tiles(hpm_ctx *c, const std::vector<hpm_ctx *> &ctxs, const std::vector
                 cudaEventCreate(&e0);
                 cudaEventCreate(&e1);
                 cudaEventRecord(e0, c->stream);
-                CK(launch_batch_propagate(one.half, one.smax, 0, 0, 0, c->stream), "tuning half-step");
+                CK(launch_batch_propagate(one.half, one.smax, 0, 0, 0, false, c->stream), "tuning half-step");
                 cudaEventRecord(e1, c->stream);
                 CK(cudaEventSynchronize(e1), "tuning");
                 float ms = 0.0f;
@@ -199,12 +208,70 @@ int tune_tiles(hpm_ctx *c, const std::vector<hpm_ctx *> &ctxs, const std::vector
     return HPM_OK;
 }
 
-}  // namespace
+/* Pass set A in the prior-net form for every problem of pc (full-scale
+ * views set): the 1/4-scale plain passes as one batched pass over the
+ * problems' coarse sub-contexts, per problem the coarse planar prior, the
+ * network and the full-scale start (net_full_setup), then 1 + extra_passes
+ * batched full-scale passes with the proposal candidate; seeds as
+ * net_problem's, so each problem's maps equal it bit for bit. */
+int net_pass_set_a(hpm_ctx *c, const std::vector<hpm_ctx *> &pc, const std::vector<HpmParams> &params, Plan &all,
+                   const HpmNetWeights *net, int extra_passes, int prior_mode,
+                   const std::vector<std::vector<const float *>> &images)
+{
+    const int n = (int)pc.size();
+    std::vector<hpm_ctx *> cc(n);
+    for (int p = 0; p < n; ++p) {
+        hpm_ctx *b = pc[p];
+        int r = net_coarse_views(b, b->n, images[p].data(), b->cams);
+        if (r) return ctx_fail(c, r, "batched prior-net form, problem %d: %s", p, hpm_last_error(b));
+        cc[p] = b->coarse;
+    }
+    {
+        const Range coarse("batched coarse passes");
+        std::vector<int> cww;
+        int r = tune_tiles(c, cc, params, cww);
+        if (r) return r;
+        Plan cplan;
+        r = make_plan(c, cc, cww, cplan);
+        if (!r) r = batch_pass(c, cplan, params);
+        if (r) return r;
+    }
+    for (int p = 0; p < n; ++p) {
+        int r = net_coarse_finish(pc[p], params[p].depth_min, params[p].depth_max);
+        if (!r) r = net_full_setup(pc[p], net, prior_mode);
+        if (r) return ctx_fail(c, r, "batched prior-net form, problem %d: %s", p, hpm_last_error(pc[p]));
+    }
+    std::vector<HpmParams> fp(params);
+    for (int e = 0; e <= extra_passes; ++e) {
+        for (int p = 0; p < n; ++p) {
+            hpm_ctx *b = pc[p];
+            if (e > 0) {
+                const size_t np = (size_t)b->cams[0].width * b->cams[0].height;
+                CK(flow_split_state(reinterpret_cast<const float4 *>(ctx_planes(b)), (int)np, b->flow.full_depth,
+                                    b->flow.full_normal, b->stream),
+                   "split");
+                const int r = flow_prior_from_maps(b, 2, ctx_costs(b), params[p].depth_min, params[p].depth_max);
+                if (r) return ctx_fail(c, r, "batched prior-net form, problem %d: %s", p, hpm_last_error(b));
+            }
+            CK(cudaStreamSynchronize(b->stream), "prior-net set-up");
+            fp[p].planar_prior = 1;
+            fp[p].seed = net_pass_seed(params[p].seed, e);
+        }
+        const int r = batch_pass(c, all, fp);
+        if (r) return r;
+    }
+    for (int p = 0; p < n; ++p) {
+        pc[p]->proposals = nullptr;
+        const int r = net_status(pc[p]);
+        if (r) return ctx_fail(c, r, "batched prior-net form, problem %d: %s", p, hpm_last_error(pc[p]));
+    }
+    return HPM_OK;
+}
 
-extern "C" int hpm_run_scene_batched(hpm_ctx *c, int n_views, const float *const *images, const HpmCamera *cams,
-                                     int n_problems, const int *ref_ids, const int *src_counts, const int *src_ids,
-                                     const HpmSceneOpts *o, float *const *out_depths, float *const *out_normals,
-                                     float *const *out_costs)
+int batched_scene(hpm_ctx *c, int n_views, const float *const *images, const HpmCamera *cams, int n_problems,
+                  const int *ref_ids, const int *src_counts, const int *src_ids, const HpmSceneOpts *o,
+                  const HpmNetWeights *net, float *const *out_depths, float *const *out_normals,
+                  float *const *out_costs)
 {
     if (!c || !images || !cams || !ref_ids || !src_counts || !src_ids || !o) return HPM_ERR_ARG;
     if (n_views < 2 || n_problems < 1)
@@ -220,7 +287,7 @@ extern "C" int hpm_run_scene_batched(hpm_ctx *c, int n_views, const float *const
     }
     int r = ctx_select_device(c);
     if (r) return r;
-    const Range range("batched scene %d views", n_views);
+    const Range range(net ? "batched scene %d views (prior-net form)" : "batched scene %d views", n_views);
     cudaStream_t s = c->stream;
     /* per view: image, pass-A depth, two geometric depth buffers, normal (3), cost */
     std::vector<float *> img(n_views), dep_a(n_views), dep_g0(n_views), dep_g1(n_views), nrm(n_views), cst(n_views);
@@ -252,10 +319,12 @@ extern "C" int hpm_run_scene_batched(hpm_ctx *c, int n_views, const float *const
     std::vector<hpm_ctx *> pc(c->batch.begin(), c->batch.begin() + n_problems);
     std::vector<HpmParams> params(n_problems);
     std::vector<int> levels(n_problems);
+    std::vector<std::vector<const float *>> pimgs(n_problems);
     for (int p = 0; p < n_problems; ++p) {
-        const float *pimg[kMaxViews];
         HpmCamera pcam[kMaxViews];
         const int ref = ref_ids[p], ns = src_counts[p];
+        std::vector<const float *> &pimg = pimgs[p];
+        pimg.assign(ns + 1, nullptr);
         pimg[0] = img[ref];
         pcam[0] = cams[ref];
         for (int j = 0; j < ns; ++j) {
@@ -263,7 +332,7 @@ extern "C" int hpm_run_scene_batched(hpm_ctx *c, int n_views, const float *const
             pimg[j + 1] = img[sv];
             pcam[j + 1] = cams[sv];
         }
-        r = hpm_set_views(pc[p], pimg, pcam, ns + 1);
+        r = hpm_set_views(pc[p], pimg.data(), pcam, ns + 1);
         if (r) return ctx_fail(c, r, "hpm_run_scene_batched, problem %d: %s", p, hpm_last_error(pc[p]));
         hpm_clear_prior(pc[p]);
         ctx_reset_salt(pc[p]);
@@ -281,11 +350,18 @@ extern "C" int hpm_run_scene_batched(hpm_ctx *c, int n_views, const float *const
     Plan all;
     r = make_plan(c, pc, ww, all);
     if (r) return r;
-    /* pass set A: the plain pass of every problem */
-    r = batch_pass(c, all, params);
-    if (r) return r;
+    if (net) {
+        /* pass set A in the prior-net form */
+        r = net_pass_set_a(c, pc, params, all, net, o->pyramid_levels > 0 ? o->pyramid_levels : 0,
+                           o->planar_prior, pimgs);
+        if (r) return r;
+    } else {
+        /* pass set A: the plain pass of every problem */
+        r = batch_pass(c, all, params);
+        if (r) return r;
+    }
     /* the prior passes, levels aligned at the full scale */
-    if (o->planar_prior) {
+    if (o->planar_prior && !net) {
         const int kmax = *std::max_element(levels.begin(), levels.end());
         for (int round = 0; round <= kmax; ++round) {
             const int level = 2 - kmax + round; /* 0: 1/4 scale, 1: 1/2, 2: full */
@@ -375,4 +451,27 @@ extern "C" int hpm_run_scene_batched(hpm_ctx *c, int n_views, const float *const
     }
     CK(cudaStreamSynchronize(s), "hpm_run_scene_batched");
     return HPM_OK;
+}
+
+}  // namespace
+
+extern "C" int hpm_run_scene_batched(hpm_ctx *c, int n_views, const float *const *images, const HpmCamera *cams,
+                                     int n_problems, const int *ref_ids, const int *src_counts, const int *src_ids,
+                                     const HpmSceneOpts *o, float *const *out_depths, float *const *out_normals,
+                                     float *const *out_costs)
+{
+    return batched_scene(c, n_views, images, cams, n_problems, ref_ids, src_counts, src_ids, o, nullptr, out_depths,
+                         out_normals, out_costs);
+}
+
+extern "C" int hpm_run_scene_batched_net(hpm_ctx *c, int n_views, const float *const *images, const HpmCamera *cams,
+                                         int n_problems, const int *ref_ids, const int *src_counts,
+                                         const int *src_ids, const HpmSceneOpts *o, const HpmNetWeights *net,
+                                         float *const *out_depths, float *const *out_normals, float *const *out_costs)
+{
+    if (!net) return HPM_ERR_ARG;
+    for (int l = 0; l < 4; ++l)
+        if (!net->packed[l] || !net->bias[l]) return HPM_ERR_ARG;
+    return batched_scene(c, n_views, images, cams, n_problems, ref_ids, src_counts, src_ids, o, net, out_depths,
+                         out_normals, out_costs);
 }

@@ -173,7 +173,12 @@ int flow_level_prior(hpm_ctx *c, const HpmCamera &cam, const float *d_cost, cons
 /* the prior of pyramid level `level` (2: full scale) from flow.full_depth /
  * full_normal and d_cost, into the context's prior planes and masks */
 int flow_prior_from_maps(hpm_ctx *c, int level, const float *d_cost, float dmin, float dmax);
-/* hpm_priornet.cu */
+/* hpm_priornet.cu: the prior-net form's stages (per problem context) */
+int net_coarse_views(hpm_ctx *c, int n, const float *const *images, const HpmCamera *cams);
+int net_coarse_finish(hpm_ctx *c, float dmin, float dmax);
+int net_full_setup(hpm_ctx *c, const HpmNetWeights *net, int prior_mode);
+uint64_t net_pass_seed(uint64_t seed, int pass);
+int net_status(hpm_ctx *c);
 int net_problem(hpm_ctx *c, int n, const float *const *images, const HpmCamera *cams, const HpmNetWeights *net,
                 uint64_t seed, int extra_passes, int prior_mode, float *depth_out, float *normal_out,
                 float *cost_out);

@@ -103,7 +103,9 @@ struct BatchList {
 /* Persistent launches over a batch (hpm_pm.cu); ctas = 0 picks the number
  * of CTAs that fit on the device at once. */
 cudaError_t launch_batch_init(const BatchList &b, int ctas, cudaStream_t s);
-cudaError_t launch_batch_propagate(const BatchList &b, int smax, int iter, int color, int ctas, cudaStream_t s);
+/* proposals: every problem of b is in the prior-net form (args.proposals set) */
+cudaError_t launch_batch_propagate(const BatchList &b, int smax, int iter, int color, int ctas, bool proposals,
+                                   cudaStream_t s);
 /* grid width of problem a's half-step tiles of width ww, and their count */
 int half_step_tiles(int W, int rows_cov, int ww, int *gx);
 

@@ -1434,7 +1434,9 @@ __global__ void __launch_bounds__(kBlock, HPM_P1_MIN_BLOCKS) k_prop_dirs_batch(c
     }
 }
 
-template <int SMAX>
+/* PROP: every problem of the list is in the prior-net form (its
+ * args.proposals set) */
+template <int SMAX, bool PROP>
 __global__ void __launch_bounds__(kBlock, HPM_P2_MIN_BLOCKS) k_prop_refine_batch(const __grid_constant__ BatchList b,
                                                                                   int iter, int color)
 {
@@ -1444,7 +1446,7 @@ __global__ void __launch_bounds__(kBlock, HPM_P2_MIN_BLOCKS) k_prop_refine_batch
         const int p = batch_problem(b.first, b.n, id), local = id - b.first[p];
         int px, py;
         half_step_pixel_at(local % b.gx[p], local / b.gx[p], b.ww[p], color, px, py);
-        prop_refine_body<SMAX, false>(b.args[p], iter, px, py, sWW, tid);
+        prop_refine_body<SMAX, PROP>(b.args[p], iter, px, py, sWW, tid);
     }
 }
 
@@ -1459,15 +1461,25 @@ int resident_ctas(K kern)
     return sms * (per_sm > 0 ? per_sm : 1);
 }
 
-template <int SMAX>
+template <int SMAX, bool PROP>
 cudaError_t launch_batch_prop_t(const BatchList &b, int iter, int color, int ctas, cudaStream_t s)
 {
     const dim3 blk(kBlockX, kBlockY);
     const int c1 = ctas > 0 ? ctas : resident_ctas(k_prop_dirs_batch);
     k_prop_dirs_batch<<<b.total < c1 ? b.total : c1, blk, 0, s>>>(b, iter, color);
-    const int c2 = ctas > 0 ? ctas : resident_ctas(k_prop_refine_batch<SMAX>);
-    k_prop_refine_batch<SMAX><<<b.total < c2 ? b.total : c2, blk, 0, s>>>(b, iter, color);
+    const int c2 = ctas > 0 ? ctas : resident_ctas(k_prop_refine_batch<SMAX, PROP>);
+    k_prop_refine_batch<SMAX, PROP><<<b.total < c2 ? b.total : c2, blk, 0, s>>>(b, iter, color);
     return cudaGetLastError();
+}
+
+template <bool PROP>
+cudaError_t launch_batch_prop_s(const BatchList &b, int smax, int iter, int color, int ctas, cudaStream_t s)
+{
+    if (smax <= 4) return launch_batch_prop_t<4, PROP>(b, iter, color, ctas, s);
+    if (smax <= 8) return launch_batch_prop_t<8, PROP>(b, iter, color, ctas, s);
+    if (smax <= 12) return launch_batch_prop_t<12, PROP>(b, iter, color, ctas, s);
+    if (smax <= 16) return launch_batch_prop_t<16, PROP>(b, iter, color, ctas, s);
+    return launch_batch_prop_t<kMaxSrc, PROP>(b, iter, color, ctas, s);
 }
 
 /* HPM_REFINE_PAIR=1 in the environment scores the two random-depth
@@ -1544,14 +1556,12 @@ cudaError_t launch_batch_init(const BatchList &b, int ctas, cudaStream_t s)
     return cudaGetLastError();
 }
 
-cudaError_t launch_batch_propagate(const BatchList &b, int smax, int iter, int color, int ctas, cudaStream_t s)
+cudaError_t launch_batch_propagate(const BatchList &b, int smax, int iter, int color, int ctas, bool proposals,
+                                   cudaStream_t s)
 {
     if (b.total <= 0) return cudaSuccess;
-    if (smax <= 4) return launch_batch_prop_t<4>(b, iter, color, ctas, s);
-    if (smax <= 8) return launch_batch_prop_t<8>(b, iter, color, ctas, s);
-    if (smax <= 12) return launch_batch_prop_t<12>(b, iter, color, ctas, s);
-    if (smax <= 16) return launch_batch_prop_t<16>(b, iter, color, ctas, s);
-    return launch_batch_prop_t<kMaxSrc>(b, iter, color, ctas, s);
+    return proposals ? launch_batch_prop_s<true>(b, smax, iter, color, ctas, s)
+                     : launch_batch_prop_s<false>(b, smax, iter, color, ctas, s);
 }
 
 cudaError_t launch_depth_normal_filter(const PMArgs &a, float4 *planes, const float *costs, cudaStream_t s)

@@ -279,14 +279,10 @@ using namespace hpm;
 
 namespace hpm {
 
-/* Coarse stage of one problem (the views of images/cams, full scale, host or
- * device): 1/4-scale views, the plain pass on them (in the context's coarse
- * sub-context, so that this context's full-scale views stay loaded), its
- * planar prior, and the network's input in ws_net.x0.  Leaves the coarse
- * prior in ws.c_prior_depth / c_prior_normal and the coarse size in
- * *cw x *ch. */
-int net_coarse_stage(hpm_ctx *c, int n, const float *const *images, const HpmCamera *cams, uint64_t seed, int *cw,
-                     int *ch)
+/* The 1/4-scale views of one problem (the views of images/cams, full scale,
+ * host or device) in the context's coarse sub-context (created once), so
+ * that this context's full-scale views stay loaded. */
+int net_coarse_views(hpm_ctx *c, int n, const float *const *images, const HpmCamera *cams)
 {
     NetWorkspace &nw = c->net;
     FlowWorkspace &ws = c->flow;
@@ -329,16 +325,52 @@ int net_coarse_stage(hpm_ctx *c, int n, const float *const *images, const HpmCam
         cimgs[j] = cur;
         cur += ((size_t)vw * vh + 63) & ~(size_t)63;
     }
-    /* the coarse problem lives in a context of its own (created once) */
     if (!c->coarse) {
         int rc = hpm_create(&c->coarse, c->device);
         if (rc) return ctx_fail(c, rc, "prior-net form: coarse context");
         c->coarse->scene_workers = 1;
     }
-    hpm_ctx *cc = c->coarse;
     CK(cudaStreamSynchronize(s), "coarse images");
-    int r = hpm_set_views(cc, cimgs, ccams, n);
-    if (r) return ctx_fail(c, r, "prior-net form: %s", hpm_last_error(cc));
+    const int r = hpm_set_views(c->coarse, cimgs, ccams, n);
+    if (r) return ctx_fail(c, r, "prior-net form: %s", hpm_last_error(c->coarse));
+    return HPM_OK;
+}
+
+/* After the coarse sub-context's plain pass: its planar prior (left in
+ * ws.c_prior_depth / c_prior_normal) and the network's input in
+ * ws_net.x0. */
+int net_coarse_finish(hpm_ctx *c, float dmin, float dmax)
+{
+    NetWorkspace &nw = c->net;
+    FlowWorkspace &ws = c->flow;
+    cudaStream_t s = c->stream;
+    hpm_ctx *cc = c->coarse;
+    const HpmCamera ccam = cc->cams[0];
+    const int w = ccam.width, h = ccam.height;
+    const size_t cn = (size_t)w * h;
+    CK(ws_reserve_coarse(c, cn), "coarse buffers");
+    const float4 *cplanes = reinterpret_cast<const float4 *>(ctx_planes(cc));
+    const float *ccost = ctx_costs(cc);
+    CK(flow_split_state(cplanes, (int)cn, ws.c_depth, ws.c_normal, s), "split");
+    const int r = flow_level_prior(c, ccam, ccost, ws.c_depth, w, h, 1.0f, dmin, dmax);
+    if (r) return r;
+    CK(prior_coarse(ccam, w, h, 1.0f, dmin, dmax, ws.mask, ws.ids, ws.tri_planes, ws.knn_planes, ws.c_prior_depth,
+                    ws.c_prior_normal, s),
+       "coarse prior");
+    k_net_input<<<grid1(cn), 256, 0, s>>>(ccam, ctx_image(cc, 0), cplanes, ccost, ws.c_prior_depth, (int)cn, dmin,
+                                          dmax, static_cast<__nv_bfloat16 *>(nw.x0));
+    CK(cudaGetLastError(), "net input");
+    return HPM_OK;
+}
+
+/* Coarse stage of one problem: the 1/4-scale views, the plain pass on them,
+ * its planar prior and the network's input; the coarse size in *cw x *ch. */
+int net_coarse_stage(hpm_ctx *c, int n, const float *const *images, const HpmCamera *cams, uint64_t seed, int *cw,
+                     int *ch)
+{
+    int r = net_coarse_views(c, n, images, cams);
+    if (r) return r;
+    hpm_ctx *cc = c->coarse;
     HpmParams p;
     hpm_default_params(&p);
     p.depth_min = cams[0].depth_min * 0.6f;
@@ -346,21 +378,10 @@ int net_coarse_stage(hpm_ctx *c, int n, const float *const *images, const HpmCam
     p.seed = seed;
     r = ctx_run_pass(cc, &p, 6, 1); /* ends with a synchronisation of its stream */
     if (r) return ctx_fail(c, r, "prior-net form: %s", hpm_last_error(cc));
-    const size_t cn = (size_t)w * h;
-    CK(ws_reserve_coarse(c, cn), "coarse buffers");
-    const float4 *cplanes = reinterpret_cast<const float4 *>(ctx_planes(cc));
-    const float *ccost = ctx_costs(cc);
-    CK(flow_split_state(cplanes, (int)cn, ws.c_depth, ws.c_normal, s), "split");
-    r = flow_level_prior(c, ccams[0], ccost, ws.c_depth, w, h, 1.0f, p.depth_min, p.depth_max);
+    r = net_coarse_finish(c, p.depth_min, p.depth_max);
     if (r) return r;
-    CK(prior_coarse(ccams[0], w, h, 1.0f, p.depth_min, p.depth_max, ws.mask, ws.ids, ws.tri_planes, ws.knn_planes,
-                    ws.c_prior_depth, ws.c_prior_normal, s),
-       "coarse prior");
-    k_net_input<<<grid1(cn), 256, 0, s>>>(ccams[0], cimgs[0], cplanes, ccost, ws.c_prior_depth, (int)cn, p.depth_min,
-                                          p.depth_max, static_cast<__nv_bfloat16 *>(nw.x0));
-    CK(cudaGetLastError(), "net input");
-    *cw = w;
-    *ch = h;
+    *cw = cc->cams[0].width;
+    *ch = cc->cams[0].height;
     return HPM_OK;
 }
 
@@ -381,47 +402,39 @@ int net_forward(hpm_ctx *c, const HpmNetWeights *net, const HpmCamera &ccam, int
     return HPM_OK;
 }
 
-/* The whole pass set A of one problem in the prior-net form: the coarse
- * stage and the network, then one full-scale PatchMatch pass with the
- * coarse planar prior (upsampled by JBU, as the plain form's coarsest level)
- * and the network's proposal as the initial hypothesis and as a sixth
- * refinement candidate, then extra_passes more full-scale prior passes.
- * prior_mode 2 makes the upsampled proposal the first pass's planar prior
- * instead of the coarse triangulation.  Outputs like hpm_process_problem. */
-int net_problem(hpm_ctx *c, int n, const float *const *images, const HpmCamera *cams, const HpmNetWeights *net,
-                uint64_t seed, int extra_passes, int prior_mode, float *depth_out, float *normal_out, float *cost_out)
+/* The full-scale start of the prior-net form, after the coarse stage, with
+ * the problem's full-scale views set in c: the network's proposal,
+ * upsampled by JBU, as every pixel's initial hypothesis and as the
+ * refinement candidate (c->proposals), and the planar prior: the coarse
+ * triangulation's, upsampled as the plain form's coarsest level, or with
+ * prior_mode 2 the upsampled proposal itself.  The next pass on c (seeded
+ * as the caller wants) is the first full-scale pass. */
+int net_full_setup(hpm_ctx *c, const HpmNetWeights *net, int prior_mode)
 {
-    const Range range("prior-net problem %dx%d", cams[0].width, cams[0].height);
-    int cw, ch;
-    int r = net_coarse_stage(c, n, images, cams, seed, &cw, &ch);
-    if (r) return r;
     const HpmCamera ccam = c->coarse->cams[0];
-    const float dmin = cams[0].depth_min * 0.6f, dmax = cams[0].depth_max * 1.2f;
+    const int cw = ccam.width, ch = ccam.height;
+    const HpmCamera cam = c->cams[0];
+    const float dmin = cam.depth_min * 0.6f, dmax = cam.depth_max * 1.2f;
+    int r;
     {
         const Range network("network %dx%d", cw, ch);
         r = net_forward(c, net, ccam, cw, ch, dmin, dmax);
     }
     if (r) return r;
-    r = hpm_set_views(c, images, cams, n);
-    if (r) return r;
     NetWorkspace &nw = c->net;
     FlowWorkspace &ws = c->flow;
     cudaStream_t s = c->stream;
-    const HpmCamera cam = cams[0];
     const int W = cam.width, H = cam.height;
     const size_t npx = (size_t)W * H, cn = (size_t)cw * ch;
     CK(ws_reserve_full(c, npx), "flow workspace");
     CK(net_reserve_full(c, npx), "prior-net buffers");
     const int sr = H / ch, sc = W / cw, scale = sr > sc ? sr : sc;
-    /* the proposal, upsampled: initial hypothesis and candidate */
     CK(launch_jbu(ctx_image(c, 0), W, H, nullptr, nw.prop, cw, ch, scale, nw.up_depth, nw.up_normal, s), "jbu");
     if (prior_mode == 2) {
-        /* the proposal is also the planar prior */
         CK(prior_reload(cam, W, H, dmin, dmax, nw.up_depth, nw.up_normal, reinterpret_cast<float4 *>(ctx_prior(c)),
                         ctx_masks(c), s),
            "prior reload");
     } else {
-        /* the coarse planar prior, as the plain form's coarsest level */
         CK(flow_pack4(ws.c_prior_depth, ws.c_prior_normal, (int)cn, ws.c_packed, s), "pack");
         CK(launch_jbu(ctx_image(c, 0), W, H, nullptr, ws.c_packed, cw, ch, scale, ws.up_depth, ws.up_normal, s),
            "jbu");
@@ -435,23 +448,55 @@ int net_problem(hpm_ctx *c, int n, const float *const *images, const HpmCamera *
                                      ctx_costs(c), nw.cand);
     CK(cudaGetLastError(), "proposal planes");
     ctx_mark_state(c);
+    c->proposals = nw.cand;
+    return HPM_OK;
+}
+
+/* Seeds of the prior-net form's full-scale passes of a problem seeded s:
+ * pass 0 is the first, pass e >= 1 the e-th extra pass. */
+uint64_t net_pass_seed(uint64_t s, int pass) { return s + 0x9E3779B97F4A7C15ull + 0x632BE59BD9B4E019ull * pass; }
+
+/* Status of the tensor-core kernels of c's network (after a synchronisation). */
+int net_status(hpm_ctx *c)
+{
+    int herr = 0;
+    CK(cudaMemcpy(&herr, c->net.err, sizeof(int), cudaMemcpyDeviceToHost), "net status");
+    if (herr) return ctx_fail(c, HPM_ERR_CUDA, "prior-net form: a tensor-core wait ran out (status %d)", herr);
+    return HPM_OK;
+}
+
+/* The whole pass set A of one problem in the prior-net form: the coarse
+ * stage, the full-scale start (net_full_setup), one full-scale PatchMatch
+ * pass with the proposal as a sixth refinement candidate, then extra_passes
+ * more full-scale prior passes, each with the planar prior rebuilt from the
+ * previous pass (the plain form's finest level) and the proposal still a
+ * candidate.  Outputs like hpm_process_problem. */
+int net_problem(hpm_ctx *c, int n, const float *const *images, const HpmCamera *cams, const HpmNetWeights *net,
+                uint64_t seed, int extra_passes, int prior_mode, float *depth_out, float *normal_out, float *cost_out)
+{
+    const Range range("prior-net problem %dx%d", cams[0].width, cams[0].height);
+    int cw, ch;
+    int r = net_coarse_stage(c, n, images, cams, seed, &cw, &ch);
+    if (r) return r;
+    r = hpm_set_views(c, images, cams, n);
+    if (r) return r;
+    r = net_full_setup(c, net, prior_mode);
+    if (r) return r;
+    FlowWorkspace &ws = c->flow;
+    cudaStream_t s = c->stream;
+    const size_t npx = (size_t)cams[0].width * cams[0].height;
+    const float dmin = cams[0].depth_min * 0.6f, dmax = cams[0].depth_max * 1.2f;
     HpmParams p;
     hpm_default_params(&p);
     p.depth_min = dmin;
     p.depth_max = dmax;
-    p.seed = seed + 0x9E3779B97F4A7C15ull;
     p.planar_prior = 1;
-    c->proposals = nw.cand;
-    r = ctx_run_pass(c, &p, 6, 1);
-    CK(flow_split_state(reinterpret_cast<const float4 *>(ctx_planes(c)), (int)npx, ws.full_depth, ws.full_normal, s),
-       "split");
-    /* optional further full-scale prior passes: the planar prior rebuilt
-     * from the last pass (the plain form's finest level), the proposal
-     * still a candidate */
-    for (int e = 0; e < extra_passes && r == HPM_OK; ++e) {
-        r = flow_prior_from_maps(c, 2, ctx_costs(c), dmin, dmax);
-        if (r) break;
-        p.seed += 0x632BE59BD9B4E019ull;
+    for (int e = 0; e <= extra_passes && r == HPM_OK; ++e) {
+        if (e > 0) {
+            r = flow_prior_from_maps(c, 2, ctx_costs(c), dmin, dmax);
+            if (r) break;
+        }
+        p.seed = net_pass_seed(seed, e);
         r = ctx_run_pass(c, &p, 6, 1);
         if (r) break;
         CK(flow_split_state(reinterpret_cast<const float4 *>(ctx_planes(c)), (int)npx, ws.full_depth, ws.full_normal,
@@ -465,10 +510,7 @@ int net_problem(hpm_ctx *c, int n, const float *const *images, const HpmCamera *
         CK(cudaMemcpyAsync(normal_out, ws.full_normal, sizeof(float) * 3 * npx, cudaMemcpyDefault, s), "out");
     if (cost_out) CK(cudaMemcpyAsync(cost_out, ctx_costs(c), sizeof(float) * npx, cudaMemcpyDefault, s), "out");
     CK(cudaStreamSynchronize(s), "prior-net problem");
-    int herr = 0;
-    CK(cudaMemcpy(&herr, nw.err, sizeof(int), cudaMemcpyDeviceToHost), "net status");
-    if (herr) return ctx_fail(c, HPM_ERR_CUDA, "prior-net form: a tensor-core wait ran out (status %d)", herr);
-    return HPM_OK;
+    return net_status(c);
 }
 
 }  // namespace hpm

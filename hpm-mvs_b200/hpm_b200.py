@@ -41,7 +41,7 @@ EXPORTED = [
     "hpm_fuse", "hpm_write_ply", "hpm_read_bgr8", "hpm_set_scene_workers", "hpm_resize_linear_u8",
     "hpm_raster_triangles", "hpm_knn6", "hpm_tap_samples", "hpm_net_pack_weights", "hpm_net_conv3x3",
     "hpm_net_conv_wgrad", "hpm_run_scene_net", "hpm_net_coarse_inputs", "hpm_net_targets", "hpm_net_loss",
-    "hpm_net_adam", "hpm_run_scene_batched",
+    "hpm_net_adam", "hpm_run_scene_batched", "hpm_run_scene_batched_net",
 ]
 
 
@@ -249,7 +249,8 @@ class Context:
         depth and prior depth (hpm_run_scene_ex), five lists in all.
         net: an HpmNetWeights (priornet.Net.weights()) to run the prior-net
         form (hpm_run_scene_net) instead of the plain form.  batched: the
-        batched form (hpm_run_scene_batched)."""
+        batched form (hpm_run_scene_batched; with net, the batched prior-net
+        form, hpm_run_scene_batched_net)."""
         n = len(cams)
         cams = np.ascontiguousarray(cams, dtype=CAMERA_DTYPE)
         if images_are_device:
@@ -283,11 +284,16 @@ class Context:
         else:
             arrs = [None, None, None]
         if batched:
-            if extra_maps or net is not None:
-                raise ValueError("run_scene: the batched form has no extra maps and no network")
-            self._check(lib().hpm_run_scene_batched(self._h, n, img_arr, _p(cams), len(pairs), _p(refs), _p(counts),
-                                                    _p(srcs), ctypes.byref(o), arrs[0], arrs[1], arrs[2]),
-                        "hpm_run_scene_batched")
+            if extra_maps:
+                raise ValueError("run_scene: the batched form has no extra maps")
+            if net is not None:
+                self._check(lib().hpm_run_scene_batched_net(self._h, n, img_arr, _p(cams), len(pairs), _p(refs),
+                                                            _p(counts), _p(srcs), ctypes.byref(o), ctypes.byref(net),
+                                                            arrs[0], arrs[1], arrs[2]), "hpm_run_scene_batched_net")
+            else:
+                self._check(lib().hpm_run_scene_batched(self._h, n, img_arr, _p(cams), len(pairs), _p(refs),
+                                                        _p(counts), _p(srcs), ctypes.byref(o), arrs[0], arrs[1],
+                                                        arrs[2]), "hpm_run_scene_batched")
         elif net is not None:
             if extra_maps:
                 raise ValueError("run_scene: extra_maps is not available in the prior-net form")

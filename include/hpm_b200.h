@@ -309,6 +309,16 @@ int hpm_run_scene_batched(hpm_ctx *ctx, int n_views, const float *const *images,
                           int n_problems, const int *ref_ids, const int *src_counts, const int *src_ids,
                           const HpmSceneOpts *opts, float *const *out_depths, float *const *out_normals,
                           float *const *out_costs);
+/* The batched prior-net form: hpm_run_scene_net's pass set A (options
+ * alike) for every problem together: the 1/4-scale plain passes of all
+ * problems in one batched pass, per problem the coarse planar prior and
+ * the network, then the full-scale passes of all problems batched, each
+ * scoring its problem's proposal; then the batched geometric iterations.
+ * Pass set A equals hpm_run_scene_net's per problem bit for bit. */
+int hpm_run_scene_batched_net(hpm_ctx *ctx, int n_views, const float *const *images, const HpmCamera *cams,
+                              int n_problems, const int *ref_ids, const int *src_counts, const int *src_ids,
+                              const HpmSceneOpts *opts, const HpmNetWeights *net, float *const *out_depths,
+                              float *const *out_normals, float *const *out_costs);
 
 /* The network's input for one problem (views as for hpm_set_views, full
  * scale): the coarse stage of the prior-net form (1/4-scale plain pass with

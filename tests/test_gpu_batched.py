@@ -55,3 +55,28 @@ def test_batched_scene_keeps_the_accuracy():
     ab = np.mean([syn.depth_accuracy(db[v], sc.gt_depth[v]) for v in range(len(SIZES))])
     ap = np.mean([syn.depth_accuracy(dp[v], sc.gt_depth[v]) for v in range(len(SIZES))])
     assert ab > 0.3 and abs(ab - ap) <= 0.015, (ab, ap)
+
+
+@pytest.mark.parametrize("extra,prior", [(0, 1), (1, 2)])
+def test_batched_prior_net_pass_set_a_equals_per_problem(extra, prior):
+    """The batched prior-net form (hpm_run_scene_batched_net): the coarse
+    passes of all problems batched, the full-scale passes batched with each
+    problem's proposal candidate.  Its pass set A equals the per-problem
+    prior-net form's (hpm_run_scene_net) bit for bit, views of three sizes,
+    with and without an extra full-scale pass and for both planar priors
+    (the coarse triangulation's, the proposal)."""
+    import priornet
+
+    sc, imgs, pairs = _scene(63)
+    wts = priornet.Net(0, seed=3).weights()
+    opts = dict(seed=40, geom_iterations=0, pyramid_levels=extra, planar_prior=prior, net=wts)
+    with hb.Context() as ctx:
+        db, nb, cb = ctx.run_scene(imgs, sc.cams, pairs, batched=True, **opts)
+        db2, _, _ = ctx.run_scene(imgs, sc.cams, pairs, batched=True, **opts)  # contexts and graphs reused
+        dp, np_, cp = ctx.run_scene(imgs, sc.cams, pairs, **opts)
+    for ref, _ in pairs:
+        np.testing.assert_array_equal(db[ref], dp[ref])
+        np.testing.assert_array_equal(nb[ref], np_[ref])
+        np.testing.assert_array_equal(cb[ref], cp[ref])
+        np.testing.assert_array_equal(db2[ref], dp[ref])
+    assert np.mean([syn.depth_accuracy(db[v], sc.gt_depth[v]) for v in range(len(SIZES))]) > 0.2
