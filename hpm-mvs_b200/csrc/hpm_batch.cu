@@ -1,23 +1,25 @@
 /*
- * The batched form of a scene (hpm_run_scene_batched): every problem of the
- * scene advances together, one persistent launch per kernel and half-step
- * covering the tiles of all problems, whatever their sizes.
+ * The batched form of a scene (hpm_run_scene_batched, and with the network
+ * hpm_run_scene_batched_net): every problem of the scene advances together.
  *
  * The reference runs the problems one after another (main.cpp:658-674),
  * each with its own launches (HPM.cu:1906-1957).  Here each problem keeps
  * its own context (views and texture arrays, hypothesis state, hand-off
- * buffers); their kernel arguments sit side by side in device memory and a
- * work list maps every CTA iteration to a (problem, tile) pair
- * (hpm_pm.cu: k_init_batch, k_prop_dirs_batch, k_prop_refine_batch).
+ * buffers), and one pass of every problem (initialisation, the half-steps,
+ * depth/normal and the filter) is one CUDA graph: each problem's kernels
+ * form an independent chain of the graph, so that the problems' kernels run
+ * side by side and one problem's tail overlaps the others' work.  The
+ * kernels are the per-problem launches' own (hpm_pm.cu), with their
+ * arguments in the parameter space, so each problem's maps equal
+ * hpm_process_problem's on a fresh context bit for bit.
  *
- *  - One pass (initialisation, 6 half-steps, depth/normal and the filter)
- *    is captured once per scene as a CUDA graph and replayed for every pass
- *    that covers all problems; before each replay only the argument array is
- *    refreshed (seeds, pass flags).
+ *  - The graph is captured once per batch and kind of pass and, for every
+ *    later pass, re-captured with the pass's arguments (seeds, pass flags)
+ *    and applied to the instantiated graph by cudaGraphExecUpdate.
  *  - The half-step tile (pixels of one colour per warp row: 4, 8 or 16) is
  *    picked per view size by timing one half-step of each on the scene's
  *    first problem of that size (kept in the context for later scenes).
- *  - Pass set A advances in lock step: the plain pass of every problem, then
+ *  - Pass set A advances pass by pass: the plain pass of every problem, then
  *    each pyramid level's prior (built per problem on the host and device,
  *    as in hpm_process_problem) and the batched prior pass.  Problems whose
  *    pyramid is shorter join at its first level (levels aligned at the full
@@ -26,9 +28,12 @@
  *    view (as the view-sharded driver does); the reference's in-place order
  *    would serialise the problems.
  *
- * Per-pixel results do not depend on the tile shape or on which CTA
- * computes them, so pass set A equals hpm_process_problem's on a fresh
- * context per problem bit for bit.
+ * A first design ran all problems of a half-step as one persistent launch
+ * whose CTAs walked a (problem, tile) work list, the arguments read from
+ * device memory.  It measured 0.61x the per-problem driver on 24 views of
+ * three sizes (argument loads from global memory in the innermost loops,
+ * more register spills) and, compiled differently, was not bit-identical
+ * to it; the graph form replaced it.
  */
 #include <algorithm>
 #include <cmath>
@@ -66,97 +71,88 @@ __global__ void k_pack_maps(const float *__restrict__ normal3, const float *__re
     planes[i] = make_float4(normal3[3 * i], normal3[3 * i + 1], normal3[3 * i + 2], depth[i]);
 }
 
-/* A batch of problem contexts with its device work lists and, once
- * captured, the graph of one pass: one graph for the plain kernels and one
- * for the prior-net form's (the proposal candidate). */
+/* A batch of problem contexts, their half-step tile widths, and the
+ * instantiated graph of each kind of pass (keyed by the number of
+ * half-steps). */
 struct Plan {
     std::vector<hpm_ctx *> ctxs;
-    std::vector<PMArgs> args; /* host copy, refreshed per pass */
-    void *dev = nullptr;      /* args + work lists */
-    BatchList init{}, half{};
-    int smax = 0;
-    cudaGraphExec_t exec[2] = {nullptr, nullptr};
+    std::vector<int> ww;
+    std::vector<std::pair<int, cudaGraphExec_t>> graphs;
+    cudaEvent_t fork = nullptr;
+    std::vector<cudaEvent_t> join;
 
     ~Plan()
     {
-        for (cudaGraphExec_t e : exec)
-            if (e) cudaGraphExecDestroy(e);
-        cudaFree(dev);
+        for (auto &g : graphs) cudaGraphExecDestroy(g.second);
+        if (fork) cudaEventDestroy(fork);
+        for (cudaEvent_t e : join) cudaEventDestroy(e);
     }
 };
 
 int make_plan(hpm_ctx *c, const std::vector<hpm_ctx *> &ctxs, const std::vector<int> &ww, Plan &pl)
 {
-    const int n = (int)ctxs.size();
     pl.ctxs = ctxs;
-    pl.args.assign(n, PMArgs());
-    std::vector<int> ifirst(n + 1, 0), igx(n), hfirst(n + 1, 0), hgx(n);
-    pl.smax = 0;
-    for (int i = 0; i < n; ++i) {
-        const HpmCamera &cam = ctxs[i]->cams[0];
-        igx[i] = (cam.width + 31) / 32;
-        ifirst[i + 1] = ifirst[i] + igx[i] * ((cam.height + 1) / 2);
-        hfirst[i + 1] = hfirst[i] + half_step_tiles(cam.width, rows_covered(cam.height), ww[i], &hgx[i]);
-        pl.smax = std::max(pl.smax, ctxs[i]->n - 1);
-    }
-    const size_t argb = sizeof(PMArgs) * n, ints = sizeof(int) * (size_t)(5 * n + 2);
-    CK(cudaMalloc(&pl.dev, argb + ints), "batch lists");
-    std::vector<int> host;
-    host.insert(host.end(), ifirst.begin(), ifirst.end());
-    host.insert(host.end(), igx.begin(), igx.end());
-    host.insert(host.end(), hfirst.begin(), hfirst.end());
-    host.insert(host.end(), hgx.begin(), hgx.end());
-    host.insert(host.end(), ww.begin(), ww.end());
-    int *d = reinterpret_cast<int *>(static_cast<char *>(pl.dev) + argb);
-    CK(cudaMemcpy(d, host.data(), sizeof(int) * host.size(), cudaMemcpyHostToDevice), "batch lists");
-    const PMArgs *dargs = static_cast<const PMArgs *>(pl.dev);
-    pl.init = BatchList{dargs, d, d + n + 1, nullptr, n, ifirst[n]};
-    pl.half = BatchList{dargs, d + 2 * n + 1, d + 3 * n + 2, d + 4 * n + 2, n, hfirst[n]};
+    pl.ww = ww;
+    CK(cudaEventCreateWithFlags(&pl.fork, cudaEventDisableTiming), "batch events");
+    pl.join.assign(ctxs.size(), nullptr);
+    for (cudaEvent_t &e : pl.join) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "batch events");
     return HPM_OK;
 }
-
-/* the launches of one pass on stream s: initialisation, 6 half-steps,
- * depth/normal and the filter of every problem */
-cudaError_t launch_pass(const Plan &pl, bool proposals, cudaStream_t s)
-{
-    cudaError_t e = launch_batch_init(pl.init, 0, s);
-    for (int hs = 0; hs < 6 && e == cudaSuccess; ++hs)
-        e = launch_batch_propagate(pl.half, pl.smax, hs / 2, hs % 2, 0, proposals, s);
-    for (size_t i = 0; i < pl.ctxs.size() && e == cudaSuccess; ++i)
-        e = launch_depth_normal_filter(pl.args[i], reinterpret_cast<float4 *>(ctx_planes(pl.ctxs[i])),
-                                       ctx_costs(pl.ctxs[i]), s);
-    return e;
-}
-
-/* One batched pass with per-problem parameters; with the proposal
- * candidate when every problem has one (the prior-net form). */
-int batch_pass(hpm_ctx *c, Plan &pl, const std::vector<HpmParams> &params)
+/* One batched pass with per-problem parameters and `half_steps` half-steps
+ * (the reference's 6 unless the prior-net forms ask for fewer iterations).
+ * Each problem's chain goes to its own context's stream, forked from and
+ * joined back to c's stream, all captured as one graph; the graph of the
+ * previous pass of this kind is updated to the new arguments and replayed.
+ * A problem whose context holds proposals runs the prior-net form's
+ * refinement (the proposal as a candidate). */
+int batch_pass(hpm_ctx *c, Plan &pl, const std::vector<HpmParams> &params, int half_steps = 6)
 {
     cudaStream_t s = c->stream;
-    int with = 0;
-    for (size_t i = 0; i < pl.ctxs.size(); ++i) {
-        const int r = ctx_pass_args(pl.ctxs[i], &params[i], &pl.args[i]);
+    const size_t n = pl.ctxs.size();
+    std::vector<PMArgs> args(n);
+    for (size_t i = 0; i < n; ++i) {
+        const int r = ctx_pass_args(pl.ctxs[i], &params[i], &args[i]);
         if (r) return ctx_fail(c, r, "batched pass, problem %zu: %s", i, hpm_last_error(pl.ctxs[i]));
-        with += pl.args[i].proposals != nullptr;
     }
-    if (with != 0 && with != (int)pl.ctxs.size())
-        return ctx_fail(c, HPM_ERR_STATE, "batched pass: %d of %zu problems have proposals", with, pl.ctxs.size());
-    const int g_id = with ? 1 : 0;
-    CK(cudaMemcpyAsync(pl.dev, pl.args.data(), sizeof(PMArgs) * pl.args.size(), cudaMemcpyHostToDevice, s), "args");
-    if (!pl.exec[g_id]) {
-        /* capture the pass once; its kernels read their arguments from pl.dev,
-         * the per-problem finalisation's arguments do not change between passes */
-        cudaGraph_t g = nullptr;
-        CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "graph capture");
-        const cudaError_t le = launch_pass(pl, g_id == 1, s);
-        const cudaError_t ce = cudaStreamEndCapture(s, &g);
-        CK(le, "batched pass launches");
-        CK(ce, "graph capture");
-        const cudaError_t ie = cudaGraphInstantiate(&pl.exec[g_id], g, 0);
-        cudaGraphDestroy(g);
-        CK(ie, "graph instantiate");
+    cudaGraph_t g = nullptr;
+    CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "graph capture");
+    cudaError_t e = cudaEventRecord(pl.fork, s);
+    for (size_t i = 0; i < n && e == cudaSuccess; ++i) {
+        hpm_ctx *b = pl.ctxs[i];
+        const cudaStream_t bs = b->stream;
+        e = cudaStreamWaitEvent(bs, pl.fork, 0);
+        if (e == cudaSuccess) e = launch_init(args[i], bs);
+        for (int hs = 0; hs < half_steps && e == cudaSuccess; ++hs)
+            e = launch_propagate(args[i], hs / 2, hs % 2, bs, pl.ww[i]);
+        if (e == cudaSuccess)
+            e = launch_depth_normal_filter(args[i], reinterpret_cast<float4 *>(ctx_planes(b)), ctx_costs(b), bs);
+        if (e == cudaSuccess) e = cudaEventRecord(pl.join[i], bs);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(s, pl.join[i], 0);
     }
-    CK(cudaGraphLaunch(pl.exec[g_id], s), "graph launch");
+    const cudaError_t ce = cudaStreamEndCapture(s, &g);
+    if (e == cudaSuccess) e = ce;
+    if (e != cudaSuccess) {
+        if (g) cudaGraphDestroy(g);
+        return ctx_cuda_fail(c, e, "batched pass capture");
+    }
+    cudaGraphExec_t *exec = nullptr;
+    for (auto &x : pl.graphs)
+        if (x.first == half_steps) exec = &x.second;
+    if (exec) {
+        cudaGraphExecUpdateResultInfo info;
+        if (cudaGraphExecUpdate(*exec, g, &info) != cudaSuccess) {
+            cudaGetLastError(); /* topology changed: instantiate anew */
+            cudaGraphExecDestroy(*exec);
+            *exec = nullptr;
+        }
+    } else {
+        pl.graphs.push_back({half_steps, nullptr});
+        exec = &pl.graphs.back().second;
+    }
+    e = *exec ? cudaSuccess : cudaGraphInstantiate(exec, g, 0);
+    cudaGraphDestroy(g);
+    CK(e, "graph instantiate");
+    CK(cudaGraphLaunch(*exec, s), "graph launch");
     CK(cudaStreamSynchronize(s), "batched pass");
     return HPM_OK;
 }
@@ -176,30 +172,27 @@ int tune_tiles(hpm_ctx *c, const std::vector<hpm_ctx *> &ctxs, const std::vector
             if (kv.first == key) found = kv.second;
         if (!found) {
             float best = 1e30f;
+            cudaEvent_t e0, e1;
+            CK(cudaEventCreate(&e0), "tuning events");
+            CK(cudaEventCreate(&e1), "tuning events");
             for (int cand : {4, 8, 16}) {
-                Plan one;
-                int r = make_plan(c, {ctxs[i]}, {cand}, one);
-                if (r) return r;
-                r = ctx_pass_args(ctxs[i], &params[i], &one.args[0]);
+                PMArgs a;
+                const int r = ctx_pass_args(ctxs[i], &params[i], &a);
                 if (r) return ctx_fail(c, r, "tile tuning: %s", hpm_last_error(ctxs[i]));
-                CK(cudaMemcpy(one.dev, one.args.data(), sizeof(PMArgs), cudaMemcpyHostToDevice), "args");
-                CK(launch_batch_init(one.init, 0, c->stream), "tuning init");
-                cudaEvent_t e0, e1;
-                cudaEventCreate(&e0);
-                cudaEventCreate(&e1);
-                cudaEventRecord(e0, c->stream);
-                CK(launch_batch_propagate(one.half, one.smax, 0, 0, 0, false, c->stream), "tuning half-step");
-                cudaEventRecord(e1, c->stream);
+                CK(launch_init(a, c->stream), "tuning init");
+                CK(cudaEventRecord(e0, c->stream), "tuning");
+                CK(launch_propagate(a, 0, 0, c->stream, cand), "tuning half-step");
+                CK(cudaEventRecord(e1, c->stream), "tuning");
                 CK(cudaEventSynchronize(e1), "tuning");
                 float ms = 0.0f;
-                cudaEventElapsedTime(&ms, e0, e1);
-                cudaEventDestroy(e0);
-                cudaEventDestroy(e1);
+                CK(cudaEventElapsedTime(&ms, e0, e1), "tuning");
                 if (ms < best) {
                     best = ms;
                     found = cand;
                 }
             }
+            cudaEventDestroy(e0);
+            cudaEventDestroy(e1);
             c->tile_ww.push_back({key, found});
             ctx_reset_salt(ctxs[i]);
         }
@@ -207,7 +200,6 @@ int tune_tiles(hpm_ctx *c, const std::vector<hpm_ctx *> &ctxs, const std::vector
     }
     return HPM_OK;
 }
-
 /* Pass set A in the prior-net form for every problem of pc (full-scale
  * views set): the 1/4-scale plain passes as one batched pass over the
  * problems' coarse sub-contexts, per problem the coarse planar prior, the
@@ -215,7 +207,7 @@ int tune_tiles(hpm_ctx *c, const std::vector<hpm_ctx *> &ctxs, const std::vector
  * batched full-scale passes with the proposal candidate; seeds as
  * net_problem's, so each problem's maps equal it bit for bit. */
 int net_pass_set_a(hpm_ctx *c, const std::vector<hpm_ctx *> &pc, const std::vector<HpmParams> &params, Plan &all,
-                   const HpmNetWeights *net, int extra_passes, int prior_mode,
+                   const HpmNetWeights *net, int extra_passes, int prior_mode, int half_steps,
                    const std::vector<std::vector<const float *>> &images)
 {
     const int n = (int)pc.size();
@@ -257,7 +249,7 @@ int net_pass_set_a(hpm_ctx *c, const std::vector<hpm_ctx *> &pc, const std::vect
             fp[p].planar_prior = 1;
             fp[p].seed = net_pass_seed(params[p].seed, e);
         }
-        const int r = batch_pass(c, all, fp);
+        const int r = batch_pass(c, all, fp, half_steps);
         if (r) return r;
     }
     for (int p = 0; p < n; ++p) {
@@ -288,6 +280,9 @@ int batched_scene(hpm_ctx *c, int n_views, const float *const *images, const Hpm
     int r = ctx_select_device(c);
     if (r) return r;
     const Range range(net ? "batched scene %d views (prior-net form)" : "batched scene %d views", n_views);
+    if (o->iterations < 0 || o->iterations > 64)
+        return ctx_fail(c, HPM_ERR_ARG, "hpm_run_scene_batched: iterations outside [0, 64]");
+    const int half_steps = net && o->iterations > 0 ? 2 * o->iterations : 6;
     cudaStream_t s = c->stream;
     /* per view: image, pass-A depth, two geometric depth buffers, normal (3), cost */
     std::vector<float *> img(n_views), dep_a(n_views), dep_g0(n_views), dep_g1(n_views), nrm(n_views), cst(n_views);
@@ -311,10 +306,9 @@ int batched_scene(hpm_ctx *c, int n_views, const float *const *images, const Hpm
     /* one context per problem, kept for later scenes */
     while ((int)c->batch.size() < n_problems) {
         hpm_ctx *b = nullptr;
-        r = hpm_create(&b, c->device);
+        r = ctx_create_child(c, &b);
+        if (b) c->batch.push_back(b); /* owned by c from here, freed with it */
         if (r) return ctx_fail(c, r, "hpm_run_scene_batched: problem context");
-        hpm_set_scene_workers(b, 1);
-        c->batch.push_back(b);
     }
     std::vector<hpm_ctx *> pc(c->batch.begin(), c->batch.begin() + n_problems);
     std::vector<HpmParams> params(n_problems);
@@ -353,7 +347,7 @@ int batched_scene(hpm_ctx *c, int n_views, const float *const *images, const Hpm
     if (net) {
         /* pass set A in the prior-net form */
         r = net_pass_set_a(c, pc, params, all, net, o->pyramid_levels > 0 ? o->pyramid_levels : 0,
-                           o->planar_prior, pimgs);
+                           o->planar_prior, half_steps, pimgs);
         if (r) return r;
     } else {
         /* pass set A: the plain pass of every problem */
@@ -426,7 +420,7 @@ int batched_scene(hpm_ctx *c, int n_views, const float *const *images, const Hpm
             gp[p].seed = o->seed + 1000003ull * (gi + 1) + (uint64_t)p;
         }
         CK(cudaStreamSynchronize(s), "geometric set-up");
-        r = batch_pass(c, all, gp);
+        r = batch_pass(c, all, gp, half_steps);
         if (r) return r;
         for (int p = 0; p < n_problems; ++p) {
             const int ref = ref_ids[p];

@@ -650,6 +650,18 @@ int hpm_jbu(hpm_ctx *c, const float *guide, int cols, int rows, const float *coa
     return HPM_OK;
 }
 
+/* The contexts a context runs work on besides itself: the second
+ * scene-worker context, the prior-net form's coarse context, the batched
+ * form's problem contexts.  Counters and profiles cover them all. */
+static std::vector<hpm_ctx *> child_contexts(hpm_ctx *c)
+{
+    std::vector<hpm_ctx *> out;
+    if (c->peer) out.push_back(c->peer);
+    if (c->coarse) out.push_back(c->coarse);
+    for (hpm_ctx *b : c->batch) out.push_back(b);
+    return out;
+}
+
 int hpm_profile_enable(hpm_ctx *c, int enable)
 {
     if (!c) return HPM_ERR_ARG;
@@ -663,7 +675,7 @@ int hpm_profile_enable(hpm_ctx *c, int enable)
         cudaEventDestroy(p.second.second);
     }
     c->prof_events.clear();
-    if (c->peer) hpm_profile_enable(c->peer, enable);
+    for (hpm_ctx *k : child_contexts(c)) hpm_profile_enable(k, enable);
     return HPM_OK;
 }
 
@@ -672,9 +684,15 @@ int hpm_profile_read(hpm_ctx *c, float *ms4, int *counts4)
     if (!c) return HPM_ERR_ARG;
     float peer_ms[4] = {0, 0, 0, 0};
     int peer_cnt[4] = {0, 0, 0, 0};
-    if (c->peer) {
-        const int r = hpm_profile_read(c->peer, peer_ms, peer_cnt);
-        if (r) return fail(c, r, "hpm_profile_read (second context): %s", hpm_last_error(c->peer));
+    for (hpm_ctx *k : child_contexts(c)) {
+        float ms[4];
+        int cnt[4];
+        const int r = hpm_profile_read(k, ms, cnt);
+        if (r) return fail(c, r, "hpm_profile_read (inner context): %s", hpm_last_error(k));
+        for (int i = 0; i < 4; ++i) {
+            peer_ms[i] += ms[i];
+            peer_cnt[i] += cnt[i];
+        }
     }
     CK(cudaStreamSynchronize(c->stream), "hpm_profile_read");
     for (auto &p : c->prof_events) {
@@ -712,9 +730,9 @@ int hpm_count_enable(hpm_ctx *c, int enable)
         CK(cudaStreamSynchronize(c->stream), "hpm_count_enable");
     }
     c->counting = enable != 0;
-    if (c->peer) {
-        const int r = hpm_count_enable(c->peer, enable);
-        if (r) return fail(c, r, "hpm_count_enable (second context): %s", hpm_last_error(c->peer));
+    for (hpm_ctx *k : child_contexts(c)) {
+        const int r = hpm_count_enable(k, enable);
+        if (r) return fail(c, r, "hpm_count_enable (inner context): %s", hpm_last_error(k));
     }
     return HPM_OK;
 }
@@ -723,9 +741,12 @@ int hpm_count_read(hpm_ctx *c, uint64_t *cv, uint64_t *geom)
 {
     if (!c) return HPM_ERR_ARG;
     uint64_t peer_cv = 0, peer_geom = 0;
-    if (c->peer) {
-        const int r = hpm_count_read(c->peer, &peer_cv, &peer_geom);
-        if (r) return fail(c, r, "hpm_count_read (second context): %s", hpm_last_error(c->peer));
+    for (hpm_ctx *k : child_contexts(c)) {
+        uint64_t cv = 0, geom = 0;
+        const int r = hpm_count_read(k, &cv, &geom);
+        if (r) return fail(c, r, "hpm_count_read (inner context): %s", hpm_last_error(k));
+        peer_cv += cv;
+        peer_geom += geom;
     }
     unsigned long long h[2] = {0, 0};
     CK(cudaMemcpyAsync(h, c->d_counters, sizeof(h), cudaMemcpyDeviceToHost, c->stream), "counters");
@@ -751,6 +772,15 @@ int ctx_fail(hpm_ctx *c, int code, const char *fmt, ...)
 }
 
 int ctx_cuda_fail(hpm_ctx *c, cudaError_t e, const char *what) { return cuda_fail(c, e, what); }
+int ctx_create_child(hpm_ctx *c, hpm_ctx **child)
+{
+    int r = hpm_create(child, c->device);
+    if (r) return r;
+    (*child)->scene_workers = 1;
+    if (c->profiling) hpm_profile_enable(*child, 1);
+    if (c->counting) r = hpm_count_enable(*child, 1);
+    return r;
+}
 int ctx_select_device(hpm_ctx *c) { return select_device(c); }
 int ctx_run_pass(hpm_ctx *c, const HpmParams *p, int half_steps, int finalize)
 {

@@ -139,6 +139,9 @@ int ctx_select_device(hpm_ctx *c);
 /* one pass: init, `half_steps` red/black half-steps, optional finalisation;
  * synchronises the context's stream at the end */
 int ctx_run_pass(hpm_ctx *c, const HpmParams *p, int half_steps, int finalize);
+/* a context on c's device for c's own use (second worker, coarse views,
+ * batched problems), counting and profiling when c does */
+int ctx_create_child(hpm_ctx *c, hpm_ctx **child);
 float *ctx_planes(hpm_ctx *c);
 cudaError_t ctx_scene_arena(hpm_ctx *c, size_t bytes);
 float *ctx_scene_base(hpm_ctx *c);
@@ -180,6 +183,6 @@ int net_full_setup(hpm_ctx *c, const HpmNetWeights *net, int prior_mode);
 uint64_t net_pass_seed(uint64_t seed, int pass);
 int net_status(hpm_ctx *c);
 int net_problem(hpm_ctx *c, int n, const float *const *images, const HpmCamera *cams, const HpmNetWeights *net,
-                uint64_t seed, int extra_passes, int prior_mode, float *depth_out, float *normal_out,
+                uint64_t seed, int extra_passes, int prior_mode, int half_steps, float *depth_out, float *normal_out,
                 float *cost_out);
 }  // namespace hpm

@@ -223,8 +223,10 @@ extern "C" int hpm_prior_level(hpm_ctx *c, int level, const float *depth, const 
     return r;
 }
 
-extern "C" int hpm_process_problem(hpm_ctx *c, const HpmProblemOpts *o, float *depth_out, float *normal_out,
-                                   float *cost_out, float *prior_depth_out)
+/* hpm_process_problem with `half_steps` half-steps per pass (the reference's
+ * 6 everywhere but in the prior-net forms' geometric passes) */
+static int process_problem(hpm_ctx *c, const HpmProblemOpts *o, int half_steps, float *depth_out, float *normal_out,
+                           float *cost_out, float *prior_depth_out)
 {
     if (!c || !o) return HPM_ERR_ARG;
     if (c->n < 2) return ctx_fail(c, HPM_ERR_STATE, "hpm_process_problem before hpm_set_views");
@@ -245,10 +247,10 @@ extern "C" int hpm_process_problem(hpm_ctx *c, const HpmProblemOpts *o, float *d
     if (o->geom_consistency) {
         p.geom_consistency = 1;
         p.multi_geometry = o->multi_geometry;
-        r = ctx_run_pass(c, &p, 6, 1);
+        r = ctx_run_pass(c, &p, half_steps, 1);
         if (r) return r;
     } else {
-        r = ctx_run_pass(c, &p, 6, 1);
+        r = ctx_run_pass(c, &p, half_steps, 1);
         if (r) return r;
         if (o->planar_prior) {
             CK(ws_reserve_full(c, npx), "flow workspace");
@@ -261,7 +263,7 @@ extern "C" int hpm_process_problem(hpm_ctx *c, const HpmProblemOpts *o, float *d
                 r = level_prior_from_maps(c, i, ctx_costs(c), p.depth_min, p.depth_max);
                 if (r) return r;
                 p.planar_prior = 1;
-                r = ctx_run_pass(c, &p, 6, 1);
+                r = ctx_run_pass(c, &p, half_steps, 1);
                 if (r) return r;
             }
         }
@@ -288,6 +290,12 @@ extern "C" int hpm_process_problem(hpm_ctx *c, const HpmProblemOpts *o, float *d
     }
     CK(cudaStreamSynchronize(s), "hpm_process_problem");
     return HPM_OK;
+}
+
+extern "C" int hpm_process_problem(hpm_ctx *c, const HpmProblemOpts *o, float *depth_out, float *normal_out,
+                                   float *cost_out, float *prior_depth_out)
+{
+    return process_problem(c, o, 6, depth_out, normal_out, cost_out, prior_depth_out);
 }
 
 extern "C" int hpm_last_prior_stats(hpm_ctx *c, int *points, int *triangles)
@@ -374,6 +382,9 @@ static int run_scene_impl(hpm_ctx *c, int n_views, const float *const *images, c
     int r = ctx_select_device(c);
     if (r) return r;
     const Range range(net ? "scene %d views (prior-net form)" : "scene %d views", n_views);
+    if (o->iterations < 0 || o->iterations > 64)
+        return ctx_fail(c, HPM_ERR_ARG, "hpm_run_scene: iterations outside [0, 64]");
+    const int half_steps = net && o->iterations > 0 ? 2 * o->iterations : 6;
     cudaStream_t s = c->stream;
     SceneMaps m;
     size_t total = 0; /* floats: image, pass-A depth, geometric depth, normal (3), cost */
@@ -416,14 +427,9 @@ static int run_scene_impl(hpm_ctx *c, int n_views, const float *const *images, c
     {
         const int workers = (c->scene_workers > 1 && n_problems > 1) ? 2 : 1;
         if (workers == 2 && !c->peer) {
-            r = hpm_create(&c->peer, c->device);
-            if (r) return ctx_fail(c, r, "hpm_run_scene: second context");
             /* the peer's work is profiled and counted with this context's */
-            if (c->profiling) hpm_profile_enable(c->peer, 1);
-            if (c->counting) {
-                r = hpm_count_enable(c->peer, 1);
-                if (r) return ctx_fail(c, r, "hpm_run_scene: second context counters");
-            }
+            r = ctx_create_child(c, &c->peer);
+            if (r) return ctx_fail(c, r, "hpm_run_scene: second context");
         }
         std::mutex token;
         hpm_ctx *ctxs[2] = {c, workers == 2 ? c->peer : nullptr};
@@ -442,8 +448,8 @@ static int run_scene_impl(hpm_ctx *c, int n_views, const float *const *images, c
                     HpmCamera pcam[kMaxViews];
                     const int n = gather(p, pimg, pcam), ref = ref_ids[p];
                     rr = net_problem(cc, n, pimg, pcam, net, o->seed + (uint64_t)p,
-                                     o->pyramid_levels > 0 ? o->pyramid_levels : 0, o->planar_prior, m.depth_a[ref],
-                                     m.normal[ref], m.cost[ref]);
+                                     o->pyramid_levels > 0 ? o->pyramid_levels : 0, o->planar_prior, half_steps,
+                                     m.depth_a[ref], m.normal[ref], m.cost[ref]);
                     if (rr == HPM_OK && out_prior_depths && out_prior_depths[ref])
                         rr = cudaMemsetAsync(out_prior_depths[ref], 0,
                                              sizeof(float) * cams[ref].width * cams[ref].height, cc->stream) ==
@@ -501,7 +507,7 @@ static int run_scene_impl(hpm_ctx *c, int n_views, const float *const *images, c
             CK(cudaMemcpyAsync(ctx_costs(c), m.cost[ref], sizeof(float) * np, cudaMemcpyDeviceToDevice, s), "costs");
             HpmProblemOpts po = {0, 1, gi >= 1, o->seed + 1000003ull * (gi + 1) + (uint64_t)p, o->pyramid_levels};
             /* the geometric depth map is rewritten view by view (depths_geom.dmb) */
-            r = hpm_process_problem(c, &po, m.depth_g[ref], m.normal[ref], m.cost[ref], nullptr);
+            r = process_problem(c, &po, net ? half_steps : 6, m.depth_g[ref], m.normal[ref], m.cost[ref], nullptr);
             if (r) return r;
         }
     }

@@ -72,7 +72,8 @@ struct PMArgs {
 /* Launchers (hpm_pm.cu / hpm_jbu.cu). All asynchronous on `s`. */
 cudaError_t launch_pair_geom(const PMArgs &a, PairGeom *out, cudaStream_t s);
 cudaError_t launch_init(const PMArgs &a, cudaStream_t s);
-cudaError_t launch_propagate(const PMArgs &a, int iter, int color, cudaStream_t s);
+/* one red/black half-step; ww = pixels of one colour per warp row (4, 8 or 16) */
+cudaError_t launch_propagate(const PMArgs &a, int iter, int color, cudaStream_t s, int ww = 8);
 cudaError_t launch_depth_normal_filter(const PMArgs &a, float4 *planes, const float *costs, cudaStream_t s);
 cudaError_t launch_cost_vectors(const PMArgs &a, const float4 *planes, float *out, cudaStream_t s);
 cudaError_t launch_initial_costs(const PMArgs &a, const float4 *planes, float *cost, uint32_t *views,
@@ -85,28 +86,5 @@ cudaError_t launch_jbu(const float *guide, int cols, int rows, const float *coar
                        float4 *out_normal, cudaStream_t s);
 
 int rows_covered(int H);
-
-/* A batch of problems for one persistent launch: problem p's PMArgs sit in
- * args[p] (device memory) and its work items are [first[p], first[p + 1]):
- * item i of problem p is tile (i % gx[p], i / gx[p]); half-step tiles have
- * warps of ww[p] pixels of one colour per row over 32 / ww[p] rows, the
- * initialisation's tiles are 32 x 2 pixels. */
-struct BatchList {
-    const PMArgs *args;
-    const int *first; /* [n + 1] */
-    const int *gx;    /* [n] */
-    const int *ww;    /* [n], half-step lists only */
-    int n;
-    int total;
-};
-
-/* Persistent launches over a batch (hpm_pm.cu); ctas = 0 picks the number
- * of CTAs that fit on the device at once. */
-cudaError_t launch_batch_init(const BatchList &b, int ctas, cudaStream_t s);
-/* proposals: every problem of b is in the prior-net form (args.proposals set) */
-cudaError_t launch_batch_propagate(const BatchList &b, int smax, int iter, int color, int ctas, bool proposals,
-                                   cudaStream_t s);
-/* grid width of problem a's half-step tiles of width ww, and their count */
-int half_step_tiles(int W, int rows_cov, int ww, int *gx);
 
 }  // namespace hpm

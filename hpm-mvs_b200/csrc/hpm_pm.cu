@@ -44,21 +44,15 @@ constexpr int kBlockX = 32;
 constexpr int kBlockY = 2;
 constexpr int kBlock = kBlockX * kBlockY;
 
-/* Pixels of one half-step (one checkerboard colour) per warp: kWarpW per
- * row over kWarpH rows, so that the 32 lanes sample a compact 2D patch of
- * each source image (the texture cache is tiled in 2D).  A block is two
- * such warps stacked vertically. */
-#ifndef HPM_WARP_W
-#define HPM_WARP_W 8
-#endif
-constexpr int kWarpW = HPM_WARP_W;
-constexpr int kWarpH = 32 / kWarpW;
-static_assert(kWarpW * kWarpH == 32 && kBlock == 64, "two warps per block");
+/* Pixels of one half-step (one checkerboard colour) per warp: ww per row
+ * over 32 / ww rows, so that the 32 lanes sample a compact 2D patch of each
+ * source image (the texture cache is tiled in 2D).  A block is two such
+ * warps stacked vertically.  ww is 8 unless the batched form's tile tuning
+ * picks 4 or 16 for a view size. */
+static_assert(kBlock == 64, "two warps per block");
 
 /* (px, py) of this thread in a half-step of `color`, for the block's tile
- * (bx, by) of tiles whose warps cover ww pixels of one colour per row over
- * 32 / ww rows (the plain launches use ww = kWarpW and the block index; the
- * batched launches take both from their work list) */
+ * (bx, by) */
 __device__ __forceinline__ void half_step_pixel_at(int bx, int by, int ww, int color, int &px, int &py)
 {
     const int lane = threadIdx.x, wv = threadIdx.y, wh = 32 / ww;
@@ -66,10 +60,6 @@ __device__ __forceinline__ void half_step_pixel_at(int bx, int by, int ww, int c
     px = bx * (2 * ww) + 2 * (lane % ww) + ((py + color) & 1);
 }
 
-__device__ __forceinline__ void half_step_pixel(int color, int &px, int &py)
-{
-    half_step_pixel_at(blockIdx.x, blockIdx.y, kWarpW, color, px, py);
-}
 #ifndef HPM_CV_INLINE
 #define HPM_CV_INLINE __noinline__
 #endif
@@ -400,79 +390,6 @@ __device__ __forceinline__ float ncc(const PMArgs &a, int v, int px, int py, flo
     const float covar = sum_ref_src - rs.mean * sum_src;
     const float vv = sqrtf(rs.var * var_src);
     return fmaxf(0.0f, fminf(2.0f, 1.0f - covar / vv));
-}
-
-/* ncc() of two planes with the same depth at the pixel (the window centres
- * coincide in every source view) in one tap loop: each tap fetches both
- * samples, so that two texture requests are in flight and the second finds
- * most of its texels in L1.  Each NCC keeps ncc()'s own accumulation order,
- * so both results equal ncc()'s bit for bit. */
-template <typename Win>
-__device__ __forceinline__ float2 ncc_pair(const PMArgs &a, int v, int px, int py, float4 h0, float4 h1,
-                                           const Win *sWW, int tid, const RefStats &rs)
-{
-    const HpmCamera &sc = a.cam[v];
-    float H0[9], H1[9];
-    homography(a.cam[0], sc, a.pair[v], h0, H0);
-    homography(a.cam[0], sc, a.pair[v], h1, H1);
-    const float fpx = (float)px, fpy = (float)py;
-    const float2 p0 = warp(H0, fpx, fpy), p1 = warp(H1, fpx, fpy);
-    const bool in0 = !(p0.x >= sc.width || p0.x < 0.0f || p0.y >= sc.height || p0.y < 0.0f);
-    const bool in1 = !(p1.x >= sc.width || p1.x < 0.0f || p1.y >= sc.height || p1.y < 0.0f);
-    if ((!in0 && !in1) || rs.var < 1e-5f) return make_float2(2.0f, 2.0f);
-    const cudaTextureObject_t tex = a.view[v].tex;
-    float s0 = 0.0f, ss0 = 0.0f, rs0 = 0.0f, s1 = 0.0f, ss1 = 0.0f, rs1 = 0.0f;
-    int t = 0;
-#pragma unroll
-    for (int i = -5; i < 6; i += 2) {
-        float a0 = 0.0f, b0 = 0.0f, c0 = 0.0f, a1 = 0.0f, b1 = 0.0f, c1 = 0.0f;
-#pragma unroll
-        for (int j = -5; j < 6; j += 2, ++t) {
-            const float sp0 = in0 ? tap_sample(tex, H0, fpx, fpy, i, j) : 0.0f;
-            const float sp1 = in1 ? tap_sample(tex, H1, fpx, fpy, i, j) : 0.0f;
-            float2 ww;
-            if constexpr (sizeof(Win) == sizeof(float)) {
-                const float wt = sWW[t * kBlock + tid];
-                ww = make_float2(wt, wt * texel(a.view[0].img, a.view[0].w, a.view[0].h, px + i, py + j));
-            } else {
-                ww = sWW[t * kBlock + tid];
-            }
-            a0 += ww.x * sp0;
-            b0 += ww.x * sp0 * sp0;
-            c0 += ww.y * sp0;
-            a1 += ww.x * sp1;
-            b1 += ww.x * sp1 * sp1;
-            c1 += ww.y * sp1;
-        }
-        s0 += a0;
-        ss0 += b0;
-        rs0 += c0;
-        s1 += a1;
-        ss1 += b1;
-        rs1 += c1;
-    }
-    float2 out = make_float2(2.0f, 2.0f);
-    if (in0) {
-        s0 *= rs.inv;
-        ss0 *= rs.inv;
-        rs0 *= rs.inv;
-        const float var0 = ss0 - s0 * s0;
-        if (!(var0 < 1e-5f)) {
-            const float cov = rs0 - rs.mean * s0;
-            out.x = fmaxf(0.0f, fminf(2.0f, 1.0f - cov / sqrtf(rs.var * var0)));
-        }
-    }
-    if (in1) {
-        s1 *= rs.inv;
-        ss1 *= rs.inv;
-        rs1 *= rs.inv;
-        const float var1 = ss1 - s1 * s1;
-        if (!(var1 < 1e-5f)) {
-            const float cov = rs1 - rs.mean * s1;
-            out.y = fmaxf(0.0f, fminf(2.0f, 1.0f - cov / sqrtf(rs.var * var1)));
-        }
-    }
-    return out;
 }
 
 /* One NCC window for the loops that score several candidates view by view
@@ -912,13 +829,16 @@ __device__ __forceinline__ void prop_dirs_body(const PMArgs &a, int iter, int px
     a.cand_flags[center] = code;
 }
 
+/* WW: pixels of one colour per warp row (the half-step tile, tuned per view
+ * size by the batched form; 8 elsewhere) */
+template <int WW>
 __global__ void __launch_bounds__(kBlock, HPM_P1_MIN_BLOCKS) k_prop_dirs(const __grid_constant__ PMArgs a, int iter,
                                                                           int color)
 {
     __shared__ WinPair sWW[kTaps * kBlock];
     const int tid = threadIdx.y * kBlockX + threadIdx.x;
     int px, py;
-    half_step_pixel(color, px, py);
+    half_step_pixel_at(blockIdx.x, blockIdx.y, WW, color, px, py);
     prop_dirs_body(a, iter, px, py, sWW, tid);
 }
 
@@ -926,7 +846,7 @@ __global__ void __launch_bounds__(kBlock, HPM_P1_MIN_BLOCKS) k_prop_dirs(const _
  * sixth refinement candidate, scored by the same NCC (and prior terms) as the
  * other five and accepted by the same rule.  It takes no random draws, so
  * the random stream of the other candidates is unchanged. */
-template <int SMAX, bool PROP, bool PAIR = false>
+template <int SMAX, bool PROP>
 __device__ __forceinline__ void prop_refine_body(const PMArgs &a, int iter, int px, int py, WinPair *sWW, int tid)
 {
     if (px >= a.W || py >= a.rows_cov) return;
@@ -1199,24 +1119,8 @@ __device__ __forceinline__ void prop_refine_body(const PMArgs &a, int iter, int 
         for (int v = 0; v < S; ++v) {
             const bool selected = (tsv >> v) & 1u;
             const float w = (float)((v < 16 ? (vw_lo >> (4 * v)) : (vw_hi >> (4 * (v - 16)))) & 15ull);
-            if constexpr (PAIR) {
-                /* candidates 0 and 2 share the random depth: one tap loop */
-                const float2 c02 = ncc_pair(a, v + 1, px, py, cand[0], cand[2], sWW, tid, rs);
-#pragma unroll
-                for (int q = 0; q < 2; ++q) {
-                    const int i = 2 * q;
-                    const float c = q ? c02.y : c02.x;
-                    CAG(kRefineRow + i, v) = c;
-                    if (selected) {
-                        if (a.geom)
-                            tc[i] += w * (c + 0.1f * geom_cost(a, v + 1, cand[i], px, py));
-                        else
-                            tc[i] += w * c;
-                    }
-                }
-            }
 #pragma unroll 1
-            for (int k = PAIR ? 2 : 0; k < NC; ++k) {
+            for (int k = 0; k < NC; ++k) {
                 /* candidates 0 and 2 share the random depth, hence the window
                  * centre in every source view; 1, 3 and 4 sit at or near the
                  * current depth: scoring 0, 2, 1, 3, 4 keeps windows with the
@@ -1266,15 +1170,15 @@ __device__ __forceinline__ void prop_refine_body(const PMArgs &a, int iter, int 
 #undef FLAG
 }
 
-template <int SMAX, bool PROP, bool PAIR>
+template <int SMAX, bool PROP, int WW>
 __global__ void __launch_bounds__(kBlock, HPM_P2_MIN_BLOCKS) k_prop_refine(const __grid_constant__ PMArgs a, int iter,
                                                                             int color)
 {
     __shared__ WinPair sWW[kTaps * kBlock];
     const int tid = threadIdx.y * kBlockX + threadIdx.x;
     int px, py;
-    half_step_pixel(color, px, py);
-    prop_refine_body<SMAX, PROP, PAIR>(a, iter, px, py, sWW, tid);
+    half_step_pixel_at(blockIdx.x, blockIdx.y, WW, color, px, py);
+    prop_refine_body<SMAX, PROP>(a, iter, px, py, sWW, tid);
 }
 #undef CAG
 
@@ -1391,121 +1295,28 @@ __global__ void k_tap_samples(const __grid_constant__ PMArgs a, const float4 *pl
         for (int j = -5; j < 6; j += 2, ++t) out[(size_t)k * kTaps + t] = tap_sample(a.view[v].tex, H, fpx, fpy, i, j);
 }
 
-/* ------------------------------------------------------------------ */
-/* Batched persistent launches: every problem of a batch in one launch  */
-/* ------------------------------------------------------------------ */
-
-/* the problem that owns work item id: the largest p with first[p] <= id */
-__device__ __forceinline__ int batch_problem(const int *first, int n, int id)
-{
-    int lo = 0, hi = n - 1;
-    while (lo < hi) {
-        const int mid = (lo + hi + 1) >> 1;
-        if (first[mid] <= id)
-            lo = mid;
-        else
-            hi = mid - 1;
-    }
-    return lo;
-}
-
-__global__ void __launch_bounds__(kBlock) k_init_batch(const __grid_constant__ BatchList b)
-{
-    __shared__ WinWeight sWW[kTaps * kBlock];
-    __shared__ float sCV[kMaxSrc * kBlock];
-    const int tid = threadIdx.y * kBlockX + threadIdx.x;
-    for (int id = blockIdx.x; id < b.total; id += gridDim.x) {
-        const int p = batch_problem(b.first, b.n, id), local = id - b.first[p];
-        const int bx = local % b.gx[p], by = local / b.gx[p];
-        init_body(b.args[p], bx * kBlockX + threadIdx.x, by * kBlockY + threadIdx.y, sWW, sCV, tid);
-    }
-}
-
-__global__ void __launch_bounds__(kBlock, HPM_P1_MIN_BLOCKS) k_prop_dirs_batch(const __grid_constant__ BatchList b,
-                                                                                int iter, int color)
-{
-    __shared__ WinPair sWW[kTaps * kBlock];
-    const int tid = threadIdx.y * kBlockX + threadIdx.x;
-    for (int id = blockIdx.x; id < b.total; id += gridDim.x) {
-        const int p = batch_problem(b.first, b.n, id), local = id - b.first[p];
-        int px, py;
-        half_step_pixel_at(local % b.gx[p], local / b.gx[p], b.ww[p], color, px, py);
-        prop_dirs_body(b.args[p], iter, px, py, sWW, tid);
-    }
-}
-
-/* PROP: every problem of the list is in the prior-net form (its
- * args.proposals set) */
-template <int SMAX, bool PROP>
-__global__ void __launch_bounds__(kBlock, HPM_P2_MIN_BLOCKS) k_prop_refine_batch(const __grid_constant__ BatchList b,
-                                                                                  int iter, int color)
-{
-    __shared__ WinPair sWW[kTaps * kBlock];
-    const int tid = threadIdx.y * kBlockX + threadIdx.x;
-    for (int id = blockIdx.x; id < b.total; id += gridDim.x) {
-        const int p = batch_problem(b.first, b.n, id), local = id - b.first[p];
-        int px, py;
-        half_step_pixel_at(local % b.gx[p], local / b.gx[p], b.ww[p], color, px, py);
-        prop_refine_body<SMAX, PROP>(b.args[p], iter, px, py, sWW, tid);
-    }
-}
-
-template <typename K>
-int resident_ctas(K kern)
-{
-    int dev = 0, sms = 0, per_sm = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) !=
-                                                  cudaSuccess ||
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kBlock, 0) != cudaSuccess)
-        return 148 * 8;
-    return sms * (per_sm > 0 ? per_sm : 1);
-}
-
-template <int SMAX, bool PROP>
-cudaError_t launch_batch_prop_t(const BatchList &b, int iter, int color, int ctas, cudaStream_t s)
-{
-    const dim3 blk(kBlockX, kBlockY);
-    const int c1 = ctas > 0 ? ctas : resident_ctas(k_prop_dirs_batch);
-    k_prop_dirs_batch<<<b.total < c1 ? b.total : c1, blk, 0, s>>>(b, iter, color);
-    const int c2 = ctas > 0 ? ctas : resident_ctas(k_prop_refine_batch<SMAX, PROP>);
-    k_prop_refine_batch<SMAX, PROP><<<b.total < c2 ? b.total : c2, blk, 0, s>>>(b, iter, color);
-    return cudaGetLastError();
-}
-
-template <bool PROP>
-cudaError_t launch_batch_prop_s(const BatchList &b, int smax, int iter, int color, int ctas, cudaStream_t s)
-{
-    if (smax <= 4) return launch_batch_prop_t<4, PROP>(b, iter, color, ctas, s);
-    if (smax <= 8) return launch_batch_prop_t<8, PROP>(b, iter, color, ctas, s);
-    if (smax <= 12) return launch_batch_prop_t<12, PROP>(b, iter, color, ctas, s);
-    if (smax <= 16) return launch_batch_prop_t<16, PROP>(b, iter, color, ctas, s);
-    return launch_batch_prop_t<kMaxSrc, PROP>(b, iter, color, ctas, s);
-}
-
-/* HPM_REFINE_PAIR=1 in the environment scores the two random-depth
- * refinement candidates in one tap loop (ncc_pair; same results) */
-bool refine_pair()
-{
-    static const bool on = [] {
-        const char *e = getenv("HPM_REFINE_PAIR");
-        return e && e[0] == '1';
-    }();
-    return on;
-}
-
-template <int SMAX>
+template <int SMAX, int WW>
 cudaError_t launch_prop_t(const PMArgs &a, int iter, int color, cudaStream_t s)
 {
-    dim3 grid((a.W + 2 * kWarpW - 1) / (2 * kWarpW), (a.rows_cov + 2 * kWarpH - 1) / (2 * kWarpH));
-    k_prop_dirs<<<grid, dim3(kBlockX, kBlockY), 0, s>>>(a, iter, color);
-    const dim3 b(kBlockX, kBlockY);
+    constexpr int WH = 32 / WW;
+    const dim3 grid((a.W + 2 * WW - 1) / (2 * WW), (a.rows_cov + 2 * WH - 1) / (2 * WH)), b(kBlockX, kBlockY);
+    k_prop_dirs<WW><<<grid, b, 0, s>>>(a, iter, color);
     if (a.proposals)
-        k_prop_refine<SMAX, true, false><<<grid, b, 0, s>>>(a, iter, color);
-    else if (refine_pair())
-        k_prop_refine<SMAX, false, true><<<grid, b, 0, s>>>(a, iter, color);
+        k_prop_refine<SMAX, true, WW><<<grid, b, 0, s>>>(a, iter, color);
     else
-        k_prop_refine<SMAX, false, false><<<grid, b, 0, s>>>(a, iter, color);
+        k_prop_refine<SMAX, false, WW><<<grid, b, 0, s>>>(a, iter, color);
     return cudaGetLastError();
+}
+
+template <int WW>
+cudaError_t launch_prop_w(const PMArgs &a, int iter, int color, cudaStream_t s)
+{
+    const int S = a.n - 1;
+    if (S <= 4) return launch_prop_t<4, WW>(a, iter, color, s);
+    if (S <= 8) return launch_prop_t<8, WW>(a, iter, color, s);
+    if (S <= 12) return launch_prop_t<12, WW>(a, iter, color, s);
+    if (S <= 16) return launch_prop_t<16, WW>(a, iter, color, s);
+    return launch_prop_t<kMaxSrc, WW>(a, iter, color, s);
 }
 
 }  // namespace
@@ -1530,38 +1341,15 @@ cudaError_t launch_init(const PMArgs &a, cudaStream_t s)
     return cudaGetLastError();
 }
 
-cudaError_t launch_propagate(const PMArgs &a, int iter, int color, cudaStream_t s)
+cudaError_t launch_propagate(const PMArgs &a, int iter, int color, cudaStream_t s, int ww)
 {
     if (a.rows_cov <= 0) return cudaSuccess;
-    const int S = a.n - 1;
-    if (S <= 4) return launch_prop_t<4>(a, iter, color, s);
-    if (S <= 8) return launch_prop_t<8>(a, iter, color, s);
-    if (S <= 12) return launch_prop_t<12>(a, iter, color, s);
-    if (S <= 16) return launch_prop_t<16>(a, iter, color, s);
-    return launch_prop_t<kMaxSrc>(a, iter, color, s);
-}
-
-int half_step_tiles(int W, int rows_cov, int ww, int *gx)
-{
-    const int wh = 32 / ww;
-    *gx = (W + 2 * ww - 1) / (2 * ww);
-    return *gx * ((rows_cov + 2 * wh - 1) / (2 * wh));
-}
-
-cudaError_t launch_batch_init(const BatchList &b, int ctas, cudaStream_t s)
-{
-    if (b.total <= 0) return cudaSuccess;
-    const int c = ctas > 0 ? ctas : resident_ctas(k_init_batch);
-    k_init_batch<<<b.total < c ? b.total : c, dim3(kBlockX, kBlockY), 0, s>>>(b);
-    return cudaGetLastError();
-}
-
-cudaError_t launch_batch_propagate(const BatchList &b, int smax, int iter, int color, int ctas, bool proposals,
-                                   cudaStream_t s)
-{
-    if (b.total <= 0) return cudaSuccess;
-    return proposals ? launch_batch_prop_s<true>(b, smax, iter, color, ctas, s)
-                     : launch_batch_prop_s<false>(b, smax, iter, color, ctas, s);
+    switch (ww) {
+    case 4: return launch_prop_w<4>(a, iter, color, s);
+    case 8: return launch_prop_w<8>(a, iter, color, s);
+    case 16: return launch_prop_w<16>(a, iter, color, s);
+    default: return cudaErrorInvalidValue;
+    }
 }
 
 cudaError_t launch_depth_normal_filter(const PMArgs &a, float4 *planes, const float *costs, cudaStream_t s)

@@ -326,9 +326,8 @@ int net_coarse_views(hpm_ctx *c, int n, const float *const *images, const HpmCam
         cur += ((size_t)vw * vh + 63) & ~(size_t)63;
     }
     if (!c->coarse) {
-        int rc = hpm_create(&c->coarse, c->device);
+        const int rc = ctx_create_child(c, &c->coarse);
         if (rc) return ctx_fail(c, rc, "prior-net form: coarse context");
-        c->coarse->scene_workers = 1;
     }
     CK(cudaStreamSynchronize(s), "coarse images");
     const int r = hpm_set_views(c->coarse, cimgs, ccams, n);
@@ -470,9 +469,11 @@ int net_status(hpm_ctx *c)
  * pass with the proposal as a sixth refinement candidate, then extra_passes
  * more full-scale prior passes, each with the planar prior rebuilt from the
  * previous pass (the plain form's finest level) and the proposal still a
- * candidate.  Outputs like hpm_process_problem. */
+ * candidate; half_steps red/black half-steps per full-scale pass.  Outputs
+ * like hpm_process_problem. */
 int net_problem(hpm_ctx *c, int n, const float *const *images, const HpmCamera *cams, const HpmNetWeights *net,
-                uint64_t seed, int extra_passes, int prior_mode, float *depth_out, float *normal_out, float *cost_out)
+                uint64_t seed, int extra_passes, int prior_mode, int half_steps, float *depth_out, float *normal_out,
+                float *cost_out)
 {
     const Range range("prior-net problem %dx%d", cams[0].width, cams[0].height);
     int cw, ch;
@@ -497,7 +498,7 @@ int net_problem(hpm_ctx *c, int n, const float *const *images, const HpmCamera *
             if (r) break;
         }
         p.seed = net_pass_seed(seed, e);
-        r = ctx_run_pass(c, &p, 6, 1);
+        r = ctx_run_pass(c, &p, half_steps, 1);
         if (r) break;
         CK(flow_split_state(reinterpret_cast<const float4 *>(ctx_planes(c)), (int)npx, ws.full_depth, ws.full_normal,
                             s),

@@ -47,7 +47,7 @@ EXPORTED = [
 
 class HpmSceneOpts(ctypes.Structure):
     _fields_ = [("planar_prior", ctypes.c_int), ("geom_iterations", ctypes.c_int), ("seed", ctypes.c_uint64),
-                ("pyramid_levels", ctypes.c_int)]
+                ("pyramid_levels", ctypes.c_int), ("iterations", ctypes.c_int)]
 
 
 class HpmNetWeights(ctypes.Structure):
@@ -239,7 +239,7 @@ class Context:
         return depth, normal, cost, prior
 
     def run_scene(self, images, cams, pairs, *, planar_prior=True, geom_iterations=2, seed=0, pyramid_levels=-1,
-                  images_are_device=False, outputs=True, extra_maps=False, net=None, batched=False):
+                  images_are_device=False, outputs=True, extra_maps=False, net=None, batched=False, iterations=0):
         """The reference's main() over a scene.  images: per-view float32 [H, W]
         arrays, or device pointers (ints) with images_are_device; pairs:
         [(ref, [sources])].  outputs: True to return new per-view (depth,
@@ -250,7 +250,8 @@ class Context:
         net: an HpmNetWeights (priornet.Net.weights()) to run the prior-net
         form (hpm_run_scene_net) instead of the plain form.  batched: the
         batched form (hpm_run_scene_batched; with net, the batched prior-net
-        form, hpm_run_scene_batched_net)."""
+        form, hpm_run_scene_batched_net).  iterations: with net, PatchMatch
+        iterations of each full-scale pass (0: the reference's 3)."""
         n = len(cams)
         cams = np.ascontiguousarray(cams, dtype=CAMERA_DTYPE)
         if images_are_device:
@@ -265,7 +266,7 @@ class Context:
         srcs = np.zeros((len(pairs), MAX_IMAGES - 1), np.int32)
         for i, (_, s) in enumerate(pairs):
             srcs[i, :len(s)] = s
-        o = HpmSceneOpts(int(planar_prior), int(geom_iterations), int(seed), int(pyramid_levels))
+        o = HpmSceneOpts(int(planar_prior), int(geom_iterations), int(seed), int(pyramid_levels), int(iterations))
         outs = None
         if isinstance(outputs, (tuple, list)):
             outs = list(zip(*outputs))

@@ -295,6 +295,15 @@ def _accuracy(sc, depths, normals):
     return acc, ne
 
 
+def parse_schedule(text: str):
+    """"extra:geom[:prior[:iterations]]" -> (extra, geom, prior, iterations);
+    prior defaults to 1 (the coarse triangulation), iterations to 3."""
+    v = [int(x) for x in text.split(":")]
+    if not 2 <= len(v) <= 4:
+        raise ValueError(f"schedule {text!r}: extra:geom[:prior[:iterations]]")
+    return tuple(v + [1, 3][len(v) - 2:])
+
+
 def main():
     import argparse
     import json
@@ -307,9 +316,13 @@ def main():
     ap.add_argument("--steps", type=int, default=1500)
     ap.add_argument("--batch", type=int, default=8)
     ap.add_argument("--lr", type=float, default=1e-3)
-    ap.add_argument("--schedules", default="0:2:1,0:2:2,1:2:1,0:1:1,0:1:2,1:1:1",
+    ap.add_argument("--schedules", default="0:2:1:3,0:1:1:3,0:1:2:3,0:1:1:2,0:1:2:2,1:1:1:2,0:2:1:2,0:1:1:1",
                     help="prior-net schedules to evaluate, extra full-scale prior passes:geometric iterations:"
-                         "planar prior of the first full-scale pass (1 the coarse triangulation, 2 the proposal)")
+                         "planar prior of the first full-scale pass (1 the coarse triangulation, 2 the proposal):"
+                         "PatchMatch iterations per full-scale pass")
+    ap.add_argument("--batched", action="store_true", help="evaluate the batched forms (plain and prior-net)")
+    ap.add_argument("--weights", default=None,
+                    help="evaluate the schedules with these weights instead of generating data and training")
     ap.add_argument("--workers", type=int, default=0)
     ap.add_argument("--size", default=None, help="WxH of the scenes (default 1600x1200)")
     ap.add_argument("--out", default=".")
@@ -318,7 +331,9 @@ def main():
     if args.size:
         recipe["width"], recipe["height"] = (int(x) for x in args.size.lower().split("x"))
     workers = args.workers or max(1, (os.cpu_count() or 2) * 2 // 3)
-    schedules = [tuple(int(x) for x in (t + ":1").split(":")[:3]) for t in args.schedules.split(",")]
+    schedules = [parse_schedule(t) for t in args.schedules.split(",")]
+    if args.weights:
+        args.scenes = 0
     train_seeds = list(range(1000, 1000 + args.scenes))
     eval_seeds = list(range(9000, 9000 + args.eval_scenes))
     log = lambda m: print(m, file=sys.stderr, flush=True)  # noqa: E731
@@ -338,13 +353,20 @@ def main():
                 log(f"scene {k}: {len(samples)} views, valid px/view {np.mean([s['valid'] for s in samples]):.0f}")
         summary["data_seconds"] = time.time() - t_data
         summary["train_views"] = len(samples)
-        net = Net(0, seed=1)
-        t_train = time.time()
-        curve = train(samples, net, steps=args.steps, batch=args.batch, lr=args.lr, log=log)
-        torch.cuda.synchronize()
-        summary["train_seconds"] = time.time() - t_train
-        summary["loss_first_last"] = [curve[0], curve[-1]]
-        summary["train_fit"] = evaluate(samples, net)
+        if args.weights:
+            net = Net.load(args.weights)
+            meta = dict(np.load(args.weights))
+            curve = [float(x) for x in meta.get("loss", np.zeros(1))]
+            args.scenes, args.steps = int(meta.get("train_scenes", 0)), int(meta.get("steps", 0))
+            summary["weights"] = args.weights
+        else:
+            net = Net(0, seed=1)
+            t_train = time.time()
+            curve = train(samples, net, steps=args.steps, batch=args.batch, lr=args.lr, log=log)
+            torch.cuda.synchronize()
+            summary["train_seconds"] = time.time() - t_train
+            summary["loss_first_last"] = [curve[0], curve[-1]]
+            summary["train_fit"] = evaluate(samples, net)
         del samples
         # held-out scenes: the network's own accuracy, then the plain form and
         # the prior-net form end to end
@@ -353,10 +375,10 @@ def main():
             sc = next(stream)
             row = {"seed": sc["seed"]}
             ev = []
-            for form, kw in [("plain", dict(geom_iterations=2))] + [
-                    (f"net_e{e}_g{g}_p{m}", dict(pyramid_levels=e, geom_iterations=g, planar_prior=m,
-                                                 net=net.weights()))
-                    for e, g, m in schedules]:
+            for form, kw in [("plain", dict(geom_iterations=2, batched=args.batched))] + [
+                    (f"net_e{e}_g{g}_p{m}_i{i}", dict(pyramid_levels=e, geom_iterations=g, planar_prior=m,
+                                                      iterations=i, net=net.weights(), batched=args.batched))
+                    for e, g, m, i in schedules]:
                 ctx.run_scene(sc["images"], sc["cams"], sc["pairs"], seed=sc["seed"], **kw)  # warm-up
                 torch.cuda.synchronize()
                 t0 = time.time()
@@ -372,23 +394,23 @@ def main():
             rows.append(row)
             log(json.dumps(row))
         summary["eval"] = rows
-        forms = ["plain"] + [f"net_e{e}_g{g}_p{m}" for e, g, m in schedules]
+        forms = ["plain"] + [f"net_e{e}_g{g}_p{m}_i{i}" for e, g, m, i in schedules]
         for form in forms:
             summary[f"eval_{form}"] = {k: float(np.mean([r[form][k] for r in rows]))
                                        for k in ("mpix_per_s", "px_relerr_lt_1pct", "median_normal_err_deg")}
         # the schedule the scene driver uses: the fastest whose accuracy is
         # within 0.5 pp of the plain form's, else the most accurate
         plain_acc = summary["eval_plain"]["px_relerr_lt_1pct"]
-        ev = lambda e, g, m: summary[f"eval_net_e{e}_g{g}_p{m}"]  # noqa: E731
-        ok = [(ev(e, g, m)["mpix_per_s"], e, g, m) for e, g, m in schedules
-              if ev(e, g, m)["px_relerr_lt_1pct"] >= plain_acc - 0.005]
+        ev = lambda e, g, m, i: summary[f"eval_net_e{e}_g{g}_p{m}_i{i}"]  # noqa: E731
+        ok = [(ev(*t)["mpix_per_s"], t) for t in schedules if ev(*t)["px_relerr_lt_1pct"] >= plain_acc - 0.005]
         if ok:
-            _, e, g, m = max(ok)
+            _, (e, g, m, i) = max(ok)
         else:
-            _, e, g, m = max((ev(e, g, m)["px_relerr_lt_1pct"], e, g, m) for e, g, m in schedules)
-        summary["chosen_schedule"] = {"extra_passes": e, "geom_iterations": g, "prior": m}
+            _, (e, g, m, i) = max((ev(*t)["px_relerr_lt_1pct"], t) for t in schedules)
+        summary["chosen_schedule"] = {"extra_passes": e, "geom_iterations": g, "prior": m, "iterations": i}
         net.save(os.path.join(args.out, "priornet_weights.npz"), loss=np.array(curve, np.float32),
-                 extra_passes=e, geom_iterations=g, prior=m, train_scenes=args.scenes, steps=args.steps)
+                 extra_passes=e, geom_iterations=g, prior=m, iterations=i, train_scenes=args.scenes,
+                 steps=args.steps)
     with open(os.path.join(args.out, "priornet_summary.json"), "w") as f:
         json.dump(summary, f, indent=1)
     print(json.dumps({k: v for k, v in summary.items() if k != "eval"}))

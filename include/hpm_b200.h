@@ -153,6 +153,8 @@ typedef struct {
     int geom_iterations; /* geometric iterations of pass set B (the reference's default: 2) */
     uint64_t seed;
     int pyramid_levels; /* -1 = the reference's rule */
+    int iterations;     /* prior-net forms only: PatchMatch iterations of each full-scale pass, the geometric
+                           ones included (0 = 3, the reference's count; the plain form always runs 3) */
 } HpmSceneOpts;
 
 /* The reference's main() (main.cpp:636-677) over a scene: ProcessProblem

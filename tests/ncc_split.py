@@ -66,16 +66,42 @@ def split(cost_a, cost_b, samples_a, samples_b, inside_a, inside_b, ref_img, pix
 MARGIN = 1.25  # first-order bounds: 25 % for the second-order terms they leave out
 
 
-def check_within_bound(got, ref, bound, what):
+def exact_costs(samples, inside, ref_img, pixels):
+    """float64 NCC (n, S) of the given tap samples (n, S, 36), 2 where the
+    window centre falls outside the source view: the exact value both FP32
+    evaluations of the same samples approximate."""
+    r, wgt = ref_window(ref_img, pixels)
+    return np.where(inside, ncc64(r, wgt, samples.astype(np.float64)), 2.0)
+
+
+def _offenders(over, got, ref, bound, exact, extra):
+    idx = np.argsort(-np.where(over, np.abs(got - ref) - bound, -np.inf).ravel())[:min(5, int(over.sum()))]
+    rows = []
+    for i in idx:
+        row = f"#{i}: got {got.flat[i]:.7f} ref {ref.flat[i]:.7f} bound {bound.flat[i]:.3g}"
+        if exact is not None:
+            row += f" exact {exact.flat[i]:.7f} (got-exact {got.flat[i] - exact.flat[i]:.3g}, " \
+                   f"ref-exact {ref.flat[i] - exact.flat[i]:.3g})"
+        for k, v in (extra or {}).items():
+            row += f" {k} {np.asarray(v).flat[i]:.4g}"
+        rows.append(row)
+    return "; ".join(rows)
+
+
+def check_within_bound(got, ref, bound, what, exact=None, extra=None):
     """|got - ref| <= 1e-4 max(1, |ref|) + MARGIN * bound for every value,
     and <= 1e-4 max(1, |ref|) alone where the bound is below 1e-4 (well
-    conditioned).  Returns the fraction of values within 1e-4."""
+    conditioned).  Returns the fraction of values within 1e-4.  exact (the
+    float64 value of the same samples) and extra arrays only enrich the
+    message of a failure."""
     got, ref = np.asarray(got, np.float64), np.asarray(ref, np.float64)
+    bound = np.broadcast_to(np.asarray(bound, np.float64), got.shape)
     d = np.abs(got - ref)
     tol = 1e-4 * np.maximum(1.0, np.abs(ref))
     over = d > tol + MARGIN * bound
     assert not over.any(), (f"{what}: {int(over.sum())} values beyond the bound, worst excess "
-                            f"{float((d - tol - MARGIN * bound).max()):.3g}")
+                            f"{float((d - tol - MARGIN * bound).max()):.3g}; "
+                            + _offenders(over, got, ref, MARGIN * bound + tol, exact, extra))
     calm = bound < 1e-4
     assert (d[calm] <= tol[calm]).all(), f"{what}: {int((d[calm] > tol[calm]).sum())} well-conditioned values off"
     return float((d <= tol).mean())

@@ -67,14 +67,17 @@ def test_cost_vectors_vs_reference_and_oracle(case):
     px = c["pixels"]
     for k, p in enumerate(c["planes"]):
         got = _sample(ctx.cost_vectors(p), px)
-        ocost, bound, acc, _ = orc.ncc_bounds(c["imgs"], c["cams"], p, K_ERR, pixels=px)
+        ocost, bound, acc, kind = orc.ncc_bounds(c["imgs"], c["cams"], p, K_ERR, pixels=px)
+        exact = None
         if orc.ref_available():
             sg, ig = ctx.tap_samples(p, px)
             sr, ir = orc.ref_tap_samples(c["imgs"], c["cams"], p, px)
             np.testing.assert_array_equal(ig, ir)
             np.testing.assert_array_equal(sg[ig], sr[ir])
+            exact = ncc_split.exact_costs(sg, ig, c["imgs"][0], px)
         ref = g["cost_vectors"][k]
-        ncc_split.check_within_bound(got, ref, acc, f"{name} field {k} vs reference")
+        ncc_split.check_within_bound(got, ref, acc, f"{name} field {k} vs reference", exact=exact,
+                                     extra={"acc": acc, "kind": kind, "oracle": ocost})
         ncc_split.check_within_bound(got, ocost, bound + acc, f"{name} field {k} vs oracle")
         ncc_split.check_within_bound(ocost, ref, bound + acc, f"{name} field {k} oracle vs reference")
 
