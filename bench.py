@@ -59,7 +59,7 @@ STRESS = dict(width=3200, height=2133, n_views=20, n_planes=20, n_spheres=5, low
 BATCHED = dict(width=1920, height=1080, n_views=24, n_planes=20, n_spheres=5, low_texture=0.40, pyramid_levels=-1,
                geom_iterations=2, depth_range=(2.0, 8.0), arc_step_deg=3.0, n_sources=10,
                sizes=[(1920, 1080)] * 8 + [(1600, 1200)] * 8 + [(960, 540)] * 8,
-               name="batched scene (8 views of 1920x1080, 8 of 1600x1200, 8 of 960x540)")
+               name="batched scene")
 
 # DRAM traffic of one half-step (k_prop_dirs + k_prop_refine), from an ncu
 # capture of `bench.py --pass-case` (1600x1200, 10 sources), per pixel: the
@@ -71,8 +71,15 @@ TAPS, NCC_FLOPS_PER_TAP, FLOPS_PER_HYP_VIEW = 36, 34, 80
 
 def workload_name():
     w = WORKLOAD
-    return (f"{w['name']}: {w['n_views']} views of {w['width']}x{w['height']}, "
-            f"{w['n_views'] - 1} sources each, planar+KNN prior on a {w['pyramid_levels'] + 1}-level pyramid, "
+    if "sizes" in w:
+        sizes = ", ".join(f"{w['sizes'].count(s)} of {s[0]}x{s[1]}" for s in dict.fromkeys(w["sizes"]))
+        views = f"{w['n_views']} views ({sizes})"
+    else:
+        views = f"{w['n_views']} views of {w['width']}x{w['height']}"
+    sources = w.get("n_sources", w["n_views"] - 1)
+    pyramid = ("a pyramid by the reference's rule per view size" if w["pyramid_levels"] < 0 else
+               f"a {w['pyramid_levels'] + 1}-level pyramid")
+    return (f"{w['name']}: {views}, {sources} sources each, planar+KNN prior on {pyramid}, "
             f"{w['geom_iterations']} geometric iterations")
 
 
@@ -306,24 +313,19 @@ def cpu_baseline():
                       "passes, CPU oracle (oracle/hpm_oracle.c, OpenMP; OpenCV resize and Delaunay)"}
 
 
-def run_ours(args, dist):
+def measure_form(args, dist, ctx, sc, images, d_ptrs, pairs, stream, opts, profile=False):
+    """One form of the scene step (opts: Context.run_scene keywords) under the
+    bench's rules: W untimed warm-up steps; work counters and the kernel
+    launch list from untimed re-runs of the first timed step; K timed steps
+    with the images resident in HBM (CUDA events on the context's stream,
+    max over ranks, SM clocks sampled meanwhile; with `profile`, CUDA events
+    around every kernel group as well); K end-to-end steps through the public
+    API from pinned host images to every view's depth, normal and cost maps
+    in pinned host memory; the accuracy of the last end-to-end step's maps."""
     import torch
 
-    import hpm_b200 as hb
-
-    torch.cuda.set_device(dist.local)
-    dev = f"cuda:{dist.local}"
     w = WORKLOAD
-    sc, images, pairs = make_scene(seed=dist.rank)
-    nv, W, H, S = w["n_views"], w["width"], w["height"], w["n_views"] - 1
-    npx = W * H
-    peak = hb.fp32_peak(dist.local)
-    ctx = hb.Context(dist.local)
-    stream = torch.cuda.ExternalStream(ctx.stream(), device=dev)
-    d_imgs = [torch.from_numpy(i).to(dev) for i in images]
-    d_ptrs = [t.data_ptr() for t in d_imgs]
-    torch.cuda.synchronize()
-    opts = dict(planar_prior=True, geom_iterations=w["geom_iterations"], pyramid_levels=w["pyramid_levels"])
+    nv, W, H = w["n_views"], w["width"], w["height"]
 
     def step(seed):
         ctx.run_scene(d_ptrs, sc.cams, pairs, seed=seed, images_are_device=True, outputs=False, **opts)
@@ -345,21 +347,21 @@ def run_ours(args, dist):
     dist.barrier()
     torch.cuda.synchronize()
     with Clocks(dist.local) as clk:
-        ctx.profile_enable(True)
+        if profile:
+            ctx.profile_enable(True)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
         for i in range(args.steps):
             step(i)
         e1.record(stream)
         e1.synchronize()
-        prof = ctx.profile_read()
-        ctx.profile_enable(False)
+        prof = ctx.profile_read() if profile else None
+        if profile:
+            ctx.profile_enable(False)
     dist.barrier()
     torch.cuda.synchronize()
     ms = dist.max(e0.elapsed_time(e1))
 
-    # end to end through the public API: pinned host images in, every
-    # view's depth, normal and cost maps out
     pin_imgs = [torch.from_numpy(i).pin_memory() for i in images]
     outs = ([torch.empty((H, W), dtype=torch.float32).pin_memory() for _ in range(nv)],
             [torch.empty((H, W, 3), dtype=torch.float32).pin_memory() for _ in range(nv)],
@@ -376,109 +378,153 @@ def run_ours(args, dist):
     f1.synchronize()
     dist.barrier()
     ms_e2e = dist.max(f0.elapsed_time(f1))
-    acc = scene_accuracy(sc, dict(enumerate(out_np[0])), dict(enumerate(out_np[1])))
-    net_form = prior_net_form(args, dist, ctx, sc, d_ptrs, pairs, stream, ms / args.steps, acc, out_np)
-    ctx.close()
-    fusion = time_fusion(sc, pairs, out_np[0], out_np[1], dist.rank == 0 and dist.world == 1)
+    npx = nv * W * H
+    return {
+        "value": job_mpix_per_s(dist.world, args.steps, npx, ms), "ms_per_step": ms / args.steps,
+        "e2e": {"value": job_mpix_per_s(dist.world, args.steps, npx, ms_e2e), "unit": "depth Mpix/s",
+                "ms_per_step": ms_e2e / args.steps, "h2d_bytes_per_step": int(sum(i.nbytes for i in images)),
+                "d2h_bytes_per_step": int(npx * 4 * 5)},
+        "accuracy": scene_accuracy(sc, dict(enumerate(out_np[0])), dict(enumerate(out_np[1]))),
+        "clocks": clk.summary(), "ncc_windows": n_ncc, "geom_terms": n_geom, "launches": launches,
+        "launch_src": launch_src, "profile": prof, "maps": out_np,
+    }
 
+
+def net_schedule(device):
+    """The trained network's weights and the schedule stored with them
+    (extra full-scale passes, geometric iterations, planar prior of the
+    first full-scale pass, PatchMatch iterations per full-scale pass), or
+    None without weights."""
+    import priornet
+
+    if not os.path.exists(priornet.WEIGHTS_FILE):
+        return None
+    net = priornet.Net.load(device=device)
+    meta = dict(np.load(priornet.WEIGHTS_FILE))
+    get = lambda k, d: int(meta[k]) if k in meta else d  # noqa: E731
+    sched = {"pyramid_levels": get("extra_passes", 0), "geom_iterations": get("geom_iterations", 2),
+             "planar_prior": get("prior", 1), "iterations": get("iterations", 3)}
+    return net, sched
+
+
+def form_summary(m):
+    """The figures of one measured form for the JSON line."""
+    return {k: m[k] for k in ("value", "ms_per_step", "e2e", "accuracy", "clocks")} | {
+        "gpu_launches_per_step": sum(m["launches"].values())}
+
+
+def run_ours(args, dist):
+    import torch
+
+    import hpm_b200 as hb
+
+    torch.cuda.set_device(dist.local)
+    dev = f"cuda:{dist.local}"
+    w = WORKLOAD
+    sc, images, pairs = make_scene(seed=dist.rank)
+    nv, W, H, S = w["n_views"], w["width"], w["height"], w["n_views"] - 1
+    npx = W * H
+    peak = hb.fp32_peak(dist.local)
+    ctx = hb.Context(dist.local)
+    stream = torch.cuda.ExternalStream(ctx.stream(), device=dev)
+    d_imgs = [torch.from_numpy(i).to(dev) for i in images]
+    d_ptrs = [t.data_ptr() for t in d_imgs]
+    torch.cuda.synchronize()
+    common = (args, dist, ctx, sc, images, d_ptrs, pairs, stream)
+
+    # the plain form: the reference's flow (hpm_run_scene), CUDA events around
+    # every kernel group of the timed steps for the roofline
+    plain = measure_form(*common, dict(planar_prior=True, geom_iterations=w["geom_iterations"],
+                                       pyramid_levels=w["pyramid_levels"]), profile=True)
+    # the batched prior-net form with the schedule stored with the weights
+    ns = net_schedule(dist.local)
+    net = None
+    if ns is not None:
+        wts, sched = ns[0].weights(), ns[1]
+        net = measure_form(*common, dict(sched, net=wts, batched=True))
+        net["schedule"] = sched
+    ctx.close()
+    fusion = time_fusion(sc, pairs, plain["maps"][0], plain["maps"][1], dist.rank == 0 and dist.world == 1)
+
+    # roofline of the dominant kernel pair (one red/black half-step), from the
+    # plain form's profiled steps; the batched prior-net form runs the same
+    # kernels (with the proposal as one more candidate)
+    prof = plain["profile"]
     n_pass = nv * passes_per_view()
     prop_ms, prop_n = prof["propagate"]
     half_steps = prop_n // max(args.steps, 1)
-    ncc_half = n_ncc - n_pass * npx * S  # k_init scores one hypothesis per pixel and pass
-    flops_step = ncc_half * (TAPS * NCC_FLOPS_PER_TAP + FLOPS_PER_HYP_VIEW) + n_geom * GEOM_TERM_FLOPS
+    ncc_half = plain["ncc_windows"] - n_pass * npx * S  # k_init scores one hypothesis per pixel and pass
+    flops_step = ncc_half * (TAPS * NCC_FLOPS_PER_TAP + FLOPS_PER_HYP_VIEW) + plain["geom_terms"] * GEOM_TERM_FLOPS
     prop_ms_step = prop_ms / args.steps
     achieved = flops_step / (prop_ms_step * 1e-3) / 1e12
-    n_launch = sum(launches.values())
+
+    plain_acc = plain["accuracy"]["px_relerr_lt_1pct"]
+    equal = net is not None and net["accuracy"]["px_relerr_lt_1pct"] >= plain_acc - 0.005
+    head = net if equal else plain
+    plain_step = ("hpm_run_scene: pass set A (plain pass, then one prior pass per pyramid level: support points, "
+                  "Delaunay, raster, KNN prior, JBU) for every view, then the geometric iterations for every view; "
+                  f"{n_pass} PatchMatch passes of 3 iterations")
+    if net is not None:
+        sc_ = net["schedule"]
+        net_step = ("hpm_run_scene_batched_net: per problem a 1/4-scale plain pass (all problems in one graph), "
+                    "the coarse planar prior and the BF16 network's plane proposal; then "
+                    f"{1 + sc_['pyramid_levels']} full-scale pass(es) with the proposal as initial hypothesis and "
+                    f"as a refinement candidate, then {sc_['geom_iterations']} geometric iteration(s); "
+                    f"{sc_['iterations']} PatchMatch iterations per full-scale pass; every pass of all problems "
+                    "one CUDA graph")
+        net_out = form_summary(net) | {
+            "schedule": sc_, "step": net_step, "speedup_vs_plain": plain["ms_per_step"] / net["ms_per_step"],
+            "e2e_speedup_vs_plain": plain["e2e"]["ms_per_step"] / net["e2e"]["ms_per_step"],
+            "px_relerr_lt_1pct_minus_plain": net["accuracy"]["px_relerr_lt_1pct"] - plain_acc,
+            "equal_accuracy": bool(equal),
+            "network": "4 layers of 3x3 conv, 32 channels, BF16 on tcgen05 (FP32 accumulation in TMEM), at "
+                       "1/4 scale; weights hpm-mvs_b200/priornet_weights.npz"}
+    else:
+        net_out = {"unavailable": "no trained weights (hpm-mvs_b200/priornet_weights.npz)"}
     line = {
-        "metric": METRIC, "value": job_mpix_per_s(dist.world, args.steps, nv * npx, ms), "unit": "depth Mpix/s",
-        "n_gpus": dist.world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "metric": METRIC, "value": head["value"], "unit": "depth Mpix/s", "n_gpus": dist.world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": head["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded procedural scene, hpm-mvs_b200/synthetic.py; one scene per rank)",
         "config": {"workload": workload_name(), "width": W, "height": H, "views": nv, "sources": S,
                    "scene": f"{w['n_planes']} planes + {w['n_spheres']} spheres, "
                             f"{int(w['low_texture'] * 100)}% low-texture",
-                   "step": "hpm_run_scene: pass set A (plain pass, then one prior pass per pyramid level: support "
-                           "points, Delaunay, raster, KNN prior, JBU) for every view, then the geometric "
-                           f"iterations for every view; {n_pass} PatchMatch passes",
+                   "form": "batched prior-net form (its %px within 0.5 pp of the plain form's)" if equal else
+                           "plain form (the batched prior-net form is not within 0.5 pp of its %px, or has no "
+                           "weights)",
+                   "step": net_step if equal else plain_step,
                    "pyramid_levels": w["pyramid_levels"] + 1, "knn_k": 6,
                    "l2": f"inputs larger than L2 ({nv} views x {W}x{H} float images + texture arrays = "
                          f"{2 * nv * npx * 4 / 1e6:.0f} MB, plus the per-view depth/normal/cost maps)",
                    "parallelism": f"one scene per GPU, {dist.world} GPU(s)"},
-        "accuracy": acc,
-        "clocks": clk.summary(),
-        "e2e": {"value": job_mpix_per_s(dist.world, args.steps, nv * npx, ms_e2e), "unit": "depth Mpix/s",
-                "h2d_bytes_per_step": int(sum(i.nbytes for i in images)),
-                "d2h_bytes_per_step": int(nv * npx * 4 * 5)},
-        "gpu_launches": n_launch * args.steps,
-        "gpu_launches_per_step": {short_kernel_name(k): v for k, v in sorted(launches.items(), key=lambda x: -x[1])},
-        "gpu_launches_source": launch_src,
+        "accuracy": head["accuracy"],
+        "clocks": head["clocks"],
+        "e2e": head["e2e"],
+        "gpu_launches": sum(head["launches"].values()) * args.steps,
+        "gpu_launches_per_step": {short_kernel_name(k): v
+                                  for k, v in sorted(head["launches"].items(), key=lambda x: -x[1])},
+        "gpu_launches_source": head["launch_src"],
         "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                      "frac": achieved / peak,
                      "traffic": TRAFFIC_BYTES_PER_PX_HALF_STEP * npx,
                      "traffic_note": "DRAM bytes per half-step (k_prop_dirs + k_prop_refine) from the ncu capture "
                                      "of bench.py --pass-case at 1600x1200 (10 sources), per pixel of the "
                                      "workload",
-                     "kernel": "k_prop_dirs + k_prop_refine (one red/black half-step)",
+                     "kernel": "k_prop_dirs + k_prop_refine (one red/black half-step), timed with CUDA events "
+                               "in the plain form's timed steps",
                      "peak_source": "measured FP32 FMA probe (hpm_fp32_peak) of measured; "
                                     "MEASURED_PEAKS.json has no FP32 figure",
                      "half_step_ms": prop_ms_step / max(half_steps, 1), "half_steps_per_step": half_steps,
                      "propagate_ms_per_step": prop_ms_step,
-                     "propagate_share": prop_ms_step / (ms / args.steps),
-                     "ncc_windows_per_step": ncc_half, "geom_terms_per_step": n_geom,
+                     "propagate_share": prop_ms_step / plain["ms_per_step"],
+                     "ncc_windows_per_step": ncc_half, "geom_terms_per_step": plain["geom_terms"],
                      "flops_per_ncc_window": TAPS * NCC_FLOPS_PER_TAP + FLOPS_PER_HYP_VIEW},
+        "plain_form": form_summary(plain) | {"step": plain_step},
+        "batched_prior_net_form": net_out,
         "fusion": fusion,
-        "prior_net_form": net_form,
         "impl": "ours",
     }
     return line
-
-
-def prior_net_form(args, dist, ctx, sc, d_ptrs, pairs, stream, plain_ms, plain_acc, out_np):
-    """The prior-net form on the same scene and timing rules (device-resident
-    images, CUDA events on the context's stream): per problem a 1/4-scale
-    plain pass, the coarse planar prior, the BF16 network's proposal, one
-    full-scale prior pass that starts from and scores the proposal, then the
-    geometric iterations.  Accuracy from an untimed run with the maps out."""
-    import torch
-
-    import priornet
-
-    if not os.path.exists(priornet.WEIGHTS_FILE):
-        return {"unavailable": "no trained weights (hpm-mvs_b200/priornet_weights.npz)"}
-    net = priornet.Net.load(device=dist.local)
-    meta = dict(np.load(priornet.WEIGHTS_FILE))
-    geom = int(meta["geom_iterations"]) if "geom_iterations" in meta else WORKLOAD["geom_iterations"]
-    extra = int(meta["extra_passes"]) if "extra_passes" in meta else 0
-    prior = int(meta["prior"]) if "prior" in meta else 1
-    wts = net.weights()
-    w = WORKLOAD
-    npx = w["n_views"] * w["width"] * w["height"]
-
-    def step(seed, outputs=False):
-        return ctx.run_scene(d_ptrs, sc.cams, pairs, seed=seed, images_are_device=True, outputs=outputs,
-                             geom_iterations=geom, pyramid_levels=extra, planar_prior=prior, net=wts)
-
-    for i in range(args.warmup):
-        step(2000 + i)
-    dist.barrier()
-    torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for i in range(args.steps):
-        step(i)
-    e1.record(stream)
-    e1.synchronize()
-    dist.barrier()
-    ms = dist.max(e0.elapsed_time(e1)) / args.steps
-    step(0, outputs=out_np)
-    acc = scene_accuracy(sc, dict(enumerate(out_np[0])), dict(enumerate(out_np[1])))
-    value = job_mpix_per_s(dist.world, 1, npx, ms)
-    return {"value": value, "unit": "depth Mpix/s", "ms_per_step": ms, "geom_iterations": geom,
-            "extra_full_scale_prior_passes": extra, "proposal_as_planar_prior": prior == 2,
-            "speedup_vs_plain": plain_ms / ms, "accuracy": acc,
-            "px_relerr_lt_1pct_minus_plain": acc["px_relerr_lt_1pct"] - plain_acc["px_relerr_lt_1pct"],
-            "network": "4 layers of 3x3 conv, 32 channels, BF16 on tcgen05 (FP32 accumulation in TMEM), "
-                       "at 1/4 scale; weights hpm-mvs_b200/priornet_weights.npz"}
 
 
 def run_batched(args, dist):
@@ -526,8 +572,8 @@ def run_batched(args, dist):
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded procedural scene of uneven view sizes)",
         "config": {"workload": workload_name(), "views": w["n_views"], "sizes": "8x1920x1080, 8x1600x1200, 8x960x540",
                    "sources": 10, "pyramid": "reference rule per view size", "geom_iterations": w["geom_iterations"],
-                   "form": "hpm_run_scene_batched: one persistent launch per kernel and half-step over all 24 "
-                           "problems, passes replayed from a CUDA graph, tiles tuned per view size"},
+                   "form": "hpm_run_scene_batched: every pass of all 24 problems one CUDA graph of per-problem "
+                           "kernel chains (updated per pass, replayed), half-step tiles tuned per view size"},
         "accuracy": b["accuracy"], "clocks": b["clocks"],
         "per_problem_form": res["per_problem"], "speedup_vs_per_problem": res["per_problem"]["ms_per_step"] /
         b["ms_per_step"], "impl": "ours",

@@ -287,10 +287,12 @@ int hpm_set_views(hpm_ctx *c, const float *const *images, const HpmCamera *cams,
         CK(cudaMalloc(&c->d_masks, sizeof(uint32_t) * n), "state alloc");
         c->px_cap = n;
     }
-    CK(ensure((void **)&c->d_cache, &c->cache_cap, sizeof(float) * n * (num_images - 1)), "cache alloc");
-    CK(ensure((void **)&c->d_cand, &c->cand_cap, sizeof(float) * n * (num_images - 1) * kCandRows), "cand alloc");
-    CK(ensure((void **)&c->d_pos, &c->pos_cap, sizeof(int) * n * 8), "cand alloc");
-    CK(ensure((void **)&c->d_flags, &c->flags_cap, sizeof(uint32_t) * n), "cand alloc");
+    /* per-colour planes of ceil(n / 2) pixels (hpm_pm.cu: Slot) */
+    const size_t nh = (n + 1) / 2;
+    CK(ensure((void **)&c->d_cache, &c->cache_cap, sizeof(float) * 2 * nh * (num_images - 1)), "cache alloc");
+    CK(ensure((void **)&c->d_cand, &c->cand_cap, sizeof(float) * nh * (num_images - 1) * kCandRows), "cand alloc");
+    CK(ensure((void **)&c->d_pos, &c->pos_cap, sizeof(int) * nh * 8), "cand alloc");
+    CK(ensure((void **)&c->d_flags, &c->flags_cap, sizeof(uint32_t) * nh), "cand alloc");
     CK(cudaMemsetAsync(c->d_planes, 0, sizeof(float4) * n, c->stream), "state clear");
     CK(cudaMemsetAsync(c->d_costs, 0, sizeof(float) * n, c->stream), "state clear");
     CK(cudaMemsetAsync(c->d_views, 0, sizeof(uint32_t) * n, c->stream), "state clear");

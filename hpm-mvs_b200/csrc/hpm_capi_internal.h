@@ -98,13 +98,13 @@ struct hpm_ctx {
     void *d_scratch = nullptr;
     size_t scratch_cap = 0;
 
-    float *d_cache = nullptr; /* cost vector of each pixel's current hypothesis, [S][H*W] */
+    float *d_cache = nullptr; /* cost vector of each pixel's current hypothesis, [S][2][ceil(H*W/2)] */
     size_t cache_cap = 0;
-    float *d_cand = nullptr; /* half-step hand-off: cost matrix rows [kCandRows*S][H*W] */
+    float *d_cand = nullptr; /* half-step hand-off: cost matrix rows [kCandRows*S][ceil(H*W/2)] */
     size_t cand_cap = 0;
-    int *d_pos = nullptr; /* chosen NESP sites [8][H*W] */
+    int *d_pos = nullptr; /* chosen NESP sites [8][ceil(H*W/2)] */
     size_t pos_cap = 0;
-    uint32_t *d_flags = nullptr; /* valid-direction bits [H*W] */
+    uint32_t *d_flags = nullptr; /* direction row codes [ceil(H*W/2)] */
     size_t flags_cap = 0;
 
     /* prior-net form: the network's proposed plane per pixel (ref-frame

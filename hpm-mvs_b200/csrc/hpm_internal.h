@@ -55,11 +55,12 @@ struct PMArgs {
     uint32_t *views;
     const float4 *prior_planes;
     const uint32_t *masks;
-    float *cost_cache; /* [S][H][W] cost vector of the current hypothesis, or nullptr */
+    float *cost_cache; /* [S][colour][ceil(H*W/2)] cost vector of the current hypothesis, or nullptr */
     /* hand-off between the two kernels of a half-step (L2-resident):
-     * cand_costs [kCandRows*S][H*W] cost matrix rows (8 NESP directions and
-     * the 5 refinement candidates), cand_pos [8][H*W] chosen sites,
-     * cand_flags [H*W] bit k = direction k valid */
+     * cand_costs [kCandRows*S][ceil(H*W/2)] cost matrix rows (8 NESP
+     * directions, the refinement candidates and the proposal), cand_pos
+     * [8][ceil(H*W/2)] chosen sites, cand_flags [ceil(H*W/2)] row codes;
+     * indexed by (y * W + x) >> 1, dense over the pixels of one colour */
     float *cand_costs;
     int *cand_pos;
     uint32_t *cand_flags;

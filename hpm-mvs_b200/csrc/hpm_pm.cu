@@ -529,14 +529,36 @@ __global__ void k_pair_geom(const __grid_constant__ PMArgs a, PairGeom *out)
     out[v] = g;
 }
 
+/* Where a pixel's per-pixel buffers live.  Linear pixel indices 2k and
+ * 2k + 1 always have different checkerboard colours (neighbours in a row, or
+ * across a row end when W is odd), so center >> 1 numbers the pixels of one
+ * colour densely: a half-step's hand-off rows (cand_*, one colour at a time)
+ * are indexed by it, and the cost-vector cache keeps one such plane per
+ * colour.  A half-step then writes whole 32-byte sectors instead of every
+ * other word of them. */
+struct Slot {
+    size_t nh; /* pixels of one colour, rounded up: ceil(W * H / 2) */
+    int hc;    /* hand-off slot: center >> 1 */
+    size_t cs; /* cache slot: colour plane + hc */
+};
+
+__device__ __forceinline__ Slot slot_of(const PMArgs &a, int px, int py)
+{
+    Slot sl;
+    sl.nh = ((size_t)a.W * a.H + 1) >> 1;
+    sl.hc = (py * a.W + px) >> 1;
+    sl.cs = (size_t)((px + py) & 1) * sl.nh + (size_t)sl.hc;
+    return sl;
+}
+
 /* Cost-vector cache: for every pixel the cost vector of its current
- * hypothesis, [view][pixel].  Written by the initialisation and by every
- * update, read instead of re-scoring the current hypothesis
+ * hypothesis, [view][colour][slot].  Written by the initialisation and by
+ * every update, read instead of re-scoring the current hypothesis
  * (HPM.cu:1637-1638): NCC is a pure function of (pixel, plane, view), so the
  * cached values are the ones the re-score would produce. */
-__device__ __forceinline__ float *cache_at(const PMArgs &a, int v, int center)
+__device__ __forceinline__ float *cache_at(const PMArgs &a, int v, const Slot &sl)
 {
-    return a.cost_cache + (size_t)v * a.W * a.H + center;
+    return a.cost_cache + (size_t)v * 2 * sl.nh + sl.cs;
 }
 
 /* RandomInitialization, HPM.cu:510-558.  One thread per pixel. */
@@ -580,8 +602,10 @@ __device__ __forceinline__ void init_body(const PMArgs &a, int px, int py, WinWe
     a.planes[center] = h;
     a.costs[center] = c;
     a.views[center] = sel;
-    if (a.cost_cache)
-        for (int v = 0; v < a.n - 1; ++v) *cache_at(a, v, center) = cv[v * kBlock];
+    if (a.cost_cache) {
+        const Slot sl = slot_of(a, px, py);
+        for (int v = 0; v < a.n - 1; ++v) *cache_at(a, v, sl) = cv[v * kBlock];
+    }
 }
 
 __global__ void __launch_bounds__(kBlock) k_init(const __grid_constant__ PMArgs a)
@@ -699,7 +723,7 @@ __device__ __forceinline__ bool same_plane(float4 p, float4 q)
  * The other colour is read-only during both kernels, so splitting the pixel
  * update changes nothing in what is computed. */
 
-#define CAG(k, v) a.cand_costs[(size_t)((k) * S + (v)) * npx + center]
+#define CAG(k, v) a.cand_costs[(size_t)((k) * S + (v)) * sl.nh + sl.hc]
 
 /* Where the cost row of direction k lives, 4 bits per direction in the
  * pixel's hand-off code (cand_flags): the row itself, the cost-vector cache
@@ -713,11 +737,11 @@ constexpr uint32_t kCodeAllNone = 0xAAAAAAAAu;
 
 __device__ __forceinline__ bool dir_valid(uint32_t code, int k) { return ((code >> (4 * k)) & 15u) != kRowNone; }
 
-__device__ __forceinline__ float dir_cost(const PMArgs &a, uint32_t code, int k, int v, int S, size_t npx, int center)
+__device__ __forceinline__ float dir_cost(const PMArgs &a, uint32_t code, int k, int v, int S, const Slot &sl)
 {
     const uint32_t src = (code >> (4 * k)) & 15u;
     if (src == kRowOwn) return CAG(k, v);
-    if (src == kRowCache) return *cache_at(a, v, center);
+    if (src == kRowCache) return *cache_at(a, v, sl);
     if (src < 8) return CAG(src, v);
     return (k == 0 && v == 0) ? 2.0f : 0.0f;
 }
@@ -726,8 +750,8 @@ __device__ __forceinline__ void prop_dirs_body(const PMArgs &a, int iter, int px
 {
     if (px >= a.W || py >= a.rows_cov) return;
     const int W = a.W, H = a.H, S = a.n - 1;
-    const size_t npx = (size_t)W * H;
     const int center = py * W + px;
+    const Slot sl = slot_of(a, px, py);
     const RefStats rs = ref_window(a, px, py, sWW, tid);
     const float4 cur = a.planes[center];
 
@@ -784,7 +808,7 @@ __device__ __forceinline__ void prop_dirs_body(const PMArgs &a, int iter, int px
             const float good = (float)(0.8 * exp(-iter * iter * (3 - r) / 90.0));
             int good_sum = 0, bad_sum = 0;
             for (int v = 0; v < S; ++v) {
-                const float c = dir_cost(a, code, 0, v, S, npx, center);
+                const float c = dir_cost(a, code, 0, v, S, sl);
                 if (c < good) good_sum++;
                 if (c > 1.2f) bad_sum++;
             }
@@ -803,7 +827,7 @@ __device__ __forceinline__ void prop_dirs_body(const PMArgs &a, int iter, int px
 #pragma unroll
                 for (int k = 1; k < 8; ++k)
                     if (((code >> (4 * k)) & 15u) == 0u) {
-                        for (int v = 0; v < S; ++v) CAG(k, v) = dir_cost(a, code, 0, v, S, npx, center);
+                        for (int v = 0; v < S; ++v) CAG(k, v) = dir_cost(a, code, 0, v, S, sl);
                         code = (code & ~(15u << (4 * k))) | (kRowOwn << (4 * k));
                     }
             }
@@ -819,14 +843,14 @@ __device__ __forceinline__ void prop_dirs_body(const PMArgs &a, int iter, int px
                 const uint32_t sj = (code >> (4 * src)) & 15u;
                 code = (code & ~15u) | (sj == kRowOwn ? (uint32_t)src : sj);
             } else {
-                cost_vector(a, px, py, p, sWW, tid, rs, &CAG(0, 0), (int)npx);
+                cost_vector(a, px, py, p, sWW, tid, rs, &CAG(0, 0), (int)sl.nh);
                 code = (code & ~15u) | kRowOwn;
             }
         }
     }
 #pragma unroll
-    for (int k = 0; k < 8; ++k) a.cand_pos[(size_t)k * npx + center] = pos[k];
-    a.cand_flags[center] = code;
+    for (int k = 0; k < 8; ++k) a.cand_pos[(size_t)k * sl.nh + sl.hc] = pos[k];
+    a.cand_flags[sl.hc] = code;
 }
 
 /* WW: pixels of one colour per warp row (the half-step tile, tuned per view
@@ -851,17 +875,17 @@ __device__ __forceinline__ void prop_refine_body(const PMArgs &a, int iter, int 
 {
     if (px >= a.W || py >= a.rows_cov) return;
     const int W = a.W, S = a.n - 1;
-    const size_t npx = (size_t)W * a.H;
     const int center = py * W + px;
+    const Slot sl = slot_of(a, px, py);
     const HpmCamera &cam = a.cam[0];
-    const uint32_t code = a.cand_flags[center];
+    const uint32_t code = a.cand_flags[sl.hc];
     uint32_t flags = 0;
 #pragma unroll
     for (int k = 0; k < 8; ++k)
         if (dir_valid(code, k)) flags |= 1u << k;
     int pos[8];
 #pragma unroll
-    for (int k = 0; k < 8; ++k) pos[k] = a.cand_pos[(size_t)k * npx + center];
+    for (int k = 0; k < 8; ++k) pos[k] = a.cand_pos[(size_t)k * sl.nh + sl.hc];
 #define FLAG(k) (((flags >> (k)) & 1u) != 0)
     Rng rng;
     rng.init(a.seed_lo, a.seed_hi, (uint32_t)center, (uint32_t)(1 + iter), a.salt);
@@ -886,7 +910,7 @@ __device__ __forceinline__ void prop_refine_body(const PMArgs &a, int iter, int 
         float tmpw = 0;
 #pragma unroll
         for (int k = 0; k < 8; ++k) {
-            const float c = dir_cost(a, code, k, v, S, npx, center);
+            const float c = dir_cost(a, code, k, v, S, sl);
             if (c < thr) {
                 tmpw += expf(c * c / (-0.18f));
                 count++;
@@ -952,11 +976,11 @@ __device__ __forceinline__ void prop_refine_body(const PMArgs &a, int iter, int 
             if (v < S && vw[v] > 0) {
                 if (a.geom) {
                     if (FLAG(k))
-                        f += vw[v] * (dir_cost(a, code, k, v, S, npx, center) + 0.1f * geom_cost(a, v + 1, hk, px, py));
+                        f += vw[v] * (dir_cost(a, code, k, v, S, sl) + 0.1f * geom_cost(a, v + 1, hk, px, py));
                     else
-                        f += vw[v] * (dir_cost(a, code, k, v, S, npx, center) + 0.1f * 5.0f);
+                        f += vw[v] * (dir_cost(a, code, k, v, S, sl) + 0.1f * 5.0f);
                 } else {
-                    f += vw[v] * dir_cost(a, code, k, v, S, npx, center);
+                    f += vw[v] * dir_cost(a, code, k, v, S, sl);
                 }
             }
         }
@@ -982,9 +1006,9 @@ __device__ __forceinline__ void prop_refine_body(const PMArgs &a, int iter, int 
     for (int v = 0; v < SMAX; ++v) {
         if (v < S && vw[v] > 0) {
             if (a.geom)
-                cost_now += vw[v] * (*cache_at(a, v, center) + 0.1f * geom_cost(a, v + 1, plane, px, py));
+                cost_now += vw[v] * (*cache_at(a, v, sl) + 0.1f * geom_cost(a, v + 1, plane, px, py));
             else
-                cost_now += vw[v] * *cache_at(a, v, center);
+                cost_now += vw[v] * *cache_at(a, v, sl);
         }
     }
     cost_now /= wn;
@@ -1163,9 +1187,9 @@ __device__ __forceinline__ void prop_refine_body(const PMArgs &a, int iter, int 
     a.costs[center] = cost;
     a.views[center] = sel;
     if (best_row >= kRefineRow) {
-        for (int v = 0; v < S; ++v) *cache_at(a, v, center) = CAG(best_row, v);
+        for (int v = 0; v < S; ++v) *cache_at(a, v, sl) = CAG(best_row, v);
     } else if (best_row >= 0 && ((code >> (4 * best_row)) & 15u) != kRowCache) {
-        for (int v = 0; v < S; ++v) *cache_at(a, v, center) = dir_cost(a, code, best_row, v, S, npx, center);
+        for (int v = 0; v < S; ++v) *cache_at(a, v, sl) = dir_cost(a, code, best_row, v, S, sl);
     }
 #undef FLAG
 }
