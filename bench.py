@@ -104,6 +104,9 @@ def parse_args():
     ap.add_argument("--pass-case", action="store_true",
                     help="kernel-capture case: plain PatchMatch passes of one view of the scene (1 warm-up, then "
                          "--steps passes); prints the half-step time instead of the bench line")
+    ap.add_argument("--net-case", action="store_true",
+                    help="kernel-capture case of the network's tensor-core convolutions: --steps training steps "
+                         "(forward, data and weight gradients, Adam) on a 400x300 input; prints their time")
     args = ap.parse_args()
     if args.config == "stress":
         WORKLOAD.update(STRESS)
@@ -661,6 +664,39 @@ def run_pass_case(args):
             "px_relerr_lt_1pct": float(syn.depth_accuracy(planes[..., 3], sc.gt_depth[ref]))}
 
 
+def run_net_case(args):
+    """Training steps of the proposal network on one 400x300 input (the
+    coarse size of a 1600x1200 view), for ncu captures of k_conv3x3 and
+    k_conv_wgrad: CUDA events around --steps steps after one warm-up."""
+    import torch
+
+    import priornet
+
+    net = priornet.Net(0, seed=3)
+    tr = priornet.Trainer(net)
+    h, w = 300, 400
+    g = torch.Generator(device="cuda").manual_seed(5)
+    x0 = torch.randn(h, w, 16, device="cuda", generator=g).to(torch.bfloat16)
+    td = torch.rand(h, w, device="cuda", generator=g) * 4 + 2
+    tn = torch.nn.functional.normalize(torch.randn(h, w, 3, device="cuda", generator=g), dim=-1)
+    tm = torch.ones(h, w, dtype=torch.uint8, device="cuda")
+
+    def one():
+        tr.accumulate(x0, td, tn, tm, 1.2, 9.6, 1.0 / (h * w))
+        tr.apply()
+
+    one()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        one()
+    e1.record()
+    e1.synchronize()
+    return {"case": "proposal network training steps at 400x300 (4 layers of 3x3 conv, 32 channels, BF16)",
+            "ms_per_training_step": e0.elapsed_time(e1) / args.steps, "loss": float(tr.take_loss())}
+
+
 def run_reference(args, dist):
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as orc
@@ -789,6 +825,10 @@ def main():
         if args.pass_case:
             if dist.rank == 0:
                 print(json.dumps(run_pass_case(args)), flush=True)
+            return
+        if args.net_case:
+            if dist.rank == 0:
+                print(json.dumps(run_net_case(args)), flush=True)
             return
         if args.impl == "reference":
             if dist.rank != 0:

@@ -334,6 +334,8 @@ int batched_scene(hpm_ctx *c, int n_views, const float *const *images, const Hpm
         params[p].depth_min = cams[ref].depth_min * 0.6f; /* InuputInitialization, HPM.cpp:553-554 */
         params[p].depth_max = cams[ref].depth_max * 1.2f;
         params[p].seed = o->seed + (uint64_t)p;
+        params[p].fix_quirks = o->fix_quirks;
+        pc[p]->fix_quirks = o->fix_quirks != 0;
         levels[p] = o->pyramid_levels >= 0 ? o->pyramid_levels : scale_levels_of(cams[ref].width, cams[ref].height);
     }
     std::vector<int> ww;

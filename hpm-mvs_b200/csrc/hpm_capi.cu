@@ -387,6 +387,8 @@ extern "C++" int ctx_pass_args(hpm_ctx *c, const HpmParams *p, PMArgs *out)
     a.seed_lo = (uint32_t)p->seed;
     a.seed_hi = (uint32_t)(p->seed >> 32);
     a.salt = c->pass_counter++;
+    a.fix_quirks = p->fix_quirks ? 1 : 0;
+    if (p->fix_quirks) a.rows_cov = a.H; /* every row, also the last of an odd height (HPM.cu:1926) */
     c->has_state = true;
     *out = a;
     return HPM_OK;
@@ -423,6 +425,8 @@ static int run_pass(hpm_ctx *c, const HpmParams *p, int half_steps, int finalize
     a.seed_lo = (uint32_t)p->seed;
     a.seed_hi = (uint32_t)(p->seed >> 32);
     a.salt = c->pass_counter++;
+    a.fix_quirks = p->fix_quirks ? 1 : 0;
+    if (p->fix_quirks) a.rows_cov = a.H; /* every row, also the last of an odd height (HPM.cu:1926) */
     cudaEvent_t e0;
     prof_begin(c, 0, &e0);
     CK(launch_init(a, c->stream), "init kernel");

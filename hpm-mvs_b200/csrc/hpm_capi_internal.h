@@ -119,6 +119,8 @@ struct hpm_ctx {
     std::vector<hpm_ctx *> batch;
     std::vector<std::pair<long long, int>> tile_ww;
     hpm::FlowWorkspace flow;
+    /* HpmProblemOpts.fix_quirks of the problem being processed (prior levels) */
+    bool fix_quirks = false;
     float *d_scene = nullptr; /* hpm_run_scene's per-view maps, grown on demand */
     size_t scene_cap = 0;
 

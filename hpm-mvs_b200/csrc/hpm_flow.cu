@@ -161,7 +161,7 @@ static int level_prior_from_maps(hpm_ctx *c, int i, const float *d_cost, float d
         r = build_level_prior(c, cam, ws.c_cost, ws.c_depth, ws_w, ws_h, f, dmin, dmax);
         if (r) return r;
         CK(prior_coarse(cam, ws_w, ws_h, f, dmin, dmax, ws.mask, ws.ids, ws.tri_planes, ws.knn_planes,
-                        ws.c_prior_depth, ws.c_prior_normal, s),
+                        ws.c_prior_depth, ws.c_prior_normal, s, !c->fix_quirks),
            "coarse prior");
         k_pack4<<<grid1((int)cn), 256, 0, s>>>(ws.c_prior_depth, ws.c_prior_normal, (int)cn, ws.c_packed);
         const int sr = H / ws_h, sc = W / ws_w;
@@ -242,6 +242,8 @@ static int process_problem(hpm_ctx *c, const HpmProblemOpts *o, int half_steps, 
     p.depth_min = cam.depth_min * 0.6f; /* InuputInitialization, HPM.cpp:553-554 */
     p.depth_max = cam.depth_max * 1.2f;
     p.seed = o->seed;
+    p.fix_quirks = o->fix_quirks;
+    c->fix_quirks = o->fix_quirks != 0;
     FlowWorkspace &ws = c->flow;
     ws.last_points = ws.last_triangles = 0;
     if (o->geom_consistency) {
@@ -460,7 +462,8 @@ static int run_scene_impl(hpm_ctx *c, int n_views, const float *const *images, c
                     rr = load_problem(cc, p);
                 }
                 if (!rr && !net) {
-                    HpmProblemOpts po = {o->planar_prior, 0, 0, o->seed + (uint64_t)p, o->pyramid_levels};
+                    HpmProblemOpts po = {o->planar_prior, 0, 0, o->seed + (uint64_t)p, o->pyramid_levels,
+                                         o->fix_quirks};
                     const int ref = ref_ids[p];
                     float *prior_out = out_prior_depths ? out_prior_depths[ref] : nullptr;
                     rr = hpm_process_problem(cc, &po, m.depth_a[ref], m.normal[ref], m.cost[ref], prior_out);
@@ -505,7 +508,8 @@ static int run_scene_impl(hpm_ctx *c, int n_views, const float *const *images, c
             k_pack_planes<<<grid1((int)np), 256, 0, s>>>(m.normal[ref], src_depths[ref], (int)np,
                                                          reinterpret_cast<float4 *>(ctx_planes(c)));
             CK(cudaMemcpyAsync(ctx_costs(c), m.cost[ref], sizeof(float) * np, cudaMemcpyDeviceToDevice, s), "costs");
-            HpmProblemOpts po = {0, 1, gi >= 1, o->seed + 1000003ull * (gi + 1) + (uint64_t)p, o->pyramid_levels};
+            HpmProblemOpts po = {0, 1, gi >= 1, o->seed + 1000003ull * (gi + 1) + (uint64_t)p, o->pyramid_levels,
+                                 o->fix_quirks};
             /* the geometric depth map is rewritten view by view (depths_geom.dmb) */
             r = process_problem(c, &po, net ? half_steps : 6, m.depth_g[ref], m.normal[ref], m.cost[ref], nullptr);
             if (r) return r;

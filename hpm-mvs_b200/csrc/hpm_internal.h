@@ -47,6 +47,7 @@ struct PMArgs {
     int radius, radius_increment;
     float sigma_spatial, sigma_color;
     int top_k;
+    int fix_quirks; /* HpmParams.fix_quirks */
     HpmCamera cam[kMaxViews];
     ViewDev view[kMaxViews];
     const PairGeom *pair; /* [n], entry 0 unused */

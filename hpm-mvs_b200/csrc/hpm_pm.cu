@@ -586,7 +586,10 @@ __device__ __forceinline__ void init_body(const PMArgs &a, int px, int py, WinWe
             h = perturbed_normal(cam, px, py, hp, rng, (float)(3 * pert * kPiD));
             h.w = dp;
         } else {
-            h = a.planes[center];
+            /* the previous pass's world-frame normal, reused as it is
+             * (HPM.cu:547-551); with fix_quirks rotated back to the
+             * reference frame first, as the geometric branch does */
+            h = a.fix_quirks ? transform_normal_to_ref(cam, a.planes[center]) : a.planes[center];
             const float depth = h.w;
             h.w = distance_to_origin(cam, px, py, depth, h);
         }
@@ -635,7 +638,8 @@ __device__ __forceinline__ bool first_site_valid(int k, int r, int px, int py, i
 }
 
 /* NESP site choice of one direction at round r.  Strips: 5 sites 2 apart
- * from +/-(5+10r), the right strip keeps the maximum (HPM.cu:1330, 744).
+ * from +/-(5+10r), the right strip keeps the maximum (HPM.cu:1330, 744;
+ * the minimum with fix_quirks).
  * Polylines: start (+/-5|6) shifted 8r outward, then 7 zig-zag steps of 2
  * (HPM.cu:1346-1471). */
 __device__ int select_site(const PMArgs &a, int k, int r, int px, int py)
@@ -659,7 +663,7 @@ __device__ int select_site(const PMArgs &a, int k, int r, int px, int py)
             if (!ok) break;
             const int q = (py + dy * (off + 2 * i)) * W + (px + dx * (off + 2 * i));
             const float cq = costs[q];
-            if (k == 7 ? (cmin < cq) : (cq < cmin)) {
+            if ((k == 7 && !a.fix_quirks) ? (cmin < cq) : (cq < cmin)) {
                 cmin = cq;
                 best = q;
             }
@@ -743,7 +747,7 @@ __device__ __forceinline__ float dir_cost(const PMArgs &a, uint32_t code, int k,
     if (src == kRowOwn) return CAG(k, v);
     if (src == kRowCache) return *cache_at(a, v, sl);
     if (src < 8) return CAG(src, v);
-    return (k == 0 && v == 0) ? 2.0f : 0.0f;
+    return (a.fix_quirks || (k == 0 && v == 0)) ? 2.0f : 0.0f; /* fix_quirks: the intended {2, 2, ...} */
 }
 
 __device__ __forceinline__ void prop_dirs_body(const PMArgs &a, int iter, int px, int py, WinPair *sWW, int tid)
@@ -1115,7 +1119,11 @@ __device__ __forceinline__ void prop_refine_body(const PMArgs &a, int iter, int 
             n_rand = random_normal(cam, px, py, rng, depth_now);
         }
         const float lo = (1 - pert) * depth_now, hi = (1 + pert) * depth_now;
-        const float depth_pert = rng.uniform() * (hi - lo) + lo;
+        float depth_pert = rng.uniform() * (hi - lo) + lo;
+        /* do { ... } while (d < min && d > max) never repeats (HPM.cu:1170-1172);
+         * with fix_quirks the draw repeats while out of range, at most 8 times */
+        for (int t = 1; a.fix_quirks && t < 8 && (depth_pert < a.dmin || depth_pert > a.dmax); ++t)
+            depth_pert = rng.uniform() * (hi - lo) + lo;
         const float4 n_pert = perturbed_normal(cam, px, py, plane, rng, (float)(pert * kPiD));
         const float depths[5] = {depth_rand, depth_now, depth_rand, depth_now, depth_pert};
         const float4 normals[5] = {plane, n_rand, n_rand, n_pert, plane};

@@ -341,10 +341,10 @@ __device__ float4 to_world(const HpmCamera &c, float4 h) /* TransformNormal, HPM
 
 /* Coarse level, main.cpp:124-162: prior depth and world normal (zero where
  * the mask ends up 0).  Triangle planes are range-checked against the
- * pass's range widened once more (x1.2 / x0.6, main.cpp:129), kNN planes
- * against the pass's range. */
-__global__ void k_prior_coarse(HpmCamera cam, int w, int h, float factor, float dmin, float dmax,
-                               float *__restrict__ mask, const int *__restrict__ ids, const float4 *__restrict__ tri_planes,
+ * pass's range widened once more (x1.2 / x0.6, main.cpp:129; hi_widen /
+ * lo_widen, 1 with fixed quirks), kNN planes against the pass's range. */
+__global__ void k_prior_coarse(HpmCamera cam, int w, int h, float factor, float dmin, float dmax, float hi_widen,
+                               float lo_widen, float *__restrict__ mask, const int *__restrict__ ids, const float4 *__restrict__ tri_planes,
                                const float4 *__restrict__ knn_planes, float *__restrict__ out_depth,
                                float *__restrict__ out_normal)
 {
@@ -358,7 +358,7 @@ __global__ void k_prior_coarse(HpmCamera cam, int w, int h, float factor, float 
     if (m > 0) {
         const float4 p = tri_planes[ids[c] - 1];
         d = depth_from_plane_f(cam, p, x, y, factor);
-        if (d <= __fmul_rn(dmax, 1.2f) && d >= __fmul_rn(dmin, 0.6f))
+        if (d <= __fmul_rn(dmax, hi_widen) && d >= __fmul_rn(dmin, lo_widen))
             n = to_world(cam, p);
         else
             m = 0, d = 0.0f;
@@ -506,10 +506,11 @@ cudaError_t prior_knn(const HpmCamera &cam, const int2 *pts, const int *cell_sta
 
 cudaError_t prior_coarse(const HpmCamera &cam, int w, int h, float factor, float dmin, float dmax, float *mask,
                          const int *ids, const float4 *tri_planes, const float4 *knn_planes, float *out_depth,
-                         float *out_normal, cudaStream_t s)
+                         float *out_normal, cudaStream_t s, bool widen)
 {
-    k_prior_coarse<<<grid2(w, h), dim3(16, 16), 0, s>>>(cam, w, h, factor, dmin, dmax, mask, ids, tri_planes,
-                                                        knn_planes, out_depth, out_normal);
+    k_prior_coarse<<<grid2(w, h), dim3(16, 16), 0, s>>>(cam, w, h, factor, dmin, dmax, widen ? 1.2f : 1.0f,
+                                                        widen ? 0.6f : 1.0f, mask, ids, tri_planes, knn_planes,
+                                                        out_depth, out_normal);
     return cudaGetLastError();
 }
 

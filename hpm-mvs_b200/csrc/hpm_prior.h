@@ -28,9 +28,12 @@ cudaError_t prior_ids_to_mask(const int *ids, int n, float *mask, cudaStream_t s
 cudaError_t prior_knn(const HpmCamera &cam, const int2 *pts, const int *cell_start, const int *cell_pts, int cell,
                       int gw, int gh, const float *depth, int w, int h, float factor, float dmin, float dmax, float *mask,
                       float4 *planes, cudaStream_t s);
+/* widen: range-check triangle planes against [dmin, dmax] widened once
+ * more (x0.6 / x1.2), as the reference does (main.cpp:129, 282); false
+ * checks them against [dmin, dmax] */
 cudaError_t prior_coarse(const HpmCamera &cam, int w, int h, float factor, float dmin, float dmax, float *mask,
                          const int *ids, const float4 *tri_planes, const float4 *knn_planes, float *out_depth,
-                         float *out_normal, cudaStream_t s);
+                         float *out_normal, cudaStream_t s, bool widen = true);
 cudaError_t prior_reload(const HpmCamera &cam, int w, int h, float dmin, float dmax, const float *up_depth,
                          const float4 *up_normal, float4 *prior, uint32_t *masks, cudaStream_t s);
 cudaError_t prior_full(const HpmCamera &cam, int w, int h, float dmin, float dmax, const float *mask, const int *ids,

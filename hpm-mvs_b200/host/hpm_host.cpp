@@ -347,6 +347,7 @@ void HPM::RunProblem(bool planar_prior, uint64_t seed, int pyramid_levels)
     o.multi_geometry = params_.multi_geometry;
     o.seed = seed;
     o.pyramid_levels = pyramid_levels;
+    o.fix_quirks = params_.fix_quirks;
     check(hpm_process_problem(ctx_, &o, depth.data(), normal.data(), cost.data(), prior_depth_.data()),
           "hpm_process_problem");
     planes_host_.resize(4 * n);
@@ -538,7 +539,8 @@ long long RunFusion(const std::string &dense_folder, const std::vector<Problem> 
 }
 
 void ProcessProblem(const std::string &dense_folder, const Problem &problem, bool geom_consistency,
-                    bool planar_prior, bool multi_geometry, uint64_t seed, int pyramid_levels, int device)
+                    bool planar_prior, bool multi_geometry, uint64_t seed, int pyramid_levels, int device,
+                    bool reference_compat)
 {
     std::cout << "Processing image " << std::setw(8) << std::setfill('0') << problem.ref_image_id << "..."
               << std::endl;
@@ -546,6 +548,7 @@ void ProcessProblem(const std::string &dense_folder, const Problem &problem, boo
     make_dir(dense_folder + "/HPM");
     make_dir(folder);
     HPM hpm(device);
+    hpm.SetReferenceCompat(reference_compat);
     if (geom_consistency) hpm.SetGeomConsistencyParams(multi_geometry);
     hpm.InuputInitialization(dense_folder, problem);
     hpm.CudaSpaceInitialization(dense_folder, problem);
@@ -571,7 +574,7 @@ void ProcessProblem(const std::string &dense_folder, const Problem &problem, boo
 }
 
 void RunScene(const std::string &dense_folder, const std::vector<Problem> &problems, bool planar_prior,
-              int geom_iterations, uint64_t seed, int pyramid_levels, int device)
+              int geom_iterations, uint64_t seed, int pyramid_levels, int device, bool reference_compat)
 {
     /* every view a problem names, numbered in order of appearance */
     std::map<int, int> index;
@@ -622,7 +625,7 @@ void RunScene(const std::string &dense_folder, const std::vector<Problem> &probl
         hpm_ctx *c;
         ~Destroy() { hpm_destroy(c); }
     } destroy{ctx};
-    const HpmSceneOpts o = {planar_prior ? 1 : 0, geom_iterations, seed, pyramid_levels, 0};
+    const HpmSceneOpts o = {planar_prior ? 1 : 0, geom_iterations, seed, pyramid_levels, 0, reference_compat ? 0 : 1};
     rc = hpm_run_scene_ex(ctx, (int)n, img_ptr.data(), cams.data(), (int)np, refs.data(), counts.data(), srcs.data(),
                           &o, pd.data(), pn.data(), pc.data(), pp.data(), pr.data());
     if (rc != HPM_OK) throw Error(rc, std::string("hpm_run_scene_ex: ") + hpm_last_error(ctx));

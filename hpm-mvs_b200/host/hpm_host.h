@@ -66,6 +66,10 @@ public:
     void SetGeomConsistencyParams(bool multi_geometry = false); /* HPM.cpp:468-475 */
     void SetPlanarPriorParams();                                 /* HPM.cpp:477-480 */
     void SetSeed(uint64_t seed) { params_.seed = seed; }
+    /* true (the default): the reference's behaviour everywhere; false fixes
+     * the quirks listed at HpmParams in hpm_b200.h (no counterpart in the
+     * reference) */
+    void SetReferenceCompat(bool on) { params_.fix_quirks = on ? 0 : 1; }
 
     int GetReferenceImageWidth() const;
     int GetReferenceImageHeight() const;
@@ -128,7 +132,7 @@ long long RunFusion(const std::string &dense_folder, const std::vector<Problem> 
  * under dense_folder/HPM/2333_%08d/. */
 void ProcessProblem(const std::string &dense_folder, const Problem &problem, bool geom_consistency,
                     bool planar_prior, bool multi_geometry = false, uint64_t seed = 0, int pyramid_levels = -1,
-                    int device = 0);
+                    int device = 0, bool reference_compat = true);
 
 /* main()'s depth estimation (main.cpp:646-674) in one hpm_run_scene_ex
  * call: pass set A, then geom_iterations geometric iterations, over every
@@ -138,7 +142,7 @@ void ProcessProblem(const std::string &dense_folder, const Problem &problem, boo
  * that loop (S + p, S + 1000003 (g + 1) + p), hence the same files.  Host
  * memory: about 20 bytes per pixel of each reference view, plus the images. */
 void RunScene(const std::string &dense_folder, const std::vector<Problem> &problems, bool planar_prior,
-              int geom_iterations, uint64_t seed, int pyramid_levels, int device);
+              int geom_iterations, uint64_t seed, int pyramid_levels, int device, bool reference_compat = true);
 
 /* What main() has finished in a dense folder, so that a run can stop and be
  * resumed (the reference has no such log; its passes only exchange .dmb

@@ -6,7 +6,7 @@
  *
  *   hpm_mvs dense_folder [--seed S] [--levels K] [--device D] [--no-prior]
  *                        [--geom-iterations G] [--no-fusion] [--per-problem]
- *                        [--resume] [--stop-after N]
+ *                        [--resume] [--stop-after N] [--no-reference-compat]
  *
  * By default the passes run as one scene (RunScene: maps in device memory
  * between passes, pass set A on two host threads, files written at the
@@ -22,6 +22,10 @@
  * of the scene form, the fusion); --resume skips the steps the log holds, so
  * a scene can be computed in several runs.  Both forms resume to the files
  * one uninterrupted run writes.
+ *
+ * The reference's behaviour is kept throughout by default (its quirks
+ * included); --no-reference-compat fixes the quirks listed at HpmParams in
+ * hpm_b200.h.
  */
 #include <cstdlib>
 #include <cstring>
@@ -36,14 +40,15 @@ int main(int argc, char **argv)
 {
     if (argc < 2 || !strcmp(argv[1], "-h") || !strcmp(argv[1], "--help")) {
         std::cout << "USAGE: hpm_mvs dense_folder [--seed S] [--levels K] [--device D] [--no-prior] "
-                     "[--geom-iterations G] [--no-fusion] [--per-problem] [--resume] [--stop-after N]"
+                     "[--geom-iterations G] [--no-fusion] [--per-problem] [--resume] [--stop-after N] "
+                     "[--no-reference-compat]"
                   << std::endl;
         return argc < 2 ? -1 : 0;
     }
     const std::string dense_folder = argv[1];
     uint64_t seed = 0;
     int levels = -1, device = 0, geom_iterations = 2;
-    bool planar_prior = true, fusion = true, per_problem = false, resume = false;
+    bool planar_prior = true, fusion = true, per_problem = false, resume = false, compat = true;
     long long stop_after = -1;
     for (int i = 2; i < argc; ++i) {
         const std::string a = argv[i];
@@ -70,6 +75,8 @@ int main(int argc, char **argv)
             per_problem = true;
         else if (a == "--resume")
             resume = true;
+        else if (a == "--no-reference-compat")
+            compat = false;
         else if (a == "--stop-after")
             stop_after = std::atoll(next("--stop-after"));
         else {
@@ -83,7 +90,8 @@ int main(int argc, char **argv)
         std::cout << "There are " << problems.size() << " problems needed to be processed!" << std::endl;
         std::ostringstream settings;
         settings << "seed=" << seed << " levels=" << levels << " prior=" << planar_prior
-                 << " geom_iterations=" << geom_iterations << " form=" << (per_problem ? "per-problem" : "scene");
+                 << " geom_iterations=" << geom_iterations << " form=" << (per_problem ? "per-problem" : "scene")
+                 << (compat ? "" : " fix_quirks=1");
         hpm_host::Progress progress(dense_folder, settings.str(), resume);
         long long steps = 0;
         /* runs one step unless the log holds it; false once --stop-after is reached */
@@ -101,21 +109,22 @@ int main(int argc, char **argv)
         };
         if (!per_problem) {
             if (!step("scene", [&] {
-                    hpm_host::RunScene(dense_folder, problems, planar_prior, geom_iterations, seed, levels, device);
+                    hpm_host::RunScene(dense_folder, problems, planar_prior, geom_iterations, seed, levels, device,
+                                       compat);
                 }))
                 return stopped();
         } else {
             for (size_t p = 0; p < problems.size(); ++p)
                 if (!step("A " + std::to_string(problems[p].ref_image_id), [&] {
                         hpm_host::ProcessProblem(dense_folder, problems[p], false, planar_prior, false, seed + p,
-                                                 levels, device);
+                                                 levels, device, compat);
                     }))
                     return stopped();
             for (int g = 0; g < geom_iterations; ++g)
                 for (size_t p = 0; p < problems.size(); ++p)
                     if (!step("G" + std::to_string(g) + " " + std::to_string(problems[p].ref_image_id), [&] {
                             hpm_host::ProcessProblem(dense_folder, problems[p], true, false, g > 0,
-                                                     seed + 1000003ull * (g + 1) + p, levels, device);
+                                                     seed + 1000003ull * (g + 1) + p, levels, device, compat);
                         }))
                         return stopped();
         }

@@ -47,7 +47,7 @@ EXPORTED = [
 
 class HpmSceneOpts(ctypes.Structure):
     _fields_ = [("planar_prior", ctypes.c_int), ("geom_iterations", ctypes.c_int), ("seed", ctypes.c_uint64),
-                ("pyramid_levels", ctypes.c_int), ("iterations", ctypes.c_int)]
+                ("pyramid_levels", ctypes.c_int), ("iterations", ctypes.c_int), ("fix_quirks", ctypes.c_int)]
 
 
 class HpmNetWeights(ctypes.Structure):
@@ -56,7 +56,7 @@ class HpmNetWeights(ctypes.Structure):
 
 class HpmProblemOpts(ctypes.Structure):
     _fields_ = [("planar_prior", ctypes.c_int), ("geom_consistency", ctypes.c_int), ("multi_geometry", ctypes.c_int),
-                ("seed", ctypes.c_uint64), ("pyramid_levels", ctypes.c_int)]
+                ("seed", ctypes.c_uint64), ("pyramid_levels", ctypes.c_int), ("fix_quirks", ctypes.c_int)]
 
 
 def delaunay(points: np.ndarray, w: int, h: int) -> np.ndarray:
@@ -107,7 +107,7 @@ class HpmParams(ctypes.Structure):
                 ("sigma_spatial", ctypes.c_float), ("sigma_color", ctypes.c_float), ("top_k", ctypes.c_int),
                 ("depth_min", ctypes.c_float), ("depth_max", ctypes.c_float), ("geom_consistency", ctypes.c_int),
                 ("multi_geometry", ctypes.c_int), ("planar_prior", ctypes.c_int),
-                ("honour_max_iterations", ctypes.c_int), ("seed", ctypes.c_uint64)]
+                ("honour_max_iterations", ctypes.c_int), ("seed", ctypes.c_uint64), ("fix_quirks", ctypes.c_int)]
 
 
 class HpmError(RuntimeError):
@@ -140,7 +140,9 @@ def _p(a):
 
 
 def default_params(depth_min: float, depth_max: float, *, seed: int = 0, geom: bool = False,
-                   prior: bool = False, multi_geometry: bool = False) -> HpmParams:
+                   prior: bool = False, multi_geometry: bool = False, fix_quirks: bool = False) -> HpmParams:
+    """HpmParams with the reference's defaults; fix_quirks: see HpmParams in
+    include/hpm_b200.h (False keeps the reference's behaviour)."""
     p = HpmParams()
     lib().hpm_default_params(ctypes.byref(p))
     p.depth_min = depth_min
@@ -149,6 +151,7 @@ def default_params(depth_min: float, depth_max: float, *, seed: int = 0, geom: b
     p.geom_consistency = int(geom)
     p.planar_prior = int(prior)
     p.multi_geometry = int(multi_geometry)
+    p.fix_quirks = int(fix_quirks)
     return p
 
 
@@ -226,20 +229,23 @@ class Context:
         self._check(lib().hpm_run_partial(self._h, ctypes.byref(params), int(half_steps), int(finalize)),
                     "hpm_run_partial")
 
-    def process_problem(self, *, planar_prior=True, geom=False, multi_geometry=False, seed=0, pyramid_levels=-1):
+    def process_problem(self, *, planar_prior=True, geom=False, multi_geometry=False, seed=0, pyramid_levels=-1,
+                        fix_quirks=False):
         """ProcessProblem for the current views: returns (depth, normal, cost, prior_depth)."""
         h, w = self.shape
         depth = np.empty((h, w), np.float32)
         normal = np.empty((h, w, 3), np.float32)
         cost = np.empty((h, w), np.float32)
         prior = np.empty((h, w), np.float32)
-        o = HpmProblemOpts(int(planar_prior), int(geom), int(multi_geometry), int(seed), int(pyramid_levels))
+        o = HpmProblemOpts(int(planar_prior), int(geom), int(multi_geometry), int(seed), int(pyramid_levels),
+                           int(fix_quirks))
         self._check(lib().hpm_process_problem(self._h, ctypes.byref(o), _p(depth), _p(normal), _p(cost), _p(prior)),
                     "hpm_process_problem")
         return depth, normal, cost, prior
 
     def run_scene(self, images, cams, pairs, *, planar_prior=True, geom_iterations=2, seed=0, pyramid_levels=-1,
-                  images_are_device=False, outputs=True, extra_maps=False, net=None, batched=False, iterations=0):
+                  images_are_device=False, outputs=True, extra_maps=False, net=None, batched=False, iterations=0,
+                  fix_quirks=False):
         """The reference's main() over a scene.  images: per-view float32 [H, W]
         arrays, or device pointers (ints) with images_are_device; pairs:
         [(ref, [sources])].  outputs: True to return new per-view (depth,
@@ -251,7 +257,8 @@ class Context:
         form (hpm_run_scene_net) instead of the plain form.  batched: the
         batched form (hpm_run_scene_batched; with net, the batched prior-net
         form, hpm_run_scene_batched_net).  iterations: with net, PatchMatch
-        iterations of each full-scale pass (0: the reference's 3)."""
+        iterations of each full-scale pass (0: the reference's 3).  fix_quirks:
+        HpmSceneOpts.fix_quirks (False keeps the reference's behaviour)."""
         n = len(cams)
         cams = np.ascontiguousarray(cams, dtype=CAMERA_DTYPE)
         if images_are_device:
@@ -266,7 +273,8 @@ class Context:
         srcs = np.zeros((len(pairs), MAX_IMAGES - 1), np.int32)
         for i, (_, s) in enumerate(pairs):
             srcs[i, :len(s)] = s
-        o = HpmSceneOpts(int(planar_prior), int(geom_iterations), int(seed), int(pyramid_levels), int(iterations))
+        o = HpmSceneOpts(int(planar_prior), int(geom_iterations), int(seed), int(pyramid_levels), int(iterations),
+                         int(fix_quirks))
         outs = None
         if isinstance(outputs, (tuple, list)):
             outs = list(zip(*outputs))

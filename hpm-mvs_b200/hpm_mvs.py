@@ -6,6 +6,7 @@ library to the bytes cv::imread gives (HPM.cpp:492, main.cpp:523).
     python hpm-mvs_b200/hpm_mvs.py dense_folder [--seed S] [--levels K]
                                    [--geom-iterations G] [--no-prior] [--device D]
                                    [--no-fusion] [--per-problem] [--resume] [--stop-after N]
+                                   [--no-reference-compat]
 
 Writes HPM/2333_%08d/{depths,depths_geom,normals,costs,depths_prior}.dmb like
 the reference's ProcessProblem, then fuses them into HPM/HPM_model.ply
@@ -59,7 +60,8 @@ def load_view(folder: str, vid: int):
     return img, cam
 
 
-def process_problem(ctx, folder, ref, srcs, views, *, geom, planar_prior, multi_geometry, seed, levels):
+def process_problem(ctx, folder, ref, srcs, views, *, geom, planar_prior, multi_geometry, seed, levels,
+                    fix_quirks=False):
     """ProcessProblem (main.cpp:35-499) for one reference view."""
     out = os.path.join(folder, "HPM", f"2333_{ref:08d}")
     os.makedirs(out, exist_ok=True)
@@ -73,7 +75,8 @@ def process_problem(ctx, folder, ref, srcs, views, *, geom, planar_prior, multi_
         ctx.set_geom_depths(depths)
         ctx.set_hypotheses(np.concatenate([normal, depths[0][..., None]], -1), cost)
     d, n, c, pd = ctx.process_problem(planar_prior=planar_prior and not geom, geom=geom,
-                                      multi_geometry=multi_geometry, seed=seed, pyramid_levels=levels)
+                                      multi_geometry=multi_geometry, seed=seed, pyramid_levels=levels,
+                                      fix_quirks=fix_quirks)
     if planar_prior and not geom:
         hb.write_dmb(os.path.join(out, "depths_prior.dmb"), pd)
     hb.write_dmb(os.path.join(out, "depths_geom.dmb" if geom else "depths.dmb"), d)
@@ -81,14 +84,15 @@ def process_problem(ctx, folder, ref, srcs, views, *, geom, planar_prior, multi_
     hb.write_dmb(os.path.join(out, "costs.dmb"), c)
 
 
-def run_scene(ctx, folder, problems, needed, views, *, planar_prior, geom_iterations, seed, levels):
+def run_scene(ctx, folder, problems, needed, views, *, planar_prior, geom_iterations, seed, levels,
+              fix_quirks=False):
     """All passes in one hpm_run_scene_ex call (maps in device memory between
     passes), then the files ProcessProblem leaves for every problem."""
     index = {v: i for i, v in enumerate(needed)}
     pairs = [(index[ref], [index[s] for s in srcs]) for ref, srcs in problems]
     d, n, c, pa, pr = ctx.run_scene([views[v][0] for v in needed], np.array([views[v][1] for v in needed]), pairs,
                                     planar_prior=planar_prior, geom_iterations=geom_iterations, seed=seed,
-                                    pyramid_levels=levels, extra_maps=True)
+                                    pyramid_levels=levels, extra_maps=True, fix_quirks=fix_quirks)
     for ref, _ in problems:
         i = index[ref]
         out = os.path.join(folder, "HPM", f"2333_{ref:08d}")
@@ -190,11 +194,16 @@ def main(argv=None):
                     help="ProcessProblem problem by problem through .dmb files, as the reference runs")
     ap.add_argument("--resume", action="store_true", help="skip the steps HPM/progress.txt lists")
     ap.add_argument("--stop-after", type=int, default=-1, help="stop once this many steps have finished")
+    ap.add_argument("--no-reference-compat", action="store_true",
+                    help="fix the reference's quirks listed at HpmParams in include/hpm_b200.h (default: keep the "
+                         "reference's behaviour)")
     a = ap.parse_args(argv)
     problems = hb.read_pair(os.path.join(a.dense_folder, "pair.txt"))
     print(f"There are {len(problems)} problems needed to be processed!")
     settings = (f"seed={a.seed} levels={a.levels} prior={int(not a.no_prior)} geom_iterations={a.geom_iterations} "
-                f"form={'per-problem' if a.per_problem else 'scene'}")
+                f"form={'per-problem' if a.per_problem else 'scene'}" + (" fix_quirks=1" if a.no_reference_compat
+                                                                         else ""))
+    fix = a.no_reference_compat
     progress = Progress(a.dense_folder, settings, a.resume)
     count = [0]
 
@@ -223,17 +232,18 @@ def main(argv=None):
             for p, (ref, srcs) in enumerate(problems):
                 step(f"A {ref}", lambda: process_problem(ctx(), a.dense_folder, ref, srcs, state["views"], geom=False,
                                                          planar_prior=not a.no_prior, multi_geometry=False,
-                                                         seed=a.seed + p, levels=a.levels))
+                                                         seed=a.seed + p, levels=a.levels, fix_quirks=fix))
             for g in range(a.geom_iterations):
                 for p, (ref, srcs) in enumerate(problems):
                     step(f"G{g} {ref}",
                          lambda: process_problem(ctx(), a.dense_folder, ref, srcs, state["views"], geom=True,
                                                  planar_prior=False, multi_geometry=g > 0,
-                                                 seed=a.seed + 1000003 * (g + 1) + p, levels=a.levels))
+                                                 seed=a.seed + 1000003 * (g + 1) + p, levels=a.levels,
+                                                 fix_quirks=fix))
         else:
             step("scene", lambda: run_scene(ctx(), a.dense_folder, problems, state["needed"], state["views"],
                                             planar_prior=not a.no_prior, geom_iterations=a.geom_iterations,
-                                            seed=a.seed, levels=a.levels))
+                                            seed=a.seed, levels=a.levels, fix_quirks=fix))
         if "ctx" in state:
             state.pop("ctx").close()
         if not a.no_fusion:

@@ -59,7 +59,23 @@ typedef struct {
  * radius_increment, sigma_spatial, sigma_color and top_k keep the
  * reference's defaults (11, 2, 5, 3, 4); max_iterations is accepted but, as in
  * the reference (HPM.cu:1933), every pass runs 3 iterations unless
- * honour_max_iterations is set. */
+ * honour_max_iterations is set.
+ *
+ * fix_quirks = 0 (the default) keeps the reference's behaviour everywhere.
+ * fix_quirks = 1 gives these places of the reference the behaviour their
+ * code evidently intends (each changes results):
+ *   - the right-far strip picks its minimum-cost site, like the other
+ *     three strips (the reference keeps the maximum, HPM.cu:1330, 744);
+ *   - an invalid direction scores 2 for every view (the reference's
+ *     float cost_array[8][32] = { 2.0f } sets only [0][0], HPM.cu:1244);
+ *   - the prior pass starts from the previous pass's normal rotated back
+ *     to the reference frame (HPM.cu:547-551 reuses the world-frame one);
+ *   - the refinement's perturbed depth is drawn again until it lies in the
+ *     depth range, at most 8 draws (the reference's do-while never
+ *     repeats, HPM.cu:1170-1172);
+ *   - every row is propagated and filtered (the reference's grid skips the
+ *     last row of an odd height, HPM.cu:1926).
+ * Q6 (max_iterations ignored) has its own switch, honour_max_iterations. */
 typedef struct {
     int max_iterations;
     int patch_size;
@@ -74,6 +90,7 @@ typedef struct {
     int planar_prior;
     int honour_max_iterations; /* 0 = reference behaviour (always 3) */
     uint64_t seed;             /* Philox key of this pass's random stream */
+    int fix_quirks;            /* 0 = the reference's behaviour (see above) */
 } HpmParams;
 
 /* Fills p with the reference defaults (HPM.h:29-46). */
@@ -132,6 +149,9 @@ typedef struct {
     uint64_t seed;        /* Philox key of the passes of this problem */
     int pyramid_levels;   /* coarse prior levels; -1 = ComputingMultiScaleSettings
                              (HPM.cpp:851-860: halvings until max side <= 1000) */
+    int fix_quirks;       /* HpmParams.fix_quirks of every pass; with 1 the coarse levels' triangle planes are
+                             also range-checked against the pass's range instead of one widened once more
+                             (main.cpp:129, 282) */
 } HpmProblemOpts;
 
 /* One reference view through ProcessProblem (main.cpp:35-499) on the
@@ -155,6 +175,7 @@ typedef struct {
     int pyramid_levels; /* -1 = the reference's rule */
     int iterations;     /* prior-net forms only: PatchMatch iterations of each full-scale pass, the geometric
                            ones included (0 = 3, the reference's count; the plain form always runs 3) */
+    int fix_quirks;     /* HpmProblemOpts.fix_quirks of every problem (0 = the reference's behaviour) */
 } HpmSceneOpts;
 
 /* The reference's main() (main.cpp:636-677) over a scene: ProcessProblem
