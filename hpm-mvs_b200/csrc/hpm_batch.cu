@@ -36,7 +36,9 @@
  * to it; the graph form replaced it.
  */
 #include <algorithm>
+#include <atomic>
 #include <cmath>
+#include <thread>
 #include <vector>
 
 #include "hpm_capi_internal.h"
@@ -69,6 +71,39 @@ __global__ void k_pack_maps(const float *__restrict__ normal3, const float *__re
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     planes[i] = make_float4(normal3[3 * i], normal3[3 * i + 1], normal3[3 * i + 2], depth[i]);
+}
+
+/* f(p) for every problem p < n on up to 4 host threads, so that one
+ * problem's host work between passes (the Delaunay of its prior levels,
+ * with the synchronisations around it) overlaps the others' device work.
+ * f may touch only problem p's own context and stream, and reports a
+ * failure there.  Returns the failure of the lowest failing problem (after
+ * all threads have stopped) and its index in *failed. */
+template <typename F>
+int for_each_problem(int n, F f, int *failed)
+{
+    const int workers = std::max(1, std::min(4, n));
+    std::atomic<int> next{0};
+    std::atomic<bool> stop{false};
+    std::vector<int> rc(n, HPM_OK);
+    auto run = [&]() {
+        for (;;) {
+            const int p = next.fetch_add(1);
+            if (p >= n || stop.load()) return;
+            rc[p] = f(p);
+            if (rc[p]) stop.store(true);
+        }
+    };
+    std::vector<std::thread> pool;
+    for (int w = 1; w < workers; ++w) pool.emplace_back(run);
+    run();
+    for (std::thread &t : pool) t.join();
+    for (int p = 0; p < n; ++p)
+        if (rc[p]) {
+            *failed = p;
+            return rc[p];
+        }
+    return HPM_OK;
 }
 
 /* A batch of problem contexts, their half-step tile widths, and the
@@ -211,50 +246,59 @@ int net_pass_set_a(hpm_ctx *c, const std::vector<hpm_ctx *> &pc, const std::vect
                    const std::vector<std::vector<const float *>> &images)
 {
     const int n = (int)pc.size();
+    int bad = 0;
+    int r = for_each_problem(
+        n, [&](int p) { return net_coarse_views(pc[p], pc[p]->n, images[p].data(), pc[p]->cams); }, &bad);
+    if (r) return ctx_fail(c, r, "batched prior-net form, problem %d: %s", bad, hpm_last_error(pc[bad]));
     std::vector<hpm_ctx *> cc(n);
-    for (int p = 0; p < n; ++p) {
-        hpm_ctx *b = pc[p];
-        int r = net_coarse_views(b, b->n, images[p].data(), b->cams);
-        if (r) return ctx_fail(c, r, "batched prior-net form, problem %d: %s", p, hpm_last_error(b));
-        cc[p] = b->coarse;
-    }
+    for (int p = 0; p < n; ++p) cc[p] = pc[p]->coarse;
     {
         const Range coarse("batched coarse passes");
         std::vector<int> cww;
-        int r = tune_tiles(c, cc, params, cww);
+        r = tune_tiles(c, cc, params, cww);
         if (r) return r;
         Plan cplan;
         r = make_plan(c, cc, cww, cplan);
         if (!r) r = batch_pass(c, cplan, params);
         if (r) return r;
     }
-    for (int p = 0; p < n; ++p) {
-        int r = net_coarse_finish(pc[p], params[p].depth_min, params[p].depth_max);
-        if (!r) r = net_full_setup(pc[p], net, prior_mode);
-        if (r) return ctx_fail(c, r, "batched prior-net form, problem %d: %s", p, hpm_last_error(pc[p]));
-    }
+    r = for_each_problem(
+        n,
+        [&](int p) {
+            int q = net_coarse_finish(pc[p], params[p].depth_min, params[p].depth_max);
+            return q ? q : net_full_setup(pc[p], net, prior_mode);
+        },
+        &bad);
+    if (r) return ctx_fail(c, r, "batched prior-net form, problem %d: %s", bad, hpm_last_error(pc[bad]));
     std::vector<HpmParams> fp(params);
     for (int e = 0; e <= extra_passes; ++e) {
+        r = for_each_problem(
+            n,
+            [&](int p) {
+                hpm_ctx *b = pc[p];
+                if (e > 0) {
+                    const size_t np = (size_t)b->cams[0].width * b->cams[0].height;
+                    const cudaError_t ce = flow_split_state(reinterpret_cast<const float4 *>(ctx_planes(b)), (int)np,
+                                                            b->flow.full_depth, b->flow.full_normal, b->stream);
+                    if (ce != cudaSuccess) return ctx_cuda_fail(b, ce, "split");
+                    const int q = flow_prior_from_maps(b, 2, ctx_costs(b), params[p].depth_min, params[p].depth_max);
+                    if (q) return q;
+                }
+                const cudaError_t ce = cudaStreamSynchronize(b->stream);
+                return ce == cudaSuccess ? HPM_OK : ctx_cuda_fail(b, ce, "prior-net set-up");
+            },
+            &bad);
+        if (r) return ctx_fail(c, r, "batched prior-net form, problem %d: %s", bad, hpm_last_error(pc[bad]));
         for (int p = 0; p < n; ++p) {
-            hpm_ctx *b = pc[p];
-            if (e > 0) {
-                const size_t np = (size_t)b->cams[0].width * b->cams[0].height;
-                CK(flow_split_state(reinterpret_cast<const float4 *>(ctx_planes(b)), (int)np, b->flow.full_depth,
-                                    b->flow.full_normal, b->stream),
-                   "split");
-                const int r = flow_prior_from_maps(b, 2, ctx_costs(b), params[p].depth_min, params[p].depth_max);
-                if (r) return ctx_fail(c, r, "batched prior-net form, problem %d: %s", p, hpm_last_error(b));
-            }
-            CK(cudaStreamSynchronize(b->stream), "prior-net set-up");
             fp[p].planar_prior = 1;
             fp[p].seed = net_pass_seed(params[p].seed, e);
         }
-        const int r = batch_pass(c, all, fp, half_steps);
+        r = batch_pass(c, all, fp, half_steps);
         if (r) return r;
     }
     for (int p = 0; p < n; ++p) {
         pc[p]->proposals = nullptr;
-        const int r = net_status(pc[p]);
+        r = net_status(pc[p]);
         if (r) return ctx_fail(c, r, "batched prior-net form, problem %d: %s", p, hpm_last_error(pc[p]));
     }
     return HPM_OK;
@@ -361,23 +405,35 @@ int batched_scene(hpm_ctx *c, int n_views, const float *const *images, const Hpm
         const int kmax = *std::max_element(levels.begin(), levels.end());
         for (int round = 0; round <= kmax; ++round) {
             const int level = 2 - kmax + round; /* 0: 1/4 scale, 1: 1/2, 2: full */
+            std::vector<int> in; /* the problems whose pyramid reaches this level */
+            for (int p = 0; p < n_problems; ++p)
+                if (level >= 2 - levels[p]) in.push_back(p);
+            int bad = 0;
+            r = for_each_problem(
+                (int)in.size(),
+                [&](int i) {
+                    const int p = in[i];
+                    hpm_ctx *b = pc[p];
+                    const size_t np = (size_t)b->cams[0].width * b->cams[0].height;
+                    cudaError_t ce = ws_reserve_full(b, np);
+                    if (ce == cudaSuccess)
+                        ce = flow_split_state(reinterpret_cast<const float4 *>(ctx_planes(b)), (int)np,
+                                              b->flow.full_depth, b->flow.full_normal, b->stream);
+                    if (ce != cudaSuccess) return ctx_cuda_fail(b, ce, "prior level");
+                    const int q = flow_prior_from_maps(b, level, ctx_costs(b), params[p].depth_min, params[p].depth_max);
+                    if (q) return q;
+                    ce = cudaStreamSynchronize(b->stream);
+                    return ce == cudaSuccess ? HPM_OK : ctx_cuda_fail(b, ce, "prior level");
+                },
+                &bad);
+            if (r) return ctx_fail(c, r, "hpm_run_scene_batched, problem %d: %s", in[bad], hpm_last_error(pc[in[bad]]));
             std::vector<hpm_ctx *> sub;
             std::vector<HpmParams> sp;
             std::vector<int> sw;
-            for (int p = 0; p < n_problems; ++p) {
-                if (level < 2 - levels[p]) continue;
-                hpm_ctx *b = pc[p];
-                const size_t np = (size_t)b->cams[0].width * b->cams[0].height;
-                CK(ws_reserve_full(b, np), "flow workspace");
-                CK(flow_split_state(reinterpret_cast<const float4 *>(ctx_planes(b)), (int)np, b->flow.full_depth,
-                                    b->flow.full_normal, b->stream),
-                   "split");
-                r = flow_prior_from_maps(b, level, ctx_costs(b), params[p].depth_min, params[p].depth_max);
-                if (r) return ctx_fail(c, r, "hpm_run_scene_batched, problem %d: %s", p, hpm_last_error(b));
-                CK(cudaStreamSynchronize(b->stream), "prior");
+            for (int p : in) {
                 HpmParams q = params[p];
                 q.planar_prior = 1;
-                sub.push_back(b);
+                sub.push_back(pc[p]);
                 sp.push_back(q);
                 sw.push_back(ww[p]);
             }
