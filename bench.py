@@ -104,6 +104,10 @@ def parse_args():
     ap.add_argument("--pass-case", action="store_true",
                     help="kernel-capture case: plain PatchMatch passes of one view of the scene (1 warm-up, then "
                          "--steps passes); prints the half-step time instead of the bench line")
+    ap.add_argument("--flow-case", action="store_true",
+                    help="kernel-capture case of the problem flow: ProcessProblem of one view of the scene with its "
+                         "prior pyramid (initialisation, prior kernels, JBU, filter), then the fusion of the "
+                         "scene's ground-truth maps; prints their wall times")
     ap.add_argument("--net-case", action="store_true",
                     help="kernel-capture case of the network's tensor-core convolutions: --steps training steps "
                          "(forward, data and weight gradients, Adam) on a 400x300 input; prints their time")
@@ -664,6 +668,35 @@ def run_pass_case(args):
             "px_relerr_lt_1pct": float(syn.depth_accuracy(planes[..., 3], sc.gt_depth[ref]))}
 
 
+def run_flow_case(args):
+    """hpm_process_problem of reference view n/2 of the bench scene (plain
+    pass, then the prior passes of every pyramid level), then hpm_fuse of
+    the scene's ground-truth depth and normal maps, for ncu captures of
+    k_init, k_support_blocks, k_tri_planes, k_tri_raster, k_knn_prior,
+    k_prior_coarse, k_jbu, k_filter and k_fuse_pairs."""
+    import hpm_b200 as hb
+
+    sc, images, pairs = make_scene(0)
+    ref = WORKLOAD["n_views"] // 2
+    ids = [ref] + pairs[ref][1]
+    out = {"case": f"ProcessProblem of view {ref} ({WORKLOAD['width']}x{WORKLOAD['height']}, {len(ids) - 1} "
+                   f"sources, {WORKLOAD['pyramid_levels'] + 1}-level prior pyramid), then fusion of "
+                   f"{WORKLOAD['n_views']} views"}
+    with hb.Context() as ctx:
+        ctx.set_views([images[i] for i in ids], sc.cams[ids])
+        t0 = time.perf_counter()
+        d, _, _, _ = ctx.process_problem(seed=1, pyramid_levels=WORKLOAD["pyramid_levels"])
+        out["process_problem_ms"] = (time.perf_counter() - t0) * 1e3
+    depths = [g.astype(np.float32) for g in sc.gt_depth]
+    normals = [g.astype(np.float32) for g in sc.gt_normal]
+    colors = [np.repeat(g[..., None], 3, -1) for g in sc.images]
+    t0 = time.perf_counter()
+    xyz, _, _ = hb.fuse(sc.cams, depths, normals, colors, pairs)
+    out["fuse_ms"] = (time.perf_counter() - t0) * 1e3
+    out["points"] = int(len(xyz))
+    return out
+
+
 def run_net_case(args):
     """Training steps of the proposal network on one 400x300 input (the
     coarse size of a 1600x1200 view), for ncu captures of k_conv3x3 and
@@ -825,6 +858,10 @@ def main():
         if args.pass_case:
             if dist.rank == 0:
                 print(json.dumps(run_pass_case(args)), flush=True)
+            return
+        if args.flow_case:
+            if dist.rank == 0:
+                print(json.dumps(run_flow_case(args)), flush=True)
             return
         if args.net_case:
             if dist.rank == 0:
