@@ -61,10 +61,10 @@ BATCHED = dict(width=1920, height=1080, n_views=24, n_planes=20, n_spheres=5, lo
                sizes=[(1920, 1080)] * 8 + [(1600, 1200)] * 8 + [(960, 540)] * 8,
                name="batched scene")
 
-# DRAM traffic of one half-step (k_prop_dirs + k_prop_refine), from an ncu
-# capture of `bench.py --pass-case` (1600x1200, 10 sources), per pixel: the
-# hand-off buffers grow with the pixel count
-TRAFFIC_BYTES_PER_PX_HALF_STEP = (847.3 + 750.8 + 1805.0 + 623.2) * 1e6 / (1600 * 1200)
+# DRAM traffic of one half-step (k_prop_dirs + k_prop_refine: read + write),
+# from an ncu capture of `bench.py --pass-case` (1600x1200, 10 sources), per
+# pixel: the hand-off buffers grow with the pixel count
+TRAFFIC_BYTES_PER_PX_HALF_STEP = (154.02 + 323.62 + 797.47 + 388.49) * 1e6 / (1600 * 1200)
 GEOM_TERM_FLOPS = 120  # two projections (world point + camera, 3x3 each) and the reprojection distance
 TAPS, NCC_FLOPS_PER_TAP, FLOPS_PER_HYP_VIEW = 36, 34, 80
 

@@ -88,6 +88,16 @@ def _offenders(over, got, ref, bound, exact, extra):
     return "; ".join(rows)
 
 
+def check_exact(got, exact, acc, what):
+    """An FP32 evaluation against the float64 NCC of its own samples: within
+    1e-4 max(1, |exact|) + MARGIN * acc / 2 everywhere (acc bounds the gap
+    between two FP32 evaluations, half of it one evaluation's error)."""
+    got, exact = np.asarray(got, np.float64), np.asarray(exact, np.float64)
+    d = np.abs(got - exact)
+    over = d > 1e-4 * np.maximum(1.0, np.abs(exact)) + MARGIN * 0.5 * np.asarray(acc, np.float64)
+    assert not over.any(), f"{what}: {int(over.sum())} values off the exact NCC of their samples, worst {d.max():.3g}"
+
+
 def check_within_bound(got, ref, bound, what, exact=None, extra=None):
     """|got - ref| <= 1e-4 max(1, |ref|) + MARGIN * bound for every value,
     and <= 1e-4 max(1, |ref|) alone where the bound is below 1e-4 (well

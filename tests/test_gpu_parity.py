@@ -36,9 +36,11 @@ def ncc_ctx():
 
 
 def test_cost_vectors_vs_reference(ncc_ctx):
-    """Every window holds the reference's texture samples bit for bit; the
-    costs differ only by FP32 arithmetic on them, within the oracle's bound
-    of it (tests/ncc_split.py)."""
+    """Every window holds the samples the reference shim exports, bit for
+    bit, and its cost is the exact NCC of them within the FP32 arithmetic
+    bound; against the reference's own kernel, which can round a tap next to
+    a 1/256 texture-weight step the other way, within the bound that also
+    covers such taps (tests/ncc_split.py, tests/test_gpu_parity_bench.py)."""
     ctx, n = ncc_ctx
     imgs = [i.astype(np.float32) for i in n["images"]]
     h, w = imgs[0].shape
@@ -53,8 +55,10 @@ def test_cost_vectors_vs_reference(ncc_ctx):
             np.testing.assert_array_equal(ig, ir)
             np.testing.assert_array_equal(sg[ig], sr[ir])
             exact = ncc_split.exact_costs(sg, ig, imgs[0], px).reshape(got.shape)
-        ncc_split.check_within_bound(got, n["cost_vectors"][k], acc, f"field {k}", exact=exact,
-                                     extra={"acc": acc, "kind": kind, "oracle": ocost})
+            ncc_split.check_exact(got, exact, acc, f"field {k} vs its samples")
+        frac = ncc_split.check_within_bound(got, n["cost_vectors"][k], bound + acc, f"field {k}", exact=exact,
+                                            extra={"acc": acc, "kind": kind, "oracle": ocost})
+        assert frac >= 0.999, frac
 
 
 def test_initial_costs_vs_reference(ncc_ctx):
@@ -63,7 +67,10 @@ def test_initial_costs_vs_reference(ncc_ctx):
         c, v = ctx.initial_costs(p)
         _, bound, acc, _ = _bounds(n, p)
         ref = n["init_cost"][k].astype(np.float64)
-        tol = 1e-4 * np.maximum(1.0, np.abs(ref)) + ncc_split.MARGIN * acc.max(-1)
+        # a tap of one view crossing a weight step moves that view's cost by
+        # at most its bound, and the initial cost (mean of the best views) by
+        # no more than the largest
+        tol = 1e-4 * np.maximum(1.0, np.abs(ref)) + ncc_split.MARGIN * (bound + acc).max(-1)
         assert (np.abs(c - ref) <= tol).all()
         assert (v == n["init_views"][k]).mean() >= 0.99
 

@@ -6,17 +6,23 @@ The reference's outputs come from its own HPM.cu kernels on a B200
 (tests/golden/make_golden.py, --only bench), kept at 4096 sampled pixels;
 the scenes and inputs are rebuilt from their seeds here.
 
-NCC tolerance.  The product's and the reference's texture samples must be
-identical (hpm_tap_samples against the reference shim's): no tap may round
-differently.  The costs then differ only by FP32 arithmetic on the same
-samples (the bilateral weights' exp and the window sums, whose variances
-cancel in flat windows), bounded by the oracle's error analysis
-(or_ncc_bounds, acc).  Against the oracle, whose tap coordinates round on
-their own, the bound adds the first-order effect of the taps whose
-coordinates lie within TWICE their propagated rounding-error bound of a
-1/256 weight step.  ncc_split.check_within_bound applies it (with a 25 %
-margin for second-order terms) and holds well-conditioned values (bound
-below 1e-4) to 1e-4 with no exceptions.
+NCC tolerance.  The product's texture samples equal the ones the reference
+shim exports for the same windows (hpm_tap_samples against
+hpm_ref_tap_samples, bit for bit), and the product's cost equals the float64
+NCC of those samples within the oracle's bound of FP32 arithmetic on them
+(or_ncc_bounds, acc: the bilateral weights' exp and the window sums, whose
+variances cancel in flat windows).  The reference's NCC kernel computes its
+tap coordinates in its own compiled code, which can round a coordinate lying
+within a few ulps of a 1/256 texture-weight step to the other side: measured
+at 800x600, 15 of the 40,960 values of one field, where the reference moves
+by up to 1.4e-3 from the exact NCC of the exported samples while the product
+stays within 5e-6 of it.  Against the reference (as against the oracle, whose coordinates
+round on their own) the bound therefore adds the first-order effect of the
+taps whose coordinates lie within TWICE their propagated rounding-error bound
+of such a step (bound).  ncc_split.check_within_bound applies it with a 25 %
+margin for second-order terms and holds well-conditioned values (bound below
+1e-4) to 1e-4 with no exceptions; at least 99.9 % of all values must agree
+to 1e-4.
 """
 import hashlib
 import os
@@ -60,9 +66,10 @@ def _sample(a, px):
 
 
 def test_cost_vectors_vs_reference_and_oracle(case):
-    """Same texture samples as the reference's kernels, costs within the
-    FP32 arithmetic bound; against the oracle within the bound that also
-    covers taps crossing a weight step."""
+    """The exported samples of the reference shim, costs within the FP32
+    arithmetic bound of the exact NCC of those samples; against the
+    reference's kernels and the oracle within the bound that also covers
+    taps crossing a weight step."""
     name, g, c, ctx = case
     px = c["pixels"]
     for k, p in enumerate(c["planes"]):
@@ -75,9 +82,11 @@ def test_cost_vectors_vs_reference_and_oracle(case):
             np.testing.assert_array_equal(ig, ir)
             np.testing.assert_array_equal(sg[ig], sr[ir])
             exact = ncc_split.exact_costs(sg, ig, c["imgs"][0], px)
+            ncc_split.check_exact(got, exact, acc, f"{name} field {k} vs its samples")
         ref = g["cost_vectors"][k]
-        ncc_split.check_within_bound(got, ref, acc, f"{name} field {k} vs reference", exact=exact,
-                                     extra={"acc": acc, "kind": kind, "oracle": ocost})
+        frac = ncc_split.check_within_bound(got, ref, bound + acc, f"{name} field {k} vs reference", exact=exact,
+                                            extra={"acc": acc, "kind": kind, "oracle": ocost})
+        assert frac >= 0.999, frac
         ncc_split.check_within_bound(got, ocost, bound + acc, f"{name} field {k} vs oracle")
         ncc_split.check_within_bound(ocost, ref, bound + acc, f"{name} field {k} oracle vs reference")
 
