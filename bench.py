@@ -411,6 +411,7 @@ def net_schedule(device):
     get = lambda k, d: int(meta[k]) if k in meta else d  # noqa: E731
     sched = {"pyramid_levels": get("extra_passes", 0), "geom_iterations": get("geom_iterations", 2),
              "planar_prior": get("prior", 1), "iterations": get("iterations", 3)}
+    sched["geom_pass_iterations"] = get("geom_pass_iterations", sched["iterations"])
     return net, sched
 
 
@@ -477,8 +478,9 @@ def run_ours(args, dist):
                     "the coarse planar prior and the BF16 network's plane proposal; then "
                     f"{1 + sc_['pyramid_levels']} full-scale pass(es) with the proposal as initial hypothesis and "
                     f"as a refinement candidate, then {sc_['geom_iterations']} geometric iteration(s); "
-                    f"{sc_['iterations']} PatchMatch iterations per full-scale pass; every pass of all problems "
-                    "one CUDA graph")
+                    f"{sc_['iterations']} PatchMatch iterations per full-scale prior pass, "
+                    f"{sc_['geom_pass_iterations']} per geometric pass; every pass of all problems one CUDA "
+                    "graph")
         net_out = form_summary(net) | {
             "schedule": sc_, "step": net_step, "speedup_vs_plain": plain["ms_per_step"] / net["ms_per_step"],
             "e2e_speedup_vs_plain": plain["e2e"]["ms_per_step"] / net["e2e"]["ms_per_step"],

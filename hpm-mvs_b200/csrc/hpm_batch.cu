@@ -324,9 +324,10 @@ int batched_scene(hpm_ctx *c, int n_views, const float *const *images, const Hpm
     int r = ctx_select_device(c);
     if (r) return r;
     const Range range(net ? "batched scene %d views (prior-net form)" : "batched scene %d views", n_views);
-    if (o->iterations < 0 || o->iterations > 64)
+    if (o->iterations < 0 || o->iterations > 64 || o->geom_pass_iterations < 0 || o->geom_pass_iterations > 64)
         return ctx_fail(c, HPM_ERR_ARG, "hpm_run_scene_batched: iterations outside [0, 64]");
     const int half_steps = net && o->iterations > 0 ? 2 * o->iterations : 6;
+    const int geom_half_steps = net && o->geom_pass_iterations > 0 ? 2 * o->geom_pass_iterations : half_steps;
     cudaStream_t s = c->stream;
     /* per view: image, pass-A depth, two geometric depth buffers, normal (3), cost */
     std::vector<float *> img(n_views), dep_a(n_views), dep_g0(n_views), dep_g1(n_views), nrm(n_views), cst(n_views);
@@ -478,7 +479,7 @@ int batched_scene(hpm_ctx *c, int n_views, const float *const *images, const Hpm
             gp[p].seed = o->seed + 1000003ull * (gi + 1) + (uint64_t)p;
         }
         CK(cudaStreamSynchronize(s), "geometric set-up");
-        r = batch_pass(c, all, gp, half_steps);
+        r = batch_pass(c, all, gp, geom_half_steps);
         if (r) return r;
         for (int p = 0; p < n_problems; ++p) {
             const int ref = ref_ids[p];

@@ -384,9 +384,10 @@ static int run_scene_impl(hpm_ctx *c, int n_views, const float *const *images, c
     int r = ctx_select_device(c);
     if (r) return r;
     const Range range(net ? "scene %d views (prior-net form)" : "scene %d views", n_views);
-    if (o->iterations < 0 || o->iterations > 64)
+    if (o->iterations < 0 || o->iterations > 64 || o->geom_pass_iterations < 0 || o->geom_pass_iterations > 64)
         return ctx_fail(c, HPM_ERR_ARG, "hpm_run_scene: iterations outside [0, 64]");
     const int half_steps = net && o->iterations > 0 ? 2 * o->iterations : 6;
+    const int geom_half_steps = net && o->geom_pass_iterations > 0 ? 2 * o->geom_pass_iterations : half_steps;
     cudaStream_t s = c->stream;
     SceneMaps m;
     size_t total = 0; /* floats: image, pass-A depth, geometric depth, normal (3), cost */
@@ -511,7 +512,7 @@ static int run_scene_impl(hpm_ctx *c, int n_views, const float *const *images, c
             HpmProblemOpts po = {0, 1, gi >= 1, o->seed + 1000003ull * (gi + 1) + (uint64_t)p, o->pyramid_levels,
                                  o->fix_quirks};
             /* the geometric depth map is rewritten view by view (depths_geom.dmb) */
-            r = process_problem(c, &po, net ? half_steps : 6, m.depth_g[ref], m.normal[ref], m.cost[ref], nullptr);
+            r = process_problem(c, &po, geom_half_steps, m.depth_g[ref], m.normal[ref], m.cost[ref], nullptr);
             if (r) return r;
         }
     }

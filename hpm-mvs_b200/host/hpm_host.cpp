@@ -625,7 +625,8 @@ void RunScene(const std::string &dense_folder, const std::vector<Problem> &probl
         hpm_ctx *c;
         ~Destroy() { hpm_destroy(c); }
     } destroy{ctx};
-    const HpmSceneOpts o = {planar_prior ? 1 : 0, geom_iterations, seed, pyramid_levels, 0, reference_compat ? 0 : 1};
+    const HpmSceneOpts o = {planar_prior ? 1 : 0, geom_iterations, seed, pyramid_levels, 0, reference_compat ? 0 : 1,
+                            0};
     rc = hpm_run_scene_ex(ctx, (int)n, img_ptr.data(), cams.data(), (int)np, refs.data(), counts.data(), srcs.data(),
                           &o, pd.data(), pn.data(), pc.data(), pp.data(), pr.data());
     if (rc != HPM_OK) throw Error(rc, std::string("hpm_run_scene_ex: ") + hpm_last_error(ctx));

@@ -47,7 +47,8 @@ EXPORTED = [
 
 class HpmSceneOpts(ctypes.Structure):
     _fields_ = [("planar_prior", ctypes.c_int), ("geom_iterations", ctypes.c_int), ("seed", ctypes.c_uint64),
-                ("pyramid_levels", ctypes.c_int), ("iterations", ctypes.c_int), ("fix_quirks", ctypes.c_int)]
+                ("pyramid_levels", ctypes.c_int), ("iterations", ctypes.c_int), ("fix_quirks", ctypes.c_int),
+                ("geom_pass_iterations", ctypes.c_int)]
 
 
 class HpmNetWeights(ctypes.Structure):
@@ -245,7 +246,7 @@ class Context:
 
     def run_scene(self, images, cams, pairs, *, planar_prior=True, geom_iterations=2, seed=0, pyramid_levels=-1,
                   images_are_device=False, outputs=True, extra_maps=False, net=None, batched=False, iterations=0,
-                  fix_quirks=False):
+                  fix_quirks=False, geom_pass_iterations=0):
         """The reference's main() over a scene.  images: per-view float32 [H, W]
         arrays, or device pointers (ints) with images_are_device; pairs:
         [(ref, [sources])].  outputs: True to return new per-view (depth,
@@ -257,7 +258,8 @@ class Context:
         form (hpm_run_scene_net) instead of the plain form.  batched: the
         batched form (hpm_run_scene_batched; with net, the batched prior-net
         form, hpm_run_scene_batched_net).  iterations: with net, PatchMatch
-        iterations of each full-scale pass (0: the reference's 3).  fix_quirks:
+        iterations of each full-scale pass (0: the reference's 3), and
+        geom_pass_iterations of each geometric pass (0: as iterations).  fix_quirks:
         HpmSceneOpts.fix_quirks (False keeps the reference's behaviour)."""
         n = len(cams)
         cams = np.ascontiguousarray(cams, dtype=CAMERA_DTYPE)
@@ -274,7 +276,7 @@ class Context:
         for i, (_, s) in enumerate(pairs):
             srcs[i, :len(s)] = s
         o = HpmSceneOpts(int(planar_prior), int(geom_iterations), int(seed), int(pyramid_levels), int(iterations),
-                         int(fix_quirks))
+                         int(fix_quirks), int(geom_pass_iterations))
         outs = None
         if isinstance(outputs, (tuple, list)):
             outs = list(zip(*outputs))

@@ -212,12 +212,17 @@ def view_samples(ctx, images, cams, pairs, depths, normals, seed):
 
 
 def train(samples, net: Net, steps=1500, batch=8, lr=1e-3, lam=0.5, seed=0, log=None):
-    """Adam over random batches of views; returns the loss curve (mean loss
-    per valid pixel, per step)."""
+    """Adam over random batches of views, the learning rate decaying from lr
+    to lr / 100 along a half cosine (so that the last weights are not one
+    noisy step of a constant rate); returns the loss curve (mean loss per
+    valid pixel, per step)."""
+    import math
+
     rng = np.random.default_rng(seed)
     tr = Trainer(net, lr=lr, lam=lam)
     curve = []
     for step in range(steps):
+        tr.lr = lr * (0.01 + 0.99 * 0.5 * (1.0 + math.cos(math.pi * step / max(1, steps - 1))))
         idx = rng.choice(len(samples), size=min(batch, len(samples)), replace=False)
         count = sum(samples[i]["valid"] for i in idx)
         if count == 0:
@@ -296,12 +301,16 @@ def _accuracy(sc, depths, normals):
 
 
 def parse_schedule(text: str):
-    """"extra:geom[:prior[:iterations]]" -> (extra, geom, prior, iterations);
-    prior defaults to 1 (the coarse triangulation), iterations to 3."""
+    """"extra:geom[:prior[:iterations[:geom_pass_iterations]]]" -> the five
+    values; prior defaults to 1 (the coarse triangulation), iterations to 3,
+    geom_pass_iterations to iterations."""
     v = [int(x) for x in text.split(":")]
-    if not 2 <= len(v) <= 4:
-        raise ValueError(f"schedule {text!r}: extra:geom[:prior[:iterations]]")
-    return tuple(v + [1, 3][len(v) - 2:])
+    if not 2 <= len(v) <= 5:
+        raise ValueError(f"schedule {text!r}: extra:geom[:prior[:iterations[:geom_pass_iterations]]]")
+    v += [None, None, 1, 3, None][len(v):]
+    if v[4] is None:
+        v[4] = v[3]
+    return tuple(v)
 
 
 def main():
@@ -316,10 +325,11 @@ def main():
     ap.add_argument("--steps", type=int, default=1500)
     ap.add_argument("--batch", type=int, default=8)
     ap.add_argument("--lr", type=float, default=1e-3)
-    ap.add_argument("--schedules", default="0:2:1:3,0:1:1:3,0:1:2:3,0:1:1:2,0:1:2:2,1:1:1:2,0:2:1:2,0:1:1:1",
+    ap.add_argument("--schedules", default="0:2:2:3,0:2:2:3:2,0:2:2:2,1:2:2:2:1,0:1:2:3,0:2:2:2:1",
                     help="prior-net schedules to evaluate, extra full-scale prior passes:geometric iterations:"
                          "planar prior of the first full-scale pass (1 the coarse triangulation, 2 the proposal):"
-                         "PatchMatch iterations per full-scale pass")
+                         "PatchMatch iterations per full-scale pass:PatchMatch iterations per geometric pass "
+                         "(default: as the full-scale passes)")
     ap.add_argument("--batched", action="store_true", help="evaluate the batched forms (plain and prior-net)")
     ap.add_argument("--weights", default=None,
                     help="evaluate the schedules with these weights instead of generating data and training")
@@ -376,9 +386,10 @@ def main():
             row = {"seed": sc["seed"]}
             ev = []
             for form, kw in [("plain", dict(geom_iterations=2, batched=args.batched))] + [
-                    (f"net_e{e}_g{g}_p{m}_i{i}", dict(pyramid_levels=e, geom_iterations=g, planar_prior=m,
-                                                      iterations=i, net=net.weights(), batched=args.batched))
-                    for e, g, m, i in schedules]:
+                    (f"net_e{e}_g{g}_p{m}_i{i}_j{j}", dict(pyramid_levels=e, geom_iterations=g, planar_prior=m,
+                                                           iterations=i, geom_pass_iterations=j, net=net.weights(),
+                                                           batched=args.batched))
+                    for e, g, m, i, j in schedules]:
                 ctx.run_scene(sc["images"], sc["cams"], sc["pairs"], seed=sc["seed"], **kw)  # warm-up
                 torch.cuda.synchronize()
                 t0 = time.time()
@@ -394,23 +405,24 @@ def main():
             rows.append(row)
             log(json.dumps(row))
         summary["eval"] = rows
-        forms = ["plain"] + [f"net_e{e}_g{g}_p{m}_i{i}" for e, g, m, i in schedules]
+        forms = ["plain"] + [f"net_e{e}_g{g}_p{m}_i{i}_j{j}" for e, g, m, i, j in schedules]
         for form in forms:
             summary[f"eval_{form}"] = {k: float(np.mean([r[form][k] for r in rows]))
                                        for k in ("mpix_per_s", "px_relerr_lt_1pct", "median_normal_err_deg")}
         # the schedule the scene driver uses: the fastest whose accuracy is
         # within 0.5 pp of the plain form's, else the most accurate
         plain_acc = summary["eval_plain"]["px_relerr_lt_1pct"]
-        ev = lambda e, g, m, i: summary[f"eval_net_e{e}_g{g}_p{m}_i{i}"]  # noqa: E731
+        ev = lambda e, g, m, i, j: summary[f"eval_net_e{e}_g{g}_p{m}_i{i}_j{j}"]  # noqa: E731
         ok = [(ev(*t)["mpix_per_s"], t) for t in schedules if ev(*t)["px_relerr_lt_1pct"] >= plain_acc - 0.005]
         if ok:
-            _, (e, g, m, i) = max(ok)
+            _, (e, g, m, i, j) = max(ok)
         else:
-            _, (e, g, m, i) = max((ev(*t)["px_relerr_lt_1pct"], t) for t in schedules)
-        summary["chosen_schedule"] = {"extra_passes": e, "geom_iterations": g, "prior": m, "iterations": i}
+            _, (e, g, m, i, j) = max((ev(*t)["px_relerr_lt_1pct"], t) for t in schedules)
+        summary["chosen_schedule"] = {"extra_passes": e, "geom_iterations": g, "prior": m, "iterations": i,
+                                      "geom_pass_iterations": j}
         net.save(os.path.join(args.out, "priornet_weights.npz"), loss=np.array(curve, np.float32),
-                 extra_passes=e, geom_iterations=g, prior=m, iterations=i, train_scenes=args.scenes,
-                 steps=args.steps)
+                 extra_passes=e, geom_iterations=g, prior=m, iterations=i, geom_pass_iterations=j,
+                 train_scenes=args.scenes, steps=args.steps)
     with open(os.path.join(args.out, "priornet_summary.json"), "w") as f:
         json.dump(summary, f, indent=1)
     print(json.dumps({k: v for k, v in summary.items() if k != "eval"}))

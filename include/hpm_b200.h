@@ -176,6 +176,8 @@ typedef struct {
     int iterations;     /* prior-net forms only: PatchMatch iterations of each full-scale pass, the geometric
                            ones included (0 = 3, the reference's count; the plain form always runs 3) */
     int fix_quirks;     /* HpmProblemOpts.fix_quirks of every problem (0 = the reference's behaviour) */
+    int geom_pass_iterations; /* prior-net forms only: PatchMatch iterations of each geometric pass
+                                 (0 = as `iterations`) */
 } HpmSceneOpts;
 
 /* The reference's main() (main.cpp:636-677) over a scene: ProcessProblem
