@@ -538,7 +538,7 @@ long long RunFusion(const std::string &dense_folder, const std::vector<Problem> 
     return count;
 }
 
-void ProcessProblem(const std::string &dense_folder, const Problem &problem, bool geom_consistency,
+long long ProcessProblem(const std::string &dense_folder, const Problem &problem, bool geom_consistency,
                     bool planar_prior, bool multi_geometry, uint64_t seed, int pyramid_levels, int device,
                     bool reference_compat)
 {
@@ -571,9 +571,10 @@ void ProcessProblem(const std::string &dense_folder, const Problem &problem, boo
     write_dmb(folder + "/costs.dmb", costs, w, h, 1);
     std::cout << "Processing image " << std::setw(8) << std::setfill('0') << problem.ref_image_id << " done!"
               << std::endl;
+    return (long long)n;
 }
 
-void RunScene(const std::string &dense_folder, const std::vector<Problem> &problems, bool planar_prior,
+long long RunScene(const std::string &dense_folder, const std::vector<Problem> &problems, bool planar_prior,
               int geom_iterations, uint64_t seed, int pyramid_levels, int device, bool reference_compat)
 {
     /* every view a problem names, numbered in order of appearance */
@@ -645,6 +646,9 @@ void RunScene(const std::string &dense_folder, const std::vector<Problem> &probl
         write_dmb(folder + "/costs.dmb", cost[v], w, h, 1);
     });
     std::cout << "Processed " << np << " problems (" << n << " views) in one scene run" << std::endl;
+    long long px = 0;
+    for (size_t p = 0; p < np; ++p) px += (long long)cams[refs[p]].width * cams[refs[p]].height;
+    return px;
 }
 
 Progress::Progress(const std::string &dense_folder, const std::string &settings, bool resume)

@@ -129,8 +129,8 @@ long long RunFusion(const std::string &dense_folder, const std::vector<Problem> 
                     int device = 0);
 
 /* ProcessProblem (main.cpp:35-499): one reference view, outputs written
- * under dense_folder/HPM/2333_%08d/. */
-void ProcessProblem(const std::string &dense_folder, const Problem &problem, bool geom_consistency,
+ * under dense_folder/HPM/2333_%08d/; returns the depth pixels written. */
+long long ProcessProblem(const std::string &dense_folder, const Problem &problem, bool geom_consistency,
                     bool planar_prior, bool multi_geometry = false, uint64_t seed = 0, int pyramid_levels = -1,
                     int device = 0, bool reference_compat = true);
 
@@ -140,8 +140,9 @@ void ProcessProblem(const std::string &dense_folder, const Problem &problem, boo
  * every problem, the files the per-problem loop leaves (depths.dmb,
  * depths_prior.dmb, depths_geom.dmb, normals.dmb, costs.dmb).  Seeds as in
  * that loop (S + p, S + 1000003 (g + 1) + p), hence the same files.  Host
- * memory: about 20 bytes per pixel of each reference view, plus the images. */
-void RunScene(const std::string &dense_folder, const std::vector<Problem> &problems, bool planar_prior,
+ * memory: about 20 bytes per pixel of each reference view, plus the images.
+ * Returns the depth pixels of all reference views. */
+long long RunScene(const std::string &dense_folder, const std::vector<Problem> &problems, bool planar_prior,
               int geom_iterations, uint64_t seed, int pyramid_levels, int device, bool reference_compat = true);
 
 /* What main() has finished in a dense folder, so that a run can stop and be

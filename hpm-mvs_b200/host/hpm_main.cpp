@@ -6,7 +6,7 @@
  *
  *   hpm_mvs dense_folder [--seed S] [--levels K] [--device D] [--no-prior]
  *                        [--geom-iterations G] [--no-fusion] [--per-problem]
- *                        [--resume] [--stop-after N] [--no-reference-compat]
+ *                        [--resume] [--stop-after N] [--no-reference-compat] [--log PATH]
  *
  * By default the passes run as one scene (RunScene: maps in device memory
  * between passes, pass set A on two host threads, files written at the
@@ -23,11 +23,17 @@
  * a scene can be computed in several runs.  Both forms resume to the files
  * one uninterrupted run writes.
  *
+ * --log PATH appends one JSON line per finished step to PATH: the step, its
+ * wall time, and the depth pixels it wrote with their rate (for the fusion,
+ * the points).
+ *
  * The reference's behaviour is kept throughout by default (its quirks
  * included); --no-reference-compat fixes the quirks listed at HpmParams in
  * hpm_b200.h.
  */
+#include <chrono>
 #include <cstdlib>
+#include <fstream>
 #include <cstring>
 #include <iostream>
 #include <sstream>
@@ -41,7 +47,7 @@ int main(int argc, char **argv)
     if (argc < 2 || !strcmp(argv[1], "-h") || !strcmp(argv[1], "--help")) {
         std::cout << "USAGE: hpm_mvs dense_folder [--seed S] [--levels K] [--device D] [--no-prior] "
                      "[--geom-iterations G] [--no-fusion] [--per-problem] [--resume] [--stop-after N] "
-                     "[--no-reference-compat]"
+                     "[--no-reference-compat] [--log PATH]"
                   << std::endl;
         return argc < 2 ? -1 : 0;
     }
@@ -50,6 +56,7 @@ int main(int argc, char **argv)
     int levels = -1, device = 0, geom_iterations = 2;
     bool planar_prior = true, fusion = true, per_problem = false, resume = false, compat = true;
     long long stop_after = -1;
+    std::string log_path;
     for (int i = 2; i < argc; ++i) {
         const std::string a = argv[i];
         auto next = [&](const char *name) -> const char * {
@@ -77,6 +84,8 @@ int main(int argc, char **argv)
             resume = true;
         else if (a == "--no-reference-compat")
             compat = false;
+        else if (a == "--log")
+            log_path = next("--log");
         else if (a == "--stop-after")
             stop_after = std::atoll(next("--stop-after"));
         else {
@@ -94,13 +103,27 @@ int main(int argc, char **argv)
                  << (compat ? "" : " fix_quirks=1");
         hpm_host::Progress progress(dense_folder, settings.str(), resume);
         long long steps = 0;
-        /* runs one step unless the log holds it; false once --stop-after is reached */
+        /* runs one step unless the log holds it; false once --stop-after is
+         * reached.  work() returns the depth pixels it wrote (the fusion: its
+         * points, as a negative number) */
         auto step = [&](const std::string &name, auto work) {
             if (progress.done(name)) return true;
             if (stop_after >= 0 && steps >= stop_after) return false;
-            work();
+            const auto t0 = std::chrono::steady_clock::now();
+            const long long out = work();
+            const double sec = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
             progress.mark(name);
             ++steps;
+            if (!log_path.empty()) {
+                std::ofstream log(log_path, std::ios::app);
+                log << "{\"step\": \"" << name << "\", \"seconds\": " << sec;
+                if (out >= 0)
+                    log << ", \"depth_pixels\": " << out << ", \"mpix_per_s\": " << (sec > 0 ? out / sec / 1e6 : 0.0);
+                else
+                    log << ", \"points\": " << -out;
+                log << "}\n";
+                if (!log) throw hpm_host::Error(HPM_ERR_IO, "cannot write " + log_path);
+            }
             return true;
         };
         auto stopped = [&]() {
@@ -109,22 +132,22 @@ int main(int argc, char **argv)
         };
         if (!per_problem) {
             if (!step("scene", [&] {
-                    hpm_host::RunScene(dense_folder, problems, planar_prior, geom_iterations, seed, levels, device,
-                                       compat);
+                    return hpm_host::RunScene(dense_folder, problems, planar_prior, geom_iterations, seed, levels,
+                                              device, compat);
                 }))
                 return stopped();
         } else {
             for (size_t p = 0; p < problems.size(); ++p)
                 if (!step("A " + std::to_string(problems[p].ref_image_id), [&] {
-                        hpm_host::ProcessProblem(dense_folder, problems[p], false, planar_prior, false, seed + p,
-                                                 levels, device, compat);
+                        return hpm_host::ProcessProblem(dense_folder, problems[p], false, planar_prior, false,
+                                                        seed + p, levels, device, compat);
                     }))
                     return stopped();
             for (int g = 0; g < geom_iterations; ++g)
                 for (size_t p = 0; p < problems.size(); ++p)
                     if (!step("G" + std::to_string(g) + " " + std::to_string(problems[p].ref_image_id), [&] {
-                            hpm_host::ProcessProblem(dense_folder, problems[p], true, false, g > 0,
-                                                     seed + 1000003ull * (g + 1) + p, levels, device, compat);
+                            return hpm_host::ProcessProblem(dense_folder, problems[p], true, false, g > 0,
+                                                            seed + 1000003ull * (g + 1) + p, levels, device, compat);
                         }))
                         return stopped();
         }
@@ -132,6 +155,7 @@ int main(int argc, char **argv)
             !step("fusion", [&] {
                 const long long n = hpm_host::RunFusion(dense_folder, problems, geom_iterations > 0, device);
                 std::cout << "Fused " << n << " points into " << dense_folder << "/HPM/HPM_model.ply" << std::endl;
+                return -n;
             }))
             return stopped();
     } catch (const hpm_host::Error &e) {

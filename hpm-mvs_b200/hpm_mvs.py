@@ -6,7 +6,7 @@ library to the bytes cv::imread gives (HPM.cpp:492, main.cpp:523).
     python hpm-mvs_b200/hpm_mvs.py dense_folder [--seed S] [--levels K]
                                    [--geom-iterations G] [--no-prior] [--device D]
                                    [--no-fusion] [--per-problem] [--resume] [--stop-after N]
-                                   [--no-reference-compat]
+                                   [--no-reference-compat] [--log PATH]
 
 Writes HPM/2333_%08d/{depths,depths_geom,normals,costs,depths_prior}.dmb like
 the reference's ProcessProblem, then fuses them into HPM/HPM_model.ply
@@ -20,8 +20,10 @@ skips the logged steps.
 from __future__ import annotations
 
 import argparse
+import json
 import os
 import sys
+import time
 
 import numpy as np
 
@@ -82,6 +84,7 @@ def process_problem(ctx, folder, ref, srcs, views, *, geom, planar_prior, multi_
     hb.write_dmb(os.path.join(out, "depths_geom.dmb" if geom else "depths.dmb"), d)
     hb.write_dmb(os.path.join(out, "normals.dmb"), n)
     hb.write_dmb(os.path.join(out, "costs.dmb"), c)
+    return int(d.size)
 
 
 def run_scene(ctx, folder, problems, needed, views, *, planar_prior, geom_iterations, seed, levels,
@@ -104,6 +107,7 @@ def run_scene(ctx, folder, problems, needed, views, *, planar_prior, geom_iterat
             hb.write_dmb(os.path.join(out, "depths_geom.dmb"), d[i])
         hb.write_dmb(os.path.join(out, "normals.dmb"), n[i])
         hb.write_dmb(os.path.join(out, "costs.dmb"), c[i])
+    return int(sum(d[index[ref]].size for ref, _ in problems))
 
 
 def run_fusion(folder, problems, geom_consistency, device=0):
@@ -194,6 +198,9 @@ def main(argv=None):
                     help="ProcessProblem problem by problem through .dmb files, as the reference runs")
     ap.add_argument("--resume", action="store_true", help="skip the steps HPM/progress.txt lists")
     ap.add_argument("--stop-after", type=int, default=-1, help="stop once this many steps have finished")
+    ap.add_argument("--log", default=None,
+                    help="append one JSON line per finished step: its wall time and the depth pixels (the fusion: "
+                         "points) it wrote")
     ap.add_argument("--no-reference-compat", action="store_true",
                     help="fix the reference's quirks listed at HpmParams in include/hpm_b200.h (default: keep the "
                          "reference's behaviour)")
@@ -208,13 +215,24 @@ def main(argv=None):
     count = [0]
 
     def step(name, work):
+        """work() returns the depth pixels it wrote (the fusion: -points)"""
         if progress.done(name):
             return
         if 0 <= a.stop_after <= count[0]:
             raise Stopped
-        work()
+        t0 = time.perf_counter()
+        out = work()
+        sec = time.perf_counter() - t0
         progress.mark(name)
         count[0] += 1
+        if a.log:
+            rec = {"step": name, "seconds": sec}
+            if out >= 0:
+                rec.update(depth_pixels=out, mpix_per_s=out / sec / 1e6 if sec > 0 else 0.0)
+            else:
+                rec["points"] = -out
+            with open(a.log, "a") as f:
+                f.write(json.dumps(rec) + "\n")
 
     state = {}
 
@@ -250,6 +268,7 @@ def main(argv=None):
             def fusion():
                 n = run_fusion(a.dense_folder, problems, a.geom_iterations > 0, a.device)
                 print(f"Fused {n} points into {a.dense_folder}/HPM/HPM_model.ply")
+                return -n
             step("fusion", fusion)
     except Stopped:
         print(f"Stopped after {count[0]} steps; --resume continues")

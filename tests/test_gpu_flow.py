@@ -262,7 +262,14 @@ def test_stopped_and_resumed_runs_write_the_files_of_one_run(tmp_path, front_end
         whole, chunked = str(tmp_path / f"whole{len(form)}"), str(tmp_path / f"chunked{len(form)}")
         syn.write_dense_folder(sc, whole)
         syn.write_dense_folder(sc, chunked)
-        run(whole, *form)
+        log = os.path.join(str(tmp_path), f"log{len(form)}_{front_end}.jsonl")
+        run(whole, *form, "--log", log)
+        import json
+
+        recs = [json.loads(ln) for ln in open(log)]
+        # one line per step: 4 + 2 x 4 problems and the fusion, or the scene and the fusion
+        assert [r["step"] for r in recs][-1] == "fusion" and len(recs) == (13 if form else 2)
+        assert all(r["depth_pixels"] > 0 and r["mpix_per_s"] > 0 for r in recs[:-1]) and recs[-1]["points"] > 0
         # per problem: 4 + 2 x 4 problem steps and the fusion, in chunks of 3; scene form: scene, fusion
         chunks = 0
         while True:

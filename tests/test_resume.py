@@ -54,3 +54,33 @@ def test_front_end_stops_before_any_work_and_refuses_other_settings(tmp_path, fr
     r = subprocess.run(exe + [f, "--seed", "4", "--per-problem", "--resume", "--stop-after", "0"], capture_output=True,
                        text=True, timeout=120)
     assert r.returncode == 0 and open(os.path.join(f, "HPM", "progress.txt")).read() == log
+
+
+@pytest.mark.parametrize("front_end", ["cpp", "py"])
+@pytest.mark.parametrize("fault", ["missing camera", "truncated camera", "truncated pair"])
+def test_front_end_reports_a_broken_dense_folder(tmp_path, front_end, fault):
+    """A missing or truncated input file ends the run with status 1 and a
+    message naming the file (the reference prints and carries on, or
+    dereferences NULL: HPM.cpp:273-304); the cameras are read before any
+    device work, so this runs without a GPU."""
+    exe = [os.path.join(PKG, "hpm_mvs")] if front_end == "cpp" else [sys.executable, os.path.join(PKG, "hpm_mvs.py")]
+    if front_end == "cpp" and not os.path.exists(exe[0]):
+        pytest.skip("make -C hpm-mvs_b200 builds hpm_mvs")
+    f = _folder(tmp_path, front_end)
+    cam = os.path.join(f, "cams", "00000001_cam.txt")
+    if fault == "missing camera":
+        os.remove(cam)
+        name = "00000001_cam.txt"
+    elif fault == "truncated camera":
+        with open(cam) as fh:
+            text = fh.read()
+        with open(cam, "w") as fh:
+            fh.write(text[: len(text) // 3])
+        name = "00000001_cam.txt"
+    else:
+        with open(os.path.join(f, "pair.txt"), "w") as fh:
+            fh.write("3\n0\n2 1")
+        name = "pair.txt"
+    r = subprocess.run(exe + [f, "--no-fusion"], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 1, (r.returncode, r.stdout[-1000:], r.stderr[-1000:])
+    assert name in r.stderr, r.stderr[-1000:]
