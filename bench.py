@@ -52,7 +52,7 @@ WORKLOAD = dict(width=1600, height=1200, n_views=11, n_planes=20, n_spheres=5, l
 # size directly; its pyramid follows the reference's rule at that size
 # (ComputingMultiScaleSettings, HPM.cpp:851-860: 2 levels below full scale)
 STRESS = dict(width=3200, height=2133, n_views=20, n_planes=20, n_spheres=5, low_texture=0.50, pyramid_levels=2,
-              geom_iterations=2, depth_range=(1.0, 30.0),
+              geom_iterations=2, depth_range=(1.0, 30.0), n_sources=10,
               name="stress scene (6048x4032 capped to 3200x2133 as the reference does)")
 # batched form: all 24 reference views of one scene at three sizes, each with
 # 10 sources, the pyramid by the reference's rule per view size
