@@ -64,22 +64,40 @@ cudaError_t ensure(void **p, size_t *cap, size_t bytes)
  * state (HPM.cpp:599-616): linear filter, unnormalised coordinates, element
  * reads.  The reference asks for wrap addressing, which the hardware treats
  * as clamp for unnormalised coordinates (pinned by tests/golden/tex_probe);
- * clamp is requested explicitly here. */
+ * clamp is requested explicitly here.  A texture's extent is its array's, so
+ * each view slot keeps a few arrays of the sizes it has held (kTexPerSlot,
+ * most recently used last): problems of a scene whose views differ in size
+ * reuse them instead of freeing one (which waits for the whole device) and
+ * allocating another for nearly every view. */
+constexpr size_t kTexPerSlot = 3;
+
 cudaError_t ensure_texture(hpm_ctx *c, int i, int w, int h)
 {
-    if (c->arr[i] && c->arr_w[i] == w && c->arr_h[i] == h) return cudaSuccess;
-    if (c->tex[i]) cudaDestroyTextureObject(c->tex[i]);
-    if (c->arr[i]) cudaFreeArray(c->arr[i]);
-    c->tex[i] = 0;
+    std::vector<TexArray> &pool = c->tex_pool[i];
+    for (size_t k = 0; k < pool.size(); ++k)
+        if (pool[k].w == w && pool[k].h == h) {
+            const TexArray t = pool[k];
+            pool.erase(pool.begin() + (long)k);
+            pool.push_back(t);
+            c->arr[i] = t.arr;
+            c->tex[i] = t.tex;
+            return cudaSuccess;
+        }
     c->arr[i] = nullptr;
-    c->arr_w[i] = c->arr_h[i] = 0;
+    c->tex[i] = 0;
+    if (pool.size() >= kTexPerSlot) {
+        cudaDestroyTextureObject(pool.front().tex);
+        cudaFreeArray(pool.front().arr);
+        pool.erase(pool.begin());
+    }
+    TexArray t;
     cudaChannelFormatDesc desc = cudaCreateChannelDesc(32, 0, 0, 0, cudaChannelFormatKindFloat);
-    cudaError_t e = cudaMallocArray(&c->arr[i], &desc, w, h);
+    cudaError_t e = cudaMallocArray(&t.arr, &desc, w, h);
     if (e != cudaSuccess) return e;
     cudaResourceDesc res;
     memset(&res, 0, sizeof(res));
     res.resType = cudaResourceTypeArray;
-    res.res.array.array = c->arr[i];
+    res.res.array.array = t.arr;
     cudaTextureDesc td;
     memset(&td, 0, sizeof(td));
     td.addressMode[0] = cudaAddressModeClamp;
@@ -87,10 +105,16 @@ cudaError_t ensure_texture(hpm_ctx *c, int i, int w, int h)
     td.filterMode = cudaFilterModeLinear;
     td.readMode = cudaReadModeElementType;
     td.normalizedCoords = 0;
-    e = cudaCreateTextureObject(&c->tex[i], &res, &td, nullptr);
-    if (e != cudaSuccess) return e;
-    c->arr_w[i] = w;
-    c->arr_h[i] = h;
+    e = cudaCreateTextureObject(&t.tex, &res, &td, nullptr);
+    if (e != cudaSuccess) {
+        cudaFreeArray(t.arr);
+        return e;
+    }
+    t.w = w;
+    t.h = h;
+    pool.push_back(t);
+    c->arr[i] = t.arr;
+    c->tex[i] = t.tex;
     return cudaSuccess;
 }
 
@@ -207,8 +231,10 @@ int hpm_destroy(hpm_ctx *c)
     for (int i = 0; i < kMaxViews; ++i) {
         cudaFree(c->d_img[i]);
         cudaFree(c->d_depth[i]);
-        if (c->tex[i]) cudaDestroyTextureObject(c->tex[i]);
-        if (c->arr[i]) cudaFreeArray(c->arr[i]);
+        for (const TexArray &t : c->tex_pool[i]) {
+            cudaDestroyTextureObject(t.tex);
+            cudaFreeArray(t.arr);
+        }
     }
     cudaFree(c->d_pair);
     cudaFree(c->d_planes);

@@ -57,6 +57,13 @@ struct NetWorkspace {
     int *err = nullptr;            /* status of the tensor-core kernels */
 };
 
+/* A view's float cudaArray with its texture object. */
+struct TexArray {
+    int w = 0, h = 0;
+    cudaArray_t arr = nullptr;
+    cudaTextureObject_t tex = 0;
+};
+
 }  // namespace hpm
 
 struct hpm_ctx {
@@ -68,9 +75,9 @@ struct hpm_ctx {
     HpmCamera cams[hpm::kMaxViews];
     float *d_img[hpm::kMaxViews] = {nullptr};
     size_t img_cap[hpm::kMaxViews] = {0};
-    cudaArray_t arr[hpm::kMaxViews] = {nullptr};
-    int arr_w[hpm::kMaxViews] = {0}, arr_h[hpm::kMaxViews] = {0};
+    cudaArray_t arr[hpm::kMaxViews] = {nullptr};      /* the current view's array and texture */
     cudaTextureObject_t tex[hpm::kMaxViews] = {0};
+    std::vector<hpm::TexArray> tex_pool[hpm::kMaxViews]; /* arrays of the sizes each slot has held */
     float *d_depth[hpm::kMaxViews] = {nullptr};
     size_t depth_cap[hpm::kMaxViews] = {0};
     bool has_depth = false;

@@ -80,3 +80,20 @@ def test_batched_prior_net_pass_set_a_equals_per_problem(extra, prior):
         np.testing.assert_array_equal(cb[ref], cp[ref])
         np.testing.assert_array_equal(db2[ref], dp[ref])
     assert np.mean([syn.depth_accuracy(db[v], sc.gt_depth[v]) for v in range(len(SIZES))]) > 0.2
+
+
+def test_texture_arrays_are_reused_across_view_sizes():
+    """One context alternating between problems whose views differ in size
+    (the texture arrays of each size kept per view slot and reused) gives a
+    problem the same maps bit for bit each time."""
+    sc, imgs, pairs = _scene(64)
+    runs = []
+    with hb.Context() as ctx:
+        for p in (0, 1, 2, 0, 2):
+            ref, srcs = pairs[p]
+            ids = [ref] + srcs
+            ctx.set_views([imgs[i] for i in ids], sc.cams[ids])
+            runs.append(ctx.process_problem(seed=9 + p, planar_prior=True, pyramid_levels=1))
+    for a, b in ((0, 3), (2, 4)):
+        for x, y in zip(runs[a][:3], runs[b][:3]):
+            np.testing.assert_array_equal(x, y)
