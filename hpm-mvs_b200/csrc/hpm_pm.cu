@@ -852,6 +852,17 @@ __device__ __forceinline__ void prop_dirs_body(const PMArgs &a, int iter, int px
             }
         }
     }
+    /* 3) every valid direction's row in its own slot: a row that refers to
+     * the cost-vector cache or to an earlier direction (always one that owns
+     * its row) is copied there, so that the refinement reads each row with
+     * one load and no decoding; the code then holds only own and none */
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        const uint32_t src = (code >> (4 * k)) & 15u;
+        if (src == kRowOwn || src == kRowNone) continue;
+        for (int v = 0; v < S; ++v) CAG(k, v) = src == kRowCache ? *cache_at(a, v, sl) : CAG(src, v);
+        code = (code & ~(15u << (4 * k))) | (kRowOwn << (4 * k));
+    }
 #pragma unroll
     for (int k = 0; k < 8; ++k) a.cand_pos[(size_t)k * sl.nh + sl.hc] = pos[k];
     a.cand_flags[sl.hc] = code;
@@ -891,6 +902,10 @@ __device__ __forceinline__ void prop_refine_body(const PMArgs &a, int iter, int 
 #pragma unroll
     for (int k = 0; k < 8; ++k) pos[k] = a.cand_pos[(size_t)k * sl.nh + sl.hc];
 #define FLAG(k) (((flags >> (k)) & 1u) != 0)
+/* cost of direction k for view v: every valid direction owns its row (step
+ * 3 of prop_dirs_body); an invalid one holds the reference's {2, 0, ...}
+ * (HPM.cu:1244), or 2 everywhere with fix_quirks */
+#define ROWC(k, v) (FLAG(k) ? CAG(k, v) : ((a.fix_quirks || ((k) == 0 && (v) == 0)) ? 2.0f : 0.0f))
     Rng rng;
     rng.init(a.seed_lo, a.seed_hi, (uint32_t)center, (uint32_t)(1 + iter), a.salt);
 
@@ -914,7 +929,7 @@ __device__ __forceinline__ void prop_refine_body(const PMArgs &a, int iter, int 
         float tmpw = 0;
 #pragma unroll
         for (int k = 0; k < 8; ++k) {
-            const float c = dir_cost(a, code, k, v, S, sl);
+            const float c = ROWC(k, v);
             if (c < thr) {
                 tmpw += expf(c * c / (-0.18f));
                 count++;
@@ -980,11 +995,11 @@ __device__ __forceinline__ void prop_refine_body(const PMArgs &a, int iter, int 
             if (v < S && vw[v] > 0) {
                 if (a.geom) {
                     if (FLAG(k))
-                        f += vw[v] * (dir_cost(a, code, k, v, S, sl) + 0.1f * geom_cost(a, v + 1, hk, px, py));
+                        f += vw[v] * (ROWC(k, v) + 0.1f * geom_cost(a, v + 1, hk, px, py));
                     else
-                        f += vw[v] * (dir_cost(a, code, k, v, S, sl) + 0.1f * 5.0f);
+                        f += vw[v] * (ROWC(k, v) + 0.1f * 5.0f);
                 } else {
-                    f += vw[v] * dir_cost(a, code, k, v, S, sl);
+                    f += vw[v] * ROWC(k, v);
                 }
             }
         }
@@ -1196,9 +1211,10 @@ __device__ __forceinline__ void prop_refine_body(const PMArgs &a, int iter, int 
     a.views[center] = sel;
     if (best_row >= kRefineRow) {
         for (int v = 0; v < S; ++v) *cache_at(a, v, sl) = CAG(best_row, v);
-    } else if (best_row >= 0 && ((code >> (4 * best_row)) & 15u) != kRowCache) {
-        for (int v = 0; v < S; ++v) *cache_at(a, v, sl) = dir_cost(a, code, best_row, v, S, sl);
+    } else if (best_row >= 0) {
+        for (int v = 0; v < S; ++v) *cache_at(a, v, sl) = CAG(best_row, v);
     }
+#undef ROWC
 #undef FLAG
 }
 
