@@ -77,16 +77,22 @@ __global__ void k_pack_maps(const float *__restrict__ normal3, const float *__re
  * problem's host work between passes (the Delaunay of its prior levels,
  * with the synchronisations around it) overlaps the others' device work.
  * f may touch only problem p's own context and stream, and reports a
- * failure there.  Returns the failure of the lowest failing problem (after
- * all threads have stopped) and its index in *failed. */
+ * failure there.  Every thread first makes `device` its current device (a
+ * new host thread starts on device 0).  Returns the failure of the lowest
+ * failing problem (after all threads have stopped) and its index in
+ * *failed. */
 template <typename F>
-int for_each_problem(int n, F f, int *failed)
+int for_each_problem(int device, int n, F f, int *failed)
 {
     const int workers = std::max(1, std::min(4, n));
     std::atomic<int> next{0};
     std::atomic<bool> stop{false};
     std::vector<int> rc(n, HPM_OK);
     auto run = [&]() {
+        if (cudaSetDevice(device) != cudaSuccess) {
+            stop.store(true);
+            return;
+        }
         for (;;) {
             const int p = next.fetch_add(1);
             if (p >= n || stop.load()) return;
@@ -103,6 +109,10 @@ int for_each_problem(int n, F f, int *failed)
             *failed = p;
             return rc[p];
         }
+    if (stop.load()) { /* a thread could not select the device */
+        *failed = 0;
+        return HPM_ERR_CUDA;
+    }
     return HPM_OK;
 }
 
@@ -248,7 +258,7 @@ int net_pass_set_a(hpm_ctx *c, const std::vector<hpm_ctx *> &pc, const std::vect
     const int n = (int)pc.size();
     int bad = 0;
     int r = for_each_problem(
-        n, [&](int p) { return net_coarse_views(pc[p], pc[p]->n, images[p].data(), pc[p]->cams); }, &bad);
+        c->device, n, [&](int p) { return net_coarse_views(pc[p], pc[p]->n, images[p].data(), pc[p]->cams); }, &bad);
     if (r) return ctx_fail(c, r, "batched prior-net form, problem %d: %s", bad, hpm_last_error(pc[bad]));
     std::vector<hpm_ctx *> cc(n);
     for (int p = 0; p < n; ++p) cc[p] = pc[p]->coarse;
@@ -263,7 +273,7 @@ int net_pass_set_a(hpm_ctx *c, const std::vector<hpm_ctx *> &pc, const std::vect
         if (r) return r;
     }
     r = for_each_problem(
-        n,
+        c->device, n,
         [&](int p) {
             int q = net_coarse_finish(pc[p], params[p].depth_min, params[p].depth_max);
             return q ? q : net_full_setup(pc[p], net, prior_mode);
@@ -273,7 +283,7 @@ int net_pass_set_a(hpm_ctx *c, const std::vector<hpm_ctx *> &pc, const std::vect
     std::vector<HpmParams> fp(params);
     for (int e = 0; e <= extra_passes; ++e) {
         r = for_each_problem(
-            n,
+            c->device, n,
             [&](int p) {
                 hpm_ctx *b = pc[p];
                 if (e > 0) {
@@ -411,7 +421,7 @@ int batched_scene(hpm_ctx *c, int n_views, const float *const *images, const Hpm
                 if (level >= 2 - levels[p]) in.push_back(p);
             int bad = 0;
             r = for_each_problem(
-                (int)in.size(),
+                c->device, (int)in.size(),
                 [&](int i) {
                     const int p = in[i];
                     hpm_ctx *b = pc[p];

@@ -476,8 +476,10 @@ int net_problem(hpm_ctx *c, int n, const float *const *images, const HpmCamera *
                 float *cost_out)
 {
     const Range range("prior-net problem %dx%d", cams[0].width, cams[0].height);
+    int r = ctx_select_device(c); /* the scene's second worker thread starts on device 0 */
+    if (r) return r;
     int cw, ch;
-    int r = net_coarse_stage(c, n, images, cams, seed, &cw, &ch);
+    r = net_coarse_stage(c, n, images, cams, seed, &cw, &ch);
     if (r) return r;
     r = hpm_set_views(c, images, cams, n);
     if (r) return r;
