@@ -55,7 +55,7 @@ def test_cost_vectors_vs_reference(ncc_ctx):
             np.testing.assert_array_equal(ig, ir)
             np.testing.assert_array_equal(sg[ig], sr[ir])
             exact = ncc_split.exact_costs(sg, ig, imgs[0], px).reshape(got.shape)
-            ncc_split.check_exact(got, exact, acc, f"field {k} vs its samples")
+            ncc_split.check_exact(got, sg, ig, imgs[0], px, f"field {k} vs its samples")
         ncc_split.check_within_bound(got, n["cost_vectors"][k], bound + acc, f"field {k}", exact=exact,
                                      extra={"acc": acc, "kind": kind, "oracle": ocost})
 

@@ -81,7 +81,7 @@ def test_cost_vectors_vs_reference_and_oracle(case):
             np.testing.assert_array_equal(ig, ir)
             np.testing.assert_array_equal(sg[ig], sr[ir])
             exact = ncc_split.exact_costs(sg, ig, c["imgs"][0], px)
-            ncc_split.check_exact(got, exact, acc, f"{name} field {k} vs its samples")
+            ncc_split.check_exact(got, sg, ig, c["imgs"][0], px, f"{name} field {k} vs its samples")
         ref = g["cost_vectors"][k]
         ncc_split.check_within_bound(got, ref, bound + acc, f"{name} field {k} vs reference", exact=exact,
                                      extra={"acc": acc, "kind": kind, "oracle": ocost})
