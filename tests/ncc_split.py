@@ -141,20 +141,45 @@ def check_exact(got, samples, inside, ref_img, pixels, what):
                             f"{float(d[over].max()):.3g} (bound {float(bound[over][np.argmax(d[over])]):.3g})")
 
 
-def check_within_bound(got, ref, bound, what, exact=None, extra=None):
-    """|got - ref| <= 1e-4 max(1, |ref|) + MARGIN * bound for every value,
-    and <= 1e-4 max(1, |ref|) alone where the bound is below 1e-4 (well
-    conditioned).  Returns the fraction of values within 1e-4.  exact (the
-    float64 value of the same samples) and extra arrays only enrich the
-    message of a failure."""
+SELF_INCONSISTENT_CAP = 1e-3  # at most this fraction of a field's values may be exempted
+
+
+def reference_self_inconsistent(ref, exact, bound):
+    """Values where the reference's NCC kernel lies beyond the tap-crossing
+    bound of the exact NCC of the samples that the reference's own
+    coordinate functions give (hpm_ref_tap_samples): the reference disagrees
+    with itself there, by more than any crossing of a weight step explains
+    (measured: 2 of 16,384 values of the 640x480 case, 4.4e-3 and 1.4e-3 off
+    its own samples; the oracle, whose coordinates round on their own, lands
+    where the reference's kernel does).  Returns the mask; at most
+    SELF_INCONSISTENT_CAP of the values may be in it."""
+    ref, exact = np.asarray(ref, np.float64), np.asarray(exact, np.float64)
+    bound = np.broadcast_to(np.asarray(bound, np.float64), ref.shape)
+    off = np.abs(ref - exact) > 1e-4 * np.maximum(1.0, np.abs(ref)) + MARGIN * bound
+    assert off.mean() <= SELF_INCONSISTENT_CAP, (
+        f"the reference's kernel is off its own samples in {int(off.sum())} of {off.size} values")
+    return off
+
+
+def check_within_bound(got, ref, bound, what, exact=None, extra=None, exempt=None):
+    """|got - ref| <= 1e-4 max(1, |ref|) + MARGIN * bound for every value
+    outside `exempt` (a mask from reference_self_inconsistent, whose values
+    the caller checks against the exact NCC instead), and <= 1e-4 max(1,
+    |ref|) alone where the bound is below 1e-4 (well conditioned).  Returns
+    the fraction of values within 1e-4.  exact (the float64 value of the
+    same samples) and extra arrays only enrich the message of a failure."""
     got, ref = np.asarray(got, np.float64), np.asarray(ref, np.float64)
     bound = np.broadcast_to(np.asarray(bound, np.float64), got.shape)
     d = np.abs(got - ref)
     tol = 1e-4 * np.maximum(1.0, np.abs(ref))
     over = d > tol + MARGIN * bound
+    if exempt is not None:
+        over &= ~np.asarray(exempt, bool).reshape(over.shape)
     assert not over.any(), (f"{what}: {int(over.sum())} values beyond the bound, worst excess "
                             f"{float((d - tol - MARGIN * bound).max()):.3g}; "
                             + _offenders(over, got, ref, MARGIN * bound + tol, exact, extra))
     calm = bound < 1e-4
+    if exempt is not None:
+        calm &= ~np.asarray(exempt, bool).reshape(calm.shape)
     assert (d[calm] <= tol[calm]).all(), f"{what}: {int((d[calm] > tol[calm]).sum())} well-conditioned values off"
     return float((d <= tol).mean())

@@ -83,9 +83,12 @@ def test_cost_vectors_vs_reference_and_oracle(case):
             exact = ncc_split.exact_costs(sg, ig, c["imgs"][0], px)
             ncc_split.check_exact(got, sg, ig, c["imgs"][0], px, f"{name} field {k} vs its samples")
         ref = g["cost_vectors"][k]
+        # where the reference's kernel is off its own exported samples, the
+        # product is held to those samples' exact NCC (check_exact) instead
+        off = None if exact is None else ncc_split.reference_self_inconsistent(ref, exact, bound + acc)
         ncc_split.check_within_bound(got, ref, bound + acc, f"{name} field {k} vs reference", exact=exact,
-                                     extra={"acc": acc, "kind": kind, "oracle": ocost})
-        ncc_split.check_within_bound(got, ocost, bound + acc, f"{name} field {k} vs oracle")
+                                     extra={"acc": acc, "kind": kind, "oracle": ocost}, exempt=off)
+        ncc_split.check_within_bound(got, ocost, bound + acc, f"{name} field {k} vs oracle", exempt=off)
         ncc_split.check_within_bound(ocost, ref, bound + acc, f"{name} field {k} oracle vs reference")
 
 
