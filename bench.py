@@ -90,11 +90,12 @@ def parse_args():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--config", choices=["plain-hpm", "stress", "batched"], default="plain-hpm",
+    ap.add_argument("--config", choices=["plain-hpm", "stress", "batched", "acmm"], default="plain-hpm",
                     help="plain-hpm: 11 views of 1600x1200 (the metric's configuration); stress: 20 views of "
                          "6048x4032 capped to 3200x2133, 50%% low texture, depth 1-30 m (one step takes minutes); "
                          "batched: 24 views at three sizes through hpm_run_scene_batched against the per-problem "
-                         "driver")
+                         "driver; acmm: the ACMM+NESP variant (hpm_run_scene_acmm, coarse-to-fine over an image "
+                         "pyramid) on the plain-hpm scene beside the plain HPM form")
     ap.add_argument("--size", default=None,
                     help="WxH override of the workload's resolution (profiling captures use a smaller case)")
     ap.add_argument("--views", type=int, default=None, help="override of the scene's view count")
@@ -589,6 +590,63 @@ def run_batched(args, dist):
     }
 
 
+def run_acmm(args, dist):
+    """The ACMM+NESP variant (hpm_run_scene_acmm: 800x600, then 1600x1200
+    started from the upsampled maps, 2 geometric iterations at each scale)
+    beside the plain HPM form (hpm_run_scene) on the same scene: host images
+    in and every view's maps out per step, CUDA events on the context's
+    stream."""
+    import torch
+
+    import hpm_b200 as hb
+
+    torch.cuda.set_device(dist.local)
+    dev = f"cuda:{dist.local}"
+    w = WORKLOAD
+    sc, images, pairs = make_scene(seed=dist.rank)
+    npx = sum(i.size for i in images)
+    ctx = hb.Context(dist.local)
+    stream = torch.cuda.ExternalStream(ctx.stream(), device=dev)
+    forms = {
+        "acmm_nesp": lambda seed: ctx.run_scene_acmm(images, sc.cams, pairs, seed=seed,
+                                                     geom_iterations=w["geom_iterations"]),
+        "plain_hpm": lambda seed: ctx.run_scene(images, sc.cams, pairs, seed=seed,
+                                                geom_iterations=w["geom_iterations"],
+                                                pyramid_levels=w["pyramid_levels"]),
+    }
+    res = {}
+    for name, run in forms.items():
+        for i in range(args.warmup):
+            run(500 + i)
+        dist.barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with Clocks(dist.local) as clk:
+            e0.record(stream)
+            for i in range(args.steps):
+                d, n, _ = run(i)
+            e1.record(stream)
+            e1.synchronize()
+        dist.barrier()
+        ms = dist.max(e0.elapsed_time(e1)) / args.steps
+        res[name] = {"ms_per_step": ms, "value": job_mpix_per_s(dist.world, 1, npx, ms),
+                     "accuracy": scene_accuracy(sc, dict(enumerate(d)), dict(enumerate(n))), "clocks": clk.summary()}
+    ctx.close()
+    a = res["acmm_nesp"]
+    return {
+        "metric": "depth Mpix/s of the ACMM+NESP variant on 1 B200", "value": a["value"], "unit": "depth Mpix/s",
+        "n_gpus": dist.world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": a["ms_per_step"],
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded procedural scene)",
+        "config": {"workload": f"ACMM+NESP variant on {workload_name()}",
+                   "scales": "800x600, then 1600x1200 (halvings until the longer side is at most 1000)",
+                   "form": "hpm_run_scene_acmm: plain pass and geometric iterations at the coarse scale; JBU of the "
+                           "geometric depth and the normals, hierarchy pass and geometric iterations at full scale"},
+        "accuracy": a["accuracy"], "clocks": a["clocks"], "plain_hpm_form": res["plain_hpm"],
+        "speedup_vs_plain_hpm": res["plain_hpm"]["ms_per_step"] / a["ms_per_step"], "impl": "ours",
+    }
+
+
 def run_view_shards(args, dist):
     """One scene, its problems split over the ranks (scene_dist.py): timed
     from the host images to every rank's final maps on the host."""
@@ -877,6 +935,8 @@ def main():
             line = run_view_shards(args, dist)
         elif args.config == "batched":
             line = run_batched(args, dist)
+        elif args.config == "acmm":
+            line = run_acmm(args, dist)
         else:
             line = run_ours(args, dist)
             if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:

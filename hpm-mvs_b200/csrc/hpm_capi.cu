@@ -157,6 +157,7 @@ PMArgs make_args(hpm_ctx *c)
     a.cand_pos = c->d_pos;
     a.cand_flags = c->d_flags;
     a.proposals = c->proposals;
+    a.geom_max = 5.0f; /* HPM.cu:485 */
     return a;
 }
 
@@ -249,6 +250,7 @@ int hpm_destroy(hpm_ctx *c)
     cudaFree(c->d_cand);
     cudaFree(c->d_pos);
     cudaFree(c->d_flags);
+    cudaFree(c->d_pre);
     ws_free(c);
     net_free(c);
     for (auto &p : c->prof_events) {
@@ -390,9 +392,11 @@ int hpm_clear_prior(hpm_ctx *c)
 
 /* The kernel arguments of one pass of context c with parameters p (checks
  * as hpm_run_patchmatch; takes the pass's random-stream salt). */
-extern "C++" int ctx_pass_args(hpm_ctx *c, const HpmParams *p, PMArgs *out)
+/* Checks p against the context's state and fills the pass fields of *out;
+ * takes the pass's random-stream salt.  Shared by run_pass and
+ * ctx_pass_args. */
+static int pass_args(hpm_ctx *c, const HpmParams *p, PMArgs *out)
 {
-    if (!c) return HPM_ERR_ARG;
     if (!p) return fail(c, HPM_ERR_ARG, "hpm_run_patchmatch: null params");
     if (c->n < 2) return fail(c, HPM_ERR_STATE, "hpm_run_patchmatch before hpm_set_views");
     if (p->patch_size != 11 || p->radius_increment != 2)
@@ -402,6 +406,15 @@ extern "C++" int ctx_pass_args(hpm_ctx *c, const HpmParams *p, PMArgs *out)
     if (p->planar_prior && !c->has_prior) return fail(c, HPM_ERR_STATE, "planar prior needs hpm_set_prior");
     if (!(p->depth_max > p->depth_min)) return fail(c, HPM_ERR_ARG, "depth range is empty");
     if (p->top_k < 1 || p->top_k > kMaxSrc) return fail(c, HPM_ERR_ARG, "top_k outside [1, %d]", kMaxSrc);
+    if (p->variant != 0 && p->variant != 1)
+        return fail(c, HPM_ERR_ARG, "variant %d: 0 (HPM-MVS) or 1 (ACMM+NESP)", p->variant);
+    if (p->variant == 1 && p->planar_prior) return fail(c, HPM_ERR_ARG, "the ACMM+NESP variant has no planar prior");
+    if (p->hierarchy < 0 || p->hierarchy > 2) return fail(c, HPM_ERR_ARG, "hierarchy %d outside [0, 2]", p->hierarchy);
+    if (p->hierarchy && (p->variant != 1 || p->geom_consistency))
+        return fail(c, HPM_ERR_ARG, "a hierarchy pass belongs to the ACMM+NESP variant and has no geometric term");
+    if (p->hierarchy && !c->has_state)
+        return fail(c, HPM_ERR_STATE, "a hierarchy pass starts from hpm_set_hypotheses");
+    if (p->hierarchy) CK(ensure((void **)&c->d_pre, &c->pre_cap, sizeof(float) * npx(c)), "pre-cost alloc");
     PMArgs a = make_args(c);
     a.dmin = p->depth_min;
     a.dmax = p->depth_max;
@@ -415,8 +428,22 @@ extern "C++" int ctx_pass_args(hpm_ctx *c, const HpmParams *p, PMArgs *out)
     a.salt = c->pass_counter++;
     a.fix_quirks = p->fix_quirks ? 1 : 0;
     if (p->fix_quirks) a.rows_cov = a.H; /* every row, also the last of an odd height (HPM.cu:1926) */
-    c->has_state = true;
+    if (p->variant == 1) {
+        a.acmm = 1;        /* weight 0.2: ACMM.cu:651, 1596 */
+        a.geom_max = 3.0f; /* ACMM.cu:496 */
+        a.hier = p->hierarchy;
+        a.pre_costs = p->hierarchy ? c->d_pre : nullptr;
+    }
     *out = a;
+    return HPM_OK;
+}
+
+extern "C++" int ctx_pass_args(hpm_ctx *c, const HpmParams *p, PMArgs *out)
+{
+    if (!c) return HPM_ERR_ARG;
+    const int r = pass_args(c, p, out);
+    if (r) return r;
+    c->has_state = true;
     return HPM_OK;
 }
 
@@ -428,31 +455,12 @@ extern "C++" void ctx_reset_salt(hpm_ctx *c) { c->pass_counter = 0; }
 static int run_pass(hpm_ctx *c, const HpmParams *p, int half_steps, int finalize, bool sync)
 {
     if (!c) return HPM_ERR_ARG;
-    if (!p) return fail(c, HPM_ERR_ARG, "hpm_run_patchmatch: null params");
-    if (c->n < 2) return fail(c, HPM_ERR_STATE, "hpm_run_patchmatch before hpm_set_views");
-    if (p->patch_size != 11 || p->radius_increment != 2)
-        return fail(c, HPM_ERR_ARG, "hpm_run_patchmatch: only the reference window (11, stride 2) is built");
-    if (p->geom_consistency && !c->has_depth)
-        return fail(c, HPM_ERR_STATE, "geometric consistency needs hpm_set_geom_depths");
-    if (p->planar_prior && !c->has_prior) return fail(c, HPM_ERR_STATE, "planar prior needs hpm_set_prior");
-    if (!(p->depth_max > p->depth_min)) return fail(c, HPM_ERR_ARG, "depth range is empty");
-    if (p->top_k < 1 || p->top_k > kMaxSrc) return fail(c, HPM_ERR_ARG, "top_k outside [1, %d]", kMaxSrc);
     int r = select_device(c);
     if (r) return r;
+    PMArgs a;
+    r = pass_args(c, p, &a);
+    if (r) return r;
     const Range range("pass geom=%d prior=%d", p->geom_consistency ? 1 : 0, p->planar_prior ? 1 : 0);
-    PMArgs a = make_args(c);
-    a.dmin = p->depth_min;
-    a.dmax = p->depth_max;
-    a.geom = p->geom_consistency ? 1 : 0;
-    a.prior = p->planar_prior ? 1 : 0;
-    a.sigma_spatial = p->sigma_spatial;
-    a.sigma_color = p->sigma_color;
-    a.top_k = p->top_k;
-    a.seed_lo = (uint32_t)p->seed;
-    a.seed_hi = (uint32_t)(p->seed >> 32);
-    a.salt = c->pass_counter++;
-    a.fix_quirks = p->fix_quirks ? 1 : 0;
-    if (p->fix_quirks) a.rows_cov = a.H; /* every row, also the last of an odd height (HPM.cu:1926) */
     cudaEvent_t e0;
     prof_begin(c, 0, &e0);
     CK(launch_init(a, c->stream), "init kernel");
@@ -475,7 +483,8 @@ static int run_pass(hpm_ctx *c, const HpmParams *p, int half_steps, int finalize
 int hpm_run_patchmatch(hpm_ctx *c, const HpmParams *p)
 {
     if (!c || !p) return HPM_ERR_ARG;
-    const int iters = p->honour_max_iterations ? p->max_iterations : 3; /* HPM.cu:1933 */
+    /* HPM.cu:1933 runs 3; the ACMM+NESP variant honours the field (ACMM.cu:1836) */
+    const int iters = (p->honour_max_iterations || p->variant == 1) ? p->max_iterations : 3;
     if (iters < 0 || iters > 64) return fail(c, HPM_ERR_ARG, "max_iterations outside [0, 64]");
     return run_pass(c, p, 2 * iters, 1, true);
 }

@@ -113,6 +113,8 @@ struct hpm_ctx {
     size_t pos_cap = 0;
     uint32_t *d_flags = nullptr; /* direction row codes [ceil(H*W/2)] */
     size_t flags_cap = 0;
+    float *d_pre = nullptr; /* ACMM+NESP hierarchy pass: acceptance threshold per pixel */
+    size_t pre_cap = 0;
 
     /* prior-net form: the network's proposed plane per pixel (ref-frame
      * normal, distance) for the next pass, or nullptr (plain form) */

@@ -69,6 +69,15 @@ struct PMArgs {
     /* prior-net form: per pixel a proposed plane (ref-frame normal, distance),
      * scored as one more refinement candidate; nullptr in the plain form */
     const float4 *proposals;
+    /* HpmParams.variant 1 (ACMM+NESP): acmm selects its refinement kernel
+     * (geometric weight 0.2 on the current and refined hypotheses, the
+     * threshold rule of a hierarchy pass), geom_max the cap of the geometric
+     * cost (5, or 3 in the variant); hier is HpmParams.hierarchy and
+     * pre_costs its per-pixel acceptance threshold, written by the
+     * initialisation */
+    int acmm, hier;
+    float geom_max;
+    float *pre_costs;
 };
 
 /* Launchers (hpm_pm.cu / hpm_jbu.cu). All asynchronous on `s`. */

@@ -477,7 +477,8 @@ __device__ __forceinline__ void project(const float *P, const HpmCamera &c, floa
     pt[1] = (c.K[3] * t0 + c.K[4] * t1 + c.K[5] * t2) / depth;
 }
 
-/* ComputeGeomConsistencyCost (HPM.cu:483-508) */
+/* ComputeGeomConsistencyCost (HPM.cu:483-508; capped at a.geom_max, 5 there
+ * and 3 in ACMM.cu:494-519) */
 __device__ __noinline__ float geom_cost(const PMArgs &a, int v, float4 h, int px, int py)
 {
     const HpmCamera &rc = a.cam[0], &sc = a.cam[v];
@@ -488,12 +489,12 @@ __device__ __noinline__ float geom_cost(const PMArgs &a, int v, float4 h, int px
     const ViewDev &sv = a.view[v];
     const float src_depth = texel(sv.depth, sv.w, sv.h, __float2int_rz(spt[0]), __float2int_rz(spt[1]));
     if (a.counters) atomicAdd(&a.counters[1], 1ull);
-    if (src_depth == 0.0f) return 5.0f;
+    if (src_depth == 0.0f) return a.geom_max;
     float Q[3], bpt[2], rd;
     world_point(sc, spt[0], spt[1], src_depth, Q);
     project(Q, rc, bpt, rd);
     const float dx = px - bpt[0], dy = py - bpt[1];
-    return fminf(5.0f, sqrtf(dx * dx + dy * dy));
+    return fminf(a.geom_max, sqrtf(dx * dx + dy * dy));
 }
 
 /* ------------------------------------------------------------------ */
@@ -571,7 +572,22 @@ __device__ __forceinline__ void init_body(const PMArgs &a, int px, int py, WinWe
     Rng rng;
     rng.init(a.seed_lo, a.seed_hi, (uint32_t)center, 0u, a.salt);
     float4 h;
-    if (a.geom) {
+    if (a.geom || a.hier) {
+        if (a.hier == 1) {
+            /* ACMM+NESP hierarchy pass (ACMM.cu:538-604): the acceptance
+             * threshold is the initial cost of the plane the reference holds
+             * before the normal is filled in, a zero normal with the depth as
+             * its distance (ACMM.cpp:707-713 sets only .w of a fresh,
+             * zero-filled array); at the maps' own size (hier 2) the
+             * reference leaves it unset, taken as 0 */
+            const float4 hz = make_float4(0.0f, 0.0f, 0.0f, a.planes[center].w);
+            float *cvz = sCV + tid;
+            cost_vector(a, px, py, hz, sWW, tid, rs, cvz, kBlock);
+            uint32_t unused;
+            a.pre_costs[center] = initial_cost_from(a, cvz, kBlock, &unused);
+        } else if (a.hier == 2) {
+            a.pre_costs[center] = 0.0f;
+        }
         h = transform_normal_to_ref(cam, a.planes[center]);
         const float depth = h.w;
         h.w = distance_to_origin(cam, px, py, depth, h);
@@ -884,10 +900,15 @@ __global__ void __launch_bounds__(kBlock, HPM_P1_MIN_BLOCKS) k_prop_dirs(const _
 /* PROP: the prior-net form, whose network proposal a.proposals[center] is a
  * sixth refinement candidate, scored by the same NCC (and prior terms) as the
  * other five and accepted by the same rule.  It takes no random draws, so
- * the random stream of the other candidates is unchanged. */
-template <int SMAX, bool PROP>
+ * the random stream of the other candidates is unchanged.
+ * ACMM: the ACMM+NESP variant (ACMM.cu:1548-1629, 623-667): geometric weight
+ * 0.2 on the current and refined hypotheses, no NaN fallback, and in a
+ * hierarchy pass the threshold rule on the result.  A separate
+ * instantiation, so that the HPM-MVS kernels keep their registers. */
+template <int SMAX, bool PROP, bool ACMM>
 __device__ __forceinline__ void prop_refine_body(const PMArgs &a, int iter, int px, int py, WinPair *sWW, int tid)
 {
+    constexpr float kGeomW = ACMM ? 0.2f : 0.1f; /* HPM.cu:1642, 1189; ACMM.cu:1596, 651 */
     if (px >= a.W || py >= a.rows_cov) return;
     const int W = a.W, S = a.n - 1;
     const int center = py * W + px;
@@ -1025,7 +1046,7 @@ __device__ __forceinline__ void prop_refine_body(const PMArgs &a, int iter, int 
     for (int v = 0; v < SMAX; ++v) {
         if (v < S && vw[v] > 0) {
             if (a.geom)
-                cost_now += vw[v] * (*cache_at(a, v, sl) + 0.1f * geom_cost(a, v + 1, plane, px, py));
+                cost_now += vw[v] * (*cache_at(a, v, sl) + kGeomW * geom_cost(a, v + 1, plane, px, py));
             else
                 cost_now += vw[v] * *cache_at(a, v, sl);
         }
@@ -1102,7 +1123,7 @@ __device__ __forceinline__ void prop_refine_body(const PMArgs &a, int iter, int 
             cost = fc[min_idx];
             sel = tsv;
         }
-        if (cost != cost) {
+        if (!ACMM && cost != cost) { /* the ACMM+NESP variant has no such fallback */
             depth_now = db;
             plane = hb;
             best_row = min_idx;
@@ -1177,7 +1198,7 @@ __device__ __forceinline__ void prop_refine_body(const PMArgs &a, int iter, int 
                 CAG(kRefineRow + i, v) = c;
                 if (selected) {
                     if (a.geom)
-                        tc[i] += w * (c + 0.1f * geom_cost(a, v + 1, cand[i], px, py));
+                        tc[i] += w * (c + kGeomW * geom_cost(a, v + 1, cand[i], px, py));
                     else
                         tc[i] += w * c;
                 }
@@ -1206,6 +1227,17 @@ __device__ __forceinline__ void prop_refine_body(const PMArgs &a, int iter, int 
             }
         }
     }
+    /* ACMM+NESP hierarchy pass (ACMM.cu:1617-1624): the update is kept only
+     * where it beats the threshold by 0.1; otherwise the pixel keeps its
+     * plane with the current hypothesis's cost under this half-step's view
+     * weights (its selected views may still have changed) */
+    if constexpr (ACMM) {
+        if (a.pre_costs && !(cost < a.pre_costs[center] - 0.1f)) {
+            plane = cur;
+            cost = cost_now;
+            best_row = -1;
+        }
+    }
     a.planes[center] = plane;
     a.costs[center] = cost;
     a.views[center] = sel;
@@ -1218,7 +1250,7 @@ __device__ __forceinline__ void prop_refine_body(const PMArgs &a, int iter, int 
 #undef FLAG
 }
 
-template <int SMAX, bool PROP, int WW>
+template <int SMAX, bool PROP, int WW, bool ACMM = false>
 __global__ void __launch_bounds__(kBlock, HPM_P2_MIN_BLOCKS) k_prop_refine(const __grid_constant__ PMArgs a, int iter,
                                                                             int color)
 {
@@ -1226,7 +1258,7 @@ __global__ void __launch_bounds__(kBlock, HPM_P2_MIN_BLOCKS) k_prop_refine(const
     const int tid = threadIdx.y * kBlockX + threadIdx.x;
     int px, py;
     half_step_pixel_at(blockIdx.x, blockIdx.y, WW, color, px, py);
-    prop_refine_body<SMAX, PROP>(a, iter, px, py, sWW, tid);
+    prop_refine_body<SMAX, PROP, ACMM>(a, iter, px, py, sWW, tid);
 }
 #undef CAG
 
@@ -1349,6 +1381,12 @@ cudaError_t launch_prop_t(const PMArgs &a, int iter, int color, cudaStream_t s)
     constexpr int WH = 32 / WW;
     const dim3 grid((a.W + 2 * WW - 1) / (2 * WW), (a.rows_cov + 2 * WH - 1) / (2 * WH)), b(kBlockX, kBlockY);
     k_prop_dirs<WW><<<grid, b, 0, s>>>(a, iter, color);
+    if constexpr (WW == 8) { /* the ACMM+NESP variant runs the default tile */
+        if (a.acmm) {
+            k_prop_refine<SMAX, false, WW, true><<<grid, b, 0, s>>>(a, iter, color);
+            return cudaGetLastError();
+        }
+    }
     if (a.proposals)
         k_prop_refine<SMAX, true, WW><<<grid, b, 0, s>>>(a, iter, color);
     else
@@ -1392,6 +1430,7 @@ cudaError_t launch_init(const PMArgs &a, cudaStream_t s)
 cudaError_t launch_propagate(const PMArgs &a, int iter, int color, cudaStream_t s, int ww)
 {
     if (a.rows_cov <= 0) return cudaSuccess;
+    if (a.acmm) ww = 8; /* its refinement kernel exists for this tile only */
     switch (ww) {
     case 4: return launch_prop_w<4>(a, iter, color, s);
     case 8: return launch_prop_w<8>(a, iter, color, s);

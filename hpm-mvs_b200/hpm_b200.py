@@ -41,7 +41,7 @@ EXPORTED = [
     "hpm_fuse", "hpm_write_ply", "hpm_read_bgr8", "hpm_set_scene_workers", "hpm_resize_linear_u8",
     "hpm_raster_triangles", "hpm_knn6", "hpm_tap_samples", "hpm_net_pack_weights", "hpm_net_conv3x3",
     "hpm_net_conv_wgrad", "hpm_run_scene_net", "hpm_net_coarse_inputs", "hpm_net_targets", "hpm_net_loss",
-    "hpm_net_adam", "hpm_run_scene_batched", "hpm_run_scene_batched_net",
+    "hpm_net_adam", "hpm_run_scene_batched", "hpm_run_scene_batched_net", "hpm_run_scene_acmm",
 ]
 
 
@@ -49,6 +49,11 @@ class HpmSceneOpts(ctypes.Structure):
     _fields_ = [("planar_prior", ctypes.c_int), ("geom_iterations", ctypes.c_int), ("seed", ctypes.c_uint64),
                 ("pyramid_levels", ctypes.c_int), ("iterations", ctypes.c_int), ("fix_quirks", ctypes.c_int),
                 ("geom_pass_iterations", ctypes.c_int)]
+
+
+class HpmAcmmOpts(ctypes.Structure):
+    _fields_ = [("geom_iterations", ctypes.c_int), ("seed", ctypes.c_uint64), ("size_bound", ctypes.c_int),
+                ("max_iterations", ctypes.c_int), ("geom_max_iterations", ctypes.c_int)]
 
 
 class HpmNetWeights(ctypes.Structure):
@@ -108,7 +113,8 @@ class HpmParams(ctypes.Structure):
                 ("sigma_spatial", ctypes.c_float), ("sigma_color", ctypes.c_float), ("top_k", ctypes.c_int),
                 ("depth_min", ctypes.c_float), ("depth_max", ctypes.c_float), ("geom_consistency", ctypes.c_int),
                 ("multi_geometry", ctypes.c_int), ("planar_prior", ctypes.c_int),
-                ("honour_max_iterations", ctypes.c_int), ("seed", ctypes.c_uint64), ("fix_quirks", ctypes.c_int)]
+                ("honour_max_iterations", ctypes.c_int), ("seed", ctypes.c_uint64), ("fix_quirks", ctypes.c_int),
+                ("variant", ctypes.c_int), ("hierarchy", ctypes.c_int)]
 
 
 class HpmError(RuntimeError):
@@ -141,9 +147,12 @@ def _p(a):
 
 
 def default_params(depth_min: float, depth_max: float, *, seed: int = 0, geom: bool = False,
-                   prior: bool = False, multi_geometry: bool = False, fix_quirks: bool = False) -> HpmParams:
+                   prior: bool = False, multi_geometry: bool = False, fix_quirks: bool = False, variant: int = 0,
+                   hierarchy: int = 0, max_iterations: int = 3) -> HpmParams:
     """HpmParams with the reference's defaults; fix_quirks: see HpmParams in
-    include/hpm_b200.h (False keeps the reference's behaviour)."""
+    include/hpm_b200.h (False keeps the reference's behaviour).  variant 1:
+    the ACMM+NESP variant's kernels (max_iterations honoured, hierarchy
+    1 or 2 for its hierarchy pass)."""
     p = HpmParams()
     lib().hpm_default_params(ctypes.byref(p))
     p.depth_min = depth_min
@@ -153,6 +162,9 @@ def default_params(depth_min: float, depth_max: float, *, seed: int = 0, geom: b
     p.planar_prior = int(prior)
     p.multi_geometry = int(multi_geometry)
     p.fix_quirks = int(fix_quirks)
+    p.variant = int(variant)
+    p.hierarchy = int(hierarchy)
+    p.max_iterations = int(max_iterations)
     return p
 
 
@@ -327,6 +339,34 @@ class Context:
             res = [o_[0] for o_ in outs], [o_[1] for o_ in outs], [o_[2] for o_ in outs]
             return res + tuple(extra) if extra_maps else res
         return None
+
+    def run_scene_acmm(self, images, cams, pairs, *, seed=0, geom_iterations=2, size_bound=0, max_iterations=0,
+                       geom_max_iterations=0):
+        """The ACMM+NESP variant's main() over a scene (hpm_run_scene_acmm):
+        coarse-to-fine over an image pyramid whose coarsest scale has every
+        longer side at most size_bound (0: the reference's 1000).  images:
+        per-view float32 [H, W]; pairs: [(v, [sources])] with pairs[v][0] ==
+        v.  Returns per-view (depth, world normal, cost) lists."""
+        n = len(cams)
+        cams = np.ascontiguousarray(cams, dtype=CAMERA_DTYPE)
+        keep = [np.ascontiguousarray(i, dtype=np.float32) for i in images]
+        img_arr = (ctypes.c_void_p * n)(*[k.ctypes.data for k in keep])
+        refs = np.array([p[0] for p in pairs], np.int32)
+        counts = np.array([len(p[1]) for p in pairs], np.int32)
+        srcs = np.zeros((len(pairs), MAX_IMAGES - 1), np.int32)
+        for i, (_, s) in enumerate(pairs):
+            srcs[i, :len(s)] = s
+        o = HpmAcmmOpts(int(geom_iterations), int(seed), int(size_bound), int(max_iterations),
+                        int(geom_max_iterations))
+        outs = [(np.empty((int(c["height"]), int(c["width"])), np.float32),
+                 np.empty((int(c["height"]), int(c["width"]), 3), np.float32),
+                 np.empty((int(c["height"]), int(c["width"])), np.float32)) for c in cams]
+        arrs = [(ctypes.c_void_p * n)(*[o_[k].ctypes.data for o_ in outs]) for k in range(3)]
+        self._check(lib().hpm_run_scene_acmm(self._h, n, img_arr, _p(cams), len(pairs), _p(refs), _p(counts),
+                                             _p(srcs), ctypes.byref(o), arrs[0], arrs[1], arrs[2]),
+                    "hpm_run_scene_acmm")
+        del keep
+        return [o_[0] for o_ in outs], [o_[1] for o_ in outs], [o_[2] for o_ in outs]
 
     def prior_level(self, level, depth, normal, cost):
         """Prior of one pyramid level from given maps: (planes, masks, prior_depth)."""

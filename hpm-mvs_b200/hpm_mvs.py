@@ -16,6 +16,11 @@ set A uses S + p, of geometric iteration g S + 1000003 (g + 1) + p.
 Finished steps are logged in HPM/progress.txt, in the C++ host's format
 (Progress): --stop-after N ends the run once N steps have finished, --resume
 skips the logged steps.
+
+--acmm runs the ACMM+NESP variant's main() (ACMM+NESP/windows/main.cpp:
+299-384) instead: coarse-to-fine over an image pyramid (hpm_run_scene_acmm),
+writing ACMM_NESP/2333_%08d/{depths_geom,normals,costs}.dmb and fusing them
+into ACMM_NESP/ACMM_NESP_model.ply.
 """
 from __future__ import annotations
 
@@ -49,7 +54,9 @@ def load_view(folder: str, vid: int):
     h, w = img.shape
     if w > MAX_IMAGE_SIZE or h > MAX_IMAGE_SIZE:
         factor = min(np.float32(MAX_IMAGE_SIZE) / np.float32(w), np.float32(MAX_IMAGE_SIZE) / np.float32(h))
-        nw, nh = int(round(w * float(factor))), int(round(h * float(factor)))
+        # std::round of the float product: halves away from zero
+        nw = int(np.floor(np.float64(np.float32(w) * factor) + 0.5))
+        nh = int(np.floor(np.float64(np.float32(h) * factor) + 0.5))
         img = hb.resize_linear(img, nw, nh)
         sx, sy = np.float32(nw) / np.float32(w), np.float32(nh) / np.float32(h)
         K = cam["K"]
@@ -110,13 +117,33 @@ def run_scene(ctx, folder, problems, needed, views, *, planar_prior, geom_iterat
     return int(sum(d[index[ref]].size for ref, _ in problems))
 
 
-def run_fusion(folder, problems, geom_consistency, device=0):
+def run_scene_acmm(ctx, folder, problems, views, *, geom_iterations, seed):
+    """The ACMM+NESP variant's main() minus fusion (hpm_run_scene_acmm), then
+    the files its ProcessProblem leaves (main.cpp:96-121)."""
+    if [ref for ref, _ in problems] != list(range(len(problems))):
+        raise hb.HpmError("the ACMM+NESP variant needs pair.txt to list views 0, 1, ... in order "
+                          "(the reference looks a source's scale up by its image id)")
+    d, n, c = ctx.run_scene_acmm([views[v][0] for v in range(len(problems))],
+                                 np.array([views[v][1] for v in range(len(problems))]),
+                                 [(ref, list(srcs)) for ref, srcs in problems], seed=seed,
+                                 geom_iterations=geom_iterations)
+    for ref, _ in problems:
+        out = os.path.join(folder, "ACMM_NESP", f"2333_{ref:08d}")
+        os.makedirs(out, exist_ok=True)
+        hb.write_dmb(os.path.join(out, "depths_geom.dmb"), d[ref])
+        hb.write_dmb(os.path.join(out, "normals.dmb"), n[ref])
+        hb.write_dmb(os.path.join(out, "costs.dmb"), c[ref])
+    return int(sum(x.size for x in d))
+
+
+def run_fusion(folder, problems, geom_consistency, device=0, tree="HPM", ply="HPM_model.ply"):
     """RunFusion (main.cpp:502-633) with RescaleImageAndCamera
     (HPM.cpp:187-208: OpenCV's 8-bit bilinear, reproduced by
-    hpm_resize_linear_u8); returns the point count."""
+    hpm_resize_linear_u8) over the maps under folder/tree; returns the point
+    count."""
     cams, depths, normals, colors = [], [], [], []
     for ref, _ in problems:
-        out = os.path.join(folder, "HPM", f"2333_{ref:08d}")
+        out = os.path.join(folder, tree, f"2333_{ref:08d}")
         d = hb.read_dmb(os.path.join(out, "depths_geom.dmb" if geom_consistency else "depths.dmb"))
         n = hb.read_dmb(os.path.join(out, "normals.dmb"))
         cam = hb.read_camera(os.path.join(folder, "cams", f"{ref:08d}_cam.txt")).copy()
@@ -145,7 +172,7 @@ def run_fusion(folder, problems, geom_consistency, device=0):
     # the reference indexes views by problem order (main.cpp:517-546)
     probs = [(i, list(srcs)) for i, (_, srcs) in enumerate(problems)]
     xyz, nrm, bgr = hb.fuse(np.array(cams), depths, normals, colors, probs, device)
-    hb.write_ply(os.path.join(folder, "HPM", "HPM_model.ply"), xyz, nrm, bgr)
+    hb.write_ply(os.path.join(folder, tree, ply), xyz, nrm, bgr)
     return len(xyz)
 
 
@@ -204,12 +231,14 @@ def main(argv=None):
     ap.add_argument("--no-reference-compat", action="store_true",
                     help="fix the reference's quirks listed at HpmParams in include/hpm_b200.h (default: keep the "
                          "reference's behaviour)")
+    ap.add_argument("--acmm", action="store_true",
+                    help="run the ACMM+NESP variant (coarse-to-fine image pyramid) into ACMM_NESP/ instead")
     a = ap.parse_args(argv)
     problems = hb.read_pair(os.path.join(a.dense_folder, "pair.txt"))
     print(f"There are {len(problems)} problems needed to be processed!")
+    form = "acmm" if a.acmm else ("per-problem" if a.per_problem else "scene")
     settings = (f"seed={a.seed} levels={a.levels} prior={int(not a.no_prior)} geom_iterations={a.geom_iterations} "
-                f"form={'per-problem' if a.per_problem else 'scene'}" + (" fix_quirks=1" if a.no_reference_compat
-                                                                         else ""))
+                f"form={form}" + (" fix_quirks=1" if a.no_reference_compat else ""))
     fix = a.no_reference_compat
     progress = Progress(a.dense_folder, settings, a.resume)
     count = [0]
@@ -246,7 +275,10 @@ def main(argv=None):
         return state["ctx"]
 
     try:
-        if a.per_problem:
+        if a.acmm:
+            step("scene", lambda: run_scene_acmm(ctx(), a.dense_folder, problems, state["views"],
+                                                 geom_iterations=a.geom_iterations, seed=a.seed))
+        elif a.per_problem:
             for p, (ref, srcs) in enumerate(problems):
                 step(f"A {ref}", lambda: process_problem(ctx(), a.dense_folder, ref, srcs, state["views"], geom=False,
                                                          planar_prior=not a.no_prior, multi_geometry=False,
@@ -266,8 +298,9 @@ def main(argv=None):
             state.pop("ctx").close()
         if not a.no_fusion:
             def fusion():
-                n = run_fusion(a.dense_folder, problems, a.geom_iterations > 0, a.device)
-                print(f"Fused {n} points into {a.dense_folder}/HPM/HPM_model.ply")
+                tree, ply = ("ACMM_NESP", "ACMM_NESP_model.ply") if a.acmm else ("HPM", "HPM_model.ply")
+                n = run_fusion(a.dense_folder, problems, a.geom_iterations > 0, a.device, tree, ply)
+                print(f"Fused {n} points into {a.dense_folder}/{tree}/{ply}")
                 return -n
             step("fusion", fusion)
     except Stopped:

@@ -91,6 +91,24 @@ typedef struct {
     int honour_max_iterations; /* 0 = reference behaviour (always 3) */
     uint64_t seed;             /* Philox key of this pass's random stream */
     int fix_quirks;            /* 0 = the reference's behaviour (see above) */
+    /* 0: the HPM-MVS kernels (HPM.cu).  1: the ACMM+NESP variant's kernels
+     * (ACMM+NESP/windows/ACMM.cu, ACMM::RunPatchMatch at ACMM.cu:1810-1862):
+     * max_iterations is honoured (ACMM.cu:1836), the geometric term weighs
+     * the current and the refined hypotheses by 0.2 (ACMM.cu:651, 1596) and
+     * the geometric cost is capped at 3 (ACMM.cu:496); no planar prior.  The
+     * reference declares the plane that collects the winner without a value
+     * (plane_hypotheses_now, ACMM.cu:1605) and reads it when no neighbour
+     * wins; here it starts from the current hypothesis. */
+    int variant;
+    /* variant 1 only: PatchMatchParams::hierarchy (ACMM.h:50).  The pass
+     * starts from the (world normal, depth) of hpm_set_hypotheses, upsampled
+     * by the caller, and keeps a pixel's update only where its cost ends 0.1
+     * below the initial cost of the plane with a zero normal and the depth
+     * as its distance (the reference's half-filled array, ACMM.cpp:707-713,
+     * ACMM.cu:596-597).  1: the maps were upsampled (params.upsample); 2: the
+     * maps have the pass's size, where the reference leaves that threshold
+     * unset (taken as 0: no update is kept). */
+    int hierarchy;
 } HpmParams;
 
 /* Fills p with the reference defaults (HPM.h:29-46). */
@@ -203,6 +221,37 @@ int hpm_run_scene_ex(hpm_ctx *ctx, int n_views, const float *const *images, cons
                      int n_problems, const int *ref_ids, const int *src_counts, const int *src_ids,
                      const HpmSceneOpts *opts, float *const *depths, float *const *normals, float *const *costs,
                      float *const *pass_depths, float *const *prior_depths);
+/* Options of the ACMM+NESP variant's scene run. */
+typedef struct {
+    int geom_iterations;     /* geometric iterations at every scale (the reference's: 2, main.cpp:319) */
+    uint64_t seed;           /* problem p's k-th pass draws from key seed + 7919 p + k */
+    int size_bound;          /* the coarsest scale has every longer side at most this (halvings of
+                                the image, main.cpp:38-64); 0 = the reference's 1000 */
+    int max_iterations;      /* PatchMatch iterations of the plain and hierarchy passes (0 = 3, ACMM.h:31) */
+    int geom_max_iterations; /* of the geometric passes (0 = 2, ACMM.cpp:437) */
+} HpmAcmmOpts;
+
+/* The ACMM+NESP variant's main() (ACMM+NESP/windows/main.cpp:298-384) minus
+ * fusion: NESP sampling inside ACMM's coarse-to-fine IMAGE pyramid.  Every
+ * problem's views are scaled down until their longer side is at most
+ * size_bound (ComputeMultiScaleSettings, main.cpp:35-71; images resized as
+ * InuputInitialization does, ACMM.cpp:489-516, cameras scaled with them).
+ * At the coarsest scale each problem runs a plain pass, then
+ * geom_iterations geometric passes over all problems; at every finer scale
+ * each problem's last geometric depth map is upsampled by the joint
+ * bilateral filter (main.cpp:126-152), a hierarchy pass starts from it
+ * (ACMM.cpp:663-719, HpmParams.hierarchy) and the geometric iterations
+ * follow.  Passes use HpmParams.variant 1.  The maps stay in HBM between
+ * passes (the reference writes .dmb files).  Problem p must have reference
+ * view p (ref_ids[p] == p): the reference looks a source's scale up by its
+ * image id (ACMM.cpp:490).  Views must be at most 3200 pixels on either
+ * side (the cap of ACMM.cpp:448-516 is the caller's job, as for
+ * hpm_run_scene), so the outputs have the input sizes.  Inputs and outputs
+ * as hpm_run_scene (host or device pointers; any output may be NULL). */
+int hpm_run_scene_acmm(hpm_ctx *ctx, int n_views, const float *const *images, const HpmCamera *cams,
+                       int n_problems, const int *ref_ids, const int *src_counts, const int *src_ids,
+                       const HpmAcmmOpts *opts, float *const *depths, float *const *normals, float *const *costs);
+
 /* Host threads of hpm_run_scene's pass set A (1 or 2, default 2; no
  * counterpart in the reference).  With 2, pass set A's problems go to this
  * context and a second one on the same device (created on first use, freed

@@ -339,6 +339,11 @@ typedef struct {
     uint32_t *views;
     const F4 *prior_planes;
     const uint32_t *masks;
+    /* ACMM+NESP variant (ACMM+NESP/windows/ACMM.cu): acmm selects its
+     * weights and update rule, hier its hierarchy pass (1 upsampled, 2 at the
+     * same size), pre_costs the hierarchy's acceptance threshold */
+    int acmm, hier;
+    float *pre_costs;
 } Ctx;
 
 /* ComputeBilateralNCC, HPM.cu:318-397 (patch 11, increment 2, sigma 5/3). */
@@ -470,9 +475,11 @@ static void project(const float *P, const OrCamera *c, float *pt, float *depth) 
 }
 
 /* ComputeGeomConsistencyCost, HPM.cu:483-508 */
-static float geom_cost(const OrCamera *ref, const OrCamera *src, const float *sdepth, F4 h, int px, int py)
+/* ComputeGeomConsistencyCost, HPM.cu:483-508; max_cost 5 there and 3 in the
+ * ACMM+NESP variant (ACMM.cu:496) */
+static float geom_cost_m(const OrCamera *ref, const OrCamera *src, const float *sdepth, F4 h, int px, int py,
+                         float max_cost)
 {
-    const float max_cost = 5.0f;
     const float depth = depth_from_plane(ref, h, px, py);
     float P[3], spt[2], sd;
     world_point(ref, (float)px, (float)py, depth, P);
@@ -487,6 +494,17 @@ static float geom_cost(const OrCamera *ref, const OrCamera *src, const float *sd
     return fminf(max_cost, sqrtf(dx * dx + dy * dy));
 }
 
+static float geom_cost(const OrCamera *ref, const OrCamera *src, const float *sdepth, F4 h, int px, int py)
+{
+    return geom_cost_m(ref, src, sdepth, h, px, py, 5.0f);
+}
+
+/* the pass's geometric term: weight w times the variant's capped cost */
+static float geom_term(const Ctx *c, int j, F4 h, int px, int py, float w)
+{
+    return w * geom_cost_m(&c->cams[0], &c->cams[j], c->depths[j], h, px, py, c->acmm ? 3.0f : 5.0f);
+}
+
 /* ------------------------------------------------------------------ */
 /* RandomInitialization, HPM.cu:510-558                                 */
 /* ------------------------------------------------------------------ */
@@ -497,7 +515,21 @@ static void init_pixel(Ctx *c, int px, int py)
     const OrCamera *cam = &c->cams[0];
     Rng rng;
     rng_init(&rng, c->seed, (uint32_t)center, 0u, c->salt);
-    if (c->geom) {
+    if (c->geom || c->hier) {
+        /* ACMM.cu:538-604: the hierarchy pass starts from the upsampled
+         * (world normal, depth).  Its acceptance threshold pre_costs is the
+         * initial cost of the plane held before the normal is filled in:
+         * normal (0, 0, 0), w = the depth itself (ACMM.cpp:707-713 sets only
+         * .w of a freshly allocated array, which is zero-filled); at the same
+         * size (upsample false) the reference leaves pre_costs unset, taken
+         * here as zero, which accepts no update. */
+        if (c->hier == 1) {
+            uint32_t v_unused;
+            F4 hz = {0.0f, 0.0f, 0.0f, c->planes[center].w};
+            c->pre_costs[center] = initial_cost(c, px, py, hz, &v_unused);
+        } else if (c->hier == 2) {
+            c->pre_costs[center] = 0.0f;
+        }
         F4 h = transform_normal_to_ref(cam, c->planes[center]);
         const float depth = h.w;
         h.w = distance_to_origin(cam, px, py, depth, h);
@@ -678,7 +710,7 @@ static void refine(Ctx *c, int px, int py, F4 *plane, float *depth, float *cost,
         for (int j = 0; j < c->n - 1; ++j) {
             if (vw[j] > 0) {
                 if (c->geom)
-                    tc += vw[j] * (cv[j] + 0.1f * geom_cost(cam, &c->cams[j + 1], c->depths[j + 1], t, px, py));
+                    tc += vw[j] * (cv[j] + geom_term(c, j + 1, t, px, py, c->acmm ? 0.2f : 0.1f));
                 else
                     tc += vw[j] * cv[j];
             }
@@ -823,8 +855,7 @@ static void propagate_pixel(Ctx *c, int px, int py, int iter)
             if (vw[j] > 0) {
                 if (c->geom) {
                     if (flag[i])
-                        fc[i] += vw[j] * (ca[i][j] + 0.1f * geom_cost(cam, &c->cams[j + 1], c->depths[j + 1],
-                                                                      c->planes[pos[i]], px, py));
+                        fc[i] += vw[j] * (ca[i][j] + geom_term(c, j + 1, c->planes[pos[i]], px, py, 0.1f));
                     else
                         fc[i] += vw[j] * (ca[i][j] + 0.1f * 5.0f);
                 } else {
@@ -849,14 +880,40 @@ static void propagate_pixel(Ctx *c, int px, int py, int iter)
     float cost_now = 0.0f;
     for (int i = 0; i < nv; ++i) {
         if (c->geom)
-            cost_now += vw[i] * (cvn[i] + 0.1f * geom_cost(cam, &c->cams[i + 1], c->depths[i + 1], c->planes[center],
-                                                           px, py));
+            cost_now += vw[i] * (cvn[i] + geom_term(c, i + 1, c->planes[center], px, py, c->acmm ? 0.2f : 0.1f));
         else
             cost_now += vw[i] * cvn[i];
     }
     cost_now /= wn;
     c->costs[center] = cost_now;
     float depth_now = depth_from_plane(cam, c->planes[center], px, py);
+
+    if (c->acmm) {
+        /* ACMM.cu:1602-1629: the winner is built in plane_hypotheses_now,
+         * which the reference declares without a value and reads when no
+         * direction wins; it starts here from the current hypothesis, the
+         * in-place update of HPM.cu:1686-1703 that the variant restructures.
+         * No planar prior and no NaN fallback; a hierarchy pass keeps the
+         * result only if it beats the upsampled plane's cost by 0.1. */
+        F4 now = c->planes[center];
+        float cost = cost_now;
+        if (flag[min_idx]) {
+            const float db = depth_from_plane(cam, c->planes[pos[min_idx]], px, py);
+            if (db >= c->dmin && db <= c->dmax && fc[min_idx] < cost_now) {
+                depth_now = db;
+                now = c->planes[pos[min_idx]];
+                cost = fc[min_idx];
+                c->views[center] = tsv;
+            }
+        }
+        float unused = 0.0f;
+        refine(c, px, py, &now, &depth_now, &cost, &rng, vw, wn, &unused);
+        if (!c->hier || cost < c->pre_costs[center] - 0.1f) {
+            c->costs[center] = cost;
+            c->planes[center] = now;
+        }
+        return;
+    }
 
     float restricted_cost = 0.0f;
     if (c->prior) {
@@ -1018,12 +1075,18 @@ int or_run_patchmatch(int n_img, const float *const *imgs, const OrCamera *cams,
     c.salt = o->salt;
     c.planes = (F4 *)planes_io;
     c.costs = costs_io;
+    c.acmm = o->variant == 1;
+    c.hier = c.acmm ? o->hierarchy : 0;
+    c.pre_costs = o->pre_costs;
+    if (c.hier && !c.pre_costs) return -3;
+    if (c.acmm && c.prior) return -4;
     const size_t npx = (size_t)c.W * c.H;
     uint32_t *views = views_io ? views_io : (uint32_t *)calloc(npx, sizeof(uint32_t));
     uint32_t *zero_masks = NULL;
     c.views = views;
     c.prior_planes = (const F4 *)prior_planes;
     c.masks = plane_masks;
+
     if (c.prior && !c.masks) {
         zero_masks = (uint32_t *)calloc(npx, sizeof(uint32_t));
         c.masks = zero_masks;
@@ -1109,6 +1172,13 @@ int or_jbu(const float *guide, int cols, int rows, const float *coarse_depth, co
     const int sr = rows / s_rows, sc = cols / s_cols;
     const int image_scale = sr > sc ? sr : sc;
     if (image_scale == 1) return 1;
+    return or_jbu_at_scale(guide, cols, rows, coarse_depth, coarse_normal, s_cols, s_rows, image_scale, out_depth,
+                           out_normal);
+}
+
+int or_jbu_at_scale(const float *guide, int cols, int rows, const float *coarse_depth, const float *coarse_normal,
+                    int s_cols, int s_rows, int image_scale, float *out_depth, float *out_normal)
+{
     const float scale = (float)(1.0 * s_cols / cols);
     const float sigmad = 0.50f, sigmar = 25.5f;
     const int win = image_scale * image_scale + 1;

@@ -49,6 +49,17 @@ typedef struct {
     uint32_t salt;        /* per-pass stream id */
     int half_steps;       /* propagation half-steps to run; the reference runs 6 */
     int finalize;         /* run GetDepthandNormal + the two filters */
+    /* The ACMM+NESP variant (ACMM+NESP/windows/ACMM.cu) when variant is 1:
+     * geometric weight 0.2 on the current and refined hypotheses and the
+     * geometric cost capped at 3 (ACMM.cu:496, 651, 1596); no planar prior;
+     * hierarchy 1 (an upsampled pass) or 2 (a pass at the size of the maps it
+     * starts from) starts from the (world normal, depth) in planes_io, writes
+     * the acceptance threshold of every pixel to pre_costs (caller's buffer,
+     * W x H floats) and keeps an update only where its cost is 0.1 below it
+     * (ACMM.cu:521-604, 1617-1629). */
+    int variant;
+    int hierarchy;
+    float *pre_costs;
 } OrRunOpts;
 
 /* 0: bilinear weight = floor(frac * 256) / 256; 1: round-to-nearest. */
@@ -87,6 +98,11 @@ int or_depth_normal_filter(const OrCamera *ref, float *planes_io, const float *c
 
 int or_jbu(const float *guide, int cols, int rows, const float *coarse_depth, const float *coarse_normal, int s_cols,
            int s_rows, float *out_depth, float *out_normal);
+/* The same weights at a given integer scale, also 1 (a 3 x 3 window): the
+ * normal average with which the ACMM+NESP variant's hierarchy pass starts
+ * (ACMM.cu:538-596) runs whatever the scale. */
+int or_jbu_at_scale(const float *guide, int cols, int rows, const float *coarse_depth, const float *coarse_normal,
+                    int s_cols, int s_rows, int image_scale, float *out_depth, float *out_normal);
 
 /* Raw Philox4x32-10 block: ctr4 is replaced by the output. */
 void or_philox4x32_10(uint32_t k0, uint32_t k1, uint32_t *ctr4);

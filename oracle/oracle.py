@@ -34,7 +34,8 @@ class OrRunOpts(ctypes.Structure):
     _fields_ = [("geom_consistency", ctypes.c_int), ("planar_prior", ctypes.c_int),
                 ("depth_min", ctypes.c_float), ("depth_max", ctypes.c_float),
                 ("seed", ctypes.c_uint64), ("salt", ctypes.c_uint32),
-                ("half_steps", ctypes.c_int), ("finalize", ctypes.c_int)]
+                ("half_steps", ctypes.c_int), ("finalize", ctypes.c_int),
+                ("variant", ctypes.c_int), ("hierarchy", ctypes.c_int), ("pre_costs", ctypes.c_void_p)]
 
 
 class RefRunOpts(ctypes.Structure):
@@ -173,8 +174,12 @@ def geom_costs(cams, depth_maps, planes) -> np.ndarray:
 
 def run_patchmatch(images, cams, *, depth_min, depth_max, seed=0, salt=0, geom=False, prior=False,
                    planes=None, costs=None, views=None, prior_planes=None, masks=None, depth_maps=None,
-                   half_steps=6, finalize=True):
-    """HPM::RunPatchMatch restated on the CPU; returns (planes, costs, views)."""
+                   half_steps=6, finalize=True, variant=0, hierarchy=0, pre_costs=None):
+    """HPM::RunPatchMatch restated on the CPU; returns (planes, costs, views).
+    variant 1: ACMM::RunPatchMatch of the ACMM+NESP variant; with hierarchy
+    (1 upsampled, 2 same size) planes hold the upsampled (world normal,
+    depth) and pre_costs, a float32 [H, W] array, receives the acceptance
+    thresholds."""
     imgs, arr = _img_ptrs(images)
     c = _cams(cams)
     h, w = imgs[0].shape
@@ -184,8 +189,12 @@ def run_patchmatch(images, cams, *, depth_min, depth_max, seed=0, salt=0, geom=F
              else np.array(costs, dtype=np.float32, copy=True, order="C"))
     views = (np.zeros((h, w), np.uint32) if views is None
              else np.array(views, dtype=np.uint32, copy=True, order="C"))
+    if hierarchy and (pre_costs is None or pre_costs.shape != (h, w) or pre_costs.dtype != np.float32
+                      or not pre_costs.flags.c_contiguous):
+        raise ValueError("run_patchmatch: hierarchy needs a float32 [H, W] pre_costs array")
     o = OrRunOpts(int(geom), int(prior), float(depth_min), float(depth_max), int(seed), int(salt),
-                  int(half_steps), int(finalize))
+                  int(half_steps), int(finalize), int(variant), int(hierarchy),
+                  None if pre_costs is None else pre_costs.ctypes.data)
     pp = None if prior_planes is None else np.ascontiguousarray(prior_planes, dtype=np.float32)
     mk = None if masks is None else np.ascontiguousarray(masks, dtype=np.uint32)
     dms, darr = (None, None) if depth_maps is None else _img_ptrs(depth_maps)
@@ -215,6 +224,19 @@ def jbu(guide, coarse_depth, coarse_normal):
     rc = lib().or_jbu(_p(guide), cols, rows, _p(cd), _p(cn), s_cols, s_rows, _p(od), _p(on))
     if rc == 1:
         return None, None
+    return od, on
+
+
+def jbu_at_scale(guide, coarse_depth, coarse_normal, image_scale):
+    """or_jbu_at_scale: the JBU's weights at a given integer scale (1 too)."""
+    guide = np.ascontiguousarray(guide, dtype=np.float32)
+    cd = np.ascontiguousarray(coarse_depth, dtype=np.float32)
+    cn = np.ascontiguousarray(coarse_normal, dtype=np.float32)
+    rows, cols = guide.shape
+    s_rows, s_cols = cd.shape
+    od = np.zeros((rows, cols), np.float32)
+    on = np.zeros((rows, cols, 3), np.float32)
+    lib().or_jbu_at_scale(_p(guide), cols, rows, _p(cd), _p(cn), s_cols, s_rows, int(image_scale), _p(od), _p(on))
     return od, on
 
 
