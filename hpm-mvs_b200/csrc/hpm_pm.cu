@@ -744,6 +744,10 @@ __device__ __forceinline__ bool same_plane(float4 p, float4 q)
  * update changes nothing in what is computed. */
 
 #define CAG(k, v) a.cand_costs[(size_t)((k) * S + (v)) * sl.nh + sl.hc]
+/* Hand-off stores use the streaming cache policy (st.global.cs, evict
+ * first): the rows are read once by the next kernel, and at ~0.5 GB a
+ * half-step they would otherwise push the source images out of L2. */
+#define CAG_PUT(k, v, x) __stcs(&CAG(k, v), (x))
 
 /* Where the cost row of direction k lives, 4 bits per direction in the
  * pixel's hand-off code (cand_flags): the row itself, the cost-vector cache
@@ -814,7 +818,7 @@ __device__ __forceinline__ void prop_dirs_body(const PMArgs &a, int iter, int px
         while (m) {
             const int k = __ffs(m) - 1;
             m &= m - 1;
-            CAG(k, v) = ncc_call(a, v + 1, px, py, a.planes[pos[k]], sWW, tid, rs);
+            CAG_PUT(k, v, ncc_call(a, v + 1, px, py, a.planes[pos[k]], sWW, tid, rs));
         }
     }
     if (a.counters && eval_mask) atomicAdd(&a.counters[0], (unsigned long long)(__popc(eval_mask) * S));
@@ -847,7 +851,7 @@ __device__ __forceinline__ void prop_dirs_body(const PMArgs &a, int iter, int px
 #pragma unroll
                 for (int k = 1; k < 8; ++k)
                     if (((code >> (4 * k)) & 15u) == 0u) {
-                        for (int v = 0; v < S; ++v) CAG(k, v) = dir_cost(a, code, 0, v, S, sl);
+                        for (int v = 0; v < S; ++v) CAG_PUT(k, v, dir_cost(a, code, 0, v, S, sl));
                         code = (code & ~(15u << (4 * k))) | (kRowOwn << (4 * k));
                     }
             }
@@ -876,12 +880,12 @@ __device__ __forceinline__ void prop_dirs_body(const PMArgs &a, int iter, int px
     for (int k = 0; k < 8; ++k) {
         const uint32_t src = (code >> (4 * k)) & 15u;
         if (src == kRowOwn || src == kRowNone) continue;
-        for (int v = 0; v < S; ++v) CAG(k, v) = src == kRowCache ? *cache_at(a, v, sl) : CAG(src, v);
+        for (int v = 0; v < S; ++v) CAG_PUT(k, v, src == kRowCache ? *cache_at(a, v, sl) : CAG(src, v));
         code = (code & ~(15u << (4 * k))) | (kRowOwn << (4 * k));
     }
 #pragma unroll
-    for (int k = 0; k < 8; ++k) a.cand_pos[(size_t)k * sl.nh + sl.hc] = pos[k];
-    a.cand_flags[sl.hc] = code;
+    for (int k = 0; k < 8; ++k) __stcs(&a.cand_pos[(size_t)k * sl.nh + sl.hc], pos[k]);
+    __stcs(&a.cand_flags[sl.hc], code);
 }
 
 /* WW: pixels of one colour per warp row (the half-step tile, tuned per view
@@ -1195,7 +1199,7 @@ __device__ __forceinline__ void prop_refine_body(const PMArgs &a, int iter, int 
                  * same centre back to back in the texture cache */
                 const int i = (0x543120 >> (4 * k)) & 15;
                 const float c = ncc_call(a, v + 1, px, py, cand[i], sWW, tid, rs);
-                CAG(kRefineRow + i, v) = c;
+                CAG_PUT(kRefineRow + i, v, c);
                 if (selected) {
                     if (a.geom)
                         tc[i] += w * (c + kGeomW * geom_cost(a, v + 1, cand[i], px, py));
@@ -1260,6 +1264,7 @@ __global__ void __launch_bounds__(kBlock, HPM_P2_MIN_BLOCKS) k_prop_refine(const
     half_step_pixel_at(blockIdx.x, blockIdx.y, WW, color, px, py);
     prop_refine_body<SMAX, PROP, ACMM>(a, iter, px, py, sWW, tid);
 }
+#undef CAG_PUT
 #undef CAG
 
 /* GetDepthandNormal, HPM.cu:1751-1764 */

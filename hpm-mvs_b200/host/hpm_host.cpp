@@ -32,10 +32,10 @@ std::string id_path(const std::string &folder, int id, const char *suffix)
     return s.str();
 }
 
-std::string result_folder(const std::string &dense_folder, int ref_id)
+std::string result_folder(const std::string &dense_folder, int ref_id, const char *tree = "HPM")
 {
     std::ostringstream s;
-    s << dense_folder << "/HPM/2333_" << std::setw(8) << std::setfill('0') << ref_id;
+    s << dense_folder << "/" << tree << "/2333_" << std::setw(8) << std::setfill('0') << ref_id;
     return s.str();
 }
 
@@ -475,8 +475,22 @@ void HPM::ReleaseProblemHostMemory()
     std::vector<float>().swap(seed_costs_);
 }
 
+static long long fuse_tree(const std::string &dense_folder, const std::vector<Problem> &problems,
+                           bool geom_consistency, int device, const char *tree, const char *ply_name);
+
 long long RunFusion(const std::string &dense_folder, const std::vector<Problem> &problems, bool geom_consistency,
                     int device)
+{
+    return fuse_tree(dense_folder, problems, geom_consistency, device, "HPM", "HPM_model.ply");
+}
+
+long long RunFusionAcmm(const std::string &dense_folder, const std::vector<Problem> &problems, int device)
+{
+    return fuse_tree(dense_folder, problems, true, device, "ACMM_NESP", "ACMM_NESP_model.ply");
+}
+
+static long long fuse_tree(const std::string &dense_folder, const std::vector<Problem> &problems,
+                           bool geom_consistency, int device, const char *tree, const char *ply_name)
 {
     const int n = (int)problems.size();
     std::vector<HpmCamera> cams(n);
@@ -486,7 +500,7 @@ long long RunFusion(const std::string &dense_folder, const std::vector<Problem> 
     for (int i = 0; i < n; ++i) {
         /* the reference indexes views by problem order (main.cpp:517-546) */
         const int id = problems[i].ref_image_id;
-        const std::string folder = result_folder(dense_folder, id);
+        const std::string folder = result_folder(dense_folder, id, tree);
         int w = 0, h = 0;
         depths[i] = read_dmb(folder + (geom_consistency ? "/depths_geom.dmb" : "/depths.dmb"), &w, &h, 1);
         normals[i] = read_dmb(folder + "/normals.dmb", &w, &h, 3);
@@ -532,7 +546,7 @@ long long RunFusion(const std::string &dense_folder, const std::vector<Problem> 
     int rc = hpm_fuse(device, n, cams.data(), dp.data(), np_.data(), cp.data(), n, refs.data(), counts.data(),
                       srcs.data(), xyz.data(), nrm.data(), col.data(), (long long)cap, &count);
     if (rc != HPM_OK) throw Error(rc, "hpm_fuse");
-    const std::string ply = dense_folder + "/HPM/HPM_model.ply";
+    const std::string ply = dense_folder + "/" + tree + "/" + ply_name;
     rc = hpm_write_ply(ply.c_str(), count, xyz.data(), nrm.data(), col.data());
     if (rc != HPM_OK) throw Error(rc, "cannot write " + ply);
     return count;
@@ -670,6 +684,64 @@ Progress::Progress(const std::string &dense_folder, const std::string &settings,
     out << head << "\n";
     out.flush();
     if (!out) throw Error(HPM_ERR_IO, "cannot write " + path_);
+}
+
+long long RunSceneAcmm(const std::string &dense_folder, const std::vector<Problem> &problems, int geom_iterations,
+                       uint64_t seed, int device)
+{
+    const size_t n = problems.size();
+    for (size_t p = 0; p < n; ++p) {
+        if (problems[p].ref_image_id != (int)p)
+            throw Error(HPM_ERR_ARG, "the ACMM+NESP variant needs pair.txt to list views 0, 1, ... in order (the "
+                                     "reference looks a source's scale up by its image id)");
+        if ((int)problems[p].src_image_ids.size() + 1 > HPM_MAX_IMAGES)
+            throw Error(HPM_ERR_ARG, "more than 32 source images");
+    }
+    const unsigned threads = std::max(1u, std::thread::hardware_concurrency());
+    std::vector<std::vector<float>> images(n);
+    std::vector<HpmCamera> cams(n);
+    parallel_for(n, threads, [&](size_t i) { load_view(dense_folder, (int)i, images[i], cams[i]); });
+    std::vector<int> refs(n), counts(n), srcs(n * (HPM_MAX_IMAGES - 1), 0);
+    std::vector<std::vector<float>> depth(n), normal(n), cost(n);
+    std::vector<const float *> img_ptr(n);
+    std::vector<float *> pd(n), pn(n), pc(n);
+    for (size_t p = 0; p < n; ++p) {
+        refs[p] = (int)p;
+        counts[p] = (int)problems[p].src_image_ids.size();
+        for (int j = 0; j < counts[p]; ++j) srcs[p * (HPM_MAX_IMAGES - 1) + j] = problems[p].src_image_ids[j];
+        const size_t npx = (size_t)cams[p].width * cams[p].height;
+        depth[p].resize(npx);
+        normal[p].resize(3 * npx);
+        cost[p].resize(npx);
+        img_ptr[p] = images[p].data();
+        pd[p] = depth[p].data();
+        pn[p] = normal[p].data();
+        pc[p] = cost[p].data();
+    }
+    hpm_ctx *ctx = nullptr;
+    int rc = hpm_create(&ctx, device);
+    if (rc != HPM_OK) throw Error(rc, "hpm_create");
+    struct Destroy {
+        hpm_ctx *c;
+        ~Destroy() { hpm_destroy(c); }
+    } destroy{ctx};
+    const HpmAcmmOpts o = {geom_iterations, seed, 0, 0, 0};
+    rc = hpm_run_scene_acmm(ctx, (int)n, img_ptr.data(), cams.data(), (int)n, refs.data(), counts.data(),
+                            srcs.data(), &o, pd.data(), pn.data(), pc.data());
+    if (rc != HPM_OK) throw Error(rc, std::string("hpm_run_scene_acmm: ") + hpm_last_error(ctx));
+    /* the files the variant's ProcessProblem leaves (ACMM+NESP/windows/main.cpp:96-121) */
+    make_dir(dense_folder + "/ACMM_NESP");
+    long long pixels = 0;
+    for (size_t p = 0; p < n; ++p) pixels += (long long)depth[p].size();
+    parallel_for(n, threads, [&](size_t p) {
+        const int w = cams[p].width, h = cams[p].height;
+        const std::string folder = result_folder(dense_folder, (int)p, "ACMM_NESP");
+        make_dir(folder);
+        write_dmb(folder + (geom_iterations > 0 ? "/depths_geom.dmb" : "/depths.dmb"), depth[p], w, h, 1);
+        write_dmb(folder + "/normals.dmb", normal[p], w, h, 3);
+        write_dmb(folder + "/costs.dmb", cost[p], w, h, 1);
+    });
+    return pixels;
 }
 
 bool Progress::done(const std::string &step) const

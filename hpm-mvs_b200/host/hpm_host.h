@@ -127,6 +127,16 @@ private:
  * (HPM.cpp:187-208, OpenCV's 8-bit bilinear, byte for byte). */
 long long RunFusion(const std::string &dense_folder, const std::vector<Problem> &problems, bool geom_consistency,
                     int device = 0);
+/* The same over the ACMM+NESP variant's tree: ACMM_NESP/2333_%08d/ into
+ * ACMM_NESP/ACMM_NESP_model.ply (ACMM+NESP/windows/main.cpp:154-297). */
+long long RunFusionAcmm(const std::string &dense_folder, const std::vector<Problem> &problems, int device = 0);
+
+/* The ACMM+NESP variant's main() minus fusion (ACMM+NESP/windows/main.cpp:
+ * 299-384) in one hpm_run_scene_acmm call, then its files for every problem
+ * (ACMM_NESP/2333_%08d/{depths_geom,normals,costs}.dmb).  Problem p must have
+ * reference view p.  Returns the depth pixels of all reference views. */
+long long RunSceneAcmm(const std::string &dense_folder, const std::vector<Problem> &problems, int geom_iterations,
+                       uint64_t seed, int device);
 
 /* ProcessProblem (main.cpp:35-499): one reference view, outputs written
  * under dense_folder/HPM/2333_%08d/; returns the depth pixels written. */

@@ -30,6 +30,11 @@
  * The reference's behaviour is kept throughout by default (its quirks
  * included); --no-reference-compat fixes the quirks listed at HpmParams in
  * hpm_b200.h.
+ *
+ * --acmm runs the reference's other product instead, the ACMM+NESP
+ * variant's main() (ACMM+NESP/windows/main.cpp:299-384): coarse-to-fine
+ * over an image pyramid (RunSceneAcmm), files under ACMM_NESP/2333_%08d/,
+ * fused into ACMM_NESP/ACMM_NESP_model.ply.
  */
 #include <chrono>
 #include <cstdlib>
@@ -47,14 +52,14 @@ int main(int argc, char **argv)
     if (argc < 2 || !strcmp(argv[1], "-h") || !strcmp(argv[1], "--help")) {
         std::cout << "USAGE: hpm_mvs dense_folder [--seed S] [--levels K] [--device D] [--no-prior] "
                      "[--geom-iterations G] [--no-fusion] [--per-problem] [--resume] [--stop-after N] "
-                     "[--no-reference-compat] [--log PATH]"
+                     "[--no-reference-compat] [--log PATH] [--acmm]"
                   << std::endl;
         return argc < 2 ? -1 : 0;
     }
     const std::string dense_folder = argv[1];
     uint64_t seed = 0;
     int levels = -1, device = 0, geom_iterations = 2;
-    bool planar_prior = true, fusion = true, per_problem = false, resume = false, compat = true;
+    bool planar_prior = true, fusion = true, per_problem = false, resume = false, compat = true, acmm = false;
     long long stop_after = -1;
     std::string log_path;
     for (int i = 2; i < argc; ++i) {
@@ -84,6 +89,8 @@ int main(int argc, char **argv)
             resume = true;
         else if (a == "--no-reference-compat")
             compat = false;
+        else if (a == "--acmm")
+            acmm = true;
         else if (a == "--log")
             log_path = next("--log");
         else if (a == "--stop-after")
@@ -99,7 +106,8 @@ int main(int argc, char **argv)
         std::cout << "There are " << problems.size() << " problems needed to be processed!" << std::endl;
         std::ostringstream settings;
         settings << "seed=" << seed << " levels=" << levels << " prior=" << planar_prior
-                 << " geom_iterations=" << geom_iterations << " form=" << (per_problem ? "per-problem" : "scene")
+                 << " geom_iterations=" << geom_iterations << " form="
+                 << (acmm ? "acmm" : (per_problem ? "per-problem" : "scene"))
                  << (compat ? "" : " fix_quirks=1");
         hpm_host::Progress progress(dense_folder, settings.str(), resume);
         long long steps = 0;
@@ -130,7 +138,12 @@ int main(int argc, char **argv)
             std::cout << "Stopped after " << steps << " steps; --resume continues" << std::endl;
             return 0;
         };
-        if (!per_problem) {
+        if (acmm) {
+            if (!step("scene", [&] {
+                    return hpm_host::RunSceneAcmm(dense_folder, problems, geom_iterations, seed, device);
+                }))
+                return stopped();
+        } else if (!per_problem) {
             if (!step("scene", [&] {
                     return hpm_host::RunScene(dense_folder, problems, planar_prior, geom_iterations, seed, levels,
                                               device, compat);
@@ -153,8 +166,10 @@ int main(int argc, char **argv)
         }
         if (fusion &&
             !step("fusion", [&] {
-                const long long n = hpm_host::RunFusion(dense_folder, problems, geom_iterations > 0, device);
-                std::cout << "Fused " << n << " points into " << dense_folder << "/HPM/HPM_model.ply" << std::endl;
+                const long long n = acmm ? hpm_host::RunFusionAcmm(dense_folder, problems, device)
+                                         : hpm_host::RunFusion(dense_folder, problems, geom_iterations > 0, device);
+                std::cout << "Fused " << n << " points into " << dense_folder
+                          << (acmm ? "/ACMM_NESP/ACMM_NESP_model.ply" : "/HPM/HPM_model.ply") << std::endl;
                 return -n;
             }))
             return stopped();

@@ -218,17 +218,22 @@ def test_scene_coarse_to_fine_beats_one_scale():
 
 
 def test_front_end_writes_the_variants_files(tmp_path):
-    """hpm_mvs.py --acmm on a dense folder: the ACMM+NESP tree of .dmb files
-    equals hpm_run_scene_acmm on the views and cameras read back, and the
-    fusion writes ACMM_NESP/ACMM_NESP_model.ply."""
+    """hpm_mvs.py --acmm and the C++ hpm_mvs --acmm on a dense folder: the
+    ACMM+NESP tree of .dmb files equals hpm_run_scene_acmm on the views and
+    cameras read back, in both front ends, and the fusion writes
+    ACMM_NESP/ACMM_NESP_model.ply (the same bytes from both)."""
     import subprocess
 
     sc = syn.make_scene(6, 96, 72, 4, n_planes=5)
-    f = str(tmp_path / "scene")
+    f, g = str(tmp_path / "scene"), str(tmp_path / "scene_cpp")
     syn.write_dense_folder(sc, f)
+    syn.write_dense_folder(sc, g)
     here = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "hpm-mvs_b200")
     r = subprocess.run([sys.executable, os.path.join(here, "hpm_mvs.py"), f, "--acmm", "--seed", "5"],
                        capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr
+    r = subprocess.run([os.path.join(here, "hpm_mvs"), g, "--acmm", "--seed", "5"], capture_output=True, text=True,
+                       timeout=600)
     assert r.returncode == 0, r.stderr
     sys.path.insert(0, here)
     import hpm_mvs
@@ -238,8 +243,10 @@ def test_front_end_writes_the_variants_files(tmp_path):
     with hb.Context() as ctx:
         d, n, c = ctx.run_scene_acmm([v[0] for v in views], np.array([v[1] for v in views]), pairs, seed=5)
     for v in range(4):
-        out = os.path.join(f, "ACMM_NESP", f"2333_{v:08d}")
-        np.testing.assert_array_equal(hb.read_dmb(os.path.join(out, "depths_geom.dmb")), d[v])
-        np.testing.assert_array_equal(hb.read_dmb(os.path.join(out, "normals.dmb")), n[v])
-        np.testing.assert_array_equal(hb.read_dmb(os.path.join(out, "costs.dmb")), c[v])
-    assert os.path.getsize(os.path.join(f, "ACMM_NESP", "ACMM_NESP_model.ply")) > 1000
+        for root in (f, g):
+            out = os.path.join(root, "ACMM_NESP", f"2333_{v:08d}")
+            np.testing.assert_array_equal(hb.read_dmb(os.path.join(out, "depths_geom.dmb")), d[v])
+            np.testing.assert_array_equal(hb.read_dmb(os.path.join(out, "normals.dmb")), n[v])
+            np.testing.assert_array_equal(hb.read_dmb(os.path.join(out, "costs.dmb")), c[v])
+    ply = [open(os.path.join(root, "ACMM_NESP", "ACMM_NESP_model.ply"), "rb").read() for root in (f, g)]
+    assert len(ply[0]) > 1000 and ply[0] == ply[1]
