@@ -22,6 +22,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libhpm_ref.so")
+ACMM_REF_SO = os.path.join(HERE, "_ref", "libacmm_ref.so")
 
 CAMERA_DTYPE = np.dtype(
     [("K", "<f4", 9), ("R", "<f4", 9), ("t", "<f4", 3), ("height", "<i4"), ("width", "<i4"),
@@ -75,6 +76,41 @@ def ref() -> ctypes.CDLL:
     if _ref is None:
         _ref = ctypes.CDLL(REF_SO)
     return _ref
+
+
+_acmm_ref = None
+
+
+def acmm_ref_available() -> bool:
+    return os.path.exists(ACMM_REF_SO)
+
+
+def ref_acmm_hier_init(images, cams, planes, scaled):
+    """The reference's own RandomInitialization of an ACMM+NESP hierarchy
+    pass with upsample set (ACMM.cu:538-604, oracle/_ref/libacmm_ref.so on a
+    GPU).  planes: [H, W, 4] as the host leaves them ((0, 0, 0, depth));
+    scaled: [sh, sw, 4] (previous scale's world normal, cost).  Returns
+    (planes, costs, pre_costs, selected views)."""
+    global _acmm_ref
+    if _acmm_ref is None:
+        _acmm_ref = ctypes.CDLL(ACMM_REF_SO)
+    imgs, arr = _img_ptrs(images)
+    c = _cams(cams)
+    h, w = imgs[0].shape
+    pl = np.ascontiguousarray(planes, dtype=np.float32)
+    sc = np.ascontiguousarray(scaled, dtype=np.float32)
+    cam0 = np.asarray(cams)[0]
+    dmin = np.float32(cam0["depth_min"]) * np.float32(0.6)
+    dmax = np.float32(cam0["depth_max"]) * np.float32(1.2)
+    op = np.empty((h, w, 4), np.float32)
+    oc = np.empty((h, w), np.float32)
+    pre = np.empty((h, w), np.float32)
+    ov = np.empty((h, w), np.uint32)
+    rc = _acmm_ref.acmm_ref_hier_init(len(imgs), arr, _p(c), _p(pl), _p(sc), sc.shape[1], sc.shape[0],
+                                      ctypes.c_float(dmin), ctypes.c_float(dmax), _p(op), _p(oc), _p(pre), _p(ov))
+    if rc != 0:
+        raise RuntimeError(f"acmm_ref_hier_init failed: {rc}")
+    return op, oc, pre, ov
 
 
 def _p(a: np.ndarray):

@@ -23,9 +23,14 @@ outputs for small seeded inputs:
                   images guards the generator); outputs are kept at 4096
                   sampled pixels, plus the reference's whole-pass accuracy
                   and kernel times over four seeds.
+  acmm_hier.npz   the ACMM+NESP variant's RandomInitialization of a
+                  hierarchy pass (ACMM+NESP/windows/ACMM.cu:538-604: JBU
+                  average of the previous scale's normals, the threshold
+                  pre_costs, the initial cost), from the reference's own
+                  ACMM.cu compiled for sm_100a (oracle/_ref/libacmm_ref.so)
 
 Usage (on a GPU machine, from the repository root):
-    python tests/golden/make_golden.py [--out tests/golden] [--only small|bench]
+    python tests/golden/make_golden.py [--out tests/golden] [--only small|bench|acmm]
 """
 from __future__ import annotations
 
@@ -120,6 +125,35 @@ N_SAMPLES = 4096
 STAT_SEEDS = (100, 101, 102, 103)
 
 
+def acmm_hier_inputs():
+    """The ACMM+NESP hierarchy case: 5 views of 128x96; the previous
+    scale's world normals (ground truth, perturbed) and costs at 64x48; the
+    upsampled depth at 128x96 (ground truth, perturbed).  Returns (scene, ref
+    view, images, cameras, planes as the host leaves them ((0, 0, 0, depth)),
+    scaled maps (normal, cost))."""
+    sc = syn.make_scene(31, 128, 96, 5)
+    ref = 2
+    imgs, cams = syn.view_set(sc, ref)
+    rng = np.random.default_rng(31)
+    n = sc.gt_normal[ref][::2, ::2] + rng.normal(0, 0.1, (48, 64, 3))
+    n = (n / np.linalg.norm(n, axis=-1, keepdims=True)).astype(np.float32)
+    cost = rng.uniform(0, 1, (48, 64)).astype(np.float32)
+    scaled = np.concatenate([n, cost[..., None]], -1).astype(np.float32)
+    planes = np.zeros((96, 128, 4), np.float32)
+    planes[..., 3] = sc.gt_depth[ref] * rng.uniform(0.95, 1.05, (96, 128)).astype(np.float32)
+    return sc, ref, imgs, cams, planes, scaled
+
+
+def acmm_case(out_dir):
+    if not orc.acmm_ref_available():
+        raise SystemExit("oracle/_ref/libacmm_ref.so is missing: build it with `make -C oracle acmm`")
+    sc, ref, imgs, cams, planes, scaled = acmm_hier_inputs()
+    op, oc, pre, ov = orc.ref_acmm_hier_init(imgs, cams, planes, scaled)
+    np.savez_compressed(os.path.join(out_dir, "acmm_hier.npz"), images_sha256=images_sha256(imgs), planes=op,
+                        costs=oc, pre_costs=pre, views=ov)
+    print("acmm_hier: finite planes", float(np.isfinite(op).all(-1).mean()), "mean pre", float(np.nanmean(pre)))
+
+
 def images_sha256(imgs):
     h = hashlib.sha256()
     for i in imgs:
@@ -191,9 +225,13 @@ def bench_cases(out_dir):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", default=os.path.join(ROOT, "tests", "golden"))
-    ap.add_argument("--only", choices=["small", "bench"], default=None)
+    ap.add_argument("--only", choices=["small", "bench", "acmm"], default=None)
     args = ap.parse_args()
     os.makedirs(args.out, exist_ok=True)
+    if args.only in (None, "acmm"):
+        acmm_case(args.out)
+    if args.only == "acmm":
+        return
     if not orc.ref_available():
         raise SystemExit("oracle/_ref/libhpm_ref.so is missing: build it with `make -C oracle ref`")
     if args.only != "small":

@@ -84,3 +84,48 @@ def test_small_scene_two_scales():
     acc = [syn.depth_accuracy(d[v], sc.gt_depth[v]) for v in range(4)]
     assert np.mean(acc) > 0.5, acc
     assert all(x.shape == (72, 96) for x in d)
+
+
+def _hier_golden():
+    import pytest
+
+    from conftest import GOLDEN, golden
+
+    path = os.path.join(GOLDEN, "acmm_hier.npz")
+    if not os.path.exists(path):
+        pytest.skip("acmm_hier.npz not generated yet (tests/golden/make_golden.py --only acmm, on a GPU)")
+    sys.path.insert(0, GOLDEN)
+    import make_golden as mg
+
+    g = golden("acmm_hier.npz")
+    sc, ref, imgs, cams, planes, scaled = mg.acmm_hier_inputs()
+    assert mg.images_sha256(imgs) == str(g["images_sha256"]), "scene generator no longer reproduces the fixture"
+    return g, imgs, cams, planes, scaled
+
+
+def test_hierarchy_init_matches_reference():
+    """The oracle's hierarchy initialisation against the reference's own
+    RandomInitialization (ACMM.cu:538-604, run by oracle/_ref/libacmm_ref.so
+    on a B200 for the fixture): the previous scale's normals averaged with
+    the JBU's weights, turned to the reference frame with the depth of
+    depths.dmb; the threshold pre_costs from the zero-normal plane; the
+    initial cost and views.  NCC values within the golden tolerances of the
+    HPM-MVS kernels (a tap near a 1/256 weight step may round the other
+    way); planes within FP32 rounding of the reference's double-precision
+    JBU weights."""
+    g, imgs, cams, planes, scaled = _hier_golden()
+    _, n_up = orc.jbu_at_scale(imgs[0], scaled[..., 3], scaled[..., :3], 2)
+    start = np.concatenate([n_up, planes[..., 3:]], -1).astype(np.float32)
+    cam0 = cams[0]
+    dmin = np.float32(cam0["depth_min"]) * np.float32(0.6)
+    dmax = np.float32(cam0["depth_max"]) * np.float32(1.2)
+    pre = np.zeros(planes.shape[:2], np.float32)
+    op, oc, ov = orc.run_patchmatch(imgs, cams, depth_min=dmin, depth_max=dmax, planes=start, half_steps=0,
+                                    finalize=False, variant=1, hierarchy=1, pre_costs=pre)
+    same = np.isclose(op, g["planes"], rtol=1e-4, atol=1e-5).all(-1)
+    assert same.mean() >= 0.995, same.mean()
+    for got, want in ((oc, g["costs"]), (pre, g["pre_costs"])):
+        d = np.abs(got.astype(np.float64) - want)
+        d = d[np.isfinite(d)]
+        assert d.mean() <= 1e-4 and (d > 1e-3).mean() <= 0.01 and d.max() <= 2e-2, (d.mean(), d.max())
+    assert (ov == g["views"]).mean() >= 0.98

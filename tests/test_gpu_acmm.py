@@ -250,3 +250,34 @@ def test_front_end_writes_the_variants_files(tmp_path):
             np.testing.assert_array_equal(hb.read_dmb(os.path.join(out, "costs.dmb")), c[v])
     ply = [open(os.path.join(root, "ACMM_NESP", "ACMM_NESP_model.ply"), "rb").read() for root in (f, g)]
     assert len(ply[0]) > 1000 and ply[0] == ply[1]
+
+
+def test_hierarchy_init_matches_reference():
+    """The product's hierarchy initialisation (k_jbu for the normals, then
+    k_init with hierarchy 1) against the reference's own RandomInitialization
+    (ACMM.cu:538-604; tests/golden/acmm_hier.npz, made by oracle/_ref on a
+    B200), with the tolerances of tests/test_acmm.py."""
+    from conftest import GOLDEN
+
+    if not os.path.exists(os.path.join(GOLDEN, "acmm_hier.npz")):
+        pytest.skip("acmm_hier.npz not generated yet")
+    sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
+    import test_acmm
+
+    g, imgs, cams, planes, scaled = test_acmm._hier_golden()
+    cam0 = cams[0]
+    dmin = float(np.float32(cam0["depth_min"]) * np.float32(0.6))
+    dmax = float(np.float32(cam0["depth_max"]) * np.float32(1.2))
+    with hb.Context() as ctx:
+        _, n_up = ctx.jbu(imgs[0], np.ascontiguousarray(scaled[..., 3]), np.ascontiguousarray(scaled[..., :3]))
+        ctx.set_views(imgs, cams)
+        ctx.set_hypotheses(np.concatenate([n_up, planes[..., 3:]], -1).astype(np.float32))
+        ctx.run_partial(hb.default_params(dmin, dmax, variant=1, hierarchy=1), 0, False)
+        gp, gc = ctx.get_result()
+        gv = ctx.get_selected_views()
+    same = np.isclose(gp, g["planes"], rtol=1e-4, atol=1e-5).all(-1)
+    assert same.mean() >= 0.995, same.mean()
+    d = np.abs(gc.astype(np.float64) - g["costs"])
+    d = d[np.isfinite(d)]
+    assert d.mean() <= 1e-4 and (d > 1e-3).mean() <= 0.01 and d.max() <= 2e-2, (d.mean(), d.max())
+    assert (gv == g["views"]).mean() >= 0.98
