@@ -238,7 +238,8 @@ extern "C" int hpm_run_scene_acmm(hpm_ctx *c, int n_views, const float *const *i
             if (scale > 1)
                 CK(cudaMemcpyAsync(m.depth[p], m.up_depth, sizeof(float) * np, cudaMemcpyDeviceToDevice, s),
                    "depths.dmb");
-            /* (upsampled normal, depth of depths.dmb) */
+            /* the upsampled normals become the view's normal map; the
+             * split's depth output lands in the JBU scratch, unused */
             CK(flow_split_state(m.up_normal, (int)np, m.up_depth, m.normal[p], s), "normals");
         }
         CK(flow_pack4(m.depth[p], m.normal[p], (int)np, planes, s), "planes");

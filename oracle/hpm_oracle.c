@@ -892,7 +892,7 @@ static void propagate_pixel(Ctx *c, int px, int py, int iter)
         /* ACMM.cu:1602-1629: the winner is built in plane_hypotheses_now,
          * which the reference declares without a value and reads when no
          * direction wins; it starts here from the current hypothesis, the
-         * in-place update of HPM.cu:1686-1703 that the variant restructures.
+         * in-place update of HPM.cu:1707-1724 that the variant restructures.
          * No planar prior and no NaN fallback; a hierarchy pass keeps the
          * result only if it beats the upsampled plane's cost by 0.1. */
         F4 now = c->planes[center];

@@ -96,6 +96,7 @@ def test_null_context_is_an_argument_error():
     assert L.hpm_clear_prior(None) == -1
     assert L.hpm_get_result(None, None, None) == -1
     assert L.hpm_create(None, 0) == -1
+    assert L.hpm_run_scene_acmm(None, 2, None, None, 2, None, None, None, None, None, None, None) == -1
 
 
 @pytest.mark.skipif(gpu_available(), reason="checks the behaviour on a machine without a GPU")
@@ -108,6 +109,8 @@ def test_create_without_gpu_reports_cuda_error():
 def test_default_params_are_the_reference_defaults():
     p = hb.default_params(1.2, 9.6)
     assert (p.max_iterations, p.patch_size, p.radius_increment, p.top_k) == (3, 11, 2, 4)
+    # the HPM-MVS kernels unless the ACMM+NESP variant is asked for
+    assert (p.variant, p.hierarchy) == (0, 0)
     assert (p.sigma_spatial, p.sigma_color) == (5.0, 3.0)
     assert p.geom_consistency == 0 and p.planar_prior == 0
 
