@@ -281,3 +281,25 @@ def test_hierarchy_init_matches_reference():
     d = d[np.isfinite(d)]
     assert d.mean() <= 1e-4 and (d > 1e-3).mean() <= 0.01 and d.max() <= 2e-2, (d.mean(), d.max())
     assert (gv == g["views"]).mean() >= 0.98
+
+
+def test_scene_of_mixed_sizes_matches_oracle_flow():
+    """Views of three sizes: each problem has its own number of scales (the
+    reference's rule per view, ACMM.cpp:483-516), so a view that is already
+    at its final size when the others are upsampled runs its hierarchy pass
+    at the same size: JBU weights at scale 1 for the normals and the depth of
+    its last non-geometric pass (RunJBU returns early, ACMM.cpp:810-813)."""
+    sizes = [(128, 96), (64, 48), (128, 96), (96, 64), (128, 96)]
+    sc = syn.make_scene(8, 128, 96, 5, n_planes=6, sizes=sizes)
+    imgs = [i.astype(np.float32) for i in sc.images]
+    pairs = [(v, [int(s) for s in sc.pairs[v][1]]) for v in range(5)]
+    with hb.Context() as ctx:
+        gd, gn, gc = ctx.run_scene_acmm(imgs, sc.cams, pairs, seed=5, size_bound=64)
+    od, on, oc, scales = acmm_flow.run_scene(imgs, sc.cams, pairs, seed=5, size_bound=64)
+    assert scales == [[64, 64, 64, 48, 64], [128, 64, 128, 96, 128]]
+    acc_g = np.array([syn.depth_accuracy(gd[v], sc.gt_depth[v]) for v in range(5)])
+    acc_o = np.array([syn.depth_accuracy(od[v], sc.gt_depth[v]) for v in range(5)])
+    print("acmm mixed sizes %px gpu", acc_g.round(3), "oracle", acc_o.round(3))
+    assert all(gd[v].shape == imgs[v].shape for v in range(5))
+    assert abs(acc_g.mean() - acc_o.mean()) <= 0.015, (acc_g.mean(), acc_o.mean())
+    assert np.abs(acc_g - acc_o).max() <= 0.05, (acc_g, acc_o)
