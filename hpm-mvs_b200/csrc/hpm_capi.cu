@@ -390,8 +390,6 @@ int hpm_clear_prior(hpm_ctx *c)
     return HPM_OK;
 }
 
-/* The kernel arguments of one pass of context c with parameters p (checks
- * as hpm_run_patchmatch; takes the pass's random-stream salt). */
 /* Checks p against the context's state and fills the pass fields of *out;
  * takes the pass's random-stream salt.  Shared by run_pass and
  * ctx_pass_args. */
@@ -438,6 +436,9 @@ static int pass_args(hpm_ctx *c, const HpmParams *p, PMArgs *out)
     return HPM_OK;
 }
 
+/* The kernel arguments of one pass of context c with parameters p (checks
+ * as hpm_run_patchmatch; takes the pass's random-stream salt), for a
+ * batched launch. */
 extern "C++" int ctx_pass_args(hpm_ctx *c, const HpmParams *p, PMArgs *out)
 {
     if (!c) return HPM_ERR_ARG;
