@@ -231,7 +231,7 @@ typedef struct {
     int geom_max_iterations; /* of the geometric passes (0 = 2, ACMM.cpp:437) */
 } HpmAcmmOpts;
 
-/* The ACMM+NESP variant's main() (ACMM+NESP/windows/main.cpp:298-384) minus
+/* The ACMM+NESP variant's main() (ACMM+NESP/windows/main.cpp:299-384) minus
  * fusion: NESP sampling inside ACMM's coarse-to-fine IMAGE pyramid.  Every
  * problem's views are scaled down until their longer side is at most
  * size_bound (ComputeMultiScaleSettings, main.cpp:35-71; images resized as

@@ -1,4 +1,4 @@
-"""The ACMM+NESP variant's main() (ACMM+NESP/windows/main.cpp:298-384)
+"""The ACMM+NESP variant's main() (ACMM+NESP/windows/main.cpp:299-384)
 restated on the CPU for small images, from the oracle's kernels
 (liboracle.so, variant 1) and the OpenCV resize the reference calls.
 
