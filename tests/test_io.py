@@ -87,3 +87,32 @@ def test_resize_linear_u8_random_sizes_match_cv2():
         np.testing.assert_array_equal(hb.resize_linear_u8(img, dw, dh),
                                       cv2.resize(img, (dw, dh), interpolation=cv2.INTER_LINEAR),
                                       err_msg=f"{sw}x{sh} -> {dw}x{dh}, {ch} channels")
+
+
+@pytest.mark.parametrize("shape", [(2201, 3300), (3300, 2201), (3201, 3201)])
+def test_python_front_end_caps_views_like_the_reference(tmp_path, shape):
+    """hpm_mvs.load_view: views over 3200 pixels are resized as
+    InuputInitialization does (HPM.cpp:524-551): factor = min(3200/w,
+    3200/h) in float, new size = std::round of the float product (halves
+    away from zero), K scaled by the float size ratios, the image by
+    cv::resize INTER_LINEAR on the float image."""
+    import hpm_mvs
+
+    h, w = shape
+    rng = np.random.default_rng(h * 7 + w)
+    img = rng.integers(0, 256, (h, w), dtype=np.uint8)
+    os.makedirs(tmp_path / "images")
+    os.makedirs(tmp_path / "cams")
+    cv2.imwrite(str(tmp_path / "images" / "00000000.pgm"), img)
+    with open(tmp_path / "cams" / "00000000_cam.txt", "w") as f:
+        f.write("extrinsic\n1 0 0 0\n0 1 0 0\n0 0 1 0\n0 0 0 1\n\nintrinsic\n"
+                f"1000 0 {w / 2}\n0 1000 {h / 2}\n0 0 1\n\n2 0.02 192 6\n")
+    out, cam = hpm_mvs.load_view(str(tmp_path), 0)
+    f32 = np.float32
+    factor = min(f32(3200) / f32(w), f32(3200) / f32(h))
+    nw = int(np.floor(np.float64(f32(w) * factor) + 0.5))
+    nh = int(np.floor(np.float64(f32(h) * factor) + 0.5))
+    assert out.shape == (nh, nw) and (cam["width"], cam["height"]) == (nw, nh)
+    np.testing.assert_array_equal(out, cv2.resize(img.astype(np.float32), (nw, nh), interpolation=cv2.INTER_LINEAR))
+    sx, sy = f32(nw) / f32(w), f32(nh) / f32(h)
+    assert cam["K"][0] == f32(1000) * sx and cam["K"][4] == f32(1000) * sy
