@@ -162,6 +162,133 @@ struct DevBuf {
     cudaError_t alloc(size_t n) { return cudaMalloc(&p, sizeof(T) * (n ? n : 1)); }
 };
 
+/* What the ordered pass reads of a view besides the pairs (host memory). */
+struct PassView {
+    HpmCamera cam;
+    const float *depth;   /* the ACMM+NESP rule only */
+    const float *normal;  /* 3 floats per pixel */
+    const uint8_t *color; /* B, G, R */
+};
+
+/* Get3DPointonWorld (HPM.cpp:210-234, ACMM.cpp:187-211) on the host: the
+ * float operations of world_point above, in order (the x86-64 host build
+ * has no fused multiply-add). */
+void host_world_point(const HpmCamera &c, int x, int y, float depth, float *X)
+{
+    const float px = depth * ((float)x - c.K[2]) / c.K[0];
+    const float py = depth * ((float)y - c.K[5]) / c.K[4];
+    const float pz = depth;
+    const float *R = c.R, *t = c.t;
+    const float tx = R[0] * px + R[3] * py + R[6] * pz;
+    const float ty = R[1] * px + R[4] * py + R[7] * pz;
+    const float tz = R[2] * px + R[5] * py + R[8] * pz;
+    const float cx = -(R[0] * t[0] + R[3] * t[1] + R[6] * t[2]);
+    const float cy = -(R[1] * t[0] + R[4] * t[1] + R[7] * t[2]);
+    const float cz = -(R[2] * t[0] + R[5] * t[1] + R[8] * t[2]);
+    X[0] = tx + cx;
+    X[1] = ty + cy;
+    X[2] = tz + cz;
+}
+
+/* The order-dependent half of RunFusion for one problem (reference view i,
+ * sources srcs), reading the pairs of the GPU pass and the masks in the
+ * reference's order.  rule 0: HPM-MVS (main.cpp:553-620): a pixel with at
+ * least one agreeing source whose mean exp(-error) exceeds 0.3 gives its own
+ * point, normal and colour.  rule 1: the ACMM+NESP variant
+ * (ACMM+NESP/windows/main.cpp:205-292): a pixel with at least 2 agreeing
+ * sources gives the mean point, normal and colour over it and those source
+ * pixels (cv::Vec3f /= divides by multiplying with the float reciprocal,
+ * OpenCV core/matx.hpp; the PLY writer truncates colours,
+ * ACMM.cpp:395-397).  Either way the accepted pixel masks the source pixels
+ * recorded in the per-view used list (main.cpp:557). */
+void ordered_problem(int rule, int i, int ns, const int *srcs, const std::vector<PassView> &views,
+                     std::vector<std::vector<uint8_t>> &masks, const int *h_src, const float *h_w, const float *h_pt,
+                     float *out_xyz, float *out_normal, uint8_t *out_bgr, long long cap, long long &n_out)
+{
+    const PassView &ref = views[i];
+    const size_t npx = (size_t)ref.cam.width * ref.cam.height;
+    int used[kMaxSrc];
+    uint8_t *msrc[kMaxSrc];
+    for (int j = 0; j < ns; ++j) {
+        used[j] = -1;
+        msrc[j] = masks[srcs[j]].data();
+    }
+    std::vector<uint8_t> &mi = masks[i];
+    for (size_t p = 0; p < npx; ++p) {
+        if (mi[p] == 1) continue;
+        const int *ps = &h_src[p * ns];
+        const float *pw = &h_w[p * ns];
+        int num = 0;
+        float dyn = 0.0f;
+        float sp[3], sn[3], sc[3]; /* the variant's sums: point, normal, colour */
+        if (rule == 1)
+            for (int k = 0; k < 3; ++k) {
+                sp[k] = h_pt[3 * p + k];
+                sn[k] = ref.normal[3 * p + k];
+                sc[k] = (float)ref.color[3 * p + k];
+            }
+        for (int j = 0; j < ns; ++j) {
+            if (ps[j] < 0) continue;
+            if (msrc[j][ps[j]] == 1) continue;
+            if (rule == 1) {
+                const PassView &s = views[srcs[j]];
+                const int sx = ps[j] % s.cam.width, sy = ps[j] / s.cam.width;
+                float Y[3];
+                host_world_point(s.cam, sx, sy, s.depth[ps[j]], Y);
+                for (int k = 0; k < 3; ++k) {
+                    sp[k] += Y[k];
+                    sn[k] = sn[k] + s.normal[3 * (size_t)ps[j] + k];
+                    sc[k] += (float)s.color[3 * (size_t)ps[j] + k];
+                }
+            }
+            used[j] = ps[j];
+            dyn += pw[j];
+            num++;
+        }
+        if (rule == 1 ? num < 2 : !(num >= 1 && (dyn > 0.3 * num))) continue;
+        if (n_out < cap) {
+            if (rule == 1) {
+                const float div = num + 1.0f, inv = 1.f / div;
+                for (int k = 0; k < 3; ++k) {
+                    if (out_xyz) out_xyz[3 * n_out + k] = sp[k] / div;
+                    if (out_normal) out_normal[3 * n_out + k] = sn[k] * inv;
+                    if (out_bgr) out_bgr[3 * n_out + k] = (uint8_t)(int)(sc[k] / div);
+                }
+            } else {
+                if (out_xyz) memcpy(out_xyz + 3 * n_out, &h_pt[3 * p], 3 * sizeof(float));
+                if (out_normal) memcpy(out_normal + 3 * n_out, &ref.normal[3 * p], 3 * sizeof(float));
+                if (out_bgr) memcpy(out_bgr + 3 * n_out, &ref.color[3 * p], 3);
+            }
+        }
+        n_out++;
+        for (int j = 0; j < ns; ++j)
+            if (used[j] != -1) msrc[j][used[j]] = 1;
+    }
+}
+
+/* hpm_fuse's argument checks (problems as hpm_run_scene's) */
+bool fuse_args_ok(int n_views, const HpmCamera *cams, const float *const *depths, const float *const *normals,
+                  const uint8_t *const *colors, int n_problems, const int *ref_ids, const int *src_counts,
+                  const int *src_ids, long long cap, long long *n_points)
+{
+    if (!cams || !depths || !normals || !colors || !ref_ids || !src_counts || !src_ids || !n_points || n_views < 1 ||
+        n_problems < 0 || cap < 0)
+        return false;
+    for (int v = 0; v < n_views; ++v)
+        if (!depths[v] || !normals[v] || !colors[v] || cams[v].width < 1 || cams[v].height < 1) return false;
+    for (int p = 0; p < n_problems; ++p) {
+        if (ref_ids[p] < 0 || ref_ids[p] >= n_views || src_counts[p] < 0 || src_counts[p] > kMaxSrc) return false;
+        for (int j = 0; j < src_counts[p]; ++j)
+            if (src_ids[p * kMaxSrc + j] < 0 || src_ids[p * kMaxSrc + j] >= n_views) return false;
+    }
+    return true;
+}
+
+int fuse_impl(int rule, int device, int n_views, const HpmCamera *cams, const float *const *depths,
+              const float *const *normals, const uint8_t *const *colors, int n_problems, const int *ref_ids,
+              const int *src_counts, const int *src_ids, float *out_xyz, float *out_normal, uint8_t *out_bgr,
+              long long cap, long long *n_points);
+
 }  // namespace
 
 extern "C" int hpm_fuse(int device, int n_views, const HpmCamera *cams, const float *const *depths,
@@ -169,16 +296,58 @@ extern "C" int hpm_fuse(int device, int n_views, const HpmCamera *cams, const fl
                         const int *ref_ids, const int *src_counts, const int *src_ids, float *out_xyz,
                         float *out_normal, uint8_t *out_bgr, long long cap, long long *n_points)
 {
-    if (!cams || !depths || !normals || !colors || !ref_ids || !src_counts || !src_ids || !n_points || n_views < 1 ||
-        n_problems < 0 || cap < 0)
+    return fuse_impl(0, device, n_views, cams, depths, normals, colors, n_problems, ref_ids, src_counts, src_ids,
+                     out_xyz, out_normal, out_bgr, cap, n_points);
+}
+
+extern "C" int hpm_fuse_acmm(int device, int n_views, const HpmCamera *cams, const float *const *depths,
+                             const float *const *normals, const uint8_t *const *colors, int n_problems,
+                             const int *ref_ids, const int *src_counts, const int *src_ids, float *out_xyz,
+                             float *out_normal, uint8_t *out_bgr, long long cap, long long *n_points)
+{
+    return fuse_impl(1, device, n_views, cams, depths, normals, colors, n_problems, ref_ids, src_counts, src_ids,
+                     out_xyz, out_normal, out_bgr, cap, n_points);
+}
+
+extern "C" int hpm_fuse_pass(int rule, int n_views, const HpmCamera *cams, const float *const *depths,
+                             const float *const *normals, const uint8_t *const *colors, int n_problems,
+                             const int *ref_ids, const int *src_counts, const int *src_ids,
+                             const int *const *pair_src, const float *const *pair_w, const float *const *points,
+                             float *out_xyz, float *out_normal, uint8_t *out_bgr, long long cap,
+                             long long *n_points)
+{
+    if ((rule != 0 && rule != 1) || !pair_src || !pair_w || !points ||
+        !fuse_args_ok(n_views, cams, depths, normals, colors, n_problems, ref_ids, src_counts, src_ids, cap,
+                      n_points))
         return HPM_ERR_ARG;
-    for (int v = 0; v < n_views; ++v)
-        if (!depths[v] || !normals[v] || !colors[v] || cams[v].width < 1 || cams[v].height < 1) return HPM_ERR_ARG;
-    for (int p = 0; p < n_problems; ++p) {
-        if (ref_ids[p] < 0 || ref_ids[p] >= n_views || src_counts[p] < 0 || src_counts[p] > kMaxSrc) return HPM_ERR_ARG;
-        for (int j = 0; j < src_counts[p]; ++j)
-            if (src_ids[p * kMaxSrc + j] < 0 || src_ids[p * kMaxSrc + j] >= n_views) return HPM_ERR_ARG;
+    for (int p = 0; p < n_problems; ++p)
+        if (src_counts[p] > 0 && (!pair_src[p] || !pair_w[p] || !points[p])) return HPM_ERR_ARG;
+    std::vector<PassView> views(n_views);
+    std::vector<std::vector<uint8_t>> masks(n_views);
+    for (int v = 0; v < n_views; ++v) {
+        views[v] = {cams[v], depths[v], normals[v], colors[v]};
+        masks[v].assign((size_t)cams[v].width * cams[v].height, 0);
     }
+    long long n_out = 0;
+    for (int p = 0; p < n_problems; ++p)
+        if (src_counts[p] > 0)
+            ordered_problem(rule, ref_ids[p], src_counts[p], src_ids + p * kMaxSrc, views, masks, pair_src[p],
+                            pair_w[p], points[p], out_xyz, out_normal, out_bgr, cap, n_out);
+    *n_points = n_out;
+    return HPM_OK;
+}
+
+namespace {
+
+int fuse_impl(int rule, int device, int n_views, const HpmCamera *cams, const float *const *depths,
+              const float *const *normals, const uint8_t *const *colors, int n_problems, const int *ref_ids,
+              const int *src_counts, const int *src_ids, float *out_xyz, float *out_normal, uint8_t *out_bgr,
+              long long cap, long long *n_points)
+{
+    if (!fuse_args_ok(n_views, cams, depths, normals, colors, n_problems, ref_ids, src_counts, src_ids, cap,
+                      n_points))
+        return HPM_ERR_ARG;
+
     if (cudaSetDevice(device) != cudaSuccess) return HPM_ERR_CUDA;
     const hpm::Range range("fusion %d problems", n_problems);
     cudaStream_t st;
@@ -194,7 +363,7 @@ extern "C" int hpm_fuse(int device, int n_views, const HpmCamera *cams, const fl
     /* the maps on the device (inputs may be host or device memory) and on
      * the host (the sequential pass reads colours and normals of points) */
     std::vector<DevBuf<float>> d_depth(n_views), d_normal(n_views);
-    std::vector<std::vector<float>> h_normal(n_views);
+    std::vector<std::vector<float>> h_normal(n_views), h_depth(n_views);
     std::vector<std::vector<uint8_t>> h_color(n_views);
     std::vector<std::vector<uint8_t>> masks(n_views);
     size_t max_px = 0;
@@ -209,8 +378,16 @@ extern "C" int hpm_fuse(int device, int n_views, const HpmCamera *cams, const fl
         h_color[v].resize(3 * np);
         FCK(cudaMemcpyAsync(h_normal[v].data(), normals[v], sizeof(float) * 3 * np, cudaMemcpyDefault, st));
         FCK(cudaMemcpyAsync(h_color[v].data(), colors[v], 3 * np, cudaMemcpyDefault, st));
+        if (rule == 1) { /* the variant also averages the agreeing source points */
+            h_depth[v].resize(np);
+            FCK(cudaMemcpyAsync(h_depth[v].data(), depths[v], sizeof(float) * np, cudaMemcpyDefault, st));
+        }
         masks[v].assign(np, 0);
     }
+    FCK(cudaStreamSynchronize(st));
+    std::vector<PassView> views(n_views);
+    for (int v = 0; v < n_views; ++v)
+        views[v] = {cams[v], rule == 1 ? h_depth[v].data() : nullptr, h_normal[v].data(), h_color[v].data()};
     int max_ns = 1;
     for (int p = 0; p < n_problems; ++p) max_ns = src_counts[p] > max_ns ? src_counts[p] : max_ns;
     /* Two slots of pair data.  A producer thread runs the kernel of problem
@@ -302,7 +479,6 @@ extern "C" int hpm_fuse(int device, int n_views, const HpmCamera *cams, const fl
     long long n_out = 0;
     for (int pi = 0; pi < n_problems; ++pi) {
         const int i = ref_ids[pi], ns = src_counts[pi];
-        const size_t npx = (size_t)cams[i].width * cams[i].height;
         const int k = pi & 1;
         {
             std::unique_lock<std::mutex> l(mu);
@@ -322,46 +498,16 @@ extern "C" int hpm_fuse(int device, int n_views, const HpmCamera *cams, const fl
                 cv.notify_all();
             }
         } release{ready[k], mu, cv};
-        const std::vector<int> &h_src = slots[k].h_src;
-        const std::vector<float> &h_w = slots[k].h_w, &h_pt = slots[k].h_pt;
         if (ns == 0) continue; /* no source: no pixel can be consistent */
-        /* main.cpp:553-620 in order: masks and the per-view used_list */
-        int used[kMaxSrc];
-        uint8_t *msrc[kMaxSrc];
-        for (int j = 0; j < ns; ++j) {
-            used[j] = -1;
-            msrc[j] = masks[src_ids[pi * kMaxSrc + j]].data();
-        }
-        std::vector<uint8_t> &mi = masks[i];
-        for (size_t p = 0; p < npx; ++p) {
-            if (mi[p] == 1) continue;
-            const int *ps = &h_src[p * ns];
-            const float *pw = &h_w[p * ns];
-            int num = 0;
-            float dyn = 0.0f;
-            for (int j = 0; j < ns; ++j) {
-                if (ps[j] < 0) continue;
-                if (msrc[j][ps[j]] == 1) continue;
-                used[j] = ps[j];
-                dyn += pw[j];
-                num++;
-            }
-            if (num >= 1 && (dyn > 0.3 * num)) {
-                if (n_out < cap) {
-                    if (out_xyz) memcpy(out_xyz + 3 * n_out, &h_pt[3 * p], 3 * sizeof(float));
-                    if (out_normal) memcpy(out_normal + 3 * n_out, &h_normal[i][3 * p], 3 * sizeof(float));
-                    if (out_bgr) memcpy(out_bgr + 3 * n_out, &h_color[i][3 * p], 3);
-                }
-                n_out++;
-                for (int j = 0; j < ns; ++j)
-                    if (used[j] != -1) msrc[j][used[j]] = 1;
-            }
-        }
+        ordered_problem(rule, i, ns, src_ids + pi * kMaxSrc, views, masks, slots[k].h_src.data(),
+                        slots[k].h_w.data(), slots[k].h_pt.data(), out_xyz, out_normal, out_bgr, cap, n_out);
     }
 #undef FCK
     *n_points = n_out;
     return HPM_OK;
 }
+
+}  // namespace
 
 extern "C" int hpm_write_ply(const char *path, long long n, const float *xyz, const float *normal, const uint8_t *bgr)
 {

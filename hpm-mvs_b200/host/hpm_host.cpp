@@ -476,21 +476,21 @@ void HPM::ReleaseProblemHostMemory()
 }
 
 static long long fuse_tree(const std::string &dense_folder, const std::vector<Problem> &problems,
-                           bool geom_consistency, int device, const char *tree, const char *ply_name);
+                           bool geom_consistency, int device, const char *tree, const char *ply_name, bool acmm);
 
 long long RunFusion(const std::string &dense_folder, const std::vector<Problem> &problems, bool geom_consistency,
                     int device)
 {
-    return fuse_tree(dense_folder, problems, geom_consistency, device, "HPM", "HPM_model.ply");
+    return fuse_tree(dense_folder, problems, geom_consistency, device, "HPM", "HPM_model.ply", false);
 }
 
 long long RunFusionAcmm(const std::string &dense_folder, const std::vector<Problem> &problems, int device)
 {
-    return fuse_tree(dense_folder, problems, true, device, "ACMM_NESP", "ACMM_NESP_model.ply");
+    return fuse_tree(dense_folder, problems, true, device, "ACMM_NESP", "ACMM_NESP_model.ply", true);
 }
 
 static long long fuse_tree(const std::string &dense_folder, const std::vector<Problem> &problems,
-                           bool geom_consistency, int device, const char *tree, const char *ply_name)
+                           bool geom_consistency, int device, const char *tree, const char *ply_name, bool acmm)
 {
     const int n = (int)problems.size();
     std::vector<HpmCamera> cams(n);
@@ -543,9 +543,10 @@ static long long fuse_tree(const std::string &dense_folder, const std::vector<Pr
     std::vector<float> xyz(3 * cap), nrm(3 * cap);
     std::vector<uint8_t> col(3 * cap);
     long long count = 0;
-    int rc = hpm_fuse(device, n, cams.data(), dp.data(), np_.data(), cp.data(), n, refs.data(), counts.data(),
-                      srcs.data(), xyz.data(), nrm.data(), col.data(), (long long)cap, &count);
-    if (rc != HPM_OK) throw Error(rc, "hpm_fuse");
+    int rc = (acmm ? hpm_fuse_acmm : hpm_fuse)(device, n, cams.data(), dp.data(), np_.data(), cp.data(), n,
+                                               refs.data(), counts.data(), srcs.data(), xyz.data(), nrm.data(),
+                                               col.data(), (long long)cap, &count);
+    if (rc != HPM_OK) throw Error(rc, acmm ? "hpm_fuse_acmm" : "hpm_fuse");
     const std::string ply = dense_folder + "/" + tree + "/" + ply_name;
     rc = hpm_write_ply(ply.c_str(), count, xyz.data(), nrm.data(), col.data());
     if (rc != HPM_OK) throw Error(rc, "cannot write " + ply);

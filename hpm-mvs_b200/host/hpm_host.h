@@ -127,8 +127,9 @@ private:
  * (HPM.cpp:187-208, OpenCV's 8-bit bilinear, byte for byte). */
 long long RunFusion(const std::string &dense_folder, const std::vector<Problem> &problems, bool geom_consistency,
                     int device = 0);
-/* The same over the ACMM+NESP variant's tree: ACMM_NESP/2333_%08d/ into
- * ACMM_NESP/ACMM_NESP_model.ply (ACMM+NESP/windows/main.cpp:154-297). */
+/* The ACMM+NESP variant's RunFusion (ACMM+NESP/windows/main.cpp:154-297,
+ * hpm_fuse_acmm: points averaged over at least 2 agreeing sources) over its
+ * tree: ACMM_NESP/2333_%08d/ into ACMM_NESP/ACMM_NESP_model.ply. */
 long long RunFusionAcmm(const std::string &dense_folder, const std::vector<Problem> &problems, int device = 0);
 
 /* The ACMM+NESP variant's main() minus fusion (ACMM+NESP/windows/main.cpp:

@@ -42,6 +42,7 @@ EXPORTED = [
     "hpm_raster_triangles", "hpm_knn6", "hpm_tap_samples", "hpm_net_pack_weights", "hpm_net_conv3x3",
     "hpm_net_conv_wgrad", "hpm_run_scene_net", "hpm_net_coarse_inputs", "hpm_net_targets", "hpm_net_loss",
     "hpm_net_adam", "hpm_run_scene_batched", "hpm_run_scene_batched_net", "hpm_run_scene_acmm",
+    "hpm_fuse_acmm", "hpm_fuse_pass",
 ]
 
 
@@ -532,9 +533,47 @@ def read_bgr8(path: str) -> np.ndarray:
     return out
 
 
-def fuse(cams, depths, normals, colors, problems, device: int = 0):
+def _fuse_inputs(cams, depths, normals, colors, problems):
+    n = len(cams)
+    cams = np.ascontiguousarray(cams, dtype=CAMERA_DTYPE)
+    ds = [np.ascontiguousarray(d, dtype=np.float32) for d in depths]
+    ns_ = [np.ascontiguousarray(x, dtype=np.float32) for x in normals]
+    cs = [np.ascontiguousarray(c, dtype=np.uint8) for c in colors]
+    refs = np.array([p[0] for p in problems], np.int32)
+    counts = np.array([len(p[1]) for p in problems], np.int32)
+    srcs = np.zeros((max(len(problems), 1), MAX_IMAGES - 1), np.int32)
+    for i, (_, s) in enumerate(problems):
+        srcs[i, :len(s)] = s
+    cap = sum(d.size for d in ds)
+    return n, cams, ds, ns_, cs, refs, counts, srcs, cap
+
+
+def fuse_pass(cams, depths, normals, colors, problems, pairs, acmm=False):
+    """hpm_fuse_pass: the ordered half of the fusion on the host (no GPU)
+    from given pairs, one (pair_src [pixels, ns], pair_w [pixels, ns], points
+    [pixels, 3]) per problem.  Returns (xyz, normal, bgr) like fuse()."""
+    n, cams, ds, ns_, cs, refs, counts, srcs, cap = _fuse_inputs(cams, depths, normals, colors, problems)
+    arr = lambda xs: (ctypes.c_void_p * len(xs))(*[x.ctypes.data for x in xs])  # noqa: E731
+    ps = [np.ascontiguousarray(p[0], dtype=np.int32) for p in pairs]
+    pw = [np.ascontiguousarray(p[1], dtype=np.float32) for p in pairs]
+    pt = [np.ascontiguousarray(p[2], dtype=np.float32) for p in pairs]
+    xyz = np.empty((cap, 3), np.float32)
+    nrm = np.empty((cap, 3), np.float32)
+    bgr = np.empty((cap, 3), np.uint8)
+    cnt = ctypes.c_longlong()
+    rc = lib().hpm_fuse_pass(int(acmm), n, _p(cams), arr(ds), arr(ns_), arr(cs), len(problems), _p(refs),
+                             _p(counts), _p(srcs), arr(ps), arr(pw), arr(pt), _p(xyz), _p(nrm), _p(bgr),
+                             ctypes.c_longlong(cap), ctypes.byref(cnt))
+    if rc != HPM_OK:
+        raise HpmError(f"hpm_fuse_pass: {STATUS_NAMES.get(rc, rc)}")
+    k = cnt.value
+    return xyz[:k].copy(), nrm[:k].copy(), bgr[:k].copy()
+
+
+def fuse(cams, depths, normals, colors, problems, device: int = 0, acmm: bool = False):
     """RunFusion (main.cpp:502-633): (xyz [n,3], normal [n,3], bgr [n,3] uint8)
-    in the reference's order.  problems: [(ref, [sources])]."""
+    in the reference's order.  problems: [(ref, [sources])].  acmm: the
+    ACMM+NESP variant's RunFusion (hpm_fuse_acmm)."""
     n = len(cams)
     cams = np.ascontiguousarray(cams, dtype=CAMERA_DTYPE)
     ds = [np.ascontiguousarray(d, dtype=np.float32) for d in depths]
@@ -551,10 +590,11 @@ def fuse(cams, depths, normals, colors, problems, device: int = 0):
     nrm = np.empty((cap, 3), np.float32)
     bgr = np.empty((cap, 3), np.uint8)
     cnt = ctypes.c_longlong()
-    rc = lib().hpm_fuse(device, n, _p(cams), arr(ds), arr(ns_), arr(cs), len(problems), _p(refs), _p(counts),
-                        _p(srcs), _p(xyz), _p(nrm), _p(bgr), ctypes.c_longlong(cap), ctypes.byref(cnt))
+    fn = lib().hpm_fuse_acmm if acmm else lib().hpm_fuse
+    rc = fn(device, n, _p(cams), arr(ds), arr(ns_), arr(cs), len(problems), _p(refs), _p(counts), _p(srcs), _p(xyz),
+            _p(nrm), _p(bgr), ctypes.c_longlong(cap), ctypes.byref(cnt))
     if rc != HPM_OK:
-        raise HpmError(f"hpm_fuse: {STATUS_NAMES.get(rc, rc)}")
+        raise HpmError(f"hpm_fuse{'_acmm' if acmm else ''}: {STATUS_NAMES.get(rc, rc)}")
     k = cnt.value
     return xyz[:k].copy(), nrm[:k].copy(), bgr[:k].copy()
 

@@ -136,11 +136,12 @@ def run_scene_acmm(ctx, folder, problems, views, *, geom_iterations, seed):
     return int(sum(x.size for x in d))
 
 
-def run_fusion(folder, problems, geom_consistency, device=0, tree="HPM", ply="HPM_model.ply"):
+def run_fusion(folder, problems, geom_consistency, device=0, tree="HPM", ply="HPM_model.ply", acmm=False):
     """RunFusion (main.cpp:502-633) with RescaleImageAndCamera
     (HPM.cpp:187-208: OpenCV's 8-bit bilinear, reproduced by
-    hpm_resize_linear_u8) over the maps under folder/tree; returns the point
-    count."""
+    hpm_resize_linear_u8) over the maps under folder/tree; acmm: the
+    ACMM+NESP variant's RunFusion (ACMM+NESP/windows/main.cpp:154-297).
+    Returns the point count."""
     cams, depths, normals, colors = [], [], [], []
     for ref, _ in problems:
         out = os.path.join(folder, tree, f"2333_{ref:08d}")
@@ -171,7 +172,7 @@ def run_fusion(folder, problems, geom_consistency, device=0, tree="HPM", ply="HP
         colors.append(img)
     # the reference indexes views by problem order (main.cpp:517-546)
     probs = [(i, list(srcs)) for i, (_, srcs) in enumerate(problems)]
-    xyz, nrm, bgr = hb.fuse(np.array(cams), depths, normals, colors, probs, device)
+    xyz, nrm, bgr = hb.fuse(np.array(cams), depths, normals, colors, probs, device, acmm=acmm)
     hb.write_ply(os.path.join(folder, tree, ply), xyz, nrm, bgr)
     return len(xyz)
 
@@ -299,7 +300,8 @@ def main(argv=None):
         if not a.no_fusion:
             def fusion():
                 tree, ply = ("ACMM_NESP", "ACMM_NESP_model.ply") if a.acmm else ("HPM", "HPM_model.ply")
-                n = run_fusion(a.dense_folder, problems, a.geom_iterations > 0, a.device, tree, ply)
+                n = run_fusion(a.dense_folder, problems, a.acmm or a.geom_iterations > 0, a.device, tree, ply,
+                               acmm=a.acmm)
                 print(f"Fused {n} points into {a.dense_folder}/{tree}/{ply}")
                 return -n
             step("fusion", fusion)

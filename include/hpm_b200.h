@@ -444,6 +444,16 @@ int hpm_fuse(int device, int n_views, const HpmCamera *cams, const float *const 
              const float *const *normals, const uint8_t *const *colors, int n_problems, const int *ref_ids,
              const int *src_counts, const int *src_ids, float *out_xyz, float *out_normal, uint8_t *out_bgr,
              long long cap, long long *n_points);
+/* RunFusion of the ACMM+NESP variant (ACMM+NESP/windows/main.cpp:154-297):
+ * hpm_fuse's arguments, consistency tests, order and masking, with the
+ * variant's rule: a pixel needs at least 2 agreeing sources, and its point,
+ * normal and colour are the means over it and the agreeing source pixels
+ * (the colour bytes truncated, as the variant's PLY writer does,
+ * ACMM.cpp:395-397). */
+int hpm_fuse_acmm(int device, int n_views, const HpmCamera *cams, const float *const *depths,
+                  const float *const *normals, const uint8_t *const *colors, int n_problems, const int *ref_ids,
+                  const int *src_counts, const int *src_ids, float *out_xyz, float *out_normal, uint8_t *out_bgr,
+                  long long cap, long long *n_points);
 /* StoreColorPlyFileBinaryPointCloud (HPM.cpp:403-456): binary little-endian
  * PLY, x y z nx ny nz as float, red green blue as uchar, non-finite
  * coordinates written as the origin.  Points are written in order (the
@@ -451,6 +461,18 @@ int hpm_fuse(int device, int n_views, const HpmCamera *cams, const float *const 
 int hpm_write_ply(const char *path, long long n, const float *xyz, const float *normal, const uint8_t *bgr);
 
 /* Deterministic building blocks exposed for parity checks. */
+
+/* The order-dependent half of hpm_fuse (rule 0) or hpm_fuse_acmm (rule 1)
+ * on the host, without a GPU, given for every problem p what their GPU pass
+ * computes: pair_src[p] and pair_w[p], [pixel][src_counts[p]] (the source
+ * pixel index of a consistent pair or -1, and its exp(-error)), and
+ * points[p], [pixel][3] (the reference pixel's world point).  Other
+ * arguments as hpm_fuse's, host memory. */
+int hpm_fuse_pass(int rule, int n_views, const HpmCamera *cams, const float *const *depths,
+                  const float *const *normals, const uint8_t *const *colors, int n_problems, const int *ref_ids,
+                  const int *src_counts, const int *src_ids, const int *const *pair_src,
+                  const float *const *pair_w, const float *const *points, float *out_xyz, float *out_normal,
+                  uint8_t *out_bgr, long long cap, long long *n_points);
 
 /* Delaunay triangulation of n integer points (xy pairs) used for the planar
  * prior (replaces cv::Subdiv2D in DelaunayTriangulation, HPM.cpp:787-809,

@@ -1645,9 +1645,16 @@ static float fu_angle(const float *a, const float *b)
     return ang != ang ? 0.0f : ang;
 }
 
-long or_fuse(int n_views, const OrCamera *cams, const float *const *depths, const float *const *normals,
-             const unsigned char *const *colors, int n_problems, const int *ref_ids, const int *src_counts,
-             const int *src_ids, float *out_xyz, float *out_normal, float *out_color, long cap)
+/* RunFusion of HPM-MVS (main.cpp:502-633, acmm 0) or of the ACMM+NESP
+ * variant (ACMM+NESP/windows/main.cpp:154-297, acmm 1).  The variant keeps a
+ * pixel consistent with at least 2 sources and writes the mean of its point,
+ * normal and colour with those of the agreeing source pixels; HPM-MVS keeps
+ * one with at least 1 source whose mean exp(-error) exceeds 0.3 and writes
+ * the reference pixel's own. */
+static long fuse_impl(int acmm, int n_views, const OrCamera *cams, const float *const *depths,
+                      const float *const *normals, const unsigned char *const *colors, int n_problems,
+                      const int *ref_ids, const int *src_counts, const int *src_ids, float *out_xyz,
+                      float *out_normal, float *out_color, long cap)
 {
     unsigned char **masks = (unsigned char **)calloc((size_t)n_views, sizeof(*masks));
     for (int v = 0; v < n_views; ++v) masks[v] = (unsigned char *)calloc((size_t)cams[v].width * cams[v].height, 1);
@@ -1669,6 +1676,9 @@ long or_fuse(int n_views, const OrCamera *cams, const float *const *depths, cons
                 fu_world(ci, c, r, ref_depth, X);
                 int num = 0;
                 float dyn = 0;
+                /* the variant's sums: point, normal (cv::Vec3f), colour */
+                float sp[3] = {X[0], X[1], X[2]}, sn[3] = {ref_n[0], ref_n[1], ref_n[2]}, scol[3];
+                for (int k = 0; k < 3; ++k) scol[k] = (float)colors[i][3 * ctr + k];
                 for (int j = 0; j < ns; ++j) {
                     const int s = src_ids[pi * 32 + j];
                     const OrCamera *cs = &cams[s];
@@ -1689,19 +1699,37 @@ long or_fuse(int n_views, const OrCamera *cams, const float *const *depths, cons
                         const float rel = fabsf(proj_depth - ref_depth) / ref_depth;
                         const float ang = fu_angle(ref_n, src_n);
                         if (reproj < 2.0f && rel < 0.01f && ang < 0.174533f) {
+                            if (acmm) { /* ACMM+NESP/windows/main.cpp:254-261 */
+                                for (int k = 0; k < 3; ++k) {
+                                    sp[k] += Y[k];
+                                    sn[k] = sn[k] + src_n[k];
+                                    scol[k] += (float)colors[s][3 * sctr + k];
+                                }
+                            }
                             used_x[j] = sc;
                             used_y[j] = sr;
                             const float idx = reproj + 200 * rel + ang * 10;
-                            dyn += expf(-idx);
+                            if (!acmm) dyn += expf(-idx);
                             num++;
                         }
                     }
                 }
-                if (num >= 1 && (dyn > 0.3 * num)) {
+                if (acmm ? num >= 2 : (num >= 1 && (dyn > 0.3 * num))) {
+                    if (acmm) { /* ACMM+NESP/windows/main.cpp:270-277 */
+                        const float div = num + 1.0f;
+                        /* cv::Vec3f /= float multiplies by the float reciprocal (OpenCV core/matx.hpp) */
+                        const float inv = 1.f / div;
+                        for (int k = 0; k < 3; ++k) {
+                            sp[k] /= div;
+                            sn[k] = sn[k] * inv;
+                            scol[k] /= div;
+                        }
+                    }
                     if (n_out < cap) {
-                        memcpy(out_xyz + 3 * n_out, X, sizeof(X));
-                        memcpy(out_normal + 3 * n_out, ref_n, 3 * sizeof(float));
-                        for (int k = 0; k < 3; ++k) out_color[3 * n_out + k] = (float)colors[i][3 * ctr + k];
+                        memcpy(out_xyz + 3 * n_out, acmm ? sp : X, sizeof(X));
+                        memcpy(out_normal + 3 * n_out, acmm ? sn : ref_n, 3 * sizeof(float));
+                        for (int k = 0; k < 3; ++k)
+                            out_color[3 * n_out + k] = acmm ? scol[k] : (float)colors[i][3 * ctr + k];
                     }
                     n_out++;
                     for (int j = 0; j < ns; ++j) {
@@ -1716,6 +1744,72 @@ long or_fuse(int n_views, const OrCamera *cams, const float *const *depths, cons
     for (int v = 0; v < n_views; ++v) free(masks[v]);
     free(masks);
     return n_out;
+}
+
+long or_fuse(int n_views, const OrCamera *cams, const float *const *depths, const float *const *normals,
+             const unsigned char *const *colors, int n_problems, const int *ref_ids, const int *src_counts,
+             const int *src_ids, float *out_xyz, float *out_normal, float *out_color, long cap)
+{
+    return fuse_impl(0, n_views, cams, depths, normals, colors, n_problems, ref_ids, src_counts, src_ids, out_xyz,
+                     out_normal, out_color, cap);
+}
+
+long or_fuse_acmm(int n_views, const OrCamera *cams, const float *const *depths, const float *const *normals,
+                  const unsigned char *const *colors, int n_problems, const int *ref_ids, const int *src_counts,
+                  const int *src_ids, float *out_xyz, float *out_normal, float *out_color, long cap)
+{
+    return fuse_impl(1, n_views, cams, depths, normals, colors, n_problems, ref_ids, src_counts, src_ids, out_xyz,
+                     out_normal, out_color, cap);
+}
+
+/* The mask-independent half of RunFusion for problem pi, as the product's
+ * GPU pass computes it: per reference pixel its world point, and per
+ * (pixel, source) the source pixel index of a consistent pair (-1
+ * otherwise) and its exp(-error). */
+int or_fuse_pairs(int n_views, const OrCamera *cams, const float *const *depths, const float *const *normals,
+                  int ref, int ns, const int *srcs, int *pair_src, float *pair_w, float *points)
+{
+    (void)n_views;
+    const OrCamera *ci = &cams[ref];
+    const int cols = ci->width, rows = ci->height;
+    for (int r = 0; r < rows; ++r)
+        for (int c = 0; c < cols; ++c) {
+            const size_t ctr = (size_t)r * cols + c;
+            const float ref_depth = depths[ref][ctr];
+            const float *ref_n = normals[ref] + 3 * ctr;
+            for (int j = 0; j < ns; ++j) {
+                pair_src[ctr * ns + j] = -1;
+                pair_w[ctr * ns + j] = 0.0f;
+            }
+            if (ref_depth <= 0.0) continue;
+            float X[3];
+            fu_world(ci, c, r, ref_depth, X);
+            memcpy(points + 3 * ctr, X, sizeof(X));
+            for (int j = 0; j < ns; ++j) {
+                const int s = srcs[j];
+                const OrCamera *cs = &cams[s];
+                float pt[2], proj_depth;
+                fu_project(X, cs, pt, &proj_depth);
+                const int sr = trunc_int(pt[1] + 0.5f), sc = trunc_int(pt[0] + 0.5f);
+                if (!(sc >= 0 && sc < cs->width && sr >= 0 && sr < cs->height)) continue;
+                const size_t sctr = (size_t)sr * cs->width + sc;
+                const float src_depth = depths[s][sctr];
+                const float *src_n = normals[s] + 3 * sctr;
+                if (src_depth <= 0.0) continue;
+                float Y[3], tp[2];
+                fu_world(cs, sc, sr, src_depth, Y);
+                fu_project(Y, ci, tp, &proj_depth);
+                const float dx = (float)c - tp[0], dy = (float)r - tp[1];
+                const float reproj = (float)sqrt((double)dx * dx + (double)dy * dy);
+                const float rel = fabsf(proj_depth - ref_depth) / ref_depth;
+                const float ang = fu_angle(ref_n, src_n);
+                if (reproj < 2.0f && rel < 0.01f && ang < 0.174533f) {
+                    pair_src[ctr * ns + j] = (int)sctr;
+                    pair_w[ctr * ns + j] = expf(-(reproj + 200 * rel + ang * 10));
+                }
+            }
+        }
+    return 0;
 }
 
 /* ------------------------------------------------------------------ */

@@ -173,6 +173,18 @@ void or_prior_full(const OrCamera *ref, const float *mask, const float *tri_plan
 long or_fuse(int n_views, const OrCamera *cams, const float *const *depths, const float *const *normals,
              const unsigned char *const *colors, int n_problems, const int *ref_ids, const int *src_counts,
              const int *src_ids, float *out_xyz, float *out_normal, float *out_color, long cap);
+/* The same with the ACMM+NESP variant's rule (ACMM+NESP/windows/main.cpp:
+ * 154-297): at least 2 consistent sources, and the point, normal and colour
+ * are means over the reference pixel and the agreeing source pixels. */
+long or_fuse_acmm(int n_views, const OrCamera *cams, const float *const *depths, const float *const *normals,
+                  const unsigned char *const *colors, int n_problems, const int *ref_ids, const int *src_counts,
+                  const int *src_ids, float *out_xyz, float *out_normal, float *out_color, long cap);
+/* The mask-independent half of RunFusion for the reference view `ref` and
+ * its ns sources srcs: pair_src / pair_w [pixel][ns] (source pixel index of
+ * a consistent pair or -1, its exp(-error)), points [pixel][3] (the world
+ * point of pixels with a positive depth). */
+int or_fuse_pairs(int n_views, const OrCamera *cams, const float *const *depths, const float *const *normals,
+                  int ref, int ns, const int *srcs, int *pair_src, float *pair_w, float *points);
 
 #ifdef __cplusplus
 }

@@ -382,9 +382,27 @@ def prior_full(ref_cam, mask, tri_planes, knn_planes, dmin, dmax):
     return out, m, d
 
 
-def fuse(cams, depths, normals, colors, problems):
+def fuse_pairs(cams, depths, normals, ref, srcs):
+    """or_fuse_pairs: (pair_src [H*W, ns], pair_w [H*W, ns], points [H*W, 3])
+    of reference view `ref` against sources `srcs`."""
+    n = len(cams)
+    c = _cams(cams)
+    ds = [np.ascontiguousarray(d, dtype=np.float32) for d in depths]
+    ns_ = [np.ascontiguousarray(x, dtype=np.float32) for x in normals]
+    arr = lambda xs: (ctypes.c_void_p * n)(*[x.ctypes.data for x in xs])  # noqa: E731
+    npx = ds[ref].size
+    s = np.array(srcs, np.int32)
+    ps = np.empty((npx, len(srcs)), np.int32)
+    pw = np.empty((npx, len(srcs)), np.float32)
+    pt = np.zeros((npx, 3), np.float32)
+    lib().or_fuse_pairs(n, _p(c), arr(ds), arr(ns_), int(ref), len(srcs), _p(s), _p(ps), _p(pw), _p(pt))
+    return ps, pw, pt
+
+
+def fuse(cams, depths, normals, colors, problems, acmm=False):
     """or_fuse: the reference's sequential RunFusion (xyz, normal, colour as
-    floats B G R), in the reference's order."""
+    floats B G R), in the reference's order; acmm: the ACMM+NESP variant's
+    rule (or_fuse_acmm)."""
     n = len(cams)
     c = _cams(cams)
     ds = [np.ascontiguousarray(d, dtype=np.float32) for d in depths]
@@ -400,9 +418,10 @@ def fuse(cams, depths, normals, colors, problems):
     xyz = np.empty((cap, 3), np.float32)
     nrm = np.empty((cap, 3), np.float32)
     col = np.empty((cap, 3), np.float32)
-    lib().or_fuse.restype = ctypes.c_long
-    k = lib().or_fuse(n, _p(c), arr(ds), arr(ns_), arr(cs), len(problems), _p(refs), _p(counts), _p(srcs), _p(xyz),
-                      _p(nrm), _p(col), ctypes.c_long(cap))
+    fn = lib().or_fuse_acmm if acmm else lib().or_fuse
+    fn.restype = ctypes.c_long
+    k = fn(n, _p(c), arr(ds), arr(ns_), arr(cs), len(problems), _p(refs), _p(counts), _p(srcs), _p(xyz), _p(nrm),
+           _p(col), ctypes.c_long(cap))
     return xyz[:k].copy(), nrm[:k].copy(), col[:k].copy()
 
 

@@ -1,7 +1,9 @@
 /*
- * C entry point of the fusion checker (oracle/_ref/libfusion_ref.so): runs
- * the reference's own RunFusion (HPM-MVS/main.cpp:502-633, compiled from the
- * reference tree by oracle/Makefile) on a dense folder.
+ * C entry point of the fusion checkers: runs the reference's own RunFusion on
+ * a dense folder, HPM-MVS/main.cpp:502-633 in oracle/_ref/libfusion_ref.so,
+ * the ACMM+NESP variant's (ACMM+NESP/windows/main.cpp:154-297) in
+ * oracle/_ref/libfusion_acmm_ref.so (both compiled from the reference tree by
+ * oracle/Makefile).
  *
  * TEST INFRASTRUCTURE ONLY.
  */
@@ -10,7 +12,8 @@
 void RunFusion(std::string &dense_folder, const std::vector<Problem> &problems, bool geom_consistency);
 
 /* problems as in hpm_run_scene: ref_ids[n], src_counts[n], src_ids[n][32];
- * writes dense_folder/HPM/HPM_model.ply as the reference does.  The
+ * writes the PLY as the reference does (dense_folder/HPM/HPM_model.ply, or
+ * dense_folder/ACMM_NESP/ACMM_NESP_model.ply for the variant).  The
  * reference's progress lines go nowhere. */
 extern "C" int ref_run_fusion(const char *dense_folder, int n, const int *ref_ids, const int *src_counts,
                               const int *src_ids, int geom_consistency)

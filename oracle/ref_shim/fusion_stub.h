@@ -3,7 +3,9 @@
  * 502-633) and the HPM.cpp helpers it calls (ReadCamera, readDepthDmb,
  * readNormalDmb, RescaleImageAndCamera, Get3DPointonWorld, ProjectonCamera,
  * GetAngle, StoreColorPlyFileBinaryPointCloud: HPM.cpp:135-456) compile on
- * the host without OpenCV or PCL.
+ * the host without OpenCV or PCL; likewise the ACMM+NESP variant's RunFusion
+ * (ACMM+NESP/windows/main.cpp:154-297) with its ACMM.cpp helpers
+ * (ACMM.cpp:137-422).
  *
  * TEST INFRASTRUCTURE ONLY: the library built from this header is the
  * checker of the fusion oracle (oracle/_ref/libfusion_ref.so), never the
@@ -77,6 +79,22 @@ struct Vec3f {
     float &operator[](int i) { return v[i]; }
     const float &operator[](int i) const { return v[i]; }
 };
+
+/* Element-wise sum, and division by a scalar as OpenCV's Vec does it
+ * (core/matx.hpp: a multiplication by the float reciprocal); used by the
+ * ACMM+NESP variant's RunFusion (ACMM+NESP/windows/main.cpp:259, 275). */
+inline Vec3f operator+(const Vec3f &a, const Vec3f &b)
+{
+    Vec3f r;
+    for (int i = 0; i < 3; ++i) r.v[i] = a.v[i] + b.v[i];
+    return r;
+}
+inline Vec3f &operator/=(Vec3f &a, float alpha)
+{
+    const float ialpha = 1.f / alpha;
+    for (int i = 0; i < 3; ++i) a.v[i] = a.v[i] * ialpha;
+    return a;
+}
 
 struct Size {
     int width, height;

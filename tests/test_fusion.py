@@ -78,3 +78,21 @@ def test_ply_layout(tmp_path):
     np.testing.assert_array_equal(rec["xyz"], [[1, 2, 3], [0, 0, 0], [0, 0, 0]])  # non-finite -> origin
     np.testing.assert_array_equal(rec["n"], nrm)
     np.testing.assert_array_equal(rec["rgb"], bgr[:, ::-1])  # red, green, blue
+
+
+@pytest.mark.parametrize("acmm", [False, True])
+def test_product_ordered_pass_matches_oracle(acmm):
+    """hpm_fuse_pass, the host half of hpm_fuse (acmm False) and of
+    hpm_fuse_acmm (acmm True), on the oracle's pairs (or_fuse_pairs, the
+    restatement of their GPU pass) against the oracle's whole RunFusion
+    (or_fuse / or_fuse_acmm, each pinned to the reference's own code in
+    tests/test_fusion_reference.py): the same points in the same order, bit
+    for bit; colour bytes as the reference's PLY writer truncates them."""
+    sc, depths, normals, colors, problems = fusion_inputs(3, 160, 120, 5, noise=0.002)
+    pairs = [orc.fuse_pairs(sc.cams, depths, normals, ref, srcs) for ref, srcs in problems]
+    xyz, nrm, bgr = hb.fuse_pass(sc.cams, depths, normals, colors, problems, pairs, acmm=acmm)
+    oxyz, onrm, ocol = orc.fuse(sc.cams, depths, normals, colors, problems, acmm=acmm)
+    assert len(xyz) == len(oxyz) and len(xyz) > 1000, (len(xyz), len(oxyz))
+    np.testing.assert_array_equal(xyz, oxyz)
+    np.testing.assert_array_equal(nrm, onrm)
+    np.testing.assert_array_equal(bgr, ocol.astype(np.int32).astype(np.uint8))

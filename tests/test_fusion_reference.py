@@ -21,6 +21,7 @@ import oracle as orc
 import synthetic as syn
 
 LIB = os.path.join(ROOT, "oracle", "_ref", "libfusion_ref.so")
+LIB_ACMM = os.path.join(ROOT, "oracle", "_ref", "libfusion_acmm_ref.so")
 pytestmark = pytest.mark.skipif(not os.path.exists(LIB), reason="reference fusion checker not built "
                                                                  "(make -C oracle fusion REF_DIR=...)")
 
@@ -51,7 +52,7 @@ def _read_ply(path):
     return np.frombuffer(body, dt, count=n)
 
 
-def _scene_folder(tmp_path, geom, seed):
+def _scene_folder(tmp_path, geom, seed, tree="HPM"):
     sc = syn.make_scene(seed, 120, 90, 6, n_planes=5, n_spheres=1)
     folder = str(tmp_path / f"scene{seed}_{geom}")
     syn.write_dense_folder(sc, folder)  # cameras and pair.txt (the images are replaced below)
@@ -68,7 +69,7 @@ def _scene_folder(tmp_path, geom, seed):
         depths.append(d.astype(np.float32))
         normals.append(n.astype(np.float32))
         colors.append(rng.integers(0, 256, d.shape + (3,), dtype=np.uint8))
-        out = os.path.join(folder, "HPM", f"2333_{v:08d}")
+        out = os.path.join(folder, tree, f"2333_{v:08d}")
         os.makedirs(out, exist_ok=True)
         _write_dmb(os.path.join(out, "depths_geom.dmb" if geom else "depths.dmb"), depths[-1])
         _write_dmb(os.path.join(out, "normals.dmb"), normals[-1])
@@ -77,10 +78,8 @@ def _scene_folder(tmp_path, geom, seed):
     return sc, folder, depths, normals, colors, problems
 
 
-@pytest.mark.parametrize("geom", [0, 1])
-def test_oracle_fusion_matches_the_reference_run_fusion(tmp_path, geom):
-    sc, folder, depths, normals, colors, problems = _scene_folder(tmp_path, geom, seed=3 + geom)
-    lib = ctypes.CDLL(LIB)
+def _run_reference(lib_path, folder, problems, geom):
+    lib = ctypes.CDLL(lib_path)
     refs = np.array([p[0] for p in problems], np.int32)
     counts = np.array([len(p[1]) for p in problems], np.int32)
     srcs = np.zeros((len(problems), 32), np.int32)
@@ -89,8 +88,32 @@ def test_oracle_fusion_matches_the_reference_run_fusion(tmp_path, geom):
     rc = lib.ref_run_fusion(folder.encode(), len(problems), refs.ctypes.data_as(ctypes.c_void_p),
                             counts.ctypes.data_as(ctypes.c_void_p), srcs.ctypes.data_as(ctypes.c_void_p), geom)
     assert rc == 0
+
+
+@pytest.mark.parametrize("geom", [0, 1])
+def test_oracle_fusion_matches_the_reference_run_fusion(tmp_path, geom):
+    sc, folder, depths, normals, colors, problems = _scene_folder(tmp_path, geom, seed=3 + geom)
+    _run_reference(LIB, folder, problems, geom)
     ref = _read_ply(os.path.join(folder, "HPM", "HPM_model.ply"))
     xyz, nrm, col = orc.fuse(sc.cams, depths, normals, colors, problems)
+    _check(ref, xyz, nrm, col)
+
+
+@pytest.mark.skipif(not os.path.exists(LIB_ACMM), reason="reference ACMM+NESP fusion checker not built")
+def test_oracle_fusion_matches_the_reference_run_fusion_acmm(tmp_path):
+    """The ACMM+NESP variant's RunFusion (ACMM+NESP/windows/main.cpp:154-297,
+    always from depths_geom.dmb): at least 2 agreeing sources, and the mean
+    of the point, normal and colour with the agreeing source pixels'."""
+    sc, folder, depths, normals, colors, problems = _scene_folder(tmp_path, 1, seed=9, tree="ACMM_NESP")
+    _run_reference(LIB_ACMM, folder, problems, 1)
+    ref = _read_ply(os.path.join(folder, "ACMM_NESP", "ACMM_NESP_model.ply"))
+    xyz, nrm, col = orc.fuse(sc.cams, depths, normals, colors, problems, acmm=True)
+    _check(ref, xyz, nrm, col)
+    # the variant's rule is another one than HPM-MVS's
+    assert len(xyz) != len(orc.fuse(sc.cams, depths, normals, colors, problems)[0])
+
+
+def _check(ref, xyz, nrm, col):
     assert len(ref) > 1000 and len(ref) == len(xyz), (len(ref), len(xyz))
     # the reference's writer replaces non-finite coordinates by 0 (HPM.cpp:433-437)
     bad = ~(np.isfinite(xyz).all(1))

@@ -50,3 +50,17 @@ def test_fuse_matches_oracle_on_patchmatch_maps():
     ref = orc.fuse(sc.cams, d, n, colors, problems)
     assert len(ref[0]) > 0.03 * nv * 200 * 150
     _compare(prod, ref)
+
+
+def test_fuse_acmm_matches_oracle():
+    """hpm_fuse_acmm, the ACMM+NESP variant's RunFusion (at least 2 agreeing
+    sources; point, normal and colour averaged), against or_fuse_acmm, which
+    tests/test_fusion_reference.py pins to the variant's own code; colour
+    bytes truncated as the variant's PLY writer does."""
+    sc, depths, normals, colors, problems = fusion_inputs(3, 160, 120, 5, noise=0.004)
+    xyz, nrm, bgr = hb.fuse(sc.cams, depths, normals, colors, problems, acmm=True)
+    oxyz, onrm, ocol = orc.fuse(sc.cams, depths, normals, colors, problems, acmm=True)
+    assert len(oxyz) > 1000
+    _compare((xyz, nrm, bgr), (oxyz, onrm, ocol.astype(np.int32).astype(np.float32)))
+    # fewer points than the HPM-MVS rule gives on the same maps: two sources needed
+    assert len(xyz) < len(hb.fuse(sc.cams, depths, normals, colors, problems)[0])
