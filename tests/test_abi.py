@@ -97,6 +97,9 @@ def test_null_context_is_an_argument_error():
     assert L.hpm_get_result(None, None, None) == -1
     assert L.hpm_create(None, 0) == -1
     assert L.hpm_run_scene_acmm(None, 2, None, None, 2, None, None, None, None, None, None, None) == -1
+    # the fusion's host pass checks its arguments before touching any
+    assert L.hpm_fuse_pass(2, 1, None, None, None, None, 0, None, None, None, None, None, None, None, None, None,
+                           ctypes.c_longlong(0), None) == -1
 
 
 @pytest.mark.skipif(gpu_available(), reason="checks the behaviour on a machine without a GPU")
