@@ -527,6 +527,8 @@ def run_ours(args, dist):
                      "half_step_ms": prop_ms_step / max(half_steps, 1), "half_steps_per_step": half_steps,
                      "propagate_ms_per_step": prop_ms_step,
                      "propagate_share": prop_ms_step / plain["ms_per_step"],
+                     # PM-only rate: the plain form's depth pixels per second of its half-step kernels
+                     "pm_only_mpix_per_s": nv * npx / (max(prop_ms_step, 1e-9) * 1e-3) / 1e6,
                      "ncc_windows_per_step": ncc_half, "geom_terms_per_step": plain["geom_terms"],
                      "flops_per_ncc_window": TAPS * NCC_FLOPS_PER_TAP + FLOPS_PER_HYP_VIEW},
         "plain_form": form_summary(plain) | {"step": plain_step},
