@@ -129,3 +129,17 @@ def test_hierarchy_init_matches_reference():
         d = d[np.isfinite(d)]
         assert d.mean() <= 1e-4 and (d > 1e-3).mean() <= 0.01 and d.max() <= 2e-2, (d.mean(), d.max())
     assert (ov == g["views"]).mean() >= 0.98
+
+
+def test_three_scales():
+    """Two halvings (32, 64, then 128 pixels on the longer side): the
+    hierarchy pass runs at two finer scales, each from the previous scale's
+    geometric maps."""
+    sc = syn.make_scene(7, 128, 96, 4, n_planes=4)
+    imgs = [i.astype(np.float32) for i in sc.images]
+    pairs = [(v, [int(s) for s in sc.pairs[v][1]]) for v in range(4)]
+    d, n, c, sizes = acmm_flow.run_scene(imgs, sc.cams, pairs, seed=2, size_bound=32)
+    assert sizes == [[32] * 4, [64] * 4, [128] * 4]
+    assert all(x.shape == (96, 128) for x in d)
+    acc = [syn.depth_accuracy(d[v], sc.gt_depth[v]) for v in range(4)]
+    assert np.mean(acc) > 0.4, acc
